@@ -1,0 +1,130 @@
+"""ctypes mirror of ``include/ggems_b200.h`` (the B200 transport C ABI).
+
+The structures here must match the header field for field; tests check the
+sizes against the compiled library.  Array-valued inputs are numpy arrays
+kept alive by the Python objects that own the structures.
+"""
+
+import ctypes as C
+
+import numpy as np
+
+GG_MAXIMUM_PARTICLES = 1048576
+GG_MAX_LOOP = 100
+GG_COMPTON_SCATTERING = 0
+GG_PHOTOELECTRIC_EFFECT = 1
+GG_RAYLEIGH_SCATTERING = 2
+GG_SOLID_VOXELIZED = 0
+GG_SOLID_BOX = 1
+GG_SOLID_MESHED = 2
+GG_SOURCE_XRAY = 0
+GG_SOURCE_VOXELIZED = 1
+
+STATUS = {0: "GG_OK", 1: "GG_ERROR_INVALID_ARGUMENT", 2: "GG_ERROR_CUDA", 3: "GG_ERROR_NO_DEVICE",
+          4: "GG_ERROR_OUT_OF_MEMORY", 5: "GG_ERROR_STATE", 6: "GG_ERROR_TIMEOUT"}
+
+FP = C.POINTER(C.c_float)
+IP = C.POINTER(C.c_int32)
+UP = C.POINTER(C.c_uint8)
+
+
+class gg_obb(C.Structure):
+    _fields_ = [("matrix", C.c_float * 16), ("border_min", C.c_float * 3), ("border_max", C.c_float * 3)]
+
+
+class gg_physics_tables(C.Structure):
+    _fields_ = [("number_of_bins", C.c_int32), ("number_of_materials", C.c_int32),
+                ("number_of_processes", C.c_int32), ("process_id", C.c_int32 * 3),
+                ("energy_bins", FP), ("cross_sections", FP), ("rayleigh_per_atom", FP),
+                ("density", FP), ("photon_energy_cut", FP), ("number_of_elements", IP),
+                ("element_offset", IP), ("atomic_number", UP), ("atomic_number_density", FP),
+                ("total_elements", C.c_int32)]
+
+
+class gg_solid(C.Structure):
+    _fields_ = [("type", C.c_int32), ("navigator", C.c_int32), ("obb", gg_obb), ("threshold", C.c_float),
+                ("number_of_voxels", C.c_int32 * 3), ("voxel_sizes", C.c_float * 3), ("labels", UP),
+                ("virtual_element_number", C.c_int32 * 3), ("box_size", C.c_float * 3),
+                ("histogram", C.c_int32), ("scatter_histogram", C.c_int32), ("dose_map", C.c_int32)]
+
+
+class gg_dose_map(C.Structure):
+    _fields_ = [("size_of_dosels", C.c_float * 3), ("inv_size_of_dosels", C.c_float * 3),
+                ("border_min", C.c_float * 3), ("border_max", C.c_float * 3),
+                ("number_of_dosels", C.c_int32 * 3), ("total_number_of_dosels", C.c_int32),
+                ("slice_number_of_dosels", C.c_int32), ("record_edep_squared", C.c_int32),
+                ("record_hit", C.c_int32), ("record_photon_tracking", C.c_int32)]
+
+
+class gg_scene(C.Structure):
+    _fields_ = [("number_of_tables", C.c_int32), ("tables", C.POINTER(gg_physics_tables)),
+                ("number_of_solids", C.c_int32), ("solids", C.POINTER(gg_solid)),
+                ("number_of_dose_maps", C.c_int32), ("dose_maps", C.POINTER(gg_dose_map)),
+                ("number_of_histograms", C.c_int32), ("histogram_sizes", IP)]
+
+
+class gg_source(C.Structure):
+    _fields_ = [("type", C.c_int32), ("particle_type", C.c_int32), ("matrix", C.c_float * 16),
+                ("beam_aperture", C.c_float), ("focal_spot_size", C.c_float * 3),
+                ("number_of_energy_bins", C.c_int32), ("energy_spectrum", FP), ("energy_cdf", FP),
+                ("is_interp", C.c_int32), ("number_of_voxels", C.c_int32 * 3), ("voxel_sizes", C.c_float * 3),
+                ("border_min", C.c_float * 3), ("number_of_activity_bins", C.c_int64),
+                ("activity_index", IP), ("activity_cdf", FP)]
+
+
+class gg_particle_buffers(C.Structure):
+    _fields_ = [("E", FP), ("px", FP), ("py", FP), ("pz", FP), ("dx", FP), ("dy", FP), ("dz", FP),
+                ("status", C.POINTER(C.c_int8)), ("scatter", C.POINTER(C.c_int8)), ("solid_id", IP)]
+
+
+class gg_tally_buffers(C.Structure):
+    _fields_ = [("histograms", C.POINTER(IP)), ("edep", C.POINTER(C.POINTER(C.c_double))),
+                ("edep_squared", C.POINTER(C.POINTER(C.c_double))), ("hit", C.POINTER(IP)),
+                ("photon_tracking", C.POINTER(IP))]
+
+
+def ptr(array, ctype):
+    """Pointer to a contiguous numpy array (None -> NULL)."""
+    if array is None:
+        return C.cast(None, C.POINTER(ctype))
+    assert array.flags["C_CONTIGUOUS"]
+    return array.ctypes.data_as(C.POINTER(ctype))
+
+
+class Particles:
+    """Host SoA buffers for the final per-slot particle states."""
+
+    FIELDS = ("E", "px", "py", "pz", "dx", "dy", "dz")
+
+    def __init__(self, n):
+        self.n = n
+        for f in self.FIELDS:
+            setattr(self, f, np.zeros(n, np.float32))
+        self.status = np.zeros(n, np.int8)
+        self.scatter = np.zeros(n, np.int8)
+        self.solid_id = np.zeros(n, np.int32)
+        self.struct = gg_particle_buffers(*[ptr(getattr(self, f), C.c_float) for f in self.FIELDS],
+                                          ptr(self.status, C.c_int8), ptr(self.scatter, C.c_int8),
+                                          ptr(self.solid_id, C.c_int32))
+
+
+class Tallies:
+    """Host tally buffers matching a scene's histograms and dose maps."""
+
+    def __init__(self, histogram_sizes, dose_sizes):
+        self.histograms = [np.zeros(n, np.int32) for n in histogram_sizes]
+        self.edep = [np.zeros(n, np.float64) for n in dose_sizes]
+        self.edep_squared = [np.zeros(n, np.float64) for n in dose_sizes]
+        self.hit = [np.zeros(n, np.int32) for n in dose_sizes]
+        self.photon_tracking = [np.zeros(n, np.int32) for n in dose_sizes]
+
+        def arr(lst, ctype):
+            a = (C.POINTER(ctype) * max(len(lst), 1))(*[ptr(x, ctype) for x in lst])
+            return C.cast(a, C.POINTER(C.POINTER(ctype))), a
+
+        self._h, self._hk = arr(self.histograms, C.c_int32)
+        self._e, self._ek = arr(self.edep, C.c_double)
+        self._e2, self._e2k = arr(self.edep_squared, C.c_double)
+        self._hit, self._hitk = arr(self.hit, C.c_int32)
+        self._pt, self._ptk = arr(self.photon_tracking, C.c_int32)
+        self.struct = gg_tally_buffers(self._h, self._e, self._e2, self._hit, self._pt)

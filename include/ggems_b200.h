@@ -1,0 +1,244 @@
+/*
+ * ggems_b200.h - C ABI of the B200 photon-transport layer.
+ *
+ * This is the thin device layer that replaces GGEMS's OpenCL manager and
+ * command-queue plumbing (include/GGEMS/global/GGEMSOpenCLManager.hh:384-495,
+ * src/global/GGEMSOpenCLManager.cc:836-1046) for the photon hot path.  The C++
+ * host classes (GGEMS, GGEMSXRaySource, GGEMSVoxelizedPhantom, GGEMSCTSystem,
+ * GGEMSDosimetryCalculator, ...) build a scene description out of plain
+ * arrays and call these entry points; nothing here exposes CUDA or torch
+ * types.  Every function returns a gg_status code; gg_last_error() gives the
+ * message of the last failure on the calling thread.
+ *
+ * Units are GGEMS's internal units (include/GGEMS/tools/GGEMSSystemOfUnits.hh):
+ * mm, MeV, rad, g = 6.241509704e21.
+ */
+#ifndef GGEMS_B200_H
+#define GGEMS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define GG_API __attribute__((visibility("default")))
+#else
+#define GG_API
+#endif
+
+/* Particle slots per batch: GGEMS's MAXIMUM_PARTICLES (CMakeLists.txt:128-132). */
+#define GG_MAXIMUM_PARTICLES 1048576
+/* Limits of the reference's fixed-size tables. */
+#define GG_MAX_CROSS_SECTION_BINS 2048 /* GGEMSProcessConstants.hh MAX_CROSS_SECTION_TABLE_NUMBER_BINS */
+#define GG_MAX_MATERIALS 255           /* GGEMSMaterialTables.hh:44-77 */
+#define GG_MAX_LOOP 100                /* src/global/GGEMS.cc:330 */
+
+typedef enum gg_status {
+  GG_OK = 0,
+  GG_ERROR_INVALID_ARGUMENT = 1,
+  GG_ERROR_CUDA = 2,
+  GG_ERROR_NO_DEVICE = 3,
+  GG_ERROR_OUT_OF_MEMORY = 4,
+  GG_ERROR_STATE = 5,
+  GG_ERROR_TIMEOUT = 6
+} gg_status;
+
+/* Photon process identifiers (include/GGEMS/physics/GGEMSProcessConstants.hh). */
+#define GG_COMPTON_SCATTERING 0
+#define GG_PHOTOELECTRIC_EFFECT 1
+#define GG_RAYLEIGH_SCATTERING 2
+#define GG_TRANSPORTATION 99
+
+/* Particle status (include/GGEMS/physics/GGEMSParticleConstants.hh). */
+#define GG_ALIVE 0
+#define GG_DEAD 1
+
+/* Oriented bounding box: GGEMSOBB (include/GGEMS/geometries/GGEMSPrimitiveGeometries.hh:41-46).
+ * matrix = GGfloat44, 4 rows of 4 floats (row-major), local -> global. */
+typedef struct gg_obb {
+  float matrix[16];
+  float border_min[3];
+  float border_max[3];
+} gg_obb;
+
+/* Per-navigator physics tables: the part of GGEMSParticleCrossSections
+ * (include/GGEMS/physics/GGEMSParticleCrossSections.hh:40-58) and of
+ * GGEMSMaterialTables (include/GGEMS/materials/GGEMSMaterialTables.hh:41-77)
+ * that photon transport reads. */
+typedef struct gg_physics_tables {
+  int32_t number_of_bins;
+  int32_t number_of_materials;
+  int32_t number_of_processes;          /* activated photon processes */
+  int32_t process_id[3];                /* photon_cs_id_: AddProcess order */
+  const float* energy_bins;             /* [number_of_bins] MeV, log spaced */
+  const float* cross_sections;          /* [3][number_of_materials*number_of_bins] mm^-1,
+                                           indexed [process][bin + number_of_bins*material] */
+  const float* rayleigh_per_atom;       /* [101*number_of_bins] mm^2, [bin + number_of_bins*Z];
+                                           NULL when Rayleigh is not activated */
+  const float* density;                 /* [number_of_materials] internal units */
+  const float* photon_energy_cut;       /* [number_of_materials] MeV */
+  const int32_t* number_of_elements;    /* [number_of_materials] */
+  const int32_t* element_offset;        /* [number_of_materials] index into the element arrays */
+  const uint8_t* atomic_number;         /* [total_elements] */
+  const float* atomic_number_density;   /* [total_elements] atoms / mm^3 */
+  int32_t total_elements;
+} gg_physics_tables;
+
+typedef enum gg_solid_type {
+  GG_SOLID_VOXELIZED = 0,
+  GG_SOLID_BOX = 1,
+  GG_SOLID_MESHED = 2
+} gg_solid_type;
+
+/* One solid.  Solids are listed in GGEMS's registration order, which is
+ * also the order of the FindSolid / ProjectToSolid / TrackThroughSolid loops
+ * (src/navigators/GGEMSNavigatorManager.cc, GGEMSNavigator.cc:320-530). */
+typedef struct gg_solid {
+  int32_t type;                 /* gg_solid_type */
+  int32_t navigator;            /* index of this solid's gg_physics_tables */
+  gg_obb obb;
+  float threshold;              /* navigator energy threshold (MeV) */
+  /* voxelized solid: GGEMSVoxelizedSolidData */
+  int32_t number_of_voxels[3];
+  float voxel_sizes[3];
+  const uint8_t* labels;        /* [nx*ny*nz] material index, x fastest */
+  /* solid box (CT detector module): GGEMSSolidBoxData */
+  int32_t virtual_element_number[3];
+  float box_size[3];
+  int32_t histogram;            /* index of the interaction histogram, -1: none */
+  int32_t scatter_histogram;    /* index of the scatter histogram, -1: none */
+  /* dosimetry */
+  int32_t dose_map;             /* index into gg_scene.dose_maps, -1: none */
+} gg_solid;
+
+/* Dose map: GGEMSDoseParams (include/GGEMS/navigators/GGEMSDoseParams.hh:40-49)
+ * plus which optional tallies are recorded. */
+typedef struct gg_dose_map {
+  float size_of_dosels[3];
+  float inv_size_of_dosels[3];
+  float border_min[3];
+  float border_max[3];
+  int32_t number_of_dosels[3];
+  int32_t total_number_of_dosels;
+  int32_t slice_number_of_dosels;
+  int32_t record_edep_squared;
+  int32_t record_hit;
+  int32_t record_photon_tracking;
+} gg_dose_map;
+
+typedef struct gg_scene {
+  int32_t number_of_tables;
+  const gg_physics_tables* tables;
+  int32_t number_of_solids;
+  const gg_solid* solids;
+  int32_t number_of_dose_maps;
+  const gg_dose_map* dose_maps;
+  int32_t number_of_histograms;
+  const int32_t* histogram_sizes;   /* elements per histogram */
+} gg_scene;
+
+typedef enum gg_source_type {
+  GG_SOURCE_XRAY = 0,
+  GG_SOURCE_VOXELIZED = 1
+} gg_source_type;
+
+/* A primary source.  X-ray cone source: GGEMSXRaySource
+ * (src/sources/GGEMSXRaySource.cc:100-148, src/kernels/GetPrimariesGGEMSXRaySource.cl). */
+typedef struct gg_source {
+  int32_t type;                  /* gg_source_type */
+  int32_t particle_type;         /* 0 photon */
+  float matrix[16];              /* source frame, GGfloat44 */
+  float beam_aperture;           /* rad */
+  float focal_spot_size[3];      /* mm */
+  int32_t number_of_energy_bins; /* n; spectrum and cdf hold n+1 values */
+  const float* energy_spectrum;  /* [n+1] MeV, last value repeated */
+  const float* energy_cdf;       /* [n+1], cdf[0] = 0, cdf[n] = 1 */
+  int32_t is_interp;             /* linear interpolation inside the cdf bin */
+  /* voxelized source (GGEMSVoxelizedSource): activity CDF over active voxels */
+  int32_t number_of_voxels[3];
+  float voxel_sizes[3];
+  float border_min[3];
+  int64_t number_of_activity_bins;  /* active voxels */
+  const int32_t* activity_index;    /* [number_of_activity_bins] voxel index */
+  const float* activity_cdf;        /* [number_of_activity_bins] */
+} gg_source;
+
+/* Final per-slot particle state (the photon part of GGEMSPrimaryParticles,
+ * include/GGEMS/physics/GGEMSPrimaryParticles.hh:40-68), host SoA buffers. */
+typedef struct gg_particle_buffers {
+  float* E;
+  float* px;
+  float* py;
+  float* pz;
+  float* dx;
+  float* dy;
+  float* dz;
+  int8_t* status;
+  int8_t* scatter;
+  int32_t* solid_id;
+} gg_particle_buffers;
+
+/* Host tally buffers, one pointer per histogram / dose map (NULL to skip). */
+typedef struct gg_tally_buffers {
+  int32_t** histograms;
+  double** edep;
+  double** edep_squared;
+  int32_t** hit;
+  int32_t** photon_tracking;
+} gg_tally_buffers;
+
+typedef struct gg_context gg_context;
+
+/* ---- device selection and context (replaces GGEMSOpenCLManager) ---- */
+GG_API int gg_device_count(int32_t* count);
+GG_API int gg_context_create(int32_t device_index, gg_context** context);
+GG_API int gg_context_destroy(gg_context* context);
+GG_API const char* gg_last_error(void);
+
+/* ---- random streams (GGEMSPseudoRandomGenerator) ----
+ * states: 5 arrays of number_of_slots uint32 (prng_state_1_ .. prng_state_5_),
+ * stored one after the other. */
+GG_API int gg_set_random_states(gg_context* context, const uint32_t* states, int64_t number_of_slots);
+GG_API int gg_get_random_states(gg_context* context, uint32_t* states, int64_t number_of_slots);
+/* JKISS seeding of GGEMSPseudoRandomGenerator::InitializeSeeds
+ * (src/randoms/GGEMSPseudoRandomGenerator.cc:140-167): slot j takes four
+ * consecutive std::mt19937(seed) outputs, starting after skip_slots*4 draws. */
+GG_API int gg_seed_random_states(uint32_t* states, int64_t number_of_slots, uint32_t seed, int64_t skip_slots);
+
+/* ---- scene upload and tallies ---- */
+GG_API int gg_upload_scene(gg_context* context, const gg_scene* scene);
+GG_API int gg_reset_tallies(gg_context* context);
+GG_API int gg_read_tallies(gg_context* context, gg_tally_buffers* tallies);
+GG_API int gg_read_particles(gg_context* context, gg_particle_buffers* particles, int64_t number_of_slots);
+
+/* ---- transport ----
+ * Runs number_of_particles primaries of one source through the scene,
+ * split into batches exactly as GGEMSSource::OrganizeParticlesInBatch
+ * (src/sources/GGEMSSource.cc:379-426) and GGEMS::RunOnDevice
+ * (src/global/GGEMS.cc:303-363): particle i of every batch uses random
+ * slot i.  Asynchronous on the context's stream. */
+GG_API int gg_run_source(gg_context* context, const gg_source* source, uint64_t number_of_particles);
+GG_API int gg_synchronize(gg_context* context);
+
+/* Batch plan of GGEMSSource::OrganizeParticlesInBatch for one device.
+ * Writes at most max_batches sizes; returns the number of batches in *count. */
+GG_API int gg_batch_plan(uint64_t number_of_particles, uint64_t* batch_sizes, int64_t max_batches, int64_t* count);
+
+/* ---- dose finalisation (ComputeDoseGGEMSVoxelizedSolid.cl) ----
+ * Converts the edep tally of dose_map (recorded inside solid) into Gy and the
+ * relative uncertainty of Ma et al.; outputs are host arrays of
+ * total_number_of_dosels floats (uncertainty may be NULL). */
+GG_API int gg_compute_dose(gg_context* context, int32_t dose_map, int32_t solid, float scale_factor,
+                           int32_t is_water_reference, float minimum_density, float* dose, float* uncertainty);
+
+/* ---- timing of the last gg_run_source (device time, ms) and launch count ---- */
+GG_API int gg_last_run_stats(gg_context* context, float* milliseconds, int64_t* kernel_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GGEMS_B200_H */

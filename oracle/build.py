@@ -1,0 +1,87 @@
+"""Build recipe for the oracle (test infrastructure only).
+
+* ``oracle/_build/libgg_oracle.so`` -- the CPU restatement (gg_oracle.cc),
+  built from this repository alone; it is the checker the GPU tests use.
+* ``oracle/_ref/libgg_ref.so`` -- GGEMS's own device kernels
+  (``src/kernels/*.cl``) compiled straight from a reference checkout through
+  ``oracle/ref_shim/ocl_shim.hh``, plus ``gg_ref_driver.cc``.  Only built when
+  the checkout exists; it pins the restatement.
+
+Both use ``-ffp-contract=off`` (no fused multiply-add) so float arithmetic
+rounds exactly as written.
+
+Usage: python oracle/build.py [--ref /path/to/reference]
+"""
+
+import argparse
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+BUILD = os.path.join(HERE, "_build")
+REF_OUT = os.path.join(HERE, "_ref")
+DEFAULT_REFERENCE = "/root/reference"
+
+CXX = ["g++", "-std=c++20", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math"]
+
+# (kernel file, extra defines, symbol renames)
+REF_KERNELS = [
+    ("GetPrimariesGGEMSXRaySource", [], []),
+    ("GetPrimariesGGEMSVoxelizedSource", [], []),
+    ("ParticleSolidDistanceGGEMSVoxelizedSolid", [], []),
+    ("ParticleSolidDistanceGGEMSSolidBox", [], []),
+    ("ProjectToGGEMSVoxelizedSolid", [], []),
+    ("ProjectToGGEMSSolidBox", [], []),
+    ("TrackThroughGGEMSVoxelizedSolid", [], []),
+    ("TrackThroughGGEMSVoxelizedSolid", ["DOSIMETRY"],
+     ["track_through_ggems_voxelized_solid=track_through_ggems_voxelized_solid_dosimetry"]),
+    ("TrackThroughGGEMSSolidBox", ["HISTOGRAM"], []),
+    ("IsAlive", [], []),
+]
+
+
+def run(cmd):
+    subprocess.check_call(cmd)
+
+
+def build_oracle():
+    os.makedirs(BUILD, exist_ok=True)
+    out = os.path.join(BUILD, "libgg_oracle.so")
+    run(CXX + ["-shared", "-I" + os.path.join(ROOT, "include"), os.path.join(HERE, "gg_oracle.cc"),
+               os.path.join(HERE, "gg_oracle_tables.cc"), "-o", out, "-lpthread"])
+    return out
+
+
+def build_ref(reference):
+    if not os.path.isdir(os.path.join(reference, "src", "kernels")):
+        return None
+    os.makedirs(REF_OUT, exist_ok=True)
+    shim = os.path.join(HERE, "ref_shim")
+    common = CXX + ["-w", "-Wno-narrowing", "-fpermissive", "-include", os.path.join(shim, "ocl_shim.hh"),
+                    "-I" + shim, "-I" + os.path.join(reference, "include"), "-I" + os.path.join(ROOT, "include")]
+    objs = []
+    for name, defines, renames in REF_KERNELS:
+        tag = name + ("_" + "_".join(defines) if defines else "")
+        obj = os.path.join(REF_OUT, tag + ".o")
+        cmd = common + ["-D" + d for d in defines] + ["-D" + r for r in renames]
+        run(cmd + ["-x", "c++", "-c", os.path.join(reference, "src", "kernels", name + ".cl"), "-o", obj])
+        objs.append(obj)
+    drv = os.path.join(REF_OUT, "gg_ref_driver.o")
+    run(common + ["-c", os.path.join(HERE, "gg_ref_driver.cc"), "-o", drv])
+    out = os.path.join(REF_OUT, "libgg_ref.so")
+    run(["g++", "-shared", "-o", out, drv] + objs + ["-lpthread"])
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default=DEFAULT_REFERENCE)
+    args = ap.parse_args()
+    print(build_oracle())
+    print(build_ref(args.ref))
+
+
+if __name__ == "__main__":
+    sys.exit(main())

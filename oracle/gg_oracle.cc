@@ -1,0 +1,720 @@
+// CPU oracle for the GGEMS photon path -- TEST INFRASTRUCTURE ONLY.
+//
+// A plain C++ restatement of GGEMS v1.3's photon transport (sources, solid
+// navigation, Compton / photoelectric / Rayleigh sampling, dose and CT
+// histogram tallies), one history at a time per random slot.  It exists to
+// check the CUDA product against; only tests/, __graft_entry__.smoke() and
+// bench.py's cpu_baseline leg load it, and the product never links it.
+//
+// Each function cites the reference file:line it follows.  Arithmetic is
+// kept in the reference's order and precision (float unless the reference
+// uses double); build with -ffp-contract=off so a*b+c is never fused.
+//
+// The restatement is pinned against the reference's own kernels, compiled
+// from the reference checkout through oracle/ref_shim (oracle/_ref), by
+// tests/test_oracle_pin.py.
+#include <atomic>
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "ggems_b200.h"
+
+namespace {
+
+constexpr float kTwoPi = 6.283185307179586f;            // GGEMSConstants.hh:39
+constexpr float kElectronMassC2 = 0.510998910f;          // GGEMSConstants.hh:52
+constexpr float kGeometryTolerance = 5.0e-04f;           // GGEMSGeometryConstants.hh:39
+constexpr float kEpsilon6 = 1.0e-06f;                    // GGEMSGeometryConstants.hh:38
+constexpr float kOutOfWorld = FLT_MAX;                   // GGEMSParticleConstants.hh:44
+constexpr int8_t kNoProcess = 99;                        // GGEMSProcessConstants.hh:37
+constexpr float kRayleighFactor = 32526509815670243328.0f;  // GGEMSRayleighScatteringModels.hh:36
+
+struct V3 {
+  float x, y, z;
+};
+inline V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+inline V3 add(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline V3 sub(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+inline V3 mul(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+inline V3 divv(V3 a, V3 b) { return v3(a.x / b.x, a.y / b.y, a.z / b.z); }
+inline V3 scale(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
+inline float dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// normalize: v * (1 / sqrt(dot(v, v))), the convention fixed for OpenCL's builtin.
+inline V3 normalize3(V3 v) { return scale(v, 1.0f / std::sqrt(dot3(v, v))); }
+
+// Row-major GGfloat44 helpers (GGEMSMatrixOperations.hh:46-125).
+inline V3 mat_mul_point(const float* m, V3 p) {  // GGfloat44MultGGfloat3
+  return v3(m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3] * 1.0f,
+            m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7] * 1.0f,
+            m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11] * 1.0f);
+}
+inline V3 mat33_mul(const float* m, V3 p) {  // GGfloat33MultGGfloat3
+  return v3(m[0] * p.x + m[1] * p.y + m[2] * p.z, m[4] * p.x + m[5] * p.y + m[6] * p.z,
+            m[8] * p.x + m[9] * p.y + m[10] * p.z);
+}
+inline V3 mat33_transpose_mul(const float* m, V3 p) {  // GGfloat33TransposeMultGGfloat3
+  return v3(m[0] * p.x + m[4] * p.y + m[8] * p.z, m[1] * p.x + m[5] * p.y + m[9] * p.z,
+            m[2] * p.x + m[6] * p.y + m[10] * p.z);
+}
+// GGEMSReferentialTransformation.hh:80-141
+inline V3 global_to_local_position(const float* m, V3 p) {
+  return mat33_transpose_mul(m, v3(p.x - m[3], p.y - m[7], p.z - m[11]));
+}
+inline V3 local_to_global_position(const float* m, V3 p) { return mat_mul_point(m, p); }
+inline V3 global_to_local_direction(const float* m, V3 d) { return normalize3(mat33_transpose_mul(m, d)); }
+inline V3 local_to_global_direction(const float* m, V3 d) { return normalize3(mat33_mul(m, d)); }
+
+// RotateUnitZ (GGEMSReferentialTransformation.hh:44-70, CLHEP rotateUz).
+inline V3 rotate_unit_z(V3 v, V3 u) {
+  float up = u.x * u.x + u.y * u.y;
+  if (up > 0) {
+    up = std::sqrt(up);
+    float px = v.x, py = v.y, pz = v.z;
+    v.x = (u.x * u.z * px - u.y * py) / up + u.x * pz;
+    v.y = (u.y * u.z * px + u.x * py) / up + u.y * pz;
+    v.z = -up * px + u.z * pz;
+  } else if (u.z < 0.) {
+    v.x = -v.x;
+    v.z = -v.z;
+  }
+  return v;
+}
+
+// BinarySearch / LinearInterpolation (GGEMSMathAlgorithms.hh:46-86).
+inline int binary_search(float key, const float* a, int size) {
+  int low = 0, mid = 0, high = size - 1;
+  while (high - low > 1) {
+    mid = (high + low) / 2;
+    if (a[mid] == key) return mid;
+    if (a[mid] < key) low = mid;
+    else high = mid;
+  }
+  return low;
+}
+inline float linear_interpolation(float xa, float ya, float xb, float yb, float x) {
+  if (xa > xb) return yb;
+  if (xa >= x) return ya;
+  if (xb <= x) return yb;
+  return ya + (x - xa) * (yb - ya) / (xb - xa);
+}
+
+// Ray tracing (GGEMSRayTracing.hh:60-326).
+inline void safety_inside_aabb(V3& p, V3 mn, V3 mx) {
+  float a = std::fabs(p.x - mn.x), b = std::fabs(p.x - mx.x);
+  p.x = (a < kGeometryTolerance) ? mn.x + kGeometryTolerance : p.x;
+  p.x = (b < kGeometryTolerance) ? mx.x - kGeometryTolerance : p.x;
+  a = std::fabs(p.y - mn.y); b = std::fabs(p.y - mx.y);
+  p.y = (a < kGeometryTolerance) ? mn.y + kGeometryTolerance : p.y;
+  p.y = (b < kGeometryTolerance) ? mx.y - kGeometryTolerance : p.y;
+  a = std::fabs(p.z - mn.z); b = std::fabs(p.z - mx.z);
+  p.z = (a < kGeometryTolerance) ? mn.z + kGeometryTolerance : p.z;
+  p.z = (b < kGeometryTolerance) ? mx.z - kGeometryTolerance : p.z;
+}
+inline void safety_outside_aabb(V3& p, V3 mn, V3 mx) {
+  float a = std::fabs(p.x - mn.x), b = std::fabs(p.x - mx.x);
+  p.x = (a < kGeometryTolerance) ? mn.x - kGeometryTolerance : p.x;
+  p.x = (b < kGeometryTolerance) ? mx.x + kGeometryTolerance : p.x;
+  a = std::fabs(p.y - mn.y); b = std::fabs(p.y - mx.y);
+  p.y = (a < kGeometryTolerance) ? mn.y - kGeometryTolerance : p.y;
+  p.y = (b < kGeometryTolerance) ? mx.y + kGeometryTolerance : p.y;
+  a = std::fabs(p.z - mn.z); b = std::fabs(p.z - mx.z);
+  p.z = (a < kGeometryTolerance) ? mn.z - kGeometryTolerance : p.z;
+  p.z = (b < kGeometryTolerance) ? mx.z + kGeometryTolerance : p.z;
+}
+inline bool in_aabb(V3 p, V3 mn, V3 mx) {
+  if (p.x < (mn.x + kGeometryTolerance) || p.x > (mx.x - kGeometryTolerance)) return false;
+  if (p.y < (mn.y + kGeometryTolerance) || p.y > (mx.y - kGeometryTolerance)) return false;
+  if (p.z < (mn.z + kGeometryTolerance) || p.z > (mx.z - kGeometryTolerance)) return false;
+  return true;
+}
+inline float distance_to_aabb(V3 p, V3 d, V3 mn, V3 mx) {
+  float tmin = FLT_MIN, tmax = FLT_MAX, t1, t2, tmp;
+  if (std::fabs(d.x) < kEpsilon6) {
+    if (p.x < mn.x || p.x > mx.x) return kOutOfWorld;
+  } else {
+    float id = 1.0f / d.x;
+    tmin = (mn.x - p.x) * id;
+    tmax = (mx.x - p.x) * id;
+    if (tmin > tmax) { tmp = tmin; tmin = tmax; tmax = tmp; }
+    if (tmin > tmax) return kOutOfWorld;
+  }
+  if (std::fabs(d.y) < kEpsilon6) {
+    if (p.y < mn.y || p.y > mx.y) return kOutOfWorld;
+  } else {
+    float id = 1.0f / d.y;
+    t1 = (mn.y - p.y) * id;
+    t2 = (mx.y - p.y) * id;
+    if (t1 > t2) { tmp = t1; t1 = t2; t2 = tmp; }
+    if (t1 > tmin) tmin = t1;
+    if (t2 < tmax) tmax = t2;
+    if (tmin > tmax) return kOutOfWorld;
+  }
+  if (std::fabs(d.z) < kEpsilon6) {
+    if (p.z < mn.z || p.z > mx.z) return kOutOfWorld;
+  } else {
+    float id = 1.0f / d.z;
+    t1 = (mn.z - p.z) * id;
+    t2 = (mx.z - p.z) * id;
+    if (t1 > t2) { tmp = t1; t1 = t2; t2 = tmp; }
+    if (t1 > tmin) tmin = t1;
+    if (t2 < tmax) tmax = t2;
+    if (tmin > tmax) return kOutOfWorld;
+  }
+  if (tmin < 0.0f && (tmax < 0.0f || tmax == 0.0f)) return kOutOfWorld;
+  if ((tmax - tmin) < (2.0 * kGeometryTolerance)) return kOutOfWorld;  // double compare, as the reference
+  if (tmin <= kEpsilon6) return tmax;
+  return tmin;
+}
+
+inline V3 obb_min(const gg_obb& o) { return v3(o.border_min[0], o.border_min[1], o.border_min[2]); }
+inline V3 obb_max(const gg_obb& o) { return v3(o.border_max[0], o.border_max[1], o.border_max[2]); }
+
+// ---------------------------------------------------------------------------
+// JKISS32 (GGEMSKissEngine.hh:50-75).
+// ---------------------------------------------------------------------------
+struct Kiss {
+  uint32_t s1, s2, s3, s4, s5;
+  float uniform() {
+    s2 ^= (s2 << 5);
+    s2 ^= (s2 >> 7);
+    s2 ^= (s2 << 22);
+    int32_t t = static_cast<int32_t>(s3 + s4 + s5);
+    s3 = s4;
+    s5 = t < 0;
+    s4 = static_cast<uint32_t>(t) & 2147483647u;
+    s1 += 1411392427u;
+    return static_cast<float>((static_cast<float>(s1 + s2 + s4) / 4294967295.0) * (1.0f - 1.0f / (1 << 23)));
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Particle state: the photon fields of GGEMSPrimaryParticles.
+// ---------------------------------------------------------------------------
+struct Photon {
+  float E;
+  V3 p, d;
+  int8_t scatter, status, next_process;
+  int32_t E_index, solid_id;
+  float psd;  // particle_solid_distance_
+  float nid;  // next_interaction_distance_
+};
+
+struct Tallies {
+  const gg_scene* scene;
+  gg_tally_buffers* out;
+};
+
+void atomic_add_double(double* addr, double v) {
+  std::atomic_ref<double> a(*addr);
+  double cur = a.load(std::memory_order_relaxed);
+  while (!a.compare_exchange_weak(cur, cur + v, std::memory_order_relaxed)) {
+  }
+}
+void atomic_add_int(int32_t* addr, int32_t v) { __atomic_fetch_add(addr, v, __ATOMIC_RELAXED); }
+
+// dose_record_standard / dose_photon_tracking (GGEMSDoseRecording.hh:65-118).
+bool dosel_index(const gg_dose_map& dm, V3 p, int* gid) {
+  if (p.x < dm.border_min[0] + kEpsilon6 || p.x > dm.border_max[0] - kEpsilon6) return false;
+  if (p.y < dm.border_min[1] + kEpsilon6 || p.y > dm.border_max[1] - kEpsilon6) return false;
+  if (p.z < dm.border_min[2] + kEpsilon6 || p.z > dm.border_max[2] - kEpsilon6) return false;
+  V3 q = mul(sub(p, v3(dm.border_min[0], dm.border_min[1], dm.border_min[2])),
+             v3(dm.inv_size_of_dosels[0], dm.inv_size_of_dosels[1], dm.inv_size_of_dosels[2]));
+  int ix = static_cast<int>(q.x), iy = static_cast<int>(q.y), iz = static_cast<int>(q.z);
+  *gid = ix + iy * dm.number_of_dosels[0] + iz * dm.number_of_dosels[0] * dm.number_of_dosels[1];
+  if (ix < 0 || ix >= dm.number_of_dosels[0]) return false;
+  if (iy < 0 || iy >= dm.number_of_dosels[1]) return false;
+  if (iz < 0 || iz >= dm.number_of_dosels[2]) return false;
+  return true;
+}
+void dose_record(const Tallies& t, int map, float edep, V3 p) {
+  const gg_dose_map& dm = t.scene->dose_maps[map];
+  int gid;
+  if (!dosel_index(dm, p, &gid)) return;
+  if (t.out->hit && t.out->hit[map]) atomic_add_int(&t.out->hit[map][gid], 1);
+  if (t.out->edep && t.out->edep[map]) atomic_add_double(&t.out->edep[map][gid], static_cast<double>(edep));
+  if (t.out->edep_squared && t.out->edep_squared[map])
+    atomic_add_double(&t.out->edep_squared[map][gid], static_cast<double>(edep) * static_cast<double>(edep));
+}
+void photon_tracking_record(const Tallies& t, int map, V3 p) {
+  const gg_dose_map& dm = t.scene->dose_maps[map];
+  int gid;
+  if (!dosel_index(dm, p, &gid)) return;
+  if (t.out->photon_tracking && t.out->photon_tracking[map]) atomic_add_int(&t.out->photon_tracking[map][gid], 1);
+}
+
+// GetPhotonNextInteraction (GGEMSPhotonNavigator.hh:57-93).
+void next_interaction(Photon& ph, Kiss& rng, const gg_physics_tables& tb, int material) {
+  int energy_id = binary_search(ph.E, tb.energy_bins, tb.number_of_bins);
+  float nid = kOutOfWorld;
+  int8_t proc = kNoProcess;
+  for (int i = 0; i < tb.number_of_processes; ++i) {
+    int pid = tb.process_id[i];
+    float dist = -std::log(rng.uniform()) /
+                 tb.cross_sections[static_cast<size_t>(pid) * tb.number_of_materials * tb.number_of_bins +
+                                   energy_id + tb.number_of_bins * material];
+    if (dist < nid) {
+      nid = dist;
+      proc = static_cast<int8_t>(pid);
+    }
+  }
+  ph.E_index = energy_id;
+  ph.nid = nid;
+  ph.next_process = proc;
+}
+
+// KleinNishinaComptonSampleSecondaries (GGEMSComptonScatteringModels.hh:47-132).
+void compton(Photon& ph, Kiss& rng) {
+  float E0 = ph.E;
+  float E0_mec2 = E0 / kElectronMassC2;
+  V3 gd = ph.d;
+  float eps0 = 1.0f / (1.0f + 2.0f * E0_mec2);
+  float eps0sq = eps0 * eps0;
+  float alpha1 = -std::log(eps0);
+  float alpha2 = alpha1 + 0.5f * (1.0f - eps0sq);
+  float r1, r2, r3, epsilon, epsilonsq, onecost, sint2, greject;
+  int nloop = 0;
+  do {
+    ++nloop;
+    if (nloop > 1000) return;
+    r1 = rng.uniform();
+    r2 = rng.uniform();
+    r3 = rng.uniform();
+    if (alpha1 > alpha2 * r1) {
+      epsilon = std::exp(-alpha1 * r2);
+      epsilonsq = epsilon * epsilon;
+    } else {
+      epsilonsq = eps0sq + (1.0f - eps0sq) * r2;
+      epsilon = std::sqrt(epsilonsq);
+    }
+    onecost = (1.0f - epsilon) / (epsilon * E0_mec2);
+    sint2 = onecost * (2.0f - onecost);
+    greject = 1.0f - epsilon * sint2 / (1.0f + epsilonsq);
+  } while (greject < r3);
+  if (sint2 < 0.0f) sint2 = 0.0f;
+  float costheta = 1.0f - onecost;
+  float sintheta = std::sqrt(sint2);
+  float phi = rng.uniform() * kTwoPi;
+  V3 g = v3(sintheta * std::cos(phi), sintheta * std::sin(phi), costheta);
+  g = rotate_unit_z(g, gd);
+  g = normalize3(g);
+  ph.E = E0 * epsilon;
+  ph.d = g;
+}
+
+// LivermoreRayleighSampleSecondaries (GGEMSRayleighScatteringModels.hh:169-316).
+struct RayleighFit {
+  const float* pp[9];
+};
+RayleighFit g_rayleigh_fit;
+
+float rayleigh_w(float x, float n) {
+  return (x < 0.02f) ? n * x * (1.0f - 0.5f * (n - 1.0f) * x * (1.0f - (n - 2.0f) * x / 3.0f))
+                     : 1.0f - std::exp(-n * std::log(1.0f + x));
+}
+
+void rayleigh(Photon& ph, Kiss& rng, const gg_physics_tables& tb, int material) {
+  float E0 = ph.E;
+  if (E0 <= 250.0e-6f) {
+    ph.status = GG_DEAD;
+    return;
+  }
+  V3 gd = ph.d;
+  int nbins = tb.number_of_bins;
+  int8_t n_minus_one = static_cast<int8_t>(tb.number_of_elements[material] - 1);
+  int mixture = tb.element_offset[material];
+  int energy_id = ph.E_index;
+  uint8_t z = tb.atomic_number[mixture + n_minus_one];
+  if (n_minus_one > 0) {
+    const float* cs = tb.cross_sections + static_cast<size_t>(GG_RAYLEIGH_SCATTERING) * tb.number_of_materials * nbins;
+    float kcs = linear_interpolation(tb.energy_bins[energy_id], cs[energy_id + nbins * material],
+                                     tb.energy_bins[energy_id + 1], cs[energy_id + 1 + nbins * material], E0);
+    float x = rng.uniform() * kcs;
+    float cross_section = 0.0f;
+    uint8_t i = 0;
+    while (i < n_minus_one) {
+      uint8_t zi = tb.atomic_number[mixture + i];
+      cross_section += tb.atomic_number_density[mixture + i] *
+                       linear_interpolation(tb.energy_bins[energy_id], tb.rayleigh_per_atom[energy_id + nbins * zi],
+                                            tb.energy_bins[energy_id + 1], tb.rayleigh_per_atom[energy_id + 1 + nbins * zi],
+                                            E0);
+      if (x < cross_section) {
+        z = zi;
+        break;
+      }
+      ++i;
+    }
+  }
+  const float* const* P = g_rayleigh_fit.pp;
+  float xx = kRayleighFactor * E0 * E0;
+  float n0 = P[6][z] - 1.0f, n1 = P[7][z] - 1.0f, n2 = P[8][z] - 1.0f;
+  float b0 = P[3][z], b1 = P[4][z], b2 = P[5][z];
+  float w0 = rayleigh_w(2.0f * xx * b0, n0);
+  float w1 = rayleigh_w(2.0f * xx * b1, n1);
+  float w2 = rayleigh_w(2.0f * xx * b2, n2);
+  float x0 = w0 * P[0][z] / (b0 * n0);
+  float x1 = w1 * P[1][z] / (b1 * n1);
+  float x2 = w2 * P[2][z] / (b2 * n2);
+  float costheta = 0.0f, x;
+  do {
+    float w = w0, n = n0, b = b0;
+    x = rng.uniform() * (x0 + x1 + x2);
+    if (x > x0) {
+      x -= x0;
+      if (x <= x1) {
+        w = w1; n = n1; b = b1;
+      } else {
+        w = w2; n = n2; b = b2;
+      }
+    }
+    n = 1.0f / n;
+    float y = rng.uniform() * w;
+    if (y < 0.02f) {
+      x = y * n * (1.0f + 0.5f * (n + 1.0f) * y * (1.0f - (n + 2.0f) * y / 3.0f));
+    } else {
+      x = std::exp(-n * std::log(1.0f - y)) - 1.0f;
+    }
+    costheta = 1.0f - x / (b * xx);
+  } while (2.0f * rng.uniform() > 1.0f + costheta * costheta || costheta < -1.0f);
+  float phi = kTwoPi * rng.uniform();
+  float sintheta = std::sqrt((1.0f - costheta) * (1.0f + costheta));
+  V3 g = v3(sintheta * std::cos(phi), sintheta * std::sin(phi), costheta);
+  g = rotate_unit_z(g, gd);
+  g = normalize3(g);
+  ph.d = g;
+}
+
+// PhotonDiscreteProcess (GGEMSPhotonNavigator.hh:107-131).
+void discrete_process(Photon& ph, Kiss& rng, const gg_physics_tables& tb, int material) {
+  if (ph.next_process == GG_COMPTON_SCATTERING) {
+    compton(ph, rng);
+  } else if (ph.next_process == GG_PHOTOELECTRIC_EFFECT) {
+    ph.status = GG_DEAD;  // StandardPhotoElectricSampleSecondaries (GGEMSPhotoElectricEffectModels.hh:46-53)
+    ph.E = 0.0f;
+  } else if (ph.next_process == GG_RAYLEIGH_SCATTERING) {
+    rayleigh(ph, rng, tb, material);
+  }
+}
+
+// get_primaries_ggems_xray_source (GetPrimariesGGEMSXRaySource.cl:52-143).
+void xray_primary(Photon& ph, Kiss& rng, const gg_source& src) {
+  double phi = rng.uniform();
+  double theta = rng.uniform();
+  phi *= static_cast<double>(kTwoPi);
+  double new_aperture = 1.0 - std::cos(static_cast<double>(src.beam_aperture));
+  theta = std::acos(1.0 - new_aperture * theta);
+  V3 rotation = v3(static_cast<float>(std::cos(phi) * std::sin(theta)), static_cast<float>(std::sin(phi) * std::sin(theta)),
+                   static_cast<float>(std::cos(theta)));
+  V3 gp = local_to_global_position(src.matrix, v3(0.0f, 0.0f, 0.0f));
+  V3 dir = normalize3(sub(v3(0.0f, 0.0f, 0.0f), gp));
+  dir = rotate_unit_z(rotation, dir);
+  dir = normalize3(dir);
+  gp.x = src.focal_spot_size[0] * (rng.uniform() - 0.5f);
+  gp.y = src.focal_spot_size[1] * (rng.uniform() - 0.5f);
+  gp.z = src.focal_spot_size[2] * (rng.uniform() - 0.5f);
+  gp = local_to_global_position(src.matrix, gp);
+  int nbins = src.number_of_energy_bins + 1;  // GGEMSXRaySource.cc:133 passes n+1
+  int index = 0;
+  float rnd = 0.0f;
+  if (nbins != 1) {
+    rnd = rng.uniform();
+    index = binary_search(rnd, src.energy_cdf, nbins + 1);
+  }
+  ph.E = !src.is_interp ? src.energy_spectrum[index]
+                        : linear_interpolation(src.energy_cdf[index], src.energy_spectrum[index], src.energy_cdf[index + 1],
+                                               src.energy_spectrum[index + 1], rnd);
+  ph.p = gp;
+  ph.d = dir;
+  ph.scatter = 0;
+  ph.status = GG_ALIVE;
+  ph.psd = kOutOfWorld;
+  ph.next_process = kNoProcess;
+  ph.nid = 0.0f;
+}
+
+// get_primaries_ggems_voxelized_source (GetPrimariesGGEMSVoxelizedSource.cl:57-150).
+void voxelized_primary(Photon& ph, Kiss& rng, const gg_source& src) {
+  double phi = rng.uniform();
+  double theta = rng.uniform();
+  phi *= static_cast<double>(kTwoPi);
+  theta = std::acos(1.0 - 2.0 * theta);
+  V3 dir = v3(static_cast<float>(std::cos(phi) * std::sin(theta)), static_cast<float>(std::sin(phi) * std::sin(theta)),
+              static_cast<float>(std::cos(theta)));
+  double rnd_act = rng.uniform();
+  // number_of_activity_bins is the count passed to the kernel (active voxels + 1,
+  // GGEMSVoxelizedSource.cc:170); the cdf and index arrays hold that many entries.
+  int index_act = binary_search(static_cast<float>(rnd_act), src.activity_cdf, static_cast<int>(src.number_of_activity_bins));
+  int32_t vox = src.activity_index[index_act];
+  int nx = src.number_of_voxels[0], ny = src.number_of_voxels[1];
+  int slice = nx * ny;
+  int iz = vox / slice;
+  int ix = (vox - iz * slice) % nx;
+  int iy = (vox - iz * slice) / nx;
+  V3 bmin = v3(src.border_min[0], src.border_min[1], src.border_min[2]);
+  V3 vs = v3(src.voxel_sizes[0], src.voxel_sizes[1], src.voxel_sizes[2]);
+  V3 vmin = add(bmin, mul(v3(static_cast<float>(ix), static_cast<float>(iy), static_cast<float>(iz)), vs));
+  V3 vmax = add(vmin, vs);
+  V3 p;
+  p.x = bmin.x + (static_cast<float>(ix) + rng.uniform()) * vs.x;
+  p.y = bmin.y + (static_cast<float>(iy) + rng.uniform()) * vs.y;
+  p.z = bmin.z + (static_cast<float>(iz) + rng.uniform()) * vs.z;
+  safety_inside_aabb(p, vmin, vmax);
+  p = local_to_global_position(src.matrix, p);
+  int nbins = src.number_of_energy_bins + 1;
+  int index = 0;
+  float rnd = 0.0f;
+  if (nbins != 1) {
+    rnd = rng.uniform();
+    index = binary_search(rnd, src.energy_cdf, nbins + 1);
+  }
+  ph.E = !src.is_interp ? src.energy_spectrum[index]
+                        : linear_interpolation(src.energy_cdf[index], src.energy_spectrum[index], src.energy_cdf[index + 1],
+                                               src.energy_spectrum[index + 1], rnd);
+  ph.p = p;
+  ph.d = dir;
+  ph.scatter = 0;
+  ph.status = GG_ALIVE;
+  ph.psd = kOutOfWorld;
+  ph.next_process = kNoProcess;
+  ph.nid = 0.0f;
+}
+
+// particle_solid_distance_* (ParticleSolidDistanceGGEMS*.cl:43-108).
+void solid_distance(Photon& ph, const gg_solid& s, int solid_index) {
+  if (ph.status == GG_DEAD) return;
+  if (ph.psd == 0.0f) return;
+  const float* m = s.obb.matrix;
+  V3 local = global_to_local_position(m, ph.p);
+  if (in_aabb(local, obb_min(s.obb), obb_max(s.obb))) {
+    ph.psd = 0.0f;
+    ph.solid_id = solid_index;
+    return;
+  }
+  V3 ld = global_to_local_direction(m, ph.d);
+  float distance = distance_to_aabb(local, ld, obb_min(s.obb), obb_max(s.obb));
+  if (distance < ph.psd) {
+    ph.psd = distance;
+    ph.solid_id = solid_index;
+  }
+}
+
+// project_to_* (ProjectToGGEMS*.cl:44-129).
+void project_to(Photon& ph, const gg_solid& s, int solid_index) {
+  if (ph.solid_id == -1) ph.status = GG_DEAD;
+  if (ph.psd == kOutOfWorld) {
+    ph.solid_id = -1;
+    ph.status = GG_DEAD;
+    return;
+  }
+  if (ph.solid_id != solid_index) return;
+  if (ph.status == GG_DEAD) return;
+  ph.p = add(ph.p, scale(ph.d, ph.psd + kGeometryTolerance));
+  // TransportGetSafetyInsideOBB (GGEMSRayTracing.hh:94-116)
+  V3 local = global_to_local_position(s.obb.matrix, ph.p);
+  safety_inside_aabb(local, obb_min(s.obb), obb_max(s.obb));
+  ph.p = local_to_global_position(s.obb.matrix, local);
+  ph.psd = 0.0f;
+}
+
+// track_through_ggems_voxelized_solid (TrackThroughGGEMSVoxelizedSolid.cl:58-323).
+void track_voxelized(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& s, int solid_index, const Tallies& t) {
+  if (ph.solid_id != solid_index) return;
+  if (ph.status == GG_DEAD) return;
+  const gg_physics_tables& tb = sc.tables[s.navigator];
+  const float* m = s.obb.matrix;
+  V3 lp = global_to_local_position(m, ph.p);
+  V3 ld = global_to_local_direction(m, ph.d);
+  ph.d = ld;
+  V3 bmin = obb_min(s.obb), bmax = obb_max(s.obb);
+  V3 vs = v3(s.voxel_sizes[0], s.voxel_sizes[1], s.voxel_sizes[2]);
+  int nx = s.number_of_voxels[0], ny = s.number_of_voxels[1], nz = s.number_of_voxels[2];
+  const int dm = s.dose_map;
+  do {
+    V3 q = divv(sub(lp, bmin), vs);
+    int ix = static_cast<int>(q.x), iy = static_cast<int>(q.y), iz = static_cast<int>(q.z);
+    if (ix >= nx || iy >= ny || iz >= nz) {
+      ph.psd = kOutOfWorld;
+      ph.solid_id = -1;
+      break;
+    }
+    int material = s.labels[ix + iy * nx + iz * nx * ny];
+    next_interaction(ph, rng, tb, material);
+    float nid = ph.nid;
+    int8_t proc = ph.next_process;
+    V3 vmin = add(bmin, mul(v3(static_cast<float>(ix), static_cast<float>(iy), static_cast<float>(iz)), vs));
+    V3 vmax = add(vmin, vs);
+    safety_inside_aabb(lp, vmin, vmax);
+    float dtb = distance_to_aabb(lp, ld, vmin, vmax);
+    if (dtb <= nid) {
+      nid = dtb + kGeometryTolerance;
+      proc = GG_TRANSPORTATION;
+      if (dm >= 0) photon_tracking_record(t, dm, lp);
+    }
+    lp = add(lp, scale(ld, nid));
+    safety_outside_aabb(lp, vmin, vmax);
+    if (!in_aabb(lp, bmin, bmax)) {
+      ph.psd = kOutOfWorld;
+      ph.solid_id = -1;
+      break;
+    }
+    ph.p = lp;
+    float initial_energy = ph.E;
+    if (proc != GG_TRANSPORTATION) {
+      discrete_process(ph, rng, tb, material);
+      if (proc == GG_COMPTON_SCATTERING || proc == GG_RAYLEIGH_SCATTERING) ph.scatter = 1;
+      if (dm >= 0) dose_record(t, dm, initial_energy - ph.E, lp);
+      ld = ph.d;
+    }
+    if (ph.E <= tb.photon_energy_cut[material]) {
+      if (dm >= 0) dose_record(t, dm, ph.E, lp);
+      ph.status = GG_DEAD;
+    }
+  } while (ph.status == GG_ALIVE);
+  ph.p = local_to_global_position(m, lp);
+  ph.d = local_to_global_direction(m, ld);
+}
+
+// track_through_ggems_solid_box (TrackThroughGGEMSSolidBox.cl:56-261), HISTOGRAM variant.
+void track_box(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& s, int solid_index, const Tallies& t) {
+  if (ph.solid_id != solid_index) return;
+  if (ph.status == GG_DEAD) return;
+  const gg_physics_tables& tb = sc.tables[s.navigator];
+  const float* m = s.obb.matrix;
+  V3 lp = global_to_local_position(m, ph.p);
+  V3 ld = global_to_local_direction(m, ph.d);
+  ph.d = ld;
+  V3 bmin = obb_min(s.obb), bmax = obb_max(s.obb);
+  V3 box = v3(s.box_size[0], s.box_size[1], s.box_size[2]);
+  int vx = s.virtual_element_number[0], vy = s.virtual_element_number[1], vz = s.virtual_element_number[2];
+  do {
+    next_interaction(ph, rng, tb, 0);
+    float nid = ph.nid;
+    int8_t proc = ph.next_process;
+    safety_inside_aabb(lp, bmin, bmax);
+    float dtb = distance_to_aabb(lp, ld, bmin, bmax);
+    if (dtb <= nid) {
+      nid = dtb + kGeometryTolerance;
+      proc = GG_TRANSPORTATION;
+    }
+    lp = add(lp, scale(ld, nid));
+    safety_outside_aabb(lp, bmin, bmax);
+    if (!in_aabb(lp, bmin, bmax)) {
+      ph.psd = kOutOfWorld;
+      ph.solid_id = -1;
+      break;
+    }
+    ph.p = lp;
+    if (ph.E < s.threshold) ph.status = GG_DEAD;
+    if (proc != GG_TRANSPORTATION) {
+      discrete_process(ph, rng, tb, 0);
+      ld = ph.d;
+      if (s.histogram >= 0 && (proc == GG_PHOTOELECTRIC_EFFECT || proc == GG_COMPTON_SCATTERING)) {
+        V3 es = divv(box, v3(static_cast<float>(vx), static_cast<float>(vy), static_cast<float>(vz)));
+        V3 q = divv(sub(lp, bmin), es);
+        int ix = static_cast<int>(q.x), iy = static_cast<int>(q.y);
+        int index = ix + iy * vx;
+        if (t.out->histograms && t.out->histograms[s.histogram]) atomic_add_int(&t.out->histograms[s.histogram][index], 1);
+        if (s.scatter_histogram >= 0 && ph.scatter == 1 && t.out->histograms && t.out->histograms[s.scatter_histogram])
+          atomic_add_int(&t.out->histograms[s.scatter_histogram][index], 1);
+      }
+    }
+  } while (ph.status == GG_ALIVE);
+  ph.p = local_to_global_position(m, lp);
+  ph.d = local_to_global_direction(m, ld);
+}
+
+// One history, following GGEMS::RunOnDevice's inner loop (src/global/GGEMS.cc:326-345):
+// FindSolid, ProjectToSolid, TrackThroughSolid over all solids in order,
+// until the particle is dead or GG_MAX_LOOP iterations were made.
+void transport(Photon& ph, Kiss& rng, const gg_scene& sc, const Tallies& t) {
+  for (int loop = 0; loop < GG_MAX_LOOP; ++loop) {
+    for (int s = 0; s < sc.number_of_solids; ++s) solid_distance(ph, sc.solids[s], s);
+    for (int s = 0; s < sc.number_of_solids; ++s) project_to(ph, sc.solids[s], s);
+    for (int s = 0; s < sc.number_of_solids; ++s) {
+      const gg_solid& solid = sc.solids[s];
+      if (solid.type == GG_SOLID_VOXELIZED) track_voxelized(ph, rng, sc, solid, s, t);
+      else if (solid.type == GG_SOLID_BOX) track_box(ph, rng, sc, solid, s, t);
+    }
+    if (ph.status == GG_DEAD) break;
+  }
+}
+
+uint64_t batch_count(uint64_t n) {
+  // GGEMSSource.cc:403 (float division, as in the reference)
+  return static_cast<uint64_t>(std::ceil(static_cast<float>(n) / GG_MAXIMUM_PARTICLES));
+}
+
+}  // namespace
+
+extern "C" {
+
+// Register the Rayleigh form-factor fit tables PP0..PP8 (101 floats each).
+__attribute__((visibility("default"))) void gg_oracle_set_rayleigh_fit(const float* const* pp) {
+  for (int i = 0; i < 9; ++i) g_rayleigh_fit.pp[i] = pp[i];
+}
+
+// Run number_of_particles primaries of `source` through `scene`, batching as
+// GGEMSSource::OrganizeParticlesInBatch for one device.  random_states holds
+// 5 arrays of GG_MAXIMUM_PARTICLES words (in/out).  Final particle states are
+// written for the slots of the last batch that touched them.
+__attribute__((visibility("default"))) int gg_oracle_run(const gg_scene* scene, const gg_source* source,
+                                                         uint64_t number_of_particles, uint32_t* random_states,
+                                                         gg_particle_buffers* particles, gg_tally_buffers* tallies,
+                                                         int threads) {
+  if (!scene || !source || !random_states) return GG_ERROR_INVALID_ARGUMENT;
+  const uint64_t nb = batch_count(number_of_particles);
+  std::vector<uint64_t> sizes(nb);
+  if (nb == 1) {
+    sizes[0] = number_of_particles;
+  } else {
+    for (uint64_t j = 0; j < nb; ++j) sizes[j] = number_of_particles / nb;
+    for (uint64_t j = 0; j < number_of_particles % nb; ++j) sizes[j]++;
+  }
+  const uint64_t slots = nb ? sizes[0] : 0;
+  Tallies t{scene, tallies};
+  const size_t S = GG_MAXIMUM_PARTICLES;
+  auto worker = [&](uint64_t begin, uint64_t end) {
+    for (uint64_t slot = begin; slot < end; ++slot) {
+      Kiss rng{random_states[slot], random_states[S + slot], random_states[2 * S + slot], random_states[3 * S + slot],
+               random_states[4 * S + slot]};
+      Photon ph{};
+      ph.solid_id = -1;
+      for (uint64_t b = 0; b < nb; ++b) {
+        if (slot >= sizes[b]) break;
+        if (source->type == GG_SOURCE_XRAY) xray_primary(ph, rng, *source);
+        else voxelized_primary(ph, rng, *source);
+        transport(ph, rng, *scene, t);
+      }
+      random_states[slot] = rng.s1;
+      random_states[S + slot] = rng.s2;
+      random_states[2 * S + slot] = rng.s3;
+      random_states[3 * S + slot] = rng.s4;
+      random_states[4 * S + slot] = rng.s5;
+      if (particles) {
+        particles->E[slot] = ph.E;
+        particles->px[slot] = ph.p.x;
+        particles->py[slot] = ph.p.y;
+        particles->pz[slot] = ph.p.z;
+        particles->dx[slot] = ph.d.x;
+        particles->dy[slot] = ph.d.y;
+        particles->dz[slot] = ph.d.z;
+        particles->status[slot] = ph.status;
+        particles->scatter[slot] = ph.scatter;
+        particles->solid_id[slot] = ph.solid_id;
+      }
+    }
+  };
+  if (threads < 1) threads = 1;
+  std::vector<std::thread> pool;
+  for (int i = 0; i < threads; ++i) {
+    uint64_t b = slots * i / threads, e = slots * (i + 1) / threads;
+    pool.emplace_back(worker, b, e);
+  }
+  for (auto& th : pool) th.join();
+  return GG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,387 @@
+"""Synthetic scenes for the parity tests, built directly in the C-ABI form
+(``include/ggems_b200.h``) with tables from the oracle's table builder.
+
+Geometry matrices follow GGEMSGeometryTransformation
+(src/maths/GGEMSGeometryTransformation.cc:143-336): the matrix starts as the
+object's axis matrix and each SetRotation / SetTranslation call left-multiplies
+it, in float32 with the reference's summation order.  cos/sin come from the
+host libm (the functions the reference's host code calls).
+"""
+
+import ctypes as C
+import ctypes.util
+import os
+
+import numpy as np
+
+from ggems_b200 import abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DATA = os.path.join(ROOT, "ggems_b200", "data")
+MATERIALS = os.path.join(DATA, "materials.txt")
+PHYSICS = os.path.join(DATA, "physics_data.bin")
+
+_libm = C.CDLL(ctypes.util.find_library("m"))
+_libm.cosf.restype = C.c_float
+_libm.cosf.argtypes = [C.c_float]
+_libm.sinf.restype = C.c_float
+_libm.sinf.argtypes = [C.c_float]
+
+F = np.float32
+DEG = F(F(3.141592653589793238463) / F(180.0))  # GGEMSSystemOfUnits.hh:80
+MEV = F(1.0)
+KEV = F(1.0e-3)
+
+SOURCE_AXIS = ((0.0, 0.0, -1.0), (0.0, 1.0, 0.0), (1.0, 0.0, 0.0))    # GGEMSXRaySource.cc:50-56
+PHANTOM_AXIS = ((1.0, 0.0, 0.0), (0.0, 1.0, 0.0), (0.0, 0.0, 1.0))   # GGEMSVoxelizedSolid.cc:56-62
+DETECTOR_AXIS = ((0.0, 0.0, 1.0), (0.0, 1.0, 0.0), (-1.0, 0.0, 0.0))  # GGEMSSolidBox.cc:77-83
+
+
+def _mat_mul(a, b):
+    """GGfloat44MultGGfloat44 in float32, products summed left to right."""
+    out = np.zeros((4, 4), np.float32)
+    for i in range(4):
+        for j in range(4):
+            s = F(a[i, 0] * b[0, j])
+            s = F(s + F(a[i, 1] * b[1, j]))
+            s = F(s + F(a[i, 2] * b[2, j]))
+            s = F(s + F(a[i, 3] * b[3, j]))
+            out[i, j] = s
+    return out
+
+
+def geometry_matrix(axis, ops):
+    """ops: sequence of ("rotation", (rx, ry, rz) rad) / ("translation", (x, y, z) mm) in call order."""
+    m = np.eye(4, dtype=np.float32)
+    m[:3, :3] = np.array(axis, np.float32)
+    for kind, v in ops:
+        v = [F(x) for x in v]
+        if kind == "translation":
+            t = np.eye(4, dtype=np.float32)
+            t[:3, 3] = v
+            m = _mat_mul(t, m)
+        else:
+            c, s = F(_libm.cosf(v[0])), F(_libm.sinf(v[0]))
+            rx = np.array([[1, 0, 0, 0], [0, c, -s, 0], [0, s, c, 0], [0, 0, 0, 1]], np.float32)
+            c, s = F(_libm.cosf(v[1])), F(_libm.sinf(v[1]))
+            ry = np.array([[c, 0, s, 0], [0, 1, 0, 0], [-s, 0, c, 0], [0, 0, 0, 1]], np.float32)
+            c, s = F(_libm.cosf(v[2])), F(_libm.sinf(v[2]))
+            rz = np.array([[c, -s, 0, 0], [s, c, 0, 0], [0, 0, 1, 0], [0, 0, 0, 1]], np.float32)
+            r = _mat_mul(rz, _mat_mul(ry, rx))
+            m = _mat_mul(r, m)
+    return m
+
+
+def _oracle_lib():
+    path = os.path.join(ROOT, "oracle", "_build", "libgg_oracle.so")
+    if not os.path.exists(path):
+        import subprocess
+        import sys
+        subprocess.check_call([sys.executable, os.path.join(ROOT, "oracle", "build.py")])
+    lib = C.CDLL(path)
+    lib.gg_oracle_run.restype = C.c_int
+    lib.gg_oracle_run.argtypes = [C.POINTER(abi.gg_scene), C.POINTER(abi.gg_source), C.c_uint64,
+                                  C.POINTER(C.c_uint32), C.POINTER(abi.gg_particle_buffers),
+                                  C.POINTER(abi.gg_tally_buffers), C.c_int]
+    return lib
+
+
+_ORACLE = None
+
+
+def oracle():
+    global _ORACLE
+    if _ORACLE is None:
+        _ORACLE = _oracle_lib()
+        pp = load_physics()
+        arrs = [np.ascontiguousarray(pp["rayleigh_pp%d" % i]) for i in range(9)]
+        _ORACLE._pp_keep = arrs
+        ptrs = (C.POINTER(C.c_float) * 9)(*[abi.ptr(a, C.c_float) for a in arrs])
+        _ORACLE.gg_oracle_set_rayleigh_fit(ptrs)
+    return _ORACLE
+
+
+def load_physics(path=PHYSICS):
+    raw = open(path, "rb").read()
+    assert raw[:8] == b"GGPHYS01"
+    n = int(np.frombuffer(raw, np.uint32, 1, 8)[0])
+    off, out = 12, {}
+    for _ in range(n):
+        name = raw[off:off + 32].split(b"\0")[0].decode()
+        code, cnt = np.frombuffer(raw, np.uint32, 2, off + 32)
+        off += 40
+        dt = {0: np.float32, 1: np.int32, 2: np.int16, 3: np.uint8}[int(code)]
+        arr = np.frombuffer(raw, dt, int(cnt), off)
+        off += arr.nbytes
+        out[name] = arr
+    return out
+
+
+class Tables:
+    """One navigator's physics tables (oracle restatement of the host builders)."""
+
+    def __init__(self, materials, number_of_bins=220, min_energy=1.0 * KEV, max_energy=1.0 * MEV,
+                 processes=(0, 1, 2), photon_cut=0.1, materials_file=MATERIALS):
+        lib = oracle()
+        nm, nb = len(materials), number_of_bins
+        self.materials = list(materials)
+        self.energy_bins = np.zeros(nb, np.float32)
+        self.cross_sections = np.zeros(3 * nm * nb, np.float32)
+        self.rayleigh = np.zeros(101 * nb, np.float32)
+        self.density = np.zeros(nm, np.float32)
+        self.photon_cut = np.zeros(nm, np.float32)
+        self.n_elements = np.zeros(nm, np.int32)
+        self.offset = np.zeros(nm, np.int32)
+        self.Z = np.zeros(nm * 32, np.uint8)
+        self.atom_density = np.zeros(nm * 32, np.float32)
+        total = C.c_int32(0)
+        names = (C.c_char_p * nm)(*[m.encode() for m in materials])
+        procs = (C.c_int * 3)(*processes)
+        lib.gg_oracle_build_tables.restype = C.c_int
+        rc = lib.gg_oracle_build_tables(
+            MATERIALS.encode() if materials_file is None else materials_file.encode(), PHYSICS.encode(), names, nm, nb,
+            C.c_float(min_energy), C.c_float(max_energy), procs, len(processes), C.c_float(photon_cut),
+            abi.ptr(self.energy_bins, C.c_float), abi.ptr(self.cross_sections, C.c_float),
+            abi.ptr(self.rayleigh, C.c_float), abi.ptr(self.density, C.c_float), abi.ptr(self.photon_cut, C.c_float),
+            abi.ptr(self.n_elements, C.c_int32), abi.ptr(self.offset, C.c_int32), abi.ptr(self.Z, C.c_uint8),
+            abi.ptr(self.atom_density, C.c_float), C.byref(total))
+        assert rc == 0, "gg_oracle_build_tables failed"
+        self.total = total.value
+        pid = list(processes) + [0] * (3 - len(processes))
+        self.struct = abi.gg_physics_tables(
+            nb, nm, len(processes), (C.c_int32 * 3)(*pid), abi.ptr(self.energy_bins, C.c_float),
+            abi.ptr(self.cross_sections, C.c_float),
+            abi.ptr(self.rayleigh, C.c_float) if 2 in processes else C.cast(None, abi.FP),
+            abi.ptr(self.density, C.c_float), abi.ptr(self.photon_cut, C.c_float),
+            abi.ptr(self.n_elements, C.c_int32), abi.ptr(self.offset, C.c_int32), abi.ptr(self.Z, C.c_uint8),
+            abi.ptr(self.atom_density, C.c_float), self.total)
+
+
+def _obb(matrix, half):
+    o = abi.gg_obb()
+    o.matrix[:] = [float(x) for x in matrix.reshape(-1)]
+    o.border_min[:] = [float(-h) for h in half]
+    o.border_max[:] = [float(h) for h in half]
+    return o
+
+
+class Scene:
+    """A gg_scene plus the numpy storage it points into."""
+
+    def __init__(self):
+        self.tables = []
+        self.solids = []
+        self.dose_maps = []
+        self.histogram_sizes = []
+        self._keep = []
+
+    def add_tables(self, tables):
+        self.tables.append(tables)
+        return len(self.tables) - 1
+
+    def add_voxelized(self, labels, voxel_size, navigator, ops=(), dose=None):
+        """labels: uint8 array shaped (nz, ny, nx).  dose: dict with dosel size or None."""
+        labels = np.ascontiguousarray(labels, np.uint8)
+        self._keep.append(labels)
+        nz, ny, nx = labels.shape
+        vs = [F(v) for v in voxel_size]
+        # GGEMSMHDImage::Read (src/io/GGEMSMHDImage.cc:209-213)
+        half = [F(F(F(n) * v) * F(0.5)) for n, v in zip((nx, ny, nz), vs)]
+        m = geometry_matrix(PHANTOM_AXIS, ops)
+        s = abi.gg_solid()
+        s.type = abi.GG_SOLID_VOXELIZED
+        s.navigator = navigator
+        s.obb = _obb(m, half)
+        s.threshold = 0.0
+        s.number_of_voxels[:] = [nx, ny, nz]
+        s.voxel_sizes[:] = [float(v) for v in vs]
+        s.labels = abi.ptr(labels, C.c_uint8)
+        s.histogram = -1
+        s.scatter_histogram = -1
+        s.dose_map = -1
+        if dose is not None:
+            s.dose_map = self._add_dose(s, dose)
+        self.solids.append(s)
+        return len(self.solids) - 1
+
+    def _add_dose(self, solid, dose):
+        # GGEMSDosimetryCalculator::Initialize (src/navigators/GGEMSDosimetryCalculator.cc:435-530)
+        d = abi.gg_dose_map()
+        size = [F(v) for v in dose.get("dosel_size", list(solid.voxel_sizes))]
+        d.size_of_dosels[:] = [float(v) for v in size]
+        d.inv_size_of_dosels[:] = [float(F(F(1.0) / v)) for v in size]
+        d.border_min[:] = list(solid.obb.border_min)
+        d.border_max[:] = list(solid.obb.border_max)
+        n = [int(F(F(F(solid.obb.border_max[i]) - F(solid.obb.border_min[i])) / size[i])) for i in range(3)]
+        d.number_of_dosels[:] = n
+        d.total_number_of_dosels = n[0] * n[1] * n[2]
+        d.slice_number_of_dosels = n[0] * n[1]
+        d.record_edep_squared = 1
+        d.record_hit = 1
+        d.record_photon_tracking = 1 if dose.get("photon_tracking") else 0
+        self.dose_maps.append(d)
+        return len(self.dose_maps) - 1
+
+    def add_flat_detector(self, navigator, elements, element_size, sdd, sid, threshold, scatter=True,
+                          extra_rotation=None):
+        """One-module flat GGEMSCTSystem (src/navigators/GGEMSCTSystem.cc:175-300)."""
+        ex, ey, ez = elements
+        sx, sy, sz = [F(v) for v in element_size]
+        box = [F(F(ex) * sx), F(F(ey) * sy), F(F(ez) * sz)]
+        half = [F(b * F(0.5)) for b in box]
+        # InitializeFlatGeometry: module (0, 0) of a 1x1 system.
+        gx = F(F(sdd) - F(sid))
+        gy = F(F(F(ey) * sy) * F(F(0.0) + F(0.5) * F(F(1.0) - F(1.0))))
+        gz = F(F(F(ex) * sx) * F(F(0.0) + F(0.5) * F(F(1.0) - F(1.0))))
+        ops = [("rotation", (0.0, 0.0, 0.0)), ("translation", (gx, gy, gz))]
+        if extra_rotation is not None:
+            ops.append(("rotation", extra_rotation))
+        m = geometry_matrix(DETECTOR_AXIS, ops)
+        s = abi.gg_solid()
+        s.type = abi.GG_SOLID_BOX
+        s.navigator = navigator
+        s.obb = _obb(m, half)
+        s.threshold = float(threshold)
+        s.virtual_element_number[:] = [ex, ey, ez]
+        s.box_size[:] = [float(b) for b in box]
+        s.histogram = len(self.histogram_sizes)
+        self.histogram_sizes.append(ex * ey)
+        s.scatter_histogram = -1
+        if scatter:
+            s.scatter_histogram = len(self.histogram_sizes)
+            self.histogram_sizes.append(ex * ey)
+        s.dose_map = -1
+        self.solids.append(s)
+        return len(self.solids) - 1
+
+    def struct(self):
+        self._t = (abi.gg_physics_tables * len(self.tables))(*[t.struct for t in self.tables])
+        self._s = (abi.gg_solid * len(self.solids))(*self.solids)
+        self._d = (abi.gg_dose_map * max(1, len(self.dose_maps)))(*self.dose_maps)
+        self._h = np.array(self.histogram_sizes + [0], np.int32)
+        return abi.gg_scene(len(self.tables), self._t, len(self.solids), self._s, len(self.dose_maps), self._d,
+                            len(self.histogram_sizes), abi.ptr(self._h, C.c_int32))
+
+    def tallies(self):
+        return abi.Tallies(self.histogram_sizes, [d.total_number_of_dosels for d in self.dose_maps])
+
+
+class XRaySource:
+    """GGEMSXRaySource (src/sources/GGEMSXRaySource.cc) in C-ABI form."""
+
+    def __init__(self, position=(-1000.0, 0.0, 0.0), rotation=(0.0, 0.0, 0.0), aperture_deg=10.0,
+                 focal=(0.0, 0.0, 0.0), monoenergy=None, spectrum=None, order=("position", "rotation")):
+        ops = []
+        for o in order:
+            ops.append(("translation", position) if o == "position" else ("rotation", rotation))
+        self.matrix = geometry_matrix(SOURCE_AXIS, ops)
+        if monoenergy is not None:
+            energies, weights, interp = [F(monoenergy)], [1.0], 0
+        else:
+            energies, weights = spectrum
+            energies = [F(e) for e in energies]
+            interp = 1
+        self.spectrum, self.cdf = fill_energy(energies, weights)
+        s = abi.gg_source()
+        s.type = abi.GG_SOURCE_XRAY
+        s.particle_type = 0
+        s.matrix[:] = [float(x) for x in self.matrix.reshape(-1)]
+        s.beam_aperture = float(F(F(aperture_deg) * DEG))
+        s.focal_spot_size[:] = [float(f) for f in focal]
+        s.number_of_energy_bins = len(energies)
+        s.energy_spectrum = abi.ptr(self.spectrum, C.c_float)
+        s.energy_cdf = abi.ptr(self.cdf, C.c_float)
+        s.is_interp = interp
+        self.struct = s
+
+
+def fill_energy(energies, weights):
+    """GGEMSSource::FillEnergy (src/sources/GGEMSSource.cc:265-316)."""
+    n = len(energies)
+    spec = np.zeros(n + 1, np.float32)
+    cdf = np.zeros(n + 1, np.float32)
+    total = 0.0
+    for w in weights:
+        total += float(w)
+    tmp = [0.0] + [float(w) for w in weights]
+    spec[:n] = energies
+    spec[n] = spec[n - 1]
+    for i in range(1, n + 1):
+        tmp[i] = tmp[i] + tmp[i - 1]
+        cdf[i] = np.float32(tmp[i] / total)
+    cdf[n] = 1.0
+    return spec, cdf
+
+
+def seed_states(seed, slots=abi.GG_MAXIMUM_PARTICLES, skip=0):
+    """GGEMSPseudoRandomGenerator::InitializeSeeds with numpy's MT19937 (same
+    generator as std::mt19937 for a 32-bit seed)."""
+    from numpy.random import MT19937
+    bg = MT19937(0)
+    bg._legacy_seeding(seed)
+    raw = bg.random_raw((skip + slots) * 4)[skip * 4:].astype(np.uint32).reshape(slots, 4)
+    st = np.zeros((5, abi.GG_MAXIMUM_PARTICLES), np.uint32)
+    st[0, :slots] = raw[:, 0]
+    st[1, :slots] = raw[:, 1]
+    st[2, :slots] = raw[:, 2]
+    st[3, :slots] = raw[:, 3]
+    return st
+
+
+def water_box_scene(n=64, voxel=2.0, dose=True, photon_tracking=False):
+    """C1: 64^3 water, 2 mm voxels, dose map on the phantom grid."""
+    sc = Scene()
+    t = sc.add_tables(Tables(["Water"]))
+    labels = np.zeros((n, n, n), np.uint8)
+    sc.add_voxelized(labels, (voxel, voxel, voxel), t, dose={"photon_tracking": photon_tracking} if dose else None)
+    return sc
+
+
+def ellipsoid_phantom(n, voxel, seed=1, n_bones=8):
+    """C2 generator: air / water ellipsoid / bone ellipsoids, labels (nz, ny, nx)."""
+    rng = np.random.default_rng(seed)
+    c = (np.arange(n, dtype=np.float64) + 0.5) * voxel - n * voxel / 2.0
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    scale = n * voxel / 256.0
+    a, b, cc = 110.0 * scale, 90.0 * scale, 120.0 * scale
+    labels = np.zeros((n, n, n), np.uint8)
+    body = (x / a) ** 2 + (y / b) ** 2 + (z / cc) ** 2 <= 1.0
+    labels[body] = 1
+    for _ in range(n_bones):
+        r = rng.uniform(5, 25, 3) * scale
+        while True:
+            p = rng.uniform(-1, 1, 3)
+            if (p ** 2).sum() <= 1.0:
+                break
+        ctr = p * np.array([a, b, cc]) * 0.7
+        bone = ((x - ctr[0]) / r[0]) ** 2 + ((y - ctr[1]) / r[1]) ** 2 + ((z - ctr[2]) / r[2]) ** 2 <= 1.0
+        labels[bone & body] = 2
+    return labels
+
+
+def synthetic_spectrum():
+    """120 kVp spectrum, 1 keV bins 10-120 keV: Kramers (120 - E)/E filtered by
+    2.5 mm Al using GGEMS's own mu table for Z = 13, normalised."""
+    pd = load_physics()
+    nb = pd["mu_nb_energy_bins"]
+    idx = pd["mu_index_energy"]
+    data = pd["mu_data"].reshape(-1, 3)
+    z = 13
+    rows = data[idx[z]: idx[z] + nb[z]]
+    e_tab, mu_tab = rows[:, 0].astype(np.float64), rows[:, 1].astype(np.float64)  # MeV, cm2/g
+    energies = np.arange(10, 121, dtype=np.float64)  # keV
+    mu = np.exp(np.interp(np.log(energies * 1e-3), np.log(e_tab), np.log(mu_tab)))
+    w = np.clip(120.0 - energies, 0.0, None) / energies * np.exp(-mu * 2.699 * 0.25)
+    w = w / w.sum()
+    return [F(e * 1e-3) for e in energies], [float(x) for x in w]
+
+
+def cbct_scene(n=256, voxel=1.0, elements=(512, 512, 1), element_size=(0.8, 0.8, 10.0), seed=1):
+    """C2: ellipsoid phantom + one-module flat detector at SDD 1500 / SID 1000."""
+    sc = Scene()
+    t_ph = sc.add_tables(Tables(["Air", "Water", "Bone185"]))
+    labels = ellipsoid_phantom(n, voxel, seed)
+    sc.add_voxelized(labels, (voxel, voxel, voxel), t_ph)
+    t_det = sc.add_tables(Tables(["GOS"]))
+    sc.add_flat_detector(t_det, elements, element_size, sdd=1500.0, sid=1000.0, threshold=F(10.0) * KEV)
+    return sc
