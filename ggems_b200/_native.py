@@ -1,0 +1,119 @@
+"""Loader for ``libggems.so`` (CUDA transport layer + C++ host API).
+
+There is no fallback: if the library is missing or was not built, importing
+this module raises, so nothing can silently run on the CPU instead.
+"""
+
+import ctypes as C
+import os
+
+from . import abi
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libggems.so")
+
+
+class GGEMSNativeError(RuntimeError):
+    pass
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise GGEMSNativeError("libggems.so is not built: run `python -m ggems_b200.build` (%s)" % LIB_PATH)
+    lib = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    sig = {
+        "gg_device_count": (C.c_int, [P(C.c_int32)]),
+        "gg_context_create": (C.c_int, [C.c_int32, P(C.c_void_p)]),
+        "gg_context_destroy": (C.c_int, [C.c_void_p]),
+        "gg_last_error": (C.c_char_p, []),
+        "gg_set_random_states": (C.c_int, [C.c_void_p, P(C.c_uint32), C.c_int64]),
+        "gg_get_random_states": (C.c_int, [C.c_void_p, P(C.c_uint32), C.c_int64]),
+        "gg_seed_random_states": (C.c_int, [P(C.c_uint32), C.c_int64, C.c_uint32, C.c_int64]),
+        "gg_upload_scene": (C.c_int, [C.c_void_p, P(abi.gg_scene)]),
+        "gg_reset_tallies": (C.c_int, [C.c_void_p]),
+        "gg_read_tallies": (C.c_int, [C.c_void_p, P(abi.gg_tally_buffers)]),
+        "gg_read_particles": (C.c_int, [C.c_void_p, P(abi.gg_particle_buffers), C.c_int64]),
+        "gg_run_source": (C.c_int, [C.c_void_p, P(abi.gg_source), C.c_uint64]),
+        "gg_synchronize": (C.c_int, [C.c_void_p]),
+        "gg_batch_plan": (C.c_int, [C.c_uint64, P(C.c_uint64), C.c_int64, P(C.c_int64)]),
+        "gg_compute_dose": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_float, C.c_int32, C.c_float,
+                                      P(C.c_float), P(C.c_float)]),
+        "gg_last_run_stats": (C.c_int, [C.c_void_p, P(C.c_float), P(C.c_int64)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def check(rc, what=""):
+    if rc != 0:
+        msg = lib.gg_last_error().decode(errors="replace")
+        raise GGEMSNativeError("%s failed (%s): %s" % (what or "ggems call", abi.STATUS.get(rc, rc), msg))
+
+
+class Context:
+    """One GPU context of the transport layer."""
+
+    def __init__(self, device=0):
+        h = C.c_void_p()
+        check(lib.gg_context_create(device, C.byref(h)), "gg_context_create")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            lib.gg_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_random_states(self, states):
+        check(lib.gg_set_random_states(self.handle, abi.ptr(states, C.c_uint32), abi.GG_MAXIMUM_PARTICLES),
+              "gg_set_random_states")
+
+    def get_random_states(self, states):
+        check(lib.gg_get_random_states(self.handle, abi.ptr(states, C.c_uint32), abi.GG_MAXIMUM_PARTICLES),
+              "gg_get_random_states")
+
+    def upload_scene(self, scene_struct):
+        self._scene = scene_struct
+        check(lib.gg_upload_scene(self.handle, C.byref(scene_struct)), "gg_upload_scene")
+
+    def reset_tallies(self):
+        check(lib.gg_reset_tallies(self.handle), "gg_reset_tallies")
+
+    def run(self, source_struct, n, sync=True):
+        check(lib.gg_run_source(self.handle, C.byref(source_struct), n), "gg_run_source")
+        if sync:
+            self.synchronize()
+
+    def synchronize(self):
+        check(lib.gg_synchronize(self.handle), "gg_synchronize")
+
+    def read_tallies(self, tallies):
+        check(lib.gg_read_tallies(self.handle, C.byref(tallies.struct)), "gg_read_tallies")
+
+    def read_particles(self, particles):
+        check(lib.gg_read_particles(self.handle, C.byref(particles.struct), particles.n), "gg_read_particles")
+
+    def last_run_stats(self):
+        ms, n = C.c_float(), C.c_int64()
+        check(lib.gg_last_run_stats(self.handle, C.byref(ms), C.byref(n)), "gg_last_run_stats")
+        return ms.value, n.value
+
+    def compute_dose(self, dose_map, solid, n, scale=1.0, water_reference=False, minimum_density=0.0,
+                     uncertainty=True):
+        import numpy as np
+        dose = np.zeros(n, np.float32)
+        unc = np.zeros(n, np.float32) if uncertainty else None
+        check(lib.gg_compute_dose(self.handle, dose_map, solid, scale, 1 if water_reference else 0, minimum_density,
+                                  abi.ptr(dose, C.c_float), abi.ptr(unc, C.c_float)), "gg_compute_dose")
+        return dose, unc

@@ -60,7 +60,7 @@ class gg_scene(C.Structure):
     _fields_ = [("number_of_tables", C.c_int32), ("tables", C.POINTER(gg_physics_tables)),
                 ("number_of_solids", C.c_int32), ("solids", C.POINTER(gg_solid)),
                 ("number_of_dose_maps", C.c_int32), ("dose_maps", C.POINTER(gg_dose_map)),
-                ("number_of_histograms", C.c_int32), ("histogram_sizes", IP)]
+                ("number_of_histograms", C.c_int32), ("histogram_sizes", IP), ("rayleigh_fit", FP)]
 
 
 class gg_source(C.Structure):

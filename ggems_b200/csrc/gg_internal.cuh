@@ -1,0 +1,154 @@
+// Device-side scene layout shared by the transport kernels and the runtime.
+//
+// HBM layout (one context = one GPU):
+//   * random states: 5 SoA arrays of GG_MAXIMUM_PARTICLES uint32 (JKISS words);
+//   * final particle states: SoA float/int8/int32 arrays per slot;
+//   * table blob: per navigator, energy bins (float[nbins], 16 B padded),
+//     cross sections packed as float4 {Compton, photoelectric, Rayleigh, 0}
+//     per (material, bin), and photon energy cuts; copied into shared memory
+//     at kernel start when it fits (cp.async.bulk + mbarrier);
+//   * element tables and Rayleigh per-atom cross sections stay in HBM (read
+//     only on Rayleigh interactions);
+//   * labels: uint8 per voxel, x fastest (L2 resident for <= 126 MB volumes);
+//   * tallies: int32 histograms, int64 fixed-point edep (LSB 2^-32 MeV),
+//     double edep^2, int32 hit / photon-tracking counters.
+#ifndef GG_INTERNAL_CUH
+#define GG_INTERNAL_CUH
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "ggems_b200.h"
+
+namespace gg {
+
+constexpr int kMaxSolids = 64;
+constexpr int kMaxNavigators = 16;
+constexpr int kBlockThreads = 256;
+// Fixed-point scale of the energy tally: edep is accumulated as int64 multiples of 2^-32 MeV.
+constexpr double kEdepScale = 4294967296.0;
+
+struct DevNavigator {
+  int32_t number_of_bins;
+  int32_t number_of_materials;
+  int32_t number_of_processes;
+  int32_t process_id[3];
+  // byte offsets into the table blob (shared memory copy when it fits)
+  uint32_t energy_bins_offset;   // float[number_of_bins]
+  uint32_t sigma_offset;         // float4[number_of_materials * number_of_bins]
+  uint32_t photon_cut_offset;    // float[number_of_materials]
+  // HBM arrays read on Rayleigh interactions
+  const int32_t* number_of_elements;
+  const int32_t* element_offset;
+  const uint8_t* atomic_number;
+  const float* atomic_number_density;
+  const float* rayleigh_per_atom;
+};
+
+struct DevDoseMap {
+  float size_of_dosels[3];
+  float inv_size_of_dosels[3];
+  float border_min[3];
+  float border_max[3];
+  int32_t number_of_dosels[3];
+  int32_t total_number_of_dosels;
+  int32_t slice_number_of_dosels;
+  unsigned long long* edep;      // fixed point, LSB 2^-32 MeV
+  double* edep_squared;          // nullptr when not recorded
+  int32_t* hit;                  // nullptr when not recorded
+  int32_t* photon_tracking;      // nullptr when not recorded
+};
+
+struct DevSolid {
+  int32_t type;
+  int32_t navigator;
+  float matrix[16];
+  float border_min[3];
+  float border_max[3];
+  float threshold;
+  int32_t number_of_voxels[3];
+  float voxel_sizes[3];
+  const uint8_t* labels;
+  int32_t virtual_element_number[3];
+  float box_size[3];
+  int32_t* histogram;            // nullptr when none
+  int32_t* scatter_histogram;    // nullptr when none
+  int32_t dose_map;              // -1 when none
+};
+
+struct DevSource {
+  int32_t type;
+  float matrix[16];
+  float beam_aperture;
+  double new_aperture;             // 1 - cos(aperture), computed on the host in double
+  float focal_spot_size[3];
+  int32_t number_of_energy_bins;   // n + 1, as passed to the reference kernel
+  const float* energy_spectrum;
+  const float* energy_cdf;
+  int32_t is_interp;
+  int32_t number_of_voxels[3];
+  float voxel_sizes[3];
+  float border_min[3];
+  int32_t number_of_activity_bins;
+  const int32_t* activity_index;
+  const float* activity_cdf;
+};
+
+struct DevParticles {
+  float* E;
+  float* px;
+  float* py;
+  float* pz;
+  float* dx;
+  float* dy;
+  float* dz;
+  int8_t* status;
+  int8_t* scatter;
+  int32_t* solid_id;
+};
+
+struct TransportParams {
+  DevSource source;
+  // batch plan (GGEMSSource::OrganizeParticlesInBatch): sizes are q+1 for the
+  // first r batches and q for the others; nb batches in total.
+  uint64_t q;
+  uint64_t r;
+  uint32_t nb;
+  uint32_t number_of_slots;     // slots touched (= size of batch 0)
+  uint32_t* rng;                // 5 * GG_MAXIMUM_PARTICLES words
+  DevParticles particles;
+  const DevSolid* solids;
+  int32_t number_of_solids;
+  const DevNavigator* navigators;
+  int32_t number_of_navigators;
+  const DevDoseMap* dose_maps;
+  const unsigned char* table_blob;  // HBM copy of the shared-memory tables
+  uint32_t table_bytes;             // multiple of 16
+  int32_t tables_in_smem;
+  unsigned int* slot_counter;       // work queue head
+  int* error;                       // 0 = ok
+};
+
+struct DoseParams {
+  DevDoseMap map;
+  int32_t number_of_voxels[3];
+  float voxel_sizes[3];
+  float border_min[3];
+  const uint8_t* labels;
+  const float* density;     // per material
+  float scale_factor;
+  int32_t is_water_reference;
+  float minimum_density;
+  float* dose;
+  float* uncertainty;
+};
+
+void launch_transport(const TransportParams& p, int grid, size_t smem, void* stream);
+cudaError_t configure_transport(size_t smem, int* blocks_per_sm);
+cudaError_t set_rayleigh_fit(const float* pp);
+void launch_compute_dose(const DoseParams& p, void* stream);
+
+}  // namespace gg
+
+#endif

@@ -1,0 +1,598 @@
+// C-ABI runtime of the B200 transport layer (include/ggems_b200.h).
+//
+// Owns one GPU context: random states, final particle states, the uploaded
+// scene (tables, labels, tallies) and the launch of the transport kernel.
+// Replaces GGEMSOpenCLManager's Allocate / GetDeviceBuffer / CleanBuffer /
+// enqueueNDRangeKernel plumbing (src/global/GGEMSOpenCLManager.cc:836-1046)
+// for the photon path.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "gg_internal.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define GG_CUDA(call)                                                                              \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      return fail(e_ == cudaErrorMemoryAllocation ? GG_ERROR_OUT_OF_MEMORY : GG_ERROR_CUDA,        \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                              \
+  } while (0)
+
+template <class T>
+struct DevArray {
+  T* ptr = nullptr;
+  size_t n = 0;
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    n = 0;
+  }
+};
+
+}  // namespace
+
+struct gg_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sm_count = 0;
+  size_t smem_optin = 0;
+  uint32_t* rng = nullptr;
+  gg::DevParticles particles{};
+  std::vector<void*> scene_allocations;  // freed on re-upload / destroy
+  std::vector<void*> run_allocations;    // source arrays of the last run
+  gg::DevSolid* solids = nullptr;
+  int number_of_solids = 0;
+  gg::DevNavigator* navigators = nullptr;
+  int number_of_navigators = 0;
+  gg::DevDoseMap* dose_maps = nullptr;
+  std::vector<gg::DevDoseMap> dose_host;
+  std::vector<int32_t*> histograms;
+  std::vector<int32_t> histogram_sizes;
+  std::vector<gg_solid> solid_host;       // host copy (labels pointers replaced by device pointers)
+  std::vector<const float*> density_dev;  // per navigator, for dose finalisation
+  unsigned char* table_blob = nullptr;
+  uint32_t table_bytes = 0;
+  bool tables_in_smem = false;
+  unsigned int* slot_counter = nullptr;
+  int* error = nullptr;
+  cudaEvent_t start = nullptr, stop = nullptr;
+  float last_ms = 0.0f;
+  int64_t last_launches = 0;
+  bool scene_ready = false;
+};
+
+namespace {
+
+template <class T>
+int dev_copy(gg_context* c, const T* host, size_t n, T** out) {
+  *out = nullptr;
+  if (n == 0) return GG_OK;
+  void* p = nullptr;
+  GG_CUDA(cudaMalloc(&p, n * sizeof(T)));
+  c->scene_allocations.push_back(p);
+  if (host) GG_CUDA(cudaMemcpyAsync(p, host, n * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+  else GG_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), c->stream));
+  *out = static_cast<T*>(p);
+  return GG_OK;
+}
+
+void free_scene(gg_context* c) {
+  for (void* p : c->scene_allocations) cudaFree(p);
+  c->scene_allocations.clear();
+  c->solids = nullptr;
+  c->navigators = nullptr;
+  c->dose_maps = nullptr;
+  c->table_blob = nullptr;
+  c->dose_host.clear();
+  c->histograms.clear();
+  c->histogram_sizes.clear();
+  c->solid_host.clear();
+  c->density_dev.clear();
+  c->scene_ready = false;
+}
+
+void free_run(gg_context* c) {
+  for (void* p : c->run_allocations) cudaFree(p);
+  c->run_allocations.clear();
+}
+
+uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
+
+}  // namespace
+
+extern "C" {
+
+GG_API const char* gg_last_error(void) { return g_last_error.c_str(); }
+
+GG_API int gg_device_count(int32_t* count) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) {
+    *count = 0;
+    return fail(GG_ERROR_NO_DEVICE, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+  }
+  *count = n;
+  return GG_OK;
+}
+
+GG_API int gg_context_create(int32_t device_index, gg_context** context) {
+  if (!context) return fail(GG_ERROR_INVALID_ARGUMENT, "context pointer is NULL");
+  *context = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(GG_ERROR_NO_DEVICE, "no CUDA device");
+  if (device_index < 0 || device_index >= n) return fail(GG_ERROR_INVALID_ARGUMENT, "device index out of range");
+  GG_CUDA(cudaSetDevice(device_index));
+  cudaDeviceProp prop;
+  GG_CUDA(cudaGetDeviceProperties(&prop, device_index));
+  if (prop.major < 10) return fail(GG_ERROR_NO_DEVICE, std::string("device is not sm_100 class: ") + prop.name);
+  gg_context* c = new gg_context();
+  c->device = device_index;
+  c->sm_count = prop.multiProcessorCount;
+  c->smem_optin = prop.sharedMemPerBlockOptin;
+  const size_t S = GG_MAXIMUM_PARTICLES;
+  auto cleanup = [&](int code) {
+    gg_context_destroy(c);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return cleanup(fail(GG_ERROR_CUDA, "stream"));
+  if (cudaMalloc(&c->rng, 5 * S * sizeof(uint32_t)) != cudaSuccess) return cleanup(fail(GG_ERROR_OUT_OF_MEMORY, "rng"));
+  cudaMemset(c->rng, 0, 5 * S * sizeof(uint32_t));
+  float** fp[7] = {&c->particles.E, &c->particles.px, &c->particles.py, &c->particles.pz,
+                   &c->particles.dx, &c->particles.dy, &c->particles.dz};
+  for (auto f : fp)
+    if (cudaMalloc(reinterpret_cast<void**>(f), S * sizeof(float)) != cudaSuccess)
+      return cleanup(fail(GG_ERROR_OUT_OF_MEMORY, "particles"));
+  if (cudaMalloc(&c->particles.status, S) != cudaSuccess || cudaMalloc(&c->particles.scatter, S) != cudaSuccess ||
+      cudaMalloc(&c->particles.solid_id, S * sizeof(int32_t)) != cudaSuccess)
+    return cleanup(fail(GG_ERROR_OUT_OF_MEMORY, "particles"));
+  if (cudaMalloc(&c->slot_counter, sizeof(unsigned int)) != cudaSuccess ||
+      cudaMalloc(&c->error, sizeof(int)) != cudaSuccess)
+    return cleanup(fail(GG_ERROR_OUT_OF_MEMORY, "counters"));
+  cudaEventCreate(&c->start);
+  cudaEventCreate(&c->stop);
+  *context = c;
+  return GG_OK;
+}
+
+GG_API int gg_context_destroy(gg_context* c) {
+  if (!c) return GG_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_scene(c);
+  free_run(c);
+  cudaFree(c->rng);
+  cudaFree(c->particles.E);
+  cudaFree(c->particles.px);
+  cudaFree(c->particles.py);
+  cudaFree(c->particles.pz);
+  cudaFree(c->particles.dx);
+  cudaFree(c->particles.dy);
+  cudaFree(c->particles.dz);
+  cudaFree(c->particles.status);
+  cudaFree(c->particles.scatter);
+  cudaFree(c->particles.solid_id);
+  cudaFree(c->slot_counter);
+  cudaFree(c->error);
+  if (c->start) cudaEventDestroy(c->start);
+  if (c->stop) cudaEventDestroy(c->stop);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return GG_OK;
+}
+
+GG_API int gg_seed_random_states(uint32_t* states, int64_t number_of_slots, uint32_t seed, int64_t skip_slots) {
+  if (!states || number_of_slots < 0 || number_of_slots > GG_MAXIMUM_PARTICLES || skip_slots < 0)
+    return fail(GG_ERROR_INVALID_ARGUMENT, "bad seeding arguments");
+  std::mt19937 mt(seed);
+  mt.discard(static_cast<unsigned long long>(skip_slots) * 4ull);
+  const size_t S = GG_MAXIMUM_PARTICLES;
+  for (int64_t j = 0; j < number_of_slots; ++j) {
+    states[j] = static_cast<uint32_t>(mt());
+    states[S + j] = static_cast<uint32_t>(mt());
+    states[2 * S + j] = static_cast<uint32_t>(mt());
+    states[3 * S + j] = static_cast<uint32_t>(mt());
+    states[4 * S + j] = 0;
+  }
+  return GG_OK;
+}
+
+GG_API int gg_set_random_states(gg_context* c, const uint32_t* states, int64_t number_of_slots) {
+  if (!c || !states || number_of_slots < 0 || number_of_slots > GG_MAXIMUM_PARTICLES)
+    return fail(GG_ERROR_INVALID_ARGUMENT, "bad random state arguments");
+  GG_CUDA(cudaSetDevice(c->device));
+  const size_t S = GG_MAXIMUM_PARTICLES;
+  for (int k = 0; k < 5; ++k)
+    GG_CUDA(cudaMemcpyAsync(c->rng + k * S, states + k * S, number_of_slots * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                            c->stream));
+  GG_CUDA(cudaStreamSynchronize(c->stream));
+  return GG_OK;
+}
+
+GG_API int gg_get_random_states(gg_context* c, uint32_t* states, int64_t number_of_slots) {
+  if (!c || !states || number_of_slots < 0 || number_of_slots > GG_MAXIMUM_PARTICLES)
+    return fail(GG_ERROR_INVALID_ARGUMENT, "bad random state arguments");
+  GG_CUDA(cudaSetDevice(c->device));
+  const size_t S = GG_MAXIMUM_PARTICLES;
+  for (int k = 0; k < 5; ++k)
+    GG_CUDA(cudaMemcpyAsync(states + k * S, c->rng + k * S, number_of_slots * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                            c->stream));
+  GG_CUDA(cudaStreamSynchronize(c->stream));
+  return GG_OK;
+}
+
+GG_API int gg_upload_scene(gg_context* c, const gg_scene* sc) {
+  if (!c || !sc) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL context or scene");
+  if (sc->number_of_solids < 0 || sc->number_of_solids > gg::kMaxSolids)
+    return fail(GG_ERROR_INVALID_ARGUMENT, "number of solids must be in [0, 64]");
+  if (sc->number_of_tables < 0 || sc->number_of_tables > gg::kMaxNavigators)
+    return fail(GG_ERROR_INVALID_ARGUMENT, "number of navigators must be in [0, 16]");
+  if (!sc->rayleigh_fit) return fail(GG_ERROR_INVALID_ARGUMENT, "scene has no Rayleigh fit table");
+  GG_CUDA(cudaSetDevice(c->device));
+  GG_CUDA(cudaStreamSynchronize(c->stream));
+  free_scene(c);
+  GG_CUDA(gg::set_rayleigh_fit(sc->rayleigh_fit));
+
+  // ---- tables: shared-memory blob + HBM element data ----
+  std::vector<unsigned char> blob;
+  std::vector<gg::DevNavigator> navs(sc->number_of_tables);
+  c->density_dev.assign(sc->number_of_tables, nullptr);
+  for (int n = 0; n < sc->number_of_tables; ++n) {
+    const gg_physics_tables& t = sc->tables[n];
+    if (t.number_of_bins < 2 || t.number_of_bins > GG_MAX_CROSS_SECTION_BINS || t.number_of_materials < 1 ||
+        t.number_of_materials > GG_MAX_MATERIALS || t.number_of_processes < 0 || t.number_of_processes > 3)
+      return fail(GG_ERROR_INVALID_ARGUMENT, "bad table dimensions for navigator " + std::to_string(n));
+    for (int p = 0; p < t.number_of_processes; ++p)
+      if (t.process_id[p] < 0 || t.process_id[p] > 2) return fail(GG_ERROR_INVALID_ARGUMENT, "bad process id");
+    gg::DevNavigator& d = navs[n];
+    d.number_of_bins = t.number_of_bins;
+    d.number_of_materials = t.number_of_materials;
+    d.number_of_processes = t.number_of_processes;
+    for (int p = 0; p < 3; ++p) d.process_id[p] = t.process_id[p];
+    const uint32_t nb = t.number_of_bins, nm = t.number_of_materials;
+    d.energy_bins_offset = static_cast<uint32_t>(blob.size());
+    blob.resize(align16(d.energy_bins_offset + nb * 4), 0);
+    std::memcpy(blob.data() + d.energy_bins_offset, t.energy_bins, nb * 4);
+    d.sigma_offset = static_cast<uint32_t>(blob.size());
+    blob.resize(d.sigma_offset + nm * nb * 16, 0);
+    float* sig = reinterpret_cast<float*>(blob.data() + d.sigma_offset);
+    const size_t block = static_cast<size_t>(nm) * nb;
+    for (uint32_t m = 0; m < nm; ++m)
+      for (uint32_t b = 0; b < nb; ++b)
+        for (int p = 0; p < 3; ++p) sig[(m * nb + b) * 4 + p] = t.cross_sections[p * block + b + nb * m];
+    d.photon_cut_offset = static_cast<uint32_t>(blob.size());
+    blob.resize(align16(d.photon_cut_offset + nm * 4), 0);
+    std::memcpy(blob.data() + d.photon_cut_offset, t.photon_energy_cut, nm * 4);
+    int rc;
+    int32_t* ne;
+    int32_t* eo;
+    uint8_t* z;
+    float* ad;
+    float* dens;
+    if ((rc = dev_copy(c, t.number_of_elements, nm, &ne)) || (rc = dev_copy(c, t.element_offset, nm, &eo)) ||
+        (rc = dev_copy(c, t.atomic_number, static_cast<size_t>(t.total_elements), &z)) ||
+        (rc = dev_copy(c, t.atomic_number_density, static_cast<size_t>(t.total_elements), &ad)) ||
+        (rc = dev_copy(c, t.density, nm, &dens)))
+      return rc;
+    d.number_of_elements = ne;
+    d.element_offset = eo;
+    d.atomic_number = z;
+    d.atomic_number_density = ad;
+    c->density_dev[n] = dens;
+    float* ray = nullptr;
+    if (t.rayleigh_per_atom) {
+      if ((rc = dev_copy(c, t.rayleigh_per_atom, static_cast<size_t>(101) * nb, &ray))) return rc;
+    } else {
+      bool uses_rayleigh = false;
+      for (int p = 0; p < t.number_of_processes; ++p) uses_rayleigh |= t.process_id[p] == GG_RAYLEIGH_SCATTERING;
+      if (uses_rayleigh) return fail(GG_ERROR_INVALID_ARGUMENT, "Rayleigh activated without per-atom table");
+    }
+    d.rayleigh_per_atom = ray;
+  }
+  blob.resize(align16(static_cast<uint32_t>(blob.size())), 0);
+  c->table_bytes = static_cast<uint32_t>(blob.size());
+  int rc;
+  if ((rc = dev_copy(c, blob.data(), blob.size(), &c->table_blob))) return rc;
+  if ((rc = dev_copy(c, navs.data(), navs.size(), &c->navigators))) return rc;
+  c->number_of_navigators = sc->number_of_tables;
+
+  // ---- tallies ----
+  c->histogram_sizes.assign(sc->histogram_sizes, sc->histogram_sizes + sc->number_of_histograms);
+  for (int h = 0; h < sc->number_of_histograms; ++h) {
+    int32_t* p;
+    if ((rc = dev_copy<int32_t>(c, nullptr, c->histogram_sizes[h], &p))) return rc;
+    c->histograms.push_back(p);
+  }
+  for (int d = 0; d < sc->number_of_dose_maps; ++d) {
+    const gg_dose_map& g = sc->dose_maps[d];
+    gg::DevDoseMap m{};
+    std::memcpy(m.size_of_dosels, g.size_of_dosels, sizeof(m.size_of_dosels));
+    std::memcpy(m.inv_size_of_dosels, g.inv_size_of_dosels, sizeof(m.inv_size_of_dosels));
+    std::memcpy(m.border_min, g.border_min, sizeof(m.border_min));
+    std::memcpy(m.border_max, g.border_max, sizeof(m.border_max));
+    std::memcpy(m.number_of_dosels, g.number_of_dosels, sizeof(m.number_of_dosels));
+    m.total_number_of_dosels = g.total_number_of_dosels;
+    m.slice_number_of_dosels = g.slice_number_of_dosels;
+    const size_t n = static_cast<size_t>(g.total_number_of_dosels);
+    if ((rc = dev_copy<unsigned long long>(c, nullptr, n, &m.edep))) return rc;
+    if (g.record_edep_squared && (rc = dev_copy<double>(c, nullptr, n, &m.edep_squared))) return rc;
+    if (g.record_hit && (rc = dev_copy<int32_t>(c, nullptr, n, &m.hit))) return rc;
+    if (g.record_photon_tracking && (rc = dev_copy<int32_t>(c, nullptr, n, &m.photon_tracking))) return rc;
+    c->dose_host.push_back(m);
+  }
+  if ((rc = dev_copy(c, c->dose_host.data(), c->dose_host.size(), &c->dose_maps))) return rc;
+
+  // ---- solids ----
+  std::vector<gg::DevSolid> solids(sc->number_of_solids);
+  c->solid_host.assign(sc->solids, sc->solids + sc->number_of_solids);
+  for (int s = 0; s < sc->number_of_solids; ++s) {
+    const gg_solid& g = sc->solids[s];
+    gg::DevSolid& d = solids[s];
+    if (g.navigator < 0 || g.navigator >= sc->number_of_tables)
+      return fail(GG_ERROR_INVALID_ARGUMENT, "solid navigator out of range");
+    d.type = g.type;
+    d.navigator = g.navigator;
+    std::memcpy(d.matrix, g.obb.matrix, sizeof(d.matrix));
+    std::memcpy(d.border_min, g.obb.border_min, sizeof(d.border_min));
+    std::memcpy(d.border_max, g.obb.border_max, sizeof(d.border_max));
+    d.threshold = g.threshold;
+    std::memcpy(d.number_of_voxels, g.number_of_voxels, sizeof(d.number_of_voxels));
+    std::memcpy(d.voxel_sizes, g.voxel_sizes, sizeof(d.voxel_sizes));
+    std::memcpy(d.virtual_element_number, g.virtual_element_number, sizeof(d.virtual_element_number));
+    std::memcpy(d.box_size, g.box_size, sizeof(d.box_size));
+    d.histogram = (g.histogram >= 0 && g.histogram < sc->number_of_histograms) ? c->histograms[g.histogram] : nullptr;
+    d.scatter_histogram = (g.scatter_histogram >= 0 && g.scatter_histogram < sc->number_of_histograms)
+                              ? c->histograms[g.scatter_histogram]
+                              : nullptr;
+    d.dose_map = (g.dose_map >= 0 && g.dose_map < sc->number_of_dose_maps) ? g.dose_map : -1;
+    d.labels = nullptr;
+    if (g.type == GG_SOLID_VOXELIZED) {
+      const size_t nv = static_cast<size_t>(g.number_of_voxels[0]) * g.number_of_voxels[1] * g.number_of_voxels[2];
+      if (!g.labels || nv == 0) return fail(GG_ERROR_INVALID_ARGUMENT, "voxelized solid without labels");
+      uint8_t* lab;
+      if ((rc = dev_copy(c, g.labels, nv, &lab))) return rc;
+      d.labels = lab;
+      c->solid_host[s].labels = lab;
+    } else if (g.type != GG_SOLID_BOX) {
+      return fail(GG_ERROR_INVALID_ARGUMENT, "solid type not supported by this build");
+    }
+  }
+  if ((rc = dev_copy(c, solids.data(), solids.size(), &c->solids))) return rc;
+  c->number_of_solids = sc->number_of_solids;
+
+  // Tables go to shared memory when they fit next to the solid / navigator copies.
+  const size_t fixed = sizeof(gg::DevSolid) * c->number_of_solids + sizeof(gg::DevNavigator) * c->number_of_navigators + 16;
+  c->tables_in_smem = c->table_bytes + fixed <= 96 * 1024;
+  GG_CUDA(cudaStreamSynchronize(c->stream));
+  c->scene_ready = true;
+  return GG_OK;
+}
+
+GG_API int gg_reset_tallies(gg_context* c) {
+  if (!c || !c->scene_ready) return fail(GG_ERROR_STATE, "no scene uploaded");
+  GG_CUDA(cudaSetDevice(c->device));
+  for (size_t h = 0; h < c->histograms.size(); ++h)
+    GG_CUDA(cudaMemsetAsync(c->histograms[h], 0, c->histogram_sizes[h] * sizeof(int32_t), c->stream));
+  for (auto& m : c->dose_host) {
+    size_t n = static_cast<size_t>(m.total_number_of_dosels);
+    GG_CUDA(cudaMemsetAsync(m.edep, 0, n * 8, c->stream));
+    if (m.edep_squared) GG_CUDA(cudaMemsetAsync(m.edep_squared, 0, n * 8, c->stream));
+    if (m.hit) GG_CUDA(cudaMemsetAsync(m.hit, 0, n * 4, c->stream));
+    if (m.photon_tracking) GG_CUDA(cudaMemsetAsync(m.photon_tracking, 0, n * 4, c->stream));
+  }
+  return GG_OK;
+}
+
+GG_API int gg_batch_plan(uint64_t number_of_particles, uint64_t* batch_sizes, int64_t max_batches, int64_t* count) {
+  if (!count) return fail(GG_ERROR_INVALID_ARGUMENT, "count is NULL");
+  // GGEMSSource::OrganizeParticlesInBatch (src/sources/GGEMSSource.cc:403-425): float ceil.
+  uint64_t nb = static_cast<uint64_t>(std::ceil(static_cast<float>(number_of_particles) / GG_MAXIMUM_PARTICLES));
+  *count = static_cast<int64_t>(nb);
+  if (batch_sizes) {
+    for (uint64_t j = 0; j < nb && static_cast<int64_t>(j) < max_batches; ++j) {
+      if (nb == 1) batch_sizes[j] = number_of_particles;
+      else batch_sizes[j] = number_of_particles / nb + (j < number_of_particles % nb ? 1 : 0);
+    }
+  }
+  return GG_OK;
+}
+
+GG_API int gg_run_source(gg_context* c, const gg_source* src, uint64_t number_of_particles) {
+  if (!c || !src) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL context or source");
+  if (!c->scene_ready) return fail(GG_ERROR_STATE, "no scene uploaded");
+  if (number_of_particles == 0) return GG_OK;
+  if (src->number_of_energy_bins < 1 || !src->energy_spectrum || !src->energy_cdf)
+    return fail(GG_ERROR_INVALID_ARGUMENT, "source has no energy spectrum");
+  GG_CUDA(cudaSetDevice(c->device));
+  GG_CUDA(cudaStreamSynchronize(c->stream));
+  free_run(c);
+  int64_t nb64 = 0;
+  gg_batch_plan(number_of_particles, nullptr, 0, &nb64);
+  const uint64_t nb = static_cast<uint64_t>(nb64);
+  if (nb == 0 || nb > 0xffffffffull) return fail(GG_ERROR_INVALID_ARGUMENT, "bad batch plan");
+  gg::TransportParams P{};
+  P.q = nb == 1 ? number_of_particles : number_of_particles / nb;
+  P.r = nb == 1 ? 0 : number_of_particles % nb;
+  P.nb = static_cast<uint32_t>(nb);
+  const uint64_t slots = P.q + (P.r ? 1 : 0);
+  if (slots > GG_MAXIMUM_PARTICLES) return fail(GG_ERROR_INVALID_ARGUMENT, "batch larger than the slot count");
+  P.number_of_slots = static_cast<uint32_t>(slots);
+
+  gg::DevSource& s = P.source;
+  s.type = src->type;
+  std::memcpy(s.matrix, src->matrix, sizeof(s.matrix));
+  s.beam_aperture = src->beam_aperture;
+  s.new_aperture = 1.0 - std::cos(static_cast<double>(src->beam_aperture));
+  std::memcpy(s.focal_spot_size, src->focal_spot_size, sizeof(s.focal_spot_size));
+  s.number_of_energy_bins = src->number_of_energy_bins + 1;  // GGEMSXRaySource.cc:133
+  s.is_interp = src->is_interp;
+  const size_t ne = static_cast<size_t>(src->number_of_energy_bins) + 1;
+  void* p = nullptr;
+  GG_CUDA(cudaMalloc(&p, ne * 4));
+  c->run_allocations.push_back(p);
+  GG_CUDA(cudaMemcpyAsync(p, src->energy_spectrum, ne * 4, cudaMemcpyHostToDevice, c->stream));
+  s.energy_spectrum = static_cast<const float*>(p);
+  GG_CUDA(cudaMalloc(&p, ne * 4));
+  c->run_allocations.push_back(p);
+  GG_CUDA(cudaMemcpyAsync(p, src->energy_cdf, ne * 4, cudaMemcpyHostToDevice, c->stream));
+  s.energy_cdf = static_cast<const float*>(p);
+  if (src->type == GG_SOURCE_VOXELIZED) {
+    if (src->number_of_activity_bins < 2 || !src->activity_index || !src->activity_cdf)
+      return fail(GG_ERROR_INVALID_ARGUMENT, "voxelized source without activity");
+    std::memcpy(s.number_of_voxels, src->number_of_voxels, sizeof(s.number_of_voxels));
+    std::memcpy(s.voxel_sizes, src->voxel_sizes, sizeof(s.voxel_sizes));
+    std::memcpy(s.border_min, src->border_min, sizeof(s.border_min));
+    s.number_of_activity_bins = static_cast<int32_t>(src->number_of_activity_bins);
+    const size_t na = static_cast<size_t>(src->number_of_activity_bins);
+    GG_CUDA(cudaMalloc(&p, na * 4));
+    c->run_allocations.push_back(p);
+    GG_CUDA(cudaMemcpyAsync(p, src->activity_index, na * 4, cudaMemcpyHostToDevice, c->stream));
+    s.activity_index = static_cast<const int32_t*>(p);
+    GG_CUDA(cudaMalloc(&p, na * 4));
+    c->run_allocations.push_back(p);
+    GG_CUDA(cudaMemcpyAsync(p, src->activity_cdf, na * 4, cudaMemcpyHostToDevice, c->stream));
+    s.activity_cdf = static_cast<const float*>(p);
+  } else if (src->type != GG_SOURCE_XRAY) {
+    return fail(GG_ERROR_INVALID_ARGUMENT, "unknown source type");
+  }
+
+  P.rng = c->rng;
+  P.particles = c->particles;
+  P.solids = c->solids;
+  P.number_of_solids = c->number_of_solids;
+  P.navigators = c->navigators;
+  P.number_of_navigators = c->number_of_navigators;
+  P.dose_maps = c->dose_maps;
+  P.table_blob = c->table_blob;
+  P.table_bytes = c->table_bytes;
+  P.tables_in_smem = c->tables_in_smem ? 1 : 0;
+  P.slot_counter = c->slot_counter;
+  P.error = c->error;
+  size_t smem = (c->tables_in_smem ? c->table_bytes : 0) + sizeof(gg::DevSolid) * c->number_of_solids +
+                sizeof(gg::DevNavigator) * c->number_of_navigators + 16;
+  int blocks_per_sm = 0;
+  GG_CUDA(gg::configure_transport(smem, &blocks_per_sm));
+  if (blocks_per_sm < 1) return fail(GG_ERROR_CUDA, "transport kernel does not fit on an SM");
+  uint64_t grid = static_cast<uint64_t>(blocks_per_sm) * c->sm_count;
+  uint64_t needed = (slots + gg::kBlockThreads - 1) / gg::kBlockThreads;
+  if (grid > needed) grid = needed;
+  GG_CUDA(cudaMemsetAsync(c->slot_counter, 0, sizeof(unsigned int), c->stream));
+  GG_CUDA(cudaMemsetAsync(c->error, 0, sizeof(int), c->stream));
+  GG_CUDA(cudaEventRecord(c->start, c->stream));
+  gg::launch_transport(P, static_cast<int>(grid), smem, c->stream);
+  GG_CUDA(cudaGetLastError());
+  GG_CUDA(cudaEventRecord(c->stop, c->stream));
+  c->last_launches = 1;
+  return GG_OK;
+}
+
+GG_API int gg_synchronize(gg_context* c) {
+  if (!c) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL context");
+  GG_CUDA(cudaSetDevice(c->device));
+  GG_CUDA(cudaStreamSynchronize(c->stream));
+  int err = 0;
+  GG_CUDA(cudaMemcpy(&err, c->error, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) return fail(GG_ERROR_TIMEOUT, "a bounded wait in the transport kernel timed out");
+  cudaEventElapsedTime(&c->last_ms, c->start, c->stop);
+  return GG_OK;
+}
+
+GG_API int gg_last_run_stats(gg_context* c, float* milliseconds, int64_t* kernel_launches) {
+  if (!c) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL context");
+  if (milliseconds) *milliseconds = c->last_ms;
+  if (kernel_launches) *kernel_launches = c->last_launches;
+  return GG_OK;
+}
+
+GG_API int gg_read_tallies(gg_context* c, gg_tally_buffers* t) {
+  if (!c || !t) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL argument");
+  if (!c->scene_ready) return fail(GG_ERROR_STATE, "no scene uploaded");
+  GG_CUDA(cudaSetDevice(c->device));
+  GG_CUDA(cudaStreamSynchronize(c->stream));
+  for (size_t h = 0; h < c->histograms.size(); ++h)
+    if (t->histograms && t->histograms[h])
+      GG_CUDA(cudaMemcpy(t->histograms[h], c->histograms[h], c->histogram_sizes[h] * 4, cudaMemcpyDeviceToHost));
+  for (size_t d = 0; d < c->dose_host.size(); ++d) {
+    const gg::DevDoseMap& m = c->dose_host[d];
+    const size_t n = static_cast<size_t>(m.total_number_of_dosels);
+    if (t->edep && t->edep[d]) {
+      std::vector<long long> q(n);
+      GG_CUDA(cudaMemcpy(q.data(), m.edep, n * 8, cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < n; ++i) t->edep[d][i] = static_cast<double>(q[i]) / gg::kEdepScale;
+    }
+    if (t->edep_squared && t->edep_squared[d] && m.edep_squared)
+      GG_CUDA(cudaMemcpy(t->edep_squared[d], m.edep_squared, n * 8, cudaMemcpyDeviceToHost));
+    if (t->hit && t->hit[d] && m.hit) GG_CUDA(cudaMemcpy(t->hit[d], m.hit, n * 4, cudaMemcpyDeviceToHost));
+    if (t->photon_tracking && t->photon_tracking[d] && m.photon_tracking)
+      GG_CUDA(cudaMemcpy(t->photon_tracking[d], m.photon_tracking, n * 4, cudaMemcpyDeviceToHost));
+  }
+  return GG_OK;
+}
+
+GG_API int gg_read_particles(gg_context* c, gg_particle_buffers* b, int64_t n) {
+  if (!c || !b || n < 0 || n > GG_MAXIMUM_PARTICLES) return fail(GG_ERROR_INVALID_ARGUMENT, "bad arguments");
+  GG_CUDA(cudaSetDevice(c->device));
+  GG_CUDA(cudaStreamSynchronize(c->stream));
+  const gg::DevParticles& p = c->particles;
+  float* dst[7] = {b->E, b->px, b->py, b->pz, b->dx, b->dy, b->dz};
+  float* src[7] = {p.E, p.px, p.py, p.pz, p.dx, p.dy, p.dz};
+  for (int k = 0; k < 7; ++k)
+    if (dst[k]) GG_CUDA(cudaMemcpy(dst[k], src[k], n * 4, cudaMemcpyDeviceToHost));
+  if (b->status) GG_CUDA(cudaMemcpy(b->status, p.status, n, cudaMemcpyDeviceToHost));
+  if (b->scatter) GG_CUDA(cudaMemcpy(b->scatter, p.scatter, n, cudaMemcpyDeviceToHost));
+  if (b->solid_id) GG_CUDA(cudaMemcpy(b->solid_id, p.solid_id, n * 4, cudaMemcpyDeviceToHost));
+  return GG_OK;
+}
+
+GG_API int gg_compute_dose(gg_context* c, int32_t dose_map, int32_t solid, float scale_factor,
+                           int32_t is_water_reference, float minimum_density, float* dose, float* uncertainty) {
+  if (!c || !c->scene_ready || !dose) return fail(GG_ERROR_INVALID_ARGUMENT, "bad arguments");
+  if (dose_map < 0 || dose_map >= static_cast<int>(c->dose_host.size()) || solid < 0 ||
+      solid >= static_cast<int>(c->solid_host.size()) || c->solid_host[solid].type != GG_SOLID_VOXELIZED)
+    return fail(GG_ERROR_INVALID_ARGUMENT, "dose map or solid out of range");
+  GG_CUDA(cudaSetDevice(c->device));
+  const gg_solid& s = c->solid_host[solid];
+  gg::DoseParams P{};
+  P.map = c->dose_host[dose_map];
+  std::memcpy(P.number_of_voxels, s.number_of_voxels, sizeof(P.number_of_voxels));
+  std::memcpy(P.voxel_sizes, s.voxel_sizes, sizeof(P.voxel_sizes));
+  std::memcpy(P.border_min, s.obb.border_min, sizeof(P.border_min));
+  P.labels = s.labels;
+  P.density = c->density_dev[s.navigator];
+  P.scale_factor = scale_factor;
+  P.is_water_reference = is_water_reference;
+  P.minimum_density = minimum_density;
+  const size_t n = static_cast<size_t>(P.map.total_number_of_dosels);
+  float* d_dose = nullptr;
+  float* d_unc = nullptr;
+  GG_CUDA(cudaMalloc(&d_dose, n * 4));
+  if (uncertainty && cudaMalloc(&d_unc, n * 4) != cudaSuccess) {
+    cudaFree(d_dose);
+    return fail(GG_ERROR_OUT_OF_MEMORY, "uncertainty buffer");
+  }
+  P.dose = d_dose;
+  P.uncertainty = d_unc;
+  gg::launch_compute_dose(P, c->stream);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dose, d_dose, n * 4, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && uncertainty) e = cudaMemcpyAsync(uncertainty, d_unc, n * 4, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(d_dose);
+  if (d_unc) cudaFree(d_unc);
+  if (e != cudaSuccess) return fail(GG_ERROR_CUDA, std::string("compute dose: ") + cudaGetErrorString(e));
+  return GG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,803 @@
+// Photon transport kernels for sm_100a.
+//
+// One persistent kernel runs the whole GGEMS photon loop for every history:
+// primary generation (X-ray cone or voxelized source), FindSolid /
+// ProjectToSolid over all solids, and the per-step tracking through the
+// current solid (voxelized phantom or CT detector box), with Compton,
+// photoelectric and Rayleigh sampling from GGEMS's tables and the dose /
+// histogram tallies.  It replaces the reference's host loop of
+// 2*S+2 launches per iteration (src/global/GGEMS.cc:303-363,
+// src/navigators/GGEMSNavigator.cc:320-530) and its is_alive round trip.
+//
+// Design:
+//  * each lane owns one random slot (JKISS state in registers) and runs that
+//    slot's histories in batch order, so every history draws exactly the
+//    random numbers the reference's slot would; lanes fetch slots from a
+//    device work counter;
+//  * a lane advances one "step" per loop iteration (a voxel step, a box step,
+//    or a FindSolid/ProjectToSolid round), and starts its next history as
+//    soon as one ends, so lanes never idle while others finish long histories;
+//  * the per-navigator cross-section tables (float4 per material and energy
+//    bin), energy bins and photon cuts are staged into shared memory with
+//    cp.async.bulk completing on an mbarrier (bounded wait);
+//  * tallies: int32 histogram counts, int64 fixed-point energy deposits
+//    (order independent), double energy^2.
+//
+// Arithmetic follows the reference operation by operation in float (double
+// where it uses double) and the file is compiled with -fmad=false so that no
+// multiply-add is contracted; the CPU oracle does the same.
+#include <cfloat>
+#include <cstdint>
+
+#include "gg_internal.cuh"
+
+namespace gg {
+namespace {
+
+constexpr float kTwoPi = 6.283185307179586f;             // GGEMSConstants.hh:39
+constexpr float kElectronMassC2 = 0.510998910f;           // GGEMSConstants.hh:52
+constexpr float kTolerance = 5.0e-04f;                    // GGEMSGeometryConstants.hh:39
+constexpr float kEps6 = 1.0e-06f;                         // GGEMSGeometryConstants.hh:38
+constexpr float kOutOfWorld = FLT_MAX;                    // GGEMSParticleConstants.hh:44
+constexpr int kNoProcess = 99;
+constexpr float kRayleighFactor = 32526509815670243328.0f;  // GGEMSRayleighScatteringModels.hh:36
+// KissUniform's (float)((double)x / 4294967295.0 * (1 - 2^-23)) equals
+// (float)((double)x * kKissScale) for every float x = (float)(uint32): checked
+// exhaustively over all 83,886,080 such values (tests/test_rng.py).
+constexpr double kKissScale = (1.0 / 4294967295.0) * 0.99999988079071044921875;
+
+enum Phase : int { kNewHistory = 0, kFind = 1, kTrackVoxel = 2, kTrackBox = 3, kDone = 4 };
+
+struct V3 {
+  float x, y, z;
+};
+__device__ __forceinline__ V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+__device__ __forceinline__ V3 add(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ V3 sub(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ V3 mul(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+__device__ __forceinline__ V3 divv(V3 a, V3 b) { return v3(a.x / b.x, a.y / b.y, a.z / b.z); }
+__device__ __forceinline__ V3 scale(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3 normalize3(V3 v) { return scale(v, 1.0f / sqrtf(dot3(v, v))); }
+
+// GGfloat44 (row-major) products, GGEMSMatrixOperations.hh:46-125.
+__device__ __forceinline__ V3 m_point(const float* m, V3 p) {
+  return v3(m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3] * 1.0f, m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7] * 1.0f,
+            m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11] * 1.0f);
+}
+__device__ __forceinline__ V3 m33(const float* m, V3 p) {
+  return v3(m[0] * p.x + m[1] * p.y + m[2] * p.z, m[4] * p.x + m[5] * p.y + m[6] * p.z, m[8] * p.x + m[9] * p.y + m[10] * p.z);
+}
+__device__ __forceinline__ V3 m33t(const float* m, V3 p) {
+  return v3(m[0] * p.x + m[4] * p.y + m[8] * p.z, m[1] * p.x + m[5] * p.y + m[9] * p.z, m[2] * p.x + m[6] * p.y + m[10] * p.z);
+}
+// GGEMSReferentialTransformation.hh:80-141
+__device__ __forceinline__ V3 g2l_pos(const float* m, V3 p) { return m33t(m, v3(p.x - m[3], p.y - m[7], p.z - m[11])); }
+__device__ __forceinline__ V3 l2g_pos(const float* m, V3 p) { return m_point(m, p); }
+__device__ __forceinline__ V3 g2l_dir(const float* m, V3 d) { return normalize3(m33t(m, d)); }
+__device__ __forceinline__ V3 l2g_dir(const float* m, V3 d) { return normalize3(m33(m, d)); }
+
+// RotateUnitZ, GGEMSReferentialTransformation.hh:44-70
+__device__ __forceinline__ V3 rotate_uz(V3 v, V3 u) {
+  float up = u.x * u.x + u.y * u.y;
+  if (up > 0) {
+    up = sqrtf(up);
+    float px = v.x, py = v.y, pz = v.z;
+    v.x = (u.x * u.z * px - u.y * py) / up + u.x * pz;
+    v.y = (u.y * u.z * px + u.x * py) / up + u.y * pz;
+    v.z = -up * px + u.z * pz;
+  } else if (u.z < 0.0f) {
+    v.x = -v.x;
+    v.z = -v.z;
+  }
+  return v;
+}
+
+// BinarySearch / LinearInterpolation, GGEMSMathAlgorithms.hh:46-86
+__device__ __forceinline__ int binary_search(float key, const float* a, int size) {
+  int low = 0, high = size - 1;
+  while (high - low > 1) {
+    int mid = (high + low) / 2;
+    float v = a[mid];
+    if (v == key) return mid;
+    if (v < key) low = mid;
+    else high = mid;
+  }
+  return low;
+}
+__device__ __forceinline__ float lerp_ref(float xa, float ya, float xb, float yb, float x) {
+  if (xa > xb) return yb;
+  if (xa >= x) return ya;
+  if (xb <= x) return yb;
+  return ya + (x - xa) * (yb - ya) / (xb - xa);
+}
+
+// Ray tracing, GGEMSRayTracing.hh:60-326
+__device__ __forceinline__ float safety_in(float p, float mn, float mx) {
+  float a = fabsf(p - mn), b = fabsf(p - mx);
+  p = (a < kTolerance) ? mn + kTolerance : p;
+  return (b < kTolerance) ? mx - kTolerance : p;
+}
+__device__ __forceinline__ float safety_out(float p, float mn, float mx) {
+  float a = fabsf(p - mn), b = fabsf(p - mx);
+  p = (a < kTolerance) ? mn - kTolerance : p;
+  return (b < kTolerance) ? mx + kTolerance : p;
+}
+__device__ __forceinline__ V3 safety_inside(V3 p, V3 mn, V3 mx) {
+  return v3(safety_in(p.x, mn.x, mx.x), safety_in(p.y, mn.y, mx.y), safety_in(p.z, mn.z, mx.z));
+}
+__device__ __forceinline__ V3 safety_outside(V3 p, V3 mn, V3 mx) {
+  return v3(safety_out(p.x, mn.x, mx.x), safety_out(p.y, mn.y, mx.y), safety_out(p.z, mn.z, mx.z));
+}
+__device__ __forceinline__ bool in_aabb(V3 p, V3 mn, V3 mx) {
+  if (p.x < (mn.x + kTolerance) || p.x > (mx.x - kTolerance)) return false;
+  if (p.y < (mn.y + kTolerance) || p.y > (mx.y - kTolerance)) return false;
+  if (p.z < (mn.z + kTolerance) || p.z > (mx.z - kTolerance)) return false;
+  return true;
+}
+__device__ __forceinline__ float distance_to_aabb(V3 p, V3 d, V3 mn, V3 mx) {
+  float tmin = FLT_MIN, tmax = FLT_MAX;
+  if (fabsf(d.x) < kEps6) {
+    if (p.x < mn.x || p.x > mx.x) return kOutOfWorld;
+  } else {
+    float id = 1.0f / d.x;
+    tmin = (mn.x - p.x) * id;
+    tmax = (mx.x - p.x) * id;
+    if (tmin > tmax) {
+      float t = tmin;
+      tmin = tmax;
+      tmax = t;
+    }
+  }
+  if (fabsf(d.y) < kEps6) {
+    if (p.y < mn.y || p.y > mx.y) return kOutOfWorld;
+  } else {
+    float id = 1.0f / d.y;
+    float lo = (mn.y - p.y) * id, hi = (mx.y - p.y) * id;
+    if (lo > hi) {
+      float t = lo;
+      lo = hi;
+      hi = t;
+    }
+    if (lo > tmin) tmin = lo;
+    if (hi < tmax) tmax = hi;
+    if (tmin > tmax) return kOutOfWorld;
+  }
+  if (fabsf(d.z) < kEps6) {
+    if (p.z < mn.z || p.z > mx.z) return kOutOfWorld;
+  } else {
+    float id = 1.0f / d.z;
+    float lo = (mn.z - p.z) * id, hi = (mx.z - p.z) * id;
+    if (lo > hi) {
+      float t = lo;
+      lo = hi;
+      hi = t;
+    }
+    if (lo > tmin) tmin = lo;
+    if (hi < tmax) tmax = hi;
+    if (tmin > tmax) return kOutOfWorld;
+  }
+  if (tmin < 0.0f && (tmax < 0.0f || tmax == 0.0f)) return kOutOfWorld;
+  if (static_cast<double>(tmax - tmin) < (2.0 * static_cast<double>(kTolerance))) return kOutOfWorld;
+  if (tmin <= kEps6) return tmax;
+  return tmin;
+}
+
+// JKISS32, GGEMSKissEngine.hh:50-75
+struct Kiss {
+  uint32_t s1, s2, s3, s4, s5;
+  __device__ __forceinline__ float uniform() {
+    s2 ^= (s2 << 5);
+    s2 ^= (s2 >> 7);
+    s2 ^= (s2 << 22);
+    int t = static_cast<int>(s3 + s4 + s5);
+    s3 = s4;
+    s5 = t < 0;
+    s4 = static_cast<uint32_t>(t) & 2147483647u;
+    s1 += 1411392427u;
+    return __double2float_rn(static_cast<double>(__uint2float_rn(s1 + s2 + s4)) * kKissScale);
+  }
+};
+
+struct Photon {
+  V3 p, d;          // global outside solids, local while tracking inside one
+  float E;
+  float psd;        // particle_solid_distance_
+  int solid_id;
+  int8_t status;
+  int8_t scatter;
+};
+
+// Tables (shared memory when they fit, otherwise the HBM blob).
+struct Tab {
+  const unsigned char* base;
+  const DevNavigator* nav;
+  __device__ __forceinline__ const float* energy_bins(int n) const {
+    return reinterpret_cast<const float*>(base + nav[n].energy_bins_offset);
+  }
+  __device__ __forceinline__ const float4* sigma(int n) const {
+    return reinterpret_cast<const float4*>(base + nav[n].sigma_offset);
+  }
+  __device__ __forceinline__ const float* photon_cut(int n) const {
+    return reinterpret_cast<const float*>(base + nav[n].photon_cut_offset);
+  }
+};
+
+__device__ __forceinline__ float pick(float4 s, int pid) { return pid == 0 ? s.x : (pid == 1 ? s.y : s.z); }
+
+// GetPhotonNextInteraction, GGEMSPhotonNavigator.hh:57-93.  Returns the
+// distance, writes the process; energy_id is the cached BinarySearch result.
+__device__ __forceinline__ float next_interaction(Kiss& rng, const DevNavigator& nv, const float4* sig, int energy_id,
+                                                  int material, int& proc) {
+  float4 s = sig[material * nv.number_of_bins + energy_id];
+  float nid = kOutOfWorld;
+  proc = kNoProcess;
+  for (int i = 0; i < nv.number_of_processes; ++i) {
+    int pid = nv.process_id[i];
+    float dist = -logf(rng.uniform()) / pick(s, pid);
+    if (dist < nid) {
+      nid = dist;
+      proc = pid;
+    }
+  }
+  return nid;
+}
+
+// KleinNishinaComptonSampleSecondaries, GGEMSComptonScatteringModels.hh:47-132
+__device__ __noinline__ void compton(Photon& ph, Kiss& rng) {
+  float E0 = ph.E;
+  float E0m = E0 / kElectronMassC2;
+  V3 gd = ph.d;
+  float eps0 = 1.0f / (1.0f + 2.0f * E0m);
+  float eps0sq = eps0 * eps0;
+  float alpha1 = -logf(eps0);
+  float alpha2 = alpha1 + 0.5f * (1.0f - eps0sq);
+  float eps, epssq, onecost, sint2, greject, r3;
+  int nloop = 0;
+  do {
+    ++nloop;
+    if (nloop > 1000) return;
+    float r1 = rng.uniform();
+    float r2 = rng.uniform();
+    r3 = rng.uniform();
+    if (alpha1 > alpha2 * r1) {
+      eps = expf(-alpha1 * r2);
+      epssq = eps * eps;
+    } else {
+      epssq = eps0sq + (1.0f - eps0sq) * r2;
+      eps = sqrtf(epssq);
+    }
+    onecost = (1.0f - eps) / (eps * E0m);
+    sint2 = onecost * (2.0f - onecost);
+    greject = 1.0f - eps * sint2 / (1.0f + epssq);
+  } while (greject < r3);
+  if (sint2 < 0.0f) sint2 = 0.0f;
+  float cost = 1.0f - onecost;
+  float sint = sqrtf(sint2);
+  float phi = rng.uniform() * kTwoPi;
+  V3 g = v3(sint * cosf(phi), sint * sinf(phi), cost);
+  g = normalize3(rotate_uz(g, gd));
+  ph.E = E0 * eps;
+  ph.d = g;
+}
+
+__constant__ float c_rayleigh_pp[9][101];
+
+__device__ __forceinline__ float rayleigh_w(float x, float n) {
+  return (x < 0.02f) ? n * x * (1.0f - 0.5f * (n - 1.0f) * x * (1.0f - (n - 2.0f) * x / 3.0f))
+                     : 1.0f - expf(-n * logf(1.0f + x));
+}
+
+// LivermoreRayleighSampleSecondaries, GGEMSRayleighScatteringModels.hh:169-316
+__device__ __noinline__ void rayleigh(Photon& ph, Kiss& rng, const DevNavigator& nv, const float* ebins,
+                                      const float4* sig, int material, int energy_id) {
+  float E0 = ph.E;
+  if (E0 <= 250.0e-6f) {
+    ph.status = GG_DEAD;
+    return;
+  }
+  V3 gd = ph.d;
+  const int nb = nv.number_of_bins;
+  int n_minus_one = static_cast<int8_t>(nv.number_of_elements[material] - 1);
+  int mixture = nv.element_offset[material];
+  int z = nv.atomic_number[mixture + n_minus_one];
+  if (n_minus_one > 0) {
+    float kcs = lerp_ref(ebins[energy_id], sig[material * nb + energy_id].z, ebins[energy_id + 1],
+                         sig[material * nb + energy_id + 1].z, E0);
+    float x = rng.uniform() * kcs;
+    float cs = 0.0f;
+    for (int i = 0; i < n_minus_one; ++i) {
+      int zi = nv.atomic_number[mixture + i];
+      const float* pa = nv.rayleigh_per_atom + nb * zi;
+      cs += nv.atomic_number_density[mixture + i] *
+            lerp_ref(ebins[energy_id], pa[energy_id], ebins[energy_id + 1], pa[energy_id + 1], E0);
+      if (x < cs) {
+        z = zi;
+        break;
+      }
+    }
+  }
+  float xx = kRayleighFactor * E0 * E0;
+  float n0 = c_rayleigh_pp[6][z] - 1.0f, n1 = c_rayleigh_pp[7][z] - 1.0f, n2 = c_rayleigh_pp[8][z] - 1.0f;
+  float b0 = c_rayleigh_pp[3][z], b1 = c_rayleigh_pp[4][z], b2 = c_rayleigh_pp[5][z];
+  float w0 = rayleigh_w(2.0f * xx * b0, n0);
+  float w1 = rayleigh_w(2.0f * xx * b1, n1);
+  float w2 = rayleigh_w(2.0f * xx * b2, n2);
+  float x0 = w0 * c_rayleigh_pp[0][z] / (b0 * n0);
+  float x1 = w1 * c_rayleigh_pp[1][z] / (b1 * n1);
+  float x2 = w2 * c_rayleigh_pp[2][z] / (b2 * n2);
+  float cost;
+  do {
+    float w = w0, n = n0, b = b0;
+    float x = rng.uniform() * (x0 + x1 + x2);
+    if (x > x0) {
+      x -= x0;
+      if (x <= x1) {
+        w = w1; n = n1; b = b1;
+      } else {
+        w = w2; n = n2; b = b2;
+      }
+    }
+    n = 1.0f / n;
+    float y = rng.uniform() * w;
+    if (y < 0.02f) x = y * n * (1.0f + 0.5f * (n + 1.0f) * y * (1.0f - (n + 2.0f) * y / 3.0f));
+    else x = expf(-n * logf(1.0f - y)) - 1.0f;
+    cost = 1.0f - x / (b * xx);
+  } while (2.0f * rng.uniform() > 1.0f + cost * cost || cost < -1.0f);
+  float phi = kTwoPi * rng.uniform();
+  float sint = sqrtf((1.0f - cost) * (1.0f + cost));
+  V3 g = v3(sint * cosf(phi), sint * sinf(phi), cost);
+  ph.d = normalize3(rotate_uz(g, gd));
+}
+
+// dose_record_standard / dose_photon_tracking, GGEMSDoseRecording.hh:65-118
+__device__ __forceinline__ int dosel(const DevDoseMap& dm, V3 p) {
+  if (p.x < dm.border_min[0] + kEps6 || p.x > dm.border_max[0] - kEps6) return -1;
+  if (p.y < dm.border_min[1] + kEps6 || p.y > dm.border_max[1] - kEps6) return -1;
+  if (p.z < dm.border_min[2] + kEps6 || p.z > dm.border_max[2] - kEps6) return -1;
+  int ix = __float2int_rz((p.x - dm.border_min[0]) * dm.inv_size_of_dosels[0]);
+  int iy = __float2int_rz((p.y - dm.border_min[1]) * dm.inv_size_of_dosels[1]);
+  int iz = __float2int_rz((p.z - dm.border_min[2]) * dm.inv_size_of_dosels[2]);
+  if (ix < 0 || ix >= dm.number_of_dosels[0]) return -1;
+  if (iy < 0 || iy >= dm.number_of_dosels[1]) return -1;
+  if (iz < 0 || iz >= dm.number_of_dosels[2]) return -1;
+  return ix + iy * dm.number_of_dosels[0] + iz * dm.number_of_dosels[0] * dm.number_of_dosels[1];
+}
+__device__ __forceinline__ void dose_record(const DevDoseMap& dm, float edep, V3 p) {
+  int id = dosel(dm, p);
+  if (id < 0) return;
+  if (dm.hit) atomicAdd(dm.hit + id, 1);
+  long long q = __double2ll_rn(static_cast<double>(edep) * kEdepScale);
+  atomicAdd(dm.edep + id, static_cast<unsigned long long>(q));
+  if (dm.edep_squared) atomicAdd(dm.edep_squared + id, static_cast<double>(edep) * static_cast<double>(edep));
+}
+
+// get_primaries_ggems_xray_source, GetPrimariesGGEMSXRaySource.cl:52-143
+__device__ void xray_primary(Photon& ph, Kiss& rng, const DevSource& s, double new_aperture) {
+  double phi = rng.uniform();
+  double theta = rng.uniform();
+  phi *= static_cast<double>(kTwoPi);
+  theta = acos(1.0 - new_aperture * theta);
+  double st = sin(theta);
+  V3 rot = v3(static_cast<float>(cos(phi) * st), static_cast<float>(sin(phi) * st), static_cast<float>(cos(theta)));
+  V3 gp = l2g_pos(s.matrix, v3(0.0f, 0.0f, 0.0f));
+  V3 dir = normalize3(sub(v3(0.0f, 0.0f, 0.0f), gp));
+  dir = normalize3(rotate_uz(rot, dir));
+  gp.x = s.focal_spot_size[0] * (rng.uniform() - 0.5f);
+  gp.y = s.focal_spot_size[1] * (rng.uniform() - 0.5f);
+  gp.z = s.focal_spot_size[2] * (rng.uniform() - 0.5f);
+  gp = l2g_pos(s.matrix, gp);
+  int index = 0;
+  float rnd = 0.0f;
+  if (s.number_of_energy_bins != 1) {
+    rnd = rng.uniform();
+    index = binary_search(rnd, s.energy_cdf, s.number_of_energy_bins + 1);
+  }
+  ph.E = !s.is_interp ? s.energy_spectrum[index]
+                      : lerp_ref(s.energy_cdf[index], s.energy_spectrum[index], s.energy_cdf[index + 1],
+                                 s.energy_spectrum[index + 1], rnd);
+  ph.p = gp;
+  ph.d = dir;
+}
+
+// get_primaries_ggems_voxelized_source, GetPrimariesGGEMSVoxelizedSource.cl:57-150
+__device__ void voxelized_primary(Photon& ph, Kiss& rng, const DevSource& s) {
+  double phi = rng.uniform();
+  double theta = rng.uniform();
+  phi *= static_cast<double>(kTwoPi);
+  theta = acos(1.0 - 2.0 * theta);
+  double st = sin(theta);
+  V3 dir = v3(static_cast<float>(cos(phi) * st), static_cast<float>(sin(phi) * st), static_cast<float>(cos(theta)));
+  float rnd_act = rng.uniform();
+  int ia = binary_search(rnd_act, s.activity_cdf, s.number_of_activity_bins);
+  int vox = s.activity_index[ia];
+  int nx = s.number_of_voxels[0], slice = nx * s.number_of_voxels[1];
+  int iz = vox / slice;
+  int ix = (vox - iz * slice) % nx;
+  int iy = (vox - iz * slice) / nx;
+  V3 bmin = v3(s.border_min[0], s.border_min[1], s.border_min[2]);
+  V3 vs = v3(s.voxel_sizes[0], s.voxel_sizes[1], s.voxel_sizes[2]);
+  V3 vmin = add(bmin, mul(v3(static_cast<float>(ix), static_cast<float>(iy), static_cast<float>(iz)), vs));
+  V3 vmax = add(vmin, vs);
+  V3 p;
+  p.x = bmin.x + (static_cast<float>(ix) + rng.uniform()) * vs.x;
+  p.y = bmin.y + (static_cast<float>(iy) + rng.uniform()) * vs.y;
+  p.z = bmin.z + (static_cast<float>(iz) + rng.uniform()) * vs.z;
+  p = safety_inside(p, vmin, vmax);
+  ph.p = l2g_pos(s.matrix, p);
+  int index = 0;
+  float rnd = 0.0f;
+  if (s.number_of_energy_bins != 1) {
+    rnd = rng.uniform();
+    index = binary_search(rnd, s.energy_cdf, s.number_of_energy_bins + 1);
+  }
+  ph.E = !s.is_interp ? s.energy_spectrum[index]
+                      : lerp_ref(s.energy_cdf[index], s.energy_spectrum[index], s.energy_cdf[index + 1],
+                                 s.energy_spectrum[index + 1], rnd);
+  ph.d = dir;
+}
+
+// ---- shared-memory staging with bounded waits ----
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Copies `bytes` (multiple of 16) from HBM into shared memory with
+// cp.async.bulk and waits on an mbarrier for at most ~`limit` polls.
+// Returns false (and sets *error) when the copy did not complete in time.
+__device__ bool stage_tables(unsigned char* dst, const unsigned char* src, uint32_t bytes, uint64_t* bar, int* error) {
+  constexpr uint32_t kChunk = 16384;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+    for (uint32_t off = 0; off < bytes; off += kChunk) {
+      uint32_t n = bytes - off < kChunk ? bytes - off : kChunk;
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              smem_u32(dst + off)),
+          "l"(src + off), "r"(n), "r"(smem_u32(bar))
+          : "memory");
+    }
+  }
+  uint32_t done = 0;
+  for (int i = 0; i < (1 << 22) && !done; ++i) {
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(smem_u32(bar))
+        : "memory");
+  }
+  if (!done) atomicExch(error, 1);
+  return __syncthreads_and(done) != 0;
+}
+
+extern __shared__ __align__(16) unsigned char g_smem[];
+
+__global__ void __launch_bounds__(kBlockThreads, 2) transport_kernel(TransportParams P) {
+  // shared memory: [tables][solids][navigators][mbarrier]
+  unsigned char* tables = g_smem;
+  DevSolid* solids = reinterpret_cast<DevSolid*>(g_smem + (P.tables_in_smem ? P.table_bytes : 0));
+  DevNavigator* navs = reinterpret_cast<DevNavigator*>(solids + P.number_of_solids);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(navs + P.number_of_navigators);
+  for (int i = threadIdx.x; i < P.number_of_solids; i += blockDim.x) solids[i] = P.solids[i];
+  for (int i = threadIdx.x; i < P.number_of_navigators; i += blockDim.x) navs[i] = P.navigators[i];
+  Tab tab{P.table_blob, navs};
+  if (P.tables_in_smem) {
+    if (!stage_tables(tables, P.table_blob, P.table_bytes, bar, P.error)) return;
+    tab.base = tables;
+  } else {
+    __syncthreads();
+  }
+
+  const double new_aperture = P.source.new_aperture;
+  const size_t S = GG_MAXIMUM_PARTICLES;
+
+  Kiss rng{0, 0, 0, 0, 0};
+  Photon ph{};
+  ph.solid_id = -1;
+  uint32_t slot = 0;
+  uint32_t histories_left = 0;
+  int rounds = 0;
+  int phase = kDone;
+  int energy_id = 0;
+  float cached_E = -1.0f;
+  int cached_nav = -1;
+
+  // Grab the first slot.
+  auto next_slot = [&]() -> bool {
+    slot = atomicAdd(P.slot_counter, 1u);
+    if (slot >= P.number_of_slots) return false;
+    rng = Kiss{P.rng[slot], P.rng[S + slot], P.rng[2 * S + slot], P.rng[3 * S + slot], P.rng[4 * S + slot]};
+    histories_left = slot < P.q ? P.nb : (slot < P.q + 1 && P.r > 0 ? static_cast<uint32_t>(P.r) : 0u);
+    ph.solid_id = -1;
+    return histories_left > 0;
+  };
+  auto finish_slot = [&]() {
+    P.rng[slot] = rng.s1;
+    P.rng[S + slot] = rng.s2;
+    P.rng[2 * S + slot] = rng.s3;
+    P.rng[3 * S + slot] = rng.s4;
+    P.rng[4 * S + slot] = rng.s5;
+    if (P.particles.E) {
+      P.particles.E[slot] = ph.E;
+      P.particles.px[slot] = ph.p.x;
+      P.particles.py[slot] = ph.p.y;
+      P.particles.pz[slot] = ph.p.z;
+      P.particles.dx[slot] = ph.d.x;
+      P.particles.dy[slot] = ph.d.y;
+      P.particles.dz[slot] = ph.d.z;
+      P.particles.status[slot] = ph.status;
+      P.particles.scatter[slot] = ph.scatter;
+      P.particles.solid_id[slot] = ph.solid_id;
+    }
+  };
+
+  if (next_slot()) phase = kNewHistory;
+
+  while (phase != kDone) {
+    if (phase == kNewHistory) {
+      if (P.source.type == GG_SOURCE_XRAY) xray_primary(ph, rng, P.source, new_aperture);
+      else voxelized_primary(ph, rng, P.source);
+      ph.scatter = 0;
+      ph.status = GG_ALIVE;
+      ph.psd = kOutOfWorld;
+      rounds = 0;
+      phase = kFind;
+      continue;
+    }
+
+    if (phase == kFind) {
+      bool end = rounds >= GG_MAX_LOOP;
+      if (!end && P.number_of_solids == 0) {
+        ++rounds;  // no navigator: the reference loop only counts iterations
+      } else if (!end) {
+        ++rounds;
+        // particle_solid_distance_* (ParticleSolidDistanceGGEMS*.cl:43-108)
+        for (int s = 0; s < P.number_of_solids; ++s) {
+          if (ph.status == GG_DEAD || ph.psd == 0.0f) break;
+          const DevSolid& so = solids[s];
+          V3 mn = v3(so.border_min[0], so.border_min[1], so.border_min[2]);
+          V3 mx = v3(so.border_max[0], so.border_max[1], so.border_max[2]);
+          V3 lp = g2l_pos(so.matrix, ph.p);
+          if (in_aabb(lp, mn, mx)) {
+            ph.psd = 0.0f;
+            ph.solid_id = s;
+            break;
+          }
+          float dist = distance_to_aabb(lp, g2l_dir(so.matrix, ph.d), mn, mx);
+          if (dist < ph.psd) {
+            ph.psd = dist;
+            ph.solid_id = s;
+          }
+        }
+        // project_to_* (ProjectToGGEMS*.cl:44-129)
+        if (ph.solid_id == -1) ph.status = GG_DEAD;
+        if (ph.psd == kOutOfWorld) {
+          ph.solid_id = -1;
+          ph.status = GG_DEAD;
+        } else if (ph.status != GG_DEAD) {
+          const DevSolid& so = solids[ph.solid_id];
+          ph.p = add(ph.p, scale(ph.d, ph.psd + kTolerance));
+          V3 lp = g2l_pos(so.matrix, ph.p);
+          lp = safety_inside(lp, v3(so.border_min[0], so.border_min[1], so.border_min[2]),
+                             v3(so.border_max[0], so.border_max[1], so.border_max[2]));
+          ph.p = l2g_pos(so.matrix, lp);
+          ph.psd = 0.0f;
+        }
+        if (ph.status == GG_DEAD) {
+          end = true;
+        } else {
+          // Enter the solid: switch to local coordinates.
+          const DevSolid& so = solids[ph.solid_id];
+          ph.p = g2l_pos(so.matrix, ph.p);
+          ph.d = g2l_dir(so.matrix, ph.d);
+          phase = so.type == GG_SOLID_VOXELIZED ? kTrackVoxel : kTrackBox;
+        }
+      }
+      if (end) {
+        if (--histories_left > 0) {
+          phase = kNewHistory;
+        } else {
+          finish_slot();
+          phase = next_slot() ? kNewHistory : kDone;
+        }
+      }
+      continue;
+    }
+
+    // ---- one tracking step inside solid ph.solid_id ----
+    const DevSolid& so = solids[ph.solid_id];
+    const int nav = so.navigator;
+    const DevNavigator& nv = navs[nav];
+    const float* ebins = tab.energy_bins(nav);
+    const float4* sig = tab.sigma(nav);
+    V3 bmin = v3(so.border_min[0], so.border_min[1], so.border_min[2]);
+    V3 bmax = v3(so.border_max[0], so.border_max[1], so.border_max[2]);
+    bool exit_solid = false;
+    bool dead = false;
+    if (ph.E != cached_E || nav != cached_nav) {
+      energy_id = binary_search(ph.E, ebins, nv.number_of_bins);
+      cached_E = ph.E;
+      cached_nav = nav;
+    }
+
+    if (phase == kTrackVoxel) {
+      // track_through_ggems_voxelized_solid, TrackThroughGGEMSVoxelizedSolid.cl:133-310
+      V3 vs = v3(so.voxel_sizes[0], so.voxel_sizes[1], so.voxel_sizes[2]);
+      V3 q = divv(sub(ph.p, bmin), vs);
+      int ix = __float2int_rz(q.x), iy = __float2int_rz(q.y), iz = __float2int_rz(q.z);
+      const int nx = so.number_of_voxels[0], ny = so.number_of_voxels[1], nz = so.number_of_voxels[2];
+      if (ix >= nx || iy >= ny || iz >= nz || ix < 0 || iy < 0 || iz < 0) {
+        exit_solid = true;
+      } else {
+        int material = __ldg(so.labels + (ix + iy * nx + iz * nx * ny));
+        int proc;
+        float nid = next_interaction(rng, nv, sig, energy_id, material, proc);
+        V3 vmin = add(bmin, mul(v3(static_cast<float>(ix), static_cast<float>(iy), static_cast<float>(iz)), vs));
+        V3 vmax = add(vmin, vs);
+        ph.p = safety_inside(ph.p, vmin, vmax);
+        float dtb = distance_to_aabb(ph.p, ph.d, vmin, vmax);
+        if (dtb <= nid) {
+          nid = dtb + kTolerance;
+          proc = GG_TRANSPORTATION;
+          if (so.dose_map >= 0) {
+            const DevDoseMap& dm = P.dose_maps[so.dose_map];
+            if (dm.photon_tracking) {
+              int id = dosel(dm, ph.p);
+              if (id >= 0) atomicAdd(dm.photon_tracking + id, 1);
+            }
+          }
+        }
+        ph.p = safety_outside(add(ph.p, scale(ph.d, nid)), vmin, vmax);
+        if (!in_aabb(ph.p, bmin, bmax)) {
+          exit_solid = true;
+        } else {
+          float e0 = ph.E;
+          if (proc != GG_TRANSPORTATION) {
+            if (proc == GG_COMPTON_SCATTERING) {
+              compton(ph, rng);
+            } else if (proc == GG_PHOTOELECTRIC_EFFECT) {
+              ph.status = GG_DEAD;
+              ph.E = 0.0f;
+            } else if (proc == GG_RAYLEIGH_SCATTERING) {
+              rayleigh(ph, rng, nv, ebins, sig, material, energy_id);
+            }
+            if (proc == GG_COMPTON_SCATTERING || proc == GG_RAYLEIGH_SCATTERING) ph.scatter = 1;
+            if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], e0 - ph.E, ph.p);
+          }
+          if (ph.E <= tab.photon_cut(nav)[material]) {
+            if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
+            ph.status = GG_DEAD;
+          }
+          dead = ph.status == GG_DEAD;
+        }
+      }
+    } else {
+      // track_through_ggems_solid_box, TrackThroughGGEMSSolidBox.cl:122-248
+      int proc;
+      float nid = next_interaction(rng, nv, sig, energy_id, 0, proc);
+      ph.p = safety_inside(ph.p, bmin, bmax);
+      float dtb = distance_to_aabb(ph.p, ph.d, bmin, bmax);
+      if (dtb <= nid) {
+        nid = dtb + kTolerance;
+        proc = GG_TRANSPORTATION;
+      }
+      ph.p = safety_outside(add(ph.p, scale(ph.d, nid)), bmin, bmax);
+      if (!in_aabb(ph.p, bmin, bmax)) {
+        exit_solid = true;
+      } else {
+        if (ph.E < so.threshold) ph.status = GG_DEAD;
+        if (proc != GG_TRANSPORTATION) {
+          if (proc == GG_COMPTON_SCATTERING) {
+            compton(ph, rng);
+          } else if (proc == GG_PHOTOELECTRIC_EFFECT) {
+            ph.status = GG_DEAD;
+            ph.E = 0.0f;
+          } else if (proc == GG_RAYLEIGH_SCATTERING) {
+            rayleigh(ph, rng, nv, ebins, sig, 0, energy_id);
+          }
+          if (so.histogram && (proc == GG_PHOTOELECTRIC_EFFECT || proc == GG_COMPTON_SCATTERING)) {
+            V3 es = divv(v3(so.box_size[0], so.box_size[1], so.box_size[2]),
+                         v3(static_cast<float>(so.virtual_element_number[0]),
+                            static_cast<float>(so.virtual_element_number[1]),
+                            static_cast<float>(so.virtual_element_number[2])));
+            V3 q = divv(sub(ph.p, bmin), es);
+            int ix = __float2int_rz(q.x), iy = __float2int_rz(q.y);
+            if (ix >= 0 && iy >= 0 && ix < so.virtual_element_number[0] && iy < so.virtual_element_number[1]) {
+              int idx = ix + iy * so.virtual_element_number[0];
+              atomicAdd(so.histogram + idx, 1);
+              if (so.scatter_histogram && ph.scatter == 1) atomicAdd(so.scatter_histogram + idx, 1);
+            }
+          }
+        }
+        dead = ph.status == GG_DEAD;
+      }
+    }
+
+    if (exit_solid) {
+      ph.psd = kOutOfWorld;
+      ph.solid_id = -1;
+    }
+    if (exit_solid || dead) {
+      // Back to the global frame (end of track_through_*).
+      ph.p = l2g_pos(so.matrix, ph.p);
+      ph.d = l2g_dir(so.matrix, ph.d);
+      if (dead) {
+        if (--histories_left > 0) {
+          phase = kNewHistory;
+        } else {
+          finish_slot();
+          phase = next_slot() ? kNewHistory : kDone;
+        }
+      } else {
+        phase = kFind;
+      }
+    }
+  }
+}
+
+// compute_dose_ggems_voxelized_solid, ComputeDoseGGEMSVoxelizedSolid.cl:53-121
+__global__ void compute_dose_kernel(DoseParams P) {
+  const DevDoseMap& dm = P.map;
+  int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= dm.total_number_of_dosels) return;
+  int z = id / dm.slice_number_of_dosels;
+  int x = (id - z * dm.slice_number_of_dosels) % dm.number_of_dosels[0];
+  int y = (id - z * dm.slice_number_of_dosels) / dm.number_of_dosels[0];
+  float px = static_cast<float>(x) * dm.size_of_dosels[0] +
+             static_cast<float>(dm.number_of_dosels[0] - 1) * (-0.5f * dm.size_of_dosels[0]);
+  float py = static_cast<float>(y) * dm.size_of_dosels[1] +
+             static_cast<float>(dm.number_of_dosels[1] - 1) * (-0.5f * dm.size_of_dosels[1]);
+  float pz = static_cast<float>(z) * dm.size_of_dosels[2] +
+             static_cast<float>(dm.number_of_dosels[2] - 1) * (-0.5f * dm.size_of_dosels[2]);
+  int vx = __float2int_rz((px - P.border_min[0]) / P.voxel_sizes[0]);
+  int vy = __float2int_rz((py - P.border_min[1]) / P.voxel_sizes[1]);
+  int vz = __float2int_rz((pz - P.border_min[2]) / P.voxel_sizes[2]);
+  int material = P.labels[vx + vy * P.number_of_voxels[0] + vz * P.number_of_voxels[0] * P.number_of_voxels[1]];
+  float vol = dm.size_of_dosels[0] * dm.size_of_dosels[1] * dm.size_of_dosels[2];
+  constexpr float kGCm3 = 6.241509704e+21f / 1.e3f;  // g/cm3
+  constexpr float kGy = 1.0e-12f;
+  float density = P.is_water_reference ? 1.0f * kGCm3 : P.density[material];
+  double edep = static_cast<double>(static_cast<long long>(dm.edep[id])) / kEdepScale;
+  P.dose[id] = density < P.minimum_density
+                   ? 0.0f
+                   : static_cast<float>(static_cast<double>(P.scale_factor) * edep / static_cast<double>(density) /
+                                        static_cast<double>(vol) / static_cast<double>(kGy));
+  if (P.uncertainty) {
+    int hit = dm.hit ? dm.hit[id] : 0;
+    if (hit > 1 && edep != 0.0) {
+      double e2 = dm.edep_squared ? dm.edep_squared[id] : 0.0;
+      double sum2 = edep * edep;
+      P.uncertainty[id] = static_cast<float>(sqrt((hit * e2 - sum2) / ((hit - 1) * sum2)));
+    } else {
+      P.uncertainty[id] = 1.0f;
+    }
+  }
+}
+
+}  // namespace
+
+void launch_transport(const TransportParams& p, int grid, size_t smem, void* stream) {
+  transport_kernel<<<grid, kBlockThreads, smem, static_cast<cudaStream_t>(stream)>>>(p);
+}
+
+void launch_compute_dose(const DoseParams& p, void* stream) {
+  int n = p.map.total_number_of_dosels;
+  compute_dose_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(p);
+}
+
+cudaError_t configure_transport(size_t smem, int* blocks_per_sm) {
+  cudaError_t e = cudaFuncSetAttribute(transport_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, transport_kernel, kBlockThreads, smem);
+}
+
+cudaError_t set_rayleigh_fit(const float* pp /* 9*101 */) {
+  return cudaMemcpyToSymbol(c_rayleigh_pp, pp, sizeof(float) * 9 * 101);
+}
+
+}  // namespace gg

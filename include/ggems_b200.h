@@ -138,6 +138,8 @@ typedef struct gg_scene {
   const gg_dose_map* dose_maps;
   int32_t number_of_histograms;
   const int32_t* histogram_sizes;   /* elements per histogram */
+  const float* rayleigh_fit;        /* [9][101] Livermore form-factor fit PP0..PP8
+                                       (GGEMSRayleighScatteringModels.hh:36-153) */
 } gg_scene;
 
 typedef enum gg_source_type {
@@ -161,9 +163,10 @@ typedef struct gg_source {
   int32_t number_of_voxels[3];
   float voxel_sizes[3];
   float border_min[3];
-  int64_t number_of_activity_bins;  /* active voxels */
-  const int32_t* activity_index;    /* [number_of_activity_bins] voxel index */
-  const float* activity_cdf;        /* [number_of_activity_bins] */
+  int64_t number_of_activity_bins;  /* entries of activity_index / activity_cdf: active voxels + 1
+                                       (the count GGEMSVoxelizedSource.cc:170 passes to the kernel) */
+  const int32_t* activity_index;    /* [number_of_activity_bins] voxel index, entry 0 unused (0) */
+  const float* activity_cdf;        /* [number_of_activity_bins], cdf[0] = 0 */
 } gg_source;
 
 /* Final per-slot particle state (the photon part of GGEMSPrimaryParticles,

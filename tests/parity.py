@@ -1,0 +1,93 @@
+"""Helpers shared by the parity tests: run a scene through the CUDA layer and
+through the CPU oracle with the same random states, and compare."""
+
+import ctypes as C
+import os
+
+import numpy as np
+
+import scenes
+from ggems_b200 import abi
+
+
+def run_oracle(sc, src, n, seed=777, states=None, threads=None):
+    st = scenes.seed_states(seed) if states is None else states.copy()
+    ss = sc.struct()
+    P = abi.Particles(min(n, abi.GG_MAXIMUM_PARTICLES))
+    T = sc.tallies()
+    rc = scenes.oracle().gg_oracle_run(C.byref(ss), C.byref(src.struct), n, abi.ptr(st, C.c_uint32), C.byref(P.struct),
+                                       C.byref(T.struct), threads or os.cpu_count())
+    assert rc == 0
+    return P, T, st
+
+
+def run_gpu(ctx, sc, src, n, seed=777, states=None):
+    st = scenes.seed_states(seed) if states is None else states.copy()
+    ss = sc.struct()
+    ctx.upload_scene(ss)
+    ctx.set_random_states(st)
+    ctx.run(src.struct, n)
+    P = abi.Particles(min(n, abi.GG_MAXIMUM_PARTICLES))
+    ctx.read_particles(P)
+    T = sc.tallies()
+    ctx.read_tallies(T)
+    ctx.get_random_states(st)
+    return P, T, st
+
+
+def history_agreement(Pa, Pb, pos_tol=1e-3, e_rel=1e-5):
+    """Fraction of slots whose final state agrees bit-exactly, and within tolerance."""
+    ints = (Pa.status == Pb.status) & (Pa.solid_id == Pb.solid_id) & (Pa.scatter == Pb.scatter)
+    exact = ints.copy()
+    for f in ("E", "px", "py", "pz", "dx", "dy", "dz"):
+        exact &= getattr(Pa, f).view(np.uint32) == getattr(Pb, f).view(np.uint32)
+    pa = np.stack([Pa.px, Pa.py, Pa.pz], 1).astype(np.float64)
+    pb = np.stack([Pb.px, Pb.py, Pb.pz], 1).astype(np.float64)
+    close = ints & (np.abs(pa - pb).max(1) <= pos_tol) & \
+        (np.abs(Pa.E.astype(np.float64) - Pb.E) <= e_rel * np.maximum(np.abs(Pb.E), 1e-6))
+    return exact.mean(), close.mean()
+
+
+def oracle_dose(sc, T, dose_map, solid, scale=1.0, water=False, min_density=0.0):
+    """ComputeDoseGGEMSVoxelizedSolid.cl:53-121 restated in numpy (double math, float stores)."""
+    dm = sc.dose_maps[dose_map]
+    s = sc.solids[solid]
+    t = sc.tables[s.navigator]
+    labels = sc._keep[solid] if False else None
+    n = dm.total_number_of_dosels
+    ids = np.arange(n)
+    nx, ny = dm.number_of_dosels[0], dm.number_of_dosels[1]
+    z = ids // dm.slice_number_of_dosels
+    x = (ids - z * dm.slice_number_of_dosels) % nx
+    y = (ids - z * dm.slice_number_of_dosels) // nx
+    F = np.float32
+    sz = [F(v) for v in dm.size_of_dosels]
+    nd = list(dm.number_of_dosels)
+    pos = [F(c.astype(np.float32) * sz[i]) + F(F(nd[i] - 1) * F(F(-0.5) * sz[i])) for i, c in enumerate((x, y, z))]
+    pos = [(c.astype(np.float32) * sz[i]).astype(np.float32) + np.float32(F(nd[i] - 1) * F(F(-0.5) * sz[i]))
+           for i, c in enumerate((x, y, z))]
+    vid = [np.trunc(((pos[i] - F(s.obb.border_min[i])).astype(np.float32) / F(s.voxel_sizes[i])).astype(np.float32))
+           .astype(np.int64) for i in range(3)]
+    lab = np.ctypeslib.as_array(s.labels, shape=(s.number_of_voxels[0] * s.number_of_voxels[1] * s.number_of_voxels[2],))
+    mat = lab[vid[0] + vid[1] * s.number_of_voxels[0] + vid[2] * s.number_of_voxels[0] * s.number_of_voxels[1]]
+    vol = F(F(sz[0] * sz[1]) * sz[2])
+    g_cm3 = F(F(6.241509704e+21) / F(1.e3))
+    density = np.full(n, F(F(1.0) * g_cm3), np.float32) if water else t.density[mat]
+    edep = T.edep[dose_map]
+    dose = np.where(density < F(min_density), F(0.0),
+                    (((F(scale) * edep) / density.astype(np.float64)) / np.float64(vol) / np.float64(F(1.0e-12)))
+                    .astype(np.float32))
+    hit = T.hit[dose_map].astype(np.float64)
+    e2 = T.edep_squared[dose_map]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        unc = np.sqrt((hit * e2 - edep * edep) / ((hit - 1) * edep * edep)).astype(np.float32)
+    unc = np.where((hit > 1) & (edep != 0.0), unc, F(1.0))
+    return dose.astype(np.float32), unc.astype(np.float32)
+
+
+def z_scores(a, b, var_a, var_b):
+    """Per-bin z of a difference of two independent estimates."""
+    v = var_a + var_b
+    with np.errstate(divide="ignore", invalid="ignore"):
+        z = np.where(v > 0, (a - b) / np.sqrt(v), 0.0)
+    return z

@@ -117,6 +117,11 @@ def load_physics(path=PHYSICS):
     return out
 
 
+def rayleigh_fit():
+    pd = load_physics()
+    return np.ascontiguousarray(np.stack([pd["rayleigh_pp%d" % i] for i in range(9)]).astype(np.float32))
+
+
 class Tables:
     """One navigator's physics tables (oracle restatement of the host builders)."""
 
@@ -259,8 +264,9 @@ class Scene:
         self._s = (abi.gg_solid * len(self.solids))(*self.solids)
         self._d = (abi.gg_dose_map * max(1, len(self.dose_maps)))(*self.dose_maps)
         self._h = np.array(self.histogram_sizes + [0], np.int32)
+        self._pp = rayleigh_fit()
         return abi.gg_scene(len(self.tables), self._t, len(self.solids), self._s, len(self.dose_maps), self._d,
-                            len(self.histogram_sizes), abi.ptr(self._h, C.c_int32))
+                            len(self.histogram_sizes), abi.ptr(self._h, C.c_int32), abi.ptr(self._pp, C.c_float))
 
     def tallies(self):
         return abi.Tallies(self.histogram_sizes, [d.total_number_of_dosels for d in self.dose_maps])
