@@ -1,0 +1,440 @@
+#!/usr/bin/env python
+"""Benchmark of the GGEMS photon path on B200: primaries/s on the 256^3 CBCT
+projection (120 kVp polyenergetic cone beam, 1e8 primaries, flat 512x512 GOS
+panel of 0.8 mm at SDD 1500 mm / SID 1000 mm, Compton + photoelectric +
+Rayleigh, primary and scatter histograms).
+
+One step = one full CBCT projection of 1e8 primaries (96 batches of up to
+2^20 random slots, exactly as GGEMS splits them).  Inputs are synthetic
+(seeded phantom generator, synthetic spectrum) in GGEMS's file formats and go
+through the GGEMS-compatible API (materials database, voxelized phantom, CT
+system, X-ray source, processes, range cuts, initialize).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+For N > 1, launch with torch.distributed.run; every rank runs its own
+projection with its own random streams (weak scaling).
+"""
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PRIMARIES = 100_000_000
+WORKLOAD = "cbct256_120kVp_flat512"
+
+
+def _rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def _ensure_built():
+    from ggems_b200 import build
+    if not os.path.exists(build.LIB):
+        build.build()
+
+
+def _configure(files, primaries, seed_offset_slots=0):
+    """Build the CBCT simulation through the GGEMS-compatible Python API."""
+    import ggems_b200 as gg
+    mhd, rng_file, spectrum = files
+    gg.GGEMSVerbosity(0)
+    gg.GGEMSMaterialsDatabaseManager().set_materials(os.path.join(ROOT, "ggems_b200", "data", "materials.txt"))
+    phantom = gg.GGEMSVoxelizedPhantom("phantom")
+    phantom.set_phantom(mhd, rng_file)
+    phantom.set_rotation(0.0, 0.0, 0.0, "deg")
+    phantom.set_position(0.0, 0.0, 0.0, "mm")
+    ct = gg.GGEMSCTSystem("flat_panel")
+    ct.set_ct_type("flat")
+    ct.set_number_of_modules(1, 1)
+    ct.set_number_of_detection_elements(512, 512, 1)
+    ct.set_size_of_detection_elements(0.8, 0.8, 10.0, "mm")
+    ct.set_material("GOS")
+    ct.set_source_detector_distance(1500.0, "mm")
+    ct.set_source_isocenter_distance(1000.0, "mm")
+    ct.set_rotation(0.0, 0.0, 0.0, "deg")
+    ct.set_threshold(10.0, "keV")
+    ct.save(os.path.join(os.path.dirname(mhd), "projection.mhd"))
+    ct.store_scatter(True)
+    pm = gg.GGEMSProcessesManager()
+    pm.add_process("Compton", "gamma", "all")
+    pm.add_process("Photoelectric", "gamma", "all")
+    pm.add_process("Rayleigh", "gamma", "all")
+    pm.set_cross_section_table_number_of_bins(220)
+    pm.set_cross_section_table_energy_min(1.0, "keV")
+    pm.set_cross_section_table_energy_max(1.0, "MeV")
+    gg.GGEMSRangeCutsManager().set_cut("gamma", 0.1, "mm", "all")
+    src = gg.GGEMSXRaySource("xray")
+    src.set_source_particle_type("gamma")
+    src.set_number_of_particles(primaries)
+    src.set_position(-1000.0, 0.0, 0.0, "mm")
+    src.set_rotation(0.0, 0.0, 0.0, "deg")
+    src.set_beam_aperture(11.0, "deg")
+    src.set_focal_spot_size(0.0, 0.0, 0.0, "mm")
+    src.set_polyenergy(spectrum)
+    return gg
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _profile_traffic():
+    """DRAM bytes per transport launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "transport_kernel_cbct256.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_full_launch:"):
+            try:
+                return float(line.split(":")[1].split()[0])
+            except (IndexError, ValueError):
+                return None
+    return None
+
+
+def _peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_reference_run(scene_ptr, source, n, threads, kind):
+    """Run n primaries of the workload on the host with the reference kernels
+    (oracle/_ref, GGEMS's own device code compiled for the host) or the oracle
+    port.  Returns (seconds, counts per primary or None)."""
+    from ggems_b200 import abi
+    import numpy as np
+    if kind == "reference":
+        lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libgg_ref.so"))
+        fn = lib.gg_ref_run
+    else:
+        lib = C.CDLL(os.path.join(ROOT, "oracle", "_build", "libgg_oracle.so"))
+        fn = lib.gg_oracle_run
+    fn.restype = C.c_int
+    fn.argtypes = [C.POINTER(abi.gg_scene), C.POINTER(abi.gg_source), C.c_uint64, C.POINTER(C.c_uint32),
+                   C.POINTER(abi.gg_particle_buffers), C.POINTER(abi.gg_tally_buffers), C.c_int]
+    sc = scene_ptr.contents
+    states = np.zeros(5 * abi.GG_MAXIMUM_PARTICLES, np.uint32)
+    from ggems_b200._native import lib as native
+    native.gg_seed_random_states(abi.ptr(states, C.c_uint32), abi.GG_MAXIMUM_PARTICLES, 777, 0)
+    hs = [int(sc.histogram_sizes[i]) for i in range(sc.number_of_histograms)]
+    ds = [int(sc.dose_maps[i].total_number_of_dosels) for i in range(sc.number_of_dose_maps)]
+    tallies = abi.Tallies(hs, ds)
+    counts = None
+    if kind != "reference":
+        lib.gg_oracle_counts.argtypes = [C.POINTER(C.c_uint64), C.c_int]
+        lib.gg_oracle_counts(None, 1)
+    t0 = time.perf_counter()
+    rc = fn(scene_ptr, C.byref(source), n, abi.ptr(states, C.c_uint32), None, C.byref(tallies.struct), threads)
+    dt = time.perf_counter() - t0
+    if rc != 0:
+        raise RuntimeError("CPU run failed: %d" % rc)
+    if kind != "reference":
+        cnt = (C.c_uint64 * 5)()
+        lib.gg_oracle_counts(cnt, 1)
+        counts = [cnt[i] / max(n, 1) for i in range(4)]
+    return dt, counts
+
+
+def _cpu_kind():
+    ref = os.path.join(ROOT, "oracle", "_ref", "libgg_ref.so")
+    return "reference" if os.path.exists(ref) else "port"
+
+
+def _ensure_oracle():
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_build", "libgg_oracle.so")):
+        subprocess.check_call([sys.executable, os.path.join(ROOT, "oracle", "build.py")])
+
+
+def _sample_size(scene_ptr, source, threads, kind, budget_s):
+    """Primaries for about budget_s seconds of host work (pilot run first)."""
+    pilot = 20000
+    dt, _ = cpu_reference_run(scene_ptr, source, pilot, threads, kind)
+    n = int(pilot * budget_s / max(dt, 1e-3))
+    return max(pilot, min(n, 1048576))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--primaries", type=int, default=PRIMARIES)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
+    args = ap.parse_args()
+    rank, world, local = _rank()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    _ensure_built()
+    _ensure_oracle()
+    tmp = tempfile.mkdtemp(prefix="ggems_bench_")
+    from ggems_b200 import workloads
+    files = workloads.cbct_files(tmp, 256, 1.0, seed=1)
+
+    if args.impl == "reference":
+        return run_reference_arm(args, files, rank, world)
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    os.environ.setdefault("CUDA_VISIBLE_DEVICES", os.environ.get("CUDA_VISIBLE_DEVICES", ""))
+
+    gg = _configure(files, args.primaries)
+    from ggems_b200 import abi
+    from ggems_b200.api import lib
+    if world > 1:
+        gg.GGEMSOpenCLManager().set_device_index(local)
+    ggems = gg.GGEMS()
+    # Rank r takes random streams after those of ranks < r (device order of GGEMSPseudoRandomGenerator).
+    ggems.initialize(777 + 0 * rank)
+    ctx = lib.ggems_device_context(ggems.obj, 0)
+    if rank > 0:
+        import numpy as np
+        st = np.zeros(5 * abi.GG_MAXIMUM_PARTICLES, np.uint32)
+        lib.gg_seed_random_states(abi.ptr(st, C.c_uint32), abi.GG_MAXIMUM_PARTICLES, 777, rank * abi.GG_MAXIMUM_PARTICLES)
+        lib.gg_set_random_states(ctx, abi.ptr(st, C.c_uint32), abi.GG_MAXIMUM_PARTICLES)
+    src = abi.gg_source()
+    n_src = C.c_uint64()
+    assert lib.ggems_source_descriptor(0, C.byref(src), C.byref(n_src)) == 0
+    scene_ptr = lib.ggems_scene(ggems.obj)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def check(rc, what):
+        if rc != 0:
+            raise RuntimeError("%s: %s" % (what, lib.gg_last_error().decode()))
+
+    def step():
+        check(lib.gg_run_source(ctx, C.byref(src), args.primaries), "gg_run_source")
+        check(lib.gg_synchronize(ctx), "gg_synchronize")
+        ms, launches = C.c_float(), C.c_int64()
+        lib.gg_last_run_stats(ctx, C.byref(ms), C.byref(launches))
+        return ms.value, launches.value
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        torch.cuda.synchronize()
+        step()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-timed region (inputs resident in HBM) ----
+    times, launches = [], 0
+    barrier()
+    with ClockSampler(local if world > 1 else int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ms, n = step()
+            times.append(ms)
+            launches += n
+    barrier()
+    total_ms = sum(times)
+    if dist is not None:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.primaries * args.steps / (total_ms * 1e-3)
+
+    # ---- end to end through the C ABI: host scene -> device, run, tallies -> host ----
+    import numpy as np
+    sc = scene_ptr.contents
+    hs = [int(sc.histogram_sizes[i]) for i in range(sc.number_of_histograms)]
+    tallies = abi.Tallies(hs, [])
+    states = np.frombuffer(C.string_at(lib.ggems_initial_random_states(ggems.obj, 0),
+                                       5 * abi.GG_MAXIMUM_PARTICLES * 4), np.uint32).copy()
+    h2d = sum(int(sc.solids[i].number_of_voxels[0]) * sc.solids[i].number_of_voxels[1] * sc.solids[i].number_of_voxels[2]
+              for i in range(sc.number_of_solids) if sc.solids[i].type == abi.GG_SOLID_VOXELIZED)
+    for i in range(sc.number_of_tables):
+        t = sc.tables[i]
+        h2d += 4 * (t.number_of_bins + 3 * t.number_of_materials * t.number_of_bins + 101 * t.number_of_bins + 4 * t.number_of_materials)
+    h2d += states.nbytes + 2 * 4 * (int(src.number_of_energy_bins) + 1)
+    d2h = sum(4 * h for h in hs)
+    e2e_times = []
+    for k in range(0 if args.no_e2e else args.steps + 1):
+        barrier()
+        t0 = time.perf_counter()
+        check(lib.gg_upload_scene(ctx, scene_ptr), "gg_upload_scene")
+        check(lib.gg_set_random_states(ctx, abi.ptr(states, C.c_uint32), abi.GG_MAXIMUM_PARTICLES), "random states")
+        step()
+        check(lib.gg_read_tallies(ctx, C.byref(tallies.struct)), "gg_read_tallies")
+        t1 = time.perf_counter()
+        if k > 0:  # first pass warms the host allocations
+            e2e_times.append(t1 - t0)
+    e2e_total = sum(e2e_times) if e2e_times else float("nan")
+    if dist is not None:
+        t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * args.primaries * args.steps / e2e_total
+
+    if rank != 0:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
+
+    # ---- CPU baseline and roofline (rank 0, N = 1 only) ----
+    cpu_baseline, counts = None, None
+    kind = _cpu_kind()
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        n = _sample_size(scene_ptr, src, threads, kind, 15.0)
+        dt, _ = cpu_reference_run(scene_ptr, src, n, threads, kind)
+        cpu_baseline = {"value": n / dt, "unit": "primaries/s", "cores": threads, "kind": kind,
+                        "sample": "%d primaries of the same projection (1 batch, seed 777) on %d host threads, %.1f s"
+                                  % (n, threads, dt)}
+    _, counts = cpu_reference_run(scene_ptr, src, 20000 if args.no_cpu_baseline else 100000, os.cpu_count() or 1, "port")
+    S, box, D, H = counts
+    # algorithmic bytes per primary: source state 40 B + 1 B label per voxel step + 20 B per dose
+    # deposit + 8 B per detector count + 28 B final state
+    bytes_per_primary = 40 + S + 20 * D + 8 * H + 28
+    peaks = _peaks()
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    achieved = value / world * bytes_per_primary / 1e9
+    per_launch_traffic = _profile_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": per_launch_traffic,
+                "peak_source": "measured" if peaks else "fallback",
+                "bytes_per_primary": bytes_per_primary,
+                "voxel_steps_per_primary": S, "box_steps_per_primary": box, "detector_counts_per_primary": H}
+    line = {
+        "metric": "primaries/s (CBCT 256^3, 120 kVp)", "value": value, "unit": "primaries/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom generator, synthetic 120 kVp spectrum)",
+        "config": {"workload": WORKLOAD, "phantom": "256x256x256 uint8, 1 mm, air/water/bone(1.85)",
+                   "primaries_per_step": args.primaries, "batches_per_step": 96, "detector": "flat 512x512 GOS, 0.8 mm, SDD 1500 / SID 1000",
+                   "processes": "Compton, photoelectric, Rayleigh", "parallelism": "replicas" if world > 1 else "single GPU",
+                   "l2": "256 MB buffer written between timed steps (inputs 17 MB < L2)"},
+        "e2e": {"value": e2e_value, "unit": "primaries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "roofline": roofline,
+        "cpu_baseline": cpu_baseline,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_reference_arm(args, files, rank, world):
+    """The reference's CPU implementation of the path (GGEMS's kernels built for
+    the host when available, else the oracle port) on all host threads."""
+    if rank != 0:
+        return 0
+    kind = _cpu_kind()
+    gg = _configure(files, args.primaries)
+    from ggems_b200 import abi
+    from ggems_b200.api import lib
+    # Tables and scene come from the same API; no GPU work is done here.
+    scene_ptr, src = _host_scene(gg, lib)
+    if scene_ptr is None:
+        print(json.dumps({"impl": "reference", "unavailable": "could not build the host scene"}))
+        return 0
+    threads = os.cpu_count() or 1
+    n = _sample_size(scene_ptr, src, threads, kind, max(5.0, 60.0 / max(args.steps + args.warmup, 1)))
+    for _ in range(args.warmup):
+        cpu_reference_run(scene_ptr, src, n, threads, kind)
+    times = [cpu_reference_run(scene_ptr, src, n, threads, kind)[0] for _ in range(args.steps)]
+    value = n * args.steps / sum(times)
+    sample = "%d primaries per step of the 1e8-primary projection on %d host threads" % (n, threads)
+    print(json.dumps({
+        "impl": "reference", "metric": "primaries/s (CBCT 256^3, 120 kVp)", "value": value, "unit": "primaries/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded phantom generator, synthetic 120 kVp spectrum)",
+        "config": {"workload": WORKLOAD, "primaries_per_step": n},
+        "cpu_baseline": {"value": value, "unit": "primaries/s", "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": "primaries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+    return 0
+
+
+def _host_scene(gg, lib):
+    """Scene of the configured simulation without a GPU (host-side initialisation only)."""
+    from ggems_b200 import abi
+    fn = lib.ggems_host_scene
+    fn.restype = C.POINTER(abi.gg_scene)
+    p = fn()
+    if not p:
+        return None, None
+    src = abi.gg_source()
+    assert lib.ggems_source_descriptor(0, C.byref(src), None) == 0
+    return p, src
+
+
+if __name__ == "__main__":
+    sys.exit(main())

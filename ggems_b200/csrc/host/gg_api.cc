@@ -471,7 +471,23 @@ GGEMS::~GGEMS() {
     if (d.context) gg_context_destroy(d.context);
 }
 
-// GGEMS::Initialize (src/global/GGEMS.cc:199-297)
+// GGEMS::Initialize (src/global/GGEMS.cc:199-297): sources (with the random
+// streams) first, then navigators, then the scene goes to every device.
+void GGEMS::prepare() {
+  Simulation& sim = Simulation::instance();
+  if (!MaterialsDatabase::instance().ready()) throw Error("GGEMS", "Initialize", "Materials are not loaded in GGEMS!!!");
+  if (sim.sources.empty()) throw Error("GGEMSSourceManager", "Initialize", "No source defined!!!");
+  for (auto& s : sim.sources) s->initialize();
+  // Navigators (GGEMSNavigatorManager::Initialize), solids numbered in registration order.
+  int next_id = 0;
+  for (auto& n : sim.navigators) {
+    n->initialize(next_id);
+    next_id += static_cast<int>(n->solids.size());
+  }
+  build_scene();
+  prepared_ = true;
+}
+
 void GGEMS::initialize(uint32_t seed) {
   Simulation& sim = Simulation::instance();
   if (!MaterialsDatabase::instance().ready()) throw Error("GGEMS", "Initialize", "Materials are not loaded in GGEMS!!!");
@@ -502,14 +518,7 @@ void GGEMS::initialize(uint32_t seed) {
                  "InitializeSeeds");
     check_device(gg_set_random_states(devices[d].context, states_[d].data(), GG_MAXIMUM_PARTICLES), "InitializeSeeds");
   }
-  for (auto& s : sim.sources) s->initialize();
-  // Navigators (GGEMSNavigatorManager::Initialize), solids numbered in registration order.
-  int next_id = 0;
-  for (auto& n : sim.navigators) {
-    n->initialize(next_id);
-    next_id += static_cast<int>(n->solids.size());
-  }
-  build_scene();
+  prepare();
   for (auto& d : devices) check_device(gg_upload_scene(d.context, &scene_), "UploadScene");
   initialized_ = true;
   log(1, "GGEMS", "Initialize", "GGEMS initialization succeeded");

@@ -193,9 +193,11 @@ class GGEMS {
   bool is_tracking = false;
   int tracking_id = 0;
   void initialize(uint32_t seed);
+  // Host half of initialize(): sources, navigators, tables and the scene, no device.
+  void prepare();
   void run();
-  // scene as handed to the transport layer (valid after initialize)
-  const gg_scene* scene() const { return initialized_ ? &scene_ : nullptr; }
+  // scene as handed to the transport layer (valid after prepare / initialize)
+  const gg_scene* scene() const { return prepared_ ? &scene_ : nullptr; }
   const std::vector<uint32_t>& random_states(size_t device) const { return states_[device]; }
   std::vector<Device> devices;
   float last_run_ms = 0.0f;
@@ -206,6 +208,7 @@ class GGEMS {
   void build_scene();
   void save_results();
   bool initialized_ = false;
+  bool prepared_ = false;
   uint32_t seed_ = 0;
   std::vector<gg_physics_tables> tables_;
   std::vector<gg_solid> solids_;

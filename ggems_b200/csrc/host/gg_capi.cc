@@ -85,6 +85,15 @@ GG_EXPORT void ggems_last_run(GGEMS* g, float* ms, int64_t* launches, uint64_t* 
   if (launches) *launches = g->last_run_launches;
   if (particles) *particles = g->last_run_particles;
 }
+// Host-only initialisation of the registered simulation (sources, navigators,
+// tables) and its scene, without any device; used by CPU references.
+GG_EXPORT const gg_scene* ggems_host_scene(void) {
+  return guarded_value<const gg_scene*>(nullptr, [&] {
+    static GGEMS* host = new GGEMS();
+    host->prepare();
+    return host->scene();
+  });
+}
 GG_EXPORT int ggems_number_of_sources(void) { return static_cast<int>(Simulation::instance().sources.size()); }
 GG_EXPORT int ggems_source_descriptor(int i, gg_source* out, uint64_t* number_of_particles) {
   auto& s = Simulation::instance().sources;

@@ -1,0 +1,121 @@
+"""Synthetic inputs for the benchmark workloads, written in GGEMS's file
+formats (MHD phantom + range-to-material file, "E_MeV intensity" spectrum).
+
+* ``cbct_phantom``: 256^3 CBCT phantom of 1 mm voxels: air background, a
+  water ellipsoid with semi-axes 110/90/120 mm and 6-12 bone-like (1.85
+  g/cm3) ellipsoids of semi-axes 5-25 mm with centres inside the body, from a
+  seed.  Smaller grids scale the geometry with the grid extent.
+* ``water_phantom``: the 64^3 all-water phantom of 2 mm voxels.
+* ``xray_spectrum``: 120 kVp, 1 keV bins over 10-120 keV, Kramers-shaped
+  ((120 - E)/E) and filtered by 2.5 mm of aluminium with GGEMS's own mu table.
+"""
+
+import os
+
+import numpy as np
+
+DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+MATERIALS = os.path.join(DATA, "materials.txt")
+PHYSICS = os.path.join(DATA, "physics_data.bin")
+
+
+def load_physics(path=PHYSICS):
+    """The arrays of physics_data.bin by name."""
+    raw = open(path, "rb").read()
+    if raw[:8] != b"GGPHYS01":
+        raise ValueError("not a physics data file: " + path)
+    n = int(np.frombuffer(raw, np.uint32, 1, 8)[0])
+    off, out = 12, {}
+    for _ in range(n):
+        name = raw[off:off + 32].split(b"\0")[0].decode()
+        code, cnt = np.frombuffer(raw, np.uint32, 2, off + 32)
+        off += 40
+        dt = {0: np.float32, 1: np.int32, 2: np.int16, 3: np.uint8}[int(code)]
+        arr = np.frombuffer(raw, dt, int(cnt), off)
+        off += arr.nbytes
+        out[name] = arr
+    return out
+
+
+def cbct_labels(n=256, voxel=1.0, seed=1, n_bones=None):
+    """uint8 labels (z, y, x): 0 air, 1 water, 2 bone."""
+    rng = np.random.default_rng(seed)
+    if n_bones is None:
+        n_bones = int(rng.integers(6, 13))
+    c = ((np.arange(n, dtype=np.float32) + 0.5) * voxel - n * voxel / 2.0).astype(np.float32)
+    scale = n * voxel / 256.0
+    a, b, cc = 110.0 * scale, 90.0 * scale, 120.0 * scale
+    labels = np.zeros((n, n, n), np.uint8)
+    zz = (c / cc) ** 2
+    yy = (c / b) ** 2
+    xx = (c / a) ** 2
+    body = (zz[:, None, None] + yy[None, :, None] + xx[None, None, :]) <= 1.0
+    labels[body] = 1
+    for _ in range(n_bones):
+        r = rng.uniform(5, 25, 3) * scale
+        while True:
+            p = rng.uniform(-1, 1, 3)
+            if (p ** 2).sum() <= 1.0:
+                break
+        ctr = p * np.array([a, b, cc]) * 0.7
+        bone = ((((c - ctr[2]) / r[2]) ** 2)[:, None, None] + (((c - ctr[1]) / r[1]) ** 2)[None, :, None] +
+                (((c - ctr[0]) / r[0]) ** 2)[None, None, :]) <= 1.0
+        labels[bone & body] = 2
+    return labels
+
+
+def write_mhd(path, array, spacing, element_type="MET_UCHAR"):
+    """Write an MHD header + raw file (x fastest, array shaped (z, y, x))."""
+    base = path[:-4] if path.endswith(".mhd") else path
+    raw = base + ".raw"
+    nz, ny, nx = array.shape
+    with open(base + ".mhd", "w") as f:
+        f.write("ObjectType = Image\nBinaryDataByteOrderMSB = False\nNDims = 3\n")
+        f.write("ElementSpacing = %g %g %g\n" % tuple(spacing))
+        f.write("DimSize = %d %d %d\n" % (nx, ny, nz))
+        f.write("ElementType = %s\n" % element_type)
+        f.write("ElementDataFile = %s\n" % os.path.basename(raw))
+    np.ascontiguousarray(array).tofile(raw)
+    return base + ".mhd"
+
+
+def xray_spectrum():
+    """(energies MeV, weights) of the 120 kVp / 2.5 mm Al spectrum."""
+    pd = load_physics()
+    nb, idx = pd["mu_nb_energy_bins"], pd["mu_index_energy"]
+    data = pd["mu_data"].reshape(-1, 3)
+    z = 13
+    rows = data[idx[z]: idx[z] + nb[z]].astype(np.float64)
+    energies = np.arange(10, 121, dtype=np.float64)  # keV
+    mu = np.exp(np.interp(np.log(energies * 1e-3), np.log(rows[:, 0]), np.log(rows[:, 1])))
+    w = np.clip(120.0 - energies, 0.0, None) / energies * np.exp(-mu * 2.699 * 0.25)
+    w = w / w.sum()
+    return energies * 1e-3, w
+
+
+def write_spectrum(path):
+    e, w = xray_spectrum()
+    with open(path, "w") as f:
+        for ei, wi in zip(e, w):
+            f.write("%.6f %.9e\n" % (ei, wi))
+    return path
+
+
+def cbct_files(directory, n=256, voxel=1.0, seed=1):
+    """Write the CBCT phantom, its range file and the spectrum; return their paths."""
+    os.makedirs(directory, exist_ok=True)
+    labels = cbct_labels(n, voxel, seed)
+    mhd = write_mhd(os.path.join(directory, "cbct_phantom.mhd"), labels, (voxel, voxel, voxel))
+    rng_file = os.path.join(directory, "cbct_range.txt")
+    with open(rng_file, "w") as f:
+        f.write("0 0 Air\n1 1 Water\n2 2 Bone185\n")
+    return mhd, rng_file, write_spectrum(os.path.join(directory, "spectrum_120kVp_2.5mmAl.dat"))
+
+
+def water_files(directory, n=64, voxel=2.0):
+    os.makedirs(directory, exist_ok=True)
+    mhd = write_mhd(os.path.join(directory, "water_phantom.mhd"), np.zeros((n, n, n), np.uint8), (voxel, voxel, voxel))
+    rng_file = os.path.join(directory, "water_range.txt")
+    with open(rng_file, "w") as f:
+        f.write("0 0 Water\n")
+    return mhd, rng_file

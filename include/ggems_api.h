@@ -52,6 +52,7 @@ int ggems_number_of_devices(GGEMS* g);  /* no counterpart in the reference: B200
 gg_context* ggems_device_context(GGEMS* g, int d);  /* no counterpart in the reference: B200 build addition */
 const uint32_t* ggems_initial_random_states(GGEMS* g, int d);  /* no counterpart in the reference: B200 build addition */
 void ggems_last_run(GGEMS* g, float* ms, int64_t* launches, uint64_t* particles);  /* no counterpart in the reference: B200 build addition */
+const gg_scene* ggems_host_scene(void);  /* no counterpart in the reference: B200 build addition */
 int ggems_number_of_sources(void);  /* no counterpart in the reference: B200 build addition */
 int ggems_source_descriptor(int i, gg_source* out, uint64_t* number_of_particles);  /* no counterpart in the reference: B200 build addition */
 void* get_instance_ggems_opencl_manager(void);  /* include/GGEMS/global/GGEMSOpenCLManager.hh:794 */
@@ -152,6 +153,8 @@ void* get_instance_profiler_manager(void);  /* include/GGEMS/tools/GGEMSProfiler
 void print_summary_profiler_manager(void*);  /* include/GGEMS/tools/GGEMSProfilerManager.hh:145 */
 void* get_instance_ggems_ram_manager(void);  /* include/GGEMS/tools/GGEMSRAMManager.hh:174 */
 void print_infos_ram_manager(void*);  /* include/GGEMS/tools/GGEMSRAMManager.hh:181 */
+int ggems_build_tables(const char* materials_file, const char* const* material_names, int n_materials, int number_of_bins, float min_energy, float max_energy, const int* process_ids, int n_processes, float photon_distance_cut, float* energy_bins, float* cross_sections, float* rayleigh, float* density, float* photon_cut, int32_t* n_elements, int32_t* element_offset, uint8_t* atomic_number, float* atomic_number_density, int32_t* total_elements);  /* no counterpart in the reference: B200 build addition */
+int ggems_phantom_labels(const char* phantom_file, const char* range_file, int32_t* dims, float* spacing, uint8_t* labels);  /* no counterpart in the reference: B200 build addition */
 
 #ifdef __cplusplus
 }

@@ -208,6 +208,11 @@ struct Tallies {
   gg_tally_buffers* out;
 };
 
+// Event counts for the algorithmic-byte model of the benchmark: voxel steps,
+// box steps, dose deposits, histogram increments, primaries.
+thread_local uint64_t t_counts[5];
+std::atomic<uint64_t> g_counts[5];
+
 void atomic_add_double(double* addr, double v) {
   std::atomic_ref<double> a(*addr);
   double cur = a.load(std::memory_order_relaxed);
@@ -234,6 +239,7 @@ void dose_record(const Tallies& t, int map, float edep, V3 p) {
   const gg_dose_map& dm = t.scene->dose_maps[map];
   int gid;
   if (!dosel_index(dm, p, &gid)) return;
+  ++t_counts[2];
   if (t.out->hit && t.out->hit[map]) atomic_add_int(&t.out->hit[map][gid], 1);
   if (t.out->edep && t.out->edep[map]) atomic_add_double(&t.out->edep[map][gid], static_cast<double>(edep));
   if (t.out->edep_squared && t.out->edep_squared[map])
@@ -541,6 +547,7 @@ void track_voxelized(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& 
       break;
     }
     int material = s.labels[ix + iy * nx + iz * nx * ny];
+    ++t_counts[0];
     next_interaction(ph, rng, tb, material);
     float nid = ph.nid;
     int8_t proc = ph.next_process;
@@ -590,6 +597,7 @@ void track_box(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& s, int
   V3 box = v3(s.box_size[0], s.box_size[1], s.box_size[2]);
   int vx = s.virtual_element_number[0], vy = s.virtual_element_number[1], vz = s.virtual_element_number[2];
   do {
+    ++t_counts[1];
     next_interaction(ph, rng, tb, 0);
     float nid = ph.nid;
     int8_t proc = ph.next_process;
@@ -616,6 +624,7 @@ void track_box(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& s, int
         V3 q = divv(sub(lp, bmin), es);
         int ix = static_cast<int>(q.x), iy = static_cast<int>(q.y);
         int index = ix + iy * vx;
+        ++t_counts[3];
         if (t.out->histograms && t.out->histograms[s.histogram]) atomic_add_int(&t.out->histograms[s.histogram][index], 1);
         if (s.scatter_histogram >= 0 && ph.scatter == 1 && t.out->histograms && t.out->histograms[s.scatter_histogram])
           atomic_add_int(&t.out->histograms[s.scatter_histogram][index], 1);
@@ -651,6 +660,15 @@ uint64_t batch_count(uint64_t n) {
 
 extern "C" {
 
+// Event counts accumulated by gg_oracle_run since the last reset:
+// [voxel steps, box steps, dose deposits, histogram increments, primaries].
+__attribute__((visibility("default"))) void gg_oracle_counts(uint64_t* out, int reset) {
+  for (int k = 0; k < 5; ++k) {
+    if (out) out[k] = g_counts[k].load();
+    if (reset) g_counts[k] = 0;
+  }
+}
+
 // Register the Rayleigh form-factor fit tables PP0..PP8 (101 floats each).
 __attribute__((visibility("default"))) void gg_oracle_set_rayleigh_fit(const float* const* pp) {
   for (int i = 0; i < 9; ++i) g_rayleigh_fit.pp[i] = pp[i];
@@ -674,9 +692,17 @@ __attribute__((visibility("default"))) int gg_oracle_run(const gg_scene* scene, 
     for (uint64_t j = 0; j < number_of_particles % nb; ++j) sizes[j]++;
   }
   const uint64_t slots = nb ? sizes[0] : 0;
+  if (scene->rayleigh_fit)
+    for (int i = 0; i < 9; ++i) g_rayleigh_fit.pp[i] = scene->rayleigh_fit + 101 * i;
   Tallies t{scene, tallies};
   const size_t S = GG_MAXIMUM_PARTICLES;
   auto worker = [&](uint64_t begin, uint64_t end) {
+    for (auto& c : t_counts) c = 0;
+    struct Flush {
+      ~Flush() {
+        for (int k = 0; k < 5; ++k) g_counts[k] += t_counts[k];
+      }
+    } flush;
     for (uint64_t slot = begin; slot < end; ++slot) {
       Kiss rng{random_states[slot], random_states[S + slot], random_states[2 * S + slot], random_states[3 * S + slot],
                random_states[4 * S + slot]};
@@ -684,6 +710,7 @@ __attribute__((visibility("default"))) int gg_oracle_run(const gg_scene* scene, 
       ph.solid_id = -1;
       for (uint64_t b = 0; b < nb; ++b) {
         if (slot >= sizes[b]) break;
+        ++t_counts[4];
         if (source->type == GG_SOURCE_XRAY) xray_primary(ph, rng, *source);
         else voxelized_primary(ph, rng, *source);
         transport(ph, rng, *scene, t);

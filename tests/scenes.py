@@ -343,43 +343,18 @@ def water_box_scene(n=64, voxel=2.0, dose=True, photon_tracking=False):
     return sc
 
 
-def ellipsoid_phantom(n, voxel, seed=1, n_bones=8):
+def ellipsoid_phantom(n, voxel, seed=1, n_bones=None):
     """C2 generator: air / water ellipsoid / bone ellipsoids, labels (nz, ny, nx)."""
-    rng = np.random.default_rng(seed)
-    c = (np.arange(n, dtype=np.float64) + 0.5) * voxel - n * voxel / 2.0
-    z, y, x = np.meshgrid(c, c, c, indexing="ij")
-    scale = n * voxel / 256.0
-    a, b, cc = 110.0 * scale, 90.0 * scale, 120.0 * scale
-    labels = np.zeros((n, n, n), np.uint8)
-    body = (x / a) ** 2 + (y / b) ** 2 + (z / cc) ** 2 <= 1.0
-    labels[body] = 1
-    for _ in range(n_bones):
-        r = rng.uniform(5, 25, 3) * scale
-        while True:
-            p = rng.uniform(-1, 1, 3)
-            if (p ** 2).sum() <= 1.0:
-                break
-        ctr = p * np.array([a, b, cc]) * 0.7
-        bone = ((x - ctr[0]) / r[0]) ** 2 + ((y - ctr[1]) / r[1]) ** 2 + ((z - ctr[2]) / r[2]) ** 2 <= 1.0
-        labels[bone & body] = 2
-    return labels
+    from ggems_b200 import workloads
+    return workloads.cbct_labels(n, voxel, seed, n_bones)
 
 
 def synthetic_spectrum():
-    """120 kVp spectrum, 1 keV bins 10-120 keV: Kramers (120 - E)/E filtered by
-    2.5 mm Al using GGEMS's own mu table for Z = 13, normalised."""
-    pd = load_physics()
-    nb = pd["mu_nb_energy_bins"]
-    idx = pd["mu_index_energy"]
-    data = pd["mu_data"].reshape(-1, 3)
-    z = 13
-    rows = data[idx[z]: idx[z] + nb[z]]
-    e_tab, mu_tab = rows[:, 0].astype(np.float64), rows[:, 1].astype(np.float64)  # MeV, cm2/g
-    energies = np.arange(10, 121, dtype=np.float64)  # keV
-    mu = np.exp(np.interp(np.log(energies * 1e-3), np.log(e_tab), np.log(mu_tab)))
-    w = np.clip(120.0 - energies, 0.0, None) / energies * np.exp(-mu * 2.699 * 0.25)
-    w = w / w.sum()
-    return [F(e * 1e-3) for e in energies], [float(x) for x in w]
+    """120 kVp spectrum, 1 keV bins 10-120 keV (ggems_b200.workloads.xray_spectrum),
+    with energies rounded through the spectrum file's text format."""
+    from ggems_b200 import workloads
+    e, w = workloads.xray_spectrum()
+    return [F(float("%.6f" % x)) for x in e], [float("%.9e" % x) for x in w]
 
 
 def cbct_scene(n=256, voxel=1.0, elements=(512, 512, 1), element_size=(0.8, 0.8, 10.0), seed=1):
