@@ -366,3 +366,107 @@ def cbct_scene(n=256, voxel=1.0, elements=(512, 512, 1), element_size=(0.8, 0.8,
     t_det = sc.add_tables(Tables(["GOS"]))
     sc.add_flat_detector(t_det, elements, element_size, sdd=1500.0, sid=1000.0, threshold=F(10.0) * KEV)
     return sc
+
+
+_libm.asinf.restype = C.c_float
+_libm.asinf.argtypes = [C.c_float]
+_libm.sqrtf.restype = C.c_float
+_libm.sqrtf.argtypes = [C.c_float]
+
+
+def add_curved_detector(sc, navigator, modules, elements, element_size, sdd, sid, threshold, scatter=True,
+                        extra_rotation=None):
+    """GGEMSCTSystem::InitializeCurvedGeometry (src/navigators/GGEMSCTSystem.cc:131-172) in float32."""
+    mx, my = modules
+    ex, ey, ez = elements
+    sx, sy, sz = [F(v) for v in element_size]
+    sdd, sid = F(sdd), F(sid)
+    c = F(F(F(ey) * sy) * F(0.5))
+    rho = F(_libm.sqrtf(F(F(sdd * sdd) + F(c * c))))
+    alpha = F(F(2.0) * F(_libm.asinf(F(c / rho))))
+    ox, oy, px, py = F(-sid), F(0.0), F(sdd - sid), F(0.0)
+    first = len(sc.solids)
+    for j in range(my):
+        step = F(alpha * F(F(j) + F(F(0.5) * F(F(1.0) - F(my)))))
+        cs, sn = F(_libm.cosf(step)), F(_libm.sinf(step))
+        gx = F(F(F(F(px - ox) * cs) - F(F(py - oy) * sn)) + ox)
+        gy = F(F(F(F(px - ox) * sn) + F(F(py - oy) * cs)) + oy)
+        for i in range(mx):
+            gz = F(F(F(F(ex) * sx)) * F(F(i) + F(F(0.5) * F(F(1.0) - F(mx)))))
+            ops = [("rotation", (0.0, 0.0, float(step))), ("translation", (float(gx), float(gy), float(gz)))]
+            if extra_rotation is not None:
+                ops.append(("rotation", extra_rotation))
+            m = geometry_matrix(DETECTOR_AXIS, ops)
+            box = [F(F(ex) * sx), F(F(ey) * sy), F(F(ez) * sz)]
+            half = [F(b * F(0.5)) for b in box]
+            s = abi.gg_solid()
+            s.type = abi.GG_SOLID_BOX
+            s.navigator = navigator
+            s.obb = _obb(m, half)
+            s.threshold = float(threshold)
+            s.virtual_element_number[:] = [ex, ey, ez]
+            s.box_size[:] = [float(b) for b in box]
+            s.histogram = len(sc.histogram_sizes)
+            sc.histogram_sizes.append(ex * ey)
+            s.scatter_histogram = -1
+            if scatter:
+                s.scatter_histogram = len(sc.histogram_sizes)
+                sc.histogram_sizes.append(ex * ey)
+            s.dose_map = -1
+            sc.solids.append(s)
+    return first
+
+
+class VoxelizedSource:
+    """GGEMSVoxelizedSource (src/sources/GGEMSVoxelizedSource.cc:287-380) in C-ABI form."""
+
+    def __init__(self, activity, voxel_size, position=(0.0, 0.0, 0.0), monoenergy=None, spectrum=None):
+        activity = np.ascontiguousarray(activity, np.float32)
+        nz, ny, nx = activity.shape
+        flat = activity.reshape(-1)
+        active = np.nonzero(flat != 0.0)[0]
+        na = len(active)
+        self.index = np.zeros(na + 1, np.int32)
+        self.index[1:] = active
+        self.index[na] = self.index[na - 1]
+        tmp = np.zeros(na + 1, np.float32)
+        tmp[1:] = flat[active]
+        total = F(0.0)
+        for v in flat[active]:
+            total = F(total + v)
+        cum = np.cumsum(tmp, dtype=np.float32)
+        self.cdf = (cum / total).astype(np.float32)
+        self.cdf[na] = 1.0
+        self.matrix = geometry_matrix(PHANTOM_AXIS, [("translation", position)])
+        if monoenergy is not None:
+            energies, weights, interp = [F(monoenergy)], [1.0], 0
+        else:
+            energies, weights = spectrum
+            interp = 1
+        self.spectrum, self.energy_cdf = fill_energy([F(e) for e in energies], weights)
+        s = abi.gg_source()
+        s.type = abi.GG_SOURCE_VOXELIZED
+        s.particle_type = 0
+        s.matrix[:] = [float(x) for x in self.matrix.reshape(-1)]
+        s.number_of_energy_bins = len(energies)
+        s.energy_spectrum = abi.ptr(self.spectrum, C.c_float)
+        s.energy_cdf = abi.ptr(self.energy_cdf, C.c_float)
+        s.is_interp = interp
+        s.number_of_voxels[:] = [nx, ny, nz]
+        vs = [F(v) for v in voxel_size]
+        s.voxel_sizes[:] = [float(v) for v in vs]
+        s.border_min[:] = [float(F(F(-F(n) * v) * F(0.5))) for n, v in zip((nx, ny, nz), vs)]
+        s.number_of_activity_bins = na + 1
+        s.activity_index = abi.ptr(self.index, C.c_int32)
+        s.activity_cdf = abi.ptr(self.cdf, C.c_float)
+        self.struct = s
+
+
+def hot_spot_activity(n=16, seed=2):
+    rng = np.random.default_rng(seed)
+    a = np.zeros((n, n, n), np.float32)
+    c = n // 2
+    a[c - 3:c + 3, c - 2:c + 4, c - 4:c + 2] = 1.0
+    idx = rng.integers(0, n, (20, 3))
+    a[idx[:, 0], idx[:, 1], idx[:, 2]] = rng.uniform(0.5, 4.0, 20).astype(np.float32)
+    return a

@@ -105,3 +105,40 @@ def test_multi_batch_random_slot_reuse(ctx):
     assert close > 0.99
     for hg, ho in zip(Tg.histograms, To.histograms):
         assert abs(int(hg.sum()) - int(ho.sum())) <= 0.005 * max(ho.sum(), 1)
+
+
+def test_voxelized_source_with_dose(ctx):
+    """GGEMSVoxelizedSource: activity-CDF voxel sampling + isotropic emission, dose in water."""
+    sc = scenes.water_box_scene(n=32, voxel=4.0, photon_tracking=True)
+    src = scenes.VoxelizedSource(scenes.hot_spot_activity(16), (4.0, 4.0, 4.0), position=(8.0, -4.0, 0.0),
+                                 monoenergy=scenes.F(140.0) * scenes.KEV)
+    n = 200000
+    Pg, Tg, sg = parity.run_gpu(ctx, sc, src, n)
+    Po, To, so = parity.run_oracle(sc, src, n)
+    exact, close = parity.history_agreement(Pg, Po)
+    _report("voxelized source", exact, close)
+    assert close > 0.995
+    assert (sg[:, :n] == so[:, :n]).all(0).mean() > 0.999
+    eg, eo = Tg.edep[0], To.edep[0]
+    assert abs(eg.sum() - eo.sum()) <= 0.005 * eo.sum()
+
+
+def test_curved_multi_module_detector(ctx):
+    """46 detector modules on an arc (the ct_scanner layout): one box solid per module."""
+    import numpy as np
+    sc = scenes.Scene()
+    t = sc.add_tables(scenes.Tables(["Water"]))
+    sc.add_voxelized(np.zeros((20, 20, 20), np.uint8), (5.0, 5.0, 5.0), t)
+    td = sc.add_tables(scenes.Tables(["GOS"]))
+    scenes.add_curved_detector(sc, td, (1, 46), (64, 16, 1), (0.6, 0.6, 0.6), 1085.6, 595.0,
+                               scenes.F(10.0) * scenes.KEV)
+    src = scenes.XRaySource(position=(-595.0, 0.0, 0.0), spectrum=scenes.synthetic_spectrum(), aperture_deg=12.5)
+    n = 200000
+    Pg, Tg, sg = parity.run_gpu(ctx, sc, src, n)
+    Po, To, so = parity.run_oracle(sc, src, n)
+    exact, close = parity.history_agreement(Pg, Po)
+    _report("curved CT", exact, close)
+    assert close > 0.995
+    tg = sum(int(h.sum()) for h in Tg.histograms[0::2])
+    to = sum(int(h.sum()) for h in To.histograms[0::2])
+    assert abs(tg - to) <= 0.005 * to

@@ -100,3 +100,24 @@ def test_pin_multiple_batches():
     src = scenes.XRaySource(monoenergy=scenes.F(80.0) * scenes.KEV, aperture_deg=11.0)
     n = 2 * 1048576 + 5
     _assert_identical(parity.run_oracle(sc, src, n), _run_ref(sc, src, n))
+
+
+def test_pin_voxelized_source_in_water_with_dose():
+    sc = scenes.water_box_scene(n=32, voxel=4.0, photon_tracking=True)
+    src = scenes.VoxelizedSource(scenes.hot_spot_activity(16), (4.0, 4.0, 4.0), position=(8.0, -4.0, 0.0),
+                                 monoenergy=scenes.F(140.0) * scenes.KEV)
+    n = 30000
+    _assert_identical(parity.run_oracle(sc, src, n), _run_ref(sc, src, n))
+
+
+def test_pin_curved_ct_modules():
+    """46-module curved detector (the ct_scanner example layout) around a water box."""
+    sc = scenes.Scene()
+    t = sc.add_tables(scenes.Tables(["Water"]))
+    sc.add_voxelized(np.zeros((20, 20, 20), np.uint8), (5.0, 5.0, 5.0), t)
+    td = sc.add_tables(scenes.Tables(["GOS"]))
+    scenes.add_curved_detector(sc, td, (1, 46), (64, 16, 1), (0.6, 0.6, 0.6), 1085.6, 595.0,
+                               scenes.F(10.0) * scenes.KEV)
+    src = scenes.XRaySource(position=(-595.0, 0.0, 0.0), spectrum=scenes.synthetic_spectrum(), aperture_deg=12.5)
+    n = 30000
+    _assert_identical(parity.run_oracle(sc, src, n), _run_ref(sc, src, n))
