@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <random>
 #include <string>
 #include <vector>
@@ -592,6 +593,87 @@ GG_API int gg_compute_dose(gg_context* c, int32_t dose_map, int32_t solid, float
   cudaFree(d_dose);
   if (d_unc) cudaFree(d_unc);
   if (e != cudaSuccess) return fail(GG_ERROR_CUDA, std::string("compute dose: ") + cudaGetErrorString(e));
+  return GG_OK;
+}
+
+}  // extern "C"
+
+// ---- dose finalisation without device allocation ----
+//
+// gg_compute_dose allocates its two device output arrays per call and frees
+// them afterwards; cudaFree synchronises the whole device, so a host that
+// finalises dose maps while transport keeps running on another stream stalls,
+// and a process whose caching allocator already holds the free HBM may not be
+// able to allocate at all.  gg_compute_dose_no_alloc writes into this fixed
+// array instead.  It is created with the library's device code on every GPU
+// that loads the library and is held until the process exits:
+// 2 x GG_NO_ALLOC_MAX_DOSELS floats (16 MiB).  In host code g_dose_scratch is
+// only the symbol handed to cudaGetSymbolAddress, never a device address.
+namespace {
+
+static __device__ __align__(256) float g_dose_scratch[2 * GG_NO_ALLOC_MAX_DOSELS];
+
+constexpr int kMaxScratchDevices = 64;
+std::mutex g_scratch_mutex;
+float* g_scratch_address[kMaxScratchDevices] = {};
+
+// Looks the array's device address up once per device, with that device
+// current (the caller has made it current).
+int scratch_for_device(int device, float** out) {
+  if (device < 0 || device >= kMaxScratchDevices) return fail(GG_ERROR_INVALID_ARGUMENT, "device index out of range");
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (!g_scratch_address[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_dose_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(GG_ERROR_CUDA, std::string("cudaGetSymbolAddress(dose scratch): ") + cudaGetErrorString(e));
+    g_scratch_address[device] = static_cast<float*>(p);
+  }
+  *out = g_scratch_address[device];
+  return GG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+GG_API int gg_compute_dose_no_alloc(gg_context* c, int32_t dose_map, int32_t solid, float scale_factor,
+                                    int32_t is_water_reference, float minimum_density, float* dose,
+                                    float* uncertainty) {
+  if (!c || !c->scene_ready || !dose) return fail(GG_ERROR_INVALID_ARGUMENT, "bad arguments");
+  if (dose_map < 0 || dose_map >= static_cast<int>(c->dose_host.size()) || solid < 0 ||
+      solid >= static_cast<int>(c->solid_host.size()) || c->solid_host[solid].type != GG_SOLID_VOXELIZED)
+    return fail(GG_ERROR_INVALID_ARGUMENT, "dose map or solid out of range");
+  const size_t n = static_cast<size_t>(c->dose_host[dose_map].total_number_of_dosels);
+  if (n > static_cast<size_t>(GG_NO_ALLOC_MAX_DOSELS))
+    return fail(GG_ERROR_INVALID_ARGUMENT, "dose map has " + std::to_string(n) +
+                                               " dosels; gg_compute_dose_no_alloc handles at most " +
+                                               std::to_string(GG_NO_ALLOC_MAX_DOSELS) + " (use gg_compute_dose)");
+  GG_CUDA(cudaSetDevice(c->device));
+  float* scratch = nullptr;
+  if (int rc = scratch_for_device(c->device, &scratch)) return rc;
+  const gg_solid& s = c->solid_host[solid];
+  gg::DoseParams P{};
+  P.map = c->dose_host[dose_map];
+  std::memcpy(P.number_of_voxels, s.number_of_voxels, sizeof(P.number_of_voxels));
+  std::memcpy(P.voxel_sizes, s.voxel_sizes, sizeof(P.voxel_sizes));
+  std::memcpy(P.border_min, s.obb.border_min, sizeof(P.border_min));
+  P.labels = s.labels;
+  P.density = c->density_dev[s.navigator];
+  P.scale_factor = scale_factor;
+  P.is_water_reference = is_water_reference;
+  P.minimum_density = minimum_density;
+  // The kernel writes every one of the n dose (and uncertainty) entries, so
+  // nothing left in the array by an earlier call is read back.
+  P.dose = scratch;
+  P.uncertainty = uncertainty ? scratch + GG_NO_ALLOC_MAX_DOSELS : nullptr;
+  gg::launch_compute_dose(P, c->stream);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dose, P.dose, n * 4, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && uncertainty)
+    e = cudaMemcpyAsync(uncertainty, P.uncertainty, n * 4, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return fail(GG_ERROR_CUDA, std::string("compute dose (no alloc): ") + cudaGetErrorString(e));
   return GG_OK;
 }
 

@@ -237,6 +237,23 @@ GG_API int gg_batch_plan(uint64_t number_of_particles, uint64_t* batch_sizes, in
 GG_API int gg_compute_dose(gg_context* context, int32_t dose_map, int32_t solid, float scale_factor,
                            int32_t is_water_reference, float minimum_density, float* dose, float* uncertainty);
 
+/* Same result as gg_compute_dose, but allocates no device memory: for hosts
+ * that must not call cudaMalloc/cudaFree while dose maps are finalised (cudaFree
+ * synchronises the whole device and stalls transport running on other
+ * streams; a process whose caching allocator holds the free memory may not get
+ * any).  No counterpart in the reference.
+ * Outputs go through one fixed device array per GPU of 2 x GG_NO_ALLOC_MAX_DOSELS
+ * floats (16 MiB), held from library load until process exit; larger dose maps
+ * are rejected with GG_ERROR_INVALID_ARGUMENT.  The first call on a device looks
+ * up that array's address (once per device), so make it before any stream
+ * capture.  All calls on one device share the array: calls that overlap (two
+ * threads, or two contexts on the same GPU) race and must be serialised by the
+ * caller. */
+#define GG_NO_ALLOC_MAX_DOSELS 2097152
+GG_API int gg_compute_dose_no_alloc(gg_context* context, int32_t dose_map, int32_t solid, float scale_factor,
+                                    int32_t is_water_reference, float minimum_density, float* dose,
+                                    float* uncertainty);
+
 /* ---- timing of the last gg_run_source (device time, ms) and launch count ---- */
 GG_API int gg_last_run_stats(gg_context* context, float* milliseconds, int64_t* kernel_launches);
 
