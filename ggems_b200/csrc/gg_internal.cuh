@@ -128,6 +128,8 @@ struct TransportParams {
   int32_t tables_in_smem;
   unsigned int* slot_counter;       // work queue head
   int* error;                       // 0 = ok
+  int32_t regroup_lanes;            // waiting lanes that start a round of the rare phases (1..32)
+  int32_t regroup_ratio4;           // ... or 4 x waiting >= regroup_ratio4 x tracking lanes
 };
 
 struct DoseParams {

@@ -7,6 +7,7 @@
 // for the photon path.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <random>
@@ -49,6 +50,9 @@ struct gg_context {
   int device = 0;
   cudaStream_t stream = nullptr;
   int sm_count = 0;
+  // warp scheduling of the transport kernel (GGEMS_B200_REGROUP_LANES / _RATIO4)
+  int regroup_lanes = 32;
+  int regroup_ratio4 = 4;
   size_t smem_optin = 0;
   uint32_t* rng = nullptr;
   gg::DevParticles particles{};
@@ -143,6 +147,14 @@ GG_API int gg_context_create(int32_t device_index, gg_context** context) {
   c->device = device_index;
   c->sm_count = prop.multiProcessorCount;
   c->smem_optin = prop.sharedMemPerBlockOptin;
+  if (const char* v = std::getenv("GGEMS_B200_REGROUP_LANES")) {
+    int r = std::atoi(v);
+    if (r >= 1 && r <= 32) c->regroup_lanes = r;
+  }
+  if (const char* v = std::getenv("GGEMS_B200_REGROUP_RATIO4")) {
+    int r = std::atoi(v);
+    if (r >= 0 && r <= 128) c->regroup_ratio4 = r;
+  }
   const size_t S = GG_MAXIMUM_PARTICLES;
   auto cleanup = [&](int code) {
     gg_context_destroy(c);
@@ -481,6 +493,8 @@ GG_API int gg_run_source(gg_context* c, const gg_source* src, uint64_t number_of
   P.tables_in_smem = c->tables_in_smem ? 1 : 0;
   P.slot_counter = c->slot_counter;
   P.error = c->error;
+  P.regroup_lanes = c->regroup_lanes;
+  P.regroup_ratio4 = c->regroup_ratio4;
   size_t smem = (c->tables_in_smem ? c->table_bytes : 0) + sizeof(gg::DevSolid) * c->number_of_solids +
                 sizeof(gg::DevNavigator) * c->number_of_navigators + 16;
   int blocks_per_sm = 0;

@@ -46,7 +46,7 @@ constexpr float kRayleighFactor = 32526509815670243328.0f;  // GGEMSRayleighScat
 // exhaustively over all 83,886,080 such values (tests/test_rng.py).
 constexpr double kKissScale = (1.0 / 4294967295.0) * 0.99999988079071044921875;
 
-enum Phase : int { kNewHistory = 0, kFind = 1, kTrackVoxel = 2, kTrackBox = 3, kDone = 4 };
+enum Phase : int { kNewHistory = 0, kFind = 1, kTrackVoxel = 2, kTrackBox = 3, kInteract = 4, kDone = 5 };
 
 struct V3 {
   float x, y, z;
@@ -243,11 +243,22 @@ __device__ __forceinline__ float next_interaction(Kiss& rng, const DevNavigator&
   return nid;
 }
 
+// State handed to and returned by the (out-of-line) interaction samplers.
+// Passed by value so that the photon and its random state stay in registers
+// in the transport loop (a reference would force them into local memory).
+struct Interaction {
+  float E;
+  V3 d;
+  Kiss rng;
+  int dead;
+};
+
 // KleinNishinaComptonSampleSecondaries, GGEMSComptonScatteringModels.hh:47-132
-__device__ __noinline__ void compton(Photon& ph, Kiss& rng) {
-  float E0 = ph.E;
+__device__ __noinline__ Interaction compton(Interaction in) {
+  Kiss rng = in.rng;
+  float E0 = in.E;
   float E0m = E0 / kElectronMassC2;
-  V3 gd = ph.d;
+  V3 gd = in.d;
   float eps0 = 1.0f / (1.0f + 2.0f * E0m);
   float eps0sq = eps0 * eps0;
   float alpha1 = -logf(eps0);
@@ -256,7 +267,10 @@ __device__ __noinline__ void compton(Photon& ph, Kiss& rng) {
   int nloop = 0;
   do {
     ++nloop;
-    if (nloop > 1000) return;
+    if (nloop > 1000) {
+      in.rng = rng;
+      return in;
+    }
     float r1 = rng.uniform();
     float r2 = rng.uniform();
     r3 = rng.uniform();
@@ -277,8 +291,10 @@ __device__ __noinline__ void compton(Photon& ph, Kiss& rng) {
   float phi = rng.uniform() * kTwoPi;
   V3 g = v3(sint * cosf(phi), sint * sinf(phi), cost);
   g = normalize3(rotate_uz(g, gd));
-  ph.E = E0 * eps;
-  ph.d = g;
+  in.E = E0 * eps;
+  in.d = g;
+  in.rng = rng;
+  return in;
 }
 
 __constant__ float c_rayleigh_pp[9][101];
@@ -289,14 +305,15 @@ __device__ __forceinline__ float rayleigh_w(float x, float n) {
 }
 
 // LivermoreRayleighSampleSecondaries, GGEMSRayleighScatteringModels.hh:169-316
-__device__ __noinline__ void rayleigh(Photon& ph, Kiss& rng, const DevNavigator& nv, const float* ebins,
-                                      const float4* sig, int material, int energy_id) {
-  float E0 = ph.E;
+__device__ __noinline__ Interaction rayleigh(Interaction in, const DevNavigator& nv, const float* ebins,
+                                             const float4* sig, int material, int energy_id) {
+  float E0 = in.E;
   if (E0 <= 250.0e-6f) {
-    ph.status = GG_DEAD;
-    return;
+    in.dead = 1;
+    return in;
   }
-  V3 gd = ph.d;
+  Kiss rng = in.rng;
+  V3 gd = in.d;
   const int nb = nv.number_of_bins;
   int n_minus_one = static_cast<int8_t>(nv.number_of_elements[material] - 1);
   int mixture = nv.element_offset[material];
@@ -347,7 +364,20 @@ __device__ __noinline__ void rayleigh(Photon& ph, Kiss& rng, const DevNavigator&
   float phi = kTwoPi * rng.uniform();
   float sint = sqrtf((1.0f - cost) * (1.0f + cost));
   V3 g = v3(sint * cosf(phi), sint * sinf(phi), cost);
-  ph.d = normalize3(rotate_uz(g, gd));
+  in.d = normalize3(rotate_uz(g, gd));
+  in.rng = rng;
+  return in;
+}
+
+// Compton or Rayleigh interaction of the photon (proc is one of the two).
+__device__ __forceinline__ void scatter(Photon& ph, Kiss& rng, int proc, const DevNavigator& nv, const float* ebins,
+                                        const float4* sig, int material, int energy_id) {
+  Interaction in{ph.E, ph.d, rng, 0};
+  in = proc == GG_COMPTON_SCATTERING ? compton(in) : rayleigh(in, nv, ebins, sig, material, energy_id);
+  ph.E = in.E;
+  ph.d = in.d;
+  rng = in.rng;
+  if (in.dead) ph.status = GG_DEAD;
 }
 
 // dose_record_standard / dose_photon_tracking, GGEMSDoseRecording.hh:65-118
@@ -437,6 +467,23 @@ __device__ void voxelized_primary(Photon& ph, Kiss& rng, const DevSource& s) {
   ph.d = dir;
 }
 
+// Histogram of interaction sites in a CT detector module (the HISTOGRAM part of
+// TrackThroughGGEMSSolidBox.cl:214-236), with the scatter histogram.
+__device__ __forceinline__ void box_histogram(const DevSolid& so, const Photon& ph) {
+  if (!so.histogram) return;
+  V3 bmin = v3(so.border_min[0], so.border_min[1], so.border_min[2]);
+  V3 es = divv(v3(so.box_size[0], so.box_size[1], so.box_size[2]),
+               v3(static_cast<float>(so.virtual_element_number[0]), static_cast<float>(so.virtual_element_number[1]),
+                  static_cast<float>(so.virtual_element_number[2])));
+  V3 q = divv(sub(ph.p, bmin), es);
+  int ix = __float2int_rz(q.x), iy = __float2int_rz(q.y);
+  if (ix >= 0 && iy >= 0 && ix < so.virtual_element_number[0] && iy < so.virtual_element_number[1]) {
+    int idx = ix + iy * so.virtual_element_number[0];
+    atomicAdd(so.histogram + idx, 1);
+    if (so.scatter_histogram && ph.scatter == 1) atomicAdd(so.scatter_histogram + idx, 1);
+  }
+}
+
 // ---- shared-memory staging with bounded waits ----
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -477,7 +524,7 @@ __device__ bool stage_tables(unsigned char* dst, const unsigned char* src, uint3
 
 extern __shared__ __align__(16) unsigned char g_smem[];
 
-__global__ void __launch_bounds__(kBlockThreads, 2) transport_kernel(TransportParams P) {
+__global__ void __launch_bounds__(kBlockThreads, 4) transport_kernel(TransportParams P) {
   // shared memory: [tables][solids][navigators][mbarrier]
   unsigned char* tables = g_smem;
   DevSolid* solids = reinterpret_cast<DevSolid*>(g_smem + (P.tables_in_smem ? P.table_bytes : 0));
@@ -506,6 +553,7 @@ __global__ void __launch_bounds__(kBlockThreads, 2) transport_kernel(TransportPa
   int energy_id = 0;
   float cached_E = -1.0f;
   int cached_nav = -1;
+  int pending = 0;  // deferred interaction: process << 8 | material
 
   // Grab the first slot.
   auto next_slot = [&]() -> bool {
@@ -536,21 +584,75 @@ __global__ void __launch_bounds__(kBlockThreads, 2) transport_kernel(TransportPa
     }
   };
 
+  auto end_history = [&]() {
+    if (--histories_left > 0) {
+      phase = kNewHistory;
+    } else {
+      finish_slot();
+      phase = next_slot() ? kNewHistory : kDone;
+    }
+  };
+  // End of track_through_*: back to the global frame; the history goes on
+  // (FindSolid) unless the photon died.
+  auto leave_solid = [&](const DevSolid& so, bool dead) {
+    ph.p = l2g_pos(so.matrix, ph.p);
+    ph.d = l2g_dir(so.matrix, ph.d);
+    if (dead) end_history();
+    else phase = kFind;
+  };
+
   if (next_slot()) phase = kNewHistory;
 
-  while (phase != kDone) {
-    if (phase == kNewHistory) {
-      if (P.source.type == GG_SOURCE_XRAY) xray_primary(ph, rng, P.source, new_aperture);
-      else voxelized_primary(ph, rng, P.source);
-      ph.scatter = 0;
-      ph.status = GG_ALIVE;
-      ph.psd = kOutOfWorld;
-      rounds = 0;
-      phase = kFind;
-      continue;
-    }
-
-    if (phase == kFind) {
+  // Warp-level phase scheduling.  Tracking steps (voxel or detector box) are
+  // ~98 % of all steps; new histories, FindSolid/ProjectToSolid rounds and
+  // Compton/Rayleigh sampling are rare but long.  Running every lane's phase
+  // each iteration would execute the rare code for one or two lanes in most
+  // iterations; instead the rare phases wait until regroup_lanes lanes need
+  // them, or until they are at least regroup_ratio4/4 times as many as the
+  // tracking lanes, and then run together.  A waiting lane draws no random
+  // number and touches no tally, so waiting changes when it computes, never
+  // what.
+  const int regroup = P.regroup_lanes;
+  const int ratio4 = P.regroup_ratio4;
+  for (;;) {
+    const unsigned active = __ballot_sync(0xffffffffu, phase != kDone);
+    if (active == 0) break;
+    const unsigned tracking = __ballot_sync(0xffffffffu, phase == kTrackVoxel || phase == kTrackBox);
+    const int n_other = __popc(active & ~tracking);
+    if (n_other > 0 && (n_other >= regroup || 4 * n_other >= ratio4 * __popc(tracking))) {
+      if (phase == kInteract) {
+        // The Compton / Rayleigh part of a tracking step (the tail of
+        // track_through_*): sample the interaction, then tally as the step would.
+        const DevSolid& so = solids[ph.solid_id];
+        const int nav = so.navigator;
+        const int material = pending & 0xff;
+        const int proc = pending >> 8;
+        float e0 = ph.E;
+        scatter(ph, rng, proc, navs[nav], tab.energy_bins(nav), tab.sigma(nav), material, energy_id);
+        if (so.type == GG_SOLID_VOXELIZED) {
+          ph.scatter = 1;  // set in voxelized solids only (TrackThroughGGEMSVoxelizedSolid.cl:253)
+          if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], e0 - ph.E, ph.p);
+          if (ph.E <= tab.photon_cut(nav)[material]) {
+            if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
+            ph.status = GG_DEAD;
+          }
+        } else if (proc == GG_COMPTON_SCATTERING) {
+          box_histogram(so, ph);
+        }
+        if (ph.status == GG_DEAD) leave_solid(so, true);
+        else phase = so.type == GG_SOLID_VOXELIZED ? kTrackVoxel : kTrackBox;
+        continue;
+      }
+      if (phase == kNewHistory) {
+        if (P.source.type == GG_SOURCE_XRAY) xray_primary(ph, rng, P.source, new_aperture);
+        else voxelized_primary(ph, rng, P.source);
+        ph.scatter = 0;
+        ph.status = GG_ALIVE;
+        ph.psd = kOutOfWorld;
+        rounds = 0;
+        phase = kFind;
+      }
+      if (phase != kFind) continue;
       bool end = rounds >= GG_MAX_LOOP;
       if (!end && P.number_of_solids == 0) {
         ++rounds;  // no navigator: the reference loop only counts iterations
@@ -598,29 +700,20 @@ __global__ void __launch_bounds__(kBlockThreads, 2) transport_kernel(TransportPa
           phase = so.type == GG_SOLID_VOXELIZED ? kTrackVoxel : kTrackBox;
         }
       }
-      if (end) {
-        if (--histories_left > 0) {
-          phase = kNewHistory;
-        } else {
-          finish_slot();
-          phase = next_slot() ? kNewHistory : kDone;
-        }
-      }
+      if (end) end_history();
       continue;
     }
+    if (phase != kTrackVoxel && phase != kTrackBox) continue;
 
     // ---- one tracking step inside solid ph.solid_id ----
     const DevSolid& so = solids[ph.solid_id];
     const int nav = so.navigator;
     const DevNavigator& nv = navs[nav];
-    const float* ebins = tab.energy_bins(nav);
     const float4* sig = tab.sigma(nav);
     V3 bmin = v3(so.border_min[0], so.border_min[1], so.border_min[2]);
     V3 bmax = v3(so.border_max[0], so.border_max[1], so.border_max[2]);
-    bool exit_solid = false;
-    bool dead = false;
     if (ph.E != cached_E || nav != cached_nav) {
-      energy_id = binary_search(ph.E, ebins, nv.number_of_bins);
+      energy_id = binary_search(ph.E, tab.energy_bins(nav), nv.number_of_bins);
       cached_E = ph.E;
       cached_nav = nav;
     }
@@ -632,50 +725,51 @@ __global__ void __launch_bounds__(kBlockThreads, 2) transport_kernel(TransportPa
       int ix = __float2int_rz(q.x), iy = __float2int_rz(q.y), iz = __float2int_rz(q.z);
       const int nx = so.number_of_voxels[0], ny = so.number_of_voxels[1], nz = so.number_of_voxels[2];
       if (ix >= nx || iy >= ny || iz >= nz || ix < 0 || iy < 0 || iz < 0) {
-        exit_solid = true;
-      } else {
-        int material = __ldg(so.labels + (ix + iy * nx + iz * nx * ny));
-        int proc;
-        float nid = next_interaction(rng, nv, sig, energy_id, material, proc);
-        V3 vmin = add(bmin, mul(v3(static_cast<float>(ix), static_cast<float>(iy), static_cast<float>(iz)), vs));
-        V3 vmax = add(vmin, vs);
-        ph.p = safety_inside(ph.p, vmin, vmax);
-        float dtb = distance_to_aabb(ph.p, ph.d, vmin, vmax);
-        if (dtb <= nid) {
-          nid = dtb + kTolerance;
-          proc = GG_TRANSPORTATION;
-          if (so.dose_map >= 0) {
-            const DevDoseMap& dm = P.dose_maps[so.dose_map];
-            if (dm.photon_tracking) {
-              int id = dosel(dm, ph.p);
-              if (id >= 0) atomicAdd(dm.photon_tracking + id, 1);
-            }
+        ph.psd = kOutOfWorld;
+        ph.solid_id = -1;
+        leave_solid(so, false);
+        continue;
+      }
+      int material = __ldg(so.labels + (ix + iy * nx + iz * nx * ny));
+      int proc;
+      float nid = next_interaction(rng, nv, sig, energy_id, material, proc);
+      V3 vmin = add(bmin, mul(v3(static_cast<float>(ix), static_cast<float>(iy), static_cast<float>(iz)), vs));
+      V3 vmax = add(vmin, vs);
+      ph.p = safety_inside(ph.p, vmin, vmax);
+      float dtb = distance_to_aabb(ph.p, ph.d, vmin, vmax);
+      if (dtb <= nid) {
+        nid = dtb + kTolerance;
+        proc = GG_TRANSPORTATION;
+        if (so.dose_map >= 0) {
+          const DevDoseMap& dm = P.dose_maps[so.dose_map];
+          if (dm.photon_tracking) {
+            int id = dosel(dm, ph.p);
+            if (id >= 0) atomicAdd(dm.photon_tracking + id, 1);
           }
-        }
-        ph.p = safety_outside(add(ph.p, scale(ph.d, nid)), vmin, vmax);
-        if (!in_aabb(ph.p, bmin, bmax)) {
-          exit_solid = true;
-        } else {
-          float e0 = ph.E;
-          if (proc != GG_TRANSPORTATION) {
-            if (proc == GG_COMPTON_SCATTERING) {
-              compton(ph, rng);
-            } else if (proc == GG_PHOTOELECTRIC_EFFECT) {
-              ph.status = GG_DEAD;
-              ph.E = 0.0f;
-            } else if (proc == GG_RAYLEIGH_SCATTERING) {
-              rayleigh(ph, rng, nv, ebins, sig, material, energy_id);
-            }
-            if (proc == GG_COMPTON_SCATTERING || proc == GG_RAYLEIGH_SCATTERING) ph.scatter = 1;
-            if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], e0 - ph.E, ph.p);
-          }
-          if (ph.E <= tab.photon_cut(nav)[material]) {
-            if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
-            ph.status = GG_DEAD;
-          }
-          dead = ph.status == GG_DEAD;
         }
       }
+      ph.p = safety_outside(add(ph.p, scale(ph.d, nid)), vmin, vmax);
+      if (!in_aabb(ph.p, bmin, bmax)) {
+        ph.psd = kOutOfWorld;
+        ph.solid_id = -1;
+        leave_solid(so, false);
+        continue;
+      }
+      if (proc == GG_COMPTON_SCATTERING || proc == GG_RAYLEIGH_SCATTERING) {
+        pending = (proc << 8) | material;
+        phase = kInteract;
+        continue;
+      }
+      if (proc == GG_PHOTOELECTRIC_EFFECT) {
+        if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
+        ph.status = GG_DEAD;
+        ph.E = 0.0f;
+      }
+      if (ph.E <= tab.photon_cut(nav)[material]) {
+        if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
+        ph.status = GG_DEAD;
+      }
+      if (ph.status == GG_DEAD) leave_solid(so, true);
     } else {
       // track_through_ggems_solid_box, TrackThroughGGEMSSolidBox.cl:122-248
       int proc;
@@ -688,54 +782,23 @@ __global__ void __launch_bounds__(kBlockThreads, 2) transport_kernel(TransportPa
       }
       ph.p = safety_outside(add(ph.p, scale(ph.d, nid)), bmin, bmax);
       if (!in_aabb(ph.p, bmin, bmax)) {
-        exit_solid = true;
-      } else {
-        if (ph.E < so.threshold) ph.status = GG_DEAD;
-        if (proc != GG_TRANSPORTATION) {
-          if (proc == GG_COMPTON_SCATTERING) {
-            compton(ph, rng);
-          } else if (proc == GG_PHOTOELECTRIC_EFFECT) {
-            ph.status = GG_DEAD;
-            ph.E = 0.0f;
-          } else if (proc == GG_RAYLEIGH_SCATTERING) {
-            rayleigh(ph, rng, nv, ebins, sig, 0, energy_id);
-          }
-          if (so.histogram && (proc == GG_PHOTOELECTRIC_EFFECT || proc == GG_COMPTON_SCATTERING)) {
-            V3 es = divv(v3(so.box_size[0], so.box_size[1], so.box_size[2]),
-                         v3(static_cast<float>(so.virtual_element_number[0]),
-                            static_cast<float>(so.virtual_element_number[1]),
-                            static_cast<float>(so.virtual_element_number[2])));
-            V3 q = divv(sub(ph.p, bmin), es);
-            int ix = __float2int_rz(q.x), iy = __float2int_rz(q.y);
-            if (ix >= 0 && iy >= 0 && ix < so.virtual_element_number[0] && iy < so.virtual_element_number[1]) {
-              int idx = ix + iy * so.virtual_element_number[0];
-              atomicAdd(so.histogram + idx, 1);
-              if (so.scatter_histogram && ph.scatter == 1) atomicAdd(so.scatter_histogram + idx, 1);
-            }
-          }
-        }
-        dead = ph.status == GG_DEAD;
+        ph.psd = kOutOfWorld;
+        ph.solid_id = -1;
+        leave_solid(so, false);
+        continue;
       }
-    }
-
-    if (exit_solid) {
-      ph.psd = kOutOfWorld;
-      ph.solid_id = -1;
-    }
-    if (exit_solid || dead) {
-      // Back to the global frame (end of track_through_*).
-      ph.p = l2g_pos(so.matrix, ph.p);
-      ph.d = l2g_dir(so.matrix, ph.d);
-      if (dead) {
-        if (--histories_left > 0) {
-          phase = kNewHistory;
-        } else {
-          finish_slot();
-          phase = next_slot() ? kNewHistory : kDone;
-        }
-      } else {
-        phase = kFind;
+      if (ph.E < so.threshold) ph.status = GG_DEAD;
+      if (proc == GG_COMPTON_SCATTERING || proc == GG_RAYLEIGH_SCATTERING) {
+        pending = proc << 8;
+        phase = kInteract;
+        continue;
       }
+      if (proc == GG_PHOTOELECTRIC_EFFECT) {
+        ph.status = GG_DEAD;
+        ph.E = 0.0f;
+        box_histogram(so, ph);
+      }
+      if (ph.status == GG_DEAD) leave_solid(so, true);
     }
   }
 }
