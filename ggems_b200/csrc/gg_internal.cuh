@@ -69,6 +69,8 @@ struct DevSolid {
   float threshold;
   int32_t number_of_voxels[3];
   float voxel_sizes[3];
+  float inv_voxel_sizes[3];      // exact 2^-k when voxel_pow2
+  int32_t voxel_pow2;            // every voxel size is a power of two
   const uint8_t* labels;
   int32_t virtual_element_number[3];
   float box_size[3];

@@ -363,6 +363,16 @@ GG_API int gg_upload_scene(gg_context* c, const gg_scene* sc) {
     d.threshold = g.threshold;
     std::memcpy(d.number_of_voxels, g.number_of_voxels, sizeof(d.number_of_voxels));
     std::memcpy(d.voxel_sizes, g.voxel_sizes, sizeof(d.voxel_sizes));
+    // x / 2^k and x * 2^-k are the same correctly rounded value for every x,
+    // so power-of-two voxel sizes let the kernel multiply instead of divide.
+    d.voxel_pow2 = 1;
+    for (int a = 0; a < 3; ++a) {
+      int e = 0;
+      const float m = std::frexp(g.voxel_sizes[a], &e);  // v = m * 2^e, m in [0.5, 1)
+      const bool pow2 = std::isfinite(g.voxel_sizes[a]) && m == 0.5f && e > -125 && e < 127;
+      d.voxel_pow2 &= pow2 ? 1 : 0;
+      d.inv_voxel_sizes[a] = pow2 ? std::ldexp(1.0f, 1 - e) : 0.0f;
+    }
     std::memcpy(d.virtual_element_number, g.virtual_element_number, sizeof(d.virtual_element_number));
     std::memcpy(d.box_size, g.box_size, sizeof(d.box_size));
     d.histogram = (g.histogram >= 0 && g.histogram < sc->number_of_histograms) ? c->histograms[g.histogram] : nullptr;

@@ -135,12 +135,14 @@ __device__ __forceinline__ bool in_aabb(V3 p, V3 mn, V3 mx) {
   if (p.z < (mn.z + kTolerance) || p.z > (mx.z - kTolerance)) return false;
   return true;
 }
-__device__ __forceinline__ float distance_to_aabb(V3 p, V3 d, V3 mn, V3 mx) {
+// inv holds 1.0f / d per axis (used only where |d| >= 1e-6, as the reference
+// computes it there), so a direction's reciprocals can be computed once.
+__device__ __forceinline__ float distance_to_aabb(V3 p, V3 d, V3 inv, V3 mn, V3 mx) {
   float tmin = FLT_MIN, tmax = FLT_MAX;
   if (fabsf(d.x) < kEps6) {
     if (p.x < mn.x || p.x > mx.x) return kOutOfWorld;
   } else {
-    float id = 1.0f / d.x;
+    float id = inv.x;
     tmin = (mn.x - p.x) * id;
     tmax = (mx.x - p.x) * id;
     if (tmin > tmax) {
@@ -152,7 +154,7 @@ __device__ __forceinline__ float distance_to_aabb(V3 p, V3 d, V3 mn, V3 mx) {
   if (fabsf(d.y) < kEps6) {
     if (p.y < mn.y || p.y > mx.y) return kOutOfWorld;
   } else {
-    float id = 1.0f / d.y;
+    float id = inv.y;
     float lo = (mn.y - p.y) * id, hi = (mx.y - p.y) * id;
     if (lo > hi) {
       float t = lo;
@@ -166,7 +168,7 @@ __device__ __forceinline__ float distance_to_aabb(V3 p, V3 d, V3 mn, V3 mx) {
   if (fabsf(d.z) < kEps6) {
     if (p.z < mn.z || p.z > mx.z) return kOutOfWorld;
   } else {
-    float id = 1.0f / d.z;
+    float id = inv.z;
     float lo = (mn.z - p.z) * id, hi = (mx.z - p.z) * id;
     if (lo > hi) {
       float t = lo;
@@ -181,6 +183,11 @@ __device__ __forceinline__ float distance_to_aabb(V3 p, V3 d, V3 mn, V3 mx) {
   if (static_cast<double>(tmax - tmin) < (2.0 * static_cast<double>(kTolerance))) return kOutOfWorld;
   if (tmin <= kEps6) return tmax;
   return tmin;
+}
+
+__device__ __forceinline__ V3 reciprocal(V3 d) { return v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z); }
+__device__ __forceinline__ float distance_to_aabb(V3 p, V3 d, V3 mn, V3 mx) {
+  return distance_to_aabb(p, d, reciprocal(d), mn, mx);
 }
 
 // JKISS32, GGEMSKissEngine.hh:50-75
@@ -554,6 +561,7 @@ __global__ void __launch_bounds__(kBlockThreads, 4) transport_kernel(TransportPa
   float cached_E = -1.0f;
   int cached_nav = -1;
   int pending = 0;  // deferred interaction: process << 8 | material
+  V3 inv_d = v3(0.0f, 0.0f, 0.0f);  // reciprocal(ph.d) while tracking inside a solid
 
   // Grab the first slot.
   auto next_slot = [&]() -> bool {
@@ -639,8 +647,12 @@ __global__ void __launch_bounds__(kBlockThreads, 4) transport_kernel(TransportPa
         } else if (proc == GG_COMPTON_SCATTERING) {
           box_histogram(so, ph);
         }
-        if (ph.status == GG_DEAD) leave_solid(so, true);
-        else phase = so.type == GG_SOLID_VOXELIZED ? kTrackVoxel : kTrackBox;
+        if (ph.status == GG_DEAD) {
+          leave_solid(so, true);
+        } else {
+          inv_d = reciprocal(ph.d);
+          phase = so.type == GG_SOLID_VOXELIZED ? kTrackVoxel : kTrackBox;
+        }
         continue;
       }
       if (phase == kNewHistory) {
@@ -697,6 +709,7 @@ __global__ void __launch_bounds__(kBlockThreads, 4) transport_kernel(TransportPa
           const DevSolid& so = solids[ph.solid_id];
           ph.p = g2l_pos(so.matrix, ph.p);
           ph.d = g2l_dir(so.matrix, ph.d);
+          inv_d = reciprocal(ph.d);
           phase = so.type == GG_SOLID_VOXELIZED ? kTrackVoxel : kTrackBox;
         }
       }
@@ -721,7 +734,8 @@ __global__ void __launch_bounds__(kBlockThreads, 4) transport_kernel(TransportPa
     if (phase == kTrackVoxel) {
       // track_through_ggems_voxelized_solid, TrackThroughGGEMSVoxelizedSolid.cl:133-310
       V3 vs = v3(so.voxel_sizes[0], so.voxel_sizes[1], so.voxel_sizes[2]);
-      V3 q = divv(sub(ph.p, bmin), vs);
+      V3 q = sub(ph.p, bmin);
+      q = so.voxel_pow2 ? mul(q, v3(so.inv_voxel_sizes[0], so.inv_voxel_sizes[1], so.inv_voxel_sizes[2])) : divv(q, vs);
       int ix = __float2int_rz(q.x), iy = __float2int_rz(q.y), iz = __float2int_rz(q.z);
       const int nx = so.number_of_voxels[0], ny = so.number_of_voxels[1], nz = so.number_of_voxels[2];
       if (ix >= nx || iy >= ny || iz >= nz || ix < 0 || iy < 0 || iz < 0) {
@@ -736,7 +750,7 @@ __global__ void __launch_bounds__(kBlockThreads, 4) transport_kernel(TransportPa
       V3 vmin = add(bmin, mul(v3(static_cast<float>(ix), static_cast<float>(iy), static_cast<float>(iz)), vs));
       V3 vmax = add(vmin, vs);
       ph.p = safety_inside(ph.p, vmin, vmax);
-      float dtb = distance_to_aabb(ph.p, ph.d, vmin, vmax);
+      float dtb = distance_to_aabb(ph.p, ph.d, inv_d, vmin, vmax);
       if (dtb <= nid) {
         nid = dtb + kTolerance;
         proc = GG_TRANSPORTATION;
@@ -775,7 +789,7 @@ __global__ void __launch_bounds__(kBlockThreads, 4) transport_kernel(TransportPa
       int proc;
       float nid = next_interaction(rng, nv, sig, energy_id, 0, proc);
       ph.p = safety_inside(ph.p, bmin, bmax);
-      float dtb = distance_to_aabb(ph.p, ph.d, bmin, bmax);
+      float dtb = distance_to_aabb(ph.p, ph.d, inv_d, bmin, bmax);
       if (dtb <= nid) {
         nid = dtb + kTolerance;
         proc = GG_TRANSPORTATION;
