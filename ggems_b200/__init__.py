@@ -8,7 +8,7 @@ of include/ggems_b200.h) can be imported without it.
 """
 
 _API = ("GGEMSError", "GGEMSVerbosity", "GGEMS", "GGEMSOpenCLManager", "GGEMSMaterialsDatabaseManager",
-        "GGEMSMaterials", "GGEMSCrossSections", "GGEMSProcessesManager", "GGEMSRangeCutsManager",
+        "GGEMSMaterials", "GGEMSCrossSections", "GGEMSAttenuations", "GGEMSProcessesManager", "GGEMSRangeCutsManager",
         "GGEMSSourceManager", "GGEMSXRaySource", "GGEMSVoxelizedSource", "GGEMSVoxelizedPhantom",
         "GGEMSCTSystem", "GGEMSDosimetryCalculator", "GGEMSProfilerManager", "GGEMSRAMManager", "clean_safely")
 

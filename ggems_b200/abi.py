@@ -9,6 +9,7 @@ import ctypes as C
 
 import numpy as np
 
+GG_ATTENUATION_BINS = 220
 GG_MAXIMUM_PARTICLES = 1048576
 GG_MAX_LOOP = 100
 GG_COMPTON_SCATTERING = 0
@@ -38,7 +39,7 @@ class gg_physics_tables(C.Structure):
                 ("energy_bins", FP), ("cross_sections", FP), ("rayleigh_per_atom", FP),
                 ("density", FP), ("photon_energy_cut", FP), ("number_of_elements", IP),
                 ("element_offset", IP), ("atomic_number", UP), ("atomic_number_density", FP),
-                ("total_elements", C.c_int32)]
+                ("total_elements", C.c_int32), ("attenuation_energy_bins", FP), ("mu_en", FP)]
 
 
 class gg_solid(C.Structure):
@@ -53,7 +54,7 @@ class gg_dose_map(C.Structure):
                 ("border_min", C.c_float * 3), ("border_max", C.c_float * 3),
                 ("number_of_dosels", C.c_int32 * 3), ("total_number_of_dosels", C.c_int32),
                 ("slice_number_of_dosels", C.c_int32), ("record_edep_squared", C.c_int32),
-                ("record_hit", C.c_int32), ("record_photon_tracking", C.c_int32)]
+                ("record_hit", C.c_int32), ("record_photon_tracking", C.c_int32), ("tle", C.c_int32)]
 
 
 class gg_scene(C.Structure):

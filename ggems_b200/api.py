@@ -109,6 +109,9 @@ _SIGNATURES = {
     "create_ggems_cross_sections": (vp, [vp]), "add_process_ggems_cross_sections": (None, [vp, s, s, b]),
     "initialize_ggems_cross_sections": (None, [vp]), "get_cs_ggems_cross_sections": (f32, [vp, s, s, f32, s]),
     "clean_ggems_cross_sections": (None, [vp]),
+    "create_ggems_attenuations": (vp, [vp, vp]), "initialize_ggems_attenuations": (None, [vp]),
+    "get_mu_ggems_attenuations": (f32, [vp, s, f32, s]), "get_mu_en_ggems_attenuations": (f32, [vp, s, f32, s]),
+    "clean_ggems_attenuations": (None, [vp]),
     "get_instance_profiler_manager": (vp, []), "print_summary_profiler_manager": (None, [vp]),
     "get_instance_ggems_ram_manager": (vp, []), "print_infos_ram_manager": (None, [vp]),
 }
@@ -275,6 +278,26 @@ class GGEMSCrossSections(object):
 
     def clean(self):
         _call("clean_ggems_cross_sections", self.obj)
+
+
+class GGEMSAttenuations(object):
+    """mu / mu_en (cm^-1) of registered materials on GGEMS's 220-bin attenuation table
+    (python_module/ggems_attenuation.py)."""
+
+    def __init__(self, materials, cross_sections):
+        self.obj = _call("create_ggems_attenuations", materials.obj, cross_sections.obj)
+
+    def initialize(self):
+        _call("initialize_ggems_attenuations", self.obj)
+
+    def get_mu(self, material_name, energy, unit):
+        return _call("get_mu_ggems_attenuations", self.obj, _e(material_name), energy, _e(unit))
+
+    def get_mu_en(self, material_name, energy, unit):
+        return _call("get_mu_en_ggems_attenuations", self.obj, _e(material_name), energy, _e(unit))
+
+    def clean(self):
+        _call("clean_ggems_attenuations", self.obj)
 
 
 class GGEMSProcessesManager(object):

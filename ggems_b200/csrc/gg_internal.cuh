@@ -38,6 +38,7 @@ struct DevNavigator {
   uint32_t energy_bins_offset;   // float[number_of_bins]
   uint32_t sigma_offset;         // float4[number_of_materials * number_of_bins]
   uint32_t photon_cut_offset;    // float[number_of_materials]
+  uint32_t attenuation_offset;   // float[GG_ATTENUATION_BINS] energies, then mu_en (TLE navigators only)
   // HBM arrays read on Rayleigh interactions
   const int32_t* number_of_elements;
   const int32_t* element_offset;
@@ -77,6 +78,7 @@ struct DevSolid {
   int32_t* histogram;            // nullptr when none
   int32_t* scatter_histogram;    // nullptr when none
   int32_t dose_map;              // -1 when none
+  int32_t dose_tle;              // the dose map uses the track-length estimator
 };
 
 struct DevSource {

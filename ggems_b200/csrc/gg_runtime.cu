@@ -258,6 +258,15 @@ GG_API int gg_upload_scene(gg_context* c, const gg_scene* sc) {
   free_scene(c);
   GG_CUDA(gg::set_rayleigh_fit(sc->rayleigh_fit));
 
+  // Navigators that need the TLE attenuation tables.
+  std::vector<char> nav_tle(sc->number_of_tables, 0);
+  for (int s = 0; s < sc->number_of_solids; ++s) {
+    const gg_solid& g = sc->solids[s];
+    if (g.type == GG_SOLID_VOXELIZED && g.dose_map >= 0 && g.dose_map < sc->number_of_dose_maps &&
+        sc->dose_maps[g.dose_map].tle && g.navigator >= 0 && g.navigator < sc->number_of_tables)
+      nav_tle[g.navigator] = 1;
+  }
+
   // ---- tables: shared-memory blob + HBM element data ----
   std::vector<unsigned char> blob;
   std::vector<gg::DevNavigator> navs(sc->number_of_tables);
@@ -288,6 +297,17 @@ GG_API int gg_upload_scene(gg_context* c, const gg_scene* sc) {
     d.photon_cut_offset = static_cast<uint32_t>(blob.size());
     blob.resize(align16(d.photon_cut_offset + nm * 4), 0);
     std::memcpy(blob.data() + d.photon_cut_offset, t.photon_energy_cut, nm * 4);
+    d.attenuation_offset = 0;
+    if (nav_tle[n]) {
+      if (!t.attenuation_energy_bins || !t.mu_en)
+        return fail(GG_ERROR_INVALID_ARGUMENT, "TLE dose map without attenuation tables (navigator " + std::to_string(n) + ")");
+      d.attenuation_offset = static_cast<uint32_t>(blob.size());
+      const size_t bytes = (1 + static_cast<size_t>(nm)) * GG_ATTENUATION_BINS * 4;
+      blob.resize(align16(static_cast<uint32_t>(d.attenuation_offset + bytes)), 0);
+      std::memcpy(blob.data() + d.attenuation_offset, t.attenuation_energy_bins, GG_ATTENUATION_BINS * 4);
+      std::memcpy(blob.data() + d.attenuation_offset + GG_ATTENUATION_BINS * 4, t.mu_en,
+                  static_cast<size_t>(nm) * GG_ATTENUATION_BINS * 4);
+    }
     int rc;
     int32_t* ne;
     int32_t* eo;
@@ -380,6 +400,7 @@ GG_API int gg_upload_scene(gg_context* c, const gg_scene* sc) {
                               ? c->histograms[g.scatter_histogram]
                               : nullptr;
     d.dose_map = (g.dose_map >= 0 && g.dose_map < sc->number_of_dose_maps) ? g.dose_map : -1;
+    d.dose_tle = (d.dose_map >= 0 && g.type == GG_SOLID_VOXELIZED && sc->dose_maps[d.dose_map].tle) ? 1 : 0;
     d.labels = nullptr;
     if (g.type == GG_SOLID_VOXELIZED) {
       const size_t nv = static_cast<size_t>(g.number_of_voxels[0]) * g.number_of_voxels[1] * g.number_of_voxels[2];

@@ -228,6 +228,10 @@ struct Tab {
   __device__ __forceinline__ const float* photon_cut(int n) const {
     return reinterpret_cast<const float*>(base + nav[n].photon_cut_offset);
   }
+  // TLE tables: GG_ATTENUATION_BINS energies followed by mu_en per material
+  __device__ __forceinline__ const float* attenuation(int n) const {
+    return reinterpret_cast<const float*>(base + nav[n].attenuation_offset);
+  }
 };
 
 __device__ __forceinline__ float pick(float4 s, int pid) { return pid == 0 ? s.x : (pid == 1 ? s.y : s.z); }
@@ -474,6 +478,16 @@ __device__ void voxelized_primary(Photon& ph, Kiss& rng, const DevSource& s) {
   ph.d = dir;
 }
 
+// Track-length-estimator deposit of one voxel step
+// (TrackThroughGGEMSVoxelizedSolid.cl:286-301): E * mu_en(E, material) * step
+// (mm -> cm), with mu_en interpolated in the 220-bin attenuation table.
+__device__ __forceinline__ float tle_edep(const float* att, int material, float energy, float step) {
+  const float* me = att + GG_ATTENUATION_BINS * (1 + material);
+  int e_index = binary_search(energy, att, GG_ATTENUATION_BINS);
+  float mu_en = e_index == 0 ? me[0] : lerp_ref(att[e_index - 1], me[e_index - 1], att[e_index], me[e_index], energy);
+  return energy * mu_en * step * 0.1f;
+}
+
 // Histogram of interaction sites in a CT detector module (the HISTOGRAM part of
 // TrackThroughGGEMSSolidBox.cl:214-236), with the scatter histogram.
 __device__ __forceinline__ void box_histogram(const DevSolid& so, const Photon& ph) {
@@ -639,7 +653,7 @@ __global__ void __launch_bounds__(kBlockThreads, 4) transport_kernel(TransportPa
         scatter(ph, rng, proc, navs[nav], tab.energy_bins(nav), tab.sigma(nav), material, energy_id);
         if (so.type == GG_SOLID_VOXELIZED) {
           ph.scatter = 1;  // set in voxelized solids only (TrackThroughGGEMSVoxelizedSolid.cl:253)
-          if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], e0 - ph.E, ph.p);
+          if (so.dose_map >= 0 && !so.dose_tle) dose_record(P.dose_maps[so.dose_map], e0 - ph.E, ph.p);
           if (ph.E <= tab.photon_cut(nav)[material]) {
             if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
             ph.status = GG_DEAD;
@@ -769,13 +783,18 @@ __global__ void __launch_bounds__(kBlockThreads, 4) transport_kernel(TransportPa
         leave_solid(so, false);
         continue;
       }
+      if (so.dose_tle) {
+        // The step's deposit depends only on the energy before the interaction,
+        // so it is recorded here even when the interaction itself is deferred.
+        dose_record(P.dose_maps[so.dose_map], tle_edep(tab.attenuation(nav), material, ph.E, nid), ph.p);
+      }
       if (proc == GG_COMPTON_SCATTERING || proc == GG_RAYLEIGH_SCATTERING) {
         pending = (proc << 8) | material;
         phase = kInteract;
         continue;
       }
       if (proc == GG_PHOTOELECTRIC_EFFECT) {
-        if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
+        if (so.dose_map >= 0 && !so.dose_tle) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
         ph.status = GG_DEAD;
         ph.E = 0.0f;
       }

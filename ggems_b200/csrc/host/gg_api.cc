@@ -447,6 +447,9 @@ void DosimetryCalculator::initialize(const SolidSpec& spec) {
   map.record_edep_squared = (edep_squared || uncertainty) ? 1 : 0;
   map.record_hit = (hit || uncertainty) ? 1 : 0;
   map.record_photon_tracking = photon_tracking ? 1 : 0;
+  // GGEMSVoxelizedPhantom::Initialize enables TLE on its voxelized solid
+  // (src/navigators/GGEMSVoxelizedPhantom.cc:115-116); other navigators ignore it.
+  map.tle = (navigator && navigator->is_tle && s.type == GG_SOLID_VOXELIZED) ? 1 : 0;
 }
 
 // ------------------------------------------------------------ simulation --
@@ -550,6 +553,8 @@ void GGEMS::build_scene() {
     pt.atomic_number = t.atomic_number.data();
     pt.atomic_number_density = t.atomic_number_density.data();
     pt.total_elements = static_cast<int32_t>(t.atomic_number.size());
+    pt.attenuation_energy_bins = t.attenuation_energy_bins.empty() ? nullptr : t.attenuation_energy_bins.data();
+    pt.mu_en = t.mu_en.empty() ? nullptr : t.mu_en.data();
     tables_.push_back(pt);
     for (size_t k = 0; k < n->solids.size(); ++k) {
       SolidSpec& spec = n->solids[k];

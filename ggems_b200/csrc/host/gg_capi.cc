@@ -396,7 +396,6 @@ GG_EXPORT void dose_tle_navigator(DosimetryCalculator* d, bool b) {
   guarded([&] {
     if (!d->navigator) throw Error("GGEMSDosimetryCalculator", "SetTLE", "attach the calculator to a navigator first");
     d->navigator->is_tle = b;
-    if (b) throw Error("GGEMSDosimetryCalculator", "SetTLE", "the TLE dose mode is not part of this build yet");
   });
 }
 GG_EXPORT void attach_to_navigator_dosimetry_calculator(DosimetryCalculator* d, const char* navigator) {
@@ -526,6 +525,70 @@ GG_EXPORT float get_cs_ggems_cross_sections(CrossSectionsHandle* c, const char* 
   });
 }
 GG_EXPORT void clean_ggems_cross_sections(CrossSectionsHandle*) {}
+
+// ---- GGEMSAttenuations.hh (mu / mu_en queries on the TLE tables) ----
+namespace {
+struct AttenuationsHandle {
+  MaterialsHandle* materials;
+  NavigatorTables tables;
+  bool built = false;
+};
+// GGEMSAttenuations::GetAttenuation / GetEnergyAttenuation
+// (src/physics/GGEMSAttenuations.cc:268-335): cm^-1, linear in the 220-bin table.
+float attenuation_query(AttenuationsHandle* a, const std::vector<float>& table, const char* material, float energy,
+                        const char* unit, const char* method) {
+  if (!a->built) throw Error("GGEMSAttenuations", method, "attenuations not initialized");
+  const std::vector<float>& eb = a->tables.attenuation_energy_bins;
+  const float e = energy_unit(energy, S(unit));
+  if (e < 0.001f || e > 1.0f) {  // ATTENUATION_ENERGY_MIN / _MAX
+    std::ostringstream oss;
+    oss << "Problem energy: " << e << " " << S(unit) << " is not in the range [" << 0.001f << ", " << 1.0f << "] MeV!!!";
+    throw Error("GGEMSAttenuations", method, oss.str());
+  }
+  const int mat = material_index(a->materials->names, S(material));
+  const int nb = GG_ATTENUATION_BINS;
+  int low = 0, high = nb - 1;
+  while (high - low > 1) {
+    int mid = (high + low) / 2;
+    if (eb[mid] == e) {
+      low = mid;
+      break;
+    }
+    if (eb[mid] < e) low = mid;
+    else high = mid;
+  }
+  const float ea = eb[low], ebb = eb[low + 1];
+  const float va = table[low + static_cast<size_t>(nb) * mat], vb = table[low + 1 + static_cast<size_t>(nb) * mat];
+  if (ea > ebb) return vb;
+  if (ea >= e) return va;
+  if (ebb <= e) return vb;
+  return va + (e - ea) * (vb - va) / (ebb - ea);
+}
+}  // namespace
+
+GG_EXPORT AttenuationsHandle* create_ggems_attenuations(MaterialsHandle* m, CrossSectionsHandle*) {
+  auto* a = new (std::nothrow) AttenuationsHandle();
+  if (a) a->materials = m;
+  return a;
+}
+GG_EXPORT void initialize_ggems_attenuations(AttenuationsHandle* a) {
+  guarded([&] {
+    const Simulation& sim = Simulation::instance();
+    a->tables = build_navigator_tables(a->materials->names, sim.cs_number_of_bins, sim.cs_min_energy,
+                                       sim.cs_max_energy, {}, a->materials->photon_cut);
+    a->built = true;
+  });
+}
+GG_EXPORT float get_mu_ggems_attenuations(AttenuationsHandle* a, const char* material, float energy, const char* unit) {
+  return guarded_value<float>(0.0f, [&] { return attenuation_query(a, a->tables.mu, material, energy, unit, "GetAttenuation"); });
+}
+GG_EXPORT float get_mu_en_ggems_attenuations(AttenuationsHandle* a, const char* material, float energy,
+                                             const char* unit) {
+  return guarded_value<float>(0.0f, [&] {
+    return attenuation_query(a, a->tables.mu_en, material, energy, unit, "GetEnergyAttenuation");
+  });
+}
+GG_EXPORT void clean_ggems_attenuations(AttenuationsHandle*) {}
 
 // ---- GGEMSProfilerManager.hh / GGEMSRAMManager.hh ----
 GG_EXPORT void* get_instance_profiler_manager(void) { return &g_profiler_manager; }

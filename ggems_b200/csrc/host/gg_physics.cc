@@ -13,7 +13,10 @@
 //   Rayleigh per atom        src/physics/GGEMSRayleighScattering.cc:80-102
 //   photon range cut         src/physics/GGEMSRangeCuts.cc:129-232, 325-384, 544-590
 //   log energy table         src/physics/GGEMSLogEnergyTable.cc:40-161
+//   attenuation (mu, mu_en)  src/physics/GGEMSAttenuations.cc:40-82, 142-230
 #include "gg_physics.hh"
+
+#include "ggems_b200.h"
 
 #include <algorithm>
 #include <cmath>
@@ -24,6 +27,13 @@ namespace gg {
 
 namespace {
 constexpr float kAvogadro = 6.02214179e+23f;
+// LinearInterpolation (GGEMSMathAlgorithms.hh:76-86)
+float lerp_table(float xa, float ya, float xb, float yb, float x) {
+  if (xa > xb) return yb;
+  if (xa >= x) return ya;
+  if (xb <= x) return yb;
+  return ya + (x - xa) * (yb - ya) / (xb - xa);
+}
 constexpr float kElectronMassC2 = 0.510998910f;
 constexpr float kAtomicMassUnit = 0.01036426891f;
 }  // namespace
@@ -318,6 +328,67 @@ float photon_energy_cut(const uint8_t* Z, const float* density, int n, float cut
   return kinetic;
 }
 
+// mu and mu_en (cm^-1) of every material on GG_ATTENUATION_BINS log-spaced
+// energies from 1 keV to 1 MeV, mixed from GGEMS's per-element tables by mass
+// fraction the way GGEMSAttenuations::Initialize does it.  Two details of that
+// code are kept because the TLE dose depends on them: the energy row of
+// element Z is searched over the whole concatenated element table up to the
+// end of Z's rows (so the search usually lands in an earlier element's rows),
+// and landing on Z's first row adds that row without the mass fraction.
+void build_attenuations(NavigatorTables& t, const MaterialsDatabase& db) {
+  const PhysicsData& pd = physics_data();
+  const int32_t* rows_of = pd.get<int32_t>("mu_nb_energy_bins");
+  const int32_t* first_row = pd.get<int32_t>("mu_index_energy");
+  const float* raw = pd.get<float>("mu_data");
+  const size_t n_rows = pd.count("mu_data", 4) / 3;
+  std::vector<float> e(n_rows), mu(n_rows), mu_en(n_rows);
+  for (size_t r = 0; r < n_rows; ++r) {
+    e[r] = raw[3 * r];
+    mu[r] = raw[3 * r + 1];
+    mu_en[r] = raw[3 * r + 2];
+  }
+  constexpr int kBins = GG_ATTENUATION_BINS;
+  const float lo = 0.001f, hi = 1.0f;
+  const float slope = logf(hi / lo);
+  t.attenuation_energy_bins.resize(kBins);
+  for (int i = 0; i < kBins; ++i)
+    t.attenuation_energy_bins[i] =
+        lo * expf(slope * (static_cast<float>(i) / (static_cast<float>(kBins) - 1.0f))) * units::MeV;
+  const size_t nm = t.materials.size();
+  t.mu.assign(nm * kBins, 0.0f);
+  t.mu_en.assign(nm * kBins, 0.0f);
+  const float g_cm3 = units::g / units::cm3;
+  for (size_t m = 0; m < nm; ++m) {
+    const SingleMaterial& mat = db.material(t.materials[m]);
+    for (int i = 0; i < kBins; ++i) {
+      const float energy = t.attenuation_energy_bins[i];
+      float a = 0.0f, b = 0.0f;
+      for (size_t k = 0; k < mat.element_names.size(); ++k) {
+        const int Z = db.element(mat.element_names[k]).Z;
+        const float w = mat.fractions[k];
+        // bisection over rows [0, first_row[Z] + rows_of[Z]) (GGEMSMathAlgorithms.hh BinarySearch)
+        int left = 0, right = first_row[Z] + rows_of[Z] - 1, row = -1;
+        while (right - left > 1 && row < 0) {
+          const int mid = (left + right) / 2;
+          if (e[mid] == energy) row = mid;
+          else if (e[mid] < energy) left = mid;
+          else right = mid;
+        }
+        if (row < 0) row = left;
+        if (row == first_row[Z]) {
+          a += mu[row];
+          b += mu_en[row];
+        } else {
+          a += w * lerp_table(e[row - 1], mu[row - 1], e[row], mu[row], energy);
+          b += w * lerp_table(e[row - 1], mu_en[row - 1], e[row], mu_en[row], energy);
+        }
+      }
+      t.mu[m * kBins + i] = a * mat.density / g_cm3;
+      t.mu_en[m * kBins + i] = b * mat.density / g_cm3;
+    }
+  }
+}
+
 }  // namespace
 
 NavigatorTables build_navigator_tables(const std::vector<std::string>& materials, int number_of_bins, float min_energy,
@@ -373,6 +444,7 @@ NavigatorTables build_navigator_tables(const std::vector<std::string>& materials
       }
     }
   }
+  build_attenuations(t, db);
   return t;
 }
 

@@ -60,6 +60,10 @@ struct NavigatorTables {
   std::vector<int32_t> element_offset;         // [nmat]
   std::vector<uint8_t> atomic_number;          // [total]
   std::vector<float> atomic_number_density;    // [total]
+  // GGEMSAttenuations tables (mu, mu_en in cm^-1), built for every navigator
+  std::vector<float> attenuation_energy_bins;  // [GG_ATTENUATION_BINS]
+  std::vector<float> mu;                       // [nmat*GG_ATTENUATION_BINS]
+  std::vector<float> mu_en;                    // [nmat*GG_ATTENUATION_BINS]
 };
 
 // Builds material tables, photon energy cuts and cross sections for

@@ -28,6 +28,7 @@ typedef struct GGEMSVoxelizedPhantom GGEMSVoxelizedPhantom;
 typedef struct GGEMSCTSystem GGEMSCTSystem;
 typedef struct GGEMSDosimetryCalculator GGEMSDosimetryCalculator;
 typedef struct GGEMSMaterials GGEMSMaterials;
+typedef struct GGEMSAttenuations GGEMSAttenuations;
 typedef struct GGEMSCrossSections GGEMSCrossSections;
 
 const char* ggems_last_error(void);  /* no counterpart in the reference: B200 build addition */
@@ -149,6 +150,11 @@ void add_process_ggems_cross_sections(GGEMSCrossSections* c, const char* process
 void initialize_ggems_cross_sections(GGEMSCrossSections* c);  /* include/GGEMS/physics/GGEMSCrossSections.hh:190 */
 float get_cs_ggems_cross_sections(GGEMSCrossSections* c, const char* process, const char* material, float energy, const char* unit);  /* include/GGEMS/physics/GGEMSCrossSections.hh:202 */
 void clean_ggems_cross_sections(GGEMSCrossSections*);  /* include/GGEMS/physics/GGEMSCrossSections.hh:209 */
+GGEMSAttenuations* create_ggems_attenuations(GGEMSMaterials* m, GGEMSCrossSections* c);  /* include/GGEMS/physics/GGEMSAttenuations.hh:157 */
+void initialize_ggems_attenuations(GGEMSAttenuations* a);  /* include/GGEMS/physics/GGEMSAttenuations.hh:164 */
+float get_mu_ggems_attenuations(GGEMSAttenuations* a, const char* material, float energy, const char* unit);  /* include/GGEMS/physics/GGEMSAttenuations.hh:175 */
+float get_mu_en_ggems_attenuations(GGEMSAttenuations* a, const char* material, float energy, const char* unit);  /* include/GGEMS/physics/GGEMSAttenuations.hh:186 */
+void clean_ggems_attenuations(GGEMSAttenuations* a);  /* include/GGEMS/physics/GGEMSAttenuations.hh:193 */
 void* get_instance_profiler_manager(void);  /* include/GGEMS/tools/GGEMSProfilerManager.hh:138 */
 void print_summary_profiler_manager(void*);  /* include/GGEMS/tools/GGEMSProfilerManager.hh:145 */
 void* get_instance_ggems_ram_manager(void);  /* include/GGEMS/tools/GGEMSRAMManager.hh:174 */

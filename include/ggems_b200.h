@@ -46,6 +46,10 @@ typedef enum gg_status {
   GG_ERROR_TIMEOUT = 6
 } gg_status;
 
+/* Attenuation (mu, mu_en) table size: ATTENUATION_TABLE_NUMBER_BINS
+ * (include/GGEMS/physics/GGEMSProcessConstants.hh:62-64). */
+#define GG_ATTENUATION_BINS 220
+
 /* Photon process identifiers (include/GGEMS/physics/GGEMSProcessConstants.hh). */
 #define GG_COMPTON_SCATTERING 0
 #define GG_PHOTOELECTRIC_EFFECT 1
@@ -85,6 +89,12 @@ typedef struct gg_physics_tables {
   const uint8_t* atomic_number;         /* [total_elements] */
   const float* atomic_number_density;   /* [total_elements] atoms / mm^3 */
   int32_t total_elements;
+  /* Track-length-estimator tables: the part of GGEMSMuMuEnData
+   * (include/GGEMS/physics/GGEMSMuData.hh:41-52) the TLE dose step reads;
+   * NULL when no dose map of this navigator uses TLE. */
+  const float* attenuation_energy_bins; /* [GG_ATTENUATION_BINS] MeV, log spaced 1 keV - 1 MeV */
+  const float* mu_en;                   /* [number_of_materials*GG_ATTENUATION_BINS] cm^-1,
+                                           indexed [bin + GG_ATTENUATION_BINS*material] */
 } gg_physics_tables;
 
 typedef enum gg_solid_type {
@@ -127,6 +137,8 @@ typedef struct gg_dose_map {
   int32_t record_edep_squared;
   int32_t record_hit;
   int32_t record_photon_tracking;
+  int32_t tle;                  /* track-length estimator instead of interaction deposits
+                                   (TrackThroughGGEMSVoxelizedSolid.cl:286-301) */
 } gg_dose_map;
 
 typedef struct gg_scene {

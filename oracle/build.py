@@ -37,6 +37,8 @@ REF_KERNELS = [
     ("TrackThroughGGEMSVoxelizedSolid", [], []),
     ("TrackThroughGGEMSVoxelizedSolid", ["DOSIMETRY"],
      ["track_through_ggems_voxelized_solid=track_through_ggems_voxelized_solid_dosimetry"]),
+    ("TrackThroughGGEMSVoxelizedSolid", ["DOSIMETRY", "TLE"],
+     ["track_through_ggems_voxelized_solid=track_through_ggems_voxelized_solid_tle"]),
     ("TrackThroughGGEMSSolidBox", ["HISTOGRAM"], []),
     ("IsAlive", [], []),
 ]

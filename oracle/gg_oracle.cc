@@ -538,6 +538,7 @@ void track_voxelized(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& 
   V3 vs = v3(s.voxel_sizes[0], s.voxel_sizes[1], s.voxel_sizes[2]);
   int nx = s.number_of_voxels[0], ny = s.number_of_voxels[1], nz = s.number_of_voxels[2];
   const int dm = s.dose_map;
+  const bool tle = dm >= 0 && sc.dose_maps[dm].tle && tb.attenuation_energy_bins && tb.mu_en;
   do {
     V3 q = divv(sub(lp, bmin), vs);
     int ix = static_cast<int>(q.x), iy = static_cast<int>(q.y), iz = static_cast<int>(q.z);
@@ -572,8 +573,18 @@ void track_voxelized(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& 
     if (proc != GG_TRANSPORTATION) {
       discrete_process(ph, rng, tb, material);
       if (proc == GG_COMPTON_SCATTERING || proc == GG_RAYLEIGH_SCATTERING) ph.scatter = 1;
-      if (dm >= 0) dose_record(t, dm, initial_energy - ph.E, lp);
+      if (dm >= 0 && !tle) dose_record(t, dm, initial_energy - ph.E, lp);
       ld = ph.d;
+    }
+    if (tle) {
+      // Track-length estimator (TrackThroughGGEMSVoxelizedSolid.cl:286-301).
+      const float* eb = tb.attenuation_energy_bins;
+      const float* me = tb.mu_en + static_cast<size_t>(material) * GG_ATTENUATION_BINS;
+      int e_index = binary_search(initial_energy, eb, GG_ATTENUATION_BINS);
+      float mu_en = e_index == 0 ? me[0]
+                                 : linear_interpolation(eb[e_index - 1], me[e_index - 1], eb[e_index], me[e_index],
+                                                        initial_energy);
+      dose_record(t, dm, initial_energy * mu_en * nid * 0.1f, lp);
     }
     if (ph.E <= tb.photon_energy_cut[material]) {
       if (dm >= 0) dose_record(t, dm, ph.E, lp);

@@ -333,6 +333,14 @@ float photon_energy_cut(const std::vector<uint8_t>& Z, const std::vector<float>&
   return kinetic;
 }
 
+// LinearInterpolation (GGEMSMathAlgorithms.hh:76-86).
+float lerp(float xa, float ya, float xb, float yb, float x) {
+  if (xa > xb) return yb;
+  if (xa >= x) return ya;
+  if (xb <= x) return yb;
+  return ya + (x - xa) * (yb - ya) / (xb - xa);
+}
+
 }  // namespace
 
 extern "C" {
@@ -405,6 +413,85 @@ __attribute__((visibility("default"))) int gg_oracle_build_tables(
         }
         cross_sections[pid * block + i + static_cast<size_t>(j) * number_of_bins] = sum;
       }
+    }
+  }
+  return GG_OK;
+}
+
+// GGEMSAttenuations::GGEMSAttenuations + Initialize (src/physics/GGEMSAttenuations.cc:40-82,
+// 142-230): mu and mu_en per material on 220 log-spaced bins (1 keV - 1 MeV),
+// mixing the per-element tables of GGEMSMuDataConstants by mass fraction.
+// Reproduced as written, including two details: the energy index is searched
+// from the start of the concatenated element table up to the end of element
+// Z's rows, and a hit on an element's first row adds that row unweighted by
+// the mass fraction.  Outputs: energy_bins[220], mu/mu_en[n_materials*220]
+// (cm^-1, [bin + 220*material]).
+__attribute__((visibility("default"))) int gg_oracle_build_attenuations(
+    const char* materials_file, const char* physics_file, const char* const* material_names, int n_materials,
+    float* energy_bins, float* mu, float* mu_en) {
+  PhysicsData pd;
+  if (!load_physics(physics_file, pd)) return GG_ERROR_INVALID_ARGUMENT;
+  std::map<std::string, Material> db;
+  if (!parse_database(materials_file, db)) return GG_ERROR_INVALID_ARGUMENT;
+  const char* names = pd.get<char>("element_names");
+  const uint8_t* ez = pd.get<uint8_t>("element_z");
+  size_t ne = pd.count("element_z", 1);
+  std::map<std::string, uint8_t> z_of;
+  for (size_t i = 0; i < ne; ++i) z_of[std::string(names + 16 * i)] = ez[i];
+  const int32_t* nb_bins = pd.get<int32_t>("mu_nb_energy_bins");
+  const int32_t* index_energy = pd.get<int32_t>("mu_index_energy");
+  const float* data = pd.get<float>("mu_data");
+  const int n_elem_tables = 92;  // kMuNbElements
+  std::vector<float> energies, mu_t, mu_en_t;
+  size_t index_data = 0;
+  for (int i = 0; i <= n_elem_tables; ++i) {
+    for (int j = 0; j < nb_bins[i]; ++j) {
+      energies.push_back(data[index_data++]);
+      mu_t.push_back(data[index_data++]);
+      mu_en_t.push_back(data[index_data++]);
+    }
+  }
+  constexpr int kBins = GG_ATTENUATION_BINS;
+  const float emin = 0.001f, emax = 1.0f;
+  float slope = logf(emax / emin);
+  for (int i = 0; i < kBins; ++i)
+    energy_bins[i] = emin * expf(slope * (static_cast<float>(i) / (static_cast<float>(kBins) - 1.0f))) * kMeV;
+  for (int m = 0; m < n_materials; ++m) {
+    auto it = db.find(material_names[m]);
+    if (it == db.end()) return GG_ERROR_INVALID_ARGUMENT;
+    const Material& mat = it->second;
+    for (int i = 0; i < kBins; ++i) {
+      const float energy = energy_bins[i];
+      float mu_over_rho = 0.0f, mu_en_over_rho = 0.0f;
+      for (size_t k = 0; k < mat.elements.size(); ++k) {
+        const int Z = z_of.at(mat.elements[k]);
+        const float frac = mat.fractions[k];
+        const int first = index_energy[Z];
+        int low = 0, high = first + nb_bins[Z] - 1;  // BinarySearch (GGEMSMathAlgorithms.hh:46-63)
+        int e_index = 0;
+        bool found = false;
+        while (high - low > 1) {
+          int mid = (high + low) / 2;
+          if (energies[mid] == energy) {
+            e_index = mid;
+            found = true;
+            break;
+          }
+          if (energies[mid] < energy) low = mid;
+          else high = mid;
+        }
+        if (!found) e_index = low;
+        if (e_index == first) {
+          mu_over_rho += mu_t[e_index];
+          mu_en_over_rho += mu_en_t[e_index];
+        } else {
+          mu_over_rho += frac * lerp(energies[e_index - 1], mu_t[e_index - 1], energies[e_index], mu_t[e_index], energy);
+          mu_en_over_rho +=
+              frac * lerp(energies[e_index - 1], mu_en_t[e_index - 1], energies[e_index], mu_en_t[e_index], energy);
+        }
+      }
+      mu[m * kBins + i] = mu_over_rho * mat.density / (kGram / kCm3);
+      mu_en[m * kBins + i] = mu_en_over_rho * mat.density / (kGram / kCm3);
     }
   }
   return GG_OK;

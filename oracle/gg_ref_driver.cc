@@ -47,6 +47,10 @@ void track_through_ggems_voxelized_solid_dosimetry(ulong, GGEMSPrimaryParticles*
                                                    const GGEMSParticleCrossSections*, const GGEMSMaterialTables*,
                                                    const GGEMSMuMuEnData*, float, GGEMSDoseParams*, double*, double*,
                                                    int*, int*);
+void track_through_ggems_voxelized_solid_tle(ulong, GGEMSPrimaryParticles*, GGEMSRandom*, const GGEMSVoxelizedSolidData*,
+                                             const uchar*, const GGEMSParticleCrossSections*, const GGEMSMaterialTables*,
+                                             const GGEMSMuMuEnData*, float, GGEMSDoseParams*, double*, double*, int*,
+                                             int*);
 void track_through_ggems_solid_box(ulong, GGEMSPrimaryParticles*, GGEMSRandom*, const GGEMSSolidBoxData*, const uchar*,
                                    const GGEMSParticleCrossSections*, const GGEMSMaterialTables*, const GGEMSMuMuEnData*,
                                    float, int*, int*);
@@ -156,6 +160,21 @@ extern "C" __attribute__((visibility("default"))) int gg_ref_run(const gg_scene*
   }
   std::unique_ptr<GGEMSMuMuEnData> att(new GGEMSMuMuEnData());
   std::memset(att.get(), 0, sizeof(GGEMSMuMuEnData));
+  // Per-navigator GGEMSMuMuEnData for the TLE kernel (energy bins and mu_en).
+  std::vector<std::unique_ptr<GGEMSMuMuEnData>> att_nav(scene->number_of_tables);
+  for (int n = 0; n < scene->number_of_tables; ++n) {
+    const gg_physics_tables& t = scene->tables[n];
+    att_nav[n].reset(new GGEMSMuMuEnData());
+    std::memset(att_nav[n].get(), 0, sizeof(GGEMSMuMuEnData));
+    att_nav[n]->number_of_bins_ = GG_ATTENUATION_BINS;
+    att_nav[n]->number_of_materials_ = t.number_of_materials;
+    att_nav[n]->energy_min_ = 0.001f;
+    att_nav[n]->energy_max_ = 1.0f;
+    if (t.attenuation_energy_bins && t.mu_en) {
+      std::memcpy(att_nav[n]->energy_bins_, t.attenuation_energy_bins, sizeof(float) * GG_ATTENUATION_BINS);
+      std::memcpy(att_nav[n]->mu_en_, t.mu_en, sizeof(float) * GG_ATTENUATION_BINS * t.number_of_materials);
+    }
+  }
 
   // Per-solid data structures.
   const int ns = scene->number_of_solids;
@@ -255,10 +274,18 @@ extern "C" __attribute__((visibility("default"))) int gg_ref_run(const gg_scene*
             double* edep2 = tallies && tallies->edep_squared ? tallies->edep_squared[d] : nullptr;
             int* hit = tallies && tallies->hit ? tallies->hit[d] : nullptr;
             int* ptrack = tallies && tallies->photon_tracking ? tallies->photon_tracking[d] : nullptr;
-            parallel_for(n, threads, [&]() {
-              track_through_ggems_voxelized_solid_dosimetry(n, P, R, &vox[s], g.labels, C, M, att.get(), g.threshold,
-                                                            &dose[d], edep, edep2, hit, ptrack);
-            });
+            if (scene->dose_maps[d].tle) {
+              const GGEMSMuMuEnData* A = att_nav[g.navigator].get();
+              parallel_for(n, threads, [&]() {
+                track_through_ggems_voxelized_solid_tle(n, P, R, &vox[s], g.labels, C, M, A, g.threshold, &dose[d],
+                                                        edep, edep2, hit, ptrack);
+              });
+            } else {
+              parallel_for(n, threads, [&]() {
+                track_through_ggems_voxelized_solid_dosimetry(n, P, R, &vox[s], g.labels, C, M, att.get(),
+                                                              g.threshold, &dose[d], edep, edep2, hit, ptrack);
+              });
+            }
           } else {
             parallel_for(n, threads, [&]() {
               track_through_ggems_voxelized_solid(n, P, R, &vox[s], g.labels, C, M, att.get(), g.threshold);

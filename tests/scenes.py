@@ -152,6 +152,16 @@ class Tables:
             abi.ptr(self.atom_density, C.c_float), C.byref(total))
         assert rc == 0, "gg_oracle_build_tables failed"
         self.total = total.value
+        # GGEMSAttenuations (mu, mu_en on 220 bins), built for every navigator as GGEMS does
+        self.attenuation_energy_bins = np.zeros(abi.GG_ATTENUATION_BINS, np.float32)
+        self.mu = np.zeros(nm * abi.GG_ATTENUATION_BINS, np.float32)
+        self.mu_en = np.zeros(nm * abi.GG_ATTENUATION_BINS, np.float32)
+        lib.gg_oracle_build_attenuations.restype = C.c_int
+        rc = lib.gg_oracle_build_attenuations(
+            MATERIALS.encode() if materials_file is None else materials_file.encode(), PHYSICS.encode(), names, nm,
+            abi.ptr(self.attenuation_energy_bins, C.c_float), abi.ptr(self.mu, C.c_float),
+            abi.ptr(self.mu_en, C.c_float))
+        assert rc == 0, "gg_oracle_build_attenuations failed"
         pid = list(processes) + [0] * (3 - len(processes))
         self.struct = abi.gg_physics_tables(
             nb, nm, len(processes), (C.c_int32 * 3)(*pid), abi.ptr(self.energy_bins, C.c_float),
@@ -159,7 +169,8 @@ class Tables:
             abi.ptr(self.rayleigh, C.c_float) if 2 in processes else C.cast(None, abi.FP),
             abi.ptr(self.density, C.c_float), abi.ptr(self.photon_cut, C.c_float),
             abi.ptr(self.n_elements, C.c_int32), abi.ptr(self.offset, C.c_int32), abi.ptr(self.Z, C.c_uint8),
-            abi.ptr(self.atom_density, C.c_float), self.total)
+            abi.ptr(self.atom_density, C.c_float), self.total, abi.ptr(self.attenuation_energy_bins, C.c_float),
+            abi.ptr(self.mu_en, C.c_float))
 
 
 def _obb(matrix, half):
@@ -224,6 +235,7 @@ class Scene:
         d.record_edep_squared = 1
         d.record_hit = 1
         d.record_photon_tracking = 1 if dose.get("photon_tracking") else 0
+        d.tle = 1 if dose.get("tle") else 0
         self.dose_maps.append(d)
         return len(self.dose_maps) - 1
 
@@ -334,12 +346,13 @@ def seed_states(seed, slots=abi.GG_MAXIMUM_PARTICLES, skip=0):
     return st
 
 
-def water_box_scene(n=64, voxel=2.0, dose=True, photon_tracking=False):
+def water_box_scene(n=64, voxel=2.0, dose=True, photon_tracking=False, tle=False):
     """C1: 64^3 water, 2 mm voxels, dose map on the phantom grid."""
     sc = Scene()
     t = sc.add_tables(Tables(["Water"]))
     labels = np.zeros((n, n, n), np.uint8)
-    sc.add_voxelized(labels, (voxel, voxel, voxel), t, dose={"photon_tracking": photon_tracking} if dose else None)
+    sc.add_voxelized(labels, (voxel, voxel, voxel), t,
+                     dose={"photon_tracking": photon_tracking, "tle": tle} if dose else None)
     return sc
 
 

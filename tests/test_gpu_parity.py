@@ -142,3 +142,38 @@ def test_curved_multi_module_detector(ctx):
     tg = sum(int(h.sum()) for h in Tg.histograms[0::2])
     to = sum(int(h.sum()) for h in To.histograms[0::2])
     assert abs(tg - to) <= 0.005 * to
+
+
+def test_tle_dose_water(ctx):
+    """Track-length-estimator dose in water: same histories, same TLE tallies."""
+    sc = scenes.water_box_scene(tle=True)
+    src = scenes.XRaySource(monoenergy=scenes.F(60.0) * scenes.KEV, aperture_deg=10.0)
+    n = 200000
+    Pg, Tg, sg = parity.run_gpu(ctx, sc, src, n)
+    Po, To, so = parity.run_oracle(sc, src, n)
+    exact, close = parity.history_agreement(Pg, Po)
+    _report("TLE water", exact, close)
+    assert close > 0.995
+    assert (sg[:, :n] == so[:, :n]).all(0).mean() > 0.999
+    eg, eo = Tg.edep[0], To.edep[0]
+    assert abs(eg.sum() - eo.sum()) <= 0.005 * eo.sum()
+    assert abs(int(Tg.hit[0].sum()) - int(To.hit[0].sum())) <= 0.005 * To.hit[0].sum()
+    var_g = np.maximum(Tg.edep_squared[0] - eg ** 2 / np.maximum(Tg.hit[0], 1), 0)
+    var_o = np.maximum(To.edep_squared[0] - eo ** 2 / np.maximum(To.hit[0], 1), 0)
+    z = parity.z_scores(eg, eo, var_g, var_o)
+    assert (np.abs(z) < 3).mean() >= 0.997
+
+
+def test_tle_dose_heterogeneous(ctx):
+    sc = scenes.Scene()
+    t = sc.add_tables(scenes.Tables(["Air", "Water", "Bone185"]))
+    sc.add_voxelized(scenes.ellipsoid_phantom(32, 8.0, seed=5, n_bones=3), (8.0, 8.0, 8.0), t, dose={"tle": True})
+    src = scenes.XRaySource(spectrum=scenes.synthetic_spectrum(), aperture_deg=11.0)
+    n = 200000
+    Pg, Tg, sg = parity.run_gpu(ctx, sc, src, n)
+    Po, To, so = parity.run_oracle(sc, src, n)
+    exact, close = parity.history_agreement(Pg, Po)
+    _report("TLE heterogeneous", exact, close)
+    assert close > 0.995
+    eg, eo = Tg.edep[0], To.edep[0]
+    assert abs(eg.sum() - eo.sum()) <= 0.005 * eo.sum()

@@ -152,3 +152,48 @@ def test_polyenergetic_spectrum_file_roundtrip(tmp_path):
         assert spec[-1] == spec[-2] and abs(spec[0] - 0.010) < 1e-9
         print("ok")
     ''', tmp_path)
+
+
+def test_dosimetry_tle_flag_reaches_the_scene(tmp_path):
+    """dose_tle_navigator(True) on a voxelized phantom marks its dose map TLE and
+    ships the attenuation tables with the navigator."""
+    _run(r'''
+        import ctypes as C, numpy as np
+        from ggems_b200 import workloads, abi
+        from ggems_b200 import (GGEMSMaterialsDatabaseManager, GGEMSVoxelizedPhantom, GGEMSDosimetryCalculator,
+                                GGEMSProcessesManager, GGEMSRangeCutsManager, GGEMSXRaySource, GGEMS)
+        import scenes
+        mhd, rng = workloads.water_files(".", 16, 4.0)
+        GGEMSMaterialsDatabaseManager().set_materials(scenes.MATERIALS)
+        ph = GGEMSVoxelizedPhantom("phantom")
+        ph.set_phantom(mhd, rng)
+        ph.set_rotation(0.0, 0.0, 0.0, "deg")
+        ph.set_position(0.0, 0.0, 0.0, "mm")
+        dose = GGEMSDosimetryCalculator()
+        dose.attach_to_navigator("phantom")
+        dose.set_output_basename("dose")
+        dose.set_tle(True)
+        pm = GGEMSProcessesManager()
+        for p in ("Compton", "Photoelectric", "Rayleigh"):
+            pm.add_process(p, "gamma", "all")
+        GGEMSRangeCutsManager().set_cut("gamma", 0.1, "mm", "all")
+        s = GGEMSXRaySource("src")
+        s.set_source_particle_type("gamma")
+        s.set_number_of_particles(1000)
+        s.set_position(-1000.0, 0.0, 0.0, "mm")
+        s.set_rotation(0.0, 0.0, 0.0, "deg")
+        s.set_beam_aperture(10.0, "deg")
+        s.set_focal_spot_size(0.0, 0.0, 0.0, "mm")
+        s.set_monoenergy(60.0, "keV")
+        from ggems_b200.api import lib
+        lib.ggems_host_scene.restype = C.POINTER(abi.gg_scene)
+        sc = lib.ggems_host_scene().contents
+        assert sc.number_of_dose_maps == 1 and sc.dose_maps[0].tle == 1
+        t = sc.tables[0]
+        bins = np.ctypeslib.as_array(t.attenuation_energy_bins, (abi.GG_ATTENUATION_BINS,))
+        ref = scenes.Tables(["Water"])
+        assert np.array_equal(bins, ref.attenuation_energy_bins)
+        mu_en = np.ctypeslib.as_array(t.mu_en, (abi.GG_ATTENUATION_BINS,))
+        assert np.array_equal(mu_en.view(np.uint32), ref.mu_en.view(np.uint32))
+        print("ok")
+    ''', tmp_path)

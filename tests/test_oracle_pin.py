@@ -121,3 +121,21 @@ def test_pin_curved_ct_modules():
     src = scenes.XRaySource(position=(-595.0, 0.0, 0.0), spectrum=scenes.synthetic_spectrum(), aperture_deg=12.5)
     n = 30000
     _assert_identical(parity.run_oracle(sc, src, n), _run_ref(sc, src, n))
+
+
+def test_pin_tle_dosimetry_water():
+    """Track-length-estimator dose (TrackThroughGGEMSVoxelizedSolid.cl built with DOSIMETRY and TLE)."""
+    sc = scenes.water_box_scene(photon_tracking=True, tle=True)
+    src = scenes.XRaySource(monoenergy=scenes.F(60.0) * scenes.KEV, aperture_deg=10.0)
+    n = 30000
+    _assert_identical(parity.run_oracle(sc, src, n), _run_ref(sc, src, n))
+
+
+def test_pin_tle_dosimetry_heterogeneous():
+    """TLE in air / water / bone with a polyenergetic beam (mu_en interpolated per material)."""
+    sc = scenes.Scene()
+    t = sc.add_tables(scenes.Tables(["Air", "Water", "Bone185"]))
+    sc.add_voxelized(scenes.ellipsoid_phantom(32, 8.0, seed=5, n_bones=3), (8.0, 8.0, 8.0), t, dose={"tle": True})
+    src = scenes.XRaySource(spectrum=scenes.synthetic_spectrum(), aperture_deg=11.0)
+    n = 30000
+    _assert_identical(parity.run_oracle(sc, src, n), _run_ref(sc, src, n))

@@ -94,3 +94,48 @@ def test_attenuation_matches_ggems_mu_table():
     # GGEMS uses the Geant4 empirical Compton and Livermore Rayleigh fits; they sit
     # within ~7 % of the tabulated mu/rho between 20 and 500 keV.
     assert np.all(np.abs(ratio - 1.0) < 0.08), ratio
+
+
+@pytest.mark.parametrize("materials", [["Water"], ["Air", "Water", "Bone185"], ["GOS", "Aluminium"]])
+def test_attenuation_tables_bit_exact(materials, tmp_path):
+    """GGEMSAttenuations through the host API (get_mu / get_mu_en at the bin energies)
+    against the oracle's restatement of GGEMSAttenuations::Initialize."""
+    import os
+    import subprocess
+    import sys
+    import textwrap
+    o = scenes.Tables(materials)
+    np.save(tmp_path / "bins.npy", o.attenuation_energy_bins)
+    code = textwrap.dedent(r'''
+        import numpy as np, sys
+        from ggems_b200 import GGEMSMaterialsDatabaseManager, GGEMSMaterials, GGEMSCrossSections, GGEMSAttenuations
+        GGEMSMaterialsDatabaseManager().set_materials(sys.argv[1])
+        mats = sys.argv[2].split(",")
+        m = GGEMSMaterials()
+        for x in mats:
+            m.add_material(x)
+        m.initialize()
+        cs = GGEMSCrossSections(m)
+        a = GGEMSAttenuations(m, cs)
+        a.initialize()
+        bins = np.load("bins.npy")
+        bins = bins[bins <= np.float32(1.0)]  # the top bin rounds above 1 MeV: outside the query range
+        mu = np.array([[a.get_mu(x, float(e), "MeV") for e in bins] for x in mats], np.float32)
+        mu_en = np.array([[a.get_mu_en(x, float(e), "MeV") for e in bins] for x in mats], np.float32)
+        np.save("mu.npy", mu.reshape(-1))
+        np.save("mu_en.npy", mu_en.reshape(-1))
+    ''')
+    (tmp_path / "case.py").write_text(code)
+    env = dict(os.environ, PYTHONPATH=scenes.ROOT)
+    out = subprocess.run([sys.executable, "case.py", scenes.MATERIALS, ",".join(materials)], capture_output=True,
+                         text=True, env=env, cwd=str(tmp_path), timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    keep = int((o.attenuation_energy_bins <= np.float32(1.0)).sum())
+    assert keep >= 218
+    nm = len(materials)
+    mu = np.load(tmp_path / "mu.npy").reshape(nm, keep)
+    mu_en = np.load(tmp_path / "mu_en.npy").reshape(nm, keep)
+    ref_mu = o.mu.reshape(nm, -1)[:, :keep]
+    ref_mu_en = o.mu_en.reshape(nm, -1)[:, :keep]
+    assert np.array_equal(mu.view(np.uint32), ref_mu.view(np.uint32))
+    assert np.array_equal(mu_en.view(np.uint32), ref_mu_en.view(np.uint32))
