@@ -10,6 +10,7 @@ import ctypes as C
 import numpy as np
 
 GG_ATTENUATION_BINS = 220
+GG_TRIANGLE_FLOATS = 13
 GG_MAXIMUM_PARTICLES = 1048576
 GG_MAX_LOOP = 100
 GG_COMPTON_SCATTERING = 0
@@ -46,7 +47,9 @@ class gg_solid(C.Structure):
     _fields_ = [("type", C.c_int32), ("navigator", C.c_int32), ("obb", gg_obb), ("threshold", C.c_float),
                 ("number_of_voxels", C.c_int32 * 3), ("voxel_sizes", C.c_float * 3), ("labels", UP),
                 ("virtual_element_number", C.c_int32 * 3), ("box_size", C.c_float * 3),
-                ("histogram", C.c_int32), ("scatter_histogram", C.c_int32), ("dose_map", C.c_int32)]
+                ("histogram", C.c_int32), ("scatter_histogram", C.c_int32), ("dose_map", C.c_int32),
+                ("number_of_triangles", C.c_int32), ("triangles", FP), ("number_of_nodes", C.c_int32),
+                ("nodes", FP), ("node_first", IP), ("node_triangles", IP)]
 
 
 class gg_dose_map(C.Structure):

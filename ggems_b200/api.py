@@ -80,6 +80,14 @@ _SIGNATURES = {
     "set_material_visible_ggems_voxelized_phantom": (None, [vp, s, b]),
     "set_material_color_ggems_voxelized_phantom": (None, [vp, s, C.c_ubyte, C.c_ubyte, C.c_ubyte]),
     "set_material_color_name_ggems_voxelized_phantom": (None, [vp, s, s]),
+    "create_ggems_meshed_phantom": (vp, [s]), "set_phantom_file_ggems_meshed_phantom": (None, [vp, s]),
+    "set_position_ggems_meshed_phantom": (None, [vp, f32, f32, f32, s]),
+    "set_rotation_ggems_meshed_phantom": (None, [vp, f32, f32, f32, s]),
+    "set_visible_ggems_meshed_phantom": (None, [vp, b]),
+    "set_material_name_ggems_meshed_phantom": (None, [vp, s]),
+    "set_material_color_ggems_meshed_phantom": (None, [vp, s, C.c_ubyte, C.c_ubyte, C.c_ubyte]),
+    "set_material_color_name_ggems_meshed_phantom": (None, [vp, s, s]),
+    "set_mesh_octree_depth_ggems_meshed_phantom": (None, [vp, C.c_int]),
     "create_ggems_ct_system": (vp, [s]), "set_number_of_modules_ggems_ct_system": (None, [vp, u64, u64]),
     "set_ct_system_type_ggems_ct_system": (None, [vp, s]),
     "set_number_of_detection_elements_ggems_ct_system": (None, [vp, u64, u64, u64]),
@@ -439,6 +447,37 @@ class GGEMSVoxelizedPhantom(object):
             _call("set_material_color_name_ggems_voxelized_phantom", self.obj, _e(material_name), _e(color_name))
         else:
             _call("set_material_color_ggems_voxelized_phantom", self.obj, _e(material_name), red, green, blue)
+
+
+class GGEMSMeshedPhantom(object):
+    """Meshed (STL) phantom navigator (ggems_phantoms.py)."""
+
+    def __init__(self, meshed_phantom_name):
+        self.obj = _call("create_ggems_meshed_phantom", _e(meshed_phantom_name))
+
+    def set_phantom(self, phantom_filename):
+        _call("set_phantom_file_ggems_meshed_phantom", self.obj, _e(phantom_filename))
+
+    def set_position(self, pos_x, pos_y, pos_z, unit):
+        _call("set_position_ggems_meshed_phantom", self.obj, pos_x, pos_y, pos_z, _e(unit))
+
+    def set_rotation(self, rx, ry, rz, unit):
+        _call("set_rotation_ggems_meshed_phantom", self.obj, rx, ry, rz, _e(unit))
+
+    def set_visible(self, flag):
+        _call("set_visible_ggems_meshed_phantom", self.obj, flag)
+
+    def set_material(self, material_name):
+        _call("set_material_name_ggems_meshed_phantom", self.obj, _e(material_name))
+
+    def set_mesh_octree_depth(self, depth):
+        _call("set_mesh_octree_depth_ggems_meshed_phantom", self.obj, depth)
+
+    def set_material_color(self, material_name, red=0, green=0, blue=0, color_name=""):
+        if color_name:
+            _call("set_material_color_name_ggems_meshed_phantom", self.obj, _e(material_name), _e(color_name))
+        else:
+            _call("set_material_color_ggems_meshed_phantom", self.obj, _e(material_name), red, green, blue)
 
 
 class GGEMSCTSystem(object):

@@ -79,6 +79,13 @@ struct DevSolid {
   int32_t* scatter_histogram;    // nullptr when none
   int32_t dose_map;              // -1 when none
   int32_t dose_tle;              // the dose map uses the track-length estimator
+  // meshed solid: octree nodes that own triangles, in node order, 2 float4
+  // each ({min xyz, max x}, {max y, max z, first, count} with first / count as
+  // int bits), and triangles grouped by node, 3 float4 each
+  // ({p0 xyz, e1 x}, {e1 yz, e2 xy}, {e2 z, -, -, -}) with e1 = p1 - p0, e2 = p2 - p0.
+  const float4* mesh_nodes;
+  int32_t mesh_node_count;
+  const float4* mesh_triangles;
 };
 
 struct DevSource {
@@ -150,8 +157,8 @@ struct DoseParams {
   float* uncertainty;
 };
 
-void launch_transport(const TransportParams& p, int grid, size_t smem, void* stream);
-cudaError_t configure_transport(size_t smem, int* blocks_per_sm);
+void launch_transport(const TransportParams& p, int grid, size_t smem, void* stream, bool mesh);
+cudaError_t configure_transport(size_t smem, int* blocks_per_sm, bool mesh);
 cudaError_t set_rayleigh_fit(const float* pp);
 void launch_compute_dose(const DoseParams& p, void* stream);
 

@@ -116,6 +116,52 @@ void free_run(gg_context* c) {
 
 uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
 
+// Meshed solid: keep the octree nodes that own triangles (GGEMS skips the
+// others), with their boxes as the reference's TestLineNode computes them,
+// and the triangles regrouped by node with their two edges precomputed
+// (the same float subtractions the Moller-Trumbore test makes).
+int upload_mesh(gg_context* c, const gg_solid& g, gg::DevSolid* d) {
+  if (g.number_of_triangles < 1 || !g.triangles || g.number_of_nodes < 1 || !g.nodes || !g.node_first ||
+      !g.node_triangles)
+    return fail(GG_ERROR_INVALID_ARGUMENT, "meshed solid without triangles or octree");
+  std::vector<float4> nodes, tris;
+  for (int n = 0; n < g.number_of_nodes; ++n) {
+    const int b = g.node_first[n], e = g.node_first[n + 1];
+    if (b < 0 || e < b || e > g.number_of_triangles) return fail(GG_ERROR_INVALID_ARGUMENT, "bad octree node list");
+    if (b == e) continue;
+    const float* nd = g.nodes + 6 * n;
+    float mn[3], mx[3];
+    for (int a = 0; a < 3; ++a) {
+      mn[a] = nd[a] - nd[3 + a];
+      mx[a] = nd[a] + nd[3 + a];
+    }
+    const int first = static_cast<int>(tris.size() / 3), count = e - b;
+    float f, k;
+    std::memcpy(&f, &first, 4);
+    std::memcpy(&k, &count, 4);
+    nodes.push_back(make_float4(mn[0], mn[1], mn[2], mx[0]));
+    nodes.push_back(make_float4(mx[1], mx[2], f, k));
+    for (int i = b; i < e; ++i) {
+      const int t = g.node_triangles[i];
+      if (t < 0 || t >= g.number_of_triangles) return fail(GG_ERROR_INVALID_ARGUMENT, "bad triangle index");
+      const float* v = g.triangles + static_cast<size_t>(t) * GG_TRIANGLE_FLOATS;
+      const float e1[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]};
+      const float e2[3] = {v[6] - v[0], v[7] - v[1], v[8] - v[2]};
+      tris.push_back(make_float4(v[0], v[1], v[2], e1[0]));
+      tris.push_back(make_float4(e1[1], e1[2], e2[0], e2[1]));
+      tris.push_back(make_float4(e2[2], 0.0f, 0.0f, 0.0f));
+    }
+  }
+  float4* dn;
+  float4* dt;
+  int rc;
+  if ((rc = dev_copy(c, nodes.data(), nodes.size(), &dn)) || (rc = dev_copy(c, tris.data(), tris.size(), &dt))) return rc;
+  d->mesh_nodes = dn;
+  d->mesh_node_count = static_cast<int32_t>(nodes.size() / 2);
+  d->mesh_triangles = dt;
+  return GG_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -409,6 +455,8 @@ GG_API int gg_upload_scene(gg_context* c, const gg_scene* sc) {
       if ((rc = dev_copy(c, g.labels, nv, &lab))) return rc;
       d.labels = lab;
       c->solid_host[s].labels = lab;
+    } else if (g.type == GG_SOLID_MESHED) {
+      if ((rc = upload_mesh(c, g, &d))) return rc;
     } else if (g.type != GG_SOLID_BOX) {
       return fail(GG_ERROR_INVALID_ARGUMENT, "solid type not supported by this build");
     }
@@ -529,7 +577,9 @@ GG_API int gg_run_source(gg_context* c, const gg_source* src, uint64_t number_of
   size_t smem = (c->tables_in_smem ? c->table_bytes : 0) + sizeof(gg::DevSolid) * c->number_of_solids +
                 sizeof(gg::DevNavigator) * c->number_of_navigators + 16;
   int blocks_per_sm = 0;
-  GG_CUDA(gg::configure_transport(smem, &blocks_per_sm));
+  bool mesh = false;
+  for (const gg_solid& g : c->solid_host) mesh |= g.type == GG_SOLID_MESHED;
+  GG_CUDA(gg::configure_transport(smem, &blocks_per_sm, mesh));
   if (blocks_per_sm < 1) return fail(GG_ERROR_CUDA, "transport kernel does not fit on an SM");
   uint64_t grid = static_cast<uint64_t>(blocks_per_sm) * c->sm_count;
   uint64_t needed = (slots + gg::kBlockThreads - 1) / gg::kBlockThreads;
@@ -537,7 +587,7 @@ GG_API int gg_run_source(gg_context* c, const gg_source* src, uint64_t number_of
   GG_CUDA(cudaMemsetAsync(c->slot_counter, 0, sizeof(unsigned int), c->stream));
   GG_CUDA(cudaMemsetAsync(c->error, 0, sizeof(int), c->stream));
   GG_CUDA(cudaEventRecord(c->start, c->stream));
-  gg::launch_transport(P, static_cast<int>(grid), smem, c->stream);
+  gg::launch_transport(P, static_cast<int>(grid), smem, c->stream, mesh);
   GG_CUDA(cudaGetLastError());
   GG_CUDA(cudaEventRecord(c->stop, c->stream));
   c->last_launches = 1;
@@ -606,7 +656,8 @@ GG_API int gg_compute_dose(gg_context* c, int32_t dose_map, int32_t solid, float
                            int32_t is_water_reference, float minimum_density, float* dose, float* uncertainty) {
   if (!c || !c->scene_ready || !dose) return fail(GG_ERROR_INVALID_ARGUMENT, "bad arguments");
   if (dose_map < 0 || dose_map >= static_cast<int>(c->dose_host.size()) || solid < 0 ||
-      solid >= static_cast<int>(c->solid_host.size()) || c->solid_host[solid].type != GG_SOLID_VOXELIZED)
+      solid >= static_cast<int>(c->solid_host.size()) ||
+      (c->solid_host[solid].type != GG_SOLID_VOXELIZED && c->solid_host[solid].type != GG_SOLID_MESHED))
     return fail(GG_ERROR_INVALID_ARGUMENT, "dose map or solid out of range");
   GG_CUDA(cudaSetDevice(c->device));
   const gg_solid& s = c->solid_host[solid];
@@ -687,7 +738,8 @@ GG_API int gg_compute_dose_no_alloc(gg_context* c, int32_t dose_map, int32_t sol
                                     float* uncertainty) {
   if (!c || !c->scene_ready || !dose) return fail(GG_ERROR_INVALID_ARGUMENT, "bad arguments");
   if (dose_map < 0 || dose_map >= static_cast<int>(c->dose_host.size()) || solid < 0 ||
-      solid >= static_cast<int>(c->solid_host.size()) || c->solid_host[solid].type != GG_SOLID_VOXELIZED)
+      solid >= static_cast<int>(c->solid_host.size()) ||
+      (c->solid_host[solid].type != GG_SOLID_VOXELIZED && c->solid_host[solid].type != GG_SOLID_MESHED))
     return fail(GG_ERROR_INVALID_ARGUMENT, "dose map or solid out of range");
   const size_t n = static_cast<size_t>(c->dose_host[dose_map].total_number_of_dosels);
   if (n > static_cast<size_t>(GG_NO_ALLOC_MAX_DOSELS))

@@ -46,7 +46,7 @@ constexpr float kRayleighFactor = 32526509815670243328.0f;  // GGEMSRayleighScat
 // exhaustively over all 83,886,080 such values (tests/test_rng.py).
 constexpr double kKissScale = (1.0 / 4294967295.0) * 0.99999988079071044921875;
 
-enum Phase : int { kNewHistory = 0, kFind = 1, kTrackVoxel = 2, kTrackBox = 3, kInteract = 4, kDone = 5 };
+enum Phase : int { kNewHistory = 0, kFind = 1, kTrackVoxel = 2, kTrackBox = 3, kTrackMesh = 4, kInteract = 5, kDone = 6 };
 
 struct V3 {
   float x, y, z;
@@ -488,6 +488,95 @@ __device__ __forceinline__ float tle_edep(const float* att, int material, float 
   return energy * mu_en * step * 0.1f;
 }
 
+// ---- meshed solid (TrackThroughGGEMSMeshSolid.cl) ----
+constexpr int kMaxMeshCrossings = 16;  // MAX_TRIANGLE_INTERACTION
+
+struct MeshCrossings {
+  V3 first, second;  // nearest and second nearest crossing
+  int count;
+};
+
+__device__ __forceinline__ V3 cross3(V3 a, V3 b) {
+  return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+// GetMeshIOPositions (l.249-318): every octree node that owns triangles, in
+// node order, is slab-tested (TestLineNode, l.182-230, with the direction's
+// reciprocals) and its triangles are intersected with the Moller-Trumbore test
+// (l.121-170).  GGEMS keeps up to 16 crossings sorted by squared distance (a
+// new crossing goes after equal ones) but only reads the first two, so only
+// those two are kept here, with the same ordering rule; the search ends at 16
+// crossings (GGEMS writes past its array beyond that).
+__device__ __noinline__ MeshCrossings mesh_crossings(V3 p, V3 d, V3 inv, const float4* nodes, int node_count,
+                                                     const float4* tris) {
+  MeshCrossings out;
+  out.count = 0;
+  out.first = out.second = p;
+  float d0 = FLT_MAX, d1 = FLT_MAX;
+  bool have0 = false, have1 = false;
+  const float dir[3] = {d.x, d.y, d.z}, pos[3] = {p.x, p.y, p.z}, ood[3] = {inv.x, inv.y, inv.z};
+  for (int n = 0; n < node_count; ++n) {
+    const float4 a = __ldg(nodes + 2 * n), b = __ldg(nodes + 2 * n + 1);
+    const float mn[3] = {a.x, a.y, a.z}, mx[3] = {a.w, b.x, b.y};
+    float tmin = 0.0f, tmax = FLT_MAX;
+    bool hit = true;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      if (!hit) break;
+      if (fabsf(dir[i]) < kEps6) {
+        if (pos[i] < mn[i] || pos[i] > mx[i]) hit = false;
+      } else {
+        float t1 = (mn[i] - pos[i]) * ood[i], t2 = (mx[i] - pos[i]) * ood[i];
+        if (t1 > t2) {
+          float t = t2;
+          t2 = t1;
+          t1 = t;
+        }
+        if (t1 > tmin) tmin = t1;
+        if (t2 < tmax) tmax = t2;
+        if (tmin > tmax) hit = false;
+      }
+    }
+    if (!hit) continue;
+    const int first = __float_as_int(b.z), count = __float_as_int(b.w);
+    for (int k = first; k < first + count; ++k) {
+      const float4 t0 = __ldg(tris + 3 * k), t1 = __ldg(tris + 3 * k + 1), t2 = __ldg(tris + 3 * k + 2);
+      const V3 p0 = v3(t0.x, t0.y, t0.z), e1 = v3(t0.w, t1.x, t1.y), e2 = v3(t1.z, t1.w, t2.x);
+      const V3 h = cross3(d, e2);
+      const float det = dot3(e1, h);
+      if (det > -kEps6 && det < kEps6) continue;
+      const float f = 1.0f / det;
+      const V3 sv = sub(p, p0);
+      const float u = f * dot3(sv, h);
+      if (u < 0.0f || u > 1.0f) continue;
+      const V3 q = cross3(sv, e1);
+      const float v = f * dot3(q, d);
+      if (v < 0.0f || u + v > 1.0f) continue;
+      const float t = f * dot3(q, e2);
+      if (!(t > kEps6)) continue;
+      const V3 x = v3(p.x + d.x * t, p.y + d.y * t, p.z + d.z * t);
+      const float dx = x.x - p.x, dy = x.y - p.y, dz = x.z - p.z;
+      const float d2 = dx * dx + dy * dy + dz * dz;
+      if (!have0 || d2 < d0) {
+        if (have0) {
+          out.second = out.first;
+          d1 = d0;
+          have1 = true;
+        }
+        out.first = x;
+        d0 = d2;
+        have0 = true;
+      } else if (!have1 || d2 < d1) {
+        out.second = x;
+        d1 = d2;
+        have1 = true;
+      }
+      if (++out.count == kMaxMeshCrossings) return out;
+    }
+  }
+  return out;
+}
+
 // Histogram of interaction sites in a CT detector module (the HISTOGRAM part of
 // TrackThroughGGEMSSolidBox.cl:214-236), with the scatter histogram.
 __device__ __forceinline__ void box_histogram(const DevSolid& so, const Photon& ph) {
@@ -545,7 +634,11 @@ __device__ bool stage_tables(unsigned char* dst, const unsigned char* src, uint3
 
 extern __shared__ __align__(16) unsigned char g_smem[];
 
-__global__ void __launch_bounds__(kBlockThreads, 4) transport_kernel(TransportParams P) {
+// kMesh: the scene has a meshed solid.  Scenes without one run the variant
+// compiled without the mesh phase, so its code and registers stay out of the
+// voxel / detector hot loop.
+template <bool kMesh>
+__global__ void __launch_bounds__(kBlockThreads, kMesh ? 2 : 4) transport_kernel(TransportParams P) {
   // shared memory: [tables][solids][navigators][mbarrier]
   unsigned char* tables = g_smem;
   DevSolid* solids = reinterpret_cast<DevSolid*>(g_smem + (P.tables_in_smem ? P.table_bytes : 0));
@@ -617,10 +710,23 @@ __global__ void __launch_bounds__(kBlockThreads, 4) transport_kernel(TransportPa
   // End of track_through_*: back to the global frame; the history goes on
   // (FindSolid) unless the photon died.
   auto leave_solid = [&](const DevSolid& so, bool dead) {
-    ph.p = l2g_pos(so.matrix, ph.p);
-    ph.d = l2g_dir(so.matrix, ph.d);
+    if (kMesh && so.type == GG_SOLID_MESHED) {
+      // A meshed solid tracks in world coordinates and, on leaving (dead or
+      // not), carries the photon to its OBB boundary (TrackThroughGGEMSMeshSolid.cl:521-533).
+      V3 mn = v3(so.border_min[0], so.border_min[1], so.border_min[2]);
+      V3 mx = v3(so.border_max[0], so.border_max[1], so.border_max[2]);
+      float dist = distance_to_aabb(g2l_pos(so.matrix, ph.p), g2l_dir(so.matrix, ph.d), mn, mx);
+      float step = dist + kTolerance;
+      ph.p = v3(ph.p.x + ph.d.x * step, ph.p.y + ph.d.y * step, ph.p.z + ph.d.z * step);
+    } else {
+      ph.p = l2g_pos(so.matrix, ph.p);
+      ph.d = l2g_dir(so.matrix, ph.d);
+    }
     if (dead) end_history();
     else phase = kFind;
+  };
+  auto track_phase = [](int type) {
+    return type == GG_SOLID_VOXELIZED ? kTrackVoxel : (kMesh && type == GG_SOLID_MESHED) ? kTrackMesh : kTrackBox;
   };
 
   if (next_slot()) phase = kNewHistory;
@@ -639,7 +745,8 @@ __global__ void __launch_bounds__(kBlockThreads, 4) transport_kernel(TransportPa
   for (;;) {
     const unsigned active = __ballot_sync(0xffffffffu, phase != kDone);
     if (active == 0) break;
-    const unsigned tracking = __ballot_sync(0xffffffffu, phase == kTrackVoxel || phase == kTrackBox);
+    const unsigned tracking =
+        __ballot_sync(0xffffffffu, phase == kTrackVoxel || phase == kTrackBox || (kMesh && phase == kTrackMesh));
     const int n_other = __popc(active & ~tracking);
     if (n_other > 0 && (n_other >= regroup || 4 * n_other >= ratio4 * __popc(tracking))) {
       if (phase == kInteract) {
@@ -651,8 +758,10 @@ __global__ void __launch_bounds__(kBlockThreads, 4) transport_kernel(TransportPa
         const int proc = pending >> 8;
         float e0 = ph.E;
         scatter(ph, rng, proc, navs[nav], tab.energy_bins(nav), tab.sigma(nav), material, energy_id);
-        if (so.type == GG_SOLID_VOXELIZED) {
-          ph.scatter = 1;  // set in voxelized solids only (TrackThroughGGEMSVoxelizedSolid.cl:253)
+        if (so.type != GG_SOLID_BOX) {
+          // voxelized and meshed solids flag scattering; boxes do not
+          // (TrackThroughGGEMSVoxelizedSolid.cl:253, TrackThroughGGEMSMeshSolid.cl:484)
+          ph.scatter = 1;
           if (so.dose_map >= 0 && !so.dose_tle) dose_record(P.dose_maps[so.dose_map], e0 - ph.E, ph.p);
           if (ph.E <= tab.photon_cut(nav)[material]) {
             if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
@@ -665,7 +774,7 @@ __global__ void __launch_bounds__(kBlockThreads, 4) transport_kernel(TransportPa
           leave_solid(so, true);
         } else {
           inv_d = reciprocal(ph.d);
-          phase = so.type == GG_SOLID_VOXELIZED ? kTrackVoxel : kTrackBox;
+          phase = track_phase(so.type);
         }
         continue;
       }
@@ -719,18 +828,21 @@ __global__ void __launch_bounds__(kBlockThreads, 4) transport_kernel(TransportPa
         if (ph.status == GG_DEAD) {
           end = true;
         } else {
-          // Enter the solid: switch to local coordinates.
+          // Enter the solid: switch to local coordinates (a meshed solid's
+          // triangles are already in world coordinates).
           const DevSolid& so = solids[ph.solid_id];
-          ph.p = g2l_pos(so.matrix, ph.p);
-          ph.d = g2l_dir(so.matrix, ph.d);
+          if (!kMesh || so.type != GG_SOLID_MESHED) {
+            ph.p = g2l_pos(so.matrix, ph.p);
+            ph.d = g2l_dir(so.matrix, ph.d);
+          }
           inv_d = reciprocal(ph.d);
-          phase = so.type == GG_SOLID_VOXELIZED ? kTrackVoxel : kTrackBox;
+          phase = track_phase(so.type);
         }
       }
       if (end) end_history();
       continue;
     }
-    if (phase != kTrackVoxel && phase != kTrackBox) continue;
+    if (phase != kTrackVoxel && phase != kTrackBox && !(kMesh && phase == kTrackMesh)) continue;
 
     // ---- one tracking step inside solid ph.solid_id ----
     const DevSolid& so = solids[ph.solid_id];
@@ -803,6 +915,53 @@ __global__ void __launch_bounds__(kBlockThreads, 4) transport_kernel(TransportPa
         ph.status = GG_DEAD;
       }
       if (ph.status == GG_DEAD) leave_solid(so, true);
+    } else if (kMesh && phase == kTrackMesh) {
+      // track_through_ggems_meshed_solid, TrackThroughGGEMSMeshSolid.cl:385-518:
+      // the parity of the crossing count says whether the photon is inside the
+      // mesh; outside, it jumps to the first crossing.  Material 0.
+      const MeshCrossings x = mesh_crossings(ph.p, ph.d, inv_d, so.mesh_nodes, so.mesh_node_count, so.mesh_triangles);
+      if (x.count == 0) {
+        ph.psd = kOutOfWorld;
+        ph.solid_id = -1;
+        leave_solid(so, false);
+        continue;
+      }
+      V3 next = x.first;
+      if ((x.count & 1) == 0) {
+        ph.p = x.first;
+        next = x.second;
+      }
+      int proc;
+      float nid = next_interaction(rng, nv, sig, energy_id, 0, proc);
+      const float dx = next.x - ph.p.x, dy = next.y - ph.p.y, dz = next.z - ph.p.z;
+      const float to_next = sqrtf(dx * dx + dy * dy + dz * dz);
+      if (to_next <= nid) {
+        nid = to_next + kTolerance;
+        proc = GG_TRANSPORTATION;
+        if (so.dose_map >= 0) {
+          const DevDoseMap& dm = P.dose_maps[so.dose_map];
+          if (dm.photon_tracking) {
+            int id = dosel(dm, ph.p);
+            if (id >= 0) atomicAdd(dm.photon_tracking + id, 1);
+          }
+        }
+      }
+      ph.p = add(ph.p, scale(ph.d, nid));
+      if (proc == GG_COMPTON_SCATTERING || proc == GG_RAYLEIGH_SCATTERING) {
+        pending = proc << 8;
+        phase = kInteract;
+        continue;
+      }
+      if (proc == GG_PHOTOELECTRIC_EFFECT) {
+        if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
+        ph.status = GG_DEAD;
+        ph.E = 0.0f;
+      }
+      if (ph.E <= tab.photon_cut(nav)[0]) {
+        if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
+        ph.status = GG_DEAD;
+      }
+      if (ph.status == GG_DEAD) leave_solid(so, true);
     } else {
       // track_through_ggems_solid_box, TrackThroughGGEMSSolidBox.cl:122-248
       int proc;
@@ -836,7 +995,8 @@ __global__ void __launch_bounds__(kBlockThreads, 4) transport_kernel(TransportPa
   }
 }
 
-// compute_dose_ggems_voxelized_solid, ComputeDoseGGEMSVoxelizedSolid.cl:53-121
+// compute_dose_ggems_{voxelized,meshed}_solid, ComputeDoseGGEMSVoxelizedSolid.cl:53-121,
+// ComputeDoseGGEMSMeshSolid.cl:53-114
 __global__ void compute_dose_kernel(DoseParams P) {
   const DevDoseMap& dm = P.map;
   int id = blockIdx.x * blockDim.x + threadIdx.x;
@@ -850,10 +1010,13 @@ __global__ void compute_dose_kernel(DoseParams P) {
              static_cast<float>(dm.number_of_dosels[1] - 1) * (-0.5f * dm.size_of_dosels[1]);
   float pz = static_cast<float>(z) * dm.size_of_dosels[2] +
              static_cast<float>(dm.number_of_dosels[2] - 1) * (-0.5f * dm.size_of_dosels[2]);
-  int vx = __float2int_rz((px - P.border_min[0]) / P.voxel_sizes[0]);
-  int vy = __float2int_rz((py - P.border_min[1]) / P.voxel_sizes[1]);
-  int vz = __float2int_rz((pz - P.border_min[2]) / P.voxel_sizes[2]);
-  int material = P.labels[vx + vy * P.number_of_voxels[0] + vz * P.number_of_voxels[0] * P.number_of_voxels[1]];
+  int material = 0;  // meshed solids (ComputeDoseGGEMSMeshSolid.cl:90): material 0, no labels
+  if (P.labels) {
+    int vx = __float2int_rz((px - P.border_min[0]) / P.voxel_sizes[0]);
+    int vy = __float2int_rz((py - P.border_min[1]) / P.voxel_sizes[1]);
+    int vz = __float2int_rz((pz - P.border_min[2]) / P.voxel_sizes[2]);
+    material = P.labels[vx + vy * P.number_of_voxels[0] + vz * P.number_of_voxels[0] * P.number_of_voxels[1]];
+  }
   float vol = dm.size_of_dosels[0] * dm.size_of_dosels[1] * dm.size_of_dosels[2];
   constexpr float kGCm3 = 6.241509704e+21f / 1.e3f;  // g/cm3
   constexpr float kGy = 1.0e-12f;
@@ -877,8 +1040,9 @@ __global__ void compute_dose_kernel(DoseParams P) {
 
 }  // namespace
 
-void launch_transport(const TransportParams& p, int grid, size_t smem, void* stream) {
-  transport_kernel<<<grid, kBlockThreads, smem, static_cast<cudaStream_t>(stream)>>>(p);
+void launch_transport(const TransportParams& p, int grid, size_t smem, void* stream, bool mesh) {
+  if (mesh) transport_kernel<true><<<grid, kBlockThreads, smem, static_cast<cudaStream_t>(stream)>>>(p);
+  else transport_kernel<false><<<grid, kBlockThreads, smem, static_cast<cudaStream_t>(stream)>>>(p);
 }
 
 void launch_compute_dose(const DoseParams& p, void* stream) {
@@ -886,10 +1050,11 @@ void launch_compute_dose(const DoseParams& p, void* stream) {
   compute_dose_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(p);
 }
 
-cudaError_t configure_transport(size_t smem, int* blocks_per_sm) {
-  cudaError_t e = cudaFuncSetAttribute(transport_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+cudaError_t configure_transport(size_t smem, int* blocks_per_sm, bool mesh) {
+  auto kernel = mesh ? transport_kernel<true> : transport_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, transport_kernel, kBlockThreads, smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, kBlockThreads, smem);
 }
 
 cudaError_t set_rayleigh_fit(const float* pp /* 9*101 */) {

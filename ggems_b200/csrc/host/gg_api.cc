@@ -337,6 +337,40 @@ void VoxelizedPhantom::initialize(int first_solid_id) {
   if (dose_calculator) dose_calculator->initialize(solids[0]);
 }
 
+MeshedPhantom::MeshedPhantom(const std::string& n) : Navigator(n) {}
+
+// GGEMSMeshedPhantom::Initialize (src/navigators/GGEMSMeshedPhantom.cc:72-130):
+// rotation then position, triangles moved by the full transformation, octree,
+// OBB = octree box with an identity matrix.  TLE is ignored with a warning.
+void MeshedPhantom::initialize(int first_solid_id) {
+  (void)first_solid_id;
+  if (phantom_file.empty()) throw Error("GGEMSMeshedPhantom", "CheckParameters", "You have to set a mesh file in STL format!!!");
+  if (materials.empty()) throw Error("GGEMSMeshedPhantom", "Initialize", "You have to set a material for the meshed phantom!!!");
+  if (is_tle) std::cerr << "[GGEMS GGEMSMeshedPhantom::Initialize] WARNING!!! TLE is not possible for meshed phantom" << std::endl;
+  Transformation tr;  // identity axis (GGEMSMeshedSolid.cc:55-62)
+  if (is_update_rot) tr.set_rotation(rotation[0], rotation[1], rotation[2]);
+  if (is_update_pos) tr.set_translation(position[0], position[1], position[2]);
+  SolidSpec spec;
+  spec.mesh = std::make_shared<MeshedSolid>(build_meshed_solid(phantom_file, tr.matrix.data(), octree_depth));
+  gg_solid& s = spec.solid;
+  s.type = GG_SOLID_MESHED;
+  for (int i = 0; i < 16; ++i) s.obb.matrix[i] = (i % 5 == 0) ? 1.0f : 0.0f;
+  for (int i = 0; i < 3; ++i) {
+    s.obb.border_min[i] = spec.mesh->border_min[i];
+    s.obb.border_max[i] = spec.mesh->border_max[i];
+  }
+  s.threshold = threshold;
+  s.histogram = -1;
+  s.scatter_histogram = -1;
+  s.dose_map = -1;
+  s.number_of_triangles = spec.mesh->number_of_triangles;
+  s.number_of_nodes = static_cast<int32_t>(spec.mesh->node_first.size()) - 1;
+  solids.clear();
+  solids.push_back(std::move(spec));
+  build_tables();
+  if (dose_calculator) dose_calculator->initialize(solids[0]);
+}
+
 CTSystem::CTSystem(const std::string& n) : Navigator(n) {}
 
 // GGEMSCTSystem::Initialize / InitializeFlatGeometry / InitializeCurvedGeometry
@@ -425,6 +459,9 @@ void DosimetryCalculator::set_dosel_size(float x, float y, float z, const std::s
 // GGEMSDosimetryCalculator::Initialize (src/navigators/GGEMSDosimetryCalculator.cc:435-530)
 void DosimetryCalculator::initialize(const SolidSpec& spec) {
   const gg_solid& s = spec.solid;
+  if (s.type == GG_SOLID_MESHED && dosel_sizes[0] <= 0.0f && dosel_sizes[1] <= 0.0f && dosel_sizes[2] <= 0.0f)
+    throw Error("GGEMSDosimetryCalculator", "Initialize",
+                "a meshed phantom has no voxel size: set the dosel size with set_dosel_size");
   float vs[3] = {dosel_sizes[0], dosel_sizes[1], dosel_sizes[2]};
   if (dosel_sizes[0] < 0.0f && dosel_sizes[1] < 0.0f && dosel_sizes[2] < 0.0f)
     for (int i = 0; i < 3; ++i) vs[i] = s.voxel_sizes[i];
@@ -561,6 +598,12 @@ void GGEMS::build_scene() {
       gg_solid s = spec.solid;
       s.navigator = static_cast<int32_t>(ni);
       s.labels = spec.labels.empty() ? nullptr : spec.labels.data();
+      if (spec.mesh) {
+        s.triangles = spec.mesh->triangles.data();
+        s.nodes = spec.mesh->nodes.data();
+        s.node_first = spec.mesh->node_first.data();
+        s.node_triangles = spec.mesh->node_triangles.empty() ? nullptr : spec.mesh->node_triangles.data();
+      }
       if (auto* ct = dynamic_cast<CTSystem*>(n)) {
         s.histogram = static_cast<int32_t>(histogram_sizes_.size());
         histogram_sizes_.push_back(static_cast<int32_t>(ct->elements[0] * ct->elements[1]));

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "ggems_b200.h"
+#include "gg_mesh.hh"
 #include "gg_physics.hh"
 
 namespace gg {
@@ -90,6 +91,7 @@ class DosimetryCalculator;
 struct SolidSpec {
   gg_solid solid{};
   std::vector<uint8_t> labels;
+  std::shared_ptr<MeshedSolid> mesh;  // meshed solids only
 };
 
 class Navigator {
@@ -132,6 +134,17 @@ class VoxelizedPhantom : public Navigator {
   std::string phantom_file, range_file;
   void initialize(int first_solid_id) override;
   std::string kind() const override { return "GGEMSVoxelizedPhantom"; }
+};
+
+// GGEMSMeshedPhantom (src/navigators/GGEMSMeshedPhantom.cc): one meshed
+// solid of one material, triangles moved to world coordinates, octree.
+class MeshedPhantom : public Navigator {
+ public:
+  explicit MeshedPhantom(const std::string& name);
+  std::string phantom_file;
+  int octree_depth = 1;  // GGEMSMeshedPhantom::mesh_octree_depth_ default
+  void initialize(int first_solid_id) override;
+  std::string kind() const override { return "GGEMSMeshedPhantom"; }
 };
 
 class CTSystem : public Navigator {

@@ -317,6 +317,48 @@ GG_EXPORT void set_material_visible_ggems_voxelized_phantom(VoxelizedPhantom*, c
 GG_EXPORT void set_material_color_ggems_voxelized_phantom(VoxelizedPhantom*, const char*, unsigned char, unsigned char, unsigned char) {}
 GG_EXPORT void set_material_color_name_ggems_voxelized_phantom(VoxelizedPhantom*, const char*, const char*) {}
 
+// ---- GGEMSMeshedPhantom.hh ----
+GG_EXPORT MeshedPhantom* create_ggems_meshed_phantom(const char* name) {
+  return guarded_value<MeshedPhantom*>(nullptr, [&] { return new MeshedPhantom(S(name)); });
+}
+GG_EXPORT void set_phantom_file_ggems_meshed_phantom(MeshedPhantom* p, const char* file) { p->phantom_file = S(file); }
+GG_EXPORT void set_position_ggems_meshed_phantom(MeshedPhantom* p, float x, float y, float z, const char* unit) {
+  guarded([&] { p->set_position(x, y, z, S(unit)); });
+}
+GG_EXPORT void set_rotation_ggems_meshed_phantom(MeshedPhantom* p, float rx, float ry, float rz, const char* unit) {
+  guarded([&] { p->set_rotation(rx, ry, rz, S(unit)); });
+}
+// GGEMSNavigator::SetMaterialName: registers the phantom's (single) material.
+GG_EXPORT void set_material_name_ggems_meshed_phantom(MeshedPhantom* p, const char* material) {
+  guarded([&] { p->materials.push_back(S(material)); });
+}
+GG_EXPORT void set_mesh_octree_depth_ggems_meshed_phantom(MeshedPhantom* p, int depth) { p->octree_depth = depth; }
+// Visualisation setters: accepted, no effect (no graphics stack in this build).
+GG_EXPORT void set_visible_ggems_meshed_phantom(MeshedPhantom*, bool) {}
+GG_EXPORT void set_material_color_ggems_meshed_phantom(MeshedPhantom*, const char*, unsigned char, unsigned char, unsigned char) {}
+GG_EXPORT void set_material_color_name_ggems_meshed_phantom(MeshedPhantom*, const char*, const char*) {}
+
+// Meshed solid of an STL file as the host API prepares it (test hook; no
+// counterpart in the reference).  Output sizes: triangles n*GG_TRIANGLE_FLOATS,
+// nodes m*6, node_first m+1, node_triangles n, with n / m from the first call
+// (all output pointers NULL).
+GG_EXPORT int ggems_build_mesh(const char* stl, const float* matrix, int depth, int32_t* n_triangles, int32_t* n_nodes,
+                               float* triangles, float* nodes, int32_t* node_first, int32_t* node_triangles,
+                               float* border_min, float* border_max) {
+  return guarded_value<int>(GG_ERROR_INVALID_ARGUMENT, [&] {
+    MeshedSolid m = build_meshed_solid(S(stl), matrix, depth);
+    *n_triangles = m.number_of_triangles;
+    *n_nodes = static_cast<int32_t>(m.node_first.size()) - 1;
+    if (triangles) std::copy(m.triangles.begin(), m.triangles.end(), triangles);
+    if (nodes) std::copy(m.nodes.begin(), m.nodes.end(), nodes);
+    if (node_first) std::copy(m.node_first.begin(), m.node_first.end(), node_first);
+    if (node_triangles) std::copy(m.node_triangles.begin(), m.node_triangles.end(), node_triangles);
+    if (border_min) std::copy(m.border_min, m.border_min + 3, border_min);
+    if (border_max) std::copy(m.border_max, m.border_max + 3, border_max);
+    return static_cast<int>(GG_OK);
+  });
+}
+
 // ---- GGEMSCTSystem.hh ----
 GG_EXPORT CTSystem* create_ggems_ct_system(const char* name) {
   return guarded_value<CTSystem*>(nullptr, [&] { return new CTSystem(S(name)); });

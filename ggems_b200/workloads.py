@@ -119,3 +119,69 @@ def water_files(directory, n=64, voxel=2.0):
     with open(rng_file, "w") as f:
         f.write("0 0 Water\n")
     return mhd, rng_file
+
+
+# ---- meshed phantom (binary STL) ----
+
+def icosphere(subdivisions):
+    """Unit icosphere: (vertices float64 [V, 3], faces int [F, 3]); F = 20 * 4**subdivisions."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+         (8, 6, 7), (9, 8, 1)]
+    verts = [np.array(p, np.float64) / np.linalg.norm(p) for p in v]
+    faces = f
+    for _ in range(subdivisions):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    return np.array(verts), np.array(faces, np.int64)
+
+
+def ellipsoid_triangles(semi_axes, center=(0.0, 0.0, 0.0), subdivisions=3):
+    """Triangles [F, 3, 3] (float32, mm) of an ellipsoid surface."""
+    v, f = icosphere(subdivisions)
+    v = v * np.asarray(semi_axes, np.float64) + np.asarray(center, np.float64)
+    return v[f].astype(np.float32)
+
+
+def write_stl(path, triangles):
+    """Binary STL: 80-byte header, uint32 count, per triangle normal + 3 vertices (float32) + uint16."""
+    tri = np.asarray(triangles, np.float32).reshape(-1, 3, 3)
+    e1, e2 = tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0]
+    n = np.cross(e1, e2)
+    n /= np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-30)
+    rec = np.zeros(len(tri), np.dtype([("n", "<f4", 3), ("v", "<f4", 9), ("a", "<u2")]))
+    rec["n"] = n
+    rec["v"] = tri.reshape(-1, 9)
+    with open(path, "wb") as out:
+        out.write(b"ggems-b200 synthetic mesh".ljust(80, b" "))
+        out.write(np.uint32(len(tri)).tobytes())
+        out.write(rec.tobytes())
+    return path
+
+
+def body_mesh(body_subdivisions=3, inner_subdivisions=2, n_inner=8, seed=1):
+    """Body ellipsoid (semi-axes 120/100/150 mm) with n_inner inner ellipsoids (cavities for a
+    one-material meshed phantom), seeded; returns triangles [F, 3, 3] float32."""
+    rng = np.random.default_rng(seed)
+    parts = [ellipsoid_triangles((120.0, 100.0, 150.0), subdivisions=body_subdivisions)]
+    for _ in range(n_inner):
+        axes = rng.uniform(10.0, 30.0, 3)
+        c = rng.uniform(-0.45, 0.45, 3) * np.array([120.0, 100.0, 150.0])
+        parts.append(ellipsoid_triangles(axes, c, subdivisions=inner_subdivisions))
+    return np.concatenate(parts)

@@ -25,6 +25,7 @@ typedef struct GGEMS GGEMS;
 typedef struct GGEMSXRaySource GGEMSXRaySource;
 typedef struct GGEMSVoxelizedSource GGEMSVoxelizedSource;
 typedef struct GGEMSVoxelizedPhantom GGEMSVoxelizedPhantom;
+typedef struct GGEMSMeshedPhantom GGEMSMeshedPhantom;
 typedef struct GGEMSCTSystem GGEMSCTSystem;
 typedef struct GGEMSDosimetryCalculator GGEMSDosimetryCalculator;
 typedef struct GGEMSMaterials GGEMSMaterials;
@@ -107,6 +108,16 @@ void set_visible_ggems_voxelized_phantom(GGEMSVoxelizedPhantom*, bool);  /* incl
 void set_material_visible_ggems_voxelized_phantom(GGEMSVoxelizedPhantom*, const char*, bool);  /* include/GGEMS/navigators/GGEMSVoxelizedPhantom.hh:167 */
 void set_material_color_ggems_voxelized_phantom(GGEMSVoxelizedPhantom*, const char*, unsigned char, unsigned char, unsigned char);  /* include/GGEMS/navigators/GGEMSVoxelizedPhantom.hh:178 */
 void set_material_color_name_ggems_voxelized_phantom(GGEMSVoxelizedPhantom*, const char*, const char*);  /* include/GGEMS/navigators/GGEMSVoxelizedPhantom.hh:187 */
+GGEMSMeshedPhantom* create_ggems_meshed_phantom(const char* name);  /* include/GGEMS/navigators/GGEMSMeshedPhantom.hh:125 */
+void set_phantom_file_ggems_meshed_phantom(GGEMSMeshedPhantom* p, const char* stl_file);  /* include/GGEMS/navigators/GGEMSMeshedPhantom.hh:133 */
+void set_position_ggems_meshed_phantom(GGEMSMeshedPhantom* p, float x, float y, float z, const char* unit);  /* include/GGEMS/navigators/GGEMSMeshedPhantom.hh:144 */
+void set_rotation_ggems_meshed_phantom(GGEMSMeshedPhantom* p, float rx, float ry, float rz, const char* unit);  /* include/GGEMS/navigators/GGEMSMeshedPhantom.hh:155 */
+void set_visible_ggems_meshed_phantom(GGEMSMeshedPhantom* p, bool flag);  /* include/GGEMS/navigators/GGEMSMeshedPhantom.hh:163 */
+void set_material_name_ggems_meshed_phantom(GGEMSMeshedPhantom* p, const char* material);  /* include/GGEMS/navigators/GGEMSMeshedPhantom.hh:171 */
+void set_material_color_ggems_meshed_phantom(GGEMSMeshedPhantom* p, const char* material, unsigned char r, unsigned char g, unsigned char b);  /* include/GGEMS/navigators/GGEMSMeshedPhantom.hh:182 */
+void set_material_color_name_ggems_meshed_phantom(GGEMSMeshedPhantom* p, const char* material, const char* color);  /* include/GGEMS/navigators/GGEMSMeshedPhantom.hh:191 */
+void set_mesh_octree_depth_ggems_meshed_phantom(GGEMSMeshedPhantom* p, int depth);  /* include/GGEMS/navigators/GGEMSMeshedPhantom.hh:199 */
+int ggems_build_mesh(const char* stl, const float* matrix, int depth, int32_t* n_triangles, int32_t* n_nodes, float* triangles, float* nodes, int32_t* node_first, int32_t* node_triangles, float* border_min, float* border_max);  /* no counterpart in the reference: B200 build addition */
 GGEMSCTSystem* create_ggems_ct_system(const char* name);  /* include/GGEMS/navigators/GGEMSCTSystem.hh:141 */
 void set_number_of_modules_ggems_ct_system(GGEMSCTSystem* c, uint64_t mx, uint64_t my);  /* include/GGEMS/navigators/GGEMSCTSystem.hh:150 */
 void set_ct_system_type_ggems_ct_system(GGEMSCTSystem* c, const char* type);  /* include/GGEMS/navigators/GGEMSCTSystem.hh:158 */

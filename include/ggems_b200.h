@@ -122,7 +122,21 @@ typedef struct gg_solid {
   int32_t scatter_histogram;    /* index of the scatter histogram, -1: none */
   /* dosimetry */
   int32_t dose_map;             /* index into gg_scene.dose_maps, -1: none */
+  /* meshed solid: GGEMSMeshedSolidData (include/GGEMS/geometries/GGEMSMeshedSolidData.hh:40-49)
+   * with its octree (src/geometries/GGEMSOctree.cc).  Triangles are in world
+   * coordinates (the solid's rotation and translation already applied) and the
+   * OBB is the octree box with an identity matrix, as GGEMS leaves them. */
+  int32_t number_of_triangles;
+  const float* triangles;       /* [number_of_triangles][GG_TRIANGLE_FLOATS]: vertices p0, p1, p2,
+                                   bounding-sphere center, radius */
+  int32_t number_of_nodes;      /* (8^depth - 1) / 7 */
+  const float* nodes;           /* [number_of_nodes][6]: center xyz, half width xyz */
+  const int32_t* node_first;    /* [number_of_nodes + 1]: node n owns node_triangles[node_first[n] .. node_first[n+1]) */
+  const int32_t* node_triangles;/* triangle indices, per node in the order GGEMS's linked list visits them */
 } gg_solid;
+
+/* Floats per triangle in gg_solid.triangles. */
+#define GG_TRIANGLE_FLOATS 13
 
 /* Dose map: GGEMSDoseParams (include/GGEMS/navigators/GGEMSDoseParams.hh:40-49)
  * plus which optional tallies are recorded. */

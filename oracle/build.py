@@ -40,6 +40,11 @@ REF_KERNELS = [
     ("TrackThroughGGEMSVoxelizedSolid", ["DOSIMETRY", "TLE"],
      ["track_through_ggems_voxelized_solid=track_through_ggems_voxelized_solid_tle"]),
     ("TrackThroughGGEMSSolidBox", ["HISTOGRAM"], []),
+    ("ParticleSolidDistanceGGEMSMeshSolid", [], []),
+    ("ProjectToGGEMSMeshSolid", [], []),
+    ("TrackThroughGGEMSMeshSolid", [], []),
+    ("TrackThroughGGEMSMeshSolid", ["DOSIMETRY"],
+     ["track_through_ggems_meshed_solid=track_through_ggems_meshed_solid_dosimetry"]),
     ("IsAlive", [], []),
 ]
 
@@ -52,7 +57,7 @@ def build_oracle():
     os.makedirs(BUILD, exist_ok=True)
     out = os.path.join(BUILD, "libgg_oracle.so")
     run(CXX + ["-shared", "-I" + os.path.join(ROOT, "include"), os.path.join(HERE, "gg_oracle.cc"),
-               os.path.join(HERE, "gg_oracle_tables.cc"), "-o", out, "-lpthread"])
+               os.path.join(HERE, "gg_oracle_tables.cc"), os.path.join(HERE, "gg_oracle_mesh.cc"), "-o", out, "-lpthread"])
     return out
 
 

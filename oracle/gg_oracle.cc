@@ -646,6 +646,142 @@ void track_box(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& s, int
   ph.d = local_to_global_direction(m, ld);
 }
 
+// ---- meshed solid (TrackThroughGGEMSMeshSolid.cl:53-534) ----
+constexpr int kMaxMeshHits = 16;  // MAX_TRIANGLE_INTERACTION
+
+inline V3 cross3(V3 a, V3 b) { return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+
+// MollerTrumboreRayTriangle (l.121-170); tri = p0, p1, p2, ...
+bool moller_trumbore(V3 p, V3 d, const float* tri, V3* hit) {
+  V3 p0 = v3(tri[0], tri[1], tri[2]);
+  V3 e1 = v3(tri[3] - tri[0], tri[4] - tri[1], tri[5] - tri[2]);
+  V3 e2 = v3(tri[6] - tri[0], tri[7] - tri[1], tri[8] - tri[2]);
+  V3 h = cross3(d, e2);
+  float a = dot3(e1, h);
+  if (a > -kEpsilon6 && a < kEpsilon6) return false;
+  float f = 1.0f / a;
+  V3 s = sub(p, p0);
+  float u = f * dot3(s, h);
+  if (u < 0.0f || u > 1.0f) return false;
+  V3 q = cross3(s, e1);
+  float v = f * dot3(q, d);
+  if (v < 0.0f || u + v > 1.0f) return false;
+  float t = f * dot3(q, e2);
+  if (!(t > kEpsilon6)) return false;
+  *hit = v3(p.x + d.x * t, p.y + d.y * t, p.z + d.z * t);
+  return true;
+}
+
+// TestLineNode (l.182-230): slab test of the ray against a node box.
+bool line_hits_node(V3 p, V3 d, const float* node) {
+  const float pos[3] = {p.x, p.y, p.z}, dir[3] = {d.x, d.y, d.z};
+  float tmin = 0.0f, tmax = FLT_MAX;
+  for (int i = 0; i < 3; ++i) {
+    float mn = node[i] - node[3 + i], mx = node[i] + node[3 + i];
+    if (std::fabs(dir[i]) < kEpsilon6) {
+      if (pos[i] < mn || pos[i] > mx) return false;
+    } else {
+      float ood = 1.0f / dir[i];
+      float t1 = (mn - pos[i]) * ood, t2 = (mx - pos[i]) * ood;
+      if (t1 > t2) std::swap(t1, t2);
+      if (t1 > tmin) tmin = t1;
+      if (t2 < tmax) tmax = t2;
+      if (tmin > tmax) return false;
+    }
+  }
+  return true;
+}
+
+// GetMeshIOPositions (l.240-318): crossings of the ray with the mesh, nearest
+// first (insertion sort on squared distance, ties keep discovery order).  The
+// reference stops a node's triangle loop at 16 crossings and goes on to the
+// next node, writing past its 16-entry array if that node has crossings too;
+// here the search ends at 16.
+int mesh_crossings(V3 p, V3 d, const gg_solid& s, V3 out[kMaxMeshHits]) {
+  float dist2[kMaxMeshHits];
+  int n = 0;
+  for (int node = 0; node < s.number_of_nodes; ++node) {
+    const int b = s.node_first[node], e = s.node_first[node + 1];
+    if (b == e) continue;
+    if (!line_hits_node(p, d, s.nodes + 6 * node)) continue;
+    for (int k = b; k < e; ++k) {
+      V3 hit;
+      if (!moller_trumbore(p, d, s.triangles + static_cast<size_t>(s.node_triangles[k]) * GG_TRIANGLE_FLOATS, &hit))
+        continue;
+      float d2 = (hit.x - p.x) * (hit.x - p.x) + (hit.y - p.y) * (hit.y - p.y) + (hit.z - p.z) * (hit.z - p.z);
+      int at = n;
+      while (at > 0 && d2 < dist2[at - 1]) {
+        out[at] = out[at - 1];
+        dist2[at] = dist2[at - 1];
+        --at;
+      }
+      out[at] = hit;
+      dist2[at] = d2;
+      if (++n == kMaxMeshHits) return n;
+    }
+  }
+  return n;
+}
+
+// track_through_ggems_meshed_solid (l.330-534): no frame change (triangles are
+// in world coordinates), material 0, parity of the crossing count decides
+// inside / outside; on leaving, the photon is carried to the OBB boundary.
+void track_meshed(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& s, int solid_index, const Tallies& t) {
+  if (ph.solid_id != solid_index) return;
+  if (ph.status == GG_DEAD) return;
+  const gg_physics_tables& tb = sc.tables[s.navigator];
+  const int dm = s.dose_map;
+  V3 lp = ph.p, ld = ph.d;
+  V3 hits[kMaxMeshHits];
+  do {
+    ++t_counts[1];
+    const int n = mesh_crossings(lp, ld, s, hits);
+    if (n == 0) {
+      ph.psd = kOutOfWorld;
+      ph.solid_id = -1;
+      break;
+    }
+    V3 next;
+    if (n % 2 == 0) {
+      lp = hits[0];
+      next = hits[1];
+    } else {
+      next = hits[0];
+    }
+    ph.p = lp;
+    ph.d = ld;
+    next_interaction(ph, rng, tb, 0);
+    float nid = ph.nid;
+    int8_t proc = ph.next_process;
+    float dx = next.x - lp.x, dy = next.y - lp.y, dz = next.z - lp.z;
+    float to_next = std::sqrt(dx * dx + dy * dy + dz * dz);
+    if (to_next <= nid) {
+      nid = to_next + kGeometryTolerance;
+      proc = GG_TRANSPORTATION;
+      if (dm >= 0) photon_tracking_record(t, dm, lp);
+    }
+    lp = add(lp, scale(ld, nid));
+    ph.p = lp;
+    float initial_energy = ph.E;
+    if (proc != GG_TRANSPORTATION) {
+      discrete_process(ph, rng, tb, 0);
+      if (proc == GG_COMPTON_SCATTERING || proc == GG_RAYLEIGH_SCATTERING) ph.scatter = 1;
+      if (dm >= 0) dose_record(t, dm, initial_energy - ph.E, lp);
+      ld = ph.d;
+    }
+    if (ph.E <= tb.photon_energy_cut[0]) {
+      if (dm >= 0) dose_record(t, dm, ph.E, lp);
+      ph.status = GG_DEAD;
+    }
+  } while (ph.status == GG_ALIVE);
+  const float* m = s.obb.matrix;
+  float dist = distance_to_aabb(global_to_local_position(m, lp), global_to_local_direction(m, ld), obb_min(s.obb),
+                                obb_max(s.obb));
+  ph.p = v3(lp.x + ld.x * (dist + kGeometryTolerance), lp.y + ld.y * (dist + kGeometryTolerance),
+            lp.z + ld.z * (dist + kGeometryTolerance));
+  ph.d = ld;
+}
+
 // One history, following GGEMS::RunOnDevice's inner loop (src/global/GGEMS.cc:326-345):
 // FindSolid, ProjectToSolid, TrackThroughSolid over all solids in order,
 // until the particle is dead or GG_MAX_LOOP iterations were made.
@@ -657,6 +793,7 @@ void transport(Photon& ph, Kiss& rng, const gg_scene& sc, const Tallies& t) {
       const gg_solid& solid = sc.solids[s];
       if (solid.type == GG_SOLID_VOXELIZED) track_voxelized(ph, rng, sc, solid, s, t);
       else if (solid.type == GG_SOLID_BOX) track_box(ph, rng, sc, solid, s, t);
+      else if (solid.type == GG_SOLID_MESHED) track_meshed(ph, rng, sc, solid, s, t);
     }
     if (ph.status == GG_DEAD) break;
   }

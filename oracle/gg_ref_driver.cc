@@ -17,6 +17,7 @@
 #include <thread>
 #include <vector>
 
+#include "GGEMS/geometries/GGEMSMeshedSolidData.hh"
 #include "GGEMS/geometries/GGEMSSolidBoxData.hh"
 #include "GGEMS/geometries/GGEMSVoxelizedSolidData.hh"
 #include "GGEMS/materials/GGEMSMaterialTables.hh"
@@ -54,6 +55,16 @@ void track_through_ggems_voxelized_solid_tle(ulong, GGEMSPrimaryParticles*, GGEM
 void track_through_ggems_solid_box(ulong, GGEMSPrimaryParticles*, GGEMSRandom*, const GGEMSSolidBoxData*, const uchar*,
                                    const GGEMSParticleCrossSections*, const GGEMSMaterialTables*, const GGEMSMuMuEnData*,
                                    float, int*, int*);
+void particle_solid_distance_ggems_meshed_solid(ulong, GGEMSPrimaryParticles*, const GGEMSMeshedSolidData*);
+void project_to_ggems_meshed_solid(ulong, GGEMSPrimaryParticles*, const GGEMSMeshedSolidData*);
+void track_through_ggems_meshed_solid(ulong, GGEMSPrimaryParticles*, GGEMSRandom*, const GGEMSMeshedSolidData*,
+                                      const uchar*, const GGEMSParticleCrossSections*, const GGEMSMaterialTables*,
+                                      const GGEMSMuMuEnData*, float);
+void track_through_ggems_meshed_solid_dosimetry(ulong, GGEMSPrimaryParticles*, GGEMSRandom*,
+                                                const GGEMSMeshedSolidData*, const uchar*,
+                                                const GGEMSParticleCrossSections*, const GGEMSMaterialTables*,
+                                                const GGEMSMuMuEnData*, float, GGEMSDoseParams*, double*, double*,
+                                                int*, int*);
 void is_alive(ulong, GGEMSPrimaryParticles*, int*);
 }
 
@@ -180,6 +191,52 @@ extern "C" __attribute__((visibility("default"))) int gg_ref_run(const gg_scene*
   const int ns = scene->number_of_solids;
   std::vector<GGEMSVoxelizedSolidData> vox(ns);
   std::vector<GGEMSSolidBoxData> box(ns);
+  std::vector<GGEMSMeshedSolidData> mesh(ns);
+  // Meshed solids: GGEMSNode array with triangle linked lists rebuilt from the
+  // per-node index lists (same visiting order).
+  std::vector<std::vector<GGEMSTriangle3>> mesh_triangles(ns);
+  std::vector<std::vector<GGEMSNode>> mesh_nodes(ns);
+  for (int s = 0; s < ns; ++s) {
+    const gg_solid& g = scene->solids[s];
+    if (g.type != GG_SOLID_MESHED) continue;
+    std::vector<GGEMSTriangle3>& tri = mesh_triangles[s];
+    tri.resize(g.number_of_triangles);
+    for (int t = 0; t < g.number_of_triangles; ++t) {
+      const float* f = g.triangles + static_cast<size_t>(t) * GG_TRIANGLE_FLOATS;
+      for (int k = 0; k < 3; ++k) {
+        tri[t].pts_[k].x_ = f[3 * k];
+        tri[t].pts_[k].y_ = f[3 * k + 1];
+        tri[t].pts_[k].z_ = f[3 * k + 2];
+      }
+      tri[t].bounding_sphere_.center_.x_ = f[9];
+      tri[t].bounding_sphere_.center_.y_ = f[10];
+      tri[t].bounding_sphere_.center_.z_ = f[11];
+      tri[t].bounding_sphere_.radius_ = f[12];
+      tri[t].next_triangle_ = nullptr;
+    }
+    std::vector<GGEMSNode>& nodes = mesh_nodes[s];
+    nodes.resize(g.number_of_nodes);
+    for (int n = 0; n < g.number_of_nodes; ++n) {
+      GGEMSNode& nd = nodes[n];
+      std::memset(&nd, 0, sizeof(nd));
+      nd.center_.x_ = g.nodes[6 * n];
+      nd.center_.y_ = g.nodes[6 * n + 1];
+      nd.center_.z_ = g.nodes[6 * n + 2];
+      for (int k = 0; k < 3; ++k) nd.half_width_[k] = g.nodes[6 * n + 3 + k];
+      nd.triangle_list_ = nullptr;
+      GGEMSTriangle3* prev = nullptr;
+      for (int k = g.node_first[n]; k < g.node_first[n + 1]; ++k) {
+        GGEMSTriangle3* t = &tri[g.node_triangles[k]];
+        if (prev) prev->next_triangle_ = t;
+        else nd.triangle_list_ = t;
+        prev = t;
+      }
+    }
+    set_obb(mesh[s].obb_geometry_, g.obb);
+    mesh[s].solid_id_ = s;
+    mesh[s].nodes_ = nodes.data();
+    mesh[s].total_nodes_ = g.number_of_nodes;
+  }
   for (int s = 0; s < ns; ++s) {
     const gg_solid& g = scene->solids[s];
     if (g.type == GG_SOLID_VOXELIZED) {
@@ -254,12 +311,16 @@ extern "C" __attribute__((visibility("default"))) int gg_ref_run(const gg_scene*
       for (int s = 0; s < ns; ++s) {
         if (scene->solids[s].type == GG_SOLID_VOXELIZED)
           parallel_for(n, threads, [&]() { particle_solid_distance_ggems_voxelized_solid(n, P, &vox[s]); });
+        else if (scene->solids[s].type == GG_SOLID_MESHED)
+          parallel_for(n, threads, [&]() { particle_solid_distance_ggems_meshed_solid(n, P, &mesh[s]); });
         else
           parallel_for(n, threads, [&]() { particle_solid_distance_ggems_solid_box(n, P, &box[s]); });
       }
       for (int s = 0; s < ns; ++s) {
         if (scene->solids[s].type == GG_SOLID_VOXELIZED)
           parallel_for(n, threads, [&]() { project_to_ggems_voxelized_solid(n, P, &vox[s]); });
+        else if (scene->solids[s].type == GG_SOLID_MESHED)
+          parallel_for(n, threads, [&]() { project_to_ggems_meshed_solid(n, P, &mesh[s]); });
         else
           parallel_for(n, threads, [&]() { project_to_ggems_solid_box(n, P, &box[s]); });
       }
@@ -289,6 +350,22 @@ extern "C" __attribute__((visibility("default"))) int gg_ref_run(const gg_scene*
           } else {
             parallel_for(n, threads, [&]() {
               track_through_ggems_voxelized_solid(n, P, R, &vox[s], g.labels, C, M, att.get(), g.threshold);
+            });
+          }
+        } else if (g.type == GG_SOLID_MESHED) {
+          if (g.dose_map >= 0) {
+            const int d = g.dose_map;
+            double* edep = tallies && tallies->edep ? tallies->edep[d] : nullptr;
+            double* edep2 = tallies && tallies->edep_squared ? tallies->edep_squared[d] : nullptr;
+            int* hit = tallies && tallies->hit ? tallies->hit[d] : nullptr;
+            int* ptrack = tallies && tallies->photon_tracking ? tallies->photon_tracking[d] : nullptr;
+            parallel_for(n, threads, [&]() {
+              track_through_ggems_meshed_solid_dosimetry(n, P, R, &mesh[s], nullptr, C, M, att.get(), g.threshold,
+                                                         &dose[d], edep, edep2, hit, ptrack);
+            });
+          } else {
+            parallel_for(n, threads, [&]() {
+              track_through_ggems_meshed_solid(n, P, R, &mesh[s], nullptr, C, M, att.get(), g.threshold);
             });
           }
         } else {

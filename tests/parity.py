@@ -49,11 +49,12 @@ def history_agreement(Pa, Pb, pos_tol=1e-3, e_rel=1e-5):
 
 
 def oracle_dose(sc, T, dose_map, solid, scale=1.0, water=False, min_density=0.0):
-    """ComputeDoseGGEMSVoxelizedSolid.cl:53-121 restated in numpy (double math, float stores)."""
+    """ComputeDoseGGEMSVoxelizedSolid.cl:53-121 (and the meshed variant,
+    ComputeDoseGGEMSMeshSolid.cl:53-114: material 0, no labels) restated in
+    numpy (double math, float stores)."""
     dm = sc.dose_maps[dose_map]
     s = sc.solids[solid]
     t = sc.tables[s.navigator]
-    labels = sc._keep[solid] if False else None
     n = dm.total_number_of_dosels
     ids = np.arange(n)
     nx, ny = dm.number_of_dosels[0], dm.number_of_dosels[1]
@@ -66,10 +67,13 @@ def oracle_dose(sc, T, dose_map, solid, scale=1.0, water=False, min_density=0.0)
     pos = [F(c.astype(np.float32) * sz[i]) + F(F(nd[i] - 1) * F(F(-0.5) * sz[i])) for i, c in enumerate((x, y, z))]
     pos = [(c.astype(np.float32) * sz[i]).astype(np.float32) + np.float32(F(nd[i] - 1) * F(F(-0.5) * sz[i]))
            for i, c in enumerate((x, y, z))]
-    vid = [np.trunc(((pos[i] - F(s.obb.border_min[i])).astype(np.float32) / F(s.voxel_sizes[i])).astype(np.float32))
-           .astype(np.int64) for i in range(3)]
-    lab = np.ctypeslib.as_array(s.labels, shape=(s.number_of_voxels[0] * s.number_of_voxels[1] * s.number_of_voxels[2],))
-    mat = lab[vid[0] + vid[1] * s.number_of_voxels[0] + vid[2] * s.number_of_voxels[0] * s.number_of_voxels[1]]
+    if s.type == abi.GG_SOLID_MESHED:
+        mat = np.zeros(n, np.int64)
+    else:
+        vid = [np.trunc(((pos[i] - F(s.obb.border_min[i])).astype(np.float32) / F(s.voxel_sizes[i])).astype(np.float32))
+               .astype(np.int64) for i in range(3)]
+        lab = np.ctypeslib.as_array(s.labels, shape=(s.number_of_voxels[0] * s.number_of_voxels[1] * s.number_of_voxels[2],))
+        mat = lab[vid[0] + vid[1] * s.number_of_voxels[0] + vid[2] * s.number_of_voxels[0] * s.number_of_voxels[1]]
     vol = F(F(sz[0] * sz[1]) * sz[2])
     g_cm3 = F(F(6.241509704e+21) / F(1.e3))
     density = np.full(n, F(F(1.0) * g_cm3), np.float32) if water else t.density[mat]

@@ -189,6 +189,7 @@ class Scene:
         self.solids = []
         self.dose_maps = []
         self.histogram_sizes = []
+        self.meshes = []
         self._keep = []
 
     def add_tables(self, tables):
@@ -238,6 +239,49 @@ class Scene:
         d.tle = 1 if dose.get("tle") else 0
         self.dose_maps.append(d)
         return len(self.dose_maps) - 1
+
+    def add_meshed(self, stl_path, navigator, ops=(), depth=4, dose=None):
+        """GGEMSMeshedPhantom: STL triangles moved by the solid's transformation (axis
+        identity, calls in `ops` order), octree of `depth` levels (oracle restatement of
+        GGEMSMeshedSolid / GGEMSOctree).  dose: dict with "dosel_size" (required) or None."""
+        lib = oracle()
+        nt, nn = C.c_int32(), C.c_int32()
+        assert lib.gg_oracle_mesh_counts(stl_path.encode(), depth, C.byref(nt), C.byref(nn)) == 0
+        m = geometry_matrix(PHANTOM_AXIS, ops)
+        tri = np.zeros(nt.value * abi.GG_TRIANGLE_FLOATS, np.float32)
+        nodes = np.zeros(nn.value * 6, np.float32)
+        first = np.zeros(nn.value + 1, np.int32)
+        order = np.zeros(max(nt.value, 1), np.int32)
+        bmin, bmax = np.zeros(3, np.float32), np.zeros(3, np.float32)
+        mat = np.ascontiguousarray(m.reshape(-1), np.float32)
+        rc = lib.gg_oracle_build_mesh(stl_path.encode(), abi.ptr(mat, C.c_float), depth, abi.ptr(tri, C.c_float),
+                                      abi.ptr(nodes, C.c_float), abi.ptr(first, C.c_int32), abi.ptr(order, C.c_int32),
+                                      abi.ptr(bmin, C.c_float), abi.ptr(bmax, C.c_float))
+        assert rc == 0, "gg_oracle_build_mesh failed"
+        self._keep += [tri, nodes, first, order]
+        s = abi.gg_solid()
+        s.type = abi.GG_SOLID_MESHED
+        s.navigator = navigator
+        o = abi.gg_obb()
+        o.matrix[:] = [float(x) for x in np.eye(4, dtype=np.float32).reshape(-1)]
+        o.border_min[:] = [float(x) for x in bmin]
+        o.border_max[:] = [float(x) for x in bmax]
+        s.obb = o
+        s.threshold = 0.0
+        s.histogram = -1
+        s.scatter_histogram = -1
+        s.dose_map = -1
+        s.number_of_triangles = nt.value
+        s.triangles = abi.ptr(tri, C.c_float)
+        s.number_of_nodes = nn.value
+        s.nodes = abi.ptr(nodes, C.c_float)
+        s.node_first = abi.ptr(first, C.c_int32)
+        s.node_triangles = abi.ptr(order, C.c_int32)
+        self.meshes.append(dict(triangles=tri, nodes=nodes, first=first, order=order, bmin=bmin, bmax=bmax))
+        if dose is not None:
+            s.dose_map = self._add_dose(s, dose)
+        self.solids.append(s)
+        return len(self.solids) - 1
 
     def add_flat_detector(self, navigator, elements, element_size, sdd, sid, threshold, scatter=True,
                           extra_rotation=None):
@@ -360,6 +404,16 @@ def ellipsoid_phantom(n, voxel, seed=1, n_bones=None):
     """C2 generator: air / water ellipsoid / bone ellipsoids, labels (nz, ny, nx)."""
     from ggems_b200 import workloads
     return workloads.cbct_labels(n, voxel, seed, n_bones)
+
+
+def mesh_phantom_scene(path, subdivisions=2, n_inner=2, depth=3, dose=False, ops=(), seed=1, material="Water"):
+    """C4-style meshed phantom (body ellipsoid + inner cavities) written to `path` as STL."""
+    from ggems_b200 import workloads
+    workloads.write_stl(path, workloads.body_mesh(subdivisions, max(subdivisions - 1, 0), n_inner, seed))
+    sc = Scene()
+    t = sc.add_tables(Tables([material]))
+    sc.add_meshed(path, t, ops=ops, depth=depth, dose={"dosel_size": (10.0, 10.0, 10.0)} if dose else None)
+    return sc
 
 
 def synthetic_spectrum():

@@ -139,3 +139,22 @@ def test_pin_tle_dosimetry_heterogeneous():
     src = scenes.XRaySource(spectrum=scenes.synthetic_spectrum(), aperture_deg=11.0)
     n = 30000
     _assert_identical(parity.run_oracle(sc, src, n), _run_ref(sc, src, n))
+
+
+def test_pin_meshed_phantom(tmp_path):
+    """GGEMSMeshedPhantom: octree node scan, Moller-Trumbore crossings, parity navigation."""
+    sc = scenes.mesh_phantom_scene(str(tmp_path / "body.stl"), subdivisions=2, n_inner=2, depth=3)
+    src = scenes.XRaySource(monoenergy=scenes.F(80.0) * scenes.KEV, aperture_deg=8.0)
+    n = 20000
+    _assert_identical(parity.run_oracle(sc, src, n), _run_ref(sc, src, n))
+
+
+def test_pin_meshed_phantom_dosimetry_rotated(tmp_path):
+    """Rotated / translated mesh with a dose map (DOSIMETRY variant of the mesh kernel)."""
+    deg = scenes.DEG
+    sc = scenes.mesh_phantom_scene(str(tmp_path / "body.stl"), subdivisions=2, n_inner=3, depth=4, dose=True,
+                                   ops=[("rotation", (float(90 * deg), float(30 * deg), 0.0)),
+                                        ("translation", (10.0, -5.0, 0.0))])
+    src = scenes.XRaySource(spectrum=scenes.synthetic_spectrum(), aperture_deg=8.0)
+    n = 20000
+    _assert_identical(parity.run_oracle(sc, src, n), _run_ref(sc, src, n))
