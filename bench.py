@@ -214,7 +214,7 @@ def _sample_size(scene_ptr, source, threads, kind, budget_s):
     pilot = 20000
     dt, _ = cpu_reference_run(scene_ptr, source, pilot, threads, kind)
     n = int(pilot * budget_s / max(dt, 1e-3))
-    return max(pilot, min(n, 1048576))
+    return max(pilot, min(n, 32 * 1048576))
 
 
 def main():
@@ -249,7 +249,7 @@ def main():
     os.environ.setdefault("CUDA_VISIBLE_DEVICES", os.environ.get("CUDA_VISIBLE_DEVICES", ""))
 
     gg = _configure(files, args.primaries)
-    from ggems_b200 import abi
+    from ggems_b200 import abi, distributed
     from ggems_b200.api import lib
     if world > 1:
         gg.GGEMSOpenCLManager().set_device_index(local)
@@ -329,6 +329,8 @@ def main():
         check(lib.gg_set_random_states(ctx, abi.ptr(states, C.c_uint32), abi.GG_MAXIMUM_PARTICLES), "random states")
         step()
         check(lib.gg_read_tallies(ctx, C.byref(tallies.struct)), "gg_read_tallies")
+        if world > 1:  # the run's one exchange: sum the detector tallies over ranks
+            distributed.reduce_tallies(tallies)
         t1 = time.perf_counter()
         if k > 0:  # first pass warms the host allocations
             e2e_times.append(t1 - t0)
@@ -345,10 +347,14 @@ def main():
             dist.destroy_process_group()
         return 0
 
+    nb = C.c_int64()
+    lib.gg_batch_plan(args.primaries, None, 0, C.byref(nb))
+    batches = int(nb.value)
+
     # ---- CPU baseline and roofline (rank 0, N = 1 only) ----
     cpu_baseline, counts = None, None
     kind = _cpu_kind()
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:
         threads = os.cpu_count() or 1
         n = _sample_size(scene_ptr, src, threads, kind, 15.0)
         dt, _ = cpu_reference_run(scene_ptr, src, n, threads, kind)
@@ -374,8 +380,8 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom generator, synthetic 120 kVp spectrum)",
         "config": {"workload": WORKLOAD, "phantom": "256x256x256 uint8, 1 mm, air/water/bone(1.85)",
-                   "primaries_per_step": args.primaries, "batches_per_step": 96, "detector": "flat 512x512 GOS, 0.8 mm, SDD 1500 / SID 1000",
-                   "processes": "Compton, photoelectric, Rayleigh", "parallelism": "replicas" if world > 1 else "single GPU",
+                   "primaries_per_step": args.primaries, "batches_per_step": batches, "detector": "flat 512x512 GOS, 0.8 mm, SDD 1500 / SID 1000",
+                   "processes": "Compton, photoelectric, Rayleigh", "parallelism": ("%d ranks, independent histories, one tally all-reduce per run" % world) if world > 1 else "single GPU",
                    "l2": "256 MB buffer written between timed steps (inputs 17 MB < L2)"},
         "e2e": {"value": e2e_value, "unit": "primaries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
