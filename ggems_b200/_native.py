@@ -39,6 +39,13 @@ def _load():
         "gg_compute_dose": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_float, C.c_int32, C.c_float,
                                       P(C.c_float), P(C.c_float)]),
         "gg_last_run_stats": (C.c_int, [C.c_void_p, P(C.c_float), P(C.c_int64)]),
+        "gg_run_jobs": (C.c_int, [C.c_void_p, P(abi.gg_job), C.c_int32]),
+        "gg_capture_jobs": (C.c_int, [C.c_void_p, P(abi.gg_job), C.c_int32, P(C.c_void_p)]),
+        "gg_graph_launch": (C.c_int, [C.c_void_p]),
+        "gg_graph_destroy": (C.c_int, [C.c_void_p]),
+        "gg_set_transport_tuning": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
+        "gg_get_transport_tuning": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32), P(C.c_int32)]),
+        "gg_autotune": (C.c_int, [C.c_void_p, P(abi.gg_source), C.c_uint64, P(C.c_float)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -109,6 +116,32 @@ class Context:
         check(lib.gg_last_run_stats(self.handle, C.byref(ms), C.byref(n)), "gg_last_run_stats")
         return ms.value, n.value
 
+    def run_jobs(self, jobs):
+        """jobs: sequence of (gg_source, number_of_particles, solids array or None); one launch."""
+        arr, keep = _job_array(jobs)
+        check(lib.gg_run_jobs(self.handle, arr, len(keep)), "gg_run_jobs")
+
+    def capture_jobs(self, jobs):
+        """The same batched launch as a CUDA graph (ggems_b200._native.Graph)."""
+        arr, keep = _job_array(jobs)
+        g = C.c_void_p()
+        check(lib.gg_capture_jobs(self.handle, arr, len(keep), C.byref(g)), "gg_capture_jobs")
+        return Graph(g, keep)
+
+    def set_tuning(self, blocks_per_sm=0, regroup_lanes=32, regroup_ratio4=4):
+        check(lib.gg_set_transport_tuning(self.handle, blocks_per_sm, regroup_lanes, regroup_ratio4),
+              "gg_set_transport_tuning")
+
+    def tuning(self):
+        a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib.gg_get_transport_tuning(self.handle, C.byref(a), C.byref(b), C.byref(c)), "gg_get_transport_tuning")
+        return a.value, b.value, c.value
+
+    def autotune(self, source, number_of_particles):
+        ms = C.c_float()
+        check(lib.gg_autotune(self.handle, C.byref(source), number_of_particles, C.byref(ms)), "gg_autotune")
+        return ms.value
+
     def compute_dose(self, dose_map, solid, n, scale=1.0, water_reference=False, minimum_density=0.0,
                      uncertainty=True):
         import numpy as np
@@ -117,3 +150,37 @@ class Context:
         check(lib.gg_compute_dose(self.handle, dose_map, solid, scale, 1 if water_reference else 0, minimum_density,
                                   abi.ptr(dose, C.c_float), abi.ptr(unc, C.c_float)), "gg_compute_dose")
         return dose, unc
+
+
+def _job_array(jobs):
+    keep = []
+    for source, n, solids in jobs:
+        j = abi.gg_job()
+        j.source = source
+        j.number_of_particles = n
+        j.solids = C.cast(solids, C.POINTER(abi.gg_solid)) if solids is not None else C.cast(None, C.POINTER(abi.gg_solid))
+        keep.append((j, solids))
+    arr = (abi.gg_job * len(keep))(*[k[0] for k in keep])
+    return arr, keep
+
+
+class Graph:
+    """A captured batched launch (gg_capture_jobs); launch() replays it."""
+
+    def __init__(self, handle, keep):
+        self.handle = handle
+        self._keep = keep
+
+    def launch(self):
+        check(lib.gg_graph_launch(self.handle), "gg_graph_launch")
+
+    def close(self):
+        if self.handle:
+            lib.gg_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -76,6 +76,10 @@ class gg_source(C.Structure):
                 ("activity_index", IP), ("activity_cdf", FP)]
 
 
+class gg_job(C.Structure):
+    _fields_ = [("source", gg_source), ("number_of_particles", C.c_uint64), ("solids", C.POINTER(gg_solid))]
+
+
 class gg_particle_buffers(C.Structure):
     _fields_ = [("E", FP), ("px", FP), ("py", FP), ("pz", FP), ("dx", FP), ("dy", FP), ("dz", FP),
                 ("status", C.POINTER(C.c_int8)), ("scatter", C.POINTER(C.c_int8)), ("solid_id", IP)]

@@ -119,14 +119,22 @@ struct DevParticles {
   int32_t* solid_id;
 };
 
-struct TransportParams {
+// One source run of a (possibly batched) launch.  Batch plan of
+// GGEMSSource::OrganizeParticlesInBatch: sizes are q+1 for the first r
+// batches and q for the others, nb batches; slot i takes part when i < slots.
+struct DevJob {
   DevSource source;
-  // batch plan (GGEMSSource::OrganizeParticlesInBatch): sizes are q+1 for the
-  // first r batches and q for the others; nb batches in total.
   uint64_t q;
   uint64_t r;
   uint32_t nb;
-  uint32_t number_of_slots;     // slots touched (= size of batch 0)
+  uint32_t slots;
+};
+
+struct TransportParams {
+  const DevJob* jobs;           // number_of_jobs runs, done in order by every slot
+  int32_t number_of_jobs;
+  const DevSolid* job_solids;   // [number_of_jobs][number_of_solids] when number_of_jobs > 1, else NULL
+  uint32_t number_of_slots;     // slots touched (largest first batch over the jobs)
   uint32_t* rng;                // 5 * GG_MAXIMUM_PARTICLES words
   DevParticles particles;
   const DevSolid* solids;
@@ -158,7 +166,7 @@ struct DoseParams {
 };
 
 void launch_transport(const TransportParams& p, int grid, size_t smem, void* stream, bool mesh);
-cudaError_t configure_transport(size_t smem, int* blocks_per_sm, bool mesh);
+cudaError_t configure_transport(size_t smem, int* blocks_per_sm, bool mesh, bool batch);
 cudaError_t set_rayleigh_fit(const float* pp);
 void launch_compute_dose(const DoseParams& p, void* stream);
 

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <random>
 #include <string>
@@ -53,6 +54,7 @@ struct gg_context {
   // warp scheduling of the transport kernel (GGEMS_B200_REGROUP_LANES / _RATIO4)
   int regroup_lanes = 32;
   int regroup_ratio4 = 4;
+  int blocks_per_sm = 0;  // 0: as many as fit (the autotuner may lower it)
   size_t smem_optin = 0;
   uint32_t* rng = nullptr;
   gg::DevParticles particles{};
@@ -67,6 +69,8 @@ struct gg_context {
   std::vector<int32_t*> histograms;
   std::vector<int32_t> histogram_sizes;
   std::vector<gg_solid> solid_host;       // host copy (labels pointers replaced by device pointers)
+  std::vector<gg::DevSolid> solid_dev_host;  // host copy of the uploaded device solids
+  std::vector<char> dose_tle;             // per dose map: track-length estimator
   std::vector<const float*> density_dev;  // per navigator, for dose finalisation
   unsigned char* table_blob = nullptr;
   uint32_t table_bytes = 0;
@@ -82,16 +86,21 @@ struct gg_context {
 namespace {
 
 template <class T>
-int dev_copy(gg_context* c, const T* host, size_t n, T** out) {
+int dev_copy_to(gg_context* c, std::vector<void*>& owner, const T* host, size_t n, T** out) {
   *out = nullptr;
   if (n == 0) return GG_OK;
   void* p = nullptr;
   GG_CUDA(cudaMalloc(&p, n * sizeof(T)));
-  c->scene_allocations.push_back(p);
+  owner.push_back(p);
   if (host) GG_CUDA(cudaMemcpyAsync(p, host, n * sizeof(T), cudaMemcpyHostToDevice, c->stream));
   else GG_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), c->stream));
   *out = static_cast<T*>(p);
   return GG_OK;
+}
+
+template <class T>
+int dev_copy(gg_context* c, const T* host, size_t n, T** out) {
+  return dev_copy_to(c, c->scene_allocations, host, n, out);
 }
 
 void free_scene(gg_context* c) {
@@ -105,6 +114,8 @@ void free_scene(gg_context* c) {
   c->histograms.clear();
   c->histogram_sizes.clear();
   c->solid_host.clear();
+  c->solid_dev_host.clear();
+  c->dose_tle.clear();
   c->density_dev.clear();
   c->scene_ready = false;
 }
@@ -120,7 +131,7 @@ uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
 // others), with their boxes as the reference's TestLineNode computes them,
 // and the triangles regrouped by node with their two edges precomputed
 // (the same float subtractions the Moller-Trumbore test makes).
-int upload_mesh(gg_context* c, const gg_solid& g, gg::DevSolid* d) {
+int upload_mesh(gg_context* c, const gg_solid& g, gg::DevSolid* d, std::vector<void*>& owner) {
   if (g.number_of_triangles < 1 || !g.triangles || g.number_of_nodes < 1 || !g.nodes || !g.node_first ||
       !g.node_triangles)
     return fail(GG_ERROR_INVALID_ARGUMENT, "meshed solid without triangles or octree");
@@ -155,13 +166,74 @@ int upload_mesh(gg_context* c, const gg_solid& g, gg::DevSolid* d) {
   float4* dn;
   float4* dt;
   int rc;
-  if ((rc = dev_copy(c, nodes.data(), nodes.size(), &dn)) || (rc = dev_copy(c, tris.data(), tris.size(), &dt))) return rc;
+  if ((rc = dev_copy_to(c, owner, nodes.data(), nodes.size(), &dn)) ||
+      (rc = dev_copy_to(c, owner, tris.data(), tris.size(), &dt)))
+    return rc;
   d->mesh_nodes = dn;
   d->mesh_node_count = static_cast<int32_t>(nodes.size() / 2);
   d->mesh_triangles = dt;
   return GG_OK;
 }
 
+
+// Device form of one solid; labels and mesh arrays are uploaded into `owner`
+// (once per host array when `labels_seen` is given).
+int make_dev_solid(gg_context* c, const gg_solid& g, gg::DevSolid* out, std::vector<void*>& owner,
+                   std::map<const void*, const void*>* labels_seen) {
+  gg::DevSolid& d = *out;
+  d = gg::DevSolid{};
+  int rc;
+  if (g.navigator < 0 || g.navigator >= c->number_of_navigators)
+    return fail(GG_ERROR_INVALID_ARGUMENT, "solid navigator out of range");
+  d.type = g.type;
+  d.navigator = g.navigator;
+  std::memcpy(d.matrix, g.obb.matrix, sizeof(d.matrix));
+  std::memcpy(d.border_min, g.obb.border_min, sizeof(d.border_min));
+  std::memcpy(d.border_max, g.obb.border_max, sizeof(d.border_max));
+  d.threshold = g.threshold;
+  std::memcpy(d.number_of_voxels, g.number_of_voxels, sizeof(d.number_of_voxels));
+  std::memcpy(d.voxel_sizes, g.voxel_sizes, sizeof(d.voxel_sizes));
+  // x / 2^k and x * 2^-k are the same correctly rounded value for every x,
+  // so power-of-two voxel sizes let the kernel multiply instead of divide.
+  d.voxel_pow2 = 1;
+  for (int a = 0; a < 3; ++a) {
+    int e = 0;
+    const float m = std::frexp(g.voxel_sizes[a], &e);  // v = m * 2^e, m in [0.5, 1)
+    const bool pow2 = std::isfinite(g.voxel_sizes[a]) && m == 0.5f && e > -125 && e < 127;
+    d.voxel_pow2 &= pow2 ? 1 : 0;
+    d.inv_voxel_sizes[a] = pow2 ? std::ldexp(1.0f, 1 - e) : 0.0f;
+  }
+  std::memcpy(d.virtual_element_number, g.virtual_element_number, sizeof(d.virtual_element_number));
+  std::memcpy(d.box_size, g.box_size, sizeof(d.box_size));
+  const int nh = static_cast<int>(c->histograms.size()), nd = static_cast<int>(c->dose_host.size());
+  d.histogram = (g.histogram >= 0 && g.histogram < nh) ? c->histograms[g.histogram] : nullptr;
+  d.scatter_histogram = (g.scatter_histogram >= 0 && g.scatter_histogram < nh) ? c->histograms[g.scatter_histogram] : nullptr;
+  d.dose_map = (g.dose_map >= 0 && g.dose_map < nd) ? g.dose_map : -1;
+  d.dose_tle = (d.dose_map >= 0 && g.type == GG_SOLID_VOXELIZED && c->dose_tle[d.dose_map]) ? 1 : 0;
+  d.labels = nullptr;
+  if (g.type == GG_SOLID_VOXELIZED) {
+    const size_t nv = static_cast<size_t>(g.number_of_voxels[0]) * g.number_of_voxels[1] * g.number_of_voxels[2];
+    if (!g.labels || nv == 0) return fail(GG_ERROR_INVALID_ARGUMENT, "voxelized solid without labels");
+    const void* known = nullptr;
+    if (labels_seen) {
+      auto it = labels_seen->find(g.labels);
+      if (it != labels_seen->end()) known = it->second;
+    }
+    if (known) {
+      d.labels = static_cast<const uint8_t*>(known);
+    } else {
+      uint8_t* lab;
+      if ((rc = dev_copy_to(c, owner, g.labels, nv, &lab))) return rc;
+      d.labels = lab;
+      if (labels_seen) (*labels_seen)[g.labels] = lab;
+    }
+  } else if (g.type == GG_SOLID_MESHED) {
+    if ((rc = upload_mesh(c, g, &d, owner))) return rc;
+  } else if (g.type != GG_SOLID_BOX) {
+    return fail(GG_ERROR_INVALID_ARGUMENT, "solid type not supported by this build");
+  }
+  return GG_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -396,6 +468,7 @@ GG_API int gg_upload_scene(gg_context* c, const gg_scene* sc) {
   }
   for (int d = 0; d < sc->number_of_dose_maps; ++d) {
     const gg_dose_map& g = sc->dose_maps[d];
+    c->dose_tle.push_back(g.tle ? 1 : 0);
     gg::DevDoseMap m{};
     std::memcpy(m.size_of_dosels, g.size_of_dosels, sizeof(m.size_of_dosels));
     std::memcpy(m.inv_size_of_dosels, g.inv_size_of_dosels, sizeof(m.inv_size_of_dosels));
@@ -417,50 +490,10 @@ GG_API int gg_upload_scene(gg_context* c, const gg_scene* sc) {
   std::vector<gg::DevSolid> solids(sc->number_of_solids);
   c->solid_host.assign(sc->solids, sc->solids + sc->number_of_solids);
   for (int s = 0; s < sc->number_of_solids; ++s) {
-    const gg_solid& g = sc->solids[s];
-    gg::DevSolid& d = solids[s];
-    if (g.navigator < 0 || g.navigator >= sc->number_of_tables)
-      return fail(GG_ERROR_INVALID_ARGUMENT, "solid navigator out of range");
-    d.type = g.type;
-    d.navigator = g.navigator;
-    std::memcpy(d.matrix, g.obb.matrix, sizeof(d.matrix));
-    std::memcpy(d.border_min, g.obb.border_min, sizeof(d.border_min));
-    std::memcpy(d.border_max, g.obb.border_max, sizeof(d.border_max));
-    d.threshold = g.threshold;
-    std::memcpy(d.number_of_voxels, g.number_of_voxels, sizeof(d.number_of_voxels));
-    std::memcpy(d.voxel_sizes, g.voxel_sizes, sizeof(d.voxel_sizes));
-    // x / 2^k and x * 2^-k are the same correctly rounded value for every x,
-    // so power-of-two voxel sizes let the kernel multiply instead of divide.
-    d.voxel_pow2 = 1;
-    for (int a = 0; a < 3; ++a) {
-      int e = 0;
-      const float m = std::frexp(g.voxel_sizes[a], &e);  // v = m * 2^e, m in [0.5, 1)
-      const bool pow2 = std::isfinite(g.voxel_sizes[a]) && m == 0.5f && e > -125 && e < 127;
-      d.voxel_pow2 &= pow2 ? 1 : 0;
-      d.inv_voxel_sizes[a] = pow2 ? std::ldexp(1.0f, 1 - e) : 0.0f;
-    }
-    std::memcpy(d.virtual_element_number, g.virtual_element_number, sizeof(d.virtual_element_number));
-    std::memcpy(d.box_size, g.box_size, sizeof(d.box_size));
-    d.histogram = (g.histogram >= 0 && g.histogram < sc->number_of_histograms) ? c->histograms[g.histogram] : nullptr;
-    d.scatter_histogram = (g.scatter_histogram >= 0 && g.scatter_histogram < sc->number_of_histograms)
-                              ? c->histograms[g.scatter_histogram]
-                              : nullptr;
-    d.dose_map = (g.dose_map >= 0 && g.dose_map < sc->number_of_dose_maps) ? g.dose_map : -1;
-    d.dose_tle = (d.dose_map >= 0 && g.type == GG_SOLID_VOXELIZED && sc->dose_maps[d.dose_map].tle) ? 1 : 0;
-    d.labels = nullptr;
-    if (g.type == GG_SOLID_VOXELIZED) {
-      const size_t nv = static_cast<size_t>(g.number_of_voxels[0]) * g.number_of_voxels[1] * g.number_of_voxels[2];
-      if (!g.labels || nv == 0) return fail(GG_ERROR_INVALID_ARGUMENT, "voxelized solid without labels");
-      uint8_t* lab;
-      if ((rc = dev_copy(c, g.labels, nv, &lab))) return rc;
-      d.labels = lab;
-      c->solid_host[s].labels = lab;
-    } else if (g.type == GG_SOLID_MESHED) {
-      if ((rc = upload_mesh(c, g, &d))) return rc;
-    } else if (g.type != GG_SOLID_BOX) {
-      return fail(GG_ERROR_INVALID_ARGUMENT, "solid type not supported by this build");
-    }
+    if ((rc = make_dev_solid(c, sc->solids[s], &solids[s], c->scene_allocations, nullptr))) return rc;
+    c->solid_host[s].labels = solids[s].labels;
   }
+  c->solid_dev_host = solids;
   if ((rc = dev_copy(c, solids.data(), solids.size(), &c->solids))) return rc;
   c->number_of_solids = sc->number_of_solids;
 
@@ -501,28 +534,16 @@ GG_API int gg_batch_plan(uint64_t number_of_particles, uint64_t* batch_sizes, in
   return GG_OK;
 }
 
-GG_API int gg_run_source(gg_context* c, const gg_source* src, uint64_t number_of_particles) {
-  if (!c || !src) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL context or source");
-  if (!c->scene_ready) return fail(GG_ERROR_STATE, "no scene uploaded");
-  if (number_of_particles == 0) return GG_OK;
+}  // extern "C"
+
+namespace {
+
+// Device copy of a source: spectrum / CDF (and activity) arrays go to `owner`.
+int make_dev_source(gg_context* c, const gg_source* src, gg::DevSource* out, std::vector<void*>& owner) {
   if (src->number_of_energy_bins < 1 || !src->energy_spectrum || !src->energy_cdf)
     return fail(GG_ERROR_INVALID_ARGUMENT, "source has no energy spectrum");
-  GG_CUDA(cudaSetDevice(c->device));
-  GG_CUDA(cudaStreamSynchronize(c->stream));
-  free_run(c);
-  int64_t nb64 = 0;
-  gg_batch_plan(number_of_particles, nullptr, 0, &nb64);
-  const uint64_t nb = static_cast<uint64_t>(nb64);
-  if (nb == 0 || nb > 0xffffffffull) return fail(GG_ERROR_INVALID_ARGUMENT, "bad batch plan");
-  gg::TransportParams P{};
-  P.q = nb == 1 ? number_of_particles : number_of_particles / nb;
-  P.r = nb == 1 ? 0 : number_of_particles % nb;
-  P.nb = static_cast<uint32_t>(nb);
-  const uint64_t slots = P.q + (P.r ? 1 : 0);
-  if (slots > GG_MAXIMUM_PARTICLES) return fail(GG_ERROR_INVALID_ARGUMENT, "batch larger than the slot count");
-  P.number_of_slots = static_cast<uint32_t>(slots);
-
-  gg::DevSource& s = P.source;
+  gg::DevSource& s = *out;
+  s = gg::DevSource{};
   s.type = src->type;
   std::memcpy(s.matrix, src->matrix, sizeof(s.matrix));
   s.beam_aperture = src->beam_aperture;
@@ -531,15 +552,12 @@ GG_API int gg_run_source(gg_context* c, const gg_source* src, uint64_t number_of
   s.number_of_energy_bins = src->number_of_energy_bins + 1;  // GGEMSXRaySource.cc:133
   s.is_interp = src->is_interp;
   const size_t ne = static_cast<size_t>(src->number_of_energy_bins) + 1;
-  void* p = nullptr;
-  GG_CUDA(cudaMalloc(&p, ne * 4));
-  c->run_allocations.push_back(p);
-  GG_CUDA(cudaMemcpyAsync(p, src->energy_spectrum, ne * 4, cudaMemcpyHostToDevice, c->stream));
-  s.energy_spectrum = static_cast<const float*>(p);
-  GG_CUDA(cudaMalloc(&p, ne * 4));
-  c->run_allocations.push_back(p);
-  GG_CUDA(cudaMemcpyAsync(p, src->energy_cdf, ne * 4, cudaMemcpyHostToDevice, c->stream));
-  s.energy_cdf = static_cast<const float*>(p);
+  float* f;
+  int rc;
+  if ((rc = dev_copy_to(c, owner, src->energy_spectrum, ne, &f))) return rc;
+  s.energy_spectrum = f;
+  if ((rc = dev_copy_to(c, owner, src->energy_cdf, ne, &f))) return rc;
+  s.energy_cdf = f;
   if (src->type == GG_SOURCE_VOXELIZED) {
     if (src->number_of_activity_bins < 2 || !src->activity_index || !src->activity_cdf)
       return fail(GG_ERROR_INVALID_ARGUMENT, "voxelized source without activity");
@@ -548,21 +566,82 @@ GG_API int gg_run_source(gg_context* c, const gg_source* src, uint64_t number_of
     std::memcpy(s.border_min, src->border_min, sizeof(s.border_min));
     s.number_of_activity_bins = static_cast<int32_t>(src->number_of_activity_bins);
     const size_t na = static_cast<size_t>(src->number_of_activity_bins);
-    GG_CUDA(cudaMalloc(&p, na * 4));
-    c->run_allocations.push_back(p);
-    GG_CUDA(cudaMemcpyAsync(p, src->activity_index, na * 4, cudaMemcpyHostToDevice, c->stream));
-    s.activity_index = static_cast<const int32_t*>(p);
-    GG_CUDA(cudaMalloc(&p, na * 4));
-    c->run_allocations.push_back(p);
-    GG_CUDA(cudaMemcpyAsync(p, src->activity_cdf, na * 4, cudaMemcpyHostToDevice, c->stream));
-    s.activity_cdf = static_cast<const float*>(p);
+    int32_t* idx;
+    if ((rc = dev_copy_to(c, owner, src->activity_index, na, &idx))) return rc;
+    s.activity_index = idx;
+    if ((rc = dev_copy_to(c, owner, src->activity_cdf, na, &f))) return rc;
+    s.activity_cdf = f;
   } else if (src->type != GG_SOURCE_XRAY) {
     return fail(GG_ERROR_INVALID_ARGUMENT, "unknown source type");
   }
+  return GG_OK;
+}
 
+struct JobLaunch {
+  gg::TransportParams params{};
+  int grid = 0;
+  size_t smem = 0;
+  bool mesh = false;
+  bool empty = true;
+};
+
+// Device tables of `n` jobs (see gg_run_jobs), allocated into `owner`, and the
+// launch shape.
+int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*>& owner, JobLaunch* out) {
+  if (!c || !jobs || n < 1) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL context or no job");
+  if (!c->scene_ready) return fail(GG_ERROR_STATE, "no scene uploaded");
+  std::vector<gg::DevJob> dj;
+  std::vector<gg::DevSolid> job_solids;
+  std::map<const void*, const void*> labels_seen;
+  bool mesh = false, own_solids = false;
+  for (const gg_solid& g : c->solid_host) mesh |= g.type == GG_SOLID_MESHED;
+  uint64_t max_slots = 0;
+  int rc;
+  for (int j = 0; j < n; ++j) {
+    if (jobs[j].number_of_particles == 0) continue;
+    int64_t nb64 = 0;
+    gg_batch_plan(jobs[j].number_of_particles, nullptr, 0, &nb64);
+    const uint64_t nb = static_cast<uint64_t>(nb64), np = jobs[j].number_of_particles;
+    if (nb == 0 || nb > 0xffffffffull) return fail(GG_ERROR_INVALID_ARGUMENT, "bad batch plan");
+    gg::DevJob J{};
+    J.q = nb == 1 ? np : np / nb;
+    J.r = nb == 1 ? 0 : np % nb;
+    J.nb = static_cast<uint32_t>(nb);
+    const uint64_t slots = J.q + (J.r ? 1 : 0);
+    if (slots > GG_MAXIMUM_PARTICLES) return fail(GG_ERROR_INVALID_ARGUMENT, "batch larger than the slot count");
+    J.slots = static_cast<uint32_t>(slots);
+    if (slots > max_slots) max_slots = slots;
+    if ((rc = make_dev_source(c, &jobs[j].source, &J.source, owner))) return rc;
+    dj.push_back(J);
+    for (int s = 0; s < c->number_of_solids; ++s) {
+      if (jobs[j].solids) {
+        gg::DevSolid d;
+        if ((rc = make_dev_solid(c, jobs[j].solids[s], &d, owner, &labels_seen))) return rc;
+        mesh |= jobs[j].solids[s].type == GG_SOLID_MESHED;
+        own_solids = true;
+        job_solids.push_back(d);
+      } else {
+        job_solids.push_back(c->solid_dev_host[s]);
+      }
+    }
+  }
+  if (dj.empty()) return GG_OK;
+  gg::TransportParams& P = out->params;
+  P = gg::TransportParams{};
+  gg::DevJob* djd;
+  if ((rc = dev_copy_to(c, owner, dj.data(), dj.size(), &djd))) return rc;
+  P.jobs = djd;
+  P.number_of_jobs = static_cast<int32_t>(dj.size());
+  P.solids = c->solids;
+  if (dj.size() > 1 || own_solids) {
+    gg::DevSolid* js;
+    if ((rc = dev_copy_to(c, owner, job_solids.data(), job_solids.size(), &js))) return rc;
+    if (dj.size() > 1) P.job_solids = js;
+    else P.solids = js;  // a single job's own solids replace the scene's for this launch
+  }
+  P.number_of_slots = static_cast<uint32_t>(max_slots);
   P.rng = c->rng;
   P.particles = c->particles;
-  P.solids = c->solids;
   P.number_of_solids = c->number_of_solids;
   P.navigators = c->navigators;
   P.number_of_navigators = c->number_of_navigators;
@@ -574,23 +653,127 @@ GG_API int gg_run_source(gg_context* c, const gg_source* src, uint64_t number_of
   P.error = c->error;
   P.regroup_lanes = c->regroup_lanes;
   P.regroup_ratio4 = c->regroup_ratio4;
-  size_t smem = (c->tables_in_smem ? c->table_bytes : 0) + sizeof(gg::DevSolid) * c->number_of_solids +
-                sizeof(gg::DevNavigator) * c->number_of_navigators + 16;
+  out->smem = (c->tables_in_smem ? c->table_bytes : 0) + sizeof(gg::DevSolid) * c->number_of_solids +
+              sizeof(gg::DevNavigator) * c->number_of_navigators + 16;
   int blocks_per_sm = 0;
-  bool mesh = false;
-  for (const gg_solid& g : c->solid_host) mesh |= g.type == GG_SOLID_MESHED;
-  GG_CUDA(gg::configure_transport(smem, &blocks_per_sm, mesh));
+  GG_CUDA(gg::configure_transport(out->smem, &blocks_per_sm, mesh, P.number_of_jobs > 1));
   if (blocks_per_sm < 1) return fail(GG_ERROR_CUDA, "transport kernel does not fit on an SM");
+  if (c->blocks_per_sm > 0 && c->blocks_per_sm < blocks_per_sm) blocks_per_sm = c->blocks_per_sm;
   uint64_t grid = static_cast<uint64_t>(blocks_per_sm) * c->sm_count;
-  uint64_t needed = (slots + gg::kBlockThreads - 1) / gg::kBlockThreads;
+  const uint64_t needed = (max_slots + gg::kBlockThreads - 1) / gg::kBlockThreads;
   if (grid > needed) grid = needed;
+  out->grid = static_cast<int>(grid);
+  out->mesh = mesh;
+  out->empty = false;
+  return GG_OK;
+}
+
+// Work-queue reset and the persistent launch, on the context's stream.
+int enqueue_jobs(gg_context* c, const JobLaunch& L) {
   GG_CUDA(cudaMemsetAsync(c->slot_counter, 0, sizeof(unsigned int), c->stream));
   GG_CUDA(cudaMemsetAsync(c->error, 0, sizeof(int), c->stream));
-  GG_CUDA(cudaEventRecord(c->start, c->stream));
-  gg::launch_transport(P, static_cast<int>(grid), smem, c->stream, mesh);
+  gg::launch_transport(L.params, L.grid, L.smem, c->stream, L.mesh);
   GG_CUDA(cudaGetLastError());
+  return GG_OK;
+}
+
+// One persistent launch for `n` jobs (see gg_run_jobs).
+int launch_jobs(gg_context* c, const gg_job* jobs, int32_t n) {
+  if (!c) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL context");
+  GG_CUDA(cudaSetDevice(c->device));
+  GG_CUDA(cudaStreamSynchronize(c->stream));
+  free_run(c);
+  JobLaunch L;
+  int rc;
+  if ((rc = prepare_jobs(c, jobs, n, c->run_allocations, &L))) return rc;
+  if (L.empty) return GG_OK;
+  GG_CUDA(cudaEventRecord(c->start, c->stream));
+  if ((rc = enqueue_jobs(c, L))) return rc;
   GG_CUDA(cudaEventRecord(c->stop, c->stream));
   c->last_launches = 1;
+  return GG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+GG_API int gg_run_source(gg_context* c, const gg_source* src, uint64_t number_of_particles) {
+  if (!c || !src) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL context or source");
+  if (!c->scene_ready) return fail(GG_ERROR_STATE, "no scene uploaded");
+  if (number_of_particles == 0) return GG_OK;
+  gg_job job{};
+  job.source = *src;
+  job.number_of_particles = number_of_particles;
+  job.solids = nullptr;
+  return launch_jobs(c, &job, 1);
+}
+
+GG_API int gg_run_jobs(gg_context* c, const gg_job* jobs, int32_t number_of_jobs) {
+  return launch_jobs(c, jobs, number_of_jobs);
+}
+
+}  // extern "C"
+
+struct gg_graph {
+  gg_context* context = nullptr;
+  std::vector<void*> allocations;  // the jobs' device tables
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" {
+
+GG_API int gg_capture_jobs(gg_context* c, const gg_job* jobs, int32_t number_of_jobs, gg_graph** out) {
+  if (!c || !out) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  GG_CUDA(cudaSetDevice(c->device));
+  GG_CUDA(cudaStreamSynchronize(c->stream));
+  gg_graph* g = new gg_graph();
+  g->context = c;
+  auto drop = [&](int rc) {
+    gg_graph_destroy(g);
+    return rc;
+  };
+  JobLaunch L;
+  int rc = prepare_jobs(c, jobs, number_of_jobs, g->allocations, &L);
+  if (rc) return drop(rc);
+  if (L.empty) return drop(fail(GG_ERROR_INVALID_ARGUMENT, "no primaries in the jobs"));
+  cudaError_t e = cudaStreamSynchronize(c->stream);  // the tables' uploads land before capture
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return drop(fail(GG_ERROR_CUDA, std::string("begin capture: ") + cudaGetErrorString(e)));
+  rc = enqueue_jobs(c, L);
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamEndCapture(c->stream, &graph);
+  g->graph = graph;
+  if (rc) return drop(rc);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+  if (e != cudaSuccess) return drop(fail(GG_ERROR_CUDA, std::string("capture: ") + cudaGetErrorString(e)));
+  *out = g;
+  return GG_OK;
+}
+
+GG_API int gg_graph_launch(gg_graph* g) {
+  if (!g || !g->exec) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL graph");
+  gg_context* c = g->context;
+  GG_CUDA(cudaSetDevice(c->device));
+  GG_CUDA(cudaEventRecord(c->start, c->stream));
+  GG_CUDA(cudaGraphLaunch(g->exec, c->stream));
+  GG_CUDA(cudaEventRecord(c->stop, c->stream));
+  c->last_launches = 1;
+  return GG_OK;
+}
+
+GG_API int gg_graph_destroy(gg_graph* g) {
+  if (!g) return GG_OK;
+  if (g->context) {
+    cudaSetDevice(g->context->device);
+    cudaStreamSynchronize(g->context->stream);
+  }
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  for (void* p : g->allocations) cudaFree(p);
+  delete g;
   return GG_OK;
 }
 
@@ -602,6 +785,68 @@ GG_API int gg_synchronize(gg_context* c) {
   GG_CUDA(cudaMemcpy(&err, c->error, sizeof(int), cudaMemcpyDeviceToHost));
   if (err) return fail(GG_ERROR_TIMEOUT, "a bounded wait in the transport kernel timed out");
   cudaEventElapsedTime(&c->last_ms, c->start, c->stop);
+  return GG_OK;
+}
+
+GG_API int gg_set_transport_tuning(gg_context* c, int32_t blocks_per_sm, int32_t regroup_lanes, int32_t regroup_ratio4) {
+  if (!c || blocks_per_sm < 0 || regroup_lanes < 1 || regroup_lanes > 32 || regroup_ratio4 < 0 || regroup_ratio4 > 128)
+    return fail(GG_ERROR_INVALID_ARGUMENT, "bad transport tuning");
+  c->blocks_per_sm = blocks_per_sm;
+  c->regroup_lanes = regroup_lanes;
+  c->regroup_ratio4 = regroup_ratio4;
+  return GG_OK;
+}
+
+GG_API int gg_get_transport_tuning(gg_context* c, int32_t* blocks_per_sm, int32_t* regroup_lanes, int32_t* regroup_ratio4) {
+  if (!c) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL context");
+  if (blocks_per_sm) *blocks_per_sm = c->blocks_per_sm;
+  if (regroup_lanes) *regroup_lanes = c->regroup_lanes;
+  if (regroup_ratio4) *regroup_ratio4 = c->regroup_ratio4;
+  return GG_OK;
+}
+
+// Times `number_of_particles` primaries of `source` for each launch shape in a
+// small grid (resident blocks per SM x rare-phase regroup ratio), restoring the
+// random states before each trial, and keeps the fastest.
+GG_API int gg_autotune(gg_context* c, const gg_source* source, uint64_t number_of_particles, float* best_ms) {
+  if (!c || !source || number_of_particles == 0) return fail(GG_ERROR_INVALID_ARGUMENT, "bad autotune arguments");
+  if (!c->scene_ready) return fail(GG_ERROR_STATE, "no scene uploaded");
+  GG_CUDA(cudaSetDevice(c->device));
+  const size_t bytes = static_cast<size_t>(5) * GG_MAXIMUM_PARTICLES * sizeof(uint32_t);
+  void* saved = nullptr;
+  GG_CUDA(cudaMalloc(&saved, bytes));
+  auto restore = [&]() { return cudaMemcpyAsync(c->rng, saved, bytes, cudaMemcpyDeviceToDevice, c->stream); };
+  cudaError_t e = cudaMemcpyAsync(saved, c->rng, bytes, cudaMemcpyDeviceToDevice, c->stream);
+  int best[3] = {c->blocks_per_sm, c->regroup_lanes, c->regroup_ratio4};
+  float best_time = -1.0f;
+  int rc = GG_OK;
+  const int ratios[3] = {3, 4, 6};
+  for (int bps = 4; bps >= 1 && e == cudaSuccess && rc == GG_OK; --bps) {
+    for (int r : ratios) {
+      c->blocks_per_sm = bps;
+      c->regroup_lanes = 32;
+      c->regroup_ratio4 = r;
+      if ((e = restore()) != cudaSuccess) break;
+      if ((rc = gg_run_source(c, source, number_of_particles)) != GG_OK) break;
+      if ((rc = gg_synchronize(c)) != GG_OK) break;
+      if (best_time < 0.0f || c->last_ms < best_time) {
+        best_time = c->last_ms;
+        best[0] = bps;
+        best[1] = 32;
+        best[2] = r;
+      }
+    }
+  }
+  if (e == cudaSuccess) e = restore();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(saved);
+  c->blocks_per_sm = best[0];
+  c->regroup_lanes = best[1];
+  c->regroup_ratio4 = best[2];
+  if (e != cudaSuccess) return fail(GG_ERROR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+  if (rc != GG_OK) return rc;
+  if ((rc = gg_reset_tallies(c)) != GG_OK) return rc;
+  if (best_ms) *best_ms = best_time;
   return GG_OK;
 }
 

@@ -637,14 +637,15 @@ extern __shared__ __align__(16) unsigned char g_smem[];
 // kMesh: the scene has a meshed solid.  Scenes without one run the variant
 // compiled without the mesh phase, so its code and registers stay out of the
 // voxel / detector hot loop.
-template <bool kMesh>
-__global__ void __launch_bounds__(kBlockThreads, kMesh ? 2 : 4) transport_kernel(TransportParams P) {
+// kBatch: several jobs (source runs) in one launch, each with its own solids.
+template <bool kMesh, bool kBatch>
+__global__ void __launch_bounds__(kBlockThreads, kMesh ? 2 : (kBatch ? 3 : 4)) transport_kernel(TransportParams P) {
   // shared memory: [tables][solids][navigators][mbarrier]
   unsigned char* tables = g_smem;
-  DevSolid* solids = reinterpret_cast<DevSolid*>(g_smem + (P.tables_in_smem ? P.table_bytes : 0));
-  DevNavigator* navs = reinterpret_cast<DevNavigator*>(solids + P.number_of_solids);
+  DevSolid* scene_solids = reinterpret_cast<DevSolid*>(g_smem + (P.tables_in_smem ? P.table_bytes : 0));
+  DevNavigator* navs = reinterpret_cast<DevNavigator*>(scene_solids + P.number_of_solids);
   uint64_t* bar = reinterpret_cast<uint64_t*>(navs + P.number_of_navigators);
-  for (int i = threadIdx.x; i < P.number_of_solids; i += blockDim.x) solids[i] = P.solids[i];
+  for (int i = threadIdx.x; i < P.number_of_solids; i += blockDim.x) scene_solids[i] = P.solids[i];
   for (int i = threadIdx.x; i < P.number_of_navigators; i += blockDim.x) navs[i] = P.navigators[i];
   Tab tab{P.table_blob, navs};
   if (P.tables_in_smem) {
@@ -654,8 +655,12 @@ __global__ void __launch_bounds__(kBlockThreads, kMesh ? 2 : 4) transport_kernel
     __syncthreads();
   }
 
-  const double new_aperture = P.source.new_aperture;
   const size_t S = GG_MAXIMUM_PARTICLES;
+  // Solids of the lane's current job: the shared-memory copy for a single
+  // run, the job's own array (global memory) in a batched launch.
+  const DevSolid* solids = scene_solids;
+  int job = 0;
+  const int number_of_jobs = kBatch ? P.number_of_jobs : 1;
 
   Kiss rng{0, 0, 0, 0, 0};
   Photon ph{};
@@ -670,14 +675,31 @@ __global__ void __launch_bounds__(kBlockThreads, kMesh ? 2 : 4) transport_kernel
   int pending = 0;  // deferred interaction: process << 8 | material
   V3 inv_d = v3(0.0f, 0.0f, 0.0f);  // reciprocal(ph.d) while tracking inside a solid
 
-  // Grab the first slot.
+  // A slot runs its histories of job 0, then of job 1, ... (each job is one
+  // GGEMS source run; the slot's random stream carries over from run to run).
+  // Returns false when the slot takes part in no job from `from` on.
+  auto enter_job = [&](int from) -> bool {
+    for (int j = from; j < number_of_jobs; ++j) {
+      const DevJob& J = P.jobs[j];
+      const uint32_t h = slot < J.q ? J.nb : (slot < J.q + 1 && J.r > 0 ? static_cast<uint32_t>(J.r) : 0u);
+      if (h > 0) {
+        if (kBatch) {
+          job = j;
+          solids = P.job_solids + static_cast<size_t>(j) * P.number_of_solids;
+        }
+        histories_left = h;
+        ph.solid_id = -1;
+        return true;
+      }
+    }
+    return false;
+  };
+  // Grab the next slot.
   auto next_slot = [&]() -> bool {
     slot = atomicAdd(P.slot_counter, 1u);
     if (slot >= P.number_of_slots) return false;
     rng = Kiss{P.rng[slot], P.rng[S + slot], P.rng[2 * S + slot], P.rng[3 * S + slot], P.rng[4 * S + slot]};
-    histories_left = slot < P.q ? P.nb : (slot < P.q + 1 && P.r > 0 ? static_cast<uint32_t>(P.r) : 0u);
-    ph.solid_id = -1;
-    return histories_left > 0;
+    return enter_job(0);
   };
   auto finish_slot = [&]() {
     P.rng[slot] = rng.s1;
@@ -700,7 +722,7 @@ __global__ void __launch_bounds__(kBlockThreads, kMesh ? 2 : 4) transport_kernel
   };
 
   auto end_history = [&]() {
-    if (--histories_left > 0) {
+    if (--histories_left > 0 || (kBatch && enter_job(job + 1))) {
       phase = kNewHistory;
     } else {
       finish_slot();
@@ -779,8 +801,9 @@ __global__ void __launch_bounds__(kBlockThreads, kMesh ? 2 : 4) transport_kernel
         continue;
       }
       if (phase == kNewHistory) {
-        if (P.source.type == GG_SOURCE_XRAY) xray_primary(ph, rng, P.source, new_aperture);
-        else voxelized_primary(ph, rng, P.source);
+        const DevSource& source = P.jobs[job].source;
+        if (source.type == GG_SOURCE_XRAY) xray_primary(ph, rng, source, source.new_aperture);
+        else voxelized_primary(ph, rng, source);
         ph.scatter = 0;
         ph.status = GG_ALIVE;
         ph.psd = kOutOfWorld;
@@ -1040,9 +1063,17 @@ __global__ void compute_dose_kernel(DoseParams P) {
 
 }  // namespace
 
+namespace {
+using TransportKernel = void (*)(TransportParams);
+TransportKernel transport_variant(bool mesh, bool batch) {
+  if (mesh) return batch ? transport_kernel<true, true> : transport_kernel<true, false>;
+  return batch ? transport_kernel<false, true> : transport_kernel<false, false>;
+}
+}  // namespace
+
 void launch_transport(const TransportParams& p, int grid, size_t smem, void* stream, bool mesh) {
-  if (mesh) transport_kernel<true><<<grid, kBlockThreads, smem, static_cast<cudaStream_t>(stream)>>>(p);
-  else transport_kernel<false><<<grid, kBlockThreads, smem, static_cast<cudaStream_t>(stream)>>>(p);
+  const bool batch = p.number_of_jobs > 1;
+  transport_variant(mesh, batch)<<<grid, kBlockThreads, smem, static_cast<cudaStream_t>(stream)>>>(p);
 }
 
 void launch_compute_dose(const DoseParams& p, void* stream) {
@@ -1050,8 +1081,8 @@ void launch_compute_dose(const DoseParams& p, void* stream) {
   compute_dose_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(p);
 }
 
-cudaError_t configure_transport(size_t smem, int* blocks_per_sm, bool mesh) {
-  auto kernel = mesh ? transport_kernel<true> : transport_kernel<false>;
+cudaError_t configure_transport(size_t smem, int* blocks_per_sm, bool mesh, bool batch) {
+  auto kernel = transport_variant(mesh, batch);
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, kBlockThreads, smem);

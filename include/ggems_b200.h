@@ -252,6 +252,46 @@ GG_API int gg_read_particles(gg_context* context, gg_particle_buffers* particles
 GG_API int gg_run_source(gg_context* context, const gg_source* source, uint64_t number_of_particles);
 GG_API int gg_synchronize(gg_context* context);
 
+/* ---- batched runs (no counterpart in the reference: GGEMS runs sources and
+ * geometries one after another) ----
+ * A job is one source run with its own geometry: `solids` lists
+ * number_of_solids solids of the uploaded scene's layout (same navigators;
+ * their matrices, labels, meshes and histogram / dose-map indices are the
+ * job's), or NULL for the scene's.  gg_run_jobs runs all jobs in ONE launch
+ * and gives exactly what gg_run_source would give for each job in turn with
+ * the solids swapped: slot i runs its histories of job 0, then of job 1, ...,
+ * its random stream carried from job to job.  Tallies of different jobs are
+ * kept apart by giving them different histogram / dose-map indices. */
+typedef struct gg_job {
+  gg_source source;
+  uint64_t number_of_particles;
+  const gg_solid* solids;
+} gg_job;
+GG_API int gg_run_jobs(gg_context* context, const gg_job* jobs, int32_t number_of_jobs);
+
+/* The same batched launch captured once in a CUDA graph (work-queue reset +
+ * persistent kernel) and replayed by gg_graph_launch: each replay is another
+ * acquisition of the same jobs, the random streams carrying on.  The jobs'
+ * device tables live with the graph; a graph stays valid until the context's
+ * scene is uploaded again or the graph is destroyed. */
+typedef struct gg_graph gg_graph;
+GG_API int gg_capture_jobs(gg_context* context, const gg_job* jobs, int32_t number_of_jobs, gg_graph** graph);
+GG_API int gg_graph_launch(gg_graph* graph);
+GG_API int gg_graph_destroy(gg_graph* graph);
+
+/* Launch shape of the transport kernel (no counterpart in the reference):
+ * resident blocks per SM (0: as many as fit) and the warp scheduling of the
+ * rare phases (regroup_lanes 1..32, regroup_ratio4 0..128).  gg_autotune
+ * times short runs of `source` over a set of shapes, keeps the fastest and
+ * reports it; it restores the random states and zeroes the tallies
+ * afterwards, so call it before the real run. */
+GG_API int gg_set_transport_tuning(gg_context* context, int32_t blocks_per_sm, int32_t regroup_lanes,
+                                   int32_t regroup_ratio4);
+GG_API int gg_get_transport_tuning(gg_context* context, int32_t* blocks_per_sm, int32_t* regroup_lanes,
+                                   int32_t* regroup_ratio4);
+GG_API int gg_autotune(gg_context* context, const gg_source* source, uint64_t number_of_particles,
+                       float* best_milliseconds);
+
 /* Batch plan of GGEMSSource::OrganizeParticlesInBatch for one device.
  * Writes at most max_batches sizes; returns the number of batches in *count. */
 GG_API int gg_batch_plan(uint64_t number_of_particles, uint64_t* batch_sizes, int64_t max_batches, int64_t* count);
