@@ -185,3 +185,114 @@ def body_mesh(body_subdivisions=3, inner_subdivisions=2, n_inner=8, seed=1):
         c = rng.uniform(-0.45, 0.45, 3) * np.array([120.0, 100.0, 150.0])
         parts.append(ellipsoid_triangles(axes, c, subdivisions=inner_subdivisions))
     return np.concatenate(parts)
+
+
+# ---- batched workload: projection angles + phantoms of uneven size ----
+
+def _rotation_z(deg):
+    a = np.float32(np.deg2rad(deg))
+    c, s = np.float32(np.cos(a)), np.float32(np.sin(a))
+    r = np.eye(4, dtype=np.float32)
+    r[0, 0], r[0, 1], r[1, 0], r[1, 1] = c, -s, s, c
+    return r
+
+
+class BatchedWorkload:
+    """Several source runs for one launch (include/ggems_b200.h, gg_run_jobs):
+
+    * `angles` projection angles of the base scene's source, rotated about z in
+      1-degree steps around the isocentre, on the base scene's phantom;
+    * `phantoms` phantoms of edge U{96..320} voxels of 1 mm (the ellipsoid
+      generator scaled to the cube: air / water / bone 1.85), each scored in a
+      dose map of `dosel_mm` dosels, hit by the base source.
+
+    The base scene and source come from the GGEMS API (one voxelized solid with
+    a dose map).  `scene` is the gg_scene to upload (base navigators + one for
+    the phantoms, base dose map + one per phantom); `jobs` the (gg_source,
+    primaries, solids) list.
+    """
+
+    def __init__(self, lib, base_scene, base_source, materials_file, angles=360, phantoms=16,
+                 primaries=10_000_000, seed=3, dosel_mm=4.0):
+        import ctypes as C
+        from . import abi
+        self._keep = []
+        base = base_scene
+        if base.number_of_solids != 1 or base.solids[0].type != abi.GG_SOLID_VOXELIZED:
+            raise ValueError("the base scene must hold one voxelized solid")
+        tables = [base.tables[i] for i in range(base.number_of_tables)]
+        dose_maps = [base.dose_maps[i] for i in range(base.number_of_dose_maps)]
+        # navigator of the phantoms
+        names = ["Air", "Water", "Bone185"]
+        nb, nm = 220, len(names)
+        t = dict(energy_bins=np.zeros(nb, np.float32), cross_sections=np.zeros(3 * nm * nb, np.float32),
+                 rayleigh=np.zeros(101 * nb, np.float32), density=np.zeros(nm, np.float32),
+                 photon_cut=np.zeros(nm, np.float32), n_elements=np.zeros(nm, np.int32),
+                 offset=np.zeros(nm, np.int32), Z=np.zeros(nm * 32, np.uint8), atom_density=np.zeros(nm * 32, np.float32))
+        total = C.c_int32()
+        cnames = (C.c_char_p * nm)(*[m.encode() for m in names])
+        procs = (C.c_int * 3)(0, 1, 2)
+        ctype = {np.float32: C.c_float, np.int32: C.c_int32, np.uint8: C.c_uint8}
+        f = lib.ggems_build_tables
+        f.restype = C.c_int
+        rc = f(materials_file.encode(), cnames, nm, nb, C.c_float(1.0e-3), C.c_float(1.0), procs, 3, C.c_float(0.1),
+               *[abi.ptr(t[k], ctype[t[k].dtype.type]) for k in ("energy_bins", "cross_sections", "rayleigh", "density",
+                                                                 "photon_cut", "n_elements", "offset", "Z",
+                                                                 "atom_density")], C.byref(total))
+        if rc != 0:
+            raise RuntimeError("ggems_build_tables failed: %s" % lib.ggems_last_error())
+        self._keep.append(t)
+        pt = abi.gg_physics_tables(nb, nm, 3, (C.c_int32 * 3)(0, 1, 2), abi.ptr(t["energy_bins"], C.c_float),
+                                   abi.ptr(t["cross_sections"], C.c_float), abi.ptr(t["rayleigh"], C.c_float),
+                                   abi.ptr(t["density"], C.c_float), abi.ptr(t["photon_cut"], C.c_float),
+                                   abi.ptr(t["n_elements"], C.c_int32), abi.ptr(t["offset"], C.c_int32),
+                                   abi.ptr(t["Z"], C.c_uint8), abi.ptr(t["atom_density"], C.c_float), total.value)
+        phantom_nav = len(tables)
+        tables.append(pt)
+        # jobs
+        self.jobs = []
+        self.primaries = []
+        m0 = np.array(list(base_source.matrix), np.float32).reshape(4, 4)
+        for k in range(angles):
+            s = abi.gg_source()
+            C.pointer(s)[0] = base_source
+            s.matrix[:] = [float(x) for x in (_rotation_z(float(k)) @ m0).reshape(-1)]
+            self.jobs.append((s, primaries, None))
+            self.primaries.append(primaries)
+        rng = np.random.default_rng(seed)
+        self.phantom_edges = [int(x) for x in rng.integers(96, 321, phantoms)]
+        for p, n in enumerate(self.phantom_edges):
+            labels = np.ascontiguousarray(cbct_labels(n, 1.0, seed + p), np.uint8)
+            self._keep.append(labels)
+            half = np.float32(n) * np.float32(0.5)
+            sol = abi.gg_solid()
+            C.pointer(sol)[0] = base.solids[0]
+            sol.navigator = phantom_nav
+            sol.obb.matrix[:] = [float(x) for x in np.eye(4, dtype=np.float32).reshape(-1)]
+            sol.obb.border_min[:] = [-float(half)] * 3
+            sol.obb.border_max[:] = [float(half)] * 3
+            sol.number_of_voxels[:] = [n, n, n]
+            sol.voxel_sizes[:] = [1.0, 1.0, 1.0]
+            sol.labels = abi.ptr(labels, C.c_uint8)
+            d = abi.gg_dose_map()
+            nd = int(np.float32(n) / np.float32(dosel_mm))
+            d.size_of_dosels[:] = [dosel_mm] * 3
+            d.inv_size_of_dosels[:] = [float(np.float32(1.0) / np.float32(dosel_mm))] * 3
+            d.border_min[:] = [-float(half)] * 3
+            d.border_max[:] = [float(half)] * 3
+            d.number_of_dosels[:] = [nd] * 3
+            d.total_number_of_dosels = nd ** 3
+            d.slice_number_of_dosels = nd * nd
+            d.record_edep_squared = 1
+            d.record_hit = 1
+            sol.dose_map = len(dose_maps)
+            dose_maps.append(d)
+            arr = (abi.gg_solid * 1)(sol)
+            self._keep.append(arr)
+            self.jobs.append((base_source, primaries, arr))
+            self.primaries.append(primaries)
+        self._tables = (abi.gg_physics_tables * len(tables))(*tables)
+        self._dose = (abi.gg_dose_map * len(dose_maps))(*dose_maps)
+        self.scene = abi.gg_scene(len(tables), self._tables, 1, base.solids, len(dose_maps), self._dose,
+                                  base.number_of_histograms, base.histogram_sizes, base.rayleigh_fit)
+        self.total_primaries = sum(self.primaries)
