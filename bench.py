@@ -226,8 +226,10 @@ def main():
     ap.add_argument("--primaries", type=int, default=PRIMARIES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
-    ap.add_argument("--workload", default="cbct", choices=["cbct", "batched"],
-                    help="cbct: the CBCT projection (default); batched: 360 angles + 16 phantoms in one launch")
+    ap.add_argument("--workload", default="cbct", choices=["cbct", "batched", "mesh"],
+                    help="cbct: the CBCT projection (default); batched: 360 angles + 16 phantoms in one launch; "
+                         "mesh: meshed-phantom dosimetry")
+    ap.add_argument("--mesh-subdivisions", type=int, default=6, help="icosphere subdivisions of the mesh body")
     ap.add_argument("--primaries-per-job", type=int, default=10_000_000)
     args = ap.parse_args()
     rank, world, local = _rank()
@@ -244,6 +246,8 @@ def main():
         return run_reference_arm(args, files, rank, world)
     if args.workload == "batched":
         return run_batched(args, tmp, rank)
+    if args.workload == "mesh":
+        return run_mesh(args, tmp, rank)
 
     import torch
     dist = None
@@ -499,6 +503,85 @@ def run_batched(args, tmp, rank):
                        "phantom_edges": w.phantom_edges, "tuning": {"blocks_per_sm": bps.value,
                                                                     "regroup_ratio4": ratio.value},
                        "launch": "one persistent kernel per step, replayed CUDA graph",
+                       "l2": "256 MB buffer written between timed steps"},
+            "gpu_launches": launches, "clocks": clk.summary()}), flush=True)
+    return 0
+
+
+def run_mesh(args, tmp, rank):
+    """Meshed dosimetry: an STL body (ellipsoid 120/100/150 mm) with 8 inner
+    ellipsoids, one material (water), 80 keV cone, dose on 2 mm dosels, through
+    the GGEMS API (GGEMSMeshedPhantom).  One step = one run of --primaries."""
+    import torch
+    import ggems_b200 as gg
+    from ggems_b200 import abi, workloads
+    from ggems_b200.api import lib
+    stl = os.path.join(tmp, "body.stl")
+    tris = workloads.body_mesh(args.mesh_subdivisions, max(args.mesh_subdivisions - 1, 0), 8, seed=1)
+    workloads.write_stl(stl, tris)
+    gg.GGEMSVerbosity(0)
+    gg.GGEMSMaterialsDatabaseManager().set_materials(os.path.join(ROOT, "ggems_b200", "data", "materials.txt"))
+    mesh = gg.GGEMSMeshedPhantom("phantom_mesh")
+    mesh.set_phantom(stl)
+    mesh.set_rotation(0.0, 0.0, 0.0, "deg")
+    mesh.set_position(0.0, 0.0, 0.0, "mm")
+    mesh.set_mesh_octree_depth(4)
+    mesh.set_material("Water")
+    dose = gg.GGEMSDosimetryCalculator()
+    dose.attach_to_navigator("phantom_mesh")
+    dose.set_output_basename(os.path.join(tmp, "mesh_dose"))
+    dose.set_dosel_size(2.0, 2.0, 2.0, "mm")
+    dose.edep(True)
+    dose.hit(True)
+    dose.edep_squared(True)
+    pm = gg.GGEMSProcessesManager()
+    for process in ("Compton", "Photoelectric", "Rayleigh"):
+        pm.add_process(process, "gamma", "all")
+    gg.GGEMSRangeCutsManager().set_cut("gamma", 0.1, "mm", "all")
+    src = gg.GGEMSXRaySource("xray")
+    src.set_source_particle_type("gamma")
+    src.set_number_of_particles(args.primaries)
+    src.set_position(-1000.0, 0.0, 0.0, "mm")
+    src.set_rotation(0.0, 0.0, 0.0, "deg")
+    src.set_beam_aperture(8.0, "deg")
+    src.set_focal_spot_size(0.0, 0.0, 0.0, "mm")
+    src.set_monoenergy(80.0, "keV")
+    ggems = gg.GGEMS()
+    ggems.initialize(777)
+    ctx = lib.ggems_device_context(ggems.obj, 0)
+    s = abi.gg_source()
+    assert lib.ggems_source_descriptor(0, C.byref(s), None) == 0
+    sc = lib.ggems_scene(ggems.obj).contents
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def step():
+        flush.zero_()
+        torch.cuda.synchronize()
+        if lib.gg_run_source(ctx, C.byref(s), args.primaries) != 0 or lib.gg_synchronize(ctx) != 0:
+            raise RuntimeError(lib.gg_last_error().decode())
+        t, n = C.c_float(), C.c_int64()
+        lib.gg_last_run_stats(ctx, C.byref(t), C.byref(n))
+        return t.value, n.value
+
+    for _ in range(args.warmup):
+        step()
+    times, launches = [], 0
+    with ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)) as clk:
+        for _ in range(args.steps):
+            t, n = step()
+            times.append(t)
+            launches += n
+    total_ms = sum(times)
+    d = sc.dose_maps[0]
+    if rank == 0:
+        print(json.dumps({
+            "metric": "primaries/s (meshed dosimetry)", "value": args.primaries * args.steps / (total_ms * 1e-3),
+            "unit": "primaries/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (icosphere ellipsoid meshes)",
+            "config": {"workload": "mesh_%dtri_80keV" % len(tris), "triangles": len(tris),
+                       "navigation": "BVH" if len(tris) > 4096 else "octree scan",
+                       "primaries_per_step": args.primaries, "dose_grid": list(d.number_of_dosels),
                        "l2": "256 MB buffer written between timed steps"},
             "gpu_launches": launches, "clocks": clk.summary()}), flush=True)
     return 0

@@ -83,9 +83,14 @@ struct DevSolid {
   // each ({min xyz, max x}, {max y, max z, first, count} with first / count as
   // int bits), and triangles grouped by node, 3 float4 each
   // ({p0 xyz, e1 x}, {e1 yz, e2 xy}, {e2 z, -, -, -}) with e1 = p1 - p0, e2 = p2 - p0.
+  // With mesh_bvh set, mesh_nodes is instead a bounding-volume hierarchy in
+  // the same 2-float4 form: count > 0 marks a leaf owning triangles
+  // [first, first + count), count == 0 an inner node whose children are
+  // first and first + 1.
   const float4* mesh_nodes;
   int32_t mesh_node_count;
   const float4* mesh_triangles;
+  int32_t mesh_bvh;
 };
 
 struct DevSource {

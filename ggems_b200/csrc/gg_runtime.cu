@@ -5,6 +5,8 @@
 // Replaces GGEMSOpenCLManager's Allocate / GetDeviceBuffer / CleanBuffer /
 // enqueueNDRangeKernel plumbing (src/global/GGEMSOpenCLManager.cc:836-1046)
 // for the photon path.
+#include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -127,15 +129,171 @@ void free_run(gg_context* c) {
 
 uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
 
-// Meshed solid: keep the octree nodes that own triangles (GGEMS skips the
-// others), with their boxes as the reference's TestLineNode computes them,
-// and the triangles regrouped by node with their two edges precomputed
-// (the same float subtractions the Moller-Trumbore test makes).
+float4 triangle_record(const float* v, int part) {
+  const float e1[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]};
+  const float e2[3] = {v[6] - v[0], v[7] - v[1], v[8] - v[2]};
+  if (part == 0) return make_float4(v[0], v[1], v[2], e1[0]);
+  if (part == 1) return make_float4(e1[1], e1[2], e2[0], e2[1]);
+  return make_float4(e2[2], 0.0f, 0.0f, 0.0f);
+}
+
+float int_bits(int x) {
+  float f;
+  std::memcpy(&f, &x, 4);
+  return f;
+}
+
+// Bounding-volume hierarchy over the mesh triangles: binned surface-area
+// heuristic (12 bins on the widest centroid axis), leaves of at most 4
+// triangles, depth at most 48 (the device walk keeps a 64-entry stack).
+// Boxes are grown by a relative 1e-5 plus 1e-4 mm so that rounding in the
+// slab test never prunes a triangle the ray actually crosses.
+void build_bvh(const gg_solid& g, std::vector<float4>* nodes_out, std::vector<float4>* tris_out) {
+  const int n = g.number_of_triangles;
+  std::vector<float> lo(3 * n), hi(3 * n), cen(3 * n);
+  for (int t = 0; t < n; ++t) {
+    const float* v = g.triangles + static_cast<size_t>(t) * GG_TRIANGLE_FLOATS;
+    for (int a = 0; a < 3; ++a) {
+      lo[3 * t + a] = std::min(v[a], std::min(v[3 + a], v[6 + a]));
+      hi[3 * t + a] = std::max(v[a], std::max(v[3 + a], v[6 + a]));
+      cen[3 * t + a] = 0.5f * (lo[3 * t + a] + hi[3 * t + a]);
+    }
+  }
+  std::vector<int> order(n);
+  for (int t = 0; t < n; ++t) order[t] = t;
+  struct Item {
+    int node, begin, end, depth;
+  };
+  std::vector<float4>& nodes = *nodes_out;
+  nodes.assign(2, make_float4(0, 0, 0, 0));
+  std::vector<Item> work{{0, 0, n, 0}};
+  auto area = [](const float* b) {
+    const float x = b[3] - b[0], y = b[4] - b[1], z = b[5] - b[2];
+    return x < 0 ? 0.0f : 2.0f * (x * y + y * z + z * x);
+  };
+  while (!work.empty()) {
+    const Item it = work.back();
+    work.pop_back();
+    float box[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+    float cb[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int i = it.begin; i < it.end; ++i) {
+      const int t = order[i];
+      for (int a = 0; a < 3; ++a) {
+        box[a] = std::min(box[a], lo[3 * t + a]);
+        box[3 + a] = std::max(box[3 + a], hi[3 * t + a]);
+        cb[a] = std::min(cb[a], cen[3 * t + a]);
+        cb[3 + a] = std::max(cb[3 + a], cen[3 * t + a]);
+      }
+    }
+    for (int a = 0; a < 3; ++a) {
+      const float pad = 1.0e-4f + 1.0e-5f * std::max(std::fabs(box[a]), std::fabs(box[3 + a]));
+      box[a] -= pad;
+      box[3 + a] += pad;
+    }
+    const int count = it.end - it.begin;
+    int split = -1;
+    if (count > 4 && it.depth < 47) {
+      int axis = 0;
+      for (int a = 1; a < 3; ++a)
+        if (cb[3 + a] - cb[a] > cb[3 + axis] - cb[axis]) axis = a;
+      const float extent = cb[3 + axis] - cb[axis];
+      if (extent > 0.0f) {
+        constexpr int kBins = 12;
+        int bin_count[kBins] = {0};
+        float bin_box[kBins][6];
+        for (auto& b : bin_box) {
+          b[0] = b[1] = b[2] = FLT_MAX;
+          b[3] = b[4] = b[5] = -FLT_MAX;
+        }
+        auto bin_of = [&](int t) {
+          int k = static_cast<int>(kBins * (cen[3 * t + axis] - cb[axis]) / extent);
+          return k < 0 ? 0 : (k >= kBins ? kBins - 1 : k);
+        };
+        for (int i = it.begin; i < it.end; ++i) {
+          const int t = order[i], k = bin_of(t);
+          ++bin_count[k];
+          for (int a = 0; a < 3; ++a) {
+            bin_box[k][a] = std::min(bin_box[k][a], lo[3 * t + a]);
+            bin_box[k][3 + a] = std::max(bin_box[k][3 + a], hi[3 * t + a]);
+          }
+        }
+        float best = FLT_MAX;
+        int best_k = -1;
+        for (int k = 1; k < kBins; ++k) {
+          float l[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX}, r[6] = {FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX};
+          int nl = 0, nr = 0;
+          for (int j = 0; j < kBins; ++j) {
+            float* dst = j < k ? l : r;
+            (j < k ? nl : nr) += bin_count[j];
+            for (int a = 0; a < 3; ++a) {
+              dst[a] = std::min(dst[a], bin_box[j][a]);
+              dst[3 + a] = std::max(dst[3 + a], bin_box[j][3 + a]);
+            }
+          }
+          if (nl == 0 || nr == 0) continue;
+          const float cost = area(l) * nl + area(r) * nr;
+          if (cost < best) {
+            best = cost;
+            best_k = k;
+          }
+        }
+        if (best_k > 0) {
+          auto mid = std::partition(order.begin() + it.begin, order.begin() + it.end,
+                                    [&](int t) { return bin_of(t) < best_k; });
+          split = static_cast<int>(mid - order.begin());
+        }
+      }
+      if (split <= it.begin || split >= it.end) split = it.begin + count / 2;  // degenerate: median
+    }
+    if (split < 0) {
+      nodes[2 * it.node] = make_float4(box[0], box[1], box[2], box[3]);
+      nodes[2 * it.node + 1] = make_float4(box[4], box[5], int_bits(it.begin), int_bits(count));
+    } else {
+      const int left = static_cast<int>(nodes.size() / 2);
+      nodes.resize(nodes.size() + 4, make_float4(0, 0, 0, 0));
+      nodes[2 * it.node] = make_float4(box[0], box[1], box[2], box[3]);
+      nodes[2 * it.node + 1] = make_float4(box[4], box[5], int_bits(left), int_bits(0));
+      work.push_back({left, it.begin, split, it.depth + 1});
+      work.push_back({left + 1, split, it.end, it.depth + 1});
+    }
+  }
+  tris_out->clear();
+  for (int i = 0; i < n; ++i)
+    for (int part = 0; part < 3; ++part)
+      tris_out->push_back(triangle_record(g.triangles + static_cast<size_t>(order[i]) * GG_TRIANGLE_FLOATS, part));
+}
+
+// Whether meshed solids use the hierarchy: GGEMS_B200_MESH_BVH = 0 (never:
+// GGEMS's octree scan), 1 (always), unset (meshes above 4096 triangles).
+bool use_bvh(int triangles) {
+  if (const char* v = std::getenv("GGEMS_B200_MESH_BVH")) return std::atoi(v) != 0;
+  return triangles > 4096;
+}
+
+// Meshed solid.  Octree form: keep the octree nodes that own triangles (GGEMS
+// skips the others), with their boxes as the reference's TestLineNode computes
+// them, and the triangles regrouped by node with their two edges precomputed
+// (the same float subtractions the Moller-Trumbore test makes).  BVH form for
+// large meshes (build_bvh).
 int upload_mesh(gg_context* c, const gg_solid& g, gg::DevSolid* d, std::vector<void*>& owner) {
   if (g.number_of_triangles < 1 || !g.triangles || g.number_of_nodes < 1 || !g.nodes || !g.node_first ||
       !g.node_triangles)
     return fail(GG_ERROR_INVALID_ARGUMENT, "meshed solid without triangles or octree");
   std::vector<float4> nodes, tris;
+  d->mesh_bvh = use_bvh(g.number_of_triangles) ? 1 : 0;
+  if (d->mesh_bvh) {
+    build_bvh(g, &nodes, &tris);
+    float4* dn;
+    float4* dt;
+    int rc;
+    if ((rc = dev_copy_to(c, owner, nodes.data(), nodes.size(), &dn)) ||
+        (rc = dev_copy_to(c, owner, tris.data(), tris.size(), &dt)))
+      return rc;
+    d->mesh_nodes = dn;
+    d->mesh_node_count = static_cast<int32_t>(nodes.size() / 2);
+    d->mesh_triangles = dt;
+    return GG_OK;
+  }
   for (int n = 0; n < g.number_of_nodes; ++n) {
     const int b = g.node_first[n], e = g.node_first[n + 1];
     if (b < 0 || e < b || e > g.number_of_triangles) return fail(GG_ERROR_INVALID_ARGUMENT, "bad octree node list");

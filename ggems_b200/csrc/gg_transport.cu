@@ -507,72 +507,118 @@ __device__ __forceinline__ V3 cross3(V3 a, V3 b) {
 // new crossing goes after equal ones) but only reads the first two, so only
 // those two are kept here, with the same ordering rule; the search ends at 16
 // crossings (GGEMS writes past its array beyond that).
+// Moller-Trumbore test of triangle k (l.121-170) and GGEMS's crossing
+// ordering: a new crossing goes before the kept ones only when strictly
+// nearer (squared distance, l.276-303).  Returns true once 16 crossings were
+// counted.
+struct CrossingState {
+  float d0, d1;
+  bool have0, have1;
+};
+__device__ __forceinline__ bool add_crossing(V3 p, V3 d, const float4* tris, int k, MeshCrossings& out, CrossingState& c) {
+  const float4 t0 = __ldg(tris + 3 * k), t1 = __ldg(tris + 3 * k + 1), t2 = __ldg(tris + 3 * k + 2);
+  const V3 p0 = v3(t0.x, t0.y, t0.z), e1 = v3(t0.w, t1.x, t1.y), e2 = v3(t1.z, t1.w, t2.x);
+  const V3 h = cross3(d, e2);
+  const float det = dot3(e1, h);
+  if (det > -kEps6 && det < kEps6) return false;
+  const float f = 1.0f / det;
+  const V3 sv = sub(p, p0);
+  const float u = f * dot3(sv, h);
+  if (u < 0.0f || u > 1.0f) return false;
+  const V3 q = cross3(sv, e1);
+  const float v = f * dot3(q, d);
+  if (v < 0.0f || u + v > 1.0f) return false;
+  const float t = f * dot3(q, e2);
+  if (!(t > kEps6)) return false;
+  const V3 x = v3(p.x + d.x * t, p.y + d.y * t, p.z + d.z * t);
+  const float dx = x.x - p.x, dy = x.y - p.y, dz = x.z - p.z;
+  const float d2 = dx * dx + dy * dy + dz * dz;
+  if (!c.have0 || d2 < c.d0) {
+    if (c.have0) {
+      out.second = out.first;
+      c.d1 = c.d0;
+      c.have1 = true;
+    }
+    out.first = x;
+    c.d0 = d2;
+    c.have0 = true;
+  } else if (!c.have1 || d2 < c.d1) {
+    out.second = x;
+    c.d1 = d2;
+    c.have1 = true;
+  }
+  return ++out.count == kMaxMeshCrossings;
+}
+
+// Slab test of the ray [0, inf) against a box (TestLineNode, l.182-230).
+__device__ __forceinline__ bool ray_hits_box(const float pos[3], const float dir[3], const float ood[3],
+                                             const float mn[3], const float mx[3]) {
+  float tmin = 0.0f, tmax = FLT_MAX;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    if (fabsf(dir[i]) < kEps6) {
+      if (pos[i] < mn[i] || pos[i] > mx[i]) return false;
+    } else {
+      float t1 = (mn[i] - pos[i]) * ood[i], t2 = (mx[i] - pos[i]) * ood[i];
+      if (t1 > t2) {
+        float t = t2;
+        t2 = t1;
+        t1 = t;
+      }
+      if (t1 > tmin) tmin = t1;
+      if (t2 < tmax) tmax = t2;
+      if (tmin > tmax) return false;
+    }
+  }
+  return true;
+}
+
+// GetMeshIOPositions (l.249-318).  GGEMS keeps up to 16 crossings sorted by
+// squared distance but only reads the first two and the count (whose parity
+// says inside / outside), so only those are kept here, with the same ordering
+// rule; the search ends at 16 crossings (GGEMS writes past its array beyond
+// that).  Octree form: every node that owns triangles, in node order, is
+// slab-tested and its triangles intersected, exactly GGEMS's scan.  BVH form
+// (large meshes): the hierarchy is walked with a stack; each triangle test is
+// the same arithmetic, so the crossings found are the same set and only their
+// discovery order (hence exact ties) can differ from the scan's.
 __device__ __noinline__ MeshCrossings mesh_crossings(V3 p, V3 d, V3 inv, const float4* nodes, int node_count,
-                                                     const float4* tris) {
+                                                     const float4* tris, int bvh) {
   MeshCrossings out;
   out.count = 0;
   out.first = out.second = p;
-  float d0 = FLT_MAX, d1 = FLT_MAX;
-  bool have0 = false, have1 = false;
+  CrossingState c{FLT_MAX, FLT_MAX, false, false};
   const float dir[3] = {d.x, d.y, d.z}, pos[3] = {p.x, p.y, p.z}, ood[3] = {inv.x, inv.y, inv.z};
-  for (int n = 0; n < node_count; ++n) {
-    const float4 a = __ldg(nodes + 2 * n), b = __ldg(nodes + 2 * n + 1);
+  if (!bvh) {
+    for (int n = 0; n < node_count; ++n) {
+      const float4 a = __ldg(nodes + 2 * n), b = __ldg(nodes + 2 * n + 1);
+      const float mn[3] = {a.x, a.y, a.z}, mx[3] = {a.w, b.x, b.y};
+      if (!ray_hits_box(pos, dir, ood, mn, mx)) continue;
+      const int first = __float_as_int(b.z), count = __float_as_int(b.w);
+      for (int k = first; k < first + count; ++k)
+        if (add_crossing(p, d, tris, k, out, c)) return out;
+    }
+    return out;
+  }
+  constexpr int kStack = 64;
+  int stack[kStack];
+  int sp = 0, node = 0;
+  for (;;) {
+    const float4 a = __ldg(nodes + 2 * node), b = __ldg(nodes + 2 * node + 1);
     const float mn[3] = {a.x, a.y, a.z}, mx[3] = {a.w, b.x, b.y};
-    float tmin = 0.0f, tmax = FLT_MAX;
-    bool hit = true;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      if (!hit) break;
-      if (fabsf(dir[i]) < kEps6) {
-        if (pos[i] < mn[i] || pos[i] > mx[i]) hit = false;
-      } else {
-        float t1 = (mn[i] - pos[i]) * ood[i], t2 = (mx[i] - pos[i]) * ood[i];
-        if (t1 > t2) {
-          float t = t2;
-          t2 = t1;
-          t1 = t;
-        }
-        if (t1 > tmin) tmin = t1;
-        if (t2 < tmax) tmax = t2;
-        if (tmin > tmax) hit = false;
+    if (ray_hits_box(pos, dir, ood, mn, mx)) {
+      const int first = __float_as_int(b.z), count = __float_as_int(b.w);
+      if (count > 0) {
+        for (int k = first; k < first + count; ++k)
+          if (add_crossing(p, d, tris, k, out, c)) return out;
+      } else if (sp < kStack) {
+        stack[sp++] = first + 1;
+        node = first;
+        continue;
       }
     }
-    if (!hit) continue;
-    const int first = __float_as_int(b.z), count = __float_as_int(b.w);
-    for (int k = first; k < first + count; ++k) {
-      const float4 t0 = __ldg(tris + 3 * k), t1 = __ldg(tris + 3 * k + 1), t2 = __ldg(tris + 3 * k + 2);
-      const V3 p0 = v3(t0.x, t0.y, t0.z), e1 = v3(t0.w, t1.x, t1.y), e2 = v3(t1.z, t1.w, t2.x);
-      const V3 h = cross3(d, e2);
-      const float det = dot3(e1, h);
-      if (det > -kEps6 && det < kEps6) continue;
-      const float f = 1.0f / det;
-      const V3 sv = sub(p, p0);
-      const float u = f * dot3(sv, h);
-      if (u < 0.0f || u > 1.0f) continue;
-      const V3 q = cross3(sv, e1);
-      const float v = f * dot3(q, d);
-      if (v < 0.0f || u + v > 1.0f) continue;
-      const float t = f * dot3(q, e2);
-      if (!(t > kEps6)) continue;
-      const V3 x = v3(p.x + d.x * t, p.y + d.y * t, p.z + d.z * t);
-      const float dx = x.x - p.x, dy = x.y - p.y, dz = x.z - p.z;
-      const float d2 = dx * dx + dy * dy + dz * dz;
-      if (!have0 || d2 < d0) {
-        if (have0) {
-          out.second = out.first;
-          d1 = d0;
-          have1 = true;
-        }
-        out.first = x;
-        d0 = d2;
-        have0 = true;
-      } else if (!have1 || d2 < d1) {
-        out.second = x;
-        d1 = d2;
-        have1 = true;
-      }
-      if (++out.count == kMaxMeshCrossings) return out;
-    }
+    if (sp == 0) break;
+    node = stack[--sp];
   }
   return out;
 }
@@ -942,7 +988,8 @@ __global__ void __launch_bounds__(kBlockThreads, kMesh ? 2 : (kBatch ? 3 : 4)) t
       // track_through_ggems_meshed_solid, TrackThroughGGEMSMeshSolid.cl:385-518:
       // the parity of the crossing count says whether the photon is inside the
       // mesh; outside, it jumps to the first crossing.  Material 0.
-      const MeshCrossings x = mesh_crossings(ph.p, ph.d, inv_d, so.mesh_nodes, so.mesh_node_count, so.mesh_triangles);
+      const MeshCrossings x =
+          mesh_crossings(ph.p, ph.d, inv_d, so.mesh_nodes, so.mesh_node_count, so.mesh_triangles, so.mesh_bvh);
       if (x.count == 0) {
         ph.psd = kOutOfWorld;
         ph.solid_id = -1;

@@ -230,3 +230,47 @@ def test_meshed_phantom_with_detector(ctx, tmp_path):
     assert close > 0.995
     for hg, ho in zip(Tg.histograms, To.histograms):
         assert abs(int(hg.sum()) - int(ho.sum())) <= 0.005 * max(ho.sum(), 1)
+
+
+def test_meshed_phantom_bvh_matches_octree_scan(ctx, tmp_path, monkeypatch):
+    """The BVH walk (used for large meshes) finds the same crossings as GGEMS's
+    octree scan: same scene run both ways on the GPU, and against the oracle."""
+    deg = scenes.DEG
+    sc = scenes.mesh_phantom_scene(str(tmp_path / "body.stl"), subdivisions=3, n_inner=4, depth=4, dose=True,
+                                   ops=[("rotation", (float(90 * deg), float(30 * deg), 0.0)),
+                                        ("translation", (10.0, -5.0, 0.0))])
+    src = scenes.XRaySource(spectrum=scenes.synthetic_spectrum(), aperture_deg=8.0)
+    n = 200000
+    monkeypatch.setenv("GGEMS_B200_MESH_BVH", "0")
+    Ps, Ts, ss = parity.run_gpu(ctx, sc, src, n)
+    monkeypatch.setenv("GGEMS_B200_MESH_BVH", "1")
+    Pb, Tb, sb = parity.run_gpu(ctx, sc, src, n)
+    exact, close = parity.history_agreement(Pb, Ps, pos_tol=1e-2)
+    _report("mesh BVH vs octree scan (GPU)", exact, close)
+    assert exact > 0.999
+    assert (sb[:, :n] == ss[:, :n]).all(0).mean() > 0.9999
+    Po, To, so = parity.run_oracle(sc, src, n)
+    exact, close = parity.history_agreement(Pb, Po, pos_tol=1e-2)
+    _report("mesh BVH vs oracle", exact, close)
+    assert close > 0.995
+    assert abs(Tb.edep[0].sum() - To.edep[0].sum()) <= 0.005 * To.edep[0].sum()
+
+
+def test_large_mesh_bvh(ctx, tmp_path):
+    """A 20k-triangle body (automatic BVH) against the oracle's octree scan."""
+    from ggems_b200 import workloads
+    path = str(tmp_path / "large.stl")
+    workloads.write_stl(path, workloads.body_mesh(5, 3, 4, seed=9))
+    sc = scenes.Scene()
+    t = sc.add_tables(scenes.Tables(["Water"]))
+    sc.add_meshed(path, t, depth=4, dose={"dosel_size": (8.0, 8.0, 8.0)})
+    assert sc.solids[0].number_of_triangles > 4096
+    src = scenes.XRaySource(monoenergy=scenes.F(80.0) * scenes.KEV, aperture_deg=8.0)
+    n = 100000
+    Pg, Tg, sg = parity.run_gpu(ctx, sc, src, n)
+    Po, To, so = parity.run_oracle(sc, src, n)
+    exact, close = parity.history_agreement(Pg, Po, pos_tol=1e-2)
+    _report("large mesh (BVH)", exact, close)
+    assert close > 0.995
+    assert (sg[:, :n] == so[:, :n]).all(0).mean() > 0.999
+    assert abs(Tg.edep[0].sum() - To.edep[0].sum()) <= 0.005 * To.edep[0].sum()
