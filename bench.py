@@ -580,7 +580,8 @@ def run_mesh(args, tmp, rank):
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (icosphere ellipsoid meshes)",
             "config": {"workload": "mesh_%dtri_80keV" % len(tris), "triangles": len(tris),
-                       "navigation": "BVH" if len(tris) > 4096 else "octree scan",
+                       "navigation": "BVH" if (os.environ.get("GGEMS_B200_MESH_BVH", "1" if len(tris) > 4096 else "0")
+                                               != "0") else "octree scan",
                        "primaries_per_step": args.primaries, "dose_grid": list(d.number_of_dosels),
                        "l2": "256 MB buffer written between timed steps"},
             "gpu_launches": launches, "clocks": clk.summary()}), flush=True)
