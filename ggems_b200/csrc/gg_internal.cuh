@@ -175,6 +175,25 @@ cudaError_t configure_transport(size_t smem, int* blocks_per_sm, bool mesh, bool
 cudaError_t set_rayleigh_fit(const float* pp);
 void launch_compute_dose(const DoseParams& p, void* stream);
 
+// Line integrals of mu through a voxelized solid, one ray per detector element
+// (source point -> element centre), for the scatter surrogate's inputs.
+struct ProjectorParams {
+  float phantom_matrix[16];
+  float border_min[3], border_max[3];
+  int32_t number_of_voxels[3];
+  float voxel_sizes[3];
+  const uint8_t* labels;
+  const float* mu;               // per material, mm^-1
+  int32_t number_of_materials;
+  float detector_matrix[16];
+  float detector_min[3];
+  float element_size[3];
+  int32_t elements[2];
+  float source[3];               // world
+  float* out;                    // [elements[1]][elements[0]]
+};
+void launch_line_integrals(const ProjectorParams& p, void* stream);
+
 }  // namespace gg
 
 #endif

@@ -1008,6 +1008,56 @@ GG_API int gg_autotune(gg_context* c, const gg_source* source, uint64_t number_o
   return GG_OK;
 }
 
+GG_API int gg_line_integrals(gg_context* c, const gg_solid* phantom, const gg_solid* detector, const float* source_position,
+                             const float* mu, int32_t number_of_materials, float* line_integrals) {
+  if (!c || !phantom || !detector || !source_position || !mu || !line_integrals || number_of_materials < 1)
+    return fail(GG_ERROR_INVALID_ARGUMENT, "bad arguments");
+  if (phantom->type != GG_SOLID_VOXELIZED || !phantom->labels || detector->type != GG_SOLID_BOX)
+    return fail(GG_ERROR_INVALID_ARGUMENT, "need a voxelized phantom solid (with labels) and a detector box solid");
+  for (int a = 0; a < 3; ++a)
+    if (phantom->number_of_voxels[a] < 1 || !(phantom->voxel_sizes[a] > 0.0f) || detector->virtual_element_number[a] < 1)
+      return fail(GG_ERROR_INVALID_ARGUMENT, "bad phantom or detector dimensions");
+  GG_CUDA(cudaSetDevice(c->device));
+  gg::ProjectorParams P{};
+  std::memcpy(P.phantom_matrix, phantom->obb.matrix, sizeof(P.phantom_matrix));
+  std::memcpy(P.border_min, phantom->obb.border_min, sizeof(P.border_min));
+  std::memcpy(P.border_max, phantom->obb.border_max, sizeof(P.border_max));
+  std::memcpy(P.number_of_voxels, phantom->number_of_voxels, sizeof(P.number_of_voxels));
+  std::memcpy(P.voxel_sizes, phantom->voxel_sizes, sizeof(P.voxel_sizes));
+  P.number_of_materials = number_of_materials;
+  std::memcpy(P.detector_matrix, detector->obb.matrix, sizeof(P.detector_matrix));
+  std::memcpy(P.detector_min, detector->obb.border_min, sizeof(P.detector_min));
+  for (int a = 0; a < 3; ++a) P.element_size[a] = detector->box_size[a] / static_cast<float>(detector->virtual_element_number[a]);
+  P.elements[0] = detector->virtual_element_number[0];
+  P.elements[1] = detector->virtual_element_number[1];
+  std::memcpy(P.source, source_position, sizeof(P.source));
+  const size_t n = static_cast<size_t>(P.elements[0]) * P.elements[1];
+  const size_t nv = static_cast<size_t>(phantom->number_of_voxels[0]) * phantom->number_of_voxels[1] * phantom->number_of_voxels[2];
+  std::vector<void*> tmp;
+  auto cleanup = [&]() {
+    for (void* p : tmp) cudaFree(p);
+  };
+  float *dmu = nullptr, *dout = nullptr;
+  uint8_t* dlab = nullptr;
+  int rc;
+  if ((rc = dev_copy_to(c, tmp, mu, static_cast<size_t>(number_of_materials), &dmu)) ||
+      (rc = dev_copy_to(c, tmp, phantom->labels, nv, &dlab)) ||
+      (rc = dev_copy_to(c, tmp, static_cast<const float*>(nullptr), n, &dout))) {
+    cleanup();
+    return rc;
+  }
+  P.mu = dmu;
+  P.labels = dlab;
+  P.out = dout;
+  gg::launch_line_integrals(P, c->stream);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(line_integrals, dout, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cleanup();
+  if (e != cudaSuccess) return fail(GG_ERROR_CUDA, std::string("line integrals: ") + cudaGetErrorString(e));
+  return GG_OK;
+}
+
 GG_API int gg_last_run_stats(gg_context* c, float* milliseconds, int64_t* kernel_launches) {
   if (!c) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL context");
   if (milliseconds) *milliseconds = c->last_ms;

@@ -1123,6 +1123,86 @@ void launch_transport(const TransportParams& p, int grid, size_t smem, void* str
   transport_variant(mesh, batch)<<<grid, kBlockThreads, smem, static_cast<cudaStream_t>(stream)>>>(p);
 }
 
+namespace {
+
+// Siddon-style ray march (Amanatides-Woo voxel walk) from the source to the
+// centre of detector element (i, j), in the phantom's frame: sum of
+// mu[label] x chord length.  Element centres follow the detector histogram's
+// binning (element (i, j) covers [bmin + i es, bmin + (i+1) es) in x, y).
+__global__ void line_integral_kernel(ProjectorParams P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i >= P.elements[0] || j >= P.elements[1]) return;
+  const V3 local_pixel = v3(P.detector_min[0] + (static_cast<float>(i) + 0.5f) * P.element_size[0],
+                            P.detector_min[1] + (static_cast<float>(j) + 0.5f) * P.element_size[1], 0.0f);
+  const V3 pixel = l2g_pos(P.detector_matrix, local_pixel);
+  const V3 s = g2l_pos(P.phantom_matrix, v3(P.source[0], P.source[1], P.source[2]));
+  const V3 e = g2l_pos(P.phantom_matrix, pixel);
+  const float dv[3] = {e.x - s.x, e.y - s.y, e.z - s.z};
+  const float sv[3] = {s.x, s.y, s.z};
+  float t0 = 0.0f, t1 = 1.0f;
+  for (int a = 0; a < 3; ++a) {
+    if (fabsf(dv[a]) < 1e-12f) {
+      if (sv[a] < P.border_min[a] || sv[a] > P.border_max[a]) t1 = -1.0f;
+    } else {
+      float ta = (P.border_min[a] - sv[a]) / dv[a], tb = (P.border_max[a] - sv[a]) / dv[a];
+      if (ta > tb) {
+        float t = ta;
+        ta = tb;
+        tb = t;
+      }
+      t0 = fmaxf(t0, ta);
+      t1 = fminf(t1, tb);
+    }
+  }
+  float sum = 0.0f;
+  if (t1 > t0) {
+    const float length = sqrtf(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+    int idx[3], step[3];
+    float tmax[3], tdelta[3];
+    const float tm = 0.5f * (t0 + t1);
+    for (int a = 0; a < 3; ++a) {
+      // start voxel: the one containing the entry point (nudged inside)
+      const float pa = sv[a] + fminf(t0 + 1e-6f * (t1 - t0), tm) * dv[a];
+      int k = static_cast<int>(floorf((pa - P.border_min[a]) / P.voxel_sizes[a]));
+      idx[a] = min(max(k, 0), P.number_of_voxels[a] - 1);
+      if (dv[a] > 0.0f) {
+        step[a] = 1;
+        tmax[a] = (P.border_min[a] + (idx[a] + 1) * P.voxel_sizes[a] - sv[a]) / dv[a];
+        tdelta[a] = P.voxel_sizes[a] / dv[a];
+      } else if (dv[a] < 0.0f) {
+        step[a] = -1;
+        tmax[a] = (P.border_min[a] + idx[a] * P.voxel_sizes[a] - sv[a]) / dv[a];
+        tdelta[a] = -P.voxel_sizes[a] / dv[a];
+      } else {
+        step[a] = 0;
+        tmax[a] = FLT_MAX;
+        tdelta[a] = FLT_MAX;
+      }
+    }
+    float t = t0;
+    const int nx = P.number_of_voxels[0], nxy = nx * P.number_of_voxels[1];
+    for (int guard = 0; guard < 4 * (P.number_of_voxels[0] + P.number_of_voxels[1] + P.number_of_voxels[2]); ++guard) {
+      const int a = (tmax[0] < tmax[1]) ? (tmax[0] < tmax[2] ? 0 : 2) : (tmax[1] < tmax[2] ? 1 : 2);
+      const float tn = fminf(tmax[a], t1);
+      const int m = P.labels[idx[0] + idx[1] * nx + idx[2] * nxy];
+      if (m < P.number_of_materials) sum += P.mu[m] * (tn - t) * length;
+      t = tn;
+      if (t >= t1) break;
+      idx[a] += step[a];
+      if (idx[a] < 0 || idx[a] >= P.number_of_voxels[a]) break;
+      tmax[a] += tdelta[a];
+    }
+  }
+  P.out[static_cast<size_t>(j) * P.elements[0] + i] = sum;
+}
+
+}  // namespace
+
+void launch_line_integrals(const ProjectorParams& p, void* stream) {
+  dim3 grid((p.elements[0] + 127) / 128, p.elements[1]);
+  line_integral_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(p);
+}
+
 void launch_compute_dose(const DoseParams& p, void* stream) {
   int n = p.map.total_number_of_dosels;
   compute_dose_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(p);

@@ -1,0 +1,662 @@
+// Scatter surrogate: a 4-level BF16 U-Net (base 32 channels) trained and run
+// with this file's own kernels, no framework.  It maps a CBCT primary
+// projection and the phantom's line-integral map (2 channels) to the scatter
+// projection (1 channel).  No counterpart in the reference (GGEMS has no
+// learned component); see include/ggems_b200.h, "scatter surrogate".
+//
+// Layout: activations NHWC in BF16 (channels innermost), activation
+// gradients NHWC in FP32, weights [ky][kx][Cout][Cin] (3x3) with FP32 master
+// copies, BF16 compute copies and the flipped / transposed copy
+// W'[ky][kx][Cin][Cout] = W[2-ky][2-kx][Cout][Cin] that turns the data
+// gradient of a convolution into another forward convolution.
+//
+// Every 3x3 convolution is an implicit GEMM on the tensor cores
+// (mma.sync m16n8k16, BF16 inputs, FP32 accumulation): rows = pixels, columns
+// = output channels, reduction = 9 x input channels.  Weight gradients are the
+// transposed GEMM (rows = output channels, columns = input channels,
+// reduction = pixels), split over blocks with FP32 atomics.
+//
+// Network (S = image side, all 3x3 convolutions followed by ReLU):
+//   enc  16->32->32 @S | pool | 32->64->64 @S/2 | pool | 64->128->128 @S/4 | pool
+//   bottleneck 128->256->256 @S/8
+//   dec  up, concat(128): 384->128->128 @S/4 | up, concat(64): 192->64->64 @S/2 |
+//        up, concat(32): 96->32->32 @S | 1x1 32->1 (linear)
+// pool = 2x2 average, up = nearest x2.  The 2 input channels are zero-padded to 16.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "ggems_b200.h"
+
+namespace {
+
+thread_local std::string g_unet_error;
+int unet_fail(int code, const std::string& m) {
+  g_unet_error = m;
+  return code;
+}
+#define UNET_CUDA(call)                                                                                  \
+  do {                                                                                                   \
+    cudaError_t e_ = (call);                                                                             \
+    if (e_ != cudaSuccess) return unet_fail(GG_ERROR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+using bf16 = __nv_bfloat16;
+
+// ---------------------------------------------------------------- GEMM core --
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+constexpr int kTileP = 64;   // pixels per block (4 warps x 16)
+constexpr int kTileC = 32;   // output channels per block (4 n8 tiles)
+constexpr int kPad = 8;      // smem row padding (bf16 elements)
+
+struct ConvShape {
+  int batch, height, width, cin, cout;
+};
+
+// 3x3 "same" convolution.  Out mode 0: y = relu(conv + bias) stored BF16;
+// mode 1: y = conv stored FP32 (data gradients: no bias, no activation).
+template <int kMode>
+__global__ void __launch_bounds__(128) conv3x3_kernel(const bf16* __restrict__ x, const bf16* __restrict__ w,
+                                                      const float* __restrict__ bias, void* __restrict__ y,
+                                                      ConvShape s) {
+  __shared__ __align__(16) bf16 As[kTileP][16 + kPad];
+  __shared__ __align__(16) bf16 Bs[kTileC][16 + kPad];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int hw = s.height * s.width;
+  const int p0 = blockIdx.x * kTileP, co0 = blockIdx.y * kTileC;
+  // the pixel this thread loads (2 threads per pixel, 8 channels each)
+  const int lp = tid >> 1, half = tid & 1;
+  const int pix = p0 + lp;
+  const int b = pix / hw, rem = pix - b * hw, py = rem / s.width, px = rem - py * s.width;
+  float acc[4][4] = {};
+  for (int tap = 0; tap < 9; ++tap) {
+    const int ky = tap / 3, kx = tap - 3 * ky;
+    const int yy = py + ky - 1, xx = px + kx - 1;
+    const bool inside = yy >= 0 && yy < s.height && xx >= 0 && xx < s.width;
+    const bf16* src = x + (static_cast<size_t>(b) * hw + yy * s.width + xx) * s.cin;
+    const bf16* wt = w + static_cast<size_t>(tap) * s.cout * s.cin;
+    for (int c0 = 0; c0 < s.cin; c0 += 16) {
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (inside) v = *reinterpret_cast<const uint4*>(src + c0 + 8 * half);
+      *reinterpret_cast<uint4*>(&As[lp][8 * half]) = v;
+      if (tid < 64) {
+        const int co = tid >> 1;
+        *reinterpret_cast<uint4*>(&Bs[co][8 * half]) =
+            *reinterpret_cast<const uint4*>(wt + static_cast<size_t>(co0 + co) * s.cin + c0 + 8 * half);
+      }
+      __syncthreads();
+      uint32_t a[4];
+      const int r = warp * 16 + g;
+      a[0] = *reinterpret_cast<const uint32_t*>(&As[r][2 * t]);
+      a[1] = *reinterpret_cast<const uint32_t*>(&As[r + 8][2 * t]);
+      a[2] = *reinterpret_cast<const uint32_t*>(&As[r][2 * t + 8]);
+      a[3] = *reinterpret_cast<const uint32_t*>(&As[r + 8][2 * t + 8]);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        uint32_t bb[2];
+        bb[0] = *reinterpret_cast<const uint32_t*>(&Bs[8 * j + g][2 * t]);
+        bb[1] = *reinterpret_cast<const uint32_t*>(&Bs[8 * j + g][2 * t + 8]);
+        mma_bf16(acc[j], a, bb);
+      }
+      __syncthreads();
+    }
+  }
+  // epilogue: rows warp*16+g (+8), columns 8j + 2t (+1)
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int co = co0 + 8 * j + 2 * t;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const size_t row = static_cast<size_t>(p0 + warp * 16 + g + 8 * h);
+      float v0 = acc[j][2 * h], v1 = acc[j][2 * h + 1];
+      if (kMode == 0) {
+        v0 = fmaxf(v0 + bias[co], 0.0f);
+        v1 = fmaxf(v1 + bias[co + 1], 0.0f);
+        *reinterpret_cast<__nv_bfloat162*>(static_cast<bf16*>(y) + row * s.cout + co) = __floats2bfloat162_rn(v0, v1);
+      } else {
+        *reinterpret_cast<float2*>(static_cast<float*>(y) + row * s.cout + co) = make_float2(v0, v1);
+      }
+    }
+  }
+}
+
+// Weight gradient dW[tap][co][ci] += sum_p dy[p][co] * x[p shifted by tap][ci]
+// (32 output x 16 input channels per block, one tap, a range of pixels).
+constexpr int kWgradPixels = 1024;
+__global__ void __launch_bounds__(128) conv3x3_wgrad_kernel(const bf16* __restrict__ x, const bf16* __restrict__ dy,
+                                                            float* __restrict__ dw, ConvShape s) {
+  __shared__ __align__(16) bf16 As[32][16 + kPad];  // [co][pixel]
+  __shared__ __align__(16) bf16 Bs[16][16 + kPad];  // [ci][pixel]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int co0 = blockIdx.x * 32, ci0 = blockIdx.y * 16;
+  const int tap = blockIdx.z % 9, split = blockIdx.z / 9;
+  const int ky = tap / 3, kx = tap - 3 * ky;
+  const int hw = s.height * s.width, total = s.batch * hw;
+  const int pbeg = split * kWgradPixels, pend = min(total, pbeg + kWgradPixels);
+  const int mt = warp >> 1, nt = warp & 1;  // warp's m16 / n8 tile
+  float acc[4] = {0, 0, 0, 0};
+  for (int q0 = pbeg; q0 < pend; q0 += 16) {
+    // A: 16 pixels x 32 co, 4 elements per thread
+    for (int e = tid; e < 512; e += 128) {
+      const int pl = e >> 5, co = e & 31, p = q0 + pl;
+      As[co][pl] = p < pend ? dy[static_cast<size_t>(p) * s.cout + co0 + co] : __float2bfloat16(0.0f);
+    }
+    // B: 16 pixels x 16 ci of the shifted input
+    for (int e = tid; e < 256; e += 128) {
+      const int pl = e >> 4, ci = e & 15, p = q0 + pl;
+      bf16 v = __float2bfloat16(0.0f);
+      if (p < pend) {
+        const int b = p / hw, rem = p - b * hw, py = rem / s.width, px = rem - py * s.width;
+        const int yy = py + ky - 1, xx = px + kx - 1;
+        if (yy >= 0 && yy < s.height && xx >= 0 && xx < s.width)
+          v = x[(static_cast<size_t>(b) * hw + yy * s.width + xx) * s.cin + ci0 + ci];
+      }
+      Bs[ci][pl] = v;
+    }
+    __syncthreads();
+    uint32_t a[4], bb[2];
+    const int r = mt * 16 + g;
+    a[0] = *reinterpret_cast<const uint32_t*>(&As[r][2 * t]);
+    a[1] = *reinterpret_cast<const uint32_t*>(&As[r + 8][2 * t]);
+    a[2] = *reinterpret_cast<const uint32_t*>(&As[r][2 * t + 8]);
+    a[3] = *reinterpret_cast<const uint32_t*>(&As[r + 8][2 * t + 8]);
+    bb[0] = *reinterpret_cast<const uint32_t*>(&Bs[8 * nt + g][2 * t]);
+    bb[1] = *reinterpret_cast<const uint32_t*>(&Bs[8 * nt + g][2 * t + 8]);
+    mma_bf16(acc, a, bb);
+    __syncthreads();
+  }
+  float* out = dw + static_cast<size_t>(tap) * s.cout * s.cin;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int co = co0 + mt * 16 + g + 8 * h, ci = ci0 + 8 * nt + 2 * t;
+    atomicAdd(out + static_cast<size_t>(co) * s.cin + ci, acc[2 * h]);
+    atomicAdd(out + static_cast<size_t>(co) * s.cin + ci + 1, acc[2 * h + 1]);
+  }
+}
+
+// ------------------------------------------------------------ elementwise --
+__global__ void pack_input_kernel(const float* __restrict__ in, bf16* __restrict__ x, int pixels) {
+  // in: [pixels][2] FP32 -> x: [pixels][16] BF16 (channels 2..15 zero)
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= pixels) return;
+  __align__(16) bf16 v[16];
+  for (int c = 0; c < 16; ++c) v[c] = __float2bfloat16(0.0f);
+  v[0] = __float2bfloat16(in[2 * p]);
+  v[1] = __float2bfloat16(in[2 * p + 1]);
+  uint4* dst = reinterpret_cast<uint4*>(x + static_cast<size_t>(p) * 16);
+  dst[0] = *reinterpret_cast<uint4*>(v);
+  dst[1] = *reinterpret_cast<uint4*>(v + 8);
+}
+
+// 2x2 average pool, NHWC
+__global__ void pool_kernel(const bf16* __restrict__ x, bf16* __restrict__ y, int batch, int h, int w, int c) {
+  const size_t n = static_cast<size_t>(batch) * (h / 2) * (w / 2) * c;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int ch = i % c;
+    size_t r = i / c;
+    const int ox = r % (w / 2);
+    r /= (w / 2);
+    const int oy = r % (h / 2);
+    const int b = static_cast<int>(r / (h / 2));
+    const size_t base = ((static_cast<size_t>(b) * h + 2 * oy) * w + 2 * ox) * c + ch;
+    const float s = __bfloat162float(x[base]) + __bfloat162float(x[base + c]) + __bfloat162float(x[base + static_cast<size_t>(w) * c]) +
+                    __bfloat162float(x[base + static_cast<size_t>(w) * c + c]);
+    y[i] = __float2bfloat16(0.25f * s);
+  }
+}
+
+// gradient of the pool: dx (FP32, h x w) += dy / 4 (dy at h/2 x w/2)
+__global__ void pool_backward_kernel(const float* __restrict__ dy, float* __restrict__ dx, int batch, int h, int w, int c) {
+  const size_t n = static_cast<size_t>(batch) * h * w * c;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int ch = i % c;
+    size_t r = i / c;
+    const int x = r % w;
+    r /= w;
+    const int y = r % h;
+    const int b = static_cast<int>(r / h);
+    dx[i] += 0.25f * dy[((static_cast<size_t>(b) * (h / 2) + y / 2) * (w / 2) + x / 2) * c + ch];
+  }
+}
+
+// concat(up2(a) [c1 channels, h/2 x w/2], skip [c2 channels, h x w]) -> y [c1 + c2, h x w]
+__global__ void up_concat_kernel(const bf16* __restrict__ a, const bf16* __restrict__ skip, bf16* __restrict__ y, int batch,
+                                 int h, int w, int c1, int c2) {
+  const int c = c1 + c2;
+  const size_t n = static_cast<size_t>(batch) * h * w * c;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int ch = i % c;
+    const size_t p = i / c;
+    const int x = p % w;
+    const size_t r = p / w;
+    const int yy = r % h;
+    const int b = static_cast<int>(r / h);
+    y[i] = ch < c1 ? a[((static_cast<size_t>(b) * (h / 2) + yy / 2) * (w / 2) + x / 2) * c1 + ch]
+                   : skip[p * c2 + (ch - c1)];
+  }
+}
+
+// gradient of up_concat: da (h/2 x w/2, FP32) = sum of the 2x2 block; dskip = (zero ? set : add)
+__global__ void up_concat_backward_kernel(const float* __restrict__ dy, float* __restrict__ da, float* __restrict__ dskip,
+                                          int batch, int h, int w, int c1, int c2, int skip_set) {
+  const int c = c1 + c2;
+  const size_t na = static_cast<size_t>(batch) * (h / 2) * (w / 2) * c1;
+  const size_t ns = static_cast<size_t>(batch) * h * w * c2;
+  const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < na + ns; i += stride) {
+    if (i < na) {
+      const int ch = i % c1;
+      size_t r = i / c1;
+      const int ox = r % (w / 2);
+      r /= (w / 2);
+      const int oy = r % (h / 2);
+      const int b = static_cast<int>(r / (h / 2));
+      const size_t base = ((static_cast<size_t>(b) * h + 2 * oy) * w + 2 * ox) * c + ch;
+      da[i] = dy[base] + dy[base + c] + dy[base + static_cast<size_t>(w) * c] + dy[base + static_cast<size_t>(w) * c + c];
+    } else {
+      const size_t j = i - na;
+      const int ch = j % c2;
+      const size_t p = j / c2;
+      const float v = dy[p * c + c1 + ch];
+      dskip[j] = skip_set ? v : dskip[j] + v;
+    }
+  }
+}
+
+// relu gradient: dpre (BF16) = dact * (act > 0)
+__global__ void relu_backward_kernel(const float* __restrict__ dact, const bf16* __restrict__ act, bf16* __restrict__ dpre,
+                                     size_t n) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    dpre[i] = __float2bfloat16(__bfloat162float(act[i]) > 0.0f ? dact[i] : 0.0f);
+}
+
+// bias gradient: db[c] += sum_p dpre[p][c]
+__global__ void bias_grad_kernel(const bf16* __restrict__ dpre, float* __restrict__ db, int pixels, int c) {
+  const int ch = blockIdx.y * blockDim.x + threadIdx.x;
+  if (ch >= c) return;
+  float s = 0.0f;
+  for (int p = blockIdx.x; p < pixels; p += gridDim.x) s += __bfloat162float(dpre[static_cast<size_t>(p) * c + ch]);
+  atomicAdd(db + ch, s);
+}
+
+// 1x1 output layer (32 -> 1, linear) and its gradients
+__global__ void out_forward_kernel(const bf16* __restrict__ a, const float* __restrict__ w, const float* __restrict__ b,
+                                   float* __restrict__ y, int pixels) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= pixels) return;
+  float s = b[0];
+#pragma unroll
+  for (int c = 0; c < 32; ++c) s += __bfloat162float(a[static_cast<size_t>(p) * 32 + c]) * w[c];
+  y[p] = s;
+}
+
+// loss = mean (y - target)^2; dy = 2 (y - target) / n; da = dy w; dw, db accumulated
+__global__ void out_backward_kernel(const bf16* __restrict__ a, const float* __restrict__ w, const float* __restrict__ y,
+                                    const float* __restrict__ target, float* __restrict__ da, float* __restrict__ dw,
+                                    float* __restrict__ db, float* __restrict__ loss, int pixels) {
+  __shared__ float red[34];
+  if (threadIdx.x < 34) red[threadIdx.x] = 0.0f;
+  __syncthreads();
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  float gw[32];
+#pragma unroll
+  for (int c = 0; c < 32; ++c) gw[c] = 0.0f;
+  float gb = 0.0f, l = 0.0f;
+  if (p < pixels) {
+    const float diff = y[p] - target[p];
+    const float dy = 2.0f * diff / static_cast<float>(pixels);
+    l = diff * diff / static_cast<float>(pixels);
+    gb = dy;
+#pragma unroll
+    for (int c = 0; c < 32; ++c) {
+      const float av = __bfloat162float(a[static_cast<size_t>(p) * 32 + c]);
+      gw[c] = dy * av;
+      da[static_cast<size_t>(p) * 32 + c] = dy * w[c];
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 32; ++c) {
+    float v = gw[c];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&red[c], v);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    gb += __shfl_xor_sync(0xffffffffu, gb, o);
+    l += __shfl_xor_sync(0xffffffffu, l, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&red[32], gb);
+    atomicAdd(&red[33], l);
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) atomicAdd(dw + threadIdx.x, red[threadIdx.x]);
+  if (threadIdx.x == 32) atomicAdd(db, red[32]);
+  if (threadIdx.x == 33) atomicAdd(loss, red[33]);
+}
+
+// Adam on the FP32 master parameters
+__global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
+                            size_t n, float lr, float b1, float b2, float eps, float c1, float c2) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  }
+}
+
+// BF16 copies of a 3x3 layer's weights: w [tap][co][ci] and the flipped /
+// transposed wt [tap][ci][co] = w[8 - tap][co][ci]
+__global__ void cast_weights_kernel(const float* __restrict__ w32, bf16* __restrict__ w, bf16* __restrict__ wt, int cout,
+                                    int cin) {
+  const int n = 9 * cout * cin;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int ci = i % cin, r = i / cin, co = r % cout, tap = r / cout;
+    const bf16 v = __float2bfloat16(w32[i]);
+    w[i] = v;
+    wt[(static_cast<size_t>(8 - tap) * cin + ci) * cout + co] = v;
+  }
+}
+
+int grid_for(size_t n) { return static_cast<int>(std::min<size_t>((n + 255) / 256, 148 * 32)); }
+
+}  // namespace
+
+// ------------------------------------------------------------------ network --
+struct gg_unet {
+  int batch = 0, size = 0;
+  cudaStream_t stream = nullptr;
+  struct Layer {
+    int cin, cout, side;  // input / output channels, spatial side
+    size_t w_off, b_off;  // offsets in the parameter vector
+    bf16* w = nullptr;    // [9][cout][cin]
+    bf16* wt = nullptr;   // [9][cin][cout]
+    bf16* act = nullptr;  // output activation [batch][side][side][cout]
+    float* dact = nullptr;
+    bf16* dpre = nullptr;
+  };
+  std::vector<Layer> layers;  // 14 convolutions
+  size_t out_w_off = 0, out_b_off = 0, n_params = 0;
+  float *params = nullptr, *grads = nullptr, *adam_m = nullptr, *adam_v = nullptr;
+  long step = 0;
+  bf16* x0 = nullptr;                      // packed input [B][S][S][16]
+  bf16 *pool1 = nullptr, *pool2 = nullptr, *pool3 = nullptr;
+  float *dpool1 = nullptr, *dpool2 = nullptr, *dpool3 = nullptr;
+  bf16 *cat8 = nullptr, *cat10 = nullptr, *cat12 = nullptr;
+  float *dcat8 = nullptr, *dcat10 = nullptr, *dcat12 = nullptr;
+  float* dx_scratch = nullptr;             // data gradient of the largest layer input
+  float* y = nullptr;                      // output [B][S][S]
+  float* loss = nullptr;
+  std::vector<void*> allocations;
+};
+
+namespace {
+
+template <class T>
+int unet_alloc(gg_unet* n, T** p, size_t count) {
+  void* q = nullptr;
+  UNET_CUDA(cudaMalloc(&q, count * sizeof(T)));
+  UNET_CUDA(cudaMemset(q, 0, count * sizeof(T)));
+  n->allocations.push_back(q);
+  *p = static_cast<T*>(q);
+  return GG_OK;
+}
+
+int run_conv(gg_unet* n, const gg_unet::Layer& L, const bf16* x, int mode, const bf16* w, int cin, int cout, void* y) {
+  ConvShape s{n->batch, L.side, L.side, cin, cout};
+  const int pixels = n->batch * L.side * L.side;
+  dim3 grid(pixels / kTileP, cout / kTileC);
+  if (mode == 0)
+    conv3x3_kernel<0><<<grid, 128, 0, n->stream>>>(x, w, n->params + L.b_off, y, s);
+  else
+    conv3x3_kernel<1><<<grid, 128, 0, n->stream>>>(x, w, nullptr, y, s);
+  UNET_CUDA(cudaGetLastError());
+  return GG_OK;
+}
+
+// input of layer i (forward)
+const bf16* layer_input(const gg_unet* n, int i) {
+  switch (i) {
+    case 0: return n->x0;
+    case 2: return n->pool1;
+    case 4: return n->pool2;
+    case 6: return n->pool3;
+    case 8: return n->cat8;
+    case 10: return n->cat10;
+    case 12: return n->cat12;
+    default: return n->layers[i - 1].act;
+  }
+}
+
+int forward(gg_unet* n, const float* input) {
+  const int B = n->batch, S = n->size;
+  const int pixels = B * S * S;
+  pack_input_kernel<<<(pixels + 255) / 256, 256, 0, n->stream>>>(input, n->x0, pixels);
+  auto& L = n->layers;
+  int rc;
+  for (int i = 0; i < 14; ++i) {
+    if (i == 2) pool_kernel<<<grid_for(static_cast<size_t>(B) * S * S / 4 * 32), 256, 0, n->stream>>>(L[1].act, n->pool1, B, S, S, 32);
+    if (i == 4) pool_kernel<<<grid_for(static_cast<size_t>(B) * S * S / 16 * 64), 256, 0, n->stream>>>(L[3].act, n->pool2, B, S / 2, S / 2, 64);
+    if (i == 6) pool_kernel<<<grid_for(static_cast<size_t>(B) * S * S / 64 * 128), 256, 0, n->stream>>>(L[5].act, n->pool3, B, S / 4, S / 4, 128);
+    if (i == 8) up_concat_kernel<<<grid_for(static_cast<size_t>(B) * (S / 4) * (S / 4) * 384), 256, 0, n->stream>>>(L[7].act, L[5].act, n->cat8, B, S / 4, S / 4, 256, 128);
+    if (i == 10) up_concat_kernel<<<grid_for(static_cast<size_t>(B) * (S / 2) * (S / 2) * 192), 256, 0, n->stream>>>(L[9].act, L[3].act, n->cat10, B, S / 2, S / 2, 128, 64);
+    if (i == 12) up_concat_kernel<<<grid_for(static_cast<size_t>(B) * S * S * 96), 256, 0, n->stream>>>(L[11].act, L[1].act, n->cat12, B, S, S, 64, 32);
+    if ((rc = run_conv(n, L[i], layer_input(n, i), 0, L[i].w, L[i].cin, L[i].cout, L[i].act))) return rc;
+  }
+  out_forward_kernel<<<(pixels + 255) / 256, 256, 0, n->stream>>>(L[13].act, n->params + n->out_w_off,
+                                                                    n->params + n->out_b_off, n->y, pixels);
+  UNET_CUDA(cudaGetLastError());
+  return GG_OK;
+}
+
+// gradients of all parameters into n->grads (zeroed first), loss into n->loss
+int backward(gg_unet* n, const float* target) {
+  const int B = n->batch, S = n->size;
+  const int pixels = B * S * S;
+  auto& L = n->layers;
+  UNET_CUDA(cudaMemsetAsync(n->grads, 0, n->n_params * sizeof(float), n->stream));
+  UNET_CUDA(cudaMemsetAsync(n->loss, 0, sizeof(float), n->stream));
+  out_backward_kernel<<<(pixels + 255) / 256, 256, 0, n->stream>>>(L[13].act, n->params + n->out_w_off, n->y, target,
+                                                                     L[13].dact, n->grads + n->out_w_off,
+                                                                     n->grads + n->out_b_off, n->loss, pixels);
+  for (int i = 13; i >= 0; --i) {
+    const auto& l = L[i];
+    const int px = B * l.side * l.side;
+    const size_t na = static_cast<size_t>(px) * l.cout;
+    relu_backward_kernel<<<grid_for(na), 256, 0, n->stream>>>(l.dact, l.act, l.dpre, na);
+    bias_grad_kernel<<<dim3(std::min(px, 1024), (l.cout + 127) / 128), 128, 0, n->stream>>>(l.dpre, n->grads + l.b_off, px, l.cout);
+    ConvShape s{B, l.side, l.side, l.cin, l.cout};
+    dim3 wg(l.cout / 32, l.cin / 16, 9 * ((px + kWgradPixels - 1) / kWgradPixels));
+    conv3x3_wgrad_kernel<<<wg, 128, 0, n->stream>>>(layer_input(n, i), l.dpre, n->grads + l.w_off, s);
+    UNET_CUDA(cudaGetLastError());
+    if (i == 0) break;
+    // data gradient of the layer input (FP32)
+    float* dx = (i == 8) ? n->dcat8 : (i == 10) ? n->dcat10 : (i == 12) ? n->dcat12
+              : (i == 2) ? n->dpool1 : (i == 4) ? n->dpool2 : (i == 6) ? n->dpool3 : L[i - 1].dact;
+    int rc;
+    if ((rc = run_conv(n, l, l.dpre, 1, l.wt, l.cout, l.cin, dx))) return rc;
+    if (i == 12) up_concat_backward_kernel<<<grid_for(static_cast<size_t>(px) * 96), 256, 0, n->stream>>>(n->dcat12, L[11].dact, L[1].dact, B, S, S, 64, 32, 1);
+    if (i == 10) up_concat_backward_kernel<<<grid_for(static_cast<size_t>(px) * 192), 256, 0, n->stream>>>(n->dcat10, L[9].dact, L[3].dact, B, S / 2, S / 2, 128, 64, 1);
+    if (i == 8) up_concat_backward_kernel<<<grid_for(static_cast<size_t>(px) * 384), 256, 0, n->stream>>>(n->dcat8, L[7].dact, L[5].dact, B, S / 4, S / 4, 256, 128, 1);
+    if (i == 6) pool_backward_kernel<<<grid_for(static_cast<size_t>(B) * (S / 4) * (S / 4) * 128), 256, 0, n->stream>>>(n->dpool3, L[5].dact, B, S / 4, S / 4, 128);
+    if (i == 4) pool_backward_kernel<<<grid_for(static_cast<size_t>(B) * (S / 2) * (S / 2) * 64), 256, 0, n->stream>>>(n->dpool2, L[3].dact, B, S / 2, S / 2, 64);
+    if (i == 2) pool_backward_kernel<<<grid_for(static_cast<size_t>(B) * S * S * 32), 256, 0, n->stream>>>(n->dpool1, L[1].dact, B, S, S, 32);
+    UNET_CUDA(cudaGetLastError());
+  }
+  return GG_OK;
+}
+
+int refresh_weights(gg_unet* n) {
+  for (auto& l : n->layers)
+    cast_weights_kernel<<<grid_for(9 * static_cast<size_t>(l.cout) * l.cin), 256, 0, n->stream>>>(n->params + l.w_off, l.w, l.wt,
+                                                                                                  l.cout, l.cin);
+  UNET_CUDA(cudaGetLastError());
+  return GG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+GG_API const char* gg_unet_last_error(void) { return g_unet_error.c_str(); }
+
+GG_API int gg_unet_create(int32_t batch, int32_t size, uint64_t seed, gg_unet** out) {
+  if (!out || batch < 1 || size < 64 || size % 64 != 0)
+    return unet_fail(GG_ERROR_INVALID_ARGUMENT, "batch >= 1 and an image side that is a multiple of 64 (>= 64) are needed");
+  *out = nullptr;
+  gg_unet* n = new gg_unet();
+  n->batch = batch;
+  n->size = size;
+  auto drop = [&](int rc) {
+    gg_unet_destroy(n);
+    return rc;
+  };
+  if (cudaStreamCreateWithFlags(&n->stream, cudaStreamNonBlocking) != cudaSuccess) return drop(unet_fail(GG_ERROR_CUDA, "stream"));
+  const int S = size;
+  const int spec[14][3] = {{16, 32, S},      {32, 32, S},      {32, 64, S / 2},   {64, 64, S / 2},  {64, 128, S / 4},
+                           {128, 128, S / 4}, {128, 256, S / 8}, {256, 256, S / 8}, {384, 128, S / 4}, {128, 128, S / 4},
+                           {192, 64, S / 2},  {64, 64, S / 2},  {96, 32, S},      {32, 32, S}};
+  size_t off = 0;
+  for (auto& sp : spec) {
+    gg_unet::Layer l;
+    l.cin = sp[0];
+    l.cout = sp[1];
+    l.side = sp[2];
+    l.w_off = off;
+    off += 9 * static_cast<size_t>(l.cin) * l.cout;
+    l.b_off = off;
+    off += l.cout;
+    n->layers.push_back(l);
+  }
+  n->out_w_off = off;
+  off += 32;
+  n->out_b_off = off;
+  off += 1;
+  n->n_params = off;
+  int rc;
+  if ((rc = unet_alloc(n, &n->params, off)) || (rc = unet_alloc(n, &n->grads, off)) || (rc = unet_alloc(n, &n->adam_m, off)) ||
+      (rc = unet_alloc(n, &n->adam_v, off)))
+    return drop(rc);
+  // He-normal initialisation of the 3x3 weights (only the 2 real input
+  // channels of layer 0 count), zero biases, small output weights.
+  std::vector<float> host(off, 0.0f);
+  std::mt19937_64 gen(seed);
+  for (auto& l : n->layers) {
+    const int fan_in = 9 * (&l == &n->layers[0] ? 2 : l.cin);
+    std::normal_distribution<float> nd(0.0f, std::sqrt(2.0f / fan_in));
+    for (int tap = 0; tap < 9; ++tap)
+      for (int co = 0; co < l.cout; ++co)
+        for (int ci = 0; ci < l.cin; ++ci)
+          host[l.w_off + (static_cast<size_t>(tap) * l.cout + co) * l.cin + ci] = (&l == &n->layers[0] && ci >= 2) ? 0.0f : nd(gen);
+  }
+  std::normal_distribution<float> nd_out(0.0f, std::sqrt(1.0f / 32.0f));
+  for (int c = 0; c < 32; ++c) host[n->out_w_off + c] = nd_out(gen);
+  if (cudaMemcpy(n->params, host.data(), off * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+    return drop(unet_fail(GG_ERROR_CUDA, "parameter upload"));
+  const size_t B = batch;
+  for (auto& l : n->layers) {
+    const size_t na = B * l.side * l.side * l.cout;
+    if ((rc = unet_alloc(n, &l.w, 9 * static_cast<size_t>(l.cin) * l.cout)) || (rc = unet_alloc(n, &l.wt, 9 * static_cast<size_t>(l.cin) * l.cout)) ||
+        (rc = unet_alloc(n, &l.act, na)) || (rc = unet_alloc(n, &l.dact, na)) || (rc = unet_alloc(n, &l.dpre, na)))
+      return drop(rc);
+  }
+  const size_t SS = static_cast<size_t>(S) * S;
+  if ((rc = unet_alloc(n, &n->x0, B * SS * 16)) || (rc = unet_alloc(n, &n->pool1, B * SS / 4 * 32)) ||
+      (rc = unet_alloc(n, &n->pool2, B * SS / 16 * 64)) || (rc = unet_alloc(n, &n->pool3, B * SS / 64 * 128)) ||
+      (rc = unet_alloc(n, &n->dpool1, B * SS / 4 * 32)) || (rc = unet_alloc(n, &n->dpool2, B * SS / 16 * 64)) ||
+      (rc = unet_alloc(n, &n->dpool3, B * SS / 64 * 128)) || (rc = unet_alloc(n, &n->cat8, B * SS / 16 * 384)) ||
+      (rc = unet_alloc(n, &n->cat10, B * SS / 4 * 192)) || (rc = unet_alloc(n, &n->cat12, B * SS * 96)) ||
+      (rc = unet_alloc(n, &n->dcat8, B * SS / 16 * 384)) || (rc = unet_alloc(n, &n->dcat10, B * SS / 4 * 192)) ||
+      (rc = unet_alloc(n, &n->dcat12, B * SS * 96)) || (rc = unet_alloc(n, &n->y, B * SS)) || (rc = unet_alloc(n, &n->loss, 1)))
+    return drop(rc);
+  if ((rc = refresh_weights(n))) return drop(rc);
+  if (cudaStreamSynchronize(n->stream) != cudaSuccess) return drop(unet_fail(GG_ERROR_CUDA, "initialisation"));
+  *out = n;
+  return GG_OK;
+}
+
+GG_API int gg_unet_destroy(gg_unet* n) {
+  if (!n) return GG_OK;
+  if (n->stream) cudaStreamSynchronize(n->stream);
+  for (void* p : n->allocations) cudaFree(p);
+  if (n->stream) cudaStreamDestroy(n->stream);
+  delete n;
+  return GG_OK;
+}
+
+GG_API int64_t gg_unet_parameter_count(const gg_unet* n) { return n ? static_cast<int64_t>(n->n_params) : 0; }
+
+GG_API int gg_unet_get_parameters(gg_unet* n, float* host) {
+  if (!n || !host) return unet_fail(GG_ERROR_INVALID_ARGUMENT, "NULL argument");
+  UNET_CUDA(cudaMemcpyAsync(host, n->params, n->n_params * sizeof(float), cudaMemcpyDeviceToHost, n->stream));
+  UNET_CUDA(cudaStreamSynchronize(n->stream));
+  return GG_OK;
+}
+
+GG_API int gg_unet_set_parameters(gg_unet* n, const float* host) {
+  if (!n || !host) return unet_fail(GG_ERROR_INVALID_ARGUMENT, "NULL argument");
+  UNET_CUDA(cudaMemcpyAsync(n->params, host, n->n_params * sizeof(float), cudaMemcpyHostToDevice, n->stream));
+  int rc;
+  if ((rc = refresh_weights(n))) return rc;
+  UNET_CUDA(cudaStreamSynchronize(n->stream));
+  return GG_OK;
+}
+
+// input: device [batch][size][size][2] FP32; output: device [batch][size][size] FP32
+GG_API int gg_unet_forward(gg_unet* n, const float* input, float* output) {
+  if (!n || !input || !output) return unet_fail(GG_ERROR_INVALID_ARGUMENT, "NULL argument");
+  int rc;
+  if ((rc = forward(n, input))) return rc;
+  UNET_CUDA(cudaMemcpyAsync(output, n->y, static_cast<size_t>(n->batch) * n->size * n->size * sizeof(float),
+                            cudaMemcpyDeviceToDevice, n->stream));
+  UNET_CUDA(cudaStreamSynchronize(n->stream));
+  return GG_OK;
+}
+
+// Loss and gradients without an update: grads_host receives the parameter gradients.
+GG_API int gg_unet_gradients(gg_unet* n, const float* input, const float* target, float* loss, float* grads_host) {
+  if (!n || !input || !target) return unet_fail(GG_ERROR_INVALID_ARGUMENT, "NULL argument");
+  int rc;
+  if ((rc = forward(n, input)) || (rc = backward(n, target))) return rc;
+  if (loss) UNET_CUDA(cudaMemcpyAsync(loss, n->loss, sizeof(float), cudaMemcpyDeviceToHost, n->stream));
+  if (grads_host)
+    UNET_CUDA(cudaMemcpyAsync(grads_host, n->grads, n->n_params * sizeof(float), cudaMemcpyDeviceToHost, n->stream));
+  UNET_CUDA(cudaStreamSynchronize(n->stream));
+  return GG_OK;
+}
+
+// One Adam step on (input, target) (device arrays as in gg_unet_forward).
+GG_API int gg_unet_train_step(gg_unet* n, const float* input, const float* target, float learning_rate, float* loss) {
+  if (!n || !input || !target) return unet_fail(GG_ERROR_INVALID_ARGUMENT, "NULL argument");
+  int rc;
+  if ((rc = forward(n, input)) || (rc = backward(n, target))) return rc;
+  ++n->step;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.0f - std::pow(b1, static_cast<float>(n->step)), c2 = 1.0f - std::pow(b2, static_cast<float>(n->step));
+  adam_kernel<<<grid_for(n->n_params), 256, 0, n->stream>>>(n->params, n->grads, n->adam_m, n->adam_v, n->n_params,
+                                                              learning_rate, b1, b2, 1e-8f, c1, c2);
+  UNET_CUDA(cudaGetLastError());
+  if ((rc = refresh_weights(n))) return rc;
+  if (loss) UNET_CUDA(cudaMemcpyAsync(loss, n->loss, sizeof(float), cudaMemcpyDeviceToHost, n->stream));
+  UNET_CUDA(cudaStreamSynchronize(n->stream));
+  return GG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,416 @@
+"""Learned scatter surrogate for CBCT projections (no counterpart in GGEMS).
+
+A 4-level BF16 U-Net (include/ggems_b200.h, gg_unet_*; kernels in
+csrc/gg_unet.cu) maps two deterministic maps of a projection -- the primary
+transmission exp(-L) and the line integral L through the phantom
+(gg_line_integrals) -- to its scatter projection.  Training pairs come from
+the Monte Carlo itself: random phantoms at random angles, all run as the jobs
+of ONE batched launch (gg_run_jobs); each job's detector keeps a total and a
+scatter histogram, the scatter histogram is the target and
+total - scatter the MC primary.  At inference every projection also gets a
+low-count plain-MC scatter estimate, which judges the network: when the two
+integrated scatter signals differ by more than 5 %, the MC estimate replaces
+the network's output.
+
+Geometry (the small water-phantom configuration): 64^3 voxels of 2 mm, random
+water ellipsoid with bone and air inserts, 60 keV cone (10 deg) at 1000 mm,
+flat GOS panel of side x side elements covering 256 mm at 1500 mm.
+
+    python -m ggems_b200.scatter --pairs 2000 --primaries 100000000   # train + evaluate, JSON line
+"""
+
+import argparse
+import ctypes as C
+import json
+import os
+import tempfile
+import time
+
+import numpy as np
+
+from . import abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+MATERIALS = os.path.join(ROOT, "ggems_b200", "data", "materials.txt")
+PHANTOM_N, PHANTOM_VOXEL = 64, 2.0
+ENERGY_MEV = 0.060
+JUDGE_TOLERANCE = 0.05
+
+
+def _lib():
+    from ._native import lib
+    P = C.POINTER
+    sig = {
+        "gg_unet_create": (C.c_int, [C.c_int32, C.c_int32, C.c_uint64, P(C.c_void_p)]),
+        "gg_unet_destroy": (C.c_int, [C.c_void_p]),
+        "gg_unet_parameter_count": (C.c_int64, [C.c_void_p]),
+        "gg_unet_get_parameters": (C.c_int, [C.c_void_p, P(C.c_float)]),
+        "gg_unet_set_parameters": (C.c_int, [C.c_void_p, P(C.c_float)]),
+        "gg_unet_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+        "gg_unet_gradients": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, P(C.c_float), P(C.c_float)]),
+        "gg_unet_train_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, P(C.c_float)]),
+        "gg_unet_last_error": (C.c_char_p, []),
+        "gg_line_integrals": (C.c_int, [C.c_void_p, P(abi.gg_solid), P(abi.gg_solid), P(C.c_float), P(C.c_float),
+                                        C.c_int32, P(C.c_float)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype, f.argtypes = res, args
+    return lib
+
+
+class UNet:
+    """The surrogate network on the GPU (device arrays: torch CUDA tensors)."""
+
+    def __init__(self, batch, side, seed=1):
+        self.lib = _lib()
+        self.batch, self.side = batch, side
+        h = C.c_void_p()
+        self._check(self.lib.gg_unet_create(batch, side, seed, C.byref(h)))
+        self.handle = h
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError("U-Net: " + self.lib.gg_unet_last_error().decode())
+
+    def close(self):
+        if self.handle:
+            self.lib.gg_unet_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def parameter_count(self):
+        return int(self.lib.gg_unet_parameter_count(self.handle))
+
+    def parameters(self):
+        p = np.zeros(self.parameter_count(), np.float32)
+        self._check(self.lib.gg_unet_get_parameters(self.handle, abi.ptr(p, C.c_float)))
+        return p
+
+    def set_parameters(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        self._check(self.lib.gg_unet_set_parameters(self.handle, abi.ptr(p, C.c_float)))
+
+    def forward(self, x):
+        """x: CUDA float32 [batch, side, side, 2] -> CUDA float32 [batch, side, side]."""
+        import torch
+        y = torch.empty((self.batch, self.side, self.side), dtype=torch.float32, device=x.device)
+        self._check(self.lib.gg_unet_forward(self.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())))
+        return y
+
+    def gradients(self, x, t):
+        g = np.zeros(self.parameter_count(), np.float32)
+        loss = C.c_float()
+        self._check(self.lib.gg_unet_gradients(self.handle, C.c_void_p(x.data_ptr()), C.c_void_p(t.data_ptr()),
+                                               C.byref(loss), abi.ptr(g, C.c_float)))
+        return loss.value, g
+
+    def train_step(self, x, t, lr):
+        loss = C.c_float()
+        self._check(self.lib.gg_unet_train_step(self.handle, C.c_void_p(x.data_ptr()), C.c_void_p(t.data_ptr()), lr,
+                                                C.byref(loss)))
+        return loss.value
+
+
+# ---------------------------------------------------------------- geometry --
+def random_phantom(rng, n=PHANTOM_N, voxel=PHANTOM_VOXEL):
+    """uint8 labels (z, y, x): 0 air, 1 water, 2 bone 1.85 -- a water ellipsoid
+    of random size with 2-6 random bone or air inserts."""
+    c = (np.arange(n, dtype=np.float32) + 0.5) * voxel - n * voxel / 2.0
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    half = n * voxel / 2.0
+    ax = rng.uniform(0.55, 0.95, 3) * half
+    labels = np.zeros((n, n, n), np.uint8)
+    labels[(x / ax[0]) ** 2 + (y / ax[1]) ** 2 + (z / ax[2]) ** 2 <= 1.0] = 1
+    for _ in range(int(rng.integers(2, 7))):
+        r = rng.uniform(0.08, 0.3, 3) * half
+        ctr = rng.uniform(-0.5, 0.5, 3) * ax
+        inside = ((x - ctr[0]) / r[0]) ** 2 + ((y - ctr[1]) / r[1]) ** 2 + ((z - ctr[2]) / r[2]) ** 2 <= 1.0
+        labels[inside & (labels > 0)] = 2 if rng.uniform() < 0.7 else 0
+    return labels
+
+
+def _rot_z(deg):
+    a = np.deg2rad(deg)
+    r = np.eye(4, dtype=np.float32)
+    r[0, 0], r[0, 1], r[1, 0], r[1, 1] = np.cos(a), -np.sin(a), np.sin(a), np.cos(a)
+    return r
+
+
+class Geometry:
+    """Base scene (phantom + flat panel + 60 keV cone) built once through the
+    GGEMS API; per-projection geometry = rotation about z + a new phantom."""
+
+    def __init__(self, side, workdir):
+        import ggems_b200 as gg
+        from .api import lib
+        from . import workloads
+        self.side = side
+        labels = random_phantom(np.random.default_rng(0))
+        mhd = workloads.write_mhd(os.path.join(workdir, "phantom.mhd"), labels, (PHANTOM_VOXEL,) * 3)
+        rng_file = os.path.join(workdir, "range.txt")
+        with open(rng_file, "w") as f:
+            f.write("0 0 Air\n1 1 Water\n2 2 Bone185\n")
+        gg.GGEMSVerbosity(0)
+        gg.GGEMSMaterialsDatabaseManager().set_materials(MATERIALS)
+        ph = gg.GGEMSVoxelizedPhantom("phantom")
+        ph.set_phantom(mhd, rng_file)
+        ph.set_rotation(0.0, 0.0, 0.0, "deg")
+        ph.set_position(0.0, 0.0, 0.0, "mm")
+        ct = gg.GGEMSCTSystem("panel")
+        ct.set_ct_type("flat")
+        ct.set_number_of_modules(1, 1)
+        ct.set_number_of_detection_elements(side, side, 1)
+        es = 256.0 / side
+        ct.set_size_of_detection_elements(es, es, 10.0, "mm")
+        ct.set_material("GOS")
+        ct.set_source_detector_distance(1500.0, "mm")
+        ct.set_source_isocenter_distance(1000.0, "mm")
+        ct.set_rotation(0.0, 0.0, 0.0, "deg")
+        ct.set_threshold(10.0, "keV")
+        ct.save(os.path.join(workdir, "projection.mhd"))
+        ct.store_scatter(True)
+        pm = gg.GGEMSProcessesManager()
+        for process in ("Compton", "Photoelectric", "Rayleigh"):
+            pm.add_process(process, "gamma", "all")
+        pm.set_cross_section_table_number_of_bins(220)
+        pm.set_cross_section_table_energy_min(1.0, "keV")
+        pm.set_cross_section_table_energy_max(1.0, "MeV")
+        gg.GGEMSRangeCutsManager().set_cut("gamma", 0.1, "mm", "all")
+        src = gg.GGEMSXRaySource("xray")
+        src.set_source_particle_type("gamma")
+        src.set_number_of_particles(1000)
+        src.set_position(-1000.0, 0.0, 0.0, "mm")
+        src.set_rotation(0.0, 0.0, 0.0, "deg")
+        src.set_beam_aperture(10.0, "deg")
+        src.set_focal_spot_size(0.0, 0.0, 0.0, "mm")
+        src.set_monoenergy(ENERGY_MEV * 1000.0, "keV")
+        self.gg = gg
+        self.ggems = gg.GGEMS()
+        self.ggems.initialize(777)
+        self.lib = lib
+        self.ctx = lib.ggems_device_context(self.ggems.obj, 0)
+        self.scene = lib.ggems_scene(self.ggems.obj).contents
+        self.source = abi.gg_source()
+        assert lib.ggems_source_descriptor(0, C.byref(self.source), None) == 0
+        assert self.scene.number_of_solids == 2
+        self.phantom = abi.gg_solid()
+        C.pointer(self.phantom)[0] = self.scene.solids[0]
+        self.detector = abi.gg_solid()
+        C.pointer(self.detector)[0] = self.scene.solids[1]
+        self.mu = self._mu(self.scene.tables[0])
+
+    @staticmethod
+    def _mu(t):
+        """Total attenuation per material (mm^-1) at ENERGY_MEV from the navigator's tables."""
+        nb, nm = t.number_of_bins, t.number_of_materials
+        e = np.ctypeslib.as_array(t.energy_bins, (nb,)).astype(np.float64)
+        cs = np.ctypeslib.as_array(t.cross_sections, (3 * nm * nb,)).reshape(3, nm, nb).astype(np.float64)
+        total = cs.sum(axis=0)
+        return np.array([np.interp(ENERGY_MEV, e, total[m]) for m in range(nm)], np.float32)
+
+    def projection(self, angle, labels, hist_base):
+        """(source, phantom solid, detector solid) of one projection; histograms hist_base, +1."""
+        src = abi.gg_source()
+        C.pointer(src)[0] = self.source
+        r = _rot_z(angle)
+        src.matrix[:] = [float(v) for v in (r @ np.array(list(self.source.matrix), np.float32).reshape(4, 4)).reshape(-1)]
+        ph = abi.gg_solid()
+        C.pointer(ph)[0] = self.phantom
+        ph.labels = abi.ptr(labels, C.c_uint8)
+        det = abi.gg_solid()
+        C.pointer(det)[0] = self.detector
+        det.obb.matrix[:] = [float(v) for v in (r @ np.array(list(self.detector.obb.matrix), np.float32).reshape(4, 4)).reshape(-1)]
+        det.histogram, det.scatter_histogram = hist_base, hist_base + 1
+        return src, ph, det
+
+    def line_integrals(self, src, ph, det):
+        out = np.zeros(self.side * self.side, np.float32)
+        pos = np.array([src.matrix[3], src.matrix[7], src.matrix[11]], np.float32)
+        lib = _lib()
+        rc = lib.gg_line_integrals(self.ctx, C.byref(ph), C.byref(det), abi.ptr(pos, C.c_float),
+                                   abi.ptr(self.mu, C.c_float), len(self.mu), abi.ptr(out, C.c_float))
+        if rc != 0:
+            raise RuntimeError(lib.gg_last_error().decode())
+        return out.reshape(self.side, self.side)
+
+    def simulate(self, projections, primaries, seed=777):
+        """Run the projections (list of (angle, labels)) as the jobs of one
+        launch; returns (total, scatter) histograms [n, side, side] (counts)."""
+        from ._native import _job_array, check
+        n = len(projections)
+        keep, jobs = [], []
+        for k, (angle, labels) in enumerate(projections):
+            src, ph, det = self.projection(angle, labels, 2 * k)
+            arr = (abi.gg_solid * 2)(ph, det)
+            keep.append((src, arr, labels))
+            jobs.append((src, primaries, arr))
+        sizes = np.full(2 * n, self.side * self.side, np.int32)
+        sc = abi.gg_scene()
+        C.pointer(sc)[0] = self.scene
+        sc.number_of_histograms = 2 * n
+        sc.histogram_sizes = abi.ptr(sizes, C.c_int32)
+        lib = self.lib
+        check(lib.gg_upload_scene(self.ctx, C.byref(sc)), "gg_upload_scene")
+        states = np.zeros(5 * abi.GG_MAXIMUM_PARTICLES, np.uint32)
+        lib.gg_seed_random_states(abi.ptr(states, C.c_uint32), abi.GG_MAXIMUM_PARTICLES, seed, 0)
+        check(lib.gg_set_random_states(self.ctx, abi.ptr(states, C.c_uint32), abi.GG_MAXIMUM_PARTICLES), "states")
+        arr, kp = _job_array(jobs)
+        check(lib.gg_run_jobs(self.ctx, arr, n), "gg_run_jobs")
+        check(lib.gg_synchronize(self.ctx), "gg_synchronize")
+        T = abi.Tallies(list(sizes), [])
+        check(lib.gg_read_tallies(self.ctx, C.byref(T.struct)), "gg_read_tallies")
+        ms, la = C.c_float(), C.c_int64()
+        lib.gg_last_run_stats(self.ctx, C.byref(ms), C.byref(la))
+        self.last_ms = ms.value
+        total = np.stack(T.histograms[0::2]).reshape(n, self.side, self.side).astype(np.float32)
+        scatter = np.stack(T.histograms[1::2]).reshape(n, self.side, self.side).astype(np.float32)
+        return total, scatter
+
+
+def normalise(counts, primaries, side):
+    """Counts -> per-primary signal times the number of elements (O(1) values)."""
+    return counts * (float(side * side) / float(primaries))
+
+
+def make_inputs(geometry, projections):
+    """[n, side, side, 2]: primary transmission exp(-L) and line integral L."""
+    out = []
+    for k, (angle, labels) in enumerate(projections):
+        src, ph, det = geometry.projection(angle, labels, 0)
+        L = geometry.line_integrals(src, ph, det)
+        out.append(np.stack([np.exp(-L), L], axis=-1))
+    return np.stack(out).astype(np.float32)
+
+
+def judge(predicted, low_count_mc, tolerance=JUDGE_TOLERANCE):
+    """Per projection: the network's output when its integrated scatter is
+    within `tolerance` of the plain-MC estimate's, else the MC estimate."""
+    out, used = [], []
+    for p, m in zip(predicted, low_count_mc):
+        ok = abs(float(p.sum()) - float(m.sum())) <= tolerance * max(float(m.sum()), 1e-12)
+        out.append(p if ok else m)
+        used.append(bool(ok))
+    return np.stack(out), np.array(used)
+
+
+def relative_error(a, ref):
+    return float(np.linalg.norm(a - ref) / max(np.linalg.norm(ref), 1e-30))
+
+
+def train(net, inputs, targets, epochs, lr=1e-3, seed=0):
+    import torch
+    n = len(inputs)
+    B = net.batch
+    rng = np.random.default_rng(seed)
+    X = torch.from_numpy(inputs).cuda()
+    Y = torch.from_numpy(targets).cuda()
+    losses = []
+    for epoch in range(epochs):
+        order = rng.permutation(n)
+        for s in range(0, n - B + 1, B):
+            idx = torch.from_numpy(order[s:s + B]).cuda()
+            xb = X.index_select(0, idx).contiguous()
+            yb = Y.index_select(0, idx).contiguous()
+            rate = lr * (0.1 if epoch >= int(0.8 * epochs) else 1.0)
+            losses.append(net.train_step(xb, yb, rate))
+    return losses
+
+
+def predict(net, inputs):
+    import torch
+    out = []
+    B = net.batch
+    for s in range(0, len(inputs), B):
+        xb = np.zeros((B,) + inputs.shape[1:], np.float32)
+        m = min(B, len(inputs) - s)
+        xb[:m] = inputs[s:s + m]
+        y = net.forward(torch.from_numpy(xb).cuda()).cpu().numpy()
+        out.append(y[:m])
+    return np.concatenate(out)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--side", type=int, default=256)
+    ap.add_argument("--pairs", type=int, default=2000)
+    ap.add_argument("--primaries", type=float, default=1e8, help="primaries per training target")
+    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--test", type=int, default=16, help="test projections (new phantoms, random angles)")
+    ap.add_argument("--judge-primaries", type=float, default=1e6)
+    ap.add_argument("--reference-primaries", type=float, default=1e9)
+    ap.add_argument("--chunk", type=int, default=64, help="projections per batched MC launch")
+    args = ap.parse_args(argv)
+    import torch  # noqa: F401  (CUDA memory for the network's device arrays)
+    work = tempfile.mkdtemp(prefix="ggems_scatter_")
+    geo = Geometry(args.side, work)
+    rng = np.random.default_rng(11)
+    side = args.side
+
+    def simulate_all(projs, primaries):
+        tot, sca, ms = [], [], 0.0
+        for s in range(0, len(projs), args.chunk):
+            t, sc = geo.simulate(projs[s:s + args.chunk], int(primaries), seed=int(rng.integers(1, 2 ** 31)))
+            tot.append(t)
+            sca.append(sc)
+            ms += geo.last_ms
+        return np.concatenate(tot), np.concatenate(sca), ms
+
+    t0 = time.time()
+    train_projs = [(float(rng.uniform(0, 360)), random_phantom(rng)) for _ in range(args.pairs)]
+    _, s_train, mc_ms = simulate_all(train_projs, args.primaries)
+    x_train = make_inputs(geo, train_projs)
+    y_train = normalise(s_train, args.primaries, side)
+    t_data = time.time() - t0
+    net = UNet(args.batch, side, seed=3)
+    t0 = time.time()
+    losses = train(net, x_train, y_train, args.epochs)
+    t_train = time.time() - t0
+    # evaluation on new phantoms
+    test_projs = [(float(rng.uniform(0, 360)), random_phantom(rng)) for _ in range(args.test)]
+    _, s_ref, ref_ms = simulate_all(test_projs, args.reference_primaries)
+    ref = normalise(s_ref, args.reference_primaries, side)
+    _, s_low, low_ms = simulate_all(test_projs, args.judge_primaries)
+    low = normalise(s_low, args.judge_primaries, side)
+    t0 = time.time()
+    x_test = make_inputs(geo, test_projs)
+    t_inputs = (time.time() - t0) / args.test
+    import torch
+    torch.cuda.synchronize()
+    t0 = time.time()
+    pred = predict(net, x_test)
+    torch.cuda.synchronize()
+    t_net = (time.time() - t0) / args.test
+    final, used = judge(pred, low)
+    err_sur = float(np.mean([relative_error(f, r) for f, r in zip(final, ref)]))
+    err_net = float(np.mean([relative_error(p, r) for p, r in zip(pred, ref)]))
+    err_low = float(np.mean([relative_error(m, r) for m, r in zip(low, ref)]))
+    # plain MC needs N with err ~ err_low * sqrt(judge / N) <= 5 %  (Poisson scaling)
+    n_plain = args.judge_primaries * (err_low / 0.05) ** 2
+    rate = args.test * args.judge_primaries / (low_ms * 1e-3)
+    t_plain = n_plain / rate
+    t_sur = args.judge_primaries / rate + t_net + t_inputs
+    print(json.dumps({
+        "metric": "scatter projections/s (surrogate + 1e6-primary MC judge vs plain MC at <=5% error)",
+        "surrogate_projections_per_s": 1.0 / t_sur, "plain_mc_projections_per_s": 1.0 / t_plain,
+        "speedup": t_plain / t_sur, "surrogate_error": err_sur, "network_error": err_net,
+        "low_count_mc_error": err_low, "judge_accepted": float(used.mean()),
+        "plain_mc_primaries_for_5pct": n_plain, "mc_primaries_per_s": rate,
+        "config": {"side": side, "pairs": args.pairs, "target_primaries": args.primaries, "epochs": args.epochs,
+                   "test": args.test, "judge_primaries": args.judge_primaries,
+                   "reference_primaries": args.reference_primaries},
+        "times_s": {"data": t_data, "train": t_train, "network_per_projection": t_net,
+                    "inputs_per_projection": t_inputs, "train_mc_ms": mc_ms},
+        "final_loss": float(np.mean(losses[-20:])) if losses else None}), flush=True)
+    net.close()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

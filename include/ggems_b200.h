@@ -292,6 +292,35 @@ GG_API int gg_get_transport_tuning(gg_context* context, int32_t* blocks_per_sm, 
 GG_API int gg_autotune(gg_context* context, const gg_source* source, uint64_t number_of_particles,
                        float* best_milliseconds);
 
+/* ---- scatter surrogate (no counterpart in the reference) ----
+ * A 4-level BF16 U-Net (base 32 channels, FP32 accumulation) mapping a CBCT
+ * primary projection and the phantom's line-integral map to the scatter
+ * projection, trained and run with this library's own kernels
+ * (ggems_b200/csrc/gg_unet.cu).  Images are square, side a multiple of 64.
+ * Arrays are DEVICE pointers: input [batch][side][side][2] (primary, line
+ * integral), target / output [batch][side][side], all FP32.  Parameters are a
+ * flat FP32 vector of gg_unet_parameter_count() values. */
+/* Line integral of mu (mm^-1 per material label) along the ray from
+ * source_position (world, mm) to the centre of every element of the detector
+ * box solid, through the voxelized phantom solid (host labels):
+ * out[j * nx + i] for element (i, j), as the detector histogram bins.  No
+ * counterpart in the reference: input of the scatter surrogate. */
+GG_API int gg_line_integrals(gg_context* context, const gg_solid* phantom, const gg_solid* detector,
+                             const float* source_position, const float* mu, int32_t number_of_materials,
+                             float* line_integrals);
+typedef struct gg_unet gg_unet;
+GG_API int gg_unet_create(int32_t batch, int32_t side, uint64_t seed, gg_unet** net);
+GG_API int gg_unet_destroy(gg_unet* net);
+GG_API int64_t gg_unet_parameter_count(const gg_unet* net);
+GG_API int gg_unet_get_parameters(gg_unet* net, float* host_parameters);
+GG_API int gg_unet_set_parameters(gg_unet* net, const float* host_parameters);
+GG_API int gg_unet_forward(gg_unet* net, const float* input, float* output);
+GG_API int gg_unet_gradients(gg_unet* net, const float* input, const float* target, float* loss,
+                             float* host_gradients);
+GG_API int gg_unet_train_step(gg_unet* net, const float* input, const float* target, float learning_rate,
+                              float* loss);
+GG_API const char* gg_unet_last_error(void);
+
 /* Batch plan of GGEMSSource::OrganizeParticlesInBatch for one device.
  * Writes at most max_batches sizes; returns the number of batches in *count. */
 GG_API int gg_batch_plan(uint64_t number_of_particles, uint64_t* batch_sizes, int64_t max_batches, int64_t* count);
