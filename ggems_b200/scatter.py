@@ -274,8 +274,23 @@ class Geometry:
 
 
 def normalise(counts, primaries, side):
-    """Counts -> per-primary signal times the number of elements (O(1) values)."""
+    """Counts -> per-primary signal times the number of elements."""
     return counts * (float(side * side) / float(primaries))
+
+
+def block_mean(img, blocks=16):
+    """Scatter is a low-frequency signal: mean over a blocks x blocks grid."""
+    img = np.asarray(img, np.float64)
+    n = img.shape[-1]
+    b = n // blocks
+    return img.reshape(img.shape[:-2] + (blocks, b, blocks, b)).mean(axis=(-3, -1))
+
+
+def smooth(img, blocks=32):
+    """Block mean expanded back to full resolution (training targets)."""
+    n = np.asarray(img).shape[-1]
+    b = n // blocks
+    return np.repeat(np.repeat(block_mean(img, blocks), b, axis=-2), b, axis=-1).astype(np.float32)
 
 
 def make_inputs(geometry, projections):
@@ -299,17 +314,23 @@ def judge(predicted, low_count_mc, tolerance=JUDGE_TOLERANCE):
     return np.stack(out), np.array(used)
 
 
-def relative_error(a, ref):
+def relative_error(a, ref, blocks=16):
+    """Relative L2 error of a scatter projection on a blocks x blocks grid."""
+    a, ref = block_mean(a, blocks), block_mean(ref, blocks)
     return float(np.linalg.norm(a - ref) / max(np.linalg.norm(ref), 1e-30))
 
 
 def train(net, inputs, targets, epochs, lr=1e-3, seed=0):
+    """Adam on (inputs, smoothed targets / their mean); the mean is kept in
+    net.target_scale and applied by predict()."""
     import torch
     n = len(inputs)
     B = net.batch
     rng = np.random.default_rng(seed)
+    targets = smooth(targets)
+    net.target_scale = float(max(targets.mean(), 1e-30))
     X = torch.from_numpy(inputs).cuda()
-    Y = torch.from_numpy(targets).cuda()
+    Y = torch.from_numpy((targets / net.target_scale).astype(np.float32)).cuda()
     losses = []
     for epoch in range(epochs):
         order = rng.permutation(n)
@@ -331,7 +352,7 @@ def predict(net, inputs):
         m = min(B, len(inputs) - s)
         xb[:m] = inputs[s:s + m]
         y = net.forward(torch.from_numpy(xb).cuda()).cpu().numpy()
-        out.append(y[:m])
+        out.append(y[:m] * getattr(net, "target_scale", 1.0))
     return np.concatenate(out)
 
 

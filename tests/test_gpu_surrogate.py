@@ -140,17 +140,17 @@ def test_surrogate_beats_low_count_mc(geometry, torch):
     from ggems_b200 import scatter as S
     rng = np.random.default_rng(6)
     side = 64
-    train = [(float(rng.uniform(0, 360)), S.random_phantom(rng)) for _ in range(96)]
-    _, s_train = geometry.simulate(train, 2_000_000, seed=21)
+    train = [(float(rng.uniform(0, 360)), S.random_phantom(rng)) for _ in range(128)]
+    _, s_train = geometry.simulate(train, 20_000_000, seed=21)
     x_train = S.make_inputs(geometry, train)
-    y_train = S.normalise(s_train, 2_000_000, side)
+    y_train = S.normalise(s_train, 20_000_000, side)
     net = S.UNet(8, side, seed=2)
-    losses = S.train(net, x_train, y_train, epochs=40, lr=2e-3)
+    losses = S.train(net, x_train, y_train, epochs=30, lr=1e-3)
     test = [(float(rng.uniform(0, 360)), S.random_phantom(rng)) for _ in range(8)]
-    _, s_ref = geometry.simulate(test, 40_000_000, seed=22)
-    _, s_low = geometry.simulate(test, 100_000, seed=23)
-    ref = S.normalise(s_ref, 40_000_000, side)
-    low = S.normalise(s_low, 100_000, side)
+    _, s_ref = geometry.simulate(test, 400_000_000, seed=22)
+    _, s_low = geometry.simulate(test, 1_000_000, seed=23)
+    ref = S.normalise(s_ref, 400_000_000, side)
+    low = S.normalise(s_low, 1_000_000, side)
     pred = S.predict(net, S.make_inputs(geometry, test))
     final, used = S.judge(pred, low)
     e_net = np.mean([S.relative_error(p, r) for p, r in zip(pred, ref)])
