@@ -10,6 +10,7 @@ of include/ggems_b200.h) can be imported without it.
 _API = ("GGEMSError", "GGEMSVerbosity", "GGEMS", "GGEMSOpenCLManager", "GGEMSMaterialsDatabaseManager",
         "GGEMSMaterials", "GGEMSCrossSections", "GGEMSAttenuations", "GGEMSProcessesManager", "GGEMSRangeCutsManager",
         "GGEMSSourceManager", "GGEMSXRaySource", "GGEMSVoxelizedSource", "GGEMSVoxelizedPhantom", "GGEMSMeshedPhantom",
+        "GGEMSWorld",
         "GGEMSCTSystem", "GGEMSDosimetryCalculator", "GGEMSProfilerManager", "GGEMSRAMManager", "clean_safely")
 
 __all__ = list(_API)

@@ -60,11 +60,17 @@ class gg_dose_map(C.Structure):
                 ("record_hit", C.c_int32), ("record_photon_tracking", C.c_int32), ("tle", C.c_int32)]
 
 
+class gg_world(C.Structure):
+    _fields_ = [("dimensions", C.c_int32 * 3), ("sizes", C.c_float * 3), ("photon_tracking", C.c_int32),
+                ("energy_tracking", C.c_int32), ("energy_squared_tracking", C.c_int32), ("momentum", C.c_int32)]
+
+
 class gg_scene(C.Structure):
     _fields_ = [("number_of_tables", C.c_int32), ("tables", C.POINTER(gg_physics_tables)),
                 ("number_of_solids", C.c_int32), ("solids", C.POINTER(gg_solid)),
                 ("number_of_dose_maps", C.c_int32), ("dose_maps", C.POINTER(gg_dose_map)),
-                ("number_of_histograms", C.c_int32), ("histogram_sizes", IP), ("rayleigh_fit", FP)]
+                ("number_of_histograms", C.c_int32), ("histogram_sizes", IP), ("rayleigh_fit", FP),
+                ("world", C.POINTER(gg_world))]
 
 
 class gg_source(C.Structure):
@@ -88,7 +94,10 @@ class gg_particle_buffers(C.Structure):
 class gg_tally_buffers(C.Structure):
     _fields_ = [("histograms", C.POINTER(IP)), ("edep", C.POINTER(C.POINTER(C.c_double))),
                 ("edep_squared", C.POINTER(C.POINTER(C.c_double))), ("hit", C.POINTER(IP)),
-                ("photon_tracking", C.POINTER(IP))]
+                ("photon_tracking", C.POINTER(IP)), ("world_photon_tracking", IP),
+                ("world_energy", C.POINTER(C.c_double)), ("world_energy_squared", C.POINTER(C.c_double)),
+                ("world_momentum_x", C.POINTER(C.c_double)), ("world_momentum_y", C.POINTER(C.c_double)),
+                ("world_momentum_z", C.POINTER(C.c_double))]
 
 
 def ptr(array, ctype):
@@ -119,7 +128,7 @@ class Particles:
 class Tallies:
     """Host tally buffers matching a scene's histograms and dose maps."""
 
-    def __init__(self, histogram_sizes, dose_sizes):
+    def __init__(self, histogram_sizes, dose_sizes, world_size=0):
         self.histograms = [np.zeros(n, np.int32) for n in histogram_sizes]
         self.edep = [np.zeros(n, np.float64) for n in dose_sizes]
         self.edep_squared = [np.zeros(n, np.float64) for n in dose_sizes]
@@ -136,3 +145,11 @@ class Tallies:
         self._hit, self._hitk = arr(self.hit, C.c_int32)
         self._pt, self._ptk = arr(self.photon_tracking, C.c_int32)
         self.struct = gg_tally_buffers(self._h, self._e, self._e2, self._hit, self._pt)
+        self.world = None
+        if world_size:
+            self.world = dict(photon_tracking=np.zeros(world_size, np.int32),
+                              **{k: np.zeros(world_size, np.float64) for k in
+                                 ("energy", "energy_squared", "momentum_x", "momentum_y", "momentum_z")})
+            self.struct.world_photon_tracking = ptr(self.world["photon_tracking"], C.c_int32)
+            for k in ("energy", "energy_squared", "momentum_x", "momentum_y", "momentum_z"):
+                setattr(self.struct, "world_" + k, ptr(self.world[k], C.c_double))

@@ -88,6 +88,12 @@ _SIGNATURES = {
     "set_material_color_ggems_meshed_phantom": (None, [vp, s, C.c_ubyte, C.c_ubyte, C.c_ubyte]),
     "set_material_color_name_ggems_meshed_phantom": (None, [vp, s, s]),
     "set_mesh_octree_depth_ggems_meshed_phantom": (None, [vp, C.c_int]),
+    "create_ggems_world": (vp, []),
+    "set_dimension_ggems_world": (None, [vp, C.c_size_t, C.c_size_t, C.c_size_t]),
+    "set_size_ggems_world": (None, [vp, f32, f32, f32, s]),
+    "photon_tracking_ggems_world": (None, [vp, b]), "energy_tracking_ggems_world": (None, [vp, b]),
+    "energy_squared_tracking_ggems_world": (None, [vp, b]), "momentum_ggems_world": (None, [vp, b]),
+    "set_output_ggems_world": (None, [vp, s]),
     "create_ggems_ct_system": (vp, [s]), "set_number_of_modules_ggems_ct_system": (None, [vp, u64, u64]),
     "set_ct_system_type_ggems_ct_system": (None, [vp, s]),
     "set_number_of_detection_elements_ggems_ct_system": (None, [vp, u64, u64, u64]),
@@ -478,6 +484,34 @@ class GGEMSMeshedPhantom(object):
             _call("set_material_color_name_ggems_meshed_phantom", self.obj, _e(material_name), _e(color_name))
         else:
             _call("set_material_color_ggems_meshed_phantom", self.obj, _e(material_name), red, green, blue)
+
+
+class GGEMSWorld(object):
+    """World grid recording photon flights between solids (ggems_phantoms.py)."""
+
+    def __init__(self):
+        self.obj = _call("create_ggems_world")
+
+    def set_dimensions(self, dim_x, dim_y, dim_z):
+        _call("set_dimension_ggems_world", self.obj, dim_x, dim_y, dim_z)
+
+    def set_element_sizes(self, size_x, size_y, size_z, unit):
+        _call("set_size_ggems_world", self.obj, size_x, size_y, size_z, _e(unit))
+
+    def photon_tracking(self, activate):
+        _call("photon_tracking_ggems_world", self.obj, activate)
+
+    def set_output_basename(self, output):
+        _call("set_output_ggems_world", self.obj, _e(output))
+
+    def energy_tracking(self, activate):
+        _call("energy_tracking_ggems_world", self.obj, activate)
+
+    def energy_squared_tracking(self, activate):
+        _call("energy_squared_tracking_ggems_world", self.obj, activate)
+
+    def momentum(self, activate):
+        _call("momentum_ggems_world", self.obj, activate)
 
 
 class GGEMSCTSystem(object):

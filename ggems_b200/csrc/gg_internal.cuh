@@ -152,6 +152,14 @@ struct TransportParams {
   int32_t tables_in_smem;
   unsigned int* slot_counter;       // work queue head
   int* error;                       // 0 = ok
+  // world tracking (GGEMSWorld): grid, tallies (NULL when not recorded);
+  // energy and momentum as int64 fixed point (LSB 2^-32), E^2 in FP64
+  int32_t world_dimensions[3];
+  float world_sizes[3];
+  int32_t* world_photon;
+  unsigned long long* world_energy;
+  double* world_energy_squared;
+  unsigned long long* world_momentum;  // [3][cells]
   int32_t regroup_lanes;            // waiting lanes that start a round of the rare phases (1..32)
   int32_t regroup_ratio4;           // ... or 4 x waiting >= regroup_ratio4 x tracking lanes
 };

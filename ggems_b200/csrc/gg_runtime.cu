@@ -74,6 +74,14 @@ struct gg_context {
   std::vector<gg::DevSolid> solid_dev_host;  // host copy of the uploaded device solids
   std::vector<char> dose_tle;             // per dose map: track-length estimator
   std::vector<const float*> density_dev;  // per navigator, for dose finalisation
+  // world tracking grid and its device tallies (NULL when not recorded)
+  int32_t world_dimensions[3] = {0, 0, 0};
+  float world_sizes[3] = {0.0f, 0.0f, 0.0f};
+  size_t world_cells = 0;
+  int32_t* world_photon = nullptr;
+  unsigned long long* world_energy = nullptr;
+  double* world_energy_squared = nullptr;
+  unsigned long long* world_momentum = nullptr;
   unsigned char* table_blob = nullptr;
   uint32_t table_bytes = 0;
   bool tables_in_smem = false;
@@ -119,6 +127,12 @@ void free_scene(gg_context* c) {
   c->solid_dev_host.clear();
   c->dose_tle.clear();
   c->density_dev.clear();
+  for (int a = 0; a < 3; ++a) c->world_dimensions[a] = 0;
+  c->world_cells = 0;
+  c->world_photon = nullptr;
+  c->world_energy = nullptr;
+  c->world_energy_squared = nullptr;
+  c->world_momentum = nullptr;
   c->scene_ready = false;
 }
 
@@ -643,6 +657,22 @@ GG_API int gg_upload_scene(gg_context* c, const gg_scene* sc) {
     c->dose_host.push_back(m);
   }
   if ((rc = dev_copy(c, c->dose_host.data(), c->dose_host.size(), &c->dose_maps))) return rc;
+  if (sc->world) {
+    // GGEMSWorld (src/navigators/GGEMSWorld.cc:191-231): one grid, centred on the origin
+    const gg_world& w = *sc->world;
+    size_t cells = 1;
+    for (int a = 0; a < 3; ++a) {
+      if (w.dimensions[a] <= 0 || !(w.sizes[a] > 0.0f)) return fail(GG_ERROR_INVALID_ARGUMENT, "world dimensions and sizes must be positive");
+      cells *= static_cast<size_t>(w.dimensions[a]);
+    }
+    std::memcpy(c->world_dimensions, w.dimensions, sizeof(c->world_dimensions));
+    std::memcpy(c->world_sizes, w.sizes, sizeof(c->world_sizes));
+    c->world_cells = cells;
+    if (w.photon_tracking && (rc = dev_copy<int32_t>(c, nullptr, cells, &c->world_photon))) return rc;
+    if (w.energy_tracking && (rc = dev_copy<unsigned long long>(c, nullptr, cells, &c->world_energy))) return rc;
+    if (w.energy_squared_tracking && (rc = dev_copy<double>(c, nullptr, cells, &c->world_energy_squared))) return rc;
+    if (w.momentum && (rc = dev_copy<unsigned long long>(c, nullptr, 3 * cells, &c->world_momentum))) return rc;
+  }
 
   // ---- solids ----
   std::vector<gg::DevSolid> solids(sc->number_of_solids);
@@ -675,6 +705,11 @@ GG_API int gg_reset_tallies(gg_context* c) {
     if (m.hit) GG_CUDA(cudaMemsetAsync(m.hit, 0, n * 4, c->stream));
     if (m.photon_tracking) GG_CUDA(cudaMemsetAsync(m.photon_tracking, 0, n * 4, c->stream));
   }
+  const size_t w = c->world_cells;
+  if (c->world_photon) GG_CUDA(cudaMemsetAsync(c->world_photon, 0, w * 4, c->stream));
+  if (c->world_energy) GG_CUDA(cudaMemsetAsync(c->world_energy, 0, w * 8, c->stream));
+  if (c->world_energy_squared) GG_CUDA(cudaMemsetAsync(c->world_energy_squared, 0, w * 8, c->stream));
+  if (c->world_momentum) GG_CUDA(cudaMemsetAsync(c->world_momentum, 0, 3 * w * 8, c->stream));
   return GG_OK;
 }
 
@@ -811,6 +846,15 @@ int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*
   P.error = c->error;
   P.regroup_lanes = c->regroup_lanes;
   P.regroup_ratio4 = c->regroup_ratio4;
+  if (c->world_cells) {
+    std::memcpy(P.world_dimensions, c->world_dimensions, sizeof(P.world_dimensions));
+    std::memcpy(P.world_sizes, c->world_sizes, sizeof(P.world_sizes));
+    P.world_photon = c->world_photon;
+    P.world_energy = c->world_energy;
+    P.world_energy_squared = c->world_energy_squared;
+    P.world_momentum = c->world_momentum;
+    mesh = true;  // the world walk lives in the full kernel variant
+  }
   out->smem = (c->tables_in_smem ? c->table_bytes : 0) + sizeof(gg::DevSolid) * c->number_of_solids +
               sizeof(gg::DevNavigator) * c->number_of_navigators + 16;
   int blocks_per_sm = 0;
@@ -1086,6 +1130,23 @@ GG_API int gg_read_tallies(gg_context* c, gg_tally_buffers* t) {
     if (t->hit && t->hit[d] && m.hit) GG_CUDA(cudaMemcpy(t->hit[d], m.hit, n * 4, cudaMemcpyDeviceToHost));
     if (t->photon_tracking && t->photon_tracking[d] && m.photon_tracking)
       GG_CUDA(cudaMemcpy(t->photon_tracking[d], m.photon_tracking, n * 4, cudaMemcpyDeviceToHost));
+  }
+  const size_t w = c->world_cells;
+  auto read_fixed = [&](double* dst, const unsigned long long* src) -> cudaError_t {
+    std::vector<long long> q(w);
+    cudaError_t e = cudaMemcpy(q.data(), src, w * 8, cudaMemcpyDeviceToHost);
+    for (size_t i = 0; e == cudaSuccess && i < w; ++i) dst[i] = static_cast<double>(q[i]) / gg::kEdepScale;
+    return e;
+  };
+  if (t->world_photon_tracking && c->world_photon)
+    GG_CUDA(cudaMemcpy(t->world_photon_tracking, c->world_photon, w * 4, cudaMemcpyDeviceToHost));
+  if (t->world_energy && c->world_energy) GG_CUDA(read_fixed(t->world_energy, c->world_energy));
+  if (t->world_energy_squared && c->world_energy_squared)
+    GG_CUDA(cudaMemcpy(t->world_energy_squared, c->world_energy_squared, w * 8, cudaMemcpyDeviceToHost));
+  if (c->world_momentum) {
+    double* m[3] = {t->world_momentum_x, t->world_momentum_y, t->world_momentum_z};
+    for (int a = 0; a < 3; ++a)
+      if (m[a]) GG_CUDA(read_fixed(m[a], c->world_momentum + a * w));
   }
   return GG_OK;
 }

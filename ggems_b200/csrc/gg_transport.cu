@@ -623,6 +623,52 @@ __device__ __noinline__ MeshCrossings mesh_crossings(V3 p, V3 d, V3 inv, const f
   return out;
 }
 
+// world_tracking (WorldTracking.cl:54-162): the flight from the photon's
+// position to the solid FindSolid chose (10 m when none) sampled in steps of
+// the world element size along the dominant axis.
+__device__ __noinline__ void world_track(V3 p1, V3 dir, float E, float psd, const TransportParams& P) {
+  float distance = psd == kOutOfWorld ? 10000.0f : psd;
+  if (distance <= kTolerance) return;
+  const V3 size = v3(P.world_sizes[0], P.world_sizes[1], P.world_sizes[2]);
+  const int nx = P.world_dimensions[0], ny = P.world_dimensions[1], nz = P.world_dimensions[2];
+  const V3 p2 = add(p1, scale(dir, distance));
+  const V3 lo = v3(size.x * static_cast<float>(nx) * -0.5f, size.y * static_cast<float>(ny) * -0.5f,
+                   size.z * static_cast<float>(nz) * -0.5f);
+  V3 q = divv(sub(p1, lo), size);
+  int ix = __float2int_rz(q.x), iy = __float2int_rz(q.y), iz = __float2int_rz(q.z);
+  const V3 diff = sub(p2, p1);
+  float length = fabsf(diff.x), main_size = size.x;
+  if (fabsf(diff.y) > length) {
+    length = fabsf(diff.y);
+    main_size = size.y;
+  } else if (fabsf(diff.z) > length) {
+    length = fabsf(diff.z);
+    main_size = size.z;
+  }
+  const float inv_length = 1.0f / length;
+  const V3 increment = v3(inv_length * diff.x, inv_length * diff.y, inv_length * diff.z);
+  const int steps = static_cast<int>(1.0f + (length / main_size));
+  const size_t cells = static_cast<size_t>(nx) * ny * nz;
+  const long long e_fixed = __double2ll_rn(static_cast<double>(E) * kEdepScale);
+  const long long m_fixed[3] = {__double2ll_rn(static_cast<double>(dir.x) * kEdepScale),
+                                __double2ll_rn(static_cast<double>(dir.y) * kEdepScale),
+                                __double2ll_rn(static_cast<double>(dir.z) * kEdepScale)};
+  for (int i = 0; i < steps; ++i) {
+    if (ix < 0 || ix >= nx || iy < 0 || iy >= ny || iz < 0 || iz >= nz) break;
+    const size_t g = ix + static_cast<size_t>(iy) * nx + static_cast<size_t>(iz) * nx * ny;
+    if (P.world_photon) atomicAdd(P.world_photon + g, 1);
+    if (P.world_energy) atomicAdd(P.world_energy + g, static_cast<unsigned long long>(e_fixed));
+    if (P.world_energy_squared) atomicAdd(P.world_energy_squared + g, static_cast<double>(E) * static_cast<double>(E));
+    if (P.world_momentum)
+      for (int a = 0; a < 3; ++a) atomicAdd(P.world_momentum + a * cells + g, static_cast<unsigned long long>(m_fixed[a]));
+    p1 = add(p1, scale(increment, main_size));
+    q = divv(sub(p1, lo), size);
+    ix = __float2int_rz(q.x);
+    iy = __float2int_rz(q.y);
+    iz = __float2int_rz(q.z);
+  }
+}
+
 // Histogram of interaction sites in a CT detector module (the HISTOGRAM part of
 // TrackThroughGGEMSSolidBox.cl:214-236), with the scatter histogram.
 __device__ __forceinline__ void box_histogram(const DevSolid& so, const Photon& ph) {
@@ -680,12 +726,12 @@ __device__ bool stage_tables(unsigned char* dst, const unsigned char* src, uint3
 
 extern __shared__ __align__(16) unsigned char g_smem[];
 
-// kMesh: the scene has a meshed solid.  Scenes without one run the variant
-// compiled without the mesh phase, so its code and registers stay out of the
-// voxel / detector hot loop.
+// kFull: the scene has a meshed solid or records world tracking.  Scenes
+// with neither run the variant compiled without the mesh phase and the world
+// walk, so their code and registers stay out of the voxel / detector hot loop.
 // kBatch: several jobs (source runs) in one launch, each with its own solids.
-template <bool kMesh, bool kBatch>
-__global__ void __launch_bounds__(kBlockThreads, kMesh ? 2 : (kBatch ? 3 : 4)) transport_kernel(TransportParams P) {
+template <bool kFull, bool kBatch>
+__global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) transport_kernel(TransportParams P) {
   // shared memory: [tables][solids][navigators][mbarrier]
   unsigned char* tables = g_smem;
   DevSolid* scene_solids = reinterpret_cast<DevSolid*>(g_smem + (P.tables_in_smem ? P.table_bytes : 0));
@@ -778,7 +824,7 @@ __global__ void __launch_bounds__(kBlockThreads, kMesh ? 2 : (kBatch ? 3 : 4)) t
   // End of track_through_*: back to the global frame; the history goes on
   // (FindSolid) unless the photon died.
   auto leave_solid = [&](const DevSolid& so, bool dead) {
-    if (kMesh && so.type == GG_SOLID_MESHED) {
+    if (kFull && so.type == GG_SOLID_MESHED) {
       // A meshed solid tracks in world coordinates and, on leaving (dead or
       // not), carries the photon to its OBB boundary (TrackThroughGGEMSMeshSolid.cl:521-533).
       V3 mn = v3(so.border_min[0], so.border_min[1], so.border_min[2]);
@@ -794,7 +840,7 @@ __global__ void __launch_bounds__(kBlockThreads, kMesh ? 2 : (kBatch ? 3 : 4)) t
     else phase = kFind;
   };
   auto track_phase = [](int type) {
-    return type == GG_SOLID_VOXELIZED ? kTrackVoxel : (kMesh && type == GG_SOLID_MESHED) ? kTrackMesh : kTrackBox;
+    return type == GG_SOLID_VOXELIZED ? kTrackVoxel : (kFull && type == GG_SOLID_MESHED) ? kTrackMesh : kTrackBox;
   };
 
   if (next_slot()) phase = kNewHistory;
@@ -814,7 +860,7 @@ __global__ void __launch_bounds__(kBlockThreads, kMesh ? 2 : (kBatch ? 3 : 4)) t
     const unsigned active = __ballot_sync(0xffffffffu, phase != kDone);
     if (active == 0) break;
     const unsigned tracking =
-        __ballot_sync(0xffffffffu, phase == kTrackVoxel || phase == kTrackBox || (kMesh && phase == kTrackMesh));
+        __ballot_sync(0xffffffffu, phase == kTrackVoxel || phase == kTrackBox || (kFull && phase == kTrackMesh));
     const int n_other = __popc(active & ~tracking);
     if (n_other > 0 && (n_other >= regroup || 4 * n_other >= ratio4 * __popc(tracking))) {
       if (phase == kInteract) {
@@ -880,6 +926,7 @@ __global__ void __launch_bounds__(kBlockThreads, kMesh ? 2 : (kBatch ? 3 : 4)) t
             ph.solid_id = s;
           }
         }
+        if (kFull && P.world_dimensions[0] > 0 && ph.status != GG_DEAD) world_track(ph.p, ph.d, ph.E, ph.psd, P);
         // project_to_* (ProjectToGGEMS*.cl:44-129)
         if (ph.solid_id == -1) ph.status = GG_DEAD;
         if (ph.psd == kOutOfWorld) {
@@ -900,7 +947,7 @@ __global__ void __launch_bounds__(kBlockThreads, kMesh ? 2 : (kBatch ? 3 : 4)) t
           // Enter the solid: switch to local coordinates (a meshed solid's
           // triangles are already in world coordinates).
           const DevSolid& so = solids[ph.solid_id];
-          if (!kMesh || so.type != GG_SOLID_MESHED) {
+          if (!kFull || so.type != GG_SOLID_MESHED) {
             ph.p = g2l_pos(so.matrix, ph.p);
             ph.d = g2l_dir(so.matrix, ph.d);
           }
@@ -911,7 +958,7 @@ __global__ void __launch_bounds__(kBlockThreads, kMesh ? 2 : (kBatch ? 3 : 4)) t
       if (end) end_history();
       continue;
     }
-    if (phase != kTrackVoxel && phase != kTrackBox && !(kMesh && phase == kTrackMesh)) continue;
+    if (phase != kTrackVoxel && phase != kTrackBox && !(kFull && phase == kTrackMesh)) continue;
 
     // ---- one tracking step inside solid ph.solid_id ----
     const DevSolid& so = solids[ph.solid_id];
@@ -984,7 +1031,7 @@ __global__ void __launch_bounds__(kBlockThreads, kMesh ? 2 : (kBatch ? 3 : 4)) t
         ph.status = GG_DEAD;
       }
       if (ph.status == GG_DEAD) leave_solid(so, true);
-    } else if (kMesh && phase == kTrackMesh) {
+    } else if (kFull && phase == kTrackMesh) {
       // track_through_ggems_meshed_solid, TrackThroughGGEMSMeshSolid.cl:385-518:
       // the parity of the crossing count says whether the photon is inside the
       // mesh; outside, it jumps to the first crossing.  Material 0.

@@ -503,6 +503,21 @@ void Simulation::clean() {
   sources.clear();
   navigators.clear();
   dosimetry.clear();
+  world.reset();
+}
+
+World::World() { Simulation::instance().world.reset(this); }
+void World::set_element_size(float x, float y, float z, const std::string& unit) {
+  sizes[0] = distance_unit(x, unit);
+  sizes[1] = distance_unit(y, unit);
+  sizes[2] = distance_unit(z, unit);
+}
+// GGEMSWorld::CheckParameters (src/navigators/GGEMSWorld.cc:172-190)
+void World::check() const {
+  if (dimensions[0] == 0 || dimensions[1] == 0 || dimensions[2] == 0)
+    throw Error("GGEMSWorld", "CheckParameters", "Dimensions of world have to be set");
+  if (sizes[0] < 0.0f || sizes[1] < 0.0f || sizes[2] < 0.0f)
+    throw Error("GGEMSWorld", "CheckParameters", "Size of elements in world");
 }
 
 GGEMS::GGEMS() {}
@@ -634,6 +649,22 @@ void GGEMS::build_scene() {
   scene_.number_of_histograms = static_cast<int32_t>(histogram_sizes_.size());
   scene_.histogram_sizes = histogram_sizes_.data();
   scene_.rayleigh_fit = rayleigh_fit_.data();
+  scene_.world = nullptr;
+  if (World* w = sim.world.get()) {
+    // GGEMSWorld::Initialize (src/navigators/GGEMSWorld.cc:264-298)
+    w->check();
+    world_ = gg_world{};
+    for (int a = 0; a < 3; ++a) {
+      if (w->dimensions[a] > 0x7fffffffull) throw Error("GGEMSWorld", "CheckParameters", "world dimension too large");
+      world_.dimensions[a] = static_cast<int32_t>(w->dimensions[a]);
+      world_.sizes[a] = w->sizes[a];
+    }
+    world_.photon_tracking = w->photon_tracking ? 1 : 0;
+    world_.energy_tracking = w->energy_tracking ? 1 : 0;
+    world_.energy_squared_tracking = w->energy_squared_tracking ? 1 : 0;
+    world_.momentum = w->momentum ? 1 : 0;
+    scene_.world = &world_;
+  }
 }
 
 // GGEMS::Run / RunOnDevice (src/global/GGEMS.cc:303-414): one host thread per
@@ -713,6 +744,11 @@ void GGEMS::save_results() {
     hit_[m].assign(n, 0);
     ptrack_[m].assign(n, 0);
   }
+  const size_t nw = scene_.world ? static_cast<size_t>(world_.dimensions[0]) * world_.dimensions[1] * world_.dimensions[2] : 0;
+  world_photon_.assign(nw, 0);
+  world_energy_.assign(nw, 0.0);
+  world_energy2_.assign(nw, 0.0);
+  for (auto& v : world_momentum_) v.assign(nw, 0.0);
   for (auto& dev : devices) {
     std::vector<std::vector<int32_t>> h(nh);
     std::vector<int32_t*> hp(nh);
@@ -736,7 +772,24 @@ void GGEMS::save_results() {
       ptp[m] = pt[m].data();
     }
     gg_tally_buffers tb{hp.data(), ep.data(), e2p.data(), hip.data(), ptp.data()};
+    std::vector<int32_t> wp(nw, 0);
+    std::vector<double> we(nw, 0.0), we2(nw, 0.0), wm[3];
+    if (nw) {
+      for (auto& v : wm) v.assign(nw, 0.0);
+      tb.world_photon_tracking = wp.data();
+      tb.world_energy = we.data();
+      tb.world_energy_squared = we2.data();
+      tb.world_momentum_x = wm[0].data();
+      tb.world_momentum_y = wm[1].data();
+      tb.world_momentum_z = wm[2].data();
+    }
     check_device(gg_read_tallies(dev.context, &tb), "ReadTallies");
+    for (size_t k = 0; k < nw; ++k) {
+      world_photon_[k] += wp[k];
+      world_energy_[k] += we[k];
+      world_energy2_[k] += we2[k];
+      for (int a = 0; a < 3; ++a) world_momentum_[a][k] += wm[a][k];
+    }
     for (size_t i = 0; i < nh; ++i)
       for (size_t k = 0; k < h[i].size(); ++k) histograms_[i][k] += h[i][k];
     for (size_t m = 0; m < nd; ++m)
@@ -781,14 +834,17 @@ void GGEMS::save_results() {
     const int m = solids_[s].dose_map;
     const gg_dose_map& dm = dose_maps_[m];
     const size_t nn = static_cast<size_t>(dm.total_number_of_dosels);
-    std::vector<float> dose(nn), unc(nn);
-    check_device(gg_compute_dose(devices[0].context, m, static_cast<int32_t>(s), dc->scale_factor, dc->water_reference ? 1 : 0,
-                                 dc->minimum_density, dose.data(), dc->uncertainty ? unc.data() : nullptr),
-                 "ComputeDose");
-    if (devices.size() > 1) {
-      // Dose of the summed tallies, computed on the host with the same formula.
+    // Every device converts its own tallies (GGEMSDosimetryCalculator::ComputeDose);
+    // the saved images are the sums over devices (SaveDose / SaveUncertainty,
+    // src/navigators/GGEMSDosimetryCalculator.cc:726-800).
+    std::vector<float> dose(nn, 0.0f), unc(nn, 0.0f), dose_d(nn), unc_d(nn);
+    for (auto& dev : devices) {
+      check_device(gg_compute_dose(dev.context, m, static_cast<int32_t>(s), dc->scale_factor, dc->water_reference ? 1 : 0,
+                                   dc->minimum_density, dose_d.data(), dc->uncertainty ? unc_d.data() : nullptr),
+                   "ComputeDose");
       for (size_t k = 0; k < nn; ++k) {
-        (void)k;
+        dose[k] += dose_d[k];
+        if (dc->uncertainty) unc[k] += unc_d[k];
       }
     }
     int32_t dim[3] = {dm.number_of_dosels[0], dm.number_of_dosels[1], dm.number_of_dosels[2]};
@@ -799,6 +855,20 @@ void GGEMS::save_results() {
     if (dc->hit) write_mhd(dc->output + "_hit.mhd", "MET_INT", dim, dm.size_of_dosels, hit_[m].data(), 4);
     if (dc->photon_tracking)
       write_mhd(dc->output + "_photon_tracking.mhd", "MET_INT", dim, dm.size_of_dosels, ptrack_[m].data(), 4);
+  }
+  // GGEMSWorld::SaveResults (src/navigators/GGEMSWorld.cc:405-602)
+  if (World* w = scene_.world ? sim.world.get() : nullptr) {
+    const int32_t* dim = world_.dimensions;
+    const std::string& b = w->output;
+    if (w->photon_tracking) write_mhd(b + "_world_photon_tracking.mhd", "MET_INT", dim, world_.sizes, world_photon_.data(), 4);
+    if (w->energy_tracking) write_mhd(b + "_world_edep.mhd", "MET_DOUBLE", dim, world_.sizes, world_energy_.data(), 8);
+    if (w->energy_squared_tracking)
+      write_mhd(b + "_world_edep_squared.mhd", "MET_DOUBLE", dim, world_.sizes, world_energy2_.data(), 8);
+    if (w->momentum) {
+      const char* axis[3] = {"x", "y", "z"};
+      for (int a = 0; a < 3; ++a)
+        write_mhd(b + "_world_momentum_" + axis[a] + ".mhd", "MET_DOUBLE", dim, world_.sizes, world_momentum_[a].data(), 8);
+    }
   }
 }
 

@@ -176,6 +176,20 @@ class DosimetryCalculator {
   void initialize(const SolidSpec& solid);
 };
 
+// GGEMSWorld (include/GGEMS/navigators/GGEMSWorld.hh:55-215): a grid centred
+// on the origin recording the photons' flights between solids.  Creating one
+// registers it with the simulation (GGEMSNavigatorManager::StoreWorld).
+class World {
+ public:
+  World();
+  std::string output = "world";
+  uint64_t dimensions[3] = {0, 0, 0};
+  float sizes[3] = {-1.0f, -1.0f, -1.0f};
+  bool photon_tracking = false, energy_tracking = false, energy_squared_tracking = false, momentum = false;
+  void set_element_size(float x, float y, float z, const std::string& unit);
+  void check() const;
+};
+
 // ------------------------------------------------------------------ GGEMS --
 struct Device {
   gg_context* context = nullptr;
@@ -189,6 +203,7 @@ class Simulation {
   std::vector<std::unique_ptr<Source>> sources;
   std::vector<std::unique_ptr<Navigator>> navigators;
   std::vector<DosimetryCalculator*> dosimetry;
+  std::unique_ptr<World> world;
   std::vector<int> device_indices;        // activated devices (empty: device 0)
   std::vector<double> device_balance;     // per activated device
   int cs_number_of_bins = 220;            // CROSS_SECTION_TABLE_NUMBER_BINS
@@ -234,6 +249,9 @@ class GGEMS {
   std::vector<std::vector<int32_t>> histograms_;
   std::vector<std::vector<double>> edep_, edep2_;
   std::vector<std::vector<int32_t>> hit_, ptrack_;
+  gg_world world_{};
+  std::vector<int32_t> world_photon_;
+  std::vector<double> world_energy_, world_energy2_, world_momentum_[3];
 };
 
 }  // namespace gg

@@ -338,6 +338,24 @@ GG_EXPORT void set_visible_ggems_meshed_phantom(MeshedPhantom*, bool) {}
 GG_EXPORT void set_material_color_ggems_meshed_phantom(MeshedPhantom*, const char*, unsigned char, unsigned char, unsigned char) {}
 GG_EXPORT void set_material_color_name_ggems_meshed_phantom(MeshedPhantom*, const char*, const char*) {}
 
+// GGEMSWorld (src/navigators/GGEMSWorld.cc:605-671)
+GG_EXPORT World* create_ggems_world(void) {
+  return guarded_value<World*>(nullptr, [&] { return new World(); });
+}
+GG_EXPORT void set_dimension_ggems_world(World* w, size_t x, size_t y, size_t z) {
+  w->dimensions[0] = x;
+  w->dimensions[1] = y;
+  w->dimensions[2] = z;
+}
+GG_EXPORT void set_size_ggems_world(World* w, float x, float y, float z, const char* unit) {
+  guarded([&] { w->set_element_size(x, y, z, S(unit)); });
+}
+GG_EXPORT void photon_tracking_ggems_world(World* w, bool on) { w->photon_tracking = on; }
+GG_EXPORT void energy_tracking_ggems_world(World* w, bool on) { w->energy_tracking = on; }
+GG_EXPORT void energy_squared_tracking_ggems_world(World* w, bool on) { w->energy_squared_tracking = on; }
+GG_EXPORT void set_output_ggems_world(World* w, const char* basename) { w->output = S(basename); }
+GG_EXPORT void momentum_ggems_world(World* w, bool on) { w->momentum = on; }
+
 // Meshed solid of an STL file as the host API prepares it (test hook; no
 // counterpart in the reference).  Output sizes: triangles n*GG_TRIANGLE_FLOATS,
 // nodes m*6, node_first m+1, node_triangles n, with n / m from the first call

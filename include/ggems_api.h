@@ -27,6 +27,7 @@ typedef struct GGEMSVoxelizedSource GGEMSVoxelizedSource;
 typedef struct GGEMSVoxelizedPhantom GGEMSVoxelizedPhantom;
 typedef struct GGEMSMeshedPhantom GGEMSMeshedPhantom;
 typedef struct GGEMSCTSystem GGEMSCTSystem;
+typedef struct GGEMSWorld GGEMSWorld;
 typedef struct GGEMSDosimetryCalculator GGEMSDosimetryCalculator;
 typedef struct GGEMSMaterials GGEMSMaterials;
 typedef struct GGEMSAttenuations GGEMSAttenuations;
@@ -117,6 +118,18 @@ void set_material_name_ggems_meshed_phantom(GGEMSMeshedPhantom* p, const char* m
 void set_material_color_ggems_meshed_phantom(GGEMSMeshedPhantom* p, const char* material, unsigned char r, unsigned char g, unsigned char b);  /* include/GGEMS/navigators/GGEMSMeshedPhantom.hh:182 */
 void set_material_color_name_ggems_meshed_phantom(GGEMSMeshedPhantom* p, const char* material, const char* color);  /* include/GGEMS/navigators/GGEMSMeshedPhantom.hh:191 */
 void set_mesh_octree_depth_ggems_meshed_phantom(GGEMSMeshedPhantom* p, int depth);  /* include/GGEMS/navigators/GGEMSMeshedPhantom.hh:199 */
+
+/* GGEMSWorld: photon flights between solids recorded on a grid centred on the
+ * origin; outputs <basename>_world_photon_tracking / _world_edep /
+ * _world_edep_squared / _world_momentum_{x,y,z}.mhd */
+GGEMSWorld* create_ggems_world(void);  /* include/GGEMS/navigators/GGEMSWorld.hh:231 */
+void set_dimension_ggems_world(GGEMSWorld* w, size_t x, size_t y, size_t z);  /* include/GGEMS/navigators/GGEMSWorld.hh:241 */
+void set_size_ggems_world(GGEMSWorld* w, float x, float y, float z, const char* unit);  /* include/GGEMS/navigators/GGEMSWorld.hh:252 */
+void photon_tracking_ggems_world(GGEMSWorld* w, bool is_activated);  /* include/GGEMS/navigators/GGEMSWorld.hh:260 */
+void energy_tracking_ggems_world(GGEMSWorld* w, bool is_activated);  /* include/GGEMS/navigators/GGEMSWorld.hh:268 */
+void energy_squared_tracking_ggems_world(GGEMSWorld* w, bool is_activated);  /* include/GGEMS/navigators/GGEMSWorld.hh:276 */
+void set_output_ggems_world(GGEMSWorld* w, const char* basename);  /* include/GGEMS/navigators/GGEMSWorld.hh:284 */
+void momentum_ggems_world(GGEMSWorld* w, bool is_activated);  /* include/GGEMS/navigators/GGEMSWorld.hh:292 */
 int ggems_build_mesh(const char* stl, const float* matrix, int depth, int32_t* n_triangles, int32_t* n_nodes, float* triangles, float* nodes, int32_t* node_first, int32_t* node_triangles, float* border_min, float* border_max);  /* no counterpart in the reference: B200 build addition */
 GGEMSCTSystem* create_ggems_ct_system(const char* name);  /* include/GGEMS/navigators/GGEMSCTSystem.hh:141 */
 void set_number_of_modules_ggems_ct_system(GGEMSCTSystem* c, uint64_t mx, uint64_t my);  /* include/GGEMS/navigators/GGEMSCTSystem.hh:150 */

@@ -155,6 +155,18 @@ typedef struct gg_dose_map {
                                    (TrackThroughGGEMSVoxelizedSolid.cl:286-301) */
 } gg_dose_map;
 
+/* World tracking: GGEMSWorld (src/navigators/GGEMSWorld.cc,
+ * src/kernels/WorldTracking.cl) -- a coarse grid centred on the origin that
+ * tallies the flight of every photon between solids. */
+typedef struct gg_world {
+  int32_t dimensions[3];
+  float sizes[3];               /* mm */
+  int32_t photon_tracking;      /* record crossings (int32) */
+  int32_t energy_tracking;      /* record E (MeV) */
+  int32_t energy_squared_tracking;
+  int32_t momentum;             /* record direction components */
+} gg_world;
+
 typedef struct gg_scene {
   int32_t number_of_tables;
   const gg_physics_tables* tables;
@@ -166,6 +178,7 @@ typedef struct gg_scene {
   const int32_t* histogram_sizes;   /* elements per histogram */
   const float* rayleigh_fit;        /* [9][101] Livermore form-factor fit PP0..PP8
                                        (GGEMSRayleighScatteringModels.hh:36-153) */
+  const gg_world* world;            /* NULL: no world tracking */
 } gg_scene;
 
 typedef enum gg_source_type {
@@ -217,6 +230,13 @@ typedef struct gg_tally_buffers {
   double** edep_squared;
   int32_t** hit;
   int32_t** photon_tracking;
+  /* world grid tallies (NULL to skip), dimensions[0]*dimensions[1]*dimensions[2] each */
+  int32_t* world_photon_tracking;
+  double* world_energy;
+  double* world_energy_squared;
+  double* world_momentum_x;
+  double* world_momentum_y;
+  double* world_momentum_z;
 } gg_tally_buffers;
 
 typedef struct gg_context gg_context;

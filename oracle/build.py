@@ -46,6 +46,7 @@ REF_KERNELS = [
     ("TrackThroughGGEMSMeshSolid", ["DOSIMETRY"],
      ["track_through_ggems_meshed_solid=track_through_ggems_meshed_solid_dosimetry"]),
     ("IsAlive", [], []),
+    ("WorldTracking", [], []),
 ]
 
 

@@ -782,12 +782,66 @@ void track_meshed(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& s, 
   ph.d = ld;
 }
 
+// world_tracking (WorldTracking.cl:54-162): the photon's flight from its
+// position to the solid FindSolid chose (10 m when none) is sampled in steps
+// of the world element size along the dominant axis.
+void world_tracking(const Photon& ph, const gg_world& w, const Tallies& t) {
+  if (ph.status == GG_DEAD) return;
+  float distance = ph.psd == kOutOfWorld ? 10000.0f : ph.psd;
+  if (distance <= kGeometryTolerance) return;
+  V3 p1 = ph.p;
+  const V3 dir = ph.d;
+  const V3 size = v3(w.sizes[0], w.sizes[1], w.sizes[2]);
+  const int dim[3] = {w.dimensions[0], w.dimensions[1], w.dimensions[2]};
+  V3 p2 = add(p1, scale(dir, distance));
+  const V3 lo = v3(size.x * static_cast<float>(dim[0]) * -0.5f, size.y * static_cast<float>(dim[1]) * -0.5f,
+                   size.z * static_cast<float>(dim[2]) * -0.5f);
+  auto index_of = [&](V3 p, int idx[3]) {
+    V3 q = divv(sub(p, lo), size);
+    idx[0] = static_cast<int>(q.x);
+    idx[1] = static_cast<int>(q.y);
+    idx[2] = static_cast<int>(q.z);
+  };
+  int idx[3];
+  index_of(p1, idx);
+  V3 diff = sub(p2, p1);
+  V3 len = v3(std::fabs(diff.x), std::fabs(diff.y), std::fabs(diff.z));
+  float length = len.x, main_size = size.x;
+  if (len.y > length) {
+    length = len.y;
+    main_size = size.y;
+  } else if (len.z > length) {
+    length = len.z;
+    main_size = size.z;
+  }
+  float inv_length = 1.0f / length;
+  V3 increment = v3(inv_length * diff.x, inv_length * diff.y, inv_length * diff.z);
+  int steps = static_cast<int>(1.0f + (length / main_size));
+  const double E = ph.E;
+  for (int i = 0; i < steps; ++i) {
+    if (idx[0] < 0 || idx[0] >= dim[0] || idx[1] < 0 || idx[1] >= dim[1] || idx[2] < 0 || idx[2] >= dim[2]) break;
+    const size_t g = idx[0] + static_cast<size_t>(idx[1]) * dim[0] + static_cast<size_t>(idx[2]) * dim[0] * dim[1];
+    const gg_tally_buffers* o = t.out;
+    if (o && w.photon_tracking && o->world_photon_tracking) atomic_add_int(&o->world_photon_tracking[g], 1);
+    if (o && w.energy_tracking && o->world_energy) atomic_add_double(&o->world_energy[g], E);
+    if (o && w.energy_squared_tracking && o->world_energy_squared) atomic_add_double(&o->world_energy_squared[g], E * E);
+    if (o && w.momentum && o->world_momentum_x) {
+      atomic_add_double(&o->world_momentum_x[g], static_cast<double>(dir.x));
+      atomic_add_double(&o->world_momentum_y[g], static_cast<double>(dir.y));
+      atomic_add_double(&o->world_momentum_z[g], static_cast<double>(dir.z));
+    }
+    p1 = add(p1, scale(increment, main_size));
+    index_of(p1, idx);
+  }
+}
+
 // One history, following GGEMS::RunOnDevice's inner loop (src/global/GGEMS.cc:326-345):
 // FindSolid, ProjectToSolid, TrackThroughSolid over all solids in order,
 // until the particle is dead or GG_MAX_LOOP iterations were made.
 void transport(Photon& ph, Kiss& rng, const gg_scene& sc, const Tallies& t) {
   for (int loop = 0; loop < GG_MAX_LOOP; ++loop) {
     for (int s = 0; s < sc.number_of_solids; ++s) solid_distance(ph, sc.solids[s], s);
+    if (sc.world) world_tracking(ph, *sc.world, t);
     for (int s = 0; s < sc.number_of_solids; ++s) project_to(ph, sc.solids[s], s);
     for (int s = 0; s < sc.number_of_solids; ++s) {
       const gg_solid& solid = sc.solids[s];

@@ -66,6 +66,8 @@ void track_through_ggems_meshed_solid_dosimetry(ulong, GGEMSPrimaryParticles*, G
                                                 const GGEMSMuMuEnData*, float, GGEMSDoseParams*, double*, double*,
                                                 int*, int*);
 void is_alive(ulong, GGEMSPrimaryParticles*, int*);
+void world_tracking(ulong, GGEMSPrimaryParticles*, int*, double*, double*, double*, double*, double*, ulong, ulong,
+                    ulong, float, float, float);
 }
 
 namespace {
@@ -315,6 +317,21 @@ extern "C" __attribute__((visibility("default"))) int gg_ref_run(const gg_scene*
           parallel_for(n, threads, [&]() { particle_solid_distance_ggems_meshed_solid(n, P, &mesh[s]); });
         else
           parallel_for(n, threads, [&]() { particle_solid_distance_ggems_solid_box(n, P, &box[s]); });
+      }
+      if (scene->world) {
+        const gg_world& w = *scene->world;
+        const gg_tally_buffers* o = tallies;
+        int* wp = (o && w.photon_tracking) ? o->world_photon_tracking : nullptr;
+        double* we = (o && w.energy_tracking) ? o->world_energy : nullptr;
+        double* we2 = (o && w.energy_squared_tracking) ? o->world_energy_squared : nullptr;
+        double* mx = (o && w.momentum) ? o->world_momentum_x : nullptr;
+        double* my = (o && w.momentum) ? o->world_momentum_y : nullptr;
+        double* mz = (o && w.momentum) ? o->world_momentum_z : nullptr;
+        parallel_for(n, threads, [&]() {
+          world_tracking(n, P, wp, we, we2, mx, my, mz, static_cast<ulong>(w.dimensions[0]),
+                         static_cast<ulong>(w.dimensions[1]), static_cast<ulong>(w.dimensions[2]), w.sizes[0], w.sizes[1],
+                         w.sizes[2]);
+        });
       }
       for (int s = 0; s < ns; ++s) {
         if (scene->solids[s].type == GG_SOLID_VOXELIZED)

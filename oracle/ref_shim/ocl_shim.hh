@@ -95,6 +95,7 @@ inline int3 operator-(int3 const& a, int s) { return int3(a.x - s, a.y - s, a.z 
 inline float dot(float3 const& a, float3 const& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 inline float dot(float4 const& a, float4 const& b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
 inline float3 normalize(float3 const& v) { return v * (1.0f / std::sqrt(dot(v, v))); }
+inline float3 fabs(float3 const& v) { return float3(std::fabs(v.x), std::fabs(v.y), std::fabs(v.z)); }
 
 inline int3 convert_int3(float3 const& v) { return int3(static_cast<int>(v.x), static_cast<int>(v.y), static_cast<int>(v.z)); }
 inline float3 convert_float3(int3 const& v) { return float3(static_cast<float>(v.x), static_cast<float>(v.y), static_cast<float>(v.z)); }

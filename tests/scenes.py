@@ -190,6 +190,7 @@ class Scene:
         self.dose_maps = []
         self.histogram_sizes = []
         self.meshes = []
+        self.world = None
         self._keep = []
 
     def add_tables(self, tables):
@@ -321,11 +322,23 @@ class Scene:
         self._d = (abi.gg_dose_map * max(1, len(self.dose_maps)))(*self.dose_maps)
         self._h = np.array(self.histogram_sizes + [0], np.int32)
         self._pp = rayleigh_fit()
+        world = C.pointer(self.world) if self.world is not None else C.cast(None, C.POINTER(abi.gg_world))
         return abi.gg_scene(len(self.tables), self._t, len(self.solids), self._s, len(self.dose_maps), self._d,
-                            len(self.histogram_sizes), abi.ptr(self._h, C.c_int32), abi.ptr(self._pp, C.c_float))
+                            len(self.histogram_sizes), abi.ptr(self._h, C.c_int32), abi.ptr(self._pp, C.c_float),
+                            world)
+
+    def set_world(self, dimensions, sizes, photon=True, energy=True, energy_squared=True, momentum=True):
+        """GGEMSWorld grid (centred on the origin)."""
+        w = abi.gg_world()
+        w.dimensions[:] = list(dimensions)
+        w.sizes[:] = [float(F(v)) for v in sizes]
+        w.photon_tracking, w.energy_tracking = int(photon), int(energy)
+        w.energy_squared_tracking, w.momentum = int(energy_squared), int(momentum)
+        self.world = w
 
     def tallies(self):
-        return abi.Tallies(self.histogram_sizes, [d.total_number_of_dosels for d in self.dose_maps])
+        ws = int(np.prod(list(self.world.dimensions))) if self.world is not None else 0
+        return abi.Tallies(self.histogram_sizes, [d.total_number_of_dosels for d in self.dose_maps], ws)
 
 
 class XRaySource:

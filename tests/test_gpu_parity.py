@@ -274,3 +274,28 @@ def test_large_mesh_bvh(ctx, tmp_path):
     assert close > 0.995
     assert (sg[:, :n] == so[:, :n]).all(0).mean() > 0.999
     assert abs(Tg.edep[0].sum() - To.edep[0].sum()) <= 0.005 * To.edep[0].sum()
+
+
+def test_world_tracking(ctx):
+    """GGEMSWorld on a CBCT scene: photon counts, energy, energy^2 and momentum
+    on the world grid agree with the oracle (same histories; int64 fixed-point
+    energy and momentum on the GPU against FP64 sums in the oracle)."""
+    sc = scenes.cbct_scene(n=32, voxel=8.0, elements=(64, 64, 1), element_size=(6.4, 6.4, 10.0))
+    sc.set_world((40, 30, 20), (60.0, 50.0, 40.0))
+    src = scenes.XRaySource(spectrum=scenes.synthetic_spectrum(), aperture_deg=11.0)
+    n = 200000
+    Pg, Tg, sg = parity.run_gpu(ctx, sc, src, n)
+    Po, To, so = parity.run_oracle(sc, src, n)
+    exact, close = parity.history_agreement(Pg, Po)
+    _report("world tracking", exact, close)
+    assert close > 0.995
+    wg, wo = Tg.world, To.world
+    assert wo["photon_tracking"].sum() > 0
+    cnt_g, cnt_o = wg["photon_tracking"].astype(np.int64), wo["photon_tracking"].astype(np.int64)
+    assert abs(int(cnt_g.sum()) - int(cnt_o.sum())) <= 0.005 * cnt_o.sum()
+    assert (cnt_g == cnt_o).mean() > 0.99
+    for k in ("energy", "energy_squared", "momentum_x", "momentum_y", "momentum_z"):
+        g, o = wg[k], wo[k]
+        scale = np.abs(o).sum()
+        assert scale > 0, k
+        assert np.abs(g - o).sum() <= 0.005 * scale, k

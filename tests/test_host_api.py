@@ -197,3 +197,50 @@ def test_dosimetry_tle_flag_reaches_the_scene(tmp_path):
         assert np.array_equal(mu_en.view(np.uint32), ref.mu_en.view(np.uint32))
         print("ok")
     ''', tmp_path)
+
+
+def test_world_reaches_the_scene(tmp_path):
+    """GGEMSWorld's grid and switches reach the scene in mm; missing
+    dimensions raise GGEMSWorld::CheckParameters's message."""
+    out = _run(r'''
+        import ctypes as C
+        from ggems_b200 import workloads, abi
+        from ggems_b200 import (GGEMSMaterialsDatabaseManager, GGEMSVoxelizedPhantom, GGEMSProcessesManager,
+                                GGEMSRangeCutsManager, GGEMSXRaySource, GGEMSWorld)
+        import scenes
+        mhd, rng = workloads.water_files(".", 16, 4.0)
+        GGEMSMaterialsDatabaseManager().set_materials(scenes.MATERIALS)
+        ph = GGEMSVoxelizedPhantom("phantom")
+        ph.set_phantom(mhd, rng)
+        ph.set_rotation(0.0, 0.0, 0.0, "deg")
+        ph.set_position(0.0, 0.0, 0.0, "mm")
+        pm = GGEMSProcessesManager()
+        pm.add_process("Compton", "gamma", "all")
+        GGEMSRangeCutsManager().set_cut("gamma", 0.1, "mm", "all")
+        s = GGEMSXRaySource("src")
+        s.set_source_particle_type("gamma")
+        s.set_number_of_particles(1000)
+        s.set_position(-1000.0, 0.0, 0.0, "mm")
+        s.set_rotation(0.0, 0.0, 0.0, "deg")
+        s.set_beam_aperture(10.0, "deg")
+        s.set_focal_spot_size(0.0, 0.0, 0.0, "mm")
+        s.set_monoenergy(60.0, "keV")
+        from ggems_b200.api import lib
+        lib.ggems_host_scene.restype = C.POINTER(abi.gg_scene)
+        w = GGEMSWorld()
+        lib.ggems_clear_error()
+        assert not lib.ggems_host_scene()
+        assert b"Dimensions of world have to be set" in lib.ggems_last_error()
+        w.set_dimensions(200, 100, 50)
+        w.set_element_sizes(1.0, 2.0, 0.5, "cm")
+        w.photon_tracking(True)
+        w.momentum(True)
+        w.set_output_basename("out/w")
+        sc = lib.ggems_host_scene().contents
+        g = sc.world.contents
+        assert list(g.dimensions) == [200, 100, 50]
+        assert list(g.sizes) == [10.0, 20.0, 5.0]
+        assert (g.photon_tracking, g.energy_tracking, g.energy_squared_tracking, g.momentum) == (1, 0, 0, 1)
+        print("ok")
+    ''', tmp_path)
+    assert "ok" in out

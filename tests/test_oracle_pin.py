@@ -49,6 +49,11 @@ def _run_ref(sc, src, n, seed=777):
 def _assert_identical(a, b):
     Pa, Ta, sa = a
     Pb, Tb, sb = b
+    if Ta.world is not None:
+        assert np.array_equal(Ta.world["photon_tracking"], Tb.world["photon_tracking"])
+        assert Ta.world["photon_tracking"].sum() > 0
+        for k in ("energy", "energy_squared", "momentum_x", "momentum_y", "momentum_z"):
+            np.testing.assert_allclose(Ta.world[k], Tb.world[k], rtol=1e-12, atol=1e-9)
     exact, _ = parity.history_agreement(Pa, Pb)
     assert exact == 1.0
     assert np.array_equal(sa, sb)
@@ -156,5 +161,15 @@ def test_pin_meshed_phantom_dosimetry_rotated(tmp_path):
                                    ops=[("rotation", (float(90 * deg), float(30 * deg), 0.0)),
                                         ("translation", (10.0, -5.0, 0.0))])
     src = scenes.XRaySource(spectrum=scenes.synthetic_spectrum(), aperture_deg=8.0)
+    n = 20000
+    _assert_identical(parity.run_oracle(sc, src, n), _run_ref(sc, src, n))
+
+
+def test_pin_world_tracking():
+    """GGEMSWorld: photon counts, energy, energy^2 and momentum on a world grid
+    (WorldTracking.cl), with a phantom and a CT panel."""
+    sc = scenes.cbct_scene(n=32, voxel=8.0, elements=(64, 64, 1), element_size=(6.4, 6.4, 10.0))
+    sc.set_world((40, 30, 20), (60.0, 50.0, 40.0))
+    src = scenes.XRaySource(spectrum=scenes.synthetic_spectrum(), aperture_deg=11.0)
     n = 20000
     _assert_identical(parity.run_oracle(sc, src, n), _run_ref(sc, src, n))
