@@ -10,7 +10,7 @@ of include/ggems_b200.h) can be imported without it.
 _API = ("GGEMSError", "GGEMSVerbosity", "GGEMS", "GGEMSOpenCLManager", "GGEMSMaterialsDatabaseManager",
         "GGEMSMaterials", "GGEMSCrossSections", "GGEMSAttenuations", "GGEMSProcessesManager", "GGEMSRangeCutsManager",
         "GGEMSSourceManager", "GGEMSXRaySource", "GGEMSVoxelizedSource", "GGEMSVoxelizedPhantom", "GGEMSMeshedPhantom",
-        "GGEMSWorld",
+        "GGEMSWorld", "GGEMSVolumeCreatorManager", "GGEMSBox", "GGEMSTube", "GGEMSSphere",
         "GGEMSCTSystem", "GGEMSDosimetryCalculator", "GGEMSProfilerManager", "GGEMSRAMManager", "clean_safely")
 
 __all__ = list(_API)

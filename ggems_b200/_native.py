@@ -46,6 +46,13 @@ def _load():
         "gg_set_transport_tuning": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
         "gg_get_transport_tuning": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32), P(C.c_int32)]),
         "gg_autotune": (C.c_int, [C.c_void_p, P(abi.gg_source), C.c_uint64, P(C.c_float)]),
+        "gg_volume_create": (C.c_int, [C.c_int32, C.c_int32, P(C.c_int32), P(C.c_float), P(C.c_void_p)]),
+        "gg_volume_destroy": (C.c_int, [C.c_void_p]),
+        "gg_volume_upload": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+        "gg_volume_download": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+        "gg_volume_draw": (C.c_int, [C.c_void_p, P(abi.gg_shape), C.c_int32]),
+        "gg_volume_labels": (C.c_int, [C.c_void_p, P(C.c_float), P(C.c_float), C.c_int32, P(C.c_uint8),
+                                       P(C.c_int64)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -184,3 +191,62 @@ class Graph:
             self.close()
         except Exception:
             pass
+
+
+class Volume:
+    """A phantom image on the device (gg_volume_*): analytic shapes drawn into
+    it, or an MHD image uploaded and converted to labels by a range table."""
+
+    def __init__(self, met_type, dimensions, element_sizes, device=0):
+        import numpy as np
+        self.met_type = met_type
+        self.dimensions = tuple(int(d) for d in dimensions)
+        self.dtype = np.dtype(abi.MET_DTYPES[met_type])
+        dims = (C.c_int32 * 3)(*self.dimensions)
+        es = (C.c_float * 3)(*[float(e) for e in element_sizes])
+        h = C.c_void_p()
+        check(lib.gg_volume_create(device, met_type, dims, es, C.byref(h)), "gg_volume_create")
+        self.handle = h
+
+    @property
+    def elements(self):
+        return self.dimensions[0] * self.dimensions[1] * self.dimensions[2]
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib.gg_volume_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def draw(self, shapes):
+        arr = (abi.gg_shape * len(shapes))(*shapes)
+        check(lib.gg_volume_draw(self.handle, arr, len(shapes)), "gg_volume_draw")
+
+    def upload(self, image):
+        import numpy as np
+        a = np.ascontiguousarray(image, self.dtype).reshape(-1)
+        if a.size != self.elements:
+            raise ValueError("image has %d elements, the volume %d" % (a.size, self.elements))
+        check(lib.gg_volume_upload(self.handle, a.ctypes.data_as(C.c_void_p), a.nbytes), "gg_volume_upload")
+
+    def download(self):
+        import numpy as np
+        a = np.empty(self.elements, self.dtype)
+        check(lib.gg_volume_download(self.handle, a.ctypes.data_as(C.c_void_p), a.nbytes), "gg_volume_download")
+        return a
+
+    def labels(self, first, last):
+        """uint8 labels of every element and the number left unconverted (255)."""
+        import numpy as np
+        f = np.ascontiguousarray(first, np.float32)
+        l_ = np.ascontiguousarray(last, np.float32)
+        out = np.empty(self.elements, np.uint8)
+        missing = C.c_int64()
+        check(lib.gg_volume_labels(self.handle, abi.ptr(f, C.c_float), abi.ptr(l_, C.c_float), len(f),
+                                   abi.ptr(out, C.c_uint8), C.byref(missing)), "gg_volume_labels")
+        return out, missing.value

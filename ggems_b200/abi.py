@@ -21,6 +21,11 @@ GG_SOLID_BOX = 1
 GG_SOLID_MESHED = 2
 GG_SOURCE_XRAY = 0
 GG_SOURCE_VOXELIZED = 1
+# gg_met_type / gg_shape_type (phantom volumes) and the numpy type of each element type
+GG_MET_CHAR, GG_MET_UCHAR, GG_MET_SHORT, GG_MET_USHORT, GG_MET_INT, GG_MET_UINT, GG_MET_FLOAT = range(7)
+MET_NAMES = ("MET_CHAR", "MET_UCHAR", "MET_SHORT", "MET_USHORT", "MET_INT", "MET_UINT", "MET_FLOAT")
+MET_DTYPES = ("int8", "uint8", "int16", "uint16", "int32", "uint32", "float32")
+GG_SHAPE_BOX, GG_SHAPE_TUBE, GG_SHAPE_SPHERE = range(3)
 
 STATUS = {0: "GG_OK", 1: "GG_ERROR_INVALID_ARGUMENT", 2: "GG_ERROR_CUDA", 3: "GG_ERROR_NO_DEVICE",
           4: "GG_ERROR_OUT_OF_MEMORY", 5: "GG_ERROR_STATE", 6: "GG_ERROR_TIMEOUT"}
@@ -80,6 +85,10 @@ class gg_source(C.Structure):
                 ("is_interp", C.c_int32), ("number_of_voxels", C.c_int32 * 3), ("voxel_sizes", C.c_float * 3),
                 ("border_min", C.c_float * 3), ("number_of_activity_bins", C.c_int64),
                 ("activity_index", IP), ("activity_cdf", FP)]
+
+
+class gg_shape(C.Structure):
+    _fields_ = [("type", C.c_int32), ("position", C.c_float * 3), ("label_value", C.c_float), ("size", C.c_float * 3)]
 
 
 class gg_job(C.Structure):

@@ -94,6 +94,19 @@ _SIGNATURES = {
     "photon_tracking_ggems_world": (None, [vp, b]), "energy_tracking_ggems_world": (None, [vp, b]),
     "energy_squared_tracking_ggems_world": (None, [vp, b]), "momentum_ggems_world": (None, [vp, b]),
     "set_output_ggems_world": (None, [vp, s]),
+    "get_instance_volume_creator_manager": (vp, []),
+    "set_volume_dimension_volume_creator_manager": (None, [vp, C.c_size_t, C.c_size_t, C.c_size_t]),
+    "set_element_sizes_volume_creator_manager": (None, [vp, f32, f32, f32, s]),
+    "set_output_image_filename_volume_creator_manager": (None, [vp, s]),
+    "set_output_range_to_material_filename_volume_creator_manager": (None, [vp, s]),
+    "initialize_volume_creator_manager": (None, [vp]), "write_volume_creator_manager": (None, [vp]),
+    "set_material_volume_creator_manager": (None, [vp, s]), "set_data_type_volume_creator_manager": (None, [vp, s]),
+    "clean_volume_creator_manager": (None, [vp]),
+    "create_box": (vp, [f32, f32, f32, s]), "create_tube": (vp, [f32, f32, f32, s]), "create_sphere": (vp, [f32, s]),
+    **{f % shape: sig for shape in ("box", "tube", "sphere") for f, sig in (
+        ("delete_%s", (None, [vp])), ("set_position_%s", (None, [vp, f32, f32, f32, s])),
+        ("set_material_%s", (None, [vp, s])), ("set_label_value_%s", (None, [vp, f32])),
+        ("initialize_%s", (None, [vp])), ("draw_%s", (None, [vp])))},
     "create_ggems_ct_system": (vp, [s]), "set_number_of_modules_ggems_ct_system": (None, [vp, u64, u64]),
     "set_ct_system_type_ggems_ct_system": (None, [vp, s]),
     "set_number_of_detection_elements_ggems_ct_system": (None, [vp, u64, u64, u64]),
@@ -512,6 +525,86 @@ class GGEMSWorld(object):
 
     def momentum(self, activate):
         _call("momentum_ggems_world", self.obj, activate)
+
+
+class GGEMSVolumeCreatorManager(object):
+    """Voxel image of analytic shapes, drawn on the device (ggems_volume_creator.py)."""
+
+    def __init__(self):
+        self.obj = _call("get_instance_volume_creator_manager")
+
+    def set_dimensions(self, width, height, depth):
+        _call("set_volume_dimension_volume_creator_manager", self.obj, width, height, depth)
+
+    def set_element_sizes(self, width, height, depth, unit):
+        _call("set_element_sizes_volume_creator_manager", self.obj, width, height, depth, _e(unit))
+
+    def set_output(self, output):
+        _call("set_output_image_filename_volume_creator_manager", self.obj, _e(output))
+
+    def set_range_output(self, output):
+        _call("set_output_range_to_material_filename_volume_creator_manager", self.obj, _e(output))
+
+    def initialize(self):
+        _call("initialize_volume_creator_manager", self.obj)
+
+    def write(self):
+        _call("write_volume_creator_manager", self.obj)
+
+    def set_material(self, material):
+        _call("set_material_volume_creator_manager", self.obj, _e(material))
+
+    def set_data_type(self, data_type):
+        _call("set_data_type_volume_creator_manager", self.obj, _e(data_type))
+
+    def clean(self):
+        _call("clean_volume_creator_manager", self.obj)
+
+
+class _Shape(object):
+    _kind = ""
+
+    def delete(self):
+        _call("delete_" + self._kind, self.obj)
+
+    def set_label_value(self, label_value):
+        _call("set_label_value_" + self._kind, self.obj, label_value)
+
+    def set_position(self, pos_x, pos_y, pos_z, unit):
+        _call("set_position_" + self._kind, self.obj, pos_x, pos_y, pos_z, _e(unit))
+
+    def set_material(self, material):
+        _call("set_material_" + self._kind, self.obj, _e(material))
+
+    def initialize(self):
+        _call("initialize_" + self._kind, self.obj)
+
+    def draw(self):
+        _call("draw_" + self._kind, self.obj)
+
+
+class GGEMSTube(_Shape):
+    """Elliptic tube along z (ggems_volume_creator.py)."""
+    _kind = "tube"
+
+    def __init__(self, radius_x, radius_y, height, unit):
+        self.obj = _call("create_tube", radius_x, radius_y, height, _e(unit))
+
+
+class GGEMSBox(_Shape):
+    """Box of width (x), height (y), depth (z) (ggems_volume_creator.py)."""
+    _kind = "box"
+
+    def __init__(self, width, height, depth, unit):
+        self.obj = _call("create_box", width, height, depth, _e(unit))
+
+
+class GGEMSSphere(_Shape):
+    """Sphere (ggems_volume_creator.py)."""
+    _kind = "sphere"
+
+    def __init__(self, radius, unit):
+        self.obj = _call("create_sphere", radius, _e(unit))
 
 
 class GGEMSCTSystem(object):

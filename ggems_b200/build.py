@@ -22,7 +22,7 @@ NVCC = ["nvcc", "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + 
 CXX = ["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-fvisibility=hidden",
        "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 # The transport kernels keep the reference's operation order: no contraction into FMA.
-FMAD = {"gg_transport.cu": ["-fmad=false"]}
+FMAD = {"gg_transport.cu": ["-fmad=false"], "gg_volume.cu": ["-fmad=false"]}
 
 
 def _newer(src, obj, deps=()):

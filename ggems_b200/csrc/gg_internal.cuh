@@ -202,6 +202,9 @@ struct ProjectorParams {
 };
 void launch_line_integrals(const ProjectorParams& p, void* stream);
 
+// Records msg as the text of gg_last_error() for this thread; returns code.
+int record_error(int code, const char* msg);
+
 }  // namespace gg
 
 #endif

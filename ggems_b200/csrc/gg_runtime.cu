@@ -49,6 +49,8 @@ struct DevArray {
 
 }  // namespace
 
+int gg::record_error(int code, const char* msg) { return fail(code, msg); }
+
 struct gg_context {
   int device = 0;
   cudaStream_t stream = nullptr;

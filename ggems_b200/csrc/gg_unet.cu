@@ -21,7 +21,16 @@
 //   bottleneck 128->256->256 @S/8
 //   dec  up, concat(128): 384->128->128 @S/4 | up, concat(64): 192->64->64 @S/2 |
 //        up, concat(32): 96->32->32 @S | 1x1 32->1 (linear)
-// pool = 2x2 average, up = nearest x2.  The 2 input channels are zero-padded to 16.
+// pool = 2x2 average, up = nearest x2.
+//
+// Input stage (fixed, not trained): the 2 input maps a = exp(-L), b = L give
+// 10 of the 16 channels of the first layer (the rest are zero):
+//   0 a, 1 b, 2-4 box means of a over (2r+1)^2 windows, r = 4, 16, 64,
+//   5-7 the same for b, 8 / 9 means of a / b over the whole image,
+// box means with zero padding outside the image (window sum / (2r+1)^2), from
+// an FP64 summed-area table per image and map.  The wide windows give every
+// pixel the phantom-scale context that its ~100-pixel receptive field lacks:
+// scatter at one detector element depends on the whole irradiated volume.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -190,14 +199,63 @@ __global__ void __launch_bounds__(128) conv3x3_wgrad_kernel(const bf16* __restri
 }
 
 // ------------------------------------------------------------ elementwise --
-__global__ void pack_input_kernel(const float* __restrict__ in, bf16* __restrict__ x, int pixels) {
-  // in: [pixels][2] FP32 -> x: [pixels][16] BF16 (channels 2..15 zero)
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= pixels) return;
+__host__ __device__ constexpr int context_radius(int k) { return k == 0 ? 4 : (k == 1 ? 16 : 64); }
+constexpr int kInputChannels = 10;  // real channels of the first layer's 16
+
+// Summed-area tables I[b][m][(S+1)^2] of the two input maps (row 0 and column 0
+// stay zero).  Pass 1: one thread per image row, prefix sums along the row.
+__global__ void sat_rows_kernel(const float* __restrict__ in, double* __restrict__ sat, int batch, int S) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // (b, m, y)
+  if (t >= batch * 2 * S) return;
+  const int y = t % S, m = (t / S) % 2, b = t / (2 * S);
+  const float* row = in + (static_cast<size_t>(b) * S + y) * S * 2 + m;
+  double* out = sat + (static_cast<size_t>(b) * 2 + m) * (S + 1) * (S + 1) + static_cast<size_t>(y + 1) * (S + 1) + 1;
+  double acc = 0.0;
+  for (int x = 0; x < S; ++x) {
+    acc += static_cast<double>(row[2 * x]);
+    out[x] = acc;
+  }
+}
+
+// Pass 2: one thread per column (coalesced across threads), prefix sums down the column.
+__global__ void sat_cols_kernel(double* __restrict__ sat, int batch, int S) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // (b, m, x)
+  if (t >= batch * 2 * S) return;
+  const int x = t % S, bm = t / S;
+  double* col = sat + static_cast<size_t>(bm) * (S + 1) * (S + 1) + x + 1;
+  double acc = 0.0;
+  for (int y = 1; y <= S; ++y) {
+    acc += col[static_cast<size_t>(y) * (S + 1)];
+    col[static_cast<size_t>(y) * (S + 1)] = acc;
+  }
+}
+
+__device__ __forceinline__ double box_sum(const double* I, int S, int x, int y, int r) {
+  const int x0 = max(x - r, 0), x1 = min(x + r, S - 1), y0 = max(y - r, 0), y1 = min(y + r, S - 1);
+  const size_t W = S + 1;
+  return I[(y1 + 1) * W + x1 + 1] - I[y0 * W + x1 + 1] - I[(y1 + 1) * W + x0] + I[y0 * W + x0];
+}
+
+// in: [B][S][S][2] FP32 -> x: [B][S][S][16] BF16, channels as listed at the top.
+__global__ void pack_input_kernel(const float* __restrict__ in, const double* __restrict__ sat, bf16* __restrict__ x,
+                                  int batch, int S) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= batch * S * S) return;
+  const int px = p % S, py = (p / S) % S, b = p / (S * S);
   __align__(16) bf16 v[16];
   for (int c = 0; c < 16; ++c) v[c] = __float2bfloat16(0.0f);
-  v[0] = __float2bfloat16(in[2 * p]);
-  v[1] = __float2bfloat16(in[2 * p + 1]);
+  v[0] = __float2bfloat16(in[2 * static_cast<size_t>(p)]);
+  v[1] = __float2bfloat16(in[2 * static_cast<size_t>(p) + 1]);
+  const size_t plane = static_cast<size_t>(S + 1) * (S + 1);
+  for (int m = 0; m < 2; ++m) {
+    const double* I = sat + (static_cast<size_t>(b) * 2 + m) * plane;
+    for (int k = 0; k < 3; ++k) {
+      const int r = context_radius(k);
+      const double area = static_cast<double>(2 * r + 1) * (2 * r + 1);
+      v[2 + 3 * m + k] = __float2bfloat16(static_cast<float>(box_sum(I, S, px, py, r) / area));
+    }
+    v[8 + m] = __float2bfloat16(static_cast<float>(I[plane - 1] / (static_cast<double>(S) * S)));
+  }
   uint4* dst = reinterpret_cast<uint4*>(x + static_cast<size_t>(p) * 16);
   dst[0] = *reinterpret_cast<uint4*>(v);
   dst[1] = *reinterpret_cast<uint4*>(v + 8);
@@ -397,6 +455,7 @@ struct gg_unet {
   float *params = nullptr, *grads = nullptr, *adam_m = nullptr, *adam_v = nullptr;
   long step = 0;
   bf16* x0 = nullptr;                      // packed input [B][S][S][16]
+  double* sat = nullptr;                   // summed-area tables [B][2][S+1][S+1]
   bf16 *pool1 = nullptr, *pool2 = nullptr, *pool3 = nullptr;
   float *dpool1 = nullptr, *dpool2 = nullptr, *dpool3 = nullptr;
   bf16 *cat8 = nullptr, *cat10 = nullptr, *cat12 = nullptr;
@@ -448,7 +507,9 @@ const bf16* layer_input(const gg_unet* n, int i) {
 int forward(gg_unet* n, const float* input) {
   const int B = n->batch, S = n->size;
   const int pixels = B * S * S;
-  pack_input_kernel<<<(pixels + 255) / 256, 256, 0, n->stream>>>(input, n->x0, pixels);
+  sat_rows_kernel<<<(B * 2 * S + 127) / 128, 128, 0, n->stream>>>(input, n->sat, B, S);
+  sat_cols_kernel<<<(B * 2 * S + 127) / 128, 128, 0, n->stream>>>(n->sat, B, S);
+  pack_input_kernel<<<(pixels + 255) / 256, 256, 0, n->stream>>>(input, n->sat, n->x0, B, S);
   auto& L = n->layers;
   int rc;
   for (int i = 0; i < 14; ++i) {
@@ -554,17 +615,17 @@ GG_API int gg_unet_create(int32_t batch, int32_t size, uint64_t seed, gg_unet** 
   if ((rc = unet_alloc(n, &n->params, off)) || (rc = unet_alloc(n, &n->grads, off)) || (rc = unet_alloc(n, &n->adam_m, off)) ||
       (rc = unet_alloc(n, &n->adam_v, off)))
     return drop(rc);
-  // He-normal initialisation of the 3x3 weights (only the 2 real input
+  // He-normal initialisation of the 3x3 weights (only the 10 real input
   // channels of layer 0 count), zero biases, small output weights.
   std::vector<float> host(off, 0.0f);
   std::mt19937_64 gen(seed);
   for (auto& l : n->layers) {
-    const int fan_in = 9 * (&l == &n->layers[0] ? 2 : l.cin);
+    const int fan_in = 9 * (&l == &n->layers[0] ? kInputChannels : l.cin);
     std::normal_distribution<float> nd(0.0f, std::sqrt(2.0f / fan_in));
     for (int tap = 0; tap < 9; ++tap)
       for (int co = 0; co < l.cout; ++co)
         for (int ci = 0; ci < l.cin; ++ci)
-          host[l.w_off + (static_cast<size_t>(tap) * l.cout + co) * l.cin + ci] = (&l == &n->layers[0] && ci >= 2) ? 0.0f : nd(gen);
+          host[l.w_off + (static_cast<size_t>(tap) * l.cout + co) * l.cin + ci] = (&l == &n->layers[0] && ci >= kInputChannels) ? 0.0f : nd(gen);
   }
   std::normal_distribution<float> nd_out(0.0f, std::sqrt(1.0f / 32.0f));
   for (int c = 0; c < 32; ++c) host[n->out_w_off + c] = nd_out(gen);
@@ -578,7 +639,7 @@ GG_API int gg_unet_create(int32_t batch, int32_t size, uint64_t seed, gg_unet** 
       return drop(rc);
   }
   const size_t SS = static_cast<size_t>(S) * S;
-  if ((rc = unet_alloc(n, &n->x0, B * SS * 16)) || (rc = unet_alloc(n, &n->pool1, B * SS / 4 * 32)) ||
+  if ((rc = unet_alloc(n, &n->x0, B * SS * 16)) || (rc = unet_alloc(n, &n->sat, B * 2 * (S + 1) * (S + 1))) || (rc = unet_alloc(n, &n->pool1, B * SS / 4 * 32)) ||
       (rc = unet_alloc(n, &n->pool2, B * SS / 16 * 64)) || (rc = unet_alloc(n, &n->pool3, B * SS / 64 * 128)) ||
       (rc = unet_alloc(n, &n->dpool1, B * SS / 4 * 32)) || (rc = unet_alloc(n, &n->dpool2, B * SS / 16 * 64)) ||
       (rc = unet_alloc(n, &n->dpool3, B * SS / 64 * 128)) || (rc = unet_alloc(n, &n->cat8, B * SS / 16 * 384)) ||

@@ -3,7 +3,9 @@
 A 4-level BF16 U-Net (include/ggems_b200.h, gg_unet_*; kernels in
 csrc/gg_unet.cu) maps two deterministic maps of a projection -- the primary
 transmission exp(-L) and the line integral L through the phantom
-(gg_line_integrals) -- to its scatter projection.  Training pairs come from
+(gg_line_integrals) -- to its scatter projection.  The network's fixed input
+stage adds wide box means and whole-image means of both maps, so every pixel
+sees the phantom-scale context that scatter depends on.  Training pairs come from
 the Monte Carlo itself: random phantoms at random angles, all run as the jobs
 of ONE batched launch (gg_run_jobs); each job's detector keeps a total and a
 scatter histogram, the scatter histogram is the target and
@@ -320,9 +322,18 @@ def relative_error(a, ref, blocks=16):
     return float(np.linalg.norm(a - ref) / max(np.linalg.norm(ref), 1e-30))
 
 
+def learning_rate(step, total, lr, warmup=100, floor=0.01):
+    """Linear warm-up over `warmup` steps, then cosine decay to floor * lr."""
+    if step < warmup:
+        return lr * (step + 1) / warmup
+    t = (step - warmup) / max(total - warmup, 1)
+    return lr * (floor + (1.0 - floor) * 0.5 * (1.0 + np.cos(np.pi * min(t, 1.0))))
+
+
 def train(net, inputs, targets, epochs, lr=1e-3, seed=0):
-    """Adam on (inputs, smoothed targets / their mean); the mean is kept in
-    net.target_scale and applied by predict()."""
+    """Adam on (inputs, smoothed targets / their mean) with a warm-up + cosine
+    learning-rate schedule; the mean is kept in net.target_scale and applied by
+    predict()."""
     import torch
     n = len(inputs)
     B = net.batch
@@ -332,14 +343,15 @@ def train(net, inputs, targets, epochs, lr=1e-3, seed=0):
     X = torch.from_numpy(inputs).cuda()
     Y = torch.from_numpy((targets / net.target_scale).astype(np.float32)).cuda()
     losses = []
+    per_epoch = n // B
+    total = epochs * per_epoch
     for epoch in range(epochs):
         order = rng.permutation(n)
         for s in range(0, n - B + 1, B):
             idx = torch.from_numpy(order[s:s + B]).cuda()
             xb = X.index_select(0, idx).contiguous()
             yb = Y.index_select(0, idx).contiguous()
-            rate = lr * (0.1 if epoch >= int(0.8 * epochs) else 1.0)
-            losses.append(net.train_step(xb, yb, rate))
+            losses.append(net.train_step(xb, yb, learning_rate(len(losses), total, lr)))
     return losses
 
 
@@ -361,7 +373,7 @@ def main(argv=None):
     ap.add_argument("--side", type=int, default=256)
     ap.add_argument("--pairs", type=int, default=2000)
     ap.add_argument("--primaries", type=float, default=1e8, help="primaries per training target")
-    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--test", type=int, default=16, help="test projections (new phantoms, random angles)")
     ap.add_argument("--judge-primaries", type=float, default=1e6)

@@ -28,6 +28,10 @@ typedef struct GGEMSVoxelizedPhantom GGEMSVoxelizedPhantom;
 typedef struct GGEMSMeshedPhantom GGEMSMeshedPhantom;
 typedef struct GGEMSCTSystem GGEMSCTSystem;
 typedef struct GGEMSWorld GGEMSWorld;
+typedef struct GGEMSVolumeCreatorManager GGEMSVolumeCreatorManager;
+typedef struct GGEMSBox GGEMSBox;
+typedef struct GGEMSTube GGEMSTube;
+typedef struct GGEMSSphere GGEMSSphere;
 typedef struct GGEMSDosimetryCalculator GGEMSDosimetryCalculator;
 typedef struct GGEMSMaterials GGEMSMaterials;
 typedef struct GGEMSAttenuations GGEMSAttenuations;
@@ -130,6 +134,40 @@ void energy_tracking_ggems_world(GGEMSWorld* w, bool is_activated);  /* include/
 void energy_squared_tracking_ggems_world(GGEMSWorld* w, bool is_activated);  /* include/GGEMS/navigators/GGEMSWorld.hh:276 */
 void set_output_ggems_world(GGEMSWorld* w, const char* basename);  /* include/GGEMS/navigators/GGEMSWorld.hh:284 */
 void momentum_ggems_world(GGEMSWorld* w, bool is_activated);  /* include/GGEMS/navigators/GGEMSWorld.hh:292 */
+
+/* Volume creator: analytic shapes drawn into a voxel image on the device,
+ * written as MHD plus a label -> material range file. */
+GGEMSVolumeCreatorManager* get_instance_volume_creator_manager(void);  /* include/GGEMS/geometries/GGEMSVolumeCreatorManager.hh:294 */
+void set_volume_dimension_volume_creator_manager(GGEMSVolumeCreatorManager* m, size_t width, size_t height, size_t depth);  /* include/GGEMS/geometries/GGEMSVolumeCreatorManager.hh:304 */
+void set_element_sizes_volume_creator_manager(GGEMSVolumeCreatorManager* m, float width, float height, float depth, const char* unit);  /* include/GGEMS/geometries/GGEMSVolumeCreatorManager.hh:315 */
+void set_output_image_filename_volume_creator_manager(GGEMSVolumeCreatorManager* m, const char* filename);  /* include/GGEMS/geometries/GGEMSVolumeCreatorManager.hh:323 */
+void set_output_range_to_material_filename_volume_creator_manager(GGEMSVolumeCreatorManager* m, const char* filename);  /* include/GGEMS/geometries/GGEMSVolumeCreatorManager.hh:331 */
+void initialize_volume_creator_manager(GGEMSVolumeCreatorManager* m);  /* include/GGEMS/geometries/GGEMSVolumeCreatorManager.hh:338 */
+void write_volume_creator_manager(GGEMSVolumeCreatorManager* m);  /* include/GGEMS/geometries/GGEMSVolumeCreatorManager.hh:345 */
+void set_material_volume_creator_manager(GGEMSVolumeCreatorManager* m, const char* material);  /* include/GGEMS/geometries/GGEMSVolumeCreatorManager.hh:353 */
+void set_data_type_volume_creator_manager(GGEMSVolumeCreatorManager* m, const char* data_type);  /* include/GGEMS/geometries/GGEMSVolumeCreatorManager.hh:361 */
+void clean_volume_creator_manager(GGEMSVolumeCreatorManager* m);  /* include/GGEMS/geometries/GGEMSVolumeCreatorManager.hh:368 */
+GGEMSBox* create_box(float width, float height, float depth, const char* unit);  /* include/GGEMS/geometries/GGEMSBox.hh:112 */
+void delete_box(GGEMSBox* box);  /* include/GGEMS/geometries/GGEMSBox.hh:119 */
+void set_position_box(GGEMSBox* box, float x, float y, float z, const char* unit);  /* include/GGEMS/geometries/GGEMSBox.hh:130 */
+void set_material_box(GGEMSBox* box, const char* material);  /* include/GGEMS/geometries/GGEMSBox.hh:138 */
+void set_label_value_box(GGEMSBox* box, float label_value);  /* include/GGEMS/geometries/GGEMSBox.hh:146 */
+void initialize_box(GGEMSBox* box);  /* include/GGEMS/geometries/GGEMSBox.hh:153 */
+void draw_box(GGEMSBox* box);  /* include/GGEMS/geometries/GGEMSBox.hh:160 */
+GGEMSTube* create_tube(float radius_x, float radius_y, float height, const char* unit);  /* include/GGEMS/geometries/GGEMSTube.hh:112 */
+void delete_tube(GGEMSTube* tube);  /* include/GGEMS/geometries/GGEMSTube.hh:119 */
+void set_position_tube(GGEMSTube* tube, float x, float y, float z, const char* unit);  /* include/GGEMS/geometries/GGEMSTube.hh:130 */
+void set_material_tube(GGEMSTube* tube, const char* material);  /* include/GGEMS/geometries/GGEMSTube.hh:138 */
+void set_label_value_tube(GGEMSTube* tube, float label_value);  /* include/GGEMS/geometries/GGEMSTube.hh:146 */
+void initialize_tube(GGEMSTube* tube);  /* include/GGEMS/geometries/GGEMSTube.hh:153 */
+void draw_tube(GGEMSTube* tube);  /* include/GGEMS/geometries/GGEMSTube.hh:160 */
+GGEMSSphere* create_sphere(float radius, const char* unit);  /* include/GGEMS/geometries/GGEMSSphere.hh:106 */
+void delete_sphere(GGEMSSphere* sphere);  /* include/GGEMS/geometries/GGEMSSphere.hh:113 */
+void set_position_sphere(GGEMSSphere* sphere, float x, float y, float z, const char* unit);  /* include/GGEMS/geometries/GGEMSSphere.hh:124 */
+void set_material_sphere(GGEMSSphere* sphere, const char* material);  /* include/GGEMS/geometries/GGEMSSphere.hh:132 */
+void set_label_value_sphere(GGEMSSphere* sphere, float label_value);  /* include/GGEMS/geometries/GGEMSSphere.hh:140 */
+void initialize_sphere(GGEMSSphere* sphere);  /* include/GGEMS/geometries/GGEMSSphere.hh:147 */
+void draw_sphere(GGEMSSphere* sphere);  /* include/GGEMS/geometries/GGEMSSphere.hh:154 */
 int ggems_build_mesh(const char* stl, const float* matrix, int depth, int32_t* n_triangles, int32_t* n_nodes, float* triangles, float* nodes, int32_t* node_first, int32_t* node_triangles, float* border_min, float* border_max);  /* no counterpart in the reference: B200 build addition */
 GGEMSCTSystem* create_ggems_ct_system(const char* name);  /* include/GGEMS/navigators/GGEMSCTSystem.hh:141 */
 void set_number_of_modules_ggems_ct_system(GGEMSCTSystem* c, uint64_t mx, uint64_t my);  /* include/GGEMS/navigators/GGEMSCTSystem.hh:150 */

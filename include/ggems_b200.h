@@ -372,6 +372,54 @@ GG_API int gg_compute_dose_no_alloc(gg_context* context, int32_t dose_map, int32
 /* ---- timing of the last gg_run_source (device time, ms) and launch count ---- */
 GG_API int gg_last_run_stats(gg_context* context, float* milliseconds, int64_t* kernel_launches);
 
+/* ---- phantom volumes on the device ----
+ * A voxel image of one MHD element type held in device memory: analytic shapes
+ * are drawn into it (GGEMSVolumeCreatorManager + GGEMSBox / GGEMSTube /
+ * GGEMSSphere, src/geometries/GGEMSVolumeCreatorManager.cc:229-294, kernels
+ * src/kernels/DrawGGEMS{Box,Tube,Sphere}.cl), and an image read from an MHD
+ * file is converted to material labels by a range table
+ * (GGEMSVoxelizedSolid::ConvertImageToLabel,
+ * include/GGEMS/geometries/GGEMSVoxelizedSolid.hh:162-257). */
+typedef enum gg_met_type {
+  GG_MET_CHAR = 0,
+  GG_MET_UCHAR = 1,
+  GG_MET_SHORT = 2,
+  GG_MET_USHORT = 3,
+  GG_MET_INT = 4,
+  GG_MET_UINT = 5,
+  GG_MET_FLOAT = 6
+} gg_met_type;
+
+typedef enum gg_shape_type { GG_SHAPE_BOX = 0, GG_SHAPE_TUBE = 1, GG_SHAPE_SPHERE = 2 } gg_shape_type;
+
+typedef struct gg_shape {
+  int32_t type;        /* gg_shape_type */
+  float position[3];   /* centre, mm, relative to the volume's centre */
+  float label_value;   /* written (converted to the element type) into covered voxels */
+  float size[3];       /* box: width (x), height (y), depth (z); tube: radius_x, radius_y,
+                          height (z); sphere: radius, -, -  (mm) */
+} gg_shape;
+
+typedef struct gg_volume gg_volume;
+/* Zero-filled volume of dimensions[0]*dimensions[1]*dimensions[2] elements on
+ * device device_index (GGEMSVolumeCreatorManager::Initialize). */
+GG_API int gg_volume_create(int32_t device_index, int32_t met_type, const int32_t dimensions[3],
+                            const float element_sizes[3], gg_volume** volume);
+GG_API int gg_volume_destroy(gg_volume* volume);
+/* Host <-> device copies of the whole image (bytes = elements * element size). */
+GG_API int gg_volume_upload(gg_volume* volume, const void* host_image, uint64_t bytes);
+GG_API int gg_volume_download(gg_volume* volume, void* host_image, uint64_t bytes);
+/* Draws the shapes in order, one launch each (GGEMSBox::Draw etc.).  GGEMS's
+ * voxel-index arithmetic is kept: its y index is (id mod dx*dx) / dx, so a
+ * volume whose x and y dimensions differ is drawn exactly as GGEMS draws it. */
+GG_API int gg_volume_draw(gg_volume* volume, const gg_shape* shapes, int32_t number_of_shapes);
+/* Range table -> uint8 labels (host array of all elements): the label of a
+ * voxel is the index of the LAST line whose range holds its value (value ==
+ * first == last, or first <= value < last, compared in float); voxels that no
+ * line holds keep 255 and are counted in *unconverted. */
+GG_API int gg_volume_labels(gg_volume* volume, const float* range_first, const float* range_last,
+                            int32_t number_of_ranges, uint8_t* labels, int64_t* unconverted);
+
 #ifdef __cplusplus
 }
 #endif

@@ -47,6 +47,12 @@ REF_KERNELS = [
      ["track_through_ggems_meshed_solid=track_through_ggems_meshed_solid_dosimetry"]),
     ("IsAlive", [], []),
     ("WorldTracking", [], []),
+    ("DrawGGEMSBox", ["MET_UCHAR"], []),
+    ("DrawGGEMSBox", ["MET_FLOAT"], ["draw_ggems_box=draw_ggems_box_float"]),
+    ("DrawGGEMSTube", ["MET_UCHAR"], []),
+    ("DrawGGEMSTube", ["MET_FLOAT"], ["draw_ggems_tube=draw_ggems_tube_float"]),
+    ("DrawGGEMSSphere", ["MET_UCHAR"], []),
+    ("DrawGGEMSSphere", ["MET_FLOAT"], ["draw_ggems_sphere=draw_ggems_sphere_float"]),
 ]
 
 
@@ -58,7 +64,8 @@ def build_oracle():
     os.makedirs(BUILD, exist_ok=True)
     out = os.path.join(BUILD, "libgg_oracle.so")
     run(CXX + ["-shared", "-I" + os.path.join(ROOT, "include"), os.path.join(HERE, "gg_oracle.cc"),
-               os.path.join(HERE, "gg_oracle_tables.cc"), os.path.join(HERE, "gg_oracle_mesh.cc"), "-o", out, "-lpthread"])
+               os.path.join(HERE, "gg_oracle_tables.cc"), os.path.join(HERE, "gg_oracle_mesh.cc"),
+               os.path.join(HERE, "gg_oracle_volume.cc"), "-o", out, "-lpthread"])
     return out
 
 

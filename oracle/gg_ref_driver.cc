@@ -68,6 +68,12 @@ void track_through_ggems_meshed_solid_dosimetry(ulong, GGEMSPrimaryParticles*, G
 void is_alive(ulong, GGEMSPrimaryParticles*, int*);
 void world_tracking(ulong, GGEMSPrimaryParticles*, int*, double*, double*, double*, double*, double*, ulong, ulong,
                     ulong, float, float, float);
+void draw_ggems_box(ulong, float3, int3, float3, float, float, float, float, uchar*);
+void draw_ggems_box_float(ulong, float3, int3, float3, float, float, float, float, float*);
+void draw_ggems_tube(ulong, float3, int3, float3, float, float, float, float, uchar*);
+void draw_ggems_tube_float(ulong, float3, int3, float3, float, float, float, float, float*);
+void draw_ggems_sphere(ulong, float3, int3, float3, float, float, uchar*);
+void draw_ggems_sphere_float(ulong, float3, int3, float3, float, float, float*);
 }
 
 namespace {
@@ -427,6 +433,37 @@ extern "C" __attribute__((visibility("default"))) int gg_ref_run(const gg_scene*
       particles->status[i] = P->status_[i];
       particles->scatter[i] = P->scatter_[i];
       particles->solid_id[i] = P->solid_id_[i];
+    }
+  }
+  return GG_OK;
+}
+
+// GGEMSBox / GGEMSTube / GGEMSSphere::Draw (src/geometries/GGEMSBox.cc, GGEMSTube.cc,
+// GGEMSSphere.cc): the reference's draw kernel of the shape over every voxel,
+// arguments in the order Draw sets them.  volume: MET_UCHAR or MET_FLOAT image.
+extern "C" __attribute__((visibility("default"))) int gg_ref_draw(void* volume, int32_t met_type, const int32_t dim[3],
+                                                                  const float es[3], const gg_shape* s) {
+  if (met_type != GG_MET_UCHAR && met_type != GG_MET_FLOAT) return GG_ERROR_INVALID_ARGUMENT;
+  const ulong n = static_cast<ulong>(dim[0]) * dim[1] * dim[2];
+  const float3 sizes(es[0], es[1], es[2]);
+  const int3 dims(dim[0], dim[1], dim[2]);
+  const float3 pos(s->position[0], s->position[1], s->position[2]);
+  const bool u8 = met_type == GG_MET_UCHAR;
+  uchar* vu = static_cast<uchar*>(volume);
+  float* vf = static_cast<float*>(volume);
+  for (ulong i = 0; i < n; ++i) {
+    gg_shim_global_id = i;
+    if (s->type == GG_SHAPE_BOX) {
+      // GGEMSBox::Draw: height_, width_, depth_
+      if (u8) draw_ggems_box(n, sizes, dims, pos, s->label_value, s->size[1], s->size[0], s->size[2], vu);
+      else draw_ggems_box_float(n, sizes, dims, pos, s->label_value, s->size[1], s->size[0], s->size[2], vf);
+    } else if (s->type == GG_SHAPE_TUBE) {
+      // GGEMSTube::Draw: height_, radius_x_, radius_y_
+      if (u8) draw_ggems_tube(n, sizes, dims, pos, s->label_value, s->size[2], s->size[0], s->size[1], vu);
+      else draw_ggems_tube_float(n, sizes, dims, pos, s->label_value, s->size[2], s->size[0], s->size[1], vf);
+    } else {
+      if (u8) draw_ggems_sphere(n, sizes, dims, pos, s->label_value, s->size[0], vu);
+      else draw_ggems_sphere_float(n, sizes, dims, pos, s->label_value, s->size[0], vf);
     }
   }
   return GG_OK;

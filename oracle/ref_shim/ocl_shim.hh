@@ -90,6 +90,7 @@ inline float3 operator*(float3 const& a, float s) { return float3(a.x * s, a.y *
 inline float3 operator*(float s, float3 const& a) { return float3(s * a.x, s * a.y, s * a.z); }
 inline float3 operator/(float3 const& a, float s) { return float3(a.x / s, a.y / s, a.z / s); }
 inline float3& operator+=(float3& a, float3 const& b) { a = a + b; return a; }
+inline float3& operator-=(float3& a, float3 const& b) { a = a - b; return a; }
 inline int3 operator-(int3 const& a, int s) { return int3(a.x - s, a.y - s, a.z - s); }
 
 inline float dot(float3 const& a, float3 const& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }

@@ -7,6 +7,11 @@ counterpart: GGEMS has no learned component, so this is the only checker.
 
 Parameter layout: for each of the 14 3x3 layers, W[tap][cout][cin] then
 b[cout]; then the 1x1 output layer w[32], b[1].
+
+Input stage: the 2 input maps (a, b) become 10 of the first layer's 16
+channels -- a, b, box means of a and of b over (2r+1)^2 windows (r = 4, 16,
+64; zero outside the image, divided by the full window area) and the means of
+a and b over the whole image.
 """
 
 import numpy as np
@@ -80,12 +85,37 @@ def up_backward(dy):
     return dy.reshape(B, H // 2, 2, W // 2, 2, C).sum(axis=(2, 4))
 
 
-def forward(params, inp):
-    """inp [B,S,S,2] -> (output [B,S,S], cache)."""
-    layers, wo, bo, _ = unpack(params)
+CONTEXT_RADII = (4, 16, 64)
+INPUT_CHANNELS = 2 + 2 * len(CONTEXT_RADII) + 2
+
+
+def box_mean(img, r):
+    """[B,S,S] -> window sums over (2r+1)^2 (zero padded) / (2r+1)^2."""
+    B, S, _ = img.shape
+    I = np.zeros((B, S + 1, S + 1))
+    I[:, 1:, 1:] = img.cumsum(1).cumsum(2)
+    lo = np.clip(np.arange(S) - r, 0, S)
+    hi = np.clip(np.arange(S) + r + 1, 0, S)
+    s = I[:, hi][:, :, hi] - I[:, lo][:, :, hi] - I[:, hi][:, :, lo] + I[:, lo][:, :, lo]
+    return s / float((2 * r + 1) ** 2)
+
+
+def input_stage(inp):
+    """[B,S,S,2] -> [B,S,S,16] first-layer input."""
     B, S, _, _ = inp.shape
     x0 = np.zeros((B, S, S, 16))
     x0[..., :2] = inp
+    for m in range(2):
+        for k, r in enumerate(CONTEXT_RADII):
+            x0[..., 2 + 3 * m + k] = box_mean(inp[..., m], r)
+        x0[..., 8 + m] = inp[..., m].mean(axis=(1, 2))[:, None, None]
+    return x0
+
+
+def forward(params, inp):
+    """inp [B,S,S,2] -> (output [B,S,S], cache)."""
+    layers, wo, bo, _ = unpack(params)
+    x0 = input_stage(np.asarray(inp, np.float64))
     acts, ins = [], []
 
     def conv(i, x):

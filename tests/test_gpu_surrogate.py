@@ -52,7 +52,7 @@ def test_unet_forward_and_gradients_match_oracle(torch):
     layers_r, wo_r, _, _ = uo.unpack(g_ref)
     for i, ((wg, bg), (wr, br)) in enumerate(zip(layers_g, layers_r)):
         if i == 0:
-            wg, wr = wg[:, :, :2], wr[:, :, :2]  # padded input channels carry no signal
+            wg, wr = wg[:, :, :uo.INPUT_CHANNELS], wr[:, :, :uo.INPUT_CHANNELS]  # padded input channels carry no signal
         for a, b in ((wg, wr), (bg, br)):
             rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
             cos = float((a * b).sum() / max(np.linalg.norm(a) * np.linalg.norm(b), 1e-30))

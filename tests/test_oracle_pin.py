@@ -173,3 +173,46 @@ def test_pin_world_tracking():
     src = scenes.XRaySource(spectrum=scenes.synthetic_spectrum(), aperture_deg=11.0)
     n = 20000
     _assert_identical(parity.run_oracle(sc, src, n), _run_ref(sc, src, n))
+
+
+def _shape(kind, pos, size, label):
+    s = abi.gg_shape()
+    s.type = kind
+    s.position[:] = [float(v) for v in pos]
+    s.size[:] = [float(v) for v in size]
+    s.label_value = float(label)
+    return s
+
+
+VOLUME_CASES = [
+    # dimensions (x, y, z), element sizes, shapes: GGEMS's y-index arithmetic is only
+    # right for x == y, so unequal x / y dimensions are included on purpose
+    ((40, 40, 24), (1.0, 1.0, 2.0), [(abi.GG_SHAPE_BOX, (0, 0, 0), (30, 20, 30), 1),
+                                     (abi.GG_SHAPE_TUBE, (3.5, -2.0, 4.0), (9.0, 6.0, 20.0), 2),
+                                     (abi.GG_SHAPE_SPHERE, (-8.0, 7.0, -5.0), (6.5, 0, 0), 3)]),
+    ((48, 32, 20), (0.5, 0.75, 1.0), [(abi.GG_SHAPE_BOX, (1.0, -1.0, 0.5), (12, 16, 10), 5),
+                                      (abi.GG_SHAPE_SPHERE, (0.25, 0.0, 0.0), (7.0, 0, 0), 7)]),
+    ((24, 36, 16), (2.0, 2.0, 2.0), [(abi.GG_SHAPE_TUBE, (0, 0, 0), (20.0, 14.0, 24.0), 9),
+                                     (abi.GG_SHAPE_SPHERE, (4.0, -6.0, 2.0), (8.0, 0, 0), 11)]),
+]
+
+
+def test_pin_volume_draw():
+    """Volume creator: the oracle draws boxes, tubes and spheres exactly as
+    GGEMS's DrawGGEMS{Box,Tube,Sphere}.cl do (uchar and float images)."""
+    ref = _ref_lib()
+    ref.gg_ref_draw.restype = C.c_int
+    ora = scenes.oracle()
+    for dims, es, shapes in VOLUME_CASES:
+        d = (C.c_int32 * 3)(*dims)
+        e = (C.c_float * 3)(*es)
+        for met, dt in ((abi.GG_MET_UCHAR, np.uint8), (abi.GG_MET_FLOAT, np.float32)):
+            a = np.zeros(int(np.prod(dims)), dt)
+            b = np.zeros_like(a)
+            for kind, pos, size, label in shapes:
+                s = _shape(kind, pos, size, label)
+                assert ora.gg_oracle_draw(a.ctypes.data_as(C.c_void_p), met, d, e, C.byref(s)) == 0
+                assert ref.gg_ref_draw(b.ctypes.data_as(C.c_void_p), met, d, e, C.byref(s)) == 0
+            assert np.array_equal(a, b), (dims, met)
+            labels = set(np.unique(a).tolist())
+            assert {0} < labels, labels

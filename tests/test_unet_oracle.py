@@ -15,7 +15,7 @@ def _random_params(seed):
     n = uo.parameter_count()
     p = rng.normal(0.0, 0.08, n)
     layers, wo, bo, _ = uo.unpack(p)
-    layers[0][0][:, :, 2:] = 0.0  # padded input channels
+    layers[0][0][:, :, uo.INPUT_CHANNELS:] = 0.0  # padded input channels
     for _, b in layers:
         b[:] = rng.uniform(0.01, 0.05, b.shape)  # keep units active
     return p
