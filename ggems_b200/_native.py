@@ -53,6 +53,7 @@ def _load():
         "gg_volume_draw": (C.c_int, [C.c_void_p, P(abi.gg_shape), C.c_int32]),
         "gg_volume_labels": (C.c_int, [C.c_void_p, P(C.c_float), P(C.c_float), C.c_int32, P(C.c_uint8),
                                        P(C.c_int64)]),
+        "gg_volume_last_kernel_ms": (C.c_int, [C.c_void_p, P(C.c_float)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -250,3 +251,8 @@ class Volume:
         check(lib.gg_volume_labels(self.handle, abi.ptr(f, C.c_float), abi.ptr(l_, C.c_float), len(f),
                                    abi.ptr(out, C.c_uint8), C.byref(missing)), "gg_volume_labels")
         return out, missing.value
+
+    def last_kernel_ms(self):
+        ms = C.c_float()
+        check(lib.gg_volume_last_kernel_ms(self.handle, C.byref(ms)), "gg_volume_last_kernel_ms")
+        return ms.value

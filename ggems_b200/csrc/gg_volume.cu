@@ -29,6 +29,12 @@ struct gg_volume {
   size_t element_bytes = 4;
   void* data = nullptr;
   cudaStream_t stream = nullptr;
+  // label conversion buffers, allocated on first use
+  uint8_t* labels = nullptr;
+  float* table = nullptr;  // [255] first, [255] last
+  unsigned long long* missing = nullptr;
+  cudaEvent_t start = nullptr, stop = nullptr;
+  float last_ms = 0.0f;  // device time of the last draw / label kernels
 };
 
 namespace {
@@ -191,6 +197,8 @@ GG_API int gg_volume_create(int32_t device_index, int32_t met_type, const int32_
   v->elements = n;
   v->element_bytes = eb;
   int rc = check(cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking), "cudaStreamCreateWithFlags");
+  if (rc == GG_OK) rc = check(cudaEventCreate(&v->start), "cudaEventCreate");
+  if (rc == GG_OK) rc = check(cudaEventCreate(&v->stop), "cudaEventCreate");
   if (rc == GG_OK) rc = check(cudaMalloc(&v->data, n * eb), "cudaMalloc");
   if (rc == GG_OK) rc = check(cudaMemsetAsync(v->data, 0, n * eb, v->stream), "cudaMemsetAsync");
   if (rc == GG_OK) rc = check(cudaStreamSynchronize(v->stream), "cudaStreamSynchronize");
@@ -207,6 +215,11 @@ GG_API int gg_volume_destroy(gg_volume* v) {
   cudaSetDevice(v->device);
   if (v->stream) cudaStreamSynchronize(v->stream);
   if (v->data) cudaFree(v->data);
+  if (v->labels) cudaFree(v->labels);
+  if (v->table) cudaFree(v->table);
+  if (v->missing) cudaFree(v->missing);
+  if (v->start) cudaEventDestroy(v->start);
+  if (v->stop) cudaEventDestroy(v->stop);
   if (v->stream) cudaStreamDestroy(v->stream);
   delete v;
   return GG_OK;
@@ -233,6 +246,7 @@ GG_API int gg_volume_download(gg_volume* v, void* host, uint64_t bytes) {
 GG_API int gg_volume_draw(gg_volume* v, const gg_shape* shapes, int32_t n) {
   if (!v || (n > 0 && !shapes) || n < 0) return gg::record_error(GG_ERROR_INVALID_ARGUMENT, "bad arguments");
   VOL_CUDA(cudaSetDevice(v->device));
+  VOL_CUDA(cudaEventRecord(v->start, v->stream));
   for (int32_t k = 0; k < n; ++k) {
     const gg_shape& s = shapes[k];
     if (s.type < GG_SHAPE_BOX || s.type > GG_SHAPE_SPHERE) return gg::record_error(GG_ERROR_INVALID_ARGUMENT, "unknown shape");
@@ -254,7 +268,9 @@ GG_API int gg_volume_draw(gg_volume* v, const gg_shape* shapes, int32_t n) {
     }
     VOL_CUDA(cudaGetLastError());
   }
+  VOL_CUDA(cudaEventRecord(v->stop, v->stream));
   VOL_CUDA(cudaStreamSynchronize(v->stream));
+  VOL_CUDA(cudaEventElapsedTime(&v->last_ms, v->start, v->stop));
   return GG_OK;
 }
 
@@ -263,41 +279,42 @@ GG_API int gg_volume_labels(gg_volume* v, const float* range_first, const float*
   if (!v || !labels || ranges < 0 || ranges > 255 || (ranges > 0 && (!range_first || !range_last)))
     return gg::record_error(GG_ERROR_INVALID_ARGUMENT, "bad arguments (at most 255 ranges)");
   VOL_CUDA(cudaSetDevice(v->device));
-  float* table = nullptr;
-  uint8_t* dlabels = nullptr;
-  unsigned long long* missing = nullptr;
-  auto release = [&]() {
-    if (table) cudaFree(table);
-    if (dlabels) cudaFree(dlabels);
-    if (missing) cudaFree(missing);
-  };
-  cudaError_t e = cudaMalloc(&table, 2 * static_cast<size_t>(ranges > 0 ? ranges : 1) * sizeof(float));
-  if (e == cudaSuccess) e = cudaMalloc(&dlabels, v->elements);
-  if (e == cudaSuccess) e = cudaMalloc(&missing, sizeof(unsigned long long));
-  if (e == cudaSuccess && ranges > 0)
-    e = cudaMemcpyAsync(table, range_first, ranges * sizeof(float), cudaMemcpyHostToDevice, v->stream);
-  if (e == cudaSuccess && ranges > 0)
-    e = cudaMemcpyAsync(table + ranges, range_last, ranges * sizeof(float), cudaMemcpyHostToDevice, v->stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(missing, 0, sizeof(unsigned long long), v->stream);
-  if (e == cudaSuccess) {
-    switch (v->met_type) {
-      case GG_MET_CHAR: launch_labels<int8_t>(v, table, table + ranges, ranges, dlabels, missing); break;
-      case GG_MET_UCHAR: launch_labels<uint8_t>(v, table, table + ranges, ranges, dlabels, missing); break;
-      case GG_MET_SHORT: launch_labels<int16_t>(v, table, table + ranges, ranges, dlabels, missing); break;
-      case GG_MET_USHORT: launch_labels<uint16_t>(v, table, table + ranges, ranges, dlabels, missing); break;
-      case GG_MET_INT: launch_labels<int32_t>(v, table, table + ranges, ranges, dlabels, missing); break;
-      case GG_MET_UINT: launch_labels<uint32_t>(v, table, table + ranges, ranges, dlabels, missing); break;
-      default: launch_labels<float>(v, table, table + ranges, ranges, dlabels, missing); break;
-    }
-    e = cudaGetLastError();
+  if (!v->labels) {
+    VOL_CUDA(cudaMalloc(&v->labels, v->elements));
+    VOL_CUDA(cudaMalloc(&v->table, 2 * 255 * sizeof(float)));
+    VOL_CUDA(cudaMalloc(&v->missing, sizeof(unsigned long long)));
   }
+  float* first = v->table;
+  float* last = v->table + ranges;
+  if (ranges > 0) {
+    VOL_CUDA(cudaMemcpyAsync(first, range_first, ranges * sizeof(float), cudaMemcpyHostToDevice, v->stream));
+    VOL_CUDA(cudaMemcpyAsync(last, range_last, ranges * sizeof(float), cudaMemcpyHostToDevice, v->stream));
+  }
+  VOL_CUDA(cudaMemsetAsync(v->missing, 0, sizeof(unsigned long long), v->stream));
+  VOL_CUDA(cudaEventRecord(v->start, v->stream));
+  switch (v->met_type) {
+    case GG_MET_CHAR: launch_labels<int8_t>(v, first, last, ranges, v->labels, v->missing); break;
+    case GG_MET_UCHAR: launch_labels<uint8_t>(v, first, last, ranges, v->labels, v->missing); break;
+    case GG_MET_SHORT: launch_labels<int16_t>(v, first, last, ranges, v->labels, v->missing); break;
+    case GG_MET_USHORT: launch_labels<uint16_t>(v, first, last, ranges, v->labels, v->missing); break;
+    case GG_MET_INT: launch_labels<int32_t>(v, first, last, ranges, v->labels, v->missing); break;
+    case GG_MET_UINT: launch_labels<uint32_t>(v, first, last, ranges, v->labels, v->missing); break;
+    default: launch_labels<float>(v, first, last, ranges, v->labels, v->missing); break;
+  }
+  VOL_CUDA(cudaGetLastError());
+  VOL_CUDA(cudaEventRecord(v->stop, v->stream));
   unsigned long long m = 0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(labels, dlabels, v->elements, cudaMemcpyDeviceToHost, v->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&m, missing, sizeof(m), cudaMemcpyDeviceToHost, v->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(v->stream);
-  release();
-  if (e != cudaSuccess) return check(e, "gg_volume_labels");
+  VOL_CUDA(cudaMemcpyAsync(labels, v->labels, v->elements, cudaMemcpyDeviceToHost, v->stream));
+  VOL_CUDA(cudaMemcpyAsync(&m, v->missing, sizeof(m), cudaMemcpyDeviceToHost, v->stream));
+  VOL_CUDA(cudaStreamSynchronize(v->stream));
+  VOL_CUDA(cudaEventElapsedTime(&v->last_ms, v->start, v->stop));
   if (unconverted) *unconverted = static_cast<int64_t>(m);
+  return GG_OK;
+}
+
+GG_API int gg_volume_last_kernel_ms(gg_volume* v, float* milliseconds) {
+  if (!v || !milliseconds) return gg::record_error(GG_ERROR_INVALID_ARGUMENT, "NULL argument");
+  *milliseconds = v->last_ms;
   return GG_OK;
 }
 

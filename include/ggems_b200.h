@@ -419,6 +419,9 @@ GG_API int gg_volume_draw(gg_volume* volume, const gg_shape* shapes, int32_t num
  * line holds keep 255 and are counted in *unconverted. */
 GG_API int gg_volume_labels(gg_volume* volume, const float* range_first, const float* range_last,
                             int32_t number_of_ranges, uint8_t* labels, int64_t* unconverted);
+/* Device time (CUDA events, ms) of the kernels of the last gg_volume_draw or
+ * gg_volume_labels call, copies excluded. */
+GG_API int gg_volume_last_kernel_ms(gg_volume* volume, float* milliseconds);
 
 #ifdef __cplusplus
 }
