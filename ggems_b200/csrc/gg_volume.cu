@@ -76,13 +76,24 @@ struct DrawParams {
 // (DrawGGEMSBox.cl:82-89): y = (id mod dx*dx) / dx, x = id mod (dx*dy) - y*dx
 // (size_t arithmetic, then int), z = id / (dx*dy); centre =
 // (es/2) * ((1 - dim) + 2*index) - position.
+// Volumes below 2^32 elements (all practical ones) take the same arithmetic in
+// 32 bits, where every intermediate fits and the results are identical.
 __device__ __forceinline__ void voxel_centre(const DrawParams& p, uint64_t id, float c[3]) {
   const int dx = p.dim[0], dy = p.dim[1];
-  const uint64_t sq = static_cast<uint64_t>(static_cast<int64_t>(dx * dx));
-  const uint64_t plane = static_cast<uint64_t>(static_cast<int64_t>(dx * dy));
-  const int iy = static_cast<int>((id % sq) / static_cast<uint64_t>(static_cast<int64_t>(dx)));
-  const int ix = static_cast<int>((id % plane) - static_cast<uint64_t>(static_cast<int64_t>(iy * dx)));
-  const int iz = static_cast<int>(id / plane);
+  int ix, iy, iz;
+  if (p.elements <= 0xffffffffull) {
+    const uint32_t i = static_cast<uint32_t>(id);
+    const uint32_t sq = static_cast<uint32_t>(dx * dx), plane = static_cast<uint32_t>(dx * dy);
+    iy = static_cast<int>((i % sq) / static_cast<uint32_t>(dx));
+    ix = static_cast<int>(static_cast<uint64_t>(i % plane) - static_cast<uint64_t>(static_cast<int64_t>(iy * dx)));
+    iz = static_cast<int>(i / plane);
+  } else {
+    const uint64_t sq = static_cast<uint64_t>(static_cast<int64_t>(dx * dx));
+    const uint64_t plane = static_cast<uint64_t>(static_cast<int64_t>(dx * dy));
+    iy = static_cast<int>((id % sq) / static_cast<uint64_t>(static_cast<int64_t>(dx)));
+    ix = static_cast<int>((id % plane) - static_cast<uint64_t>(static_cast<int64_t>(iy * dx)));
+    iz = static_cast<int>(id / plane);
+  }
   const int idx[3] = {ix, iy, iz};
   for (int a = 0; a < 3; ++a) {
     const float half = p.es[a] / 2.0f;
@@ -117,6 +128,19 @@ __global__ void draw_kernel(T* __restrict__ volume, DrawParams p) {
 
 // The LAST range line holding the value gives the label (the reference
 // rewrites the whole image once per line, in file order); 255 = none.
+__device__ __forceinline__ int range_label(float v, const float* table, int ranges) {
+  for (int r = ranges - 1; r >= 0; --r) {
+    const float a = table[r], b = table[ranges + r];
+    if ((v == a && v == b) || (v >= a && v < b)) return r;
+  }
+  return 255;
+}
+
+// Each thread converts chunks of 16 elements: sizeof(T) 16-byte streaming
+// loads in, one 16-byte store of labels out (the image and the labels are
+// touched once, so both bypass L2 residency with the .cs hint); the last
+// elements % 16 go one per thread.  Both arrays come from cudaMalloc, so every
+// chunk is 16-byte aligned.
 template <class T>
 __global__ void labels_kernel(const T* __restrict__ image, uint64_t elements, const float* __restrict__ first,
                               const float* __restrict__ last, int ranges, uint8_t* __restrict__ labels,
@@ -128,17 +152,31 @@ __global__ void labels_kernel(const T* __restrict__ image, uint64_t elements, co
   }
   __syncthreads();
   unsigned long long missing = 0;
+  const uint64_t tid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < elements; i += stride) {
-    const float v = static_cast<float>(image[i]);
-    int label = 255;
-    for (int r = ranges - 1; r >= 0; --r) {
-      const float a = table[r], b = table[ranges + r];
-      if ((v == a && v == b) || (v >= a && v < b)) {
-        label = r;
-        break;
-      }
+  const uint64_t chunks = elements / 16;
+  for (uint64_t c = tid; c < chunks; c += stride) {
+    union {
+      uint4 q[sizeof(T)];
+      T e[16];
+    } in;
+    const uint4* src = reinterpret_cast<const uint4*>(image + c * 16);
+#pragma unroll
+    for (int k = 0; k < static_cast<int>(sizeof(T)); ++k) in.q[k] = __ldcs(src + k);
+    union {
+      uint4 q;
+      uint8_t b[16];
+    } out;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int label = range_label(static_cast<float>(in.e[j]), table, ranges);
+      out.b[j] = static_cast<uint8_t>(label);
+      missing += label == 255;
     }
+    __stcs(reinterpret_cast<uint4*>(labels + c * 16), out.q);
+  }
+  for (uint64_t i = chunks * 16 + tid; i < elements; i += stride) {
+    const int label = range_label(static_cast<float>(image[i]), table, ranges);
     labels[i] = static_cast<uint8_t>(label);
     missing += label == 255;
   }
@@ -149,7 +187,7 @@ __global__ void labels_kernel(const T* __restrict__ image, uint64_t elements, co
 int grid_for(const gg_volume* v) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, v->device);
-  const uint64_t blocks = (v->elements + 255) / 256;
+  const uint64_t blocks = (v->elements / 16 + 255) / 256;
   const uint64_t cap = static_cast<uint64_t>(sms) * 8;
   return static_cast<int>(blocks < cap ? (blocks ? blocks : 1) : cap);
 }
