@@ -18,7 +18,8 @@ Geometry (the small water-phantom configuration): 64^3 voxels of 2 mm, random
 water ellipsoid with bone and air inserts, 60 keV cone (10 deg) at 1000 mm,
 flat GOS panel of side x side elements covering 256 mm at 1500 mm.
 
-    python -m ggems_b200.scatter --pairs 2000 --primaries 100000000   # train + evaluate, JSON line
+    python -m ggems_b200.scatter --pairs 2000 --primaries 1e8 --save net.npz   # train + evaluate, JSON line
+    python -m ggems_b200.scatter --load net.npz                                # evaluate a trained network
 """
 
 import argparse
@@ -368,6 +369,36 @@ def predict(net, inputs):
     return np.concatenate(out)
 
 
+def save_network(net, path):
+    np.savez(path, parameters=net.parameters(), target_scale=np.float64(getattr(net, "target_scale", 1.0)))
+
+
+def load_network(net, path):
+    z = np.load(path)
+    net.set_parameters(z["parameters"])
+    net.target_scale = float(z["target_scale"])
+
+
+def surrogate_pipeline(geo, net, projections, judge_primaries, seed):
+    """The surrogate at inference: per projection the deterministic inputs and
+    the network's scatter estimate, the low-count plain-MC estimate of all
+    projections (one batched launch per chunk of jobs) and the 5 % judge.
+    Returns (final, prediction, low-count MC, kept flags, seconds)."""
+    import torch
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    x = make_inputs(geo, projections)
+    pred = predict(net, x)
+    low = []
+    for s in range(0, len(projections), 64):
+        _, sc = geo.simulate(projections[s:s + 64], int(judge_primaries), seed=seed + s)
+        low.append(sc)
+    low = normalise(np.concatenate(low), judge_primaries, geo.side)
+    final, used = judge(pred, low)
+    torch.cuda.synchronize()
+    return final, pred, low, used, time.perf_counter() - t0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--side", type=int, default=256)
@@ -376,11 +407,15 @@ def main(argv=None):
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--test", type=int, default=16, help="test projections (new phantoms, random angles)")
+    ap.add_argument("--angles", type=int, default=360, help="inference angles of one new phantom")
+    ap.add_argument("--reference-every", type=int, default=10, help="1e9-primary reference on every n-th angle")
     ap.add_argument("--judge-primaries", type=float, default=1e6)
     ap.add_argument("--reference-primaries", type=float, default=1e9)
     ap.add_argument("--chunk", type=int, default=64, help="projections per batched MC launch")
+    ap.add_argument("--save", help="write the trained network (.npz)")
+    ap.add_argument("--load", help="skip data generation and training: load a trained network (.npz)")
     args = ap.parse_args(argv)
-    import torch  # noqa: F401  (CUDA memory for the network's device arrays)
+    import torch  # (CUDA memory for the network's device arrays)
     work = tempfile.mkdtemp(prefix="ggems_scatter_")
     geo = Geometry(args.side, work)
     rng = np.random.default_rng(11)
@@ -395,51 +430,72 @@ def main(argv=None):
             ms += geo.last_ms
         return np.concatenate(tot), np.concatenate(sca), ms
 
-    t0 = time.time()
-    train_projs = [(float(rng.uniform(0, 360)), random_phantom(rng)) for _ in range(args.pairs)]
-    _, s_train, mc_ms = simulate_all(train_projs, args.primaries)
-    x_train = make_inputs(geo, train_projs)
-    y_train = normalise(s_train, args.primaries, side)
-    t_data = time.time() - t0
     net = UNet(args.batch, side, seed=3)
-    t0 = time.time()
-    losses = train(net, x_train, y_train, args.epochs)
-    t_train = time.time() - t0
-    # evaluation on new phantoms
+    t_data = t_train = mc_ms = 0.0
+    losses = []
+    if args.load:
+        load_network(net, args.load)
+    else:
+        t0 = time.time()
+        train_projs = [(float(rng.uniform(0, 360)), random_phantom(rng)) for _ in range(args.pairs)]
+        _, s_train, mc_ms = simulate_all(train_projs, args.primaries)
+        x_train = make_inputs(geo, train_projs)
+        y_train = normalise(s_train, args.primaries, side)
+        t_data = time.time() - t0
+        del train_projs
+        t0 = time.time()
+        losses = train(net, x_train, y_train, args.epochs)
+        t_train = time.time() - t0
+        del x_train, y_train
+        if args.save:
+            save_network(net, args.save)
+    # (1) new phantoms at random angles
     test_projs = [(float(rng.uniform(0, 360)), random_phantom(rng)) for _ in range(args.test)]
-    _, s_ref, ref_ms = simulate_all(test_projs, args.reference_primaries)
+    _, s_ref, _ = simulate_all(test_projs, args.reference_primaries)
     ref = normalise(s_ref, args.reference_primaries, side)
-    _, s_low, low_ms = simulate_all(test_projs, args.judge_primaries)
-    low = normalise(s_low, args.judge_primaries, side)
-    t0 = time.time()
-    x_test = make_inputs(geo, test_projs)
-    t_inputs = (time.time() - t0) / args.test
-    import torch
+    final, pred, low, used, _ = surrogate_pipeline(geo, net, test_projs, args.judge_primaries, 1234)
+    err_sur = [relative_error(f, r) for f, r in zip(final, ref)]
+    err_net = [relative_error(p, r) for p, r in zip(pred, ref)]
+    err_low = [relative_error(m, r) for m, r in zip(low, ref)]
+    # (2) a CBCT scan: one new phantom, `angles` projections through the whole pipeline
+    phantom = random_phantom(rng)
+    scan = [(360.0 * k / args.angles, phantom) for k in range(args.angles)]
+    surrogate_pipeline(geo, net, scan[:8], args.judge_primaries, 99)  # warm-up
+    s_final, s_pred, s_low, s_used, t_scan = surrogate_pipeline(geo, net, scan, args.judge_primaries, 4321)
+    picked = list(range(0, args.angles, args.reference_every))
+    _, s_ref_scan, _ = simulate_all([scan[k] for k in picked], args.reference_primaries)
+    ref_scan = normalise(s_ref_scan, args.reference_primaries, side)
+    scan_err = [relative_error(s_final[k], r) for k, r in zip(picked, ref_scan)]
+    scan_low = [relative_error(s_low[k], r) for k, r in zip(picked, ref_scan)]
+    # plain MC: primaries for 5 % error by Poisson scaling of the low-count error; its
+    # projections/s timed directly on 16 scan angles at that count (one batched launch)
+    e_low = float(np.mean(scan_low))
+    n_plain = args.judge_primaries * (e_low / 0.05) ** 2
     torch.cuda.synchronize()
-    t0 = time.time()
-    pred = predict(net, x_test)
-    torch.cuda.synchronize()
-    t_net = (time.time() - t0) / args.test
-    final, used = judge(pred, low)
-    err_sur = float(np.mean([relative_error(f, r) for f, r in zip(final, ref)]))
-    err_net = float(np.mean([relative_error(p, r) for p, r in zip(pred, ref)]))
-    err_low = float(np.mean([relative_error(m, r) for m, r in zip(low, ref)]))
-    # plain MC needs N with err ~ err_low * sqrt(judge / N) <= 5 %  (Poisson scaling)
-    n_plain = args.judge_primaries * (err_low / 0.05) ** 2
-    rate = args.test * args.judge_primaries / (low_ms * 1e-3)
-    t_plain = n_plain / rate
-    t_sur = args.judge_primaries / rate + t_net + t_inputs
+    t0 = time.perf_counter()
+    _, s_plain, _ = simulate_all(scan[:16], n_plain)
+    t_plain = time.perf_counter() - t0
+    plain_err = [relative_error(normalise(s_plain[k], n_plain, side), ref_scan[k // args.reference_every])
+                 for k in range(0, 16, args.reference_every)]
+    rate = 16 * n_plain / t_plain
+    plain_per_s = 16 / t_plain
+    sur_per_s = args.angles / t_scan
     print(json.dumps({
         "metric": "scatter projections/s (surrogate + 1e6-primary MC judge vs plain MC at <=5% error)",
-        "surrogate_projections_per_s": 1.0 / t_sur, "plain_mc_projections_per_s": 1.0 / t_plain,
-        "speedup": t_plain / t_sur, "surrogate_error": err_sur, "network_error": err_net,
-        "low_count_mc_error": err_low, "judge_accepted": float(used.mean()),
-        "plain_mc_primaries_for_5pct": n_plain, "mc_primaries_per_s": rate,
+        "surrogate_projections_per_s": sur_per_s, "plain_mc_projections_per_s": plain_per_s,
+        "speedup": sur_per_s / plain_per_s,
+        "scan": {"angles": args.angles, "seconds": t_scan, "judge_kept": float(s_used.mean()),
+                 "error_mean": float(np.mean(scan_err)), "error_max": float(np.max(scan_err)),
+                 "low_count_mc_error": e_low, "reference_angles": len(picked)},
+        "new_phantoms": {"projections": args.test, "network_error": float(np.mean(err_net)),
+                         "judged_error": float(np.mean(err_sur)), "judged_error_max": float(np.max(err_sur)),
+                         "low_count_mc_error": float(np.mean(err_low)), "judge_kept": float(used.mean())},
+        "plain_mc_primaries_for_5pct": n_plain, "plain_mc_error": float(np.mean(plain_err)),
+        "mc_primaries_per_s": rate,
         "config": {"side": side, "pairs": args.pairs, "target_primaries": args.primaries, "epochs": args.epochs,
-                   "test": args.test, "judge_primaries": args.judge_primaries,
-                   "reference_primaries": args.reference_primaries},
-        "times_s": {"data": t_data, "train": t_train, "network_per_projection": t_net,
-                    "inputs_per_projection": t_inputs, "train_mc_ms": mc_ms},
+                   "judge_primaries": args.judge_primaries, "reference_primaries": args.reference_primaries,
+                   "loaded": bool(args.load)},
+        "times_s": {"data": t_data, "train": t_train, "train_mc_ms": mc_ms},
         "final_loss": float(np.mean(losses[-20:])) if losses else None}), flush=True)
     net.close()
     return 0
