@@ -17,6 +17,7 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <type_traits>
 
 #include "gg_internal.cuh"
 
@@ -32,6 +33,7 @@ struct gg_volume {
   // label conversion buffers, allocated on first use
   uint8_t* labels = nullptr;
   float* table = nullptr;  // [255] first, [255] last
+  uint8_t* lut = nullptr;  // label of every value of an 8- or 16-bit element type
   unsigned long long* missing = nullptr;
   cudaEvent_t start = nullptr, stop = nullptr;
   float last_ms = 0.0f;  // device time of the last draw / label kernels
@@ -184,6 +186,91 @@ __global__ void labels_kernel(const T* __restrict__ image, uint64_t elements, co
   if ((threadIdx.x & 31) == 0 && missing) atomicAdd(unconverted, missing);
 }
 
+template <class T>
+__host__ __device__ constexpr int lowest_value() {
+  return std::is_signed<T>::value ? -(1 << (8 * sizeof(T) - 1)) : 0;
+}
+
+// 8- and 16-bit images: the label of every representable value is computed
+// once (range_label on its float value, as above), and the image pass is a
+// table lookup in shared memory.
+template <class T>
+__global__ void label_table_kernel(const float* __restrict__ first, const float* __restrict__ last, int ranges,
+                                   uint8_t* __restrict__ lut) {
+  __shared__ float table[2 * 255];
+  for (int i = threadIdx.x; i < ranges; i += blockDim.x) {
+    table[i] = first[i];
+    table[ranges + i] = last[i];
+  }
+  __syncthreads();
+  constexpr int kValues = 1 << (8 * sizeof(T));
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kValues) return;
+  // index i holds value i + lowest (two's complement offset for signed types)
+  const T value = static_cast<T>(i + lowest_value<T>());
+  lut[i] = static_cast<uint8_t>(range_label(static_cast<float>(value), table, ranges));
+}
+
+// Two 16-element chunks per thread and iteration, so that 2 * 16 * sizeof(T)
+// bytes per thread are in flight before the lookups.
+template <class T>
+__global__ void __launch_bounds__(512) labels_lut_kernel(const T* __restrict__ image, uint64_t elements,
+                                                          const uint8_t* __restrict__ lut, uint8_t* __restrict__ labels,
+                                                          unsigned long long* __restrict__ unconverted) {
+  constexpr int kValues = 1 << (8 * sizeof(T));
+  extern __shared__ uint4 lut_words[];
+  uint8_t* table = reinterpret_cast<uint8_t*>(lut_words);
+  for (int i = threadIdx.x; i < kValues / 16; i += blockDim.x) lut_words[i] = reinterpret_cast<const uint4*>(lut)[i];
+  __syncthreads();
+  constexpr int kLowest = lowest_value<T>();
+  unsigned long long missing = 0;
+  const uint64_t tid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  const uint64_t chunks = elements / 16;
+  union Chunk {
+    uint4 q[sizeof(T)];
+    T e[16];
+  };
+  union Out {
+    uint4 q;
+    uint8_t b[16];
+  };
+  for (uint64_t c = tid; c < chunks; c += 2 * stride) {
+    const bool two = c + stride < chunks;
+    Chunk in0, in1;
+    const uint4* s0 = reinterpret_cast<const uint4*>(image + c * 16);
+#pragma unroll
+    for (int k = 0; k < static_cast<int>(sizeof(T)); ++k) in0.q[k] = __ldcs(s0 + k);
+    if (two) {
+      const uint4* s1 = reinterpret_cast<const uint4*>(image + (c + stride) * 16);
+#pragma unroll
+      for (int k = 0; k < static_cast<int>(sizeof(T)); ++k) in1.q[k] = __ldcs(s1 + k);
+    }
+    Out o0, o1;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      o0.b[j] = table[static_cast<int>(in0.e[j]) - kLowest];
+      missing += o0.b[j] == 255;
+    }
+    __stcs(reinterpret_cast<uint4*>(labels + c * 16), o0.q);
+    if (two) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        o1.b[j] = table[static_cast<int>(in1.e[j]) - kLowest];
+        missing += o1.b[j] == 255;
+      }
+      __stcs(reinterpret_cast<uint4*>(labels + (c + stride) * 16), o1.q);
+    }
+  }
+  for (uint64_t i = chunks * 16 + tid; i < elements; i += stride) {
+    const uint8_t l = table[static_cast<int>(image[i]) - kLowest];
+    labels[i] = l;
+    missing += l == 255;
+  }
+  for (int o = 16; o > 0; o >>= 1) missing += __shfl_down_sync(0xffffffffu, missing, o);
+  if ((threadIdx.x & 31) == 0 && missing) atomicAdd(unconverted, missing);
+}
+
 int grid_for(const gg_volume* v) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, v->device);
@@ -204,6 +291,18 @@ void launch_draw(gg_volume* v, const DrawParams& p, int shape) {
 template <class T>
 void launch_labels(gg_volume* v, const float* first, const float* last, int ranges, uint8_t* labels,
                    unsigned long long* missing) {
+  if constexpr (sizeof(T) <= 2) {
+    constexpr int kValues = 1 << (8 * sizeof(T));
+    label_table_kernel<T><<<(kValues + 255) / 256, 256, 0, v->stream>>>(first, last, ranges, v->lut);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, v->device);
+    const uint64_t blocks = (v->elements / 32 + 511) / 512;
+    const int grid = static_cast<int>(blocks < static_cast<uint64_t>(2 * sms) ? (blocks ? blocks : 1) : 2 * sms);
+    cudaFuncSetAttribute(labels_lut_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kValues);
+    labels_lut_kernel<T><<<grid, 512, kValues, v->stream>>>(static_cast<const T*>(v->data), v->elements, v->lut, labels,
+                                                             missing);
+    return;
+  }
   labels_kernel<T><<<grid_for(v), 256, 2 * ranges * sizeof(float), v->stream>>>(
       static_cast<const T*>(v->data), v->elements, first, last, ranges, labels, missing);
 }
@@ -255,6 +354,7 @@ GG_API int gg_volume_destroy(gg_volume* v) {
   if (v->data) cudaFree(v->data);
   if (v->labels) cudaFree(v->labels);
   if (v->table) cudaFree(v->table);
+  if (v->lut) cudaFree(v->lut);
   if (v->missing) cudaFree(v->missing);
   if (v->start) cudaEventDestroy(v->start);
   if (v->stop) cudaEventDestroy(v->stop);
@@ -321,6 +421,7 @@ GG_API int gg_volume_labels(gg_volume* v, const float* range_first, const float*
     VOL_CUDA(cudaMalloc(&v->labels, v->elements));
     VOL_CUDA(cudaMalloc(&v->table, 2 * 255 * sizeof(float)));
     VOL_CUDA(cudaMalloc(&v->missing, sizeof(unsigned long long)));
+    VOL_CUDA(cudaMalloc(&v->lut, 65536));
   }
   float* first = v->table;
   float* last = v->table + ranges;

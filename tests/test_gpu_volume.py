@@ -74,6 +74,9 @@ def test_labels_match_oracle():
         (abi.GG_MET_FLOAT, rng.uniform(-2, 2, n).astype(np.float32), [-2.0, -0.5, 0.0, 1.0], [-0.5, 0.5, 1.0, 1.5]),
         (abi.GG_MET_INT, rng.integers(-5, 5, n).astype(np.int32), [-5, -1, 0, 0], [0, 3, 1, 0]),
         (abi.GG_MET_UINT, rng.integers(0, 70000, n).astype(np.uint32), [0, 1000, 60000], [1000, 60000, 70000]),
+        (abi.GG_MET_CHAR, rng.integers(-128, 128, n).astype(np.int8), [-128, -20, 0, 50], [-20, 0, 50, 100]),
+        (abi.GG_MET_USHORT, rng.integers(0, 65536, n).astype(np.uint16), [0, 100, 30000, 65535],
+         [100, 30000, 65535, 65535]),
     ]
     for met, img, first, last in cases:
         v = Volume(met, dims, (1.0, 1.0, 1.0))
