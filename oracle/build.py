@@ -66,6 +66,9 @@ def build_oracle():
     run(CXX + ["-shared", "-I" + os.path.join(ROOT, "include"), os.path.join(HERE, "gg_oracle.cc"),
                os.path.join(HERE, "gg_oracle_tables.cc"), os.path.join(HERE, "gg_oracle_mesh.cc"),
                os.path.join(HERE, "gg_oracle_volume.cc"), "-o", out, "-lpthread"])
+    # the same transport restatement in FP64 (precision reference for the results)
+    run(CXX + ["-shared", "-DGG_ORACLE_REAL=double", "-I" + os.path.join(ROOT, "include"),
+               os.path.join(HERE, "gg_oracle.cc"), "-o", os.path.join(BUILD, "libgg_oracle_fp64.so"), "-lpthread"])
     return out
 
 

@@ -23,26 +23,36 @@
 
 #include "ggems_b200.h"
 
+// Arithmetic type of the restatement: float (the reference's precision, pinned
+// bit for bit against its kernels) or, built with -DGG_ORACLE_REAL=double, the
+// same algorithm in FP64 (the reference's float constants kept) -- the FP64
+// oracle the CUDA results' precision is measured against.
+#ifndef GG_ORACLE_REAL
+#define GG_ORACLE_REAL float
+#endif
+
 namespace {
 
-constexpr float kTwoPi = 6.283185307179586f;            // GGEMSConstants.hh:39
-constexpr float kElectronMassC2 = 0.510998910f;          // GGEMSConstants.hh:52
-constexpr float kGeometryTolerance = 5.0e-04f;           // GGEMSGeometryConstants.hh:39
-constexpr float kEpsilon6 = 1.0e-06f;                    // GGEMSGeometryConstants.hh:38
-constexpr float kOutOfWorld = FLT_MAX;                   // GGEMSParticleConstants.hh:44
+using Real = GG_ORACLE_REAL;
+
+constexpr Real kTwoPi = 6.283185307179586f;            // GGEMSConstants.hh:39
+constexpr Real kElectronMassC2 = 0.510998910f;          // GGEMSConstants.hh:52
+constexpr Real kGeometryTolerance = 5.0e-04f;           // GGEMSGeometryConstants.hh:39
+constexpr Real kEpsilon6 = 1.0e-06f;                    // GGEMSGeometryConstants.hh:38
+constexpr Real kOutOfWorld = FLT_MAX;                   // GGEMSParticleConstants.hh:44
 constexpr int8_t kNoProcess = 99;                        // GGEMSProcessConstants.hh:37
-constexpr float kRayleighFactor = 32526509815670243328.0f;  // GGEMSRayleighScatteringModels.hh:36
+constexpr Real kRayleighFactor = 32526509815670243328.0f;  // GGEMSRayleighScatteringModels.hh:36
 
 struct V3 {
-  float x, y, z;
+  Real x, y, z;
 };
-inline V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+inline V3 v3(Real x, Real y, Real z) { return V3{x, y, z}; }
 inline V3 add(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
 inline V3 sub(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
 inline V3 mul(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
 inline V3 divv(V3 a, V3 b) { return v3(a.x / b.x, a.y / b.y, a.z / b.z); }
-inline V3 scale(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
-inline float dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 scale(V3 a, Real s) { return v3(a.x * s, a.y * s, a.z * s); }
+inline Real dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 // normalize: v * (1 / sqrt(dot(v, v))), the convention fixed for OpenCL's builtin.
 inline V3 normalize3(V3 v) { return scale(v, 1.0f / std::sqrt(dot3(v, v))); }
 
@@ -70,10 +80,10 @@ inline V3 local_to_global_direction(const float* m, V3 d) { return normalize3(ma
 
 // RotateUnitZ (GGEMSReferentialTransformation.hh:44-70, CLHEP rotateUz).
 inline V3 rotate_unit_z(V3 v, V3 u) {
-  float up = u.x * u.x + u.y * u.y;
+  Real up = u.x * u.x + u.y * u.y;
   if (up > 0) {
     up = std::sqrt(up);
-    float px = v.x, py = v.y, pz = v.z;
+    Real px = v.x, py = v.y, pz = v.z;
     v.x = (u.x * u.z * px - u.y * py) / up + u.x * pz;
     v.y = (u.y * u.z * px + u.x * py) / up + u.y * pz;
     v.z = -up * px + u.z * pz;
@@ -85,7 +95,7 @@ inline V3 rotate_unit_z(V3 v, V3 u) {
 }
 
 // BinarySearch / LinearInterpolation (GGEMSMathAlgorithms.hh:46-86).
-inline int binary_search(float key, const float* a, int size) {
+inline int binary_search(Real key, const float* a, int size) {
   int low = 0, mid = 0, high = size - 1;
   while (high - low > 1) {
     mid = (high + low) / 2;
@@ -95,7 +105,7 @@ inline int binary_search(float key, const float* a, int size) {
   }
   return low;
 }
-inline float linear_interpolation(float xa, float ya, float xb, float yb, float x) {
+inline Real linear_interpolation(Real xa, Real ya, Real xb, Real yb, Real x) {
   if (xa > xb) return yb;
   if (xa >= x) return ya;
   if (xb <= x) return yb;
@@ -104,7 +114,7 @@ inline float linear_interpolation(float xa, float ya, float xb, float yb, float 
 
 // Ray tracing (GGEMSRayTracing.hh:60-326).
 inline void safety_inside_aabb(V3& p, V3 mn, V3 mx) {
-  float a = std::fabs(p.x - mn.x), b = std::fabs(p.x - mx.x);
+  Real a = std::fabs(p.x - mn.x), b = std::fabs(p.x - mx.x);
   p.x = (a < kGeometryTolerance) ? mn.x + kGeometryTolerance : p.x;
   p.x = (b < kGeometryTolerance) ? mx.x - kGeometryTolerance : p.x;
   a = std::fabs(p.y - mn.y); b = std::fabs(p.y - mx.y);
@@ -115,7 +125,7 @@ inline void safety_inside_aabb(V3& p, V3 mn, V3 mx) {
   p.z = (b < kGeometryTolerance) ? mx.z - kGeometryTolerance : p.z;
 }
 inline void safety_outside_aabb(V3& p, V3 mn, V3 mx) {
-  float a = std::fabs(p.x - mn.x), b = std::fabs(p.x - mx.x);
+  Real a = std::fabs(p.x - mn.x), b = std::fabs(p.x - mx.x);
   p.x = (a < kGeometryTolerance) ? mn.x - kGeometryTolerance : p.x;
   p.x = (b < kGeometryTolerance) ? mx.x + kGeometryTolerance : p.x;
   a = std::fabs(p.y - mn.y); b = std::fabs(p.y - mx.y);
@@ -131,12 +141,12 @@ inline bool in_aabb(V3 p, V3 mn, V3 mx) {
   if (p.z < (mn.z + kGeometryTolerance) || p.z > (mx.z - kGeometryTolerance)) return false;
   return true;
 }
-inline float distance_to_aabb(V3 p, V3 d, V3 mn, V3 mx) {
-  float tmin = FLT_MIN, tmax = FLT_MAX, t1, t2, tmp;
+inline Real distance_to_aabb(V3 p, V3 d, V3 mn, V3 mx) {
+  Real tmin = FLT_MIN, tmax = FLT_MAX, t1, t2, tmp;
   if (std::fabs(d.x) < kEpsilon6) {
     if (p.x < mn.x || p.x > mx.x) return kOutOfWorld;
   } else {
-    float id = 1.0f / d.x;
+    Real id = 1.0f / d.x;
     tmin = (mn.x - p.x) * id;
     tmax = (mx.x - p.x) * id;
     if (tmin > tmax) { tmp = tmin; tmin = tmax; tmax = tmp; }
@@ -145,7 +155,7 @@ inline float distance_to_aabb(V3 p, V3 d, V3 mn, V3 mx) {
   if (std::fabs(d.y) < kEpsilon6) {
     if (p.y < mn.y || p.y > mx.y) return kOutOfWorld;
   } else {
-    float id = 1.0f / d.y;
+    Real id = 1.0f / d.y;
     t1 = (mn.y - p.y) * id;
     t2 = (mx.y - p.y) * id;
     if (t1 > t2) { tmp = t1; t1 = t2; t2 = tmp; }
@@ -156,7 +166,7 @@ inline float distance_to_aabb(V3 p, V3 d, V3 mn, V3 mx) {
   if (std::fabs(d.z) < kEpsilon6) {
     if (p.z < mn.z || p.z > mx.z) return kOutOfWorld;
   } else {
-    float id = 1.0f / d.z;
+    Real id = 1.0f / d.z;
     t1 = (mn.z - p.z) * id;
     t2 = (mx.z - p.z) * id;
     if (t1 > t2) { tmp = t1; t1 = t2; t2 = tmp; }
@@ -178,7 +188,7 @@ inline V3 obb_max(const gg_obb& o) { return v3(o.border_max[0], o.border_max[1],
 // ---------------------------------------------------------------------------
 struct Kiss {
   uint32_t s1, s2, s3, s4, s5;
-  float uniform() {
+  Real uniform() {
     s2 ^= (s2 << 5);
     s2 ^= (s2 >> 7);
     s2 ^= (s2 << 22);
@@ -187,7 +197,7 @@ struct Kiss {
     s5 = t < 0;
     s4 = static_cast<uint32_t>(t) & 2147483647u;
     s1 += 1411392427u;
-    return static_cast<float>((static_cast<float>(s1 + s2 + s4) / 4294967295.0) * (1.0f - 1.0f / (1 << 23)));
+    return static_cast<Real>((static_cast<Real>(s1 + s2 + s4) / 4294967295.0) * (1.0f - 1.0f / (1 << 23)));
   }
 };
 
@@ -195,12 +205,12 @@ struct Kiss {
 // Particle state: the photon fields of GGEMSPrimaryParticles.
 // ---------------------------------------------------------------------------
 struct Photon {
-  float E;
+  Real E;
   V3 p, d;
   int8_t scatter, status, next_process;
   int32_t E_index, solid_id;
-  float psd;  // particle_solid_distance_
-  float nid;  // next_interaction_distance_
+  Real psd;  // particle_solid_distance_
+  Real nid;  // next_interaction_distance_
 };
 
 struct Tallies {
@@ -235,7 +245,7 @@ bool dosel_index(const gg_dose_map& dm, V3 p, int* gid) {
   if (iz < 0 || iz >= dm.number_of_dosels[2]) return false;
   return true;
 }
-void dose_record(const Tallies& t, int map, float edep, V3 p) {
+void dose_record(const Tallies& t, int map, Real edep, V3 p) {
   const gg_dose_map& dm = t.scene->dose_maps[map];
   int gid;
   if (!dosel_index(dm, p, &gid)) return;
@@ -255,11 +265,11 @@ void photon_tracking_record(const Tallies& t, int map, V3 p) {
 // GetPhotonNextInteraction (GGEMSPhotonNavigator.hh:57-93).
 void next_interaction(Photon& ph, Kiss& rng, const gg_physics_tables& tb, int material) {
   int energy_id = binary_search(ph.E, tb.energy_bins, tb.number_of_bins);
-  float nid = kOutOfWorld;
+  Real nid = kOutOfWorld;
   int8_t proc = kNoProcess;
   for (int i = 0; i < tb.number_of_processes; ++i) {
     int pid = tb.process_id[i];
-    float dist = -std::log(rng.uniform()) /
+    Real dist = -std::log(rng.uniform()) /
                  tb.cross_sections[static_cast<size_t>(pid) * tb.number_of_materials * tb.number_of_bins +
                                    energy_id + tb.number_of_bins * material];
     if (dist < nid) {
@@ -274,14 +284,14 @@ void next_interaction(Photon& ph, Kiss& rng, const gg_physics_tables& tb, int ma
 
 // KleinNishinaComptonSampleSecondaries (GGEMSComptonScatteringModels.hh:47-132).
 void compton(Photon& ph, Kiss& rng) {
-  float E0 = ph.E;
-  float E0_mec2 = E0 / kElectronMassC2;
+  Real E0 = ph.E;
+  Real E0_mec2 = E0 / kElectronMassC2;
   V3 gd = ph.d;
-  float eps0 = 1.0f / (1.0f + 2.0f * E0_mec2);
-  float eps0sq = eps0 * eps0;
-  float alpha1 = -std::log(eps0);
-  float alpha2 = alpha1 + 0.5f * (1.0f - eps0sq);
-  float r1, r2, r3, epsilon, epsilonsq, onecost, sint2, greject;
+  Real eps0 = 1.0f / (1.0f + 2.0f * E0_mec2);
+  Real eps0sq = eps0 * eps0;
+  Real alpha1 = -std::log(eps0);
+  Real alpha2 = alpha1 + 0.5f * (1.0f - eps0sq);
+  Real r1, r2, r3, epsilon, epsilonsq, onecost, sint2, greject;
   int nloop = 0;
   do {
     ++nloop;
@@ -301,9 +311,9 @@ void compton(Photon& ph, Kiss& rng) {
     greject = 1.0f - epsilon * sint2 / (1.0f + epsilonsq);
   } while (greject < r3);
   if (sint2 < 0.0f) sint2 = 0.0f;
-  float costheta = 1.0f - onecost;
-  float sintheta = std::sqrt(sint2);
-  float phi = rng.uniform() * kTwoPi;
+  Real costheta = 1.0f - onecost;
+  Real sintheta = std::sqrt(sint2);
+  Real phi = rng.uniform() * kTwoPi;
   V3 g = v3(sintheta * std::cos(phi), sintheta * std::sin(phi), costheta);
   g = rotate_unit_z(g, gd);
   g = normalize3(g);
@@ -317,13 +327,13 @@ struct RayleighFit {
 };
 RayleighFit g_rayleigh_fit;
 
-float rayleigh_w(float x, float n) {
+Real rayleigh_w(Real x, Real n) {
   return (x < 0.02f) ? n * x * (1.0f - 0.5f * (n - 1.0f) * x * (1.0f - (n - 2.0f) * x / 3.0f))
                      : 1.0f - std::exp(-n * std::log(1.0f + x));
 }
 
 void rayleigh(Photon& ph, Kiss& rng, const gg_physics_tables& tb, int material) {
-  float E0 = ph.E;
+  Real E0 = ph.E;
   if (E0 <= 250.0e-6f) {
     ph.status = GG_DEAD;
     return;
@@ -336,10 +346,10 @@ void rayleigh(Photon& ph, Kiss& rng, const gg_physics_tables& tb, int material) 
   uint8_t z = tb.atomic_number[mixture + n_minus_one];
   if (n_minus_one > 0) {
     const float* cs = tb.cross_sections + static_cast<size_t>(GG_RAYLEIGH_SCATTERING) * tb.number_of_materials * nbins;
-    float kcs = linear_interpolation(tb.energy_bins[energy_id], cs[energy_id + nbins * material],
+    Real kcs = linear_interpolation(tb.energy_bins[energy_id], cs[energy_id + nbins * material],
                                      tb.energy_bins[energy_id + 1], cs[energy_id + 1 + nbins * material], E0);
-    float x = rng.uniform() * kcs;
-    float cross_section = 0.0f;
+    Real x = rng.uniform() * kcs;
+    Real cross_section = 0.0f;
     uint8_t i = 0;
     while (i < n_minus_one) {
       uint8_t zi = tb.atomic_number[mixture + i];
@@ -355,18 +365,18 @@ void rayleigh(Photon& ph, Kiss& rng, const gg_physics_tables& tb, int material) 
     }
   }
   const float* const* P = g_rayleigh_fit.pp;
-  float xx = kRayleighFactor * E0 * E0;
-  float n0 = P[6][z] - 1.0f, n1 = P[7][z] - 1.0f, n2 = P[8][z] - 1.0f;
-  float b0 = P[3][z], b1 = P[4][z], b2 = P[5][z];
-  float w0 = rayleigh_w(2.0f * xx * b0, n0);
-  float w1 = rayleigh_w(2.0f * xx * b1, n1);
-  float w2 = rayleigh_w(2.0f * xx * b2, n2);
-  float x0 = w0 * P[0][z] / (b0 * n0);
-  float x1 = w1 * P[1][z] / (b1 * n1);
-  float x2 = w2 * P[2][z] / (b2 * n2);
-  float costheta = 0.0f, x;
+  Real xx = kRayleighFactor * E0 * E0;
+  Real n0 = P[6][z] - 1.0f, n1 = P[7][z] - 1.0f, n2 = P[8][z] - 1.0f;
+  Real b0 = P[3][z], b1 = P[4][z], b2 = P[5][z];
+  Real w0 = rayleigh_w(2.0f * xx * b0, n0);
+  Real w1 = rayleigh_w(2.0f * xx * b1, n1);
+  Real w2 = rayleigh_w(2.0f * xx * b2, n2);
+  Real x0 = w0 * P[0][z] / (b0 * n0);
+  Real x1 = w1 * P[1][z] / (b1 * n1);
+  Real x2 = w2 * P[2][z] / (b2 * n2);
+  Real costheta = 0.0f, x;
   do {
-    float w = w0, n = n0, b = b0;
+    Real w = w0, n = n0, b = b0;
     x = rng.uniform() * (x0 + x1 + x2);
     if (x > x0) {
       x -= x0;
@@ -377,7 +387,7 @@ void rayleigh(Photon& ph, Kiss& rng, const gg_physics_tables& tb, int material) 
       }
     }
     n = 1.0f / n;
-    float y = rng.uniform() * w;
+    Real y = rng.uniform() * w;
     if (y < 0.02f) {
       x = y * n * (1.0f + 0.5f * (n + 1.0f) * y * (1.0f - (n + 2.0f) * y / 3.0f));
     } else {
@@ -385,8 +395,8 @@ void rayleigh(Photon& ph, Kiss& rng, const gg_physics_tables& tb, int material) 
     }
     costheta = 1.0f - x / (b * xx);
   } while (2.0f * rng.uniform() > 1.0f + costheta * costheta || costheta < -1.0f);
-  float phi = kTwoPi * rng.uniform();
-  float sintheta = std::sqrt((1.0f - costheta) * (1.0f + costheta));
+  Real phi = kTwoPi * rng.uniform();
+  Real sintheta = std::sqrt((1.0f - costheta) * (1.0f + costheta));
   V3 g = v3(sintheta * std::cos(phi), sintheta * std::sin(phi), costheta);
   g = rotate_unit_z(g, gd);
   g = normalize3(g);
@@ -412,8 +422,8 @@ void xray_primary(Photon& ph, Kiss& rng, const gg_source& src) {
   phi *= static_cast<double>(kTwoPi);
   double new_aperture = 1.0 - std::cos(static_cast<double>(src.beam_aperture));
   theta = std::acos(1.0 - new_aperture * theta);
-  V3 rotation = v3(static_cast<float>(std::cos(phi) * std::sin(theta)), static_cast<float>(std::sin(phi) * std::sin(theta)),
-                   static_cast<float>(std::cos(theta)));
+  V3 rotation = v3(static_cast<Real>(std::cos(phi) * std::sin(theta)), static_cast<Real>(std::sin(phi) * std::sin(theta)),
+                   static_cast<Real>(std::cos(theta)));
   V3 gp = local_to_global_position(src.matrix, v3(0.0f, 0.0f, 0.0f));
   V3 dir = normalize3(sub(v3(0.0f, 0.0f, 0.0f), gp));
   dir = rotate_unit_z(rotation, dir);
@@ -424,7 +434,7 @@ void xray_primary(Photon& ph, Kiss& rng, const gg_source& src) {
   gp = local_to_global_position(src.matrix, gp);
   int nbins = src.number_of_energy_bins + 1;  // GGEMSXRaySource.cc:133 passes n+1
   int index = 0;
-  float rnd = 0.0f;
+  Real rnd = 0.0f;
   if (nbins != 1) {
     rnd = rng.uniform();
     index = binary_search(rnd, src.energy_cdf, nbins + 1);
@@ -447,12 +457,12 @@ void voxelized_primary(Photon& ph, Kiss& rng, const gg_source& src) {
   double theta = rng.uniform();
   phi *= static_cast<double>(kTwoPi);
   theta = std::acos(1.0 - 2.0 * theta);
-  V3 dir = v3(static_cast<float>(std::cos(phi) * std::sin(theta)), static_cast<float>(std::sin(phi) * std::sin(theta)),
-              static_cast<float>(std::cos(theta)));
+  V3 dir = v3(static_cast<Real>(std::cos(phi) * std::sin(theta)), static_cast<Real>(std::sin(phi) * std::sin(theta)),
+              static_cast<Real>(std::cos(theta)));
   double rnd_act = rng.uniform();
   // number_of_activity_bins is the count passed to the kernel (active voxels + 1,
   // GGEMSVoxelizedSource.cc:170); the cdf and index arrays hold that many entries.
-  int index_act = binary_search(static_cast<float>(rnd_act), src.activity_cdf, static_cast<int>(src.number_of_activity_bins));
+  int index_act = binary_search(static_cast<Real>(rnd_act), src.activity_cdf, static_cast<int>(src.number_of_activity_bins));
   int32_t vox = src.activity_index[index_act];
   int nx = src.number_of_voxels[0], ny = src.number_of_voxels[1];
   int slice = nx * ny;
@@ -461,17 +471,17 @@ void voxelized_primary(Photon& ph, Kiss& rng, const gg_source& src) {
   int iy = (vox - iz * slice) / nx;
   V3 bmin = v3(src.border_min[0], src.border_min[1], src.border_min[2]);
   V3 vs = v3(src.voxel_sizes[0], src.voxel_sizes[1], src.voxel_sizes[2]);
-  V3 vmin = add(bmin, mul(v3(static_cast<float>(ix), static_cast<float>(iy), static_cast<float>(iz)), vs));
+  V3 vmin = add(bmin, mul(v3(static_cast<Real>(ix), static_cast<Real>(iy), static_cast<Real>(iz)), vs));
   V3 vmax = add(vmin, vs);
   V3 p;
-  p.x = bmin.x + (static_cast<float>(ix) + rng.uniform()) * vs.x;
-  p.y = bmin.y + (static_cast<float>(iy) + rng.uniform()) * vs.y;
-  p.z = bmin.z + (static_cast<float>(iz) + rng.uniform()) * vs.z;
+  p.x = bmin.x + (static_cast<Real>(ix) + rng.uniform()) * vs.x;
+  p.y = bmin.y + (static_cast<Real>(iy) + rng.uniform()) * vs.y;
+  p.z = bmin.z + (static_cast<Real>(iz) + rng.uniform()) * vs.z;
   safety_inside_aabb(p, vmin, vmax);
   p = local_to_global_position(src.matrix, p);
   int nbins = src.number_of_energy_bins + 1;
   int index = 0;
-  float rnd = 0.0f;
+  Real rnd = 0.0f;
   if (nbins != 1) {
     rnd = rng.uniform();
     index = binary_search(rnd, src.energy_cdf, nbins + 1);
@@ -500,7 +510,7 @@ void solid_distance(Photon& ph, const gg_solid& s, int solid_index) {
     return;
   }
   V3 ld = global_to_local_direction(m, ph.d);
-  float distance = distance_to_aabb(local, ld, obb_min(s.obb), obb_max(s.obb));
+  Real distance = distance_to_aabb(local, ld, obb_min(s.obb), obb_max(s.obb));
   if (distance < ph.psd) {
     ph.psd = distance;
     ph.solid_id = solid_index;
@@ -550,12 +560,12 @@ void track_voxelized(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& 
     int material = s.labels[ix + iy * nx + iz * nx * ny];
     ++t_counts[0];
     next_interaction(ph, rng, tb, material);
-    float nid = ph.nid;
+    Real nid = ph.nid;
     int8_t proc = ph.next_process;
-    V3 vmin = add(bmin, mul(v3(static_cast<float>(ix), static_cast<float>(iy), static_cast<float>(iz)), vs));
+    V3 vmin = add(bmin, mul(v3(static_cast<Real>(ix), static_cast<Real>(iy), static_cast<Real>(iz)), vs));
     V3 vmax = add(vmin, vs);
     safety_inside_aabb(lp, vmin, vmax);
-    float dtb = distance_to_aabb(lp, ld, vmin, vmax);
+    Real dtb = distance_to_aabb(lp, ld, vmin, vmax);
     if (dtb <= nid) {
       nid = dtb + kGeometryTolerance;
       proc = GG_TRANSPORTATION;
@@ -569,7 +579,7 @@ void track_voxelized(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& 
       break;
     }
     ph.p = lp;
-    float initial_energy = ph.E;
+    Real initial_energy = ph.E;
     if (proc != GG_TRANSPORTATION) {
       discrete_process(ph, rng, tb, material);
       if (proc == GG_COMPTON_SCATTERING || proc == GG_RAYLEIGH_SCATTERING) ph.scatter = 1;
@@ -581,7 +591,7 @@ void track_voxelized(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& 
       const float* eb = tb.attenuation_energy_bins;
       const float* me = tb.mu_en + static_cast<size_t>(material) * GG_ATTENUATION_BINS;
       int e_index = binary_search(initial_energy, eb, GG_ATTENUATION_BINS);
-      float mu_en = e_index == 0 ? me[0]
+      Real mu_en = e_index == 0 ? me[0]
                                  : linear_interpolation(eb[e_index - 1], me[e_index - 1], eb[e_index], me[e_index],
                                                         initial_energy);
       dose_record(t, dm, initial_energy * mu_en * nid * 0.1f, lp);
@@ -610,10 +620,10 @@ void track_box(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& s, int
   do {
     ++t_counts[1];
     next_interaction(ph, rng, tb, 0);
-    float nid = ph.nid;
+    Real nid = ph.nid;
     int8_t proc = ph.next_process;
     safety_inside_aabb(lp, bmin, bmax);
-    float dtb = distance_to_aabb(lp, ld, bmin, bmax);
+    Real dtb = distance_to_aabb(lp, ld, bmin, bmax);
     if (dtb <= nid) {
       nid = dtb + kGeometryTolerance;
       proc = GG_TRANSPORTATION;
@@ -631,7 +641,7 @@ void track_box(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& s, int
       discrete_process(ph, rng, tb, 0);
       ld = ph.d;
       if (s.histogram >= 0 && (proc == GG_PHOTOELECTRIC_EFFECT || proc == GG_COMPTON_SCATTERING)) {
-        V3 es = divv(box, v3(static_cast<float>(vx), static_cast<float>(vy), static_cast<float>(vz)));
+        V3 es = divv(box, v3(static_cast<Real>(vx), static_cast<Real>(vy), static_cast<Real>(vz)));
         V3 q = divv(sub(lp, bmin), es);
         int ix = static_cast<int>(q.x), iy = static_cast<int>(q.y);
         int index = ix + iy * vx;
@@ -657,16 +667,16 @@ bool moller_trumbore(V3 p, V3 d, const float* tri, V3* hit) {
   V3 e1 = v3(tri[3] - tri[0], tri[4] - tri[1], tri[5] - tri[2]);
   V3 e2 = v3(tri[6] - tri[0], tri[7] - tri[1], tri[8] - tri[2]);
   V3 h = cross3(d, e2);
-  float a = dot3(e1, h);
+  Real a = dot3(e1, h);
   if (a > -kEpsilon6 && a < kEpsilon6) return false;
-  float f = 1.0f / a;
+  Real f = 1.0f / a;
   V3 s = sub(p, p0);
-  float u = f * dot3(s, h);
+  Real u = f * dot3(s, h);
   if (u < 0.0f || u > 1.0f) return false;
   V3 q = cross3(s, e1);
-  float v = f * dot3(q, d);
+  Real v = f * dot3(q, d);
   if (v < 0.0f || u + v > 1.0f) return false;
-  float t = f * dot3(q, e2);
+  Real t = f * dot3(q, e2);
   if (!(t > kEpsilon6)) return false;
   *hit = v3(p.x + d.x * t, p.y + d.y * t, p.z + d.z * t);
   return true;
@@ -674,15 +684,15 @@ bool moller_trumbore(V3 p, V3 d, const float* tri, V3* hit) {
 
 // TestLineNode (l.182-230): slab test of the ray against a node box.
 bool line_hits_node(V3 p, V3 d, const float* node) {
-  const float pos[3] = {p.x, p.y, p.z}, dir[3] = {d.x, d.y, d.z};
-  float tmin = 0.0f, tmax = FLT_MAX;
+  const Real pos[3] = {p.x, p.y, p.z}, dir[3] = {d.x, d.y, d.z};
+  Real tmin = 0.0f, tmax = FLT_MAX;
   for (int i = 0; i < 3; ++i) {
-    float mn = node[i] - node[3 + i], mx = node[i] + node[3 + i];
+    Real mn = node[i] - node[3 + i], mx = node[i] + node[3 + i];
     if (std::fabs(dir[i]) < kEpsilon6) {
       if (pos[i] < mn || pos[i] > mx) return false;
     } else {
-      float ood = 1.0f / dir[i];
-      float t1 = (mn - pos[i]) * ood, t2 = (mx - pos[i]) * ood;
+      Real ood = 1.0f / dir[i];
+      Real t1 = (mn - pos[i]) * ood, t2 = (mx - pos[i]) * ood;
       if (t1 > t2) std::swap(t1, t2);
       if (t1 > tmin) tmin = t1;
       if (t2 < tmax) tmax = t2;
@@ -698,7 +708,7 @@ bool line_hits_node(V3 p, V3 d, const float* node) {
 // next node, writing past its 16-entry array if that node has crossings too;
 // here the search ends at 16.
 int mesh_crossings(V3 p, V3 d, const gg_solid& s, V3 out[kMaxMeshHits]) {
-  float dist2[kMaxMeshHits];
+  Real dist2[kMaxMeshHits];
   int n = 0;
   for (int node = 0; node < s.number_of_nodes; ++node) {
     const int b = s.node_first[node], e = s.node_first[node + 1];
@@ -708,7 +718,7 @@ int mesh_crossings(V3 p, V3 d, const gg_solid& s, V3 out[kMaxMeshHits]) {
       V3 hit;
       if (!moller_trumbore(p, d, s.triangles + static_cast<size_t>(s.node_triangles[k]) * GG_TRIANGLE_FLOATS, &hit))
         continue;
-      float d2 = (hit.x - p.x) * (hit.x - p.x) + (hit.y - p.y) * (hit.y - p.y) + (hit.z - p.z) * (hit.z - p.z);
+      Real d2 = (hit.x - p.x) * (hit.x - p.x) + (hit.y - p.y) * (hit.y - p.y) + (hit.z - p.z) * (hit.z - p.z);
       int at = n;
       while (at > 0 && d2 < dist2[at - 1]) {
         out[at] = out[at - 1];
@@ -751,10 +761,10 @@ void track_meshed(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& s, 
     ph.p = lp;
     ph.d = ld;
     next_interaction(ph, rng, tb, 0);
-    float nid = ph.nid;
+    Real nid = ph.nid;
     int8_t proc = ph.next_process;
-    float dx = next.x - lp.x, dy = next.y - lp.y, dz = next.z - lp.z;
-    float to_next = std::sqrt(dx * dx + dy * dy + dz * dz);
+    Real dx = next.x - lp.x, dy = next.y - lp.y, dz = next.z - lp.z;
+    Real to_next = std::sqrt(dx * dx + dy * dy + dz * dz);
     if (to_next <= nid) {
       nid = to_next + kGeometryTolerance;
       proc = GG_TRANSPORTATION;
@@ -762,7 +772,7 @@ void track_meshed(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& s, 
     }
     lp = add(lp, scale(ld, nid));
     ph.p = lp;
-    float initial_energy = ph.E;
+    Real initial_energy = ph.E;
     if (proc != GG_TRANSPORTATION) {
       discrete_process(ph, rng, tb, 0);
       if (proc == GG_COMPTON_SCATTERING || proc == GG_RAYLEIGH_SCATTERING) ph.scatter = 1;
@@ -775,7 +785,7 @@ void track_meshed(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& s, 
     }
   } while (ph.status == GG_ALIVE);
   const float* m = s.obb.matrix;
-  float dist = distance_to_aabb(global_to_local_position(m, lp), global_to_local_direction(m, ld), obb_min(s.obb),
+  Real dist = distance_to_aabb(global_to_local_position(m, lp), global_to_local_direction(m, ld), obb_min(s.obb),
                                 obb_max(s.obb));
   ph.p = v3(lp.x + ld.x * (dist + kGeometryTolerance), lp.y + ld.y * (dist + kGeometryTolerance),
             lp.z + ld.z * (dist + kGeometryTolerance));
@@ -787,15 +797,15 @@ void track_meshed(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& s, 
 // of the world element size along the dominant axis.
 void world_tracking(const Photon& ph, const gg_world& w, const Tallies& t) {
   if (ph.status == GG_DEAD) return;
-  float distance = ph.psd == kOutOfWorld ? 10000.0f : ph.psd;
+  Real distance = ph.psd == kOutOfWorld ? 10000.0f : ph.psd;
   if (distance <= kGeometryTolerance) return;
   V3 p1 = ph.p;
   const V3 dir = ph.d;
   const V3 size = v3(w.sizes[0], w.sizes[1], w.sizes[2]);
   const int dim[3] = {w.dimensions[0], w.dimensions[1], w.dimensions[2]};
   V3 p2 = add(p1, scale(dir, distance));
-  const V3 lo = v3(size.x * static_cast<float>(dim[0]) * -0.5f, size.y * static_cast<float>(dim[1]) * -0.5f,
-                   size.z * static_cast<float>(dim[2]) * -0.5f);
+  const V3 lo = v3(size.x * static_cast<Real>(dim[0]) * -0.5f, size.y * static_cast<Real>(dim[1]) * -0.5f,
+                   size.z * static_cast<Real>(dim[2]) * -0.5f);
   auto index_of = [&](V3 p, int idx[3]) {
     V3 q = divv(sub(p, lo), size);
     idx[0] = static_cast<int>(q.x);
@@ -806,7 +816,7 @@ void world_tracking(const Photon& ph, const gg_world& w, const Tallies& t) {
   index_of(p1, idx);
   V3 diff = sub(p2, p1);
   V3 len = v3(std::fabs(diff.x), std::fabs(diff.y), std::fabs(diff.z));
-  float length = len.x, main_size = size.x;
+  Real length = len.x, main_size = size.x;
   if (len.y > length) {
     length = len.y;
     main_size = size.y;
@@ -814,7 +824,7 @@ void world_tracking(const Photon& ph, const gg_world& w, const Tallies& t) {
     length = len.z;
     main_size = size.z;
   }
-  float inv_length = 1.0f / length;
+  Real inv_length = 1.0f / length;
   V3 increment = v3(inv_length * diff.x, inv_length * diff.y, inv_length * diff.z);
   int steps = static_cast<int>(1.0f + (length / main_size));
   const double E = ph.E;

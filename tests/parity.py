@@ -10,13 +10,14 @@ import scenes
 from ggems_b200 import abi
 
 
-def run_oracle(sc, src, n, seed=777, states=None, threads=None):
+def run_oracle(sc, src, n, seed=777, states=None, threads=None, fp64=False):
     st = scenes.seed_states(seed) if states is None else states.copy()
     ss = sc.struct()
     P = abi.Particles(min(n, abi.GG_MAXIMUM_PARTICLES))
     T = sc.tallies()
-    rc = scenes.oracle().gg_oracle_run(C.byref(ss), C.byref(src.struct), n, abi.ptr(st, C.c_uint32), C.byref(P.struct),
-                                       C.byref(T.struct), threads or os.cpu_count())
+    lib = scenes.oracle_fp64() if fp64 else scenes.oracle()
+    rc = lib.gg_oracle_run(C.byref(ss), C.byref(src.struct), n, abi.ptr(st, C.c_uint32), C.byref(P.struct),
+                           C.byref(T.struct), threads or os.cpu_count())
     assert rc == 0
     return P, T, st
 

@@ -101,6 +101,27 @@ def oracle():
     return _ORACLE
 
 
+_ORACLE_FP64 = None
+
+
+def oracle_fp64():
+    """The oracle's transport restatement built in FP64 (libgg_oracle_fp64.so):
+    the precision reference the FP32 results are compared with."""
+    global _ORACLE_FP64
+    if _ORACLE_FP64 is None:
+        oracle()  # builds both libraries when missing
+        lib = C.CDLL(os.path.join(ROOT, "oracle", "_build", "libgg_oracle_fp64.so"))
+        lib.gg_oracle_run.restype = C.c_int
+        lib.gg_oracle_run.argtypes = _ORACLE.gg_oracle_run.argtypes
+        pp = load_physics()
+        arrs = [np.ascontiguousarray(pp["rayleigh_pp%d" % i]) for i in range(9)]
+        lib._pp_keep = arrs
+        ptrs = (C.POINTER(C.c_float) * 9)(*[abi.ptr(a, C.c_float) for a in arrs])
+        lib.gg_oracle_set_rayleigh_fit(ptrs)
+        _ORACLE_FP64 = lib
+    return _ORACLE_FP64
+
+
 def load_physics(path=PHYSICS):
     raw = open(path, "rb").read()
     assert raw[:8] == b"GGPHYS01"

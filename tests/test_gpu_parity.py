@@ -299,3 +299,36 @@ def test_world_tracking(ctx):
         scale = np.abs(o).sum()
         assert scale > 0, k
         assert np.abs(g - o).sum() <= 0.005 * scale, k
+
+
+def test_error_against_fp64_oracle(ctx):
+    """The CUDA results' error against the oracle's FP64 build on the same
+    random streams: water dose (C1 configuration) and the CBCT projection
+    (total and scatter histograms)."""
+    sc = scenes.water_box_scene()
+    src = scenes.XRaySource(monoenergy=scenes.F(60.0) * scenes.KEV, aperture_deg=10.0)
+    n = 1_000_000
+    Pg, Tg, _ = parity.run_gpu(ctx, sc, src, n)
+    P64, T64, _ = parity.run_oracle(sc, src, n, fp64=True)
+    eg, e64 = Tg.edep[0], T64.edep[0]
+    rel = abs(eg.sum() - e64.sum()) / e64.sum()
+    var = np.maximum(T64.edep_squared[0] - e64 ** 2 / np.maximum(T64.hit[0], 1), 0)
+    z = parity.z_scores(eg, e64, var, var)
+    same = ((Pg.status == P64.status) & (Pg.solid_id == P64.solid_id) & (Pg.scatter == P64.scatter)).mean()
+    print("water 1e6: edep GPU vs FP64 oracle rel %.2e, |z|<3 in %.5f of dosels, same outcome %.4f"
+          % (rel, (np.abs(z) < 3).mean(), same))
+    assert rel < 5e-3
+    assert (np.abs(z) < 3).mean() >= 0.997
+    sc = scenes.cbct_scene(n=64, voxel=4.0, elements=(128, 128, 1), element_size=(3.2, 3.2, 10.0))
+    src = scenes.XRaySource(spectrum=scenes.synthetic_spectrum(), aperture_deg=11.0)
+    n = 1_000_000
+    _, Tg, _ = parity.run_gpu(ctx, sc, src, n)
+    _, T64, _ = parity.run_oracle(sc, src, n, fp64=True)
+    for k, name in ((0, "total"), (1, "scatter")):
+        hg, h64 = Tg.histograms[k].astype(np.float64), T64.histograms[k].astype(np.float64)
+        rel = abs(hg.sum() - h64.sum()) / h64.sum()
+        z = (hg - h64) / np.sqrt(np.maximum(hg + h64, 1.0))
+        print("CBCT 1e6 %s histogram: GPU vs FP64 oracle rel %.2e, |z|<3 in %.5f of elements"
+              % (name, rel, (np.abs(z) < 3).mean()))
+        assert rel < 5e-3
+        assert (np.abs(z) < 3).mean() >= 0.997
