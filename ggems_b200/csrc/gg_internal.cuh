@@ -198,7 +198,8 @@ struct ProjectorParams {
   float element_size[3];
   int32_t elements[2];
   float source[3];               // world
-  float* out;                    // [elements[1]][elements[0]]
+  float* out;                    // [elements[1]][elements[0]], or [..][..][2] with network_input
+  int32_t network_input;         // 1: write (exp(-L), L) pairs, the surrogate network's input
 };
 void launch_line_integrals(const ProjectorParams& p, void* stream);
 

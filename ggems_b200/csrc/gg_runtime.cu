@@ -1104,6 +1104,67 @@ GG_API int gg_line_integrals(gg_context* c, const gg_solid* phantom, const gg_so
   return GG_OK;
 }
 
+GG_API int gg_line_integrals_batch(gg_context* c, const gg_solid* phantom, const gg_solid* detectors,
+                                   const float* source_positions, int32_t count, const float* mu,
+                                   int32_t number_of_materials, float* inputs) {
+  if (!c || !phantom || !detectors || !source_positions || !mu || !inputs || number_of_materials < 1 || count < 1)
+    return fail(GG_ERROR_INVALID_ARGUMENT, "bad arguments");
+  if (phantom->type != GG_SOLID_VOXELIZED || !phantom->labels)
+    return fail(GG_ERROR_INVALID_ARGUMENT, "need a voxelized phantom solid (with labels)");
+  for (int a = 0; a < 3; ++a)
+    if (phantom->number_of_voxels[a] < 1 || !(phantom->voxel_sizes[a] > 0.0f))
+      return fail(GG_ERROR_INVALID_ARGUMENT, "bad phantom dimensions");
+  const int32_t ex = detectors[0].virtual_element_number[0], ey = detectors[0].virtual_element_number[1];
+  for (int k = 0; k < count; ++k)
+    if (detectors[k].type != GG_SOLID_BOX || detectors[k].virtual_element_number[0] != ex ||
+        detectors[k].virtual_element_number[1] != ey || ex < 1 || ey < 1)
+      return fail(GG_ERROR_INVALID_ARGUMENT, "detectors must be boxes with the same element grid");
+  GG_CUDA(cudaSetDevice(c->device));
+  const size_t n = static_cast<size_t>(ex) * ey;
+  const size_t nv = static_cast<size_t>(phantom->number_of_voxels[0]) * phantom->number_of_voxels[1] * phantom->number_of_voxels[2];
+  std::vector<void*> tmp;
+  auto cleanup = [&]() {
+    for (void* p : tmp) cudaFree(p);
+  };
+  float *dmu = nullptr, *dout = nullptr;
+  uint8_t* dlab = nullptr;
+  int rc;
+  if ((rc = dev_copy_to(c, tmp, mu, static_cast<size_t>(number_of_materials), &dmu)) ||
+      (rc = dev_copy_to(c, tmp, phantom->labels, nv, &dlab)) ||
+      (rc = dev_copy_to(c, tmp, static_cast<const float*>(nullptr), 2 * n * count, &dout))) {
+    cleanup();
+    return rc;
+  }
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < count && e == cudaSuccess; ++k) {
+    gg::ProjectorParams P{};
+    std::memcpy(P.phantom_matrix, phantom->obb.matrix, sizeof(P.phantom_matrix));
+    std::memcpy(P.border_min, phantom->obb.border_min, sizeof(P.border_min));
+    std::memcpy(P.border_max, phantom->obb.border_max, sizeof(P.border_max));
+    std::memcpy(P.number_of_voxels, phantom->number_of_voxels, sizeof(P.number_of_voxels));
+    std::memcpy(P.voxel_sizes, phantom->voxel_sizes, sizeof(P.voxel_sizes));
+    P.number_of_materials = number_of_materials;
+    const gg_solid& d = detectors[k];
+    std::memcpy(P.detector_matrix, d.obb.matrix, sizeof(P.detector_matrix));
+    std::memcpy(P.detector_min, d.obb.border_min, sizeof(P.detector_min));
+    for (int a = 0; a < 3; ++a) P.element_size[a] = d.box_size[a] / static_cast<float>(d.virtual_element_number[a]);
+    P.elements[0] = ex;
+    P.elements[1] = ey;
+    std::memcpy(P.source, source_positions + 3 * k, sizeof(P.source));
+    P.mu = dmu;
+    P.labels = dlab;
+    P.out = dout + 2 * n * k;
+    P.network_input = 1;
+    gg::launch_line_integrals(P, c->stream);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(inputs, dout, 2 * n * count * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cleanup();
+  if (e != cudaSuccess) return fail(GG_ERROR_CUDA, std::string("line integrals: ") + cudaGetErrorString(e));
+  return GG_OK;
+}
+
 GG_API int gg_last_run_stats(gg_context* c, float* milliseconds, int64_t* kernel_launches) {
   if (!c) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL context");
   if (milliseconds) *milliseconds = c->last_ms;

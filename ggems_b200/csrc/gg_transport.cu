@@ -1240,7 +1240,13 @@ __global__ void line_integral_kernel(ProjectorParams P) {
       tmax[a] += tdelta[a];
     }
   }
-  P.out[static_cast<size_t>(j) * P.elements[0] + i] = sum;
+  const size_t o = static_cast<size_t>(j) * P.elements[0] + i;
+  if (P.network_input) {
+    P.out[2 * o] = expf(-sum);
+    P.out[2 * o + 1] = sum;
+  } else {
+    P.out[o] = sum;
+  }
 }
 
 }  // namespace

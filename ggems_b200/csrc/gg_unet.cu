@@ -10,11 +10,13 @@
 // W'[ky][kx][Cin][Cout] = W[2-ky][2-kx][Cout][Cin] that turns the data
 // gradient of a convolution into another forward convolution.
 //
-// Every 3x3 convolution is an implicit GEMM on the tensor cores
-// (mma.sync m16n8k16, BF16 inputs, FP32 accumulation): rows = pixels, columns
-// = output channels, reduction = 9 x input channels.  Weight gradients are the
+// The forward 3x3 convolutions and their data gradients are implicit GEMMs on
+// the 5th-generation tensor cores (tcgen05.mma with TMEM accumulators, TMA
+// operand staging; gg_unet_umma.cu): rows = pixels, columns = output
+// channels, reduction = 9 x input channels.  Weight gradients are the
 // transposed GEMM (rows = output channels, columns = input channels,
-// reduction = pixels), split over blocks with FP32 atomics.
+// reduction = pixels), split over blocks with FP32 atomics on mma.sync
+// m16n8k16 (BF16 inputs, FP32 accumulation).
 //
 // Network (S = image side, all 3x3 convolutions followed by ReLU):
 //   enc  16->32->32 @S | pool | 32->64->64 @S/2 | pool | 64->128->128 @S/4 | pool
@@ -42,6 +44,7 @@
 #include <vector>
 
 #include "ggems_b200.h"
+#include "gg_unet_umma.cuh"
 
 namespace {
 
@@ -67,81 +70,11 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], 
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-constexpr int kTileP = 64;   // pixels per block (4 warps x 16)
-constexpr int kTileC = 32;   // output channels per block (4 n8 tiles)
 constexpr int kPad = 8;      // smem row padding (bf16 elements)
 
 struct ConvShape {
   int batch, height, width, cin, cout;
 };
-
-// 3x3 "same" convolution.  Out mode 0: y = relu(conv + bias) stored BF16;
-// mode 1: y = conv stored FP32 (data gradients: no bias, no activation).
-template <int kMode>
-__global__ void __launch_bounds__(128) conv3x3_kernel(const bf16* __restrict__ x, const bf16* __restrict__ w,
-                                                      const float* __restrict__ bias, void* __restrict__ y,
-                                                      ConvShape s) {
-  __shared__ __align__(16) bf16 As[kTileP][16 + kPad];
-  __shared__ __align__(16) bf16 Bs[kTileC][16 + kPad];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int g = lane >> 2, t = lane & 3;
-  const int hw = s.height * s.width;
-  const int p0 = blockIdx.x * kTileP, co0 = blockIdx.y * kTileC;
-  // the pixel this thread loads (2 threads per pixel, 8 channels each)
-  const int lp = tid >> 1, half = tid & 1;
-  const int pix = p0 + lp;
-  const int b = pix / hw, rem = pix - b * hw, py = rem / s.width, px = rem - py * s.width;
-  float acc[4][4] = {};
-  for (int tap = 0; tap < 9; ++tap) {
-    const int ky = tap / 3, kx = tap - 3 * ky;
-    const int yy = py + ky - 1, xx = px + kx - 1;
-    const bool inside = yy >= 0 && yy < s.height && xx >= 0 && xx < s.width;
-    const bf16* src = x + (static_cast<size_t>(b) * hw + yy * s.width + xx) * s.cin;
-    const bf16* wt = w + static_cast<size_t>(tap) * s.cout * s.cin;
-    for (int c0 = 0; c0 < s.cin; c0 += 16) {
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if (inside) v = *reinterpret_cast<const uint4*>(src + c0 + 8 * half);
-      *reinterpret_cast<uint4*>(&As[lp][8 * half]) = v;
-      if (tid < 64) {
-        const int co = tid >> 1;
-        *reinterpret_cast<uint4*>(&Bs[co][8 * half]) =
-            *reinterpret_cast<const uint4*>(wt + static_cast<size_t>(co0 + co) * s.cin + c0 + 8 * half);
-      }
-      __syncthreads();
-      uint32_t a[4];
-      const int r = warp * 16 + g;
-      a[0] = *reinterpret_cast<const uint32_t*>(&As[r][2 * t]);
-      a[1] = *reinterpret_cast<const uint32_t*>(&As[r + 8][2 * t]);
-      a[2] = *reinterpret_cast<const uint32_t*>(&As[r][2 * t + 8]);
-      a[3] = *reinterpret_cast<const uint32_t*>(&As[r + 8][2 * t + 8]);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        uint32_t bb[2];
-        bb[0] = *reinterpret_cast<const uint32_t*>(&Bs[8 * j + g][2 * t]);
-        bb[1] = *reinterpret_cast<const uint32_t*>(&Bs[8 * j + g][2 * t + 8]);
-        mma_bf16(acc[j], a, bb);
-      }
-      __syncthreads();
-    }
-  }
-  // epilogue: rows warp*16+g (+8), columns 8j + 2t (+1)
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int co = co0 + 8 * j + 2 * t;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const size_t row = static_cast<size_t>(p0 + warp * 16 + g + 8 * h);
-      float v0 = acc[j][2 * h], v1 = acc[j][2 * h + 1];
-      if (kMode == 0) {
-        v0 = fmaxf(v0 + bias[co], 0.0f);
-        v1 = fmaxf(v1 + bias[co + 1], 0.0f);
-        *reinterpret_cast<__nv_bfloat162*>(static_cast<bf16*>(y) + row * s.cout + co) = __floats2bfloat162_rn(v0, v1);
-      } else {
-        *reinterpret_cast<float2*>(static_cast<float*>(y) + row * s.cout + co) = make_float2(v0, v1);
-      }
-    }
-  }
-}
 
 // Weight gradient dW[tap][co][ci] += sum_p dy[p][co] * x[p shifted by tap][ci]
 // (32 output x 16 input channels per block, one tap, a range of pixels).
@@ -449,6 +382,8 @@ struct gg_unet {
     bf16* act = nullptr;  // output activation [batch][side][side][cout]
     float* dact = nullptr;
     bf16* dpre = nullptr;
+    gg_umma::ConvPlan fwd{};  // y = relu(conv(input, w) + b)
+    gg_umma::ConvPlan bwd{};  // data gradient: conv(dpre, wt), layers 1..13
   };
   std::vector<Layer> layers;  // 14 convolutions
   size_t out_w_off = 0, out_b_off = 0, n_params = 0;
@@ -464,6 +399,8 @@ struct gg_unet {
   float* y = nullptr;                      // output [B][S][S]
   float* loss = nullptr;
   std::vector<void*> allocations;
+  int* conv_error = nullptr;        // set by a convolution whose wait gave up
+  int* conv_error_host = nullptr;   // pinned copy read after each call
 };
 
 namespace {
@@ -478,15 +415,25 @@ int unet_alloc(gg_unet* n, T** p, size_t count) {
   return GG_OK;
 }
 
-int run_conv(gg_unet* n, const gg_unet::Layer& L, const bf16* x, int mode, const bf16* w, int cin, int cout, void* y) {
-  ConvShape s{n->batch, L.side, L.side, cin, cout};
-  const int pixels = n->batch * L.side * L.side;
-  dim3 grid(pixels / kTileP, cout / kTileC);
-  if (mode == 0)
-    conv3x3_kernel<0><<<grid, 128, 0, n->stream>>>(x, w, n->params + L.b_off, y, s);
-  else
-    conv3x3_kernel<1><<<grid, 128, 0, n->stream>>>(x, w, nullptr, y, s);
-  UNET_CUDA(cudaGetLastError());
+int run_conv(gg_unet* n, const gg_unet::Layer& L, int mode, void* y) {
+  const cudaError_t e = gg_umma::launch(mode == 0 ? L.fwd : L.bwd, mode, mode == 0 ? n->params + L.b_off : nullptr, y,
+                                        n->conv_error, n->stream);
+  if (e != cudaSuccess) return unet_fail(GG_ERROR_CUDA, std::string("convolution launch: ") + cudaGetErrorString(e));
+  return GG_OK;
+}
+
+// Queues the read-back of the convolutions' error flag (checked after the
+// stream synchronisation by conv_status).
+int queue_conv_status(gg_unet* n) {
+  UNET_CUDA(cudaMemcpyAsync(n->conv_error_host, n->conv_error, sizeof(int), cudaMemcpyDeviceToHost, n->stream));
+  return GG_OK;
+}
+int conv_status(gg_unet* n) {
+  if (*n->conv_error_host) {
+    *n->conv_error_host = 0;
+    cudaMemsetAsync(n->conv_error, 0, sizeof(int), n->stream);
+    return unet_fail(GG_ERROR_TIMEOUT, "a tensor-core convolution gave up waiting for its operands");
+  }
   return GG_OK;
 }
 
@@ -519,7 +466,7 @@ int forward(gg_unet* n, const float* input) {
     if (i == 8) up_concat_kernel<<<grid_for(static_cast<size_t>(B) * (S / 4) * (S / 4) * 384), 256, 0, n->stream>>>(L[7].act, L[5].act, n->cat8, B, S / 4, S / 4, 256, 128);
     if (i == 10) up_concat_kernel<<<grid_for(static_cast<size_t>(B) * (S / 2) * (S / 2) * 192), 256, 0, n->stream>>>(L[9].act, L[3].act, n->cat10, B, S / 2, S / 2, 128, 64);
     if (i == 12) up_concat_kernel<<<grid_for(static_cast<size_t>(B) * S * S * 96), 256, 0, n->stream>>>(L[11].act, L[1].act, n->cat12, B, S, S, 64, 32);
-    if ((rc = run_conv(n, L[i], layer_input(n, i), 0, L[i].w, L[i].cin, L[i].cout, L[i].act))) return rc;
+    if ((rc = run_conv(n, L[i], 0, L[i].act))) return rc;
   }
   out_forward_kernel<<<(pixels + 255) / 256, 256, 0, n->stream>>>(L[13].act, n->params + n->out_w_off,
                                                                     n->params + n->out_b_off, n->y, pixels);
@@ -552,7 +499,7 @@ int backward(gg_unet* n, const float* target) {
     float* dx = (i == 8) ? n->dcat8 : (i == 10) ? n->dcat10 : (i == 12) ? n->dcat12
               : (i == 2) ? n->dpool1 : (i == 4) ? n->dpool2 : (i == 6) ? n->dpool3 : L[i - 1].dact;
     int rc;
-    if ((rc = run_conv(n, l, l.dpre, 1, l.wt, l.cout, l.cin, dx))) return rc;
+    if ((rc = run_conv(n, l, 1, dx))) return rc;
     if (i == 12) up_concat_backward_kernel<<<grid_for(static_cast<size_t>(px) * 96), 256, 0, n->stream>>>(n->dcat12, L[11].dact, L[1].dact, B, S, S, 64, 32, 1);
     if (i == 10) up_concat_backward_kernel<<<grid_for(static_cast<size_t>(px) * 192), 256, 0, n->stream>>>(n->dcat10, L[9].dact, L[3].dact, B, S / 2, S / 2, 128, 64, 1);
     if (i == 8) up_concat_backward_kernel<<<grid_for(static_cast<size_t>(px) * 384), 256, 0, n->stream>>>(n->dcat8, L[7].dact, L[5].dact, B, S / 4, S / 4, 256, 128, 1);
@@ -579,8 +526,8 @@ extern "C" {
 GG_API const char* gg_unet_last_error(void) { return g_unet_error.c_str(); }
 
 GG_API int gg_unet_create(int32_t batch, int32_t size, uint64_t seed, gg_unet** out) {
-  if (!out || batch < 1 || size < 64 || size % 64 != 0)
-    return unet_fail(GG_ERROR_INVALID_ARGUMENT, "batch >= 1 and an image side that is a multiple of 64 (>= 64) are needed");
+  if (!out || batch < 1 || size < 64 || (size & (size - 1)) != 0)
+    return unet_fail(GG_ERROR_INVALID_ARGUMENT, "batch >= 1 and an image side that is a power of two (>= 64) are needed");
   *out = nullptr;
   gg_unet* n = new gg_unet();
   n->batch = batch;
@@ -647,6 +594,16 @@ GG_API int gg_unet_create(int32_t batch, int32_t size, uint64_t seed, gg_unet** 
       (rc = unet_alloc(n, &n->dcat8, B * SS / 16 * 384)) || (rc = unet_alloc(n, &n->dcat10, B * SS / 4 * 192)) ||
       (rc = unet_alloc(n, &n->dcat12, B * SS * 96)) || (rc = unet_alloc(n, &n->y, B * SS)) || (rc = unet_alloc(n, &n->loss, 1)))
     return drop(rc);
+  if ((rc = unet_alloc(n, &n->conv_error, 1))) return drop(rc);
+  if (cudaMallocHost(&n->conv_error_host, sizeof(int)) != cudaSuccess) return drop(unet_fail(GG_ERROR_CUDA, "pinned flag"));
+  *n->conv_error_host = 0;
+  // tensor maps and tile plans of every convolution (the buffers never move)
+  for (int i = 0; i < 14; ++i) {
+    auto& l = n->layers[i];
+    const char* why = gg_umma::make_plan(&l.fwd, layer_input(n, i), l.w, batch, l.side, l.side, l.cin, l.cout);
+    if (!why && i > 0) why = gg_umma::make_plan(&l.bwd, l.dpre, l.wt, batch, l.side, l.side, l.cout, l.cin);
+    if (why) return drop(unet_fail(GG_ERROR_INVALID_ARGUMENT, std::string("convolution plan: ") + why));
+  }
   if ((rc = refresh_weights(n))) return drop(rc);
   if (cudaStreamSynchronize(n->stream) != cudaSuccess) return drop(unet_fail(GG_ERROR_CUDA, "initialisation"));
   *out = n;
@@ -657,6 +614,7 @@ GG_API int gg_unet_destroy(gg_unet* n) {
   if (!n) return GG_OK;
   if (n->stream) cudaStreamSynchronize(n->stream);
   for (void* p : n->allocations) cudaFree(p);
+  if (n->conv_error_host) cudaFreeHost(n->conv_error_host);
   if (n->stream) cudaStreamDestroy(n->stream);
   delete n;
   return GG_OK;
@@ -687,8 +645,9 @@ GG_API int gg_unet_forward(gg_unet* n, const float* input, float* output) {
   if ((rc = forward(n, input))) return rc;
   UNET_CUDA(cudaMemcpyAsync(output, n->y, static_cast<size_t>(n->batch) * n->size * n->size * sizeof(float),
                             cudaMemcpyDeviceToDevice, n->stream));
+  if ((rc = queue_conv_status(n))) return rc;
   UNET_CUDA(cudaStreamSynchronize(n->stream));
-  return GG_OK;
+  return conv_status(n);
 }
 
 // Loss and gradients without an update: grads_host receives the parameter gradients.
@@ -699,8 +658,9 @@ GG_API int gg_unet_gradients(gg_unet* n, const float* input, const float* target
   if (loss) UNET_CUDA(cudaMemcpyAsync(loss, n->loss, sizeof(float), cudaMemcpyDeviceToHost, n->stream));
   if (grads_host)
     UNET_CUDA(cudaMemcpyAsync(grads_host, n->grads, n->n_params * sizeof(float), cudaMemcpyDeviceToHost, n->stream));
+  if ((rc = queue_conv_status(n))) return rc;
   UNET_CUDA(cudaStreamSynchronize(n->stream));
-  return GG_OK;
+  return conv_status(n);
 }
 
 // One Adam step on (input, target) (device arrays as in gg_unet_forward).
@@ -716,8 +676,9 @@ GG_API int gg_unet_train_step(gg_unet* n, const float* input, const float* targe
   UNET_CUDA(cudaGetLastError());
   if ((rc = refresh_weights(n))) return rc;
   if (loss) UNET_CUDA(cudaMemcpyAsync(loss, n->loss, sizeof(float), cudaMemcpyDeviceToHost, n->stream));
+  if ((rc = queue_conv_status(n))) return rc;
   UNET_CUDA(cudaStreamSynchronize(n->stream));
-  return GG_OK;
+  return conv_status(n);
 }
 
 }  // extern "C"

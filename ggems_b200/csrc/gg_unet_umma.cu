@@ -1,0 +1,361 @@
+// 3x3 "same" convolutions of the scatter-surrogate U-Net on the 5th-generation
+// tensor cores (tcgen05), one implicit GEMM per launch:
+//
+//   D[pixel][co] = sum over taps t and input channels c of X[pixel + offset(t)][c] * W[t][co][c]
+//
+// rows = 128 pixels per CTA (M = 128), columns = an output-channel tile
+// (N <= 256), reduction = 9 taps x input channels in chunks of Kc = 16/32/64.
+//
+//   * operands: TMA (cp.async.bulk.tensor, no multicast) brings per (tap,
+//     chunk) the 128 x Kc activation tile -- the box of a 4-D NHWC tensor map
+//     at the tap's shifted (x, y), whose out-of-range rows and columns TMA
+//     fills with zeros, which is exactly the convolution's zero padding -- and
+//     the N x Kc weight tile, both K-major with the 128/64/32-byte swizzle of
+//     their row length, into a ring of shared-memory stages;
+//   * one thread issues tcgen05.mma (kind::f16, BF16 x BF16 -> FP32) into a
+//     TMEM accumulator and frees each stage with tcgen05.commit;
+//   * all four warps read their 32 TMEM lanes (= 32 pixels) with tcgen05.ld
+//     and store: mode 0 adds the bias, applies ReLU and writes BF16 (the
+//     forward activations), mode 1 writes FP32 (data gradients, no bias).
+//
+// Every mbarrier wait is bounded; a wait that gives up sets *error, the CTA
+// stops issuing work, waits (bounded) for the copies it started, frees its
+// TMEM and returns.  The shared-memory descriptors and the instruction
+// descriptor use CuTe's bitfield definitions (cute/arch/mma_sm100_desc.hpp).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+
+#include <cute/arch/mma_sm100_desc.hpp>
+
+#include "gg_unet_umma.cuh"
+
+namespace gg_umma {
+namespace {
+
+constexpr int kThreads = 128;
+constexpr uint64_t kWaitNs = 2000000000ull;  // a wait gives up after 2 s of device time
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+// Waits for the phase of parity `parity` of the mbarrier at `bar`; gives up
+// after kWaitNs, or as soon as another CTA of the launch has given up (*error).
+__device__ __forceinline__ bool wait_parity(uint32_t bar, uint32_t parity, const int* error) {
+  uint32_t done = 0;
+  const uint64_t t0 = global_ns();
+  for (uint32_t i = 0; !done; ++i) {
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (!done && (i & 255) == 255 && (global_ns() - t0 > kWaitNs || *reinterpret_cast<const volatile int*>(error)))
+      break;
+  }
+  return done != 0;
+}
+
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
+          "r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{ .reg .pred p; setp.ne.b32 p, %4, 0; tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p; }" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// 32 lanes x 32 columns of FP32 from TMEM into 32 registers per thread.
+__device__ __forceinline__ void tmem_load_32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// K-major operand tile of `rows` rows of `row_bytes` (32, 64 or 128) bytes,
+// swizzled over the row length, 8-row groups `8 * row_bytes` apart.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, int row_bytes) {
+  cute::UMMA::SmemDescriptor d;
+  d.desc_ = 0;
+  d.start_address_ = static_cast<uint16_t>(addr >> 4);
+  d.leading_byte_offset_ = 1;
+  d.stride_byte_offset_ = static_cast<uint16_t>((8 * row_bytes) >> 4);
+  d.version_ = 1;
+  d.base_offset_ = 0;
+  d.lbo_mode_ = 0;
+  d.layout_type_ = static_cast<uint8_t>(row_bytes == 128 ? cute::UMMA::LayoutType::SWIZZLE_128B
+                                        : row_bytes == 64 ? cute::UMMA::LayoutType::SWIZZLE_64B
+                                                          : cute::UMMA::LayoutType::SWIZZLE_32B);
+  return d.desc_;
+}
+
+template <int kMode>
+__global__ void __launch_bounds__(kThreads, 1) conv_umma_kernel(const __grid_constant__ CUtensorMap tmx,
+                                                             const __grid_constant__ CUtensorMap tmw, ConvArgs a) {
+  extern __shared__ unsigned char smem_raw[];
+  // 1024-byte alignment for the 128-byte swizzle
+  unsigned char* smem = smem_raw + ((1024 - (smem_addr(smem_raw) & 1023)) & 1023);
+  const int S = a.stages;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + static_cast<size_t>(S) * a.stage_bytes);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + S;
+  uint64_t* acc = bars + 2 * S;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc + 1);
+  __shared__ int cta_error;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * 128;
+  const int n0 = blockIdx.y * a.n_tile;
+  // the tile's first pixel: image b0, row y0, column x0 (boxes of whole rows / images)
+  const int hw = a.height * a.width;
+  const int b0 = m0 / hw, rem = m0 - b0 * hw, y0 = rem / a.width, x0 = rem - y0 * a.width;
+
+  if (threadIdx.x == 0) {
+    cta_error = 0;
+    for (int i = 0; i < 2 * S + 1; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bars + i)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                 "r"(a.tmem_cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  const int chunks = a.cin / a.kc;
+  const int iters = 9 * chunks;
+  const uint32_t tx_bytes = static_cast<uint32_t>(a.a_bytes + a.b_bytes);
+  if (warp == 0 && lane == 0) {
+    // ---- producer: TMA loads of (tap, chunk) operand tiles ----
+    int issued = 0;
+    for (int it = 0; it < iters; ++it) {
+      const int s = it % S;
+      if (it >= S && !wait_parity(smem_addr(empty + s), ((it / S) + 1) & 1, a.error)) {
+        atomicExch(&cta_error, 1);
+        break;
+      }
+      const int tap = it / chunks, c0 = (it - tap * chunks) * a.kc;
+      const int ky = tap / 3, kx = tap - 3 * ky;
+      unsigned char* st = smem + static_cast<size_t>(s) * a.stage_bytes;
+      const uint32_t bar = smem_addr(full + s);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(tx_bytes) : "memory");
+      tma_load_4d(smem_addr(st), &tmx, c0, x0 + kx - 1, y0 + ky - 1, b0, bar);
+      tma_load_3d(smem_addr(st + a.a_tile_bytes), &tmw, c0, n0, tap, bar);
+      ++issued;
+    }
+    // copies still in flight land before the CTA can end (no-op when all were consumed)
+    for (int it = issued > S ? issued - S : 0; it < issued; ++it)
+      if (!wait_parity(smem_addr(full + it % S), (it / S) & 1, a.error)) atomicExch(&cta_error, 1);
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer ----
+    bool ok = true;
+    for (int it = 0; it < iters && ok; ++it) {
+      const int s = it % S;
+      if (!wait_parity(smem_addr(full + s), (it / S) & 1, a.error)) {
+        atomicExch(&cta_error, 1);
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      unsigned char* st = smem + static_cast<size_t>(s) * a.stage_bytes;
+      const uint64_t ad = smem_desc(smem_addr(st), a.kc * 2);
+      const uint64_t bd = smem_desc(smem_addr(st + a.a_tile_bytes), a.kc * 2);
+      for (int k = 0; k < a.kc / 16; ++k)  // 16 elements = 32 bytes = 2 descriptor units
+        umma_f16(tmem, ad + 2 * k, bd + 2 * k, a.idesc, (it > 0 || k > 0) ? 1u : 0u);
+      umma_commit(smem_addr(empty + s));
+    }
+    if (ok) umma_commit(smem_addr(acc));
+  }
+  __syncwarp();
+
+  // ---- epilogue: TMEM lanes 32*warp .. +31 = pixels, columns = output channels ----
+  const bool ready = wait_parity(smem_addr(acc), 0, a.error);
+  if (!ready) atomicExch(&cta_error, 1);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (!cta_error) {
+    const int row = warp * 32 + lane;
+    const long long pixel = static_cast<long long>(m0) + row;
+    const bool valid = pixel < a.pixels;
+    for (int cb = 0; cb < a.n_tile / 32; ++cb) {
+      float v[32];
+      tmem_load_32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + cb * 32, v);
+      if (!valid) continue;
+      const int co = n0 + cb * 32;
+      if (kMode == 0) {
+        __align__(16) __nv_bfloat162 h[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const float x0v = fmaxf(v[2 * j] + a.bias[co + 2 * j], 0.0f);
+          const float x1v = fmaxf(v[2 * j + 1] + a.bias[co + 2 * j + 1], 0.0f);
+          h[j] = __floats2bfloat162_rn(x0v, x1v);
+        }
+        uint4* dst = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(a.y) + pixel * a.cout + co);
+        const uint4* src = reinterpret_cast<const uint4*>(h);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dst[j] = src[j];
+      } else {
+        float4* dst = reinterpret_cast<float4*>(static_cast<float*>(a.y) + pixel * a.cout + co);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.tmem_cols));
+  if (threadIdx.x == 0 && cta_error) atomicExch(a.error, 1);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+CUtensorMapSwizzle swizzle_for(int row_bytes) {
+  return row_bytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
+         : row_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
+                           : CU_TENSOR_MAP_SWIZZLE_32B;
+}
+
+int pow2_at_least(int v, int lo) {
+  int p = lo;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
+
+}  // namespace
+
+const char* make_plan(ConvPlan* p, const void* x, const void* w, int batch, int height, int width, int cin, int cout) {
+  std::memset(p, 0, sizeof(*p));
+  if (!is_pow2(width) || !is_pow2(height) || batch < 1) return "image sides must be powers of two";
+  if (cin % 16 != 0 || cout % 32 != 0) return "channel counts must be multiples of 16 (in) and 32 (out)";
+  auto fn = encode_fn();
+  if (!fn) return "cuTensorMapEncodeTiled is not available";
+  ConvArgs& a = p->args;
+  a.height = height;
+  a.width = width;
+  a.cin = cin;
+  a.cout = cout;
+  a.pixels = static_cast<long long>(batch) * height * width;
+  a.kc = cin % 64 == 0 ? 64 : (cin % 32 == 0 ? 32 : 16);
+  a.n_tile = cout <= 256 ? cout : (cout % 128 == 0 ? 128 : 64);
+  if (cout > 256 && cout % a.n_tile != 0) return "unsupported output channel count";
+  a.tmem_cols = pow2_at_least(a.n_tile, 32);
+  a.a_tile_bytes = 128 * a.kc * 2;
+  const int b_tile = a.n_tile * a.kc * 2;
+  a.a_bytes = a.a_tile_bytes;
+  a.b_bytes = b_tile;
+  a.stage_bytes = a.a_tile_bytes + ((b_tile + 1023) / 1024) * 1024;
+  // a ring of at most ~100 KB, so that two CTAs fit on an SM (one's epilogue
+  // overlaps the other's main loop; 2 x 256 TMEM columns at most)
+  a.stages = 100 * 1024 / a.stage_bytes;
+  if (a.stages > 8) a.stages = 8;
+  if (a.stages < 2) return "operand tiles do not fit in shared memory";
+  p->smem = static_cast<size_t>(a.stages) * a.stage_bytes + (2 * a.stages + 1) * 8 + 16 + 1024;
+  // instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128, N = n_tile
+  cute::UMMA::InstrDescriptor id;
+  id.desc_ = 0;
+  id.c_format_ = 1;  // F32
+  id.a_format_ = 1;  // BF16
+  id.b_format_ = 1;  // BF16
+  id.a_major_ = 0;
+  id.b_major_ = 0;
+  id.n_dim_ = static_cast<uint16_t>(a.n_tile >> 3);
+  id.m_dim_ = static_cast<uint16_t>(128 >> 4);
+  a.idesc = id.desc_;
+  // activation boxes: 128 pixels as whole rows, or whole images
+  const int bw = width < 128 ? width : 128;
+  const int bh = (128 / bw) < height ? 128 / bw : height;
+  const int bb = 128 / (bw * bh);
+  cuuint64_t xd[4] = {static_cast<cuuint64_t>(cin), static_cast<cuuint64_t>(width), static_cast<cuuint64_t>(height),
+                      static_cast<cuuint64_t>(batch)};
+  cuuint64_t xs[3] = {static_cast<cuuint64_t>(cin) * 2, static_cast<cuuint64_t>(width) * cin * 2,
+                      static_cast<cuuint64_t>(height) * width * cin * 2};
+  cuuint32_t xbox[4] = {static_cast<cuuint32_t>(a.kc), static_cast<cuuint32_t>(bw), static_cast<cuuint32_t>(bh),
+                        static_cast<cuuint32_t>(bb)};
+  cuuint32_t ones[4] = {1, 1, 1, 1};
+  if (fn(&p->tmap_x, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(x), xd, xs, xbox, ones,
+         CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_for(a.kc * 2), CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return "activation tensor map rejected";
+  cuuint64_t wd[3] = {static_cast<cuuint64_t>(cin), static_cast<cuuint64_t>(cout), 9};
+  cuuint64_t ws[2] = {static_cast<cuuint64_t>(cin) * 2, static_cast<cuuint64_t>(cout) * cin * 2};
+  cuuint32_t wbox[3] = {static_cast<cuuint32_t>(a.kc), static_cast<cuuint32_t>(a.n_tile), 1};
+  if (fn(&p->tmap_w, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(w), wd, ws, wbox, ones,
+         CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_for(a.kc * 2), CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return "weight tensor map rejected";
+  p->grid_m = static_cast<int>((a.pixels + 127) / 128);
+  p->grid_n = cout / a.n_tile;
+  return nullptr;
+}
+
+cudaError_t launch(const ConvPlan& p, int mode, const float* bias, void* y, int* error, cudaStream_t stream) {
+  ConvArgs a = p.args;
+  a.bias = bias;
+  a.y = y;
+  a.error = error;
+  dim3 grid(p.grid_m, p.grid_n);
+  if (mode == 0) {
+    cudaFuncSetAttribute(conv_umma_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(p.smem));
+    conv_umma_kernel<0><<<grid, kThreads, p.smem, stream>>>(p.tmap_x, p.tmap_w, a);
+  } else {
+    cudaFuncSetAttribute(conv_umma_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(p.smem));
+    conv_umma_kernel<1><<<grid, kThreads, p.smem, stream>>>(p.tmap_x, p.tmap_w, a);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace gg_umma

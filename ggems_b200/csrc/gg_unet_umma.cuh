@@ -1,0 +1,48 @@
+// tcgen05 implicit-GEMM 3x3 convolution of the scatter-surrogate U-Net
+// (gg_unet_umma.cu).  A plan holds the two TMA tensor maps (NHWC BF16
+// activations, [tap][cout][cin] BF16 weights) and the tile configuration of one
+// convolution; it is made once per layer and direction and launched as often
+// as needed (the tensors it points to must stay where they are).
+#ifndef GG_UNET_UMMA_CUH
+#define GG_UNET_UMMA_CUH
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace gg_umma {
+
+struct ConvArgs {
+  int height, width, cin, cout;
+  long long pixels;   // batch * height * width
+  int kc;             // input channels per reduction chunk (16, 32 or 64)
+  int n_tile;         // output channels per CTA
+  int tmem_cols;      // TMEM columns allocated (power of two >= n_tile)
+  int stages;         // shared-memory ring depth
+  int a_tile_bytes, a_bytes, b_bytes, stage_bytes;
+  uint32_t idesc;     // tcgen05.mma instruction descriptor
+  const float* bias;  // mode 0 only
+  void* y;            // mode 0: BF16 [pixels][cout]; mode 1: FP32 [pixels][cout]
+  int* error;         // set to 1 when a wait gave up
+};
+
+struct ConvPlan {
+  CUtensorMap tmap_x;
+  CUtensorMap tmap_w;
+  ConvArgs args;
+  size_t smem;
+  int grid_m, grid_n;
+};
+
+// x: [batch][height][width][cin] BF16, w: [9][cout][cin] BF16 (device).
+// Returns NULL, or why the shape is not supported.
+const char* make_plan(ConvPlan* plan, const void* x, const void* w, int batch, int height, int width, int cin, int cout);
+
+// mode 0: y = relu(conv + bias) as BF16; mode 1: y = conv as FP32.
+cudaError_t launch(const ConvPlan& plan, int mode, const float* bias, void* y, int* error, cudaStream_t stream);
+
+}  // namespace gg_umma
+
+#endif

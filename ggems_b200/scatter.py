@@ -55,6 +55,8 @@ def _lib():
         "gg_unet_last_error": (C.c_char_p, []),
         "gg_line_integrals": (C.c_int, [C.c_void_p, P(abi.gg_solid), P(abi.gg_solid), P(C.c_float), P(C.c_float),
                                         C.c_int32, P(C.c_float)]),
+        "gg_line_integrals_batch": (C.c_int, [C.c_void_p, P(abi.gg_solid), P(abi.gg_solid), P(C.c_float), C.c_int32,
+                                              P(C.c_float), C.c_int32, P(C.c_float)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -242,18 +244,48 @@ class Geometry:
             raise RuntimeError(lib.gg_last_error().decode())
         return out.reshape(self.side, self.side)
 
-    def simulate(self, projections, primaries, seed=777):
+    def network_inputs(self, projections):
+        """[n, side, side, 2] FP32 network inputs (exp(-L), L): one batched
+        projector call per run of projections that share a phantom."""
+        out = np.empty((len(projections), self.side, self.side, 2), np.float32)
+        lib = _lib()
+        k = 0
+        while k < len(projections):
+            labels = projections[k][1]
+            e = k
+            while e < len(projections) and projections[e][1] is labels:
+                e += 1
+            dets = (abi.gg_solid * (e - k))()
+            pos = np.empty((e - k, 3), np.float32)
+            ph = None
+            for j in range(k, e):
+                src, ph, det = self.projection(projections[j][0], labels, 0)
+                dets[j - k] = det
+                pos[j - k] = (src.matrix[3], src.matrix[7], src.matrix[11])
+            rc = lib.gg_line_integrals_batch(self.ctx, C.byref(ph), dets, abi.ptr(pos, C.c_float), e - k,
+                                             abi.ptr(self.mu, C.c_float), len(self.mu),
+                                             abi.ptr(out[k:e], C.c_float))
+            if rc != 0:
+                raise RuntimeError(lib.gg_last_error().decode())
+            k = e
+        return out
+
+    def simulate(self, projections, primaries, seed=777, totals=True):
         """Run the projections (list of (angle, labels)) as the jobs of one
-        launch; returns (total, scatter) histograms [n, side, side] (counts)."""
+        launch; returns (total, scatter) histograms [n, side, side] (counts).
+        With totals=False every job's total histogram is one shared scratch
+        histogram and `total` is None (the judge needs scatter only)."""
         from ._native import _job_array, check
         n = len(projections)
         keep, jobs = [], []
         for k, (angle, labels) in enumerate(projections):
-            src, ph, det = self.projection(angle, labels, 2 * k)
+            src, ph, det = self.projection(angle, labels, 2 * k if totals else 0)
+            if not totals:
+                det.scatter_histogram = 1 + k
             arr = (abi.gg_solid * 2)(ph, det)
             keep.append((src, arr, labels))
             jobs.append((src, primaries, arr))
-        sizes = np.full(2 * n, self.side * self.side, np.int32)
+        sizes = np.full(2 * n if totals else n + 1, self.side * self.side, np.int32)
         sc = abi.gg_scene()
         C.pointer(sc)[0] = self.scene
         sc.number_of_histograms = 2 * n
@@ -271,6 +303,8 @@ class Geometry:
         ms, la = C.c_float(), C.c_int64()
         lib.gg_last_run_stats(self.ctx, C.byref(ms), C.byref(la))
         self.last_ms = ms.value
+        if not totals:
+            return None, np.stack(T.histograms[1:]).reshape(n, self.side, self.side).astype(np.float32)
         total = np.stack(T.histograms[0::2]).reshape(n, self.side, self.side).astype(np.float32)
         scatter = np.stack(T.histograms[1::2]).reshape(n, self.side, self.side).astype(np.float32)
         return total, scatter
@@ -298,12 +332,7 @@ def smooth(img, blocks=32):
 
 def make_inputs(geometry, projections):
     """[n, side, side, 2]: primary transmission exp(-L) and line integral L."""
-    out = []
-    for k, (angle, labels) in enumerate(projections):
-        src, ph, det = geometry.projection(angle, labels, 0)
-        L = geometry.line_integrals(src, ph, det)
-        out.append(np.stack([np.exp(-L), L], axis=-1))
-    return np.stack(out).astype(np.float32)
+    return geometry.network_inputs(projections)
 
 
 def judge(predicted, low_count_mc, tolerance=JUDGE_TOLERANCE):
@@ -369,6 +398,37 @@ def predict(net, inputs):
     return np.concatenate(out)
 
 
+# (C_in, C_out, down-sampling factor) of the 14 3x3 convolutions (csrc/gg_unet.cu)
+LAYERS = [(16, 32, 1), (32, 32, 1), (32, 64, 2), (64, 64, 2), (64, 128, 4), (128, 128, 4), (128, 256, 8),
+          (256, 256, 8), (384, 128, 4), (128, 128, 4), (192, 64, 2), (64, 64, 2), (96, 32, 1), (32, 32, 1)]
+
+
+def forward_flops(side, batch):
+    """Tensor-core FLOPs of one forward pass: sum over the convolutions of
+    2 * 9 * C_in * C_out * pixels (the first layer's 16 input channels are the
+    padded width the tensor cores compute)."""
+    return sum(2 * 9 * ci * co * batch * (side // d) ** 2 for ci, co, d in LAYERS)
+
+
+def time_network(side=256, batch=8, repeats=20):
+    """Device time of the forward pass (CUDA events) and its TFLOP/s."""
+    import torch
+    net = UNet(batch, side, seed=1)
+    x = torch.rand((batch, side, side, 2), device="cuda")
+    for _ in range(3):
+        net.forward(x)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    for _ in range(repeats):
+        net.forward(x)
+    stop.record()
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(stop) / repeats
+    net.close()
+    return ms, forward_flops(side, batch) / (ms * 1e-3) / 1e12
+
+
 def save_network(net, path):
     np.savez(path, parameters=net.parameters(), target_scale=np.float64(getattr(net, "target_scale", 1.0)))
 
@@ -386,17 +446,19 @@ def surrogate_pipeline(geo, net, projections, judge_primaries, seed):
     Returns (final, prediction, low-count MC, kept flags, seconds)."""
     import torch
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    t = [time.perf_counter()]
     x = make_inputs(geo, projections)
+    t.append(time.perf_counter())
     pred = predict(net, x)
-    low = []
-    for s in range(0, len(projections), 64):
-        _, sc = geo.simulate(projections[s:s + 64], int(judge_primaries), seed=seed + s)
-        low.append(sc)
-    low = normalise(np.concatenate(low), judge_primaries, geo.side)
-    final, used = judge(pred, low)
     torch.cuda.synchronize()
-    return final, pred, low, used, time.perf_counter() - t0
+    t.append(time.perf_counter())
+    _, low = geo.simulate(projections, int(judge_primaries), seed=seed, totals=False)
+    low = normalise(low, judge_primaries, geo.side)
+    t.append(time.perf_counter())
+    final, used = judge(pred, low)
+    t.append(time.perf_counter())
+    geo.last_breakdown = {"inputs": t[1] - t[0], "network": t[2] - t[1], "judge_mc": t[3] - t[2], "judge": t[4] - t[3]}
+    return final, pred, low, used, t[-1] - t[0]
 
 
 def main(argv=None):
@@ -414,7 +476,22 @@ def main(argv=None):
     ap.add_argument("--chunk", type=int, default=64, help="projections per batched MC launch")
     ap.add_argument("--save", help="write the trained network (.npz)")
     ap.add_argument("--load", help="skip data generation and training: load a trained network (.npz)")
+    ap.add_argument("--network-only", action="store_true", help="time the network's forward pass only")
     args = ap.parse_args(argv)
+    if args.network_only:
+        ms, tflops = time_network(args.side, args.batch)
+        peaks = None
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except (OSError, ValueError):
+            pass
+        peak = peaks["bf16_tflops"] if peaks else 1590.0
+        print(json.dumps({"metric": "U-Net forward TFLOP/s", "side": args.side, "batch": args.batch,
+                          "ms_per_forward": ms, "ms_per_projection": ms / args.batch,
+                          "gflop_per_forward": forward_flops(args.side, args.batch) / 1e9,
+                          "tflops": tflops, "peak_tflops": peak, "frac": tflops / peak,
+                          "peak_source": "measured" if peaks else "fallback"}), flush=True)
+        return 0
     import torch  # (CUDA memory for the network's device arrays)
     work = tempfile.mkdtemp(prefix="ggems_scatter_")
     geo = Geometry(args.side, work)
@@ -462,11 +539,17 @@ def main(argv=None):
     scan = [(360.0 * k / args.angles, phantom) for k in range(args.angles)]
     surrogate_pipeline(geo, net, scan[:8], args.judge_primaries, 99)  # warm-up
     s_final, s_pred, s_low, s_used, t_scan = surrogate_pipeline(geo, net, scan, args.judge_primaries, 4321)
+    breakdown = {k: v / args.angles * 1e3 for k, v in geo.last_breakdown.items()}
     picked = list(range(0, args.angles, args.reference_every))
     _, s_ref_scan, _ = simulate_all([scan[k] for k in picked], args.reference_primaries)
     ref_scan = normalise(s_ref_scan, args.reference_primaries, side)
     scan_err = [relative_error(s_final[k], r) for k, r in zip(picked, ref_scan)]
     scan_low = [relative_error(s_low[k], r) for k, r in zip(picked, ref_scan)]
+
+    def integral_errors(est, refs):
+        return [abs(float(e.sum()) - float(r.sum())) / float(r.sum()) for e, r in zip(est, refs)]
+    net_int = integral_errors([s_pred[k] for k in picked], ref_scan) + integral_errors(pred, ref)
+    low_int = integral_errors([s_low[k] for k in picked], ref_scan) + integral_errors(low, ref)
     # plain MC: primaries for 5 % error by Poisson scaling of the low-count error; its
     # projections/s timed directly on 16 scan angles at that count (one batched launch)
     e_low = float(np.mean(scan_low))
@@ -486,7 +569,12 @@ def main(argv=None):
         "speedup": sur_per_s / plain_per_s,
         "scan": {"angles": args.angles, "seconds": t_scan, "judge_kept": float(s_used.mean()),
                  "error_mean": float(np.mean(scan_err)), "error_max": float(np.max(scan_err)),
-                 "low_count_mc_error": e_low, "reference_angles": len(picked)},
+                 "low_count_mc_error": e_low, "reference_angles": len(picked),
+                 "ms_per_projection": breakdown},
+        "integrated_scatter_error": {"network_rms": float(np.sqrt(np.mean(np.square(net_int)))),
+                                     "network_max": float(np.max(net_int)),
+                                     "judge_mc_rms": float(np.sqrt(np.mean(np.square(low_int)))),
+                                     "projections": len(net_int)},
         "new_phantoms": {"projections": args.test, "network_error": float(np.mean(err_net)),
                          "judged_error": float(np.mean(err_sur)), "judged_error_max": float(np.max(err_sur)),
                          "low_count_mc_error": float(np.mean(err_low)), "judge_kept": float(used.mean())},

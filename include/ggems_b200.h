@@ -316,7 +316,9 @@ GG_API int gg_autotune(gg_context* context, const gg_source* source, uint64_t nu
  * A 4-level BF16 U-Net (base 32 channels, FP32 accumulation) mapping a CBCT
  * primary projection and the phantom's line-integral map to the scatter
  * projection, trained and run with this library's own kernels
- * (ggems_b200/csrc/gg_unet.cu).  Images are square, side a multiple of 64.
+ * (ggems_b200/csrc/gg_unet.cu, convolutions on tcgen05 in gg_unet_umma.cu).
+ * Images are square, side a power of two (>= 64).  A call whose tensor-core
+ * convolution gave up waiting for its operands returns GG_ERROR_TIMEOUT.
  * Arrays are DEVICE pointers: input [batch][side][side][2] (primary, line
  * integral), target / output [batch][side][side], all FP32.  Parameters are a
  * flat FP32 vector of gg_unet_parameter_count() values. */
@@ -328,6 +330,12 @@ GG_API int gg_autotune(gg_context* context, const gg_source* source, uint64_t nu
 GG_API int gg_line_integrals(gg_context* context, const gg_solid* phantom, const gg_solid* detector,
                              const float* source_position, const float* mu, int32_t number_of_materials,
                              float* line_integrals);
+/* The same for `count` projections of one phantom (a scan): detectors[count]
+ * and source_positions[count][3], written as the surrogate network's input,
+ * inputs[count][ey][ex][2] = (exp(-L), L) (host array, FP32). */
+GG_API int gg_line_integrals_batch(gg_context* context, const gg_solid* phantom, const gg_solid* detectors,
+                                   const float* source_positions, int32_t count, const float* mu,
+                                   int32_t number_of_materials, float* inputs);
 typedef struct gg_unet gg_unet;
 GG_API int gg_unet_create(int32_t batch, int32_t side, uint64_t seed, gg_unet** net);
 GG_API int gg_unet_destroy(gg_unet* net);

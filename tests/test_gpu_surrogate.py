@@ -117,6 +117,19 @@ def test_line_integrals_match_ray_sampling(geometry):
         assert abs(L[j, i] - ref) <= 0.01 * max(ref, 0.05), (i, j, L[j, i], ref)
 
 
+def test_batched_inputs_match_single_projections(geometry):
+    """gg_line_integrals_batch (one phantom, several angles) writes (exp(-L), L)
+    equal to the single-projection projector's L."""
+    from ggems_b200.scatter import random_phantom
+    labels = random_phantom(np.random.default_rng(8))
+    projs = [(a, labels) for a in (0.0, 33.0, 90.0, 211.5)]
+    x = geometry.network_inputs(projs)
+    for k, (angle, lab) in enumerate(projs):
+        L = geometry.line_integrals(*geometry.projection(angle, lab, 0))
+        assert np.array_equal(x[k, ..., 1], L)
+        np.testing.assert_allclose(x[k, ..., 0], np.exp(-L), rtol=2e-6, atol=0)
+
+
 def test_projector_primary_matches_mc_primary(geometry):
     """exp(-L) (projector) vs total - scatter (MC) at 60 keV: same shape."""
     from ggems_b200.scatter import random_phantom
