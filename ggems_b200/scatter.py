@@ -288,7 +288,7 @@ class Geometry:
         sizes = np.full(2 * n if totals else n + 1, self.side * self.side, np.int32)
         sc = abi.gg_scene()
         C.pointer(sc)[0] = self.scene
-        sc.number_of_histograms = 2 * n
+        sc.number_of_histograms = len(sizes)
         sc.histogram_sizes = abi.ptr(sizes, C.c_int32)
         lib = self.lib
         check(lib.gg_upload_scene(self.ctx, C.byref(sc)), "gg_upload_scene")
