@@ -226,9 +226,10 @@ def main():
     ap.add_argument("--primaries", type=int, default=PRIMARIES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
-    ap.add_argument("--workload", default="cbct", choices=["cbct", "batched", "mesh", "volume"],
-                    help="cbct: the CBCT projection (default); batched: 360 angles + 16 phantoms in one launch; "
-                         "mesh: meshed-phantom dosimetry; volume: CT image -> material labels on the device")
+    ap.add_argument("--workload", default="cbct", choices=["cbct", "water", "batched", "mesh", "volume"],
+                    help="cbct: the CBCT projection (default); water: 64^3 water dosimetry, 1e6 primaries; "
+                         "batched: 360 angles + 16 phantoms in one launch; mesh: meshed-phantom dosimetry; "
+                         "volume: CT image -> material labels on the device")
     ap.add_argument("--mesh-subdivisions", type=int, default=6, help="icosphere subdivisions of the mesh body")
     ap.add_argument("--primaries-per-job", type=int, default=10_000_000)
     args = ap.parse_args()
@@ -250,6 +251,8 @@ def main():
         return run_mesh(args, tmp, rank)
     if args.workload == "volume":
         return run_volume(args, rank)
+    if args.workload == "water":
+        return run_water(args, tmp, rank)
 
     import torch
     dist = None
@@ -587,6 +590,91 @@ def run_mesh(args, tmp, rank):
                        "primaries_per_step": args.primaries, "dose_grid": list(d.number_of_dosels),
                        "l2": "256 MB buffer written between timed steps"},
             "gpu_launches": launches, "clocks": clk.summary()}), flush=True)
+    return 0
+
+
+def run_water(args, tmp, rank):
+    """Water dosimetry: 64^3 water of 2 mm voxels, 60 keV cone, edep / E^2 / hit
+    tallies and the dose + uncertainty finalisation, 1e6 primaries per step,
+    through the GGEMS API.  `value` = device-timed primaries/s of the transport
+    launch; `e2e` = scene and random states uploaded, run, dose finalised and
+    tallies read back to host memory, wall-clocked."""
+    import numpy as np
+    import torch
+    from ggems_b200 import abi, workloads
+    from ggems_b200.api import lib
+    n = 1_000_000 if args.primaries == PRIMARIES else args.primaries
+    files = workloads.water_files(tmp, 64, 2.0)
+    gg, _ = _configure_water(files, n)
+    ggems = gg.GGEMS()
+    ggems.initialize(777)
+    ctx = lib.ggems_device_context(ggems.obj, 0)
+    src = abi.gg_source()
+    assert lib.ggems_source_descriptor(0, C.byref(src), None) == 0
+    scene_ptr = lib.ggems_scene(ggems.obj)
+    sc = scene_ptr.contents
+    dm = sc.dose_maps[0]
+    nd = int(dm.total_number_of_dosels)
+    dose, unc = np.empty(nd, np.float32), np.empty(nd, np.float32)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def check(rc, what):
+        if rc != 0:
+            raise RuntimeError("%s: %s" % (what, lib.gg_last_error().decode()))
+
+    def step():
+        check(lib.gg_run_source(ctx, C.byref(src), n), "gg_run_source")
+        check(lib.gg_synchronize(ctx), "gg_synchronize")
+        t, k = C.c_float(), C.c_int64()
+        lib.gg_last_run_stats(ctx, C.byref(t), C.byref(k))
+        return t.value, k.value
+
+    for _ in range(args.warmup):
+        step()
+    times, launches = [], 0
+    with ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t, k = step()
+            times.append(t)
+            launches += k
+    total_ms = sum(times)
+    value = n * args.steps / (total_ms * 1e-3)
+    states = np.frombuffer(C.string_at(lib.ggems_initial_random_states(ggems.obj, 0), 5 * abi.GG_MAXIMUM_PARTICLES * 4),
+                           np.uint32).copy()
+    tallies = abi.Tallies([], [nd])
+    e2e = []
+    for k in range(args.steps + 1):
+        t0 = time.perf_counter()
+        check(lib.gg_upload_scene(ctx, scene_ptr), "gg_upload_scene")
+        check(lib.gg_set_random_states(ctx, abi.ptr(states, C.c_uint32), abi.GG_MAXIMUM_PARTICLES), "states")
+        step()
+        check(lib.gg_compute_dose(ctx, 0, 0, C.c_float(1.0), 0, C.c_float(0.0), abi.ptr(dose, C.c_float),
+                                  abi.ptr(unc, C.c_float)), "gg_compute_dose")
+        check(lib.gg_read_tallies(ctx, C.byref(tallies.struct)), "gg_read_tallies")
+        if k:
+            e2e.append(time.perf_counter() - t0)
+    cpu = None
+    if not args.no_cpu_baseline:
+        kind = _cpu_kind()
+        threads = os.cpu_count() or 1
+        m = _sample_size(scene_ptr, src, threads, kind, 10.0)
+        dt, _ = cpu_reference_run(scene_ptr, src, m, threads, kind)
+        cpu = {"value": m / dt, "unit": "primaries/s", "cores": threads, "kind": kind,
+               "sample": "%d primaries of the same run (seed 777) on %d host threads, %.1f s" % (m, threads, dt)}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "primaries/s (64^3 water dosimetry, 60 keV)", "value": value, "unit": "primaries/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (uniform water phantom)",
+            "config": {"workload": "water64_2mm_60keV_dose", "primaries_per_step": n,
+                       "tallies": "edep, edep^2, hit; dose + uncertainty in e2e",
+                       "l2": "256 MB buffer written between timed steps"},
+            "e2e": {"value": n * len(e2e) / sum(e2e), "unit": "primaries/s",
+                    "h2d_bytes_per_step": 64 ** 3 + states.nbytes, "d2h_bytes_per_step": nd * (4 + 4 + 8 + 8 + 4)},
+            "gpu_launches": launches, "cpu_baseline": cpu, "clocks": clk.summary()}), flush=True)
     return 0
 
 
