@@ -140,18 +140,23 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def _profile_traffic():
-    """DRAM bytes per transport launch from the committed ncu summary, if present."""
+def _profile_value(key):
+    """A figure from the committed ncu summary of the transport kernel ("key: value" lines)."""
     path = os.path.join(ROOT, "profiles", "transport_kernel_cbct256.md")
     if not os.path.exists(path):
         return None
     for line in open(path):
-        if line.startswith("dram_bytes_per_full_launch:"):
+        if line.startswith(key + ":"):
             try:
                 return float(line.split(":")[1].split()[0])
             except (IndexError, ValueError):
                 return None
     return None
+
+
+def _profile_traffic():
+    """DRAM bytes per transport launch from the committed ncu summary, if present."""
+    return _profile_value("dram_bytes_per_full_launch")
 
 
 def _peaks():
@@ -388,7 +393,11 @@ def main():
                 "traffic": per_launch_traffic,
                 "peak_source": "measured" if peaks else "fallback",
                 "bytes_per_primary": bytes_per_primary,
-                "voxel_steps_per_primary": S, "box_steps_per_primary": box, "detector_counts_per_primary": H}
+                "voxel_steps_per_primary": S, "box_steps_per_primary": box, "detector_counts_per_primary": H,
+                # issue-bound kernel: what the ncu summary says about the issue slots and lanes
+                "l2_hit_rate_pct": _profile_value("l2_hit_rate_pct"),
+                "issue_active_pct": _profile_value("issue_active_pct"),
+                "lanes_active_pct": _profile_value("lanes_active_pct")}
     line = {
         "metric": "primaries/s (CBCT 256^3, 120 kVp)", "value": value, "unit": "primaries/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
