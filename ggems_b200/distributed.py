@@ -75,4 +75,7 @@ def reduce_tallies(tallies, group=None):
     for arrays in (tallies.histograms, tallies.edep, tallies.edep_squared, tallies.hit, tallies.photon_tracking):
         for a in arrays:
             _all_reduce_sum(a, dist, group)
+    # world grid (GGEMSWorld::SaveResults sums its devices' grids, GGEMSWorld.cc:423-602)
+    for a in (tallies.world or {}).values():
+        _all_reduce_sum(a, dist, group)
     return tallies

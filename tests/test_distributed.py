@@ -39,6 +39,7 @@ def test_random_streams_follow_device_order():
 
 def _scene():
     sc = scenes.cbct_scene(n=32, voxel=8.0, elements=(64, 64, 1), element_size=(6.4, 6.4, 10.0))
+    sc.set_world((20, 16, 10), (120.0, 100.0, 80.0))
     src = scenes.XRaySource(spectrum=scenes.synthetic_spectrum(), aperture_deg=11.0)
     return sc, src
 
@@ -56,6 +57,7 @@ def _rank_main(rank, world, port, total, out_dir):
         _, T, _ = parity.run_oracle(sc, src, n, states=states, threads=2)
         distributed.reduce_tallies(T)
         np.save(os.path.join(out_dir, "h%d.npy" % rank), np.concatenate(T.histograms))
+        np.save(os.path.join(out_dir, "w%d.npy" % rank), T.world["photon_tracking"])
     finally:
         dist.destroy_process_group()
 
@@ -83,10 +85,16 @@ def test_two_gloo_ranks_match_two_ggems_devices(tmp_path):
     # GGEMS with two devices: device d simulates its share with its streams; histograms summed.
     sc, src = _scene()
     expected = None
+    world_expected = None
     for d in range(world):
         n = total // world + (1 if d < total % world else 0)
         _, T, _ = parity.run_oracle(sc, src, n, states=scenes.seed_states(777, skip=d * abi.GG_MAXIMUM_PARTICLES))
         h = np.concatenate(T.histograms).astype(np.int64)
         expected = h if expected is None else expected + h
+        w = T.world["photon_tracking"].astype(np.int64)
+        world_expected = w if world_expected is None else world_expected + w
     assert np.array_equal(h0.astype(np.int64), expected)
     assert expected.sum() > 0
+    w0, w1 = np.load(tmp_path / "w0.npy"), np.load(tmp_path / "w1.npy")
+    assert np.array_equal(w0, w1) and np.array_equal(w0.astype(np.int64), world_expected)
+    assert world_expected.sum() > 0
