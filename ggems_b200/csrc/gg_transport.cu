@@ -879,6 +879,13 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
         __ballot_sync(0xffffffffu, phase == kTrackVoxel || phase == kTrackBox || (kFull && phase == kTrackMesh));
     const int n_other = __popc(active & ~tracking);
     if (n_other > 0 && (n_other >= regroup || 4 * n_other >= ratio4 * __popc(tracking))) {
+      // A round serves one kind of rare work: the interaction samplers, or the
+      // new-history / FindSolid chain, whichever more lanes wait for; the
+      // others wait for the next round (their code paths stay out of this
+      // one).  Measured +1.4 % on the CBCT projection.
+      const int n_interact = __popc(__ballot_sync(0xffffffffu, phase == kInteract));
+      const bool serve_interact = 2 * n_interact >= n_other;
+      if ((phase == kInteract) != serve_interact) continue;
       if (phase == kInteract) {
         // The Compton / Rayleigh part of a tracking step (the tail of
         // track_through_*): sample the interaction, then tally as the step would.

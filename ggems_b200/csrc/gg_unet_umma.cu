@@ -293,6 +293,16 @@ const char* make_plan(ConvPlan* p, const void* x, const void* w, int batch, int 
   a.kc = cin % 64 == 0 ? 64 : (cin % 32 == 0 ? 32 : 16);
   a.n_tile = cout <= 256 ? cout : (cout % 128 == 0 ? 128 : 64);
   if (cout > 256 && cout % a.n_tile != 0) return "unsupported output channel count";
+  // small images: thinner output-channel tiles until about two CTAs per SM exist
+  // (the 32^2 bottleneck has only 64 pixel tiles)
+  {
+    const long long m_tiles = (a.pixels + 127) / 128;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    while (m_tiles * (cout / a.n_tile) < 2LL * sms && a.n_tile > 64 && (a.n_tile / 2) % 32 == 0 &&
+           cout % (a.n_tile / 2) == 0)
+      a.n_tile /= 2;
+  }
   a.tmem_cols = pow2_at_least(a.n_tile, 32);
   a.a_tile_bytes = 128 * a.kc * 2;
   const int b_tile = a.n_tile * a.kc * 2;
