@@ -1122,20 +1122,21 @@ GG_API int gg_line_integrals_batch(gg_context* c, const gg_solid* phantom, const
   GG_CUDA(cudaSetDevice(c->device));
   const size_t n = static_cast<size_t>(ex) * ey;
   const size_t nv = static_cast<size_t>(phantom->number_of_voxels[0]) * phantom->number_of_voxels[1] * phantom->number_of_voxels[2];
-  std::vector<void*> tmp;
-  auto cleanup = [&]() {
-    for (void* p : tmp) cudaFree(p);
-  };
+  // stream-ordered buffers: no device-wide synchronisation (cudaFree would wait
+  // for transport running on other streams)
   float *dmu = nullptr, *dout = nullptr;
   uint8_t* dlab = nullptr;
-  int rc;
-  if ((rc = dev_copy_to(c, tmp, mu, static_cast<size_t>(number_of_materials), &dmu)) ||
-      (rc = dev_copy_to(c, tmp, phantom->labels, nv, &dlab)) ||
-      (rc = dev_copy_to(c, tmp, static_cast<const float*>(nullptr), 2 * n * count, &dout))) {
-    cleanup();
-    return rc;
-  }
-  cudaError_t e = cudaSuccess;
+  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&dmu), number_of_materials * sizeof(float), c->stream);
+  if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void**>(&dlab), nv, c->stream);
+  if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void**>(&dout), 2 * n * count * sizeof(float), c->stream);
+  auto cleanup = [&]() {
+    if (dmu) cudaFreeAsync(dmu, c->stream);
+    if (dlab) cudaFreeAsync(dlab, c->stream);
+    if (dout) cudaFreeAsync(dout, c->stream);
+  };
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dmu, mu, number_of_materials * sizeof(float), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dlab, phantom->labels, nv, cudaMemcpyHostToDevice, c->stream);
   for (int k = 0; k < count && e == cudaSuccess; ++k) {
     gg::ProjectorParams P{};
     std::memcpy(P.phantom_matrix, phantom->obb.matrix, sizeof(P.phantom_matrix));
@@ -1159,8 +1160,8 @@ GG_API int gg_line_integrals_batch(gg_context* c, const gg_solid* phantom, const
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(inputs, dout, 2 * n * count * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   cleanup();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return fail(GG_ERROR_CUDA, std::string("line integrals: ") + cudaGetErrorString(e));
   return GG_OK;
 }

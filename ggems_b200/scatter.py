@@ -101,14 +101,23 @@ class UNet:
         p = np.ascontiguousarray(p, np.float32)
         self._check(self.lib.gg_unet_set_parameters(self.handle, abi.ptr(p, C.c_float)))
 
+    @staticmethod
+    def _ready(*tensors):
+        """The network runs on its own stream: wait for the work of torch's
+        current stream (e.g. the copies that filled the inputs) first."""
+        import torch
+        torch.cuda.current_stream(tensors[0].device).synchronize()
+
     def forward(self, x):
         """x: CUDA float32 [batch, side, side, 2] -> CUDA float32 [batch, side, side]."""
         import torch
         y = torch.empty((self.batch, self.side, self.side), dtype=torch.float32, device=x.device)
+        self._ready(x, y)
         self._check(self.lib.gg_unet_forward(self.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())))
         return y
 
     def gradients(self, x, t):
+        self._ready(x, t)
         g = np.zeros(self.parameter_count(), np.float32)
         loss = C.c_float()
         self._check(self.lib.gg_unet_gradients(self.handle, C.c_void_p(x.data_ptr()), C.c_void_p(t.data_ptr()),
@@ -116,6 +125,7 @@ class UNet:
         return loss.value, g
 
     def train_step(self, x, t, lr):
+        self._ready(x, t)
         loss = C.c_float()
         self._check(self.lib.gg_unet_train_step(self.handle, C.c_void_p(x.data_ptr()), C.c_void_p(t.data_ptr()), lr,
                                                 C.byref(loss)))
@@ -200,6 +210,12 @@ class Geometry:
         self.ggems.initialize(777)
         self.lib = lib
         self.ctx = lib.ggems_device_context(self.ggems.obj, 0)
+        # the projector works in a context of its own: its stream does not queue
+        # behind the transport launches of self.ctx
+        from ._native import lib as native, check
+        h = C.c_void_p()
+        check(native.gg_context_create(0, C.byref(h)), "gg_context_create")
+        self.projector_ctx = h
         self.scene = lib.ggems_scene(self.ggems.obj).contents
         self.source = abi.gg_source()
         assert lib.ggems_source_descriptor(0, C.byref(self.source), None) == 0
@@ -238,7 +254,7 @@ class Geometry:
         out = np.zeros(self.side * self.side, np.float32)
         pos = np.array([src.matrix[3], src.matrix[7], src.matrix[11]], np.float32)
         lib = _lib()
-        rc = lib.gg_line_integrals(self.ctx, C.byref(ph), C.byref(det), abi.ptr(pos, C.c_float),
+        rc = lib.gg_line_integrals(self.projector_ctx, C.byref(ph), C.byref(det), abi.ptr(pos, C.c_float),
                                    abi.ptr(self.mu, C.c_float), len(self.mu), abi.ptr(out, C.c_float))
         if rc != 0:
             raise RuntimeError(lib.gg_last_error().decode())
@@ -262,7 +278,7 @@ class Geometry:
                 src, ph, det = self.projection(projections[j][0], labels, 0)
                 dets[j - k] = det
                 pos[j - k] = (src.matrix[3], src.matrix[7], src.matrix[11])
-            rc = lib.gg_line_integrals_batch(self.ctx, C.byref(ph), dets, abi.ptr(pos, C.c_float), e - k,
+            rc = lib.gg_line_integrals_batch(self.projector_ctx, C.byref(ph), dets, abi.ptr(pos, C.c_float), e - k,
                                              abi.ptr(self.mu, C.c_float), len(self.mu),
                                              abi.ptr(out[k:e], C.c_float))
             if rc != 0:
@@ -270,11 +286,21 @@ class Geometry:
             k = e
         return out
 
-    def simulate(self, projections, primaries, seed=777, totals=True):
-        """Run the projections (list of (angle, labels)) as the jobs of one
-        launch; returns (total, scatter) histograms [n, side, side] (counts).
+    def _states(self, seed):
+        """JKISS states of `seed` (seeded once per seed; std::mt19937 over 2^20 slots)."""
+        cache = self.__dict__.setdefault("_state_cache", {})
+        if seed not in cache:
+            st = np.zeros(5 * abi.GG_MAXIMUM_PARTICLES, np.uint32)
+            self.lib.gg_seed_random_states(abi.ptr(st, C.c_uint32), abi.GG_MAXIMUM_PARTICLES, seed, 0)
+            cache.clear()
+            cache[seed] = st
+        return cache[seed]
+
+    def start_simulation(self, projections, primaries, seed=777, totals=True):
+        """Launch the projections (list of (angle, labels)) as the jobs of one
+        asynchronous launch; finish_simulation() waits and reads the histograms.
         With totals=False every job's total histogram is one shared scratch
-        histogram and `total` is None (the judge needs scatter only)."""
+        histogram (the 5 % check needs scatter only)."""
         from ._native import _job_array, check
         n = len(projections)
         keep, jobs = [], []
@@ -285,29 +311,42 @@ class Geometry:
             arr = (abi.gg_solid * 2)(ph, det)
             keep.append((src, arr, labels))
             jobs.append((src, primaries, arr))
-        sizes = np.full(2 * n if totals else n + 1, self.side * self.side, np.int32)
+        nh = 2 * n if totals else n + 1
+        sizes = np.full(nh, self.side * self.side, np.int32)
         sc = abi.gg_scene()
         C.pointer(sc)[0] = self.scene
-        sc.number_of_histograms = len(sizes)
+        sc.number_of_histograms = nh
         sc.histogram_sizes = abi.ptr(sizes, C.c_int32)
         lib = self.lib
         check(lib.gg_upload_scene(self.ctx, C.byref(sc)), "gg_upload_scene")
-        states = np.zeros(5 * abi.GG_MAXIMUM_PARTICLES, np.uint32)
-        lib.gg_seed_random_states(abi.ptr(states, C.c_uint32), abi.GG_MAXIMUM_PARTICLES, seed, 0)
+        states = self._states(seed)
         check(lib.gg_set_random_states(self.ctx, abi.ptr(states, C.c_uint32), abi.GG_MAXIMUM_PARTICLES), "states")
         arr, kp = _job_array(jobs)
         check(lib.gg_run_jobs(self.ctx, arr, n), "gg_run_jobs")
+        return dict(n=n, nh=nh, totals=totals, keep=(keep, jobs, arr, kp, sizes, sc))
+
+    def finish_simulation(self, run):
+        """(total, scatter) histograms [n, side, side] as float32 counts (total
+        None without totals)."""
+        from ._native import check
+        lib, n, side = self.lib, run["n"], self.side
         check(lib.gg_synchronize(self.ctx), "gg_synchronize")
-        T = abi.Tallies(list(sizes), [])
-        check(lib.gg_read_tallies(self.ctx, C.byref(T.struct)), "gg_read_tallies")
+        hist = np.zeros((run["nh"], side * side), np.int32)
+        rows = (C.POINTER(C.c_int32) * run["nh"])(*[abi.ptr(hist[i], C.c_int32) for i in range(run["nh"])])
+        tb = abi.gg_tally_buffers()
+        tb.histograms = C.cast(rows, C.POINTER(C.POINTER(C.c_int32)))
+        check(lib.gg_read_tallies(self.ctx, C.byref(tb)), "gg_read_tallies")
         ms, la = C.c_float(), C.c_int64()
         lib.gg_last_run_stats(self.ctx, C.byref(ms), C.byref(la))
         self.last_ms = ms.value
-        if not totals:
-            return None, np.stack(T.histograms[1:]).reshape(n, self.side, self.side).astype(np.float32)
-        total = np.stack(T.histograms[0::2]).reshape(n, self.side, self.side).astype(np.float32)
-        scatter = np.stack(T.histograms[1::2]).reshape(n, self.side, self.side).astype(np.float32)
-        return total, scatter
+        if not run["totals"]:
+            return None, hist[1:].reshape(n, side, side).astype(np.float32)
+        h = hist.reshape(n, 2, side, side)
+        return h[:, 0].astype(np.float32), h[:, 1].astype(np.float32)
+
+    def simulate(self, projections, primaries, seed=777, totals=True):
+        """start_simulation + finish_simulation."""
+        return self.finish_simulation(self.start_simulation(projections, primaries, seed, totals))
 
 
 def normalise(counts, primaries, side):
@@ -447,17 +486,21 @@ def surrogate_pipeline(geo, net, projections, judge_primaries, seed):
     import torch
     torch.cuda.synchronize()
     t = [time.perf_counter()]
+    # the MC estimates run on the transport context's stream while the
+    # projector (its own context) and the network (its own stream) work
+    run = geo.start_simulation(projections, int(judge_primaries), seed=seed, totals=False)
+    t.append(time.perf_counter())
     x = make_inputs(geo, projections)
     t.append(time.perf_counter())
-    pred = predict(net, x)
-    torch.cuda.synchronize()
+    pred = predict(net, x)  # host arrays: the network's own stream is synchronised
     t.append(time.perf_counter())
-    _, low = geo.simulate(projections, int(judge_primaries), seed=seed, totals=False)
+    _, low = geo.finish_simulation(run)
     low = normalise(low, judge_primaries, geo.side)
     t.append(time.perf_counter())
     final, used = judge(pred, low)
     t.append(time.perf_counter())
-    geo.last_breakdown = {"inputs": t[1] - t[0], "network": t[2] - t[1], "judge_mc": t[3] - t[2], "judge": t[4] - t[3]}
+    geo.last_breakdown = {"judge_mc_launch": t[1] - t[0], "inputs": t[2] - t[1], "network": t[3] - t[2],
+                          "judge_mc_wait": t[4] - t[3], "judge": t[5] - t[4]}
     return final, pred, low, used, t[-1] - t[0]
 
 
