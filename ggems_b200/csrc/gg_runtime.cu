@@ -1079,27 +1079,27 @@ GG_API int gg_line_integrals(gg_context* c, const gg_solid* phantom, const gg_so
   std::memcpy(P.source, source_position, sizeof(P.source));
   const size_t n = static_cast<size_t>(P.elements[0]) * P.elements[1];
   const size_t nv = static_cast<size_t>(phantom->number_of_voxels[0]) * phantom->number_of_voxels[1] * phantom->number_of_voxels[2];
-  std::vector<void*> tmp;
-  auto cleanup = [&]() {
-    for (void* p : tmp) cudaFree(p);
-  };
+  // stream-ordered buffers (no device-wide synchronisation)
   float *dmu = nullptr, *dout = nullptr;
   uint8_t* dlab = nullptr;
-  int rc;
-  if ((rc = dev_copy_to(c, tmp, mu, static_cast<size_t>(number_of_materials), &dmu)) ||
-      (rc = dev_copy_to(c, tmp, phantom->labels, nv, &dlab)) ||
-      (rc = dev_copy_to(c, tmp, static_cast<const float*>(nullptr), n, &dout))) {
-    cleanup();
-    return rc;
+  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&dmu), number_of_materials * sizeof(float), c->stream);
+  if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void**>(&dlab), nv, c->stream);
+  if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void**>(&dout), n * sizeof(float), c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dmu, mu, number_of_materials * sizeof(float), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dlab, phantom->labels, nv, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) {
+    P.mu = dmu;
+    P.labels = dlab;
+    P.out = dout;
+    gg::launch_line_integrals(P, c->stream);
+    e = cudaGetLastError();
   }
-  P.mu = dmu;
-  P.labels = dlab;
-  P.out = dout;
-  gg::launch_line_integrals(P, c->stream);
-  cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(line_integrals, dout, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
+  if (dmu) cudaFreeAsync(dmu, c->stream);
+  if (dlab) cudaFreeAsync(dlab, c->stream);
+  if (dout) cudaFreeAsync(dout, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  cleanup();
   if (e != cudaSuccess) return fail(GG_ERROR_CUDA, std::string("line integrals: ") + cudaGetErrorString(e));
   return GG_OK;
 }

@@ -136,30 +136,49 @@ __host__ __device__ constexpr int context_radius(int k) { return k == 0 ? 4 : (k
 constexpr int kInputChannels = 10;  // real channels of the first layer's 16
 
 // Summed-area tables I[b][m][(S+1)^2] of the two input maps (row 0 and column 0
-// stay zero).  Pass 1: one thread per image row, prefix sums along the row.
+// stay zero).  Pass 1: one warp per image row; each lane sums S/32 consecutive
+// values, a warp scan adds the lanes before it.
 __global__ void sat_rows_kernel(const float* __restrict__ in, double* __restrict__ sat, int batch, int S) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // (b, m, y)
-  if (t >= batch * 2 * S) return;
-  const int y = t % S, m = (t / S) % 2, b = t / (2 * S);
-  const float* row = in + (static_cast<size_t>(b) * S + y) * S * 2 + m;
-  double* out = sat + (static_cast<size_t>(b) * 2 + m) * (S + 1) * (S + 1) + static_cast<size_t>(y + 1) * (S + 1) + 1;
-  double acc = 0.0;
-  for (int x = 0; x < S; ++x) {
-    acc += static_cast<double>(row[2 * x]);
-    out[x] = acc;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // (b, m, y)
+  const int lane = threadIdx.x & 31;
+  if (row >= batch * 2 * S) return;  // whole warps: blockDim is a multiple of 32
+  const int y = row % S, m = (row / S) % 2, b = row / (2 * S);
+  const int per = S / 32;  // S is a power of two >= 64
+  const float* src = in + (static_cast<size_t>(b) * S + y) * S * 2 + m + 2 * lane * per;
+  double* out = sat + (static_cast<size_t>(b) * 2 + m) * (S + 1) * (S + 1) + static_cast<size_t>(y + 1) * (S + 1) + 1 +
+                lane * per;
+  double local = 0.0;
+  for (int k = 0; k < per; ++k) local += static_cast<double>(src[2 * k]);
+  double before = local;
+  for (int o = 1; o < 32; o <<= 1) {
+    const double v = __shfl_up_sync(0xffffffffu, before, o);
+    if (lane >= o) before += v;
+  }
+  double acc = before - local;  // sum of the lanes before this one
+  for (int k = 0; k < per; ++k) {
+    acc += static_cast<double>(src[2 * k]);
+    out[k] = acc;
   }
 }
 
-// Pass 2: one thread per column (coalesced across threads), prefix sums down the column.
+// Pass 2: one thread per column (coalesced across threads), prefix sums down the
+// column, the next rows' loads issued ahead of the dependent additions.
 __global__ void sat_cols_kernel(double* __restrict__ sat, int batch, int S) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;  // (b, m, x)
   if (t >= batch * 2 * S) return;
   const int x = t % S, bm = t / S;
   double* col = sat + static_cast<size_t>(bm) * (S + 1) * (S + 1) + x + 1;
+  const size_t W = S + 1;
   double acc = 0.0;
-  for (int y = 1; y <= S; ++y) {
-    acc += col[static_cast<size_t>(y) * (S + 1)];
-    col[static_cast<size_t>(y) * (S + 1)] = acc;
+  for (int y = 1; y <= S; y += 8) {
+    double v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = col[static_cast<size_t>(y + k) * W];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      acc += v[k];
+      col[static_cast<size_t>(y + k) * W] = acc;
+    }
   }
 }
 
@@ -454,7 +473,7 @@ const bf16* layer_input(const gg_unet* n, int i) {
 int forward(gg_unet* n, const float* input) {
   const int B = n->batch, S = n->size;
   const int pixels = B * S * S;
-  sat_rows_kernel<<<(B * 2 * S + 127) / 128, 128, 0, n->stream>>>(input, n->sat, B, S);
+  sat_rows_kernel<<<(B * 2 * S * 32 + 255) / 256, 256, 0, n->stream>>>(input, n->sat, B, S);
   sat_cols_kernel<<<(B * 2 * S + 127) / 128, 128, 0, n->stream>>>(n->sat, B, S);
   pack_input_kernel<<<(pixels + 255) / 256, 256, 0, n->stream>>>(input, n->sat, n->x0, B, S);
   auto& L = n->layers;

@@ -297,8 +297,8 @@ const char* make_plan(ConvPlan* p, const void* x, const void* w, int batch, int 
   // (the 32^2 bottleneck has only 64 pixel tiles)
   {
     const long long m_tiles = (a.pixels + 127) / 128;
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    int sms = 148, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     while (m_tiles * (cout / a.n_tile) < 2LL * sms && a.n_tile > 64 && (a.n_tile / 2) % 32 == 0 &&
            cout % (a.n_tile / 2) == 0)
       a.n_tile /= 2;
