@@ -46,6 +46,8 @@ def _load():
         "gg_set_transport_tuning": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
         "gg_get_transport_tuning": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32), P(C.c_int32)]),
         "gg_autotune": (C.c_int, [C.c_void_p, P(abi.gg_source), C.c_uint64, P(C.c_float)]),
+        "gg_set_tracking": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+        "gg_read_tracking": (C.c_int, [C.c_void_p, P(abi.gg_track_point), C.c_int32, P(C.c_int32)]),
         "gg_volume_create": (C.c_int, [C.c_int32, C.c_int32, P(C.c_int32), P(C.c_float), P(C.c_void_p)]),
         "gg_volume_destroy": (C.c_int, [C.c_void_p]),
         "gg_volume_upload": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
@@ -149,6 +151,16 @@ class Context:
         ms = C.c_float()
         check(lib.gg_autotune(self.handle, C.byref(source), number_of_particles, C.byref(ms)), "gg_autotune")
         return ms.value
+
+    def set_tracking(self, slot, capacity=4096):
+        check(lib.gg_set_tracking(self.handle, slot, capacity), "gg_set_tracking")
+
+    def read_tracking(self, capacity=4096):
+        """The tracked slot's points of the last run (list of abi.gg_track_point), and how many were recorded."""
+        pts = (abi.gg_track_point * capacity)()
+        count = C.c_int32()
+        check(lib.gg_read_tracking(self.handle, pts, capacity, C.byref(count)), "gg_read_tracking")
+        return list(pts[:min(count.value, capacity)]), count.value
 
     def compute_dose(self, dose_map, solid, n, scale=1.0, water_reference=False, minimum_density=0.0,
                      uncertainty=True):

@@ -91,6 +91,14 @@ class gg_shape(C.Structure):
     _fields_ = [("type", C.c_int32), ("position", C.c_float * 3), ("label_value", C.c_float), ("size", C.c_float * 3)]
 
 
+GG_TRACK_PRIMARY, GG_TRACK_ENTER, GG_TRACK_STEP, GG_TRACK_SCATTER, GG_TRACK_LEAVE, GG_TRACK_DEAD = range(6)
+
+
+class gg_track_point(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("solid", C.c_int32), ("process", C.c_int32), ("history", C.c_int32),
+                ("E", C.c_float), ("position", C.c_float * 3), ("direction", C.c_float * 3), ("pad", C.c_float)]
+
+
 class gg_job(C.Structure):
     _fields_ = [("source", gg_source), ("number_of_particles", C.c_uint64), ("solids", C.POINTER(gg_solid))]
 

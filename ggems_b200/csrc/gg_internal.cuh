@@ -160,6 +160,11 @@ struct TransportParams {
   unsigned long long* world_energy;
   double* world_energy_squared;
   unsigned long long* world_momentum;  // [3][cells]
+  // particle tracking: the points of slot tracking_slot (-1: off), kFull variant only
+  int32_t tracking_slot;
+  int32_t tracking_capacity;
+  gg_track_point* tracking_points;
+  int32_t* tracking_count;
   int32_t regroup_lanes;            // waiting lanes that start a round of the rare phases (1..32)
   int32_t regroup_ratio4;           // ... or 4 x waiting >= regroup_ratio4 x tracking lanes
 };

@@ -76,6 +76,11 @@ struct gg_context {
   std::vector<gg::DevSolid> solid_dev_host;  // host copy of the uploaded device solids
   std::vector<char> dose_tle;             // per dose map: track-length estimator
   std::vector<const float*> density_dev;  // per navigator, for dose finalisation
+  // particle tracking: slot (-1 off) and its point buffer
+  int tracking_slot = -1;
+  int tracking_capacity = 0;
+  gg_track_point* tracking_points = nullptr;
+  int32_t* tracking_count = nullptr;
   // world tracking grid and its device tallies (NULL when not recorded)
   int32_t world_dimensions[3] = {0, 0, 0};
   float world_sizes[3] = {0.0f, 0.0f, 0.0f};
@@ -478,6 +483,8 @@ GG_API int gg_context_destroy(gg_context* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_scene(c);
   free_run(c);
+  if (c->tracking_points) cudaFree(c->tracking_points);
+  if (c->tracking_count) cudaFree(c->tracking_count);
   cudaFree(c->rng);
   cudaFree(c->particles.E);
   cudaFree(c->particles.px);
@@ -848,6 +855,14 @@ int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*
   P.error = c->error;
   P.regroup_lanes = c->regroup_lanes;
   P.regroup_ratio4 = c->regroup_ratio4;
+  P.tracking_slot = -1;
+  if (c->tracking_slot >= 0 && c->tracking_points) {
+    P.tracking_slot = c->tracking_slot;
+    P.tracking_capacity = c->tracking_capacity;
+    P.tracking_points = c->tracking_points;
+    P.tracking_count = c->tracking_count;
+    mesh = true;  // recorded by the full kernel variant
+  }
   if (c->world_cells) {
     std::memcpy(P.world_dimensions, c->world_dimensions, sizeof(P.world_dimensions));
     std::memcpy(P.world_sizes, c->world_sizes, sizeof(P.world_sizes));
@@ -875,6 +890,7 @@ int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*
 // Work-queue reset and the persistent launch, on the context's stream.
 int enqueue_jobs(gg_context* c, const JobLaunch& L) {
   GG_CUDA(cudaMemsetAsync(c->slot_counter, 0, sizeof(unsigned int), c->stream));
+  if (L.params.tracking_count) GG_CUDA(cudaMemsetAsync(L.params.tracking_count, 0, sizeof(int32_t), c->stream));
   GG_CUDA(cudaMemsetAsync(c->error, 0, sizeof(int), c->stream));
   gg::launch_transport(L.params, L.grid, L.smem, c->stream, L.mesh);
   GG_CUDA(cudaGetLastError());
@@ -1163,6 +1179,42 @@ GG_API int gg_line_integrals_batch(gg_context* c, const gg_solid* phantom, const
   cleanup();
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return fail(GG_ERROR_CUDA, std::string("line integrals: ") + cudaGetErrorString(e));
+  return GG_OK;
+}
+
+GG_API int gg_set_tracking(gg_context* c, int32_t slot, int32_t capacity) {
+  if (!c || slot >= GG_MAXIMUM_PARTICLES || (slot >= 0 && capacity < 1))
+    return fail(GG_ERROR_INVALID_ARGUMENT, "bad tracking slot or capacity");
+  GG_CUDA(cudaSetDevice(c->device));
+  GG_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->tracking_points) cudaFree(c->tracking_points);
+  if (c->tracking_count) cudaFree(c->tracking_count);
+  c->tracking_points = nullptr;
+  c->tracking_count = nullptr;
+  c->tracking_slot = -1;
+  c->tracking_capacity = 0;
+  if (slot < 0) return GG_OK;
+  GG_CUDA(cudaMalloc(&c->tracking_points, static_cast<size_t>(capacity) * sizeof(gg_track_point)));
+  GG_CUDA(cudaMalloc(&c->tracking_count, sizeof(int32_t)));
+  GG_CUDA(cudaMemset(c->tracking_count, 0, sizeof(int32_t)));
+  c->tracking_slot = slot;
+  c->tracking_capacity = capacity;
+  return GG_OK;
+}
+
+GG_API int gg_read_tracking(gg_context* c, gg_track_point* points, int32_t capacity, int32_t* count) {
+  if (!c || !count || capacity < 0 || (capacity > 0 && !points)) return fail(GG_ERROR_INVALID_ARGUMENT, "bad arguments");
+  *count = 0;
+  if (!c->tracking_points) return GG_OK;
+  GG_CUDA(cudaSetDevice(c->device));
+  GG_CUDA(cudaStreamSynchronize(c->stream));
+  int32_t n = 0;
+  GG_CUDA(cudaMemcpy(&n, c->tracking_count, sizeof(n), cudaMemcpyDeviceToHost));
+  *count = n;
+  const int32_t stored = std::min(std::min(n, c->tracking_capacity), capacity);
+  if (stored > 0)
+    GG_CUDA(cudaMemcpy(points, c->tracking_points, static_cast<size_t>(stored) * sizeof(gg_track_point),
+                       cudaMemcpyDeviceToHost));
   return GG_OK;
 }
 

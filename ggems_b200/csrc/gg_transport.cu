@@ -685,6 +685,26 @@ __device__ __noinline__ void world_track(V3 p1, V3 dir, float E, float psd, cons
   }
 }
 
+// One point of the tracked slot's trajectory (gg_track_point).
+__device__ __noinline__ void track_point(gg_track_point* points, int32_t* count, int capacity, int kind, int solid,
+                                         int process, int history, V3 p, V3 d, float E) {
+  const int i = atomicAdd(count, 1);
+  if (i >= capacity) return;
+  gg_track_point& t = points[i];
+  t.kind = kind;
+  t.solid = solid;
+  t.process = process;
+  t.history = history;
+  t.E = E;
+  t.position[0] = p.x;
+  t.position[1] = p.y;
+  t.position[2] = p.z;
+  t.direction[0] = d.x;
+  t.direction[1] = d.y;
+  t.direction[2] = d.z;
+  t.pad = 0.0f;
+}
+
 // Histogram of interaction sites in a CT detector module (the HISTOGRAM part of
 // TrackThroughGGEMSSolidBox.cl:214-236), with the scatter histogram.
 __device__ __forceinline__ void box_histogram(const DevSolid& so, const Photon& ph) {
@@ -782,6 +802,14 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
   int cached_nav = -1;
   int pending = 0;  // deferred interaction: process << 8 | material
   V3 inv_d = v3(0.0f, 0.0f, 0.0f);  // reciprocal(ph.d) while tracking inside a solid
+  int history_number = -1;           // particle tracking: histories of the slot so far
+  // particle tracking (full variant only): a point of this lane's photon when
+  // its slot is the tracked one
+  auto trk = [&](int kind, int solid, int process) {
+    if (kFull && P.tracking_points && static_cast<int>(slot) == P.tracking_slot)
+      track_point(P.tracking_points, P.tracking_count, P.tracking_capacity, kind, solid, process, history_number, ph.p,
+                  ph.d, ph.E);
+  };
 
   // A slot runs its histories of job 0, then of job 1, ... (each job is one
   // GGEMS source run; the slot's random stream carries over from run to run).
@@ -852,6 +880,7 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
       ph.p = l2g_pos(so.matrix, ph.p);
       ph.d = l2g_dir(so.matrix, ph.d);
     }
+    trk(dead ? GG_TRACK_DEAD : GG_TRACK_LEAVE, -1, -1);
     if (dead) end_history();
     else phase = kFind;
   };
@@ -895,6 +924,7 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
         const int proc = pending >> 8;
         float e0 = ph.E;
         scatter(ph, rng, proc, navs[nav], tab.energy_bins(nav), tab.sigma(nav), material, energy_id);
+        trk(GG_TRACK_SCATTER, ph.solid_id, proc);
         if (so.type != GG_SOLID_BOX) {
           // voxelized and meshed solids flag scattering; boxes do not
           // (TrackThroughGGEMSVoxelizedSolid.cl:253, TrackThroughGGEMSMeshSolid.cl:484)
@@ -927,6 +957,10 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
         ph.psd = kOutOfWorld;
         rounds = 0;
         phase = kFind;
+        if (kFull) {
+          ++history_number;
+          trk(GG_TRACK_PRIMARY, -1, -1);
+        }
       }
       if (phase != kFind) continue;
       bool end = rounds >= GG_MAX_LOOP;
@@ -969,6 +1003,7 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
         }
         if (ph.status == GG_DEAD) {
           end = true;
+          trk(GG_TRACK_DEAD, -1, -1);
         } else {
           // Enter the solid: switch to local coordinates (a meshed solid's
           // triangles are already in world coordinates).
@@ -977,6 +1012,7 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
             ph.p = g2l_pos(so.matrix, ph.p);
             ph.d = g2l_dir(so.matrix, ph.d);
           }
+          trk(GG_TRACK_ENTER, ph.solid_id, -1);
           inv_d = reciprocal(ph.d);
           phase = track_phase(so.type);
         }
@@ -1042,6 +1078,7 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
         // so it is recorded here even when the interaction itself is deferred.
         dose_record(P.dose_maps[so.dose_map], tle_edep(tab.attenuation(nav), material, ph.E, nid), ph.p);
       }
+      trk(GG_TRACK_STEP, ph.solid_id, proc);
       if (proc == GG_COMPTON_SCATTERING || proc == GG_RAYLEIGH_SCATTERING) {
         pending = (proc << 8) | material;
         phase = kInteract;
@@ -1090,6 +1127,7 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
         }
       }
       ph.p = add(ph.p, scale(ph.d, nid));
+      trk(GG_TRACK_STEP, ph.solid_id, proc);
       if (proc == GG_COMPTON_SCATTERING || proc == GG_RAYLEIGH_SCATTERING) {
         pending = proc << 8;
         phase = kInteract;
@@ -1123,6 +1161,7 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
         continue;
       }
       if (ph.E < so.threshold) ph.status = GG_DEAD;
+      trk(GG_TRACK_STEP, ph.solid_id, proc);
       if (proc == GG_COMPTON_SCATTERING || proc == GG_RAYLEIGH_SCATTERING) {
         pending = proc << 8;
         phase = kInteract;

@@ -575,6 +575,9 @@ void GGEMS::initialize(uint32_t seed) {
   }
   prepare();
   for (auto& d : devices) check_device(gg_upload_scene(d.context, &scene_), "UploadScene");
+  // GGEMS_TRACKING (set_tracking_ggems): the kernels record the tracked particle id's states
+  for (auto& d : devices)
+    check_device(gg_set_tracking(d.context, is_tracking ? tracking_id : -1, kTrackingCapacity), "Tracking");
   initialized_ = true;
   log(1, "GGEMS", "Initialize", "GGEMS initialization succeeded");
 }
@@ -667,6 +670,64 @@ void GGEMS::build_scene() {
   }
 }
 
+Profiler& Profiler::instance() {
+  static Profiler p;
+  return p;
+}
+void Profiler::add(const std::string& label, double ms) {
+  std::lock_guard<std::mutex> lock(mutex_);
+  for (auto& kv : labels_)
+    if (kv.first == label) {
+      kv.second += ms;
+      return;
+    }
+  labels_.emplace_back(label, ms);
+}
+void Profiler::reset() {
+  std::lock_guard<std::mutex> lock(mutex_);
+  labels_.clear();
+}
+// GGEMSChrono::DisplayTime (src/tools/GGEMSChrono.cc:38-49) format
+void Profiler::print_summary(std::ostream& out) const {
+  std::lock_guard<std::mutex> lock(mutex_);
+  for (const auto& kv : labels_) {
+    const long long ms = static_cast<long long>(kv.second);
+    char line[256];
+    std::snprintf(line, sizeof(line), "Elapsed time (%s): %02lld hours %02lld mins %02lld secs %03lld ms",
+                  kv.first.c_str(), ms / 3600000, (ms / 60000) % 60, (ms / 1000) % 60, ms % 1000);
+    out << "[GGEMS GGEMSChrono::DisplayTime] " << line << std::endl;
+  }
+}
+
+// The tracked particle's states in the spirit of the GGEMS_TRACKING printf
+// blocks of the reference kernels (e.g. TrackThroughGGEMSVoxelizedSolid.cl:184-210).
+void print_track(std::ostream& out, const std::vector<gg_track_point>& pts, int id, int device, int source) {
+  static const char* kKind[] = {"primary", "enter solid", "step", "interaction", "leave solid", "dead"};
+  auto process = [](int p) -> const char* {
+    switch (p) {
+      case GG_COMPTON_SCATTERING: return "Compton";
+      case GG_PHOTOELECTRIC_EFFECT: return "photoelectric";
+      case GG_RAYLEIGH_SCATTERING: return "Rayleigh";
+      case GG_TRANSPORTATION: return "transportation";
+      default: return "-";
+    }
+  };
+  const char* tag = "[GGEMS Tracking] ";
+  out << tag << "################################################################################\n";
+  out << tag << "Particle id: " << id << ", device " << device << ", source " << source << ", " << pts.size()
+      << " points\n";
+  char line[320];
+  for (const auto& t : pts) {
+    std::snprintf(line, sizeof(line),
+                  "history %d %-12s solid %2d %-14s position (x, y, z): %e %e %e mm, direction: %e %e %e, energy: %e keV\n",
+                  t.history, (t.kind >= 0 && t.kind < 6) ? kKind[t.kind] : "?", t.solid, process(t.process),
+                  t.position[0], t.position[1], t.position[2], t.direction[0], t.direction[1], t.direction[2],
+                  t.E / units::keV);
+    out << tag << line;
+  }
+  out.flush();
+}
+
 // GGEMS::Run / RunOnDevice (src/global/GGEMS.cc:303-414): one host thread per
 // device; each runs every source's share of primaries; then results are saved.
 void GGEMS::run() {
@@ -678,6 +739,7 @@ void GGEMS::run() {
   std::vector<int64_t> launches(devices.size(), 0);
   uint64_t total = 0;
   for (auto& s : sim.sources) total += s->number_of_particles;
+  std::vector<std::vector<std::vector<gg_track_point>>> traces(devices.size());  // per device, per source
   auto worker = [&](size_t d) {
     for (auto& src : sim.sources) {
       // GGEMSSource::OrganizeParticlesInBatch (src/sources/GGEMSSource.cc:379-401)
@@ -711,11 +773,22 @@ void GGEMS::run() {
       gg_last_run_stats(devices[d].context, &t, &l);
       ms[d] += t;
       launches[d] += l;
+      Profiler::instance().add("transport kernel, device index " + std::to_string(devices[d].index), t);
+      if (is_tracking) {
+        std::vector<gg_track_point> pts(kTrackingCapacity);
+        int32_t count = 0;
+        if (gg_read_tracking(devices[d].context, pts.data(), kTrackingCapacity, &count) == GG_OK) {
+          pts.resize(std::min(count, kTrackingCapacity));
+          traces[d].push_back(std::move(pts));
+        }
+      }
     }
   };
   std::vector<std::thread> threads;
   for (size_t d = 0; d < devices.size(); ++d) threads.emplace_back(worker, d);
   for (auto& t : threads) t.join();
+  for (size_t d = 0; d < devices.size(); ++d)
+    for (size_t s = 0; s < traces[d].size(); ++s) print_track(std::cout, traces[d][s], tracking_id, static_cast<int>(d), static_cast<int>(s));
   for (size_t d = 0; d < devices.size(); ++d)
     if (errors[d] != GG_OK) throw Error("GGEMS", "RunOnDevice", messages[d]);
   last_run_ms = *std::max_element(ms.begin(), ms.end());
@@ -723,6 +796,8 @@ void GGEMS::run() {
   for (auto l : launches) last_run_launches += l;
   last_run_particles = total;
   save_results();
+  // GGEMS::Run ends with the profiler summary when profiling is verbose (src/global/GGEMS.cc)
+  if (verbose[8]) Profiler::instance().print_summary(std::cout);
 }
 
 // SaveResults of GGEMSSystem (src/navigators/GGEMSSystem.cc:165-260) and

@@ -11,6 +11,7 @@
 #include <cfloat>
 #include <cstdint>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
@@ -197,6 +198,20 @@ struct Device {
   double balance = 1.0;
 };
 
+// GGEMSProfilerManager (src/tools/GGEMSProfilerManager.cc:83-104): device time
+// per label (CUDA events of the launches), summed over runs.
+class Profiler {
+ public:
+  static Profiler& instance();
+  void add(const std::string& label, double ms);
+  void print_summary(std::ostream& out) const;
+  void reset();
+
+ private:
+  std::vector<std::pair<std::string, double>> labels_;
+  mutable std::mutex mutex_;
+};
+
 class Simulation {
  public:
   static Simulation& instance();
@@ -220,6 +235,7 @@ class GGEMS {
   bool verbose[10] = {false};
   bool is_tracking = false;
   int tracking_id = 0;
+  static constexpr int kTrackingCapacity = 4096;  // recorded points per run and device
   void initialize(uint32_t seed);
   // Host half of initialize(): sources, navigators, tables and the scene, no device.
   void prepare();

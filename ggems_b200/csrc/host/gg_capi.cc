@@ -652,7 +652,7 @@ GG_EXPORT void clean_ggems_attenuations(AttenuationsHandle*) {}
 
 // ---- GGEMSProfilerManager.hh / GGEMSRAMManager.hh ----
 GG_EXPORT void* get_instance_profiler_manager(void) { return &g_profiler_manager; }
-GG_EXPORT void print_summary_profiler_manager(void*) {}
+GG_EXPORT void print_summary_profiler_manager(void*) { Profiler::instance().print_summary(std::cout); }
 GG_EXPORT void* get_instance_ggems_ram_manager(void) { return &g_ram_manager; }
 GG_EXPORT void print_infos_ram_manager(void*) {}
 

@@ -377,6 +377,35 @@ GG_API int gg_compute_dose_no_alloc(gg_context* context, int32_t dose_map, int32
                                     int32_t is_water_reference, float minimum_density, float* dose,
                                     float* uncertainty);
 
+/* ---- particle tracking (GGEMS_TRACKING, e.g. TrackThroughGGEMSVoxelizedSolid.cl:184-210) ----
+ * The states of one random slot (GGEMS's particle_tracking_id: particle i of
+ * every batch) recorded by the transport kernel at each stage of its
+ * histories, up to a capacity; read back after a run.  slot < 0 turns it off. */
+typedef enum gg_track_kind {
+  GG_TRACK_PRIMARY = 0,   /* a new history: global position and direction */
+  GG_TRACK_ENTER = 1,     /* projected into a solid (solid-local frame, meshed solids global) */
+  GG_TRACK_STEP = 2,      /* a step inside a solid: process (GG_TRANSPORTATION when none) */
+  GG_TRACK_SCATTER = 3,   /* after a Compton / Rayleigh interaction */
+  GG_TRACK_LEAVE = 4,     /* left the solid (global frame) */
+  GG_TRACK_DEAD = 5       /* the history ended */
+} gg_track_kind;
+
+typedef struct gg_track_point {
+  int32_t kind;           /* gg_track_kind */
+  int32_t solid;          /* solid index, -1 outside */
+  int32_t process;        /* GG_COMPTON_SCATTERING ... GG_TRANSPORTATION, -1 */
+  int32_t history;        /* history of the slot within the run (0, 1, ...) */
+  float E;                /* MeV */
+  float position[3];      /* mm */
+  float direction[3];
+  float pad;
+} gg_track_point;
+
+GG_API int gg_set_tracking(gg_context* context, int32_t slot, int32_t capacity);
+/* Copies up to `capacity` points of the last run; *count = points recorded
+ * (may exceed what was stored: the buffer keeps the first ones). */
+GG_API int gg_read_tracking(gg_context* context, gg_track_point* points, int32_t capacity, int32_t* count);
+
 /* ---- timing of the last gg_run_source (device time, ms) and launch count ---- */
 GG_API int gg_last_run_stats(gg_context* context, float* milliseconds, int64_t* kernel_launches);
 

@@ -44,10 +44,10 @@ def test_struct_layouts_match_c():
 #include <stddef.h>
 #include "ggems_b200.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(gg_obb), sizeof(gg_physics_tables),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(gg_obb), sizeof(gg_physics_tables),
          sizeof(gg_solid), sizeof(gg_dose_map), sizeof(gg_scene), sizeof(gg_source), sizeof(gg_particle_buffers),
          sizeof(gg_tally_buffers), offsetof(gg_source, number_of_activity_bins), sizeof(gg_world), sizeof(gg_job),
-         sizeof(gg_shape), offsetof(gg_shape, size));
+         sizeof(gg_shape), offsetof(gg_shape, size), sizeof(gg_track_point));
   return 0;
 }
 '''
@@ -61,7 +61,7 @@ int main(void) {
     ours = [C.sizeof(abi.gg_obb), C.sizeof(abi.gg_physics_tables), C.sizeof(abi.gg_solid), C.sizeof(abi.gg_dose_map),
             C.sizeof(abi.gg_scene), C.sizeof(abi.gg_source), C.sizeof(abi.gg_particle_buffers),
             C.sizeof(abi.gg_tally_buffers), abi.gg_source.number_of_activity_bins.offset, C.sizeof(abi.gg_world),
-            C.sizeof(abi.gg_job), C.sizeof(abi.gg_shape), abi.gg_shape.size.offset]
+            C.sizeof(abi.gg_job), C.sizeof(abi.gg_shape), abi.gg_shape.size.offset, C.sizeof(abi.gg_track_point)]
     assert sizes == ours
 
 

@@ -332,3 +332,41 @@ def test_error_against_fp64_oracle(ctx):
               % (name, rel, (np.abs(z) < 3).mean()))
         assert rel < 5e-3
         assert (np.abs(z) < 3).mean() >= 0.997
+
+
+def test_particle_tracking(ctx):
+    """GGEMS_TRACKING: the tracked slot's trajectory starts with its primary,
+    enters solids before stepping in them, and ends dead at the slot's final
+    state; the histories are the same with tracking on (it only records)."""
+    sc = scenes.cbct_scene(n=32, voxel=8.0, elements=(64, 64, 1), element_size=(6.4, 6.4, 10.0))
+    src = scenes.XRaySource(spectrum=scenes.synthetic_spectrum(), aperture_deg=11.0)
+    n = 50000
+    P0, T0, s0 = parity.run_gpu(ctx, sc, src, n)
+    slot = int(np.nonzero(P0.scatter[:n] == 1)[0][0])  # a photon that scattered in the phantom
+    ctx.set_tracking(slot)
+    try:
+        P1, T1, s1 = parity.run_gpu(ctx, sc, src, n)
+        pts, count = ctx.read_tracking()
+    finally:
+        ctx.set_tracking(-1)
+    assert np.array_equal(s0, s1)
+    for f in ("E", "px", "py", "pz", "status"):
+        assert np.array_equal(getattr(P0, f), getattr(P1, f)), f
+    assert count == len(pts) and count >= 4
+    assert pts[0].kind == abi.GG_TRACK_PRIMARY and pts[-1].kind == abi.GG_TRACK_DEAD
+    kinds = [p.kind for p in pts]
+    assert abi.GG_TRACK_ENTER in kinds and abi.GG_TRACK_SCATTER in kinds
+    assert all(p.history == 0 for p in pts)  # one history per slot at n < 2^20
+    inside = None
+    for p in pts[1:]:
+        if p.kind == abi.GG_TRACK_ENTER:
+            inside = p.solid
+        elif p.kind in (abi.GG_TRACK_STEP, abi.GG_TRACK_SCATTER):
+            assert p.solid == inside
+        elif p.kind == abi.GG_TRACK_LEAVE:
+            inside = None
+    last = pts[-1]
+    assert last.E == P1.E[slot]
+    assert [last.position[i] for i in range(3)] == [P1.px[slot], P1.py[slot], P1.pz[slot]]
+    _, count_off = ctx.read_tracking()
+    assert count_off == 0
