@@ -14,6 +14,8 @@ tallies statistically identical (|z| < 3 in >= 99.7 % of bins, totals within
 import numpy as np
 import pytest
 
+from ggems_b200 import abi
+
 import parity
 import scenes
 
