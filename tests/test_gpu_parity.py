@@ -35,10 +35,10 @@ def _report(name, exact, close):
 
 
 def test_water_box_histories_and_dose(ctx):
-    """C1 geometry: 64^3 water at 2 mm, 60 keV cone from 1 m, dose map."""
+    """C1 at its full size: 64^3 water at 2 mm, 60 keV cone from 1 m, dose map, 1e6 primaries."""
     sc = scenes.water_box_scene(photon_tracking=True)
     src = scenes.XRaySource(monoenergy=scenes.F(60.0) * scenes.KEV, aperture_deg=10.0)
-    n = 200000
+    n = 1_000_000
     Pg, Tg, sg = parity.run_gpu(ctx, sc, src, n)
     Po, To, so = parity.run_oracle(sc, src, n)
     exact, close = parity.history_agreement(Pg, Po)
@@ -93,6 +93,40 @@ def test_cbct_histories_and_projection(ctx):
         assert abs(int(hg.sum()) - int(ho.sum())) <= 0.005 * max(ho.sum(), 1)
         z = parity.z_scores(hg.astype(float), ho.astype(float), hg.astype(float), ho.astype(float))
         assert (np.abs(z) < 3).mean() >= 0.997
+
+
+def test_cbct_full_size_properties(ctx):
+    """C2 at its full size (256^3 phantom, 512^2 panel, 1e8 primaries in 96 batches),
+    through properties that do not need the oracle to run 1e8 histories: two runs
+    from the same random states give identical histograms and identical final
+    streams (integer tallies are order-independent); every scatter count is also a
+    total count; and the detected and scattered fractions per primary, and the
+    projection's shape on a 16x16 grid of blocks, agree with the oracle's first batch
+    (the same 1,041,667 slots from the same states) within binomial noise."""
+    sc = scenes.cbct_scene()
+    src = scenes.XRaySource(spectrum=scenes.synthetic_spectrum(), aperture_deg=11.0)
+    n = 100_000_000
+    _, T1, s1 = parity.run_gpu(ctx, sc, src, n)
+    _, T2, s2 = parity.run_gpu(ctx, sc, src, n)
+    total, scat = T1.histograms[0].astype(np.int64), T1.histograms[1].astype(np.int64)
+    assert np.array_equal(total, T2.histograms[0]) and np.array_equal(scat, T2.histograms[1])
+    assert np.array_equal(s1, s2)
+    assert (scat <= total).all() and total.sum() <= n
+    n_ref = 1_041_667  # GGEMSSource::OrganizeParticlesInBatch: the first of 96 batches
+    _, To, _ = parity.run_oracle(sc, src, n_ref)
+    t_ref, s_ref = To.histograms[0].astype(np.int64), To.histograms[1].astype(np.int64)
+    for g, r in ((total.sum(), t_ref.sum()), (scat.sum(), s_ref.sum())):
+        p = r / n_ref
+        sigma = np.sqrt(p * (1 - p) / n_ref + p * (1 - p) / n)
+        print("fraction per primary: %.5f (GPU, 1e8) vs %.5f (oracle, 1 batch), z = %.2f" % (g / n, p, (g / n - p) / sigma))
+        assert abs(g / n - p) < 4 * sigma
+    side = total.reshape(512, 512)
+    blocks_g = side.reshape(16, 32, 16, 32).sum((1, 3)).astype(float)
+    blocks_r = t_ref.reshape(512, 512).reshape(16, 32, 16, 32).sum((1, 3)).astype(float)
+    scale = n_ref / n
+    z = (blocks_r - blocks_g * scale) / np.sqrt(np.maximum(blocks_r + blocks_g * scale * scale, 1.0))
+    print("blocks with |z| < 4: %.4f, max |z| %.2f" % ((np.abs(z) < 4).mean(), np.abs(z).max()))
+    assert (np.abs(z) < 4).mean() >= 0.99
 
 
 def test_multi_batch_random_slot_reuse(ctx):
