@@ -14,9 +14,9 @@
 // the 5th-generation tensor cores (tcgen05.mma with TMEM accumulators, TMA
 // operand staging; gg_unet_umma.cu): rows = pixels, columns = output
 // channels, reduction = 9 x input channels.  Weight gradients are the
-// transposed GEMM (rows = output channels, columns = input channels,
-// reduction = pixels), split over blocks with FP32 atomics on mma.sync
-// m16n8k16 (BF16 inputs, FP32 accumulation).
+// transposed GEMM on the same tensor cores (rows = (tap, output channel),
+// columns = input channels, reduction = pixels, both operands MN-major),
+// split over CTAs whose partial tiles are added to the FP32 gradient.
 //
 // Network (S = image side, all 3x3 convolutions followed by ReLU):
 //   enc  16->32->32 @S | pool | 32->64->64 @S/2 | pool | 64->128->128 @S/4 | pool
@@ -60,76 +60,6 @@ int unet_fail(int code, const std::string& m) {
   } while (0)
 
 using bf16 = __nv_bfloat16;
-
-// ---------------------------------------------------------------- GEMM core --
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-constexpr int kPad = 8;      // smem row padding (bf16 elements)
-
-struct ConvShape {
-  int batch, height, width, cin, cout;
-};
-
-// Weight gradient dW[tap][co][ci] += sum_p dy[p][co] * x[p shifted by tap][ci]
-// (32 output x 16 input channels per block, one tap, a range of pixels).
-constexpr int kWgradPixels = 1024;
-__global__ void __launch_bounds__(128) conv3x3_wgrad_kernel(const bf16* __restrict__ x, const bf16* __restrict__ dy,
-                                                            float* __restrict__ dw, ConvShape s) {
-  __shared__ __align__(16) bf16 As[32][16 + kPad];  // [co][pixel]
-  __shared__ __align__(16) bf16 Bs[16][16 + kPad];  // [ci][pixel]
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int g = lane >> 2, t = lane & 3;
-  const int co0 = blockIdx.x * 32, ci0 = blockIdx.y * 16;
-  const int tap = blockIdx.z % 9, split = blockIdx.z / 9;
-  const int ky = tap / 3, kx = tap - 3 * ky;
-  const int hw = s.height * s.width, total = s.batch * hw;
-  const int pbeg = split * kWgradPixels, pend = min(total, pbeg + kWgradPixels);
-  const int mt = warp >> 1, nt = warp & 1;  // warp's m16 / n8 tile
-  float acc[4] = {0, 0, 0, 0};
-  for (int q0 = pbeg; q0 < pend; q0 += 16) {
-    // A: 16 pixels x 32 co, 4 elements per thread
-    for (int e = tid; e < 512; e += 128) {
-      const int pl = e >> 5, co = e & 31, p = q0 + pl;
-      As[co][pl] = p < pend ? dy[static_cast<size_t>(p) * s.cout + co0 + co] : __float2bfloat16(0.0f);
-    }
-    // B: 16 pixels x 16 ci of the shifted input
-    for (int e = tid; e < 256; e += 128) {
-      const int pl = e >> 4, ci = e & 15, p = q0 + pl;
-      bf16 v = __float2bfloat16(0.0f);
-      if (p < pend) {
-        const int b = p / hw, rem = p - b * hw, py = rem / s.width, px = rem - py * s.width;
-        const int yy = py + ky - 1, xx = px + kx - 1;
-        if (yy >= 0 && yy < s.height && xx >= 0 && xx < s.width)
-          v = x[(static_cast<size_t>(b) * hw + yy * s.width + xx) * s.cin + ci0 + ci];
-      }
-      Bs[ci][pl] = v;
-    }
-    __syncthreads();
-    uint32_t a[4], bb[2];
-    const int r = mt * 16 + g;
-    a[0] = *reinterpret_cast<const uint32_t*>(&As[r][2 * t]);
-    a[1] = *reinterpret_cast<const uint32_t*>(&As[r + 8][2 * t]);
-    a[2] = *reinterpret_cast<const uint32_t*>(&As[r][2 * t + 8]);
-    a[3] = *reinterpret_cast<const uint32_t*>(&As[r + 8][2 * t + 8]);
-    bb[0] = *reinterpret_cast<const uint32_t*>(&Bs[8 * nt + g][2 * t]);
-    bb[1] = *reinterpret_cast<const uint32_t*>(&Bs[8 * nt + g][2 * t + 8]);
-    mma_bf16(acc, a, bb);
-    __syncthreads();
-  }
-  float* out = dw + static_cast<size_t>(tap) * s.cout * s.cin;
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int co = co0 + mt * 16 + g + 8 * h, ci = ci0 + 8 * nt + 2 * t;
-    atomicAdd(out + static_cast<size_t>(co) * s.cin + ci, acc[2 * h]);
-    atomicAdd(out + static_cast<size_t>(co) * s.cin + ci + 1, acc[2 * h + 1]);
-  }
-}
 
 // ------------------------------------------------------------ elementwise --
 __host__ __device__ constexpr int context_radius(int k) { return k == 0 ? 4 : (k == 1 ? 16 : 64); }
@@ -403,6 +333,7 @@ struct gg_unet {
     bf16* dpre = nullptr;
     gg_umma::ConvPlan fwd{};  // y = relu(conv(input, w) + b)
     gg_umma::ConvPlan bwd{};  // data gradient: conv(dpre, wt), layers 1..13
+    gg_umma::WgradPlan wgrad{};  // weight gradient from (input, dpre)
   };
   std::vector<Layer> layers;  // 14 convolutions
   size_t out_w_off = 0, out_b_off = 0, n_params = 0;
@@ -509,10 +440,7 @@ int backward(gg_unet* n, const float* target) {
     const size_t na = static_cast<size_t>(px) * l.cout;
     relu_backward_kernel<<<grid_for(na), 256, 0, n->stream>>>(l.dact, l.act, l.dpre, na);
     bias_grad_kernel<<<dim3(std::min(px, 1024), (l.cout + 127) / 128), 128, 0, n->stream>>>(l.dpre, n->grads + l.b_off, px, l.cout);
-    ConvShape s{B, l.side, l.side, l.cin, l.cout};
-    dim3 wg(l.cout / 32, l.cin / 16, 9 * ((px + kWgradPixels - 1) / kWgradPixels));
-    conv3x3_wgrad_kernel<<<wg, 128, 0, n->stream>>>(layer_input(n, i), l.dpre, n->grads + l.w_off, s);
-    UNET_CUDA(cudaGetLastError());
+    UNET_CUDA(gg_umma::launch_wgrad(l.wgrad, n->grads + l.w_off, n->conv_error, n->stream));
     if (i == 0) break;
     // data gradient of the layer input (FP32)
     float* dx = (i == 8) ? n->dcat8 : (i == 10) ? n->dcat10 : (i == 12) ? n->dcat12
@@ -621,6 +549,7 @@ GG_API int gg_unet_create(int32_t batch, int32_t size, uint64_t seed, gg_unet** 
     auto& l = n->layers[i];
     const char* why = gg_umma::make_plan(&l.fwd, layer_input(n, i), l.w, batch, l.side, l.side, l.cin, l.cout);
     if (!why && i > 0) why = gg_umma::make_plan(&l.bwd, l.dpre, l.wt, batch, l.side, l.side, l.cout, l.cin);
+    if (!why) why = gg_umma::make_wgrad_plan(&l.wgrad, layer_input(n, i), l.dpre, batch, l.side, l.side, l.cin, l.cout);
     if (why) return drop(unet_fail(GG_ERROR_INVALID_ARGUMENT, std::string("convolution plan: ") + why));
   }
   if ((rc = refresh_weights(n))) return drop(rc);

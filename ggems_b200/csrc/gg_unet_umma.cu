@@ -250,6 +250,164 @@ __global__ void __launch_bounds__(kThreads, 1) conv_umma_kernel(const __grid_con
   if (threadIdx.x == 0 && cta_error) atomicExch(a.error, 1);
 }
 
+// 32 lanes x 16 columns of FP32 from TMEM into 16 registers per thread.
+__device__ __forceinline__ void tmem_load_16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+      "[%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// MN-major operand tile: 64 pixel rows (the reduction) of `atom` channels
+// (32/64/128-byte rows, swizzled over that length), 8-row groups 16 * atom
+// bytes apart, successive channel atoms `lbo` bytes apart.
+__device__ __forceinline__ uint64_t smem_desc_mn(uint32_t addr, int atom, uint32_t lbo) {
+  cute::UMMA::SmemDescriptor d;
+  d.desc_ = 0;
+  d.start_address_ = static_cast<uint16_t>(addr >> 4);
+  d.leading_byte_offset_ = static_cast<uint16_t>(lbo >> 4);
+  d.stride_byte_offset_ = static_cast<uint16_t>((8 * atom * 2) >> 4);
+  d.version_ = 1;
+  d.base_offset_ = 0;
+  d.lbo_mode_ = 0;
+  d.layout_type_ = static_cast<uint8_t>(atom == 64 ? cute::UMMA::LayoutType::SWIZZLE_128B
+                                        : atom == 32 ? cute::UMMA::LayoutType::SWIZZLE_64B
+                                                     : cute::UMMA::LayoutType::SWIZZLE_32B);
+  return d.desc_;
+}
+
+constexpr int kChunk = 64;               // pixels per reduction chunk
+constexpr int kWgradATileBytes = 128 * kChunk * 2;
+
+// Weight gradient: D[(tap, co)][ci] = sum over the CTA's pixels q of
+// dY[q - offset(tap)][co] * X[q][ci].  The dY boxes are loaded at the shifted
+// position (TMA zero-fills what falls outside the image, which is the
+// convolution's zero padding seen from the other side), the X boxes at q.
+__global__ void __launch_bounds__(kThreads, 1) wgrad_umma_kernel(const __grid_constant__ CUtensorMap tmdy,
+                                                              const __grid_constant__ CUtensorMap tmx, WgradArgs a) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem = smem_raw + ((1024 - (smem_addr(smem_raw) & 1023)) & 1023);
+  const int S = a.stages;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + static_cast<size_t>(S) * a.stage_bytes);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + S;
+  uint64_t* acc = bars + 2 * S;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc + 1);
+  __shared__ int cta_error;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tap0 = (blockIdx.x / a.co_blocks) * a.taps_per_tile;
+  const int co0 = (blockIdx.x % a.co_blocks) * a.co_tile;
+  const int n0 = blockIdx.y * a.n_tile;
+  const int c_begin = blockIdx.z * a.chunks_per_split;
+  const int c_end = min(a.chunks, c_begin + a.chunks_per_split);
+  const int iters = c_end - c_begin;
+  const int taps_here = min(a.taps_per_tile, 9 - tap0);
+  const int boxes_per_tap = a.co_tile / a.a_atom;
+  const int a_boxes = taps_here * boxes_per_tap;
+  const int b_boxes = a.n_tile / a.b_atom;
+  const uint32_t tx_bytes = static_cast<uint32_t>(a_boxes * a.a_bytes_per_box + a.b_bytes);
+  const int hw = a.height * a.width;
+
+  if (threadIdx.x == 0) {
+    cta_error = 0;
+    for (int i = 0; i < 2 * S + 1; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bars + i)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                 "r"(a.tmem_cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---- producer: per 64-pixel chunk, the shifted dY boxes of the tile's taps and the X boxes ----
+    int issued = 0;
+    for (int it = 0; it < iters; ++it) {
+      const int s = it % S;
+      if (it >= S && !wait_parity(smem_addr(empty + s), ((it / S) + 1) & 1, a.error)) {
+        atomicExch(&cta_error, 1);
+        break;
+      }
+      const int p0 = (c_begin + it) * kChunk;
+      const int b0 = p0 / hw, rem = p0 - b0 * hw, y0 = rem / a.width, x0 = rem - y0 * a.width;
+      unsigned char* st = smem + static_cast<size_t>(s) * a.stage_bytes;
+      const uint32_t bar = smem_addr(full + s);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(tx_bytes) : "memory");
+      for (int j = 0; j < a_boxes; ++j) {
+        const int t = j / boxes_per_tap, cb = j - t * boxes_per_tap;
+        const int tap = tap0 + t, ky = tap / 3, kx = tap - 3 * ky;
+        tma_load_4d(smem_addr(st + j * a.a_bytes_per_box), &tmdy, co0 + cb * a.a_atom, x0 - (kx - 1), y0 - (ky - 1),
+                    b0, bar);
+      }
+      for (int j = 0; j < b_boxes; ++j)
+        tma_load_4d(smem_addr(st + kWgradATileBytes + j * a.b_atom * kChunk * 2), &tmx, n0 + j * a.b_atom, x0, y0, b0,
+                    bar);
+      ++issued;
+    }
+    for (int it = issued > S ? issued - S : 0; it < issued; ++it)
+      if (!wait_parity(smem_addr(full + it % S), (it / S) & 1, a.error)) atomicExch(&cta_error, 1);
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer: 4 x K=16 per chunk; K advances by two 8-row groups ----
+    bool ok = true;
+    const uint32_t a_step = (2 * 8 * a.a_atom * 2) >> 4, b_step = (2 * 8 * a.b_atom * 2) >> 4;
+    for (int it = 0; it < iters && ok; ++it) {
+      const int s = it % S;
+      if (!wait_parity(smem_addr(full + s), (it / S) & 1, a.error)) {
+        atomicExch(&cta_error, 1);
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      unsigned char* st = smem + static_cast<size_t>(s) * a.stage_bytes;
+      const uint64_t ad = smem_desc_mn(smem_addr(st), a.a_atom, static_cast<uint32_t>(a.a_bytes_per_box));
+      const uint64_t bd =
+          smem_desc_mn(smem_addr(st + kWgradATileBytes), a.b_atom, static_cast<uint32_t>(a.b_atom * kChunk * 2));
+      for (int k = 0; k < kChunk / 16; ++k)
+        umma_f16(tmem, ad + k * a_step, bd + k * b_step, a.idesc, (it > 0 || k > 0) ? 1u : 0u);
+      umma_commit(smem_addr(empty + s));
+    }
+    if (ok) umma_commit(smem_addr(acc));
+  }
+  __syncwarp();
+
+  // ---- epilogue: TMEM lane = (tap, co) row, columns = input channels; add to dW ----
+  const bool ready = wait_parity(smem_addr(acc), 0, a.error);
+  if (!ready) atomicExch(&cta_error, 1);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (!cta_error && iters > 0) {
+    const int row = warp * 32 + lane;
+    const int t = row / a.co_tile;
+    const bool valid = t < taps_here;
+    const int tap = tap0 + t, co = co0 + row - t * a.co_tile;
+    float* out = a.dw + (static_cast<size_t>(valid ? tap : 0) * a.cout + co) * a.cin + n0;
+    for (int cb = 0; cb < a.n_tile / 16; ++cb) {
+      float v[16];
+      tmem_load_16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + cb * 16, v);
+      if (!valid) continue;
+      float4* dst = reinterpret_cast<float4*>(out + cb * 16);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) atomicAdd(dst + j, make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]));
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.tmem_cols));
+  if (threadIdx.x == 0 && cta_error) atomicExch(a.error, 1);
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -377,6 +535,98 @@ cudaError_t launch(const ConvPlan& p, int mode, const float* bias, void* y, int*
     cudaFuncSetAttribute(conv_umma_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(p.smem));
     conv_umma_kernel<1><<<grid, kThreads, p.smem, stream>>>(p.tmap_x, p.tmap_w, a);
   }
+  return cudaGetLastError();
+}
+
+const char* make_wgrad_plan(WgradPlan* p, const void* x, const void* dy, int batch, int height, int width, int cin,
+                            int cout) {
+  std::memset(p, 0, sizeof(*p));
+  if (!is_pow2(width) || !is_pow2(height) || batch < 1 || width * height < kChunk)
+    return "image sides must be powers of two with at least 64 pixels per image";
+  if (cin % 16 != 0) return "input channels must be a multiple of 16";
+  if (!(cout == 32 || cout == 64 || cout % 128 == 0)) return "output channels must be 32, 64 or a multiple of 128";
+  auto fn = encode_fn();
+  if (!fn) return "cuTensorMapEncodeTiled is not available";
+  WgradArgs& a = p->args;
+  a.height = height;
+  a.width = width;
+  a.cin = cin;
+  a.cout = cout;
+  a.co_tile = cout < 128 ? cout : 128;
+  a.taps_per_tile = 128 / a.co_tile;
+  a.co_blocks = cout / a.co_tile;
+  a.a_atom = a.co_tile < 64 ? a.co_tile : 64;
+  a.n_tile = cin <= 256 ? cin : (cin % 128 == 0 ? 128 : (cin % 64 == 0 ? 64 : 0));
+  if (a.n_tile == 0) return "unsupported input channel count";
+  a.b_atom = a.n_tile % 64 == 0 ? 64 : (a.n_tile % 32 == 0 ? 32 : 16);
+  a.tmem_cols = pow2_at_least(a.n_tile, 32);
+  a.a_bytes_per_box = a.a_atom * kChunk * 2;
+  a.b_bytes = a.n_tile * kChunk * 2;
+  a.stage_bytes = kWgradATileBytes + ((a.b_bytes + 1023) / 1024) * 1024;
+  a.stages = 96 * 1024 / a.stage_bytes;
+  if (a.stages > 6) a.stages = 6;
+  if (a.stages < 2) a.stages = 2;
+  p->smem = static_cast<size_t>(a.stages) * a.stage_bytes + (2 * a.stages + 1) * 8 + 16 + 1024;
+  const size_t tmem_cap_smem = 228 * 1024 / (512 / a.tmem_cols + 1) + 1;
+  if (p->smem < tmem_cap_smem) p->smem = tmem_cap_smem;
+  if (p->smem > 227 * 1024) return "operand tiles do not fit in shared memory";
+  cute::UMMA::InstrDescriptor id;
+  id.desc_ = 0;
+  id.c_format_ = 1;  // F32
+  id.a_format_ = 1;  // BF16
+  id.b_format_ = 1;  // BF16
+  id.a_major_ = 1;   // MN-major: channels contiguous, pixels (the reduction) strided
+  id.b_major_ = 1;
+  id.n_dim_ = static_cast<uint16_t>(a.n_tile >> 3);
+  id.m_dim_ = static_cast<uint16_t>(128 >> 4);
+  a.idesc = id.desc_;
+  // 64-pixel boxes: a run of one row, or whole rows
+  const int bw = width < kChunk ? width : kChunk;
+  const int bh = (kChunk / bw) < height ? kChunk / bw : height;
+  const int bb = kChunk / (bw * bh);
+  cuuint32_t ones[4] = {1, 1, 1, 1};
+  cuuint64_t dd[4] = {static_cast<cuuint64_t>(cout), static_cast<cuuint64_t>(width), static_cast<cuuint64_t>(height),
+                      static_cast<cuuint64_t>(batch)};
+  cuuint64_t ds[3] = {static_cast<cuuint64_t>(cout) * 2, static_cast<cuuint64_t>(width) * cout * 2,
+                      static_cast<cuuint64_t>(height) * width * cout * 2};
+  cuuint32_t dbox[4] = {static_cast<cuuint32_t>(a.a_atom), static_cast<cuuint32_t>(bw), static_cast<cuuint32_t>(bh),
+                        static_cast<cuuint32_t>(bb)};
+  if (fn(&p->tmap_dy, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(dy), dd, ds, dbox, ones,
+         CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_for(a.a_atom * 2), CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return "gradient tensor map rejected";
+  cuuint64_t xd[4] = {static_cast<cuuint64_t>(cin), static_cast<cuuint64_t>(width), static_cast<cuuint64_t>(height),
+                      static_cast<cuuint64_t>(batch)};
+  cuuint64_t xs[3] = {static_cast<cuuint64_t>(cin) * 2, static_cast<cuuint64_t>(width) * cin * 2,
+                      static_cast<cuuint64_t>(height) * width * cin * 2};
+  cuuint32_t xbox[4] = {static_cast<cuuint32_t>(a.b_atom), static_cast<cuuint32_t>(bw), static_cast<cuuint32_t>(bh),
+                        static_cast<cuuint32_t>(bb)};
+  if (fn(&p->tmap_x, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(x), xd, xs, xbox, ones,
+         CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_for(a.b_atom * 2), CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return "activation tensor map rejected";
+  a.chunks = static_cast<int>(static_cast<long long>(batch) * height * width / kChunk);
+  p->grid_m = ((9 + a.taps_per_tile - 1) / a.taps_per_tile) * a.co_blocks;
+  p->grid_n = cin / a.n_tile;
+  // split the pixels so that about two CTAs per SM exist; partial tiles are added to dW
+  int sms = 148, dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int tiles = p->grid_m * p->grid_n;
+  int splits = (2 * sms + tiles - 1) / tiles;
+  if (splits > a.chunks) splits = a.chunks;
+  if (splits < 1) splits = 1;
+  a.chunks_per_split = (a.chunks + splits - 1) / splits;
+  p->splits = (a.chunks + a.chunks_per_split - 1) / a.chunks_per_split;
+  return nullptr;
+}
+
+cudaError_t launch_wgrad(const WgradPlan& p, float* dw, int* error, cudaStream_t stream) {
+  if (reinterpret_cast<uintptr_t>(dw) & 15) return cudaErrorMisalignedAddress;
+  WgradArgs a = p.args;
+  a.dw = dw;
+  a.error = error;
+  cudaFuncSetAttribute(wgrad_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(p.smem));
+  wgrad_umma_kernel<<<dim3(p.grid_m, p.grid_n, p.splits), kThreads, p.smem, stream>>>(p.tmap_dy, p.tmap_x, a);
   return cudaGetLastError();
 }
 

@@ -464,8 +464,20 @@ def time_network(side=256, batch=8, repeats=20):
     stop.record()
     torch.cuda.synchronize()
     ms = start.elapsed_time(stop) / repeats
+    # one training step: forward, backward (data and weight gradients: twice the
+    # forward's FLOP) and the Adam update
+    t = torch.rand((batch, side, side), device="cuda")
+    for _ in range(3):
+        net.train_step(x, t, 1e-4)
+    torch.cuda.synchronize()
+    start.record()
+    for _ in range(repeats):
+        net.train_step(x, t, 1e-4)
+    stop.record()
+    torch.cuda.synchronize()
+    train_ms = start.elapsed_time(stop) / repeats
     net.close()
-    return ms, forward_flops(side, batch) / (ms * 1e-3) / 1e12
+    return ms, forward_flops(side, batch) / (ms * 1e-3) / 1e12, train_ms
 
 
 def save_network(net, path):
@@ -519,10 +531,10 @@ def main(argv=None):
     ap.add_argument("--chunk", type=int, default=64, help="projections per batched MC launch")
     ap.add_argument("--save", help="write the trained network (.npz)")
     ap.add_argument("--load", help="skip data generation and training: load a trained network (.npz)")
-    ap.add_argument("--network-only", action="store_true", help="time the network's forward pass only")
+    ap.add_argument("--network-only", action="store_true", help="time the network's forward pass and training step only")
     args = ap.parse_args(argv)
     if args.network_only:
-        ms, tflops = time_network(args.side, args.batch)
+        ms, tflops, train_ms = time_network(args.side, args.batch)
         peaks = None
         try:
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -533,6 +545,8 @@ def main(argv=None):
                           "ms_per_forward": ms, "ms_per_projection": ms / args.batch,
                           "gflop_per_forward": forward_flops(args.side, args.batch) / 1e9,
                           "tflops": tflops, "peak_tflops": peak, "frac": tflops / peak,
+                          "ms_per_train_step": train_ms,
+                          "train_tflops": 3 * forward_flops(args.side, args.batch) / (train_ms * 1e-3) / 1e12,
                           "peak_source": "measured" if peaks else "fallback"}), flush=True)
         return 0
     import torch  # (CUDA memory for the network's device arrays)
