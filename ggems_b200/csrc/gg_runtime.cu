@@ -784,6 +784,7 @@ struct JobLaunch {
   int grid = 0;
   size_t smem = 0;
   bool mesh = false;
+  bool dose = false;  // some solid tallies into a dose map
   bool empty = true;
 };
 
@@ -828,6 +829,9 @@ int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*
     }
   }
   if (dj.empty()) return GG_OK;
+  bool dose = false;
+  for (int s = 0; s < c->number_of_solids; ++s) dose |= c->solid_dev_host[s].dose_map >= 0;
+  for (const gg::DevSolid& d : job_solids) dose |= d.dose_map >= 0;
   gg::TransportParams& P = out->params;
   P = gg::TransportParams{};
   gg::DevJob* djd;
@@ -875,7 +879,7 @@ int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*
   out->smem = (c->tables_in_smem ? c->table_bytes : 0) + sizeof(gg::DevSolid) * c->number_of_solids +
               sizeof(gg::DevNavigator) * c->number_of_navigators + 16;
   int blocks_per_sm = 0;
-  GG_CUDA(gg::configure_transport(out->smem, &blocks_per_sm, mesh, P.number_of_jobs > 1));
+  GG_CUDA(gg::configure_transport(out->smem, &blocks_per_sm, mesh, P.number_of_jobs > 1, dose));
   if (blocks_per_sm < 1) return fail(GG_ERROR_CUDA, "transport kernel does not fit on an SM");
   if (c->blocks_per_sm > 0 && c->blocks_per_sm < blocks_per_sm) blocks_per_sm = c->blocks_per_sm;
   uint64_t grid = static_cast<uint64_t>(blocks_per_sm) * c->sm_count;
@@ -883,6 +887,7 @@ int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*
   if (grid > needed) grid = needed;
   out->grid = static_cast<int>(grid);
   out->mesh = mesh;
+  out->dose = dose;
   out->empty = false;
   return GG_OK;
 }
@@ -892,7 +897,7 @@ int enqueue_jobs(gg_context* c, const JobLaunch& L) {
   GG_CUDA(cudaMemsetAsync(c->slot_counter, 0, sizeof(unsigned int), c->stream));
   if (L.params.tracking_count) GG_CUDA(cudaMemsetAsync(L.params.tracking_count, 0, sizeof(int32_t), c->stream));
   GG_CUDA(cudaMemsetAsync(c->error, 0, sizeof(int), c->stream));
-  gg::launch_transport(L.params, L.grid, L.smem, c->stream, L.mesh);
+  gg::launch_transport(L.params, L.grid, L.smem, c->stream, L.mesh, L.dose);
   GG_CUDA(cudaGetLastError());
   return GG_OK;
 }

@@ -766,7 +766,7 @@ extern __shared__ __align__(16) unsigned char g_smem[];
 // with neither run the variant compiled without the mesh phase and the world
 // walk, so their code and registers stay out of the voxel / detector hot loop.
 // kBatch: several jobs (source runs) in one launch, each with its own solids.
-template <bool kFull, bool kBatch>
+template <bool kFull, bool kBatch, bool kDose>
 __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) transport_kernel(TransportParams P) {
   // shared memory: [tables][solids][navigators][mbarrier]
   unsigned char* tables = g_smem;
@@ -929,9 +929,9 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
           // voxelized and meshed solids flag scattering; boxes do not
           // (TrackThroughGGEMSVoxelizedSolid.cl:253, TrackThroughGGEMSMeshSolid.cl:484)
           ph.scatter = 1;
-          if (so.dose_map >= 0 && !so.dose_tle) dose_record(P.dose_maps[so.dose_map], e0 - ph.E, ph.p);
+          if ((kDose && so.dose_map >= 0) && !so.dose_tle) dose_record(P.dose_maps[so.dose_map], e0 - ph.E, ph.p);
           if (ph.E <= tab.photon_cut(nav)[material]) {
-            if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
+            if ((kDose && so.dose_map >= 0)) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
             ph.status = GG_DEAD;
           }
         } else if (proc == GG_COMPTON_SCATTERING) {
@@ -1058,7 +1058,7 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
       if (dtb <= nid) {
         nid = dtb + kTolerance;
         proc = GG_TRANSPORTATION;
-        if (so.dose_map >= 0) {
+        if ((kDose && so.dose_map >= 0)) {
           const DevDoseMap& dm = P.dose_maps[so.dose_map];
           if (dm.photon_tracking) {
             int id = dosel(dm, ph.p);
@@ -1073,7 +1073,7 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
         leave_solid(so, false);
         continue;
       }
-      if (so.dose_tle) {
+      if (kDose && so.dose_tle) {
         // The step's deposit depends only on the energy before the interaction,
         // so it is recorded here even when the interaction itself is deferred.
         dose_record(P.dose_maps[so.dose_map], tle_edep(tab.attenuation(nav), material, ph.E, nid), ph.p);
@@ -1085,12 +1085,12 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
         continue;
       }
       if (proc == GG_PHOTOELECTRIC_EFFECT) {
-        if (so.dose_map >= 0 && !so.dose_tle) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
+        if ((kDose && so.dose_map >= 0) && !so.dose_tle) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
         ph.status = GG_DEAD;
         ph.E = 0.0f;
       }
       if (ph.E <= tab.photon_cut(nav)[material]) {
-        if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
+        if ((kDose && so.dose_map >= 0)) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
         ph.status = GG_DEAD;
       }
       if (ph.status == GG_DEAD) leave_solid(so, true);
@@ -1118,7 +1118,7 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
       if (to_next <= nid) {
         nid = to_next + kTolerance;
         proc = GG_TRANSPORTATION;
-        if (so.dose_map >= 0) {
+        if ((kDose && so.dose_map >= 0)) {
           const DevDoseMap& dm = P.dose_maps[so.dose_map];
           if (dm.photon_tracking) {
             int id = dosel(dm, ph.p);
@@ -1134,12 +1134,12 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
         continue;
       }
       if (proc == GG_PHOTOELECTRIC_EFFECT) {
-        if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
+        if ((kDose && so.dose_map >= 0)) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
         ph.status = GG_DEAD;
         ph.E = 0.0f;
       }
       if (ph.E <= tab.photon_cut(nav)[0]) {
-        if (so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
+        if ((kDose && so.dose_map >= 0)) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
         ph.status = GG_DEAD;
       }
       if (ph.status == GG_DEAD) leave_solid(so, true);
@@ -1224,15 +1224,18 @@ __global__ void compute_dose_kernel(DoseParams P) {
 
 namespace {
 using TransportKernel = void (*)(TransportParams);
-TransportKernel transport_variant(bool mesh, bool batch) {
-  if (mesh) return batch ? transport_kernel<true, true> : transport_kernel<true, false>;
-  return batch ? transport_kernel<false, true> : transport_kernel<false, false>;
+// kFull: meshes, world grid or particle tracking (dose code always in);
+// otherwise the dose-map code is compiled in only for scenes that tally dose.
+TransportKernel transport_variant(bool mesh, bool batch, bool dose) {
+  if (mesh) return batch ? transport_kernel<true, true, true> : transport_kernel<true, false, true>;
+  if (dose) return batch ? transport_kernel<false, true, true> : transport_kernel<false, false, true>;
+  return batch ? transport_kernel<false, true, false> : transport_kernel<false, false, false>;
 }
 }  // namespace
 
-void launch_transport(const TransportParams& p, int grid, size_t smem, void* stream, bool mesh) {
+void launch_transport(const TransportParams& p, int grid, size_t smem, void* stream, bool mesh, bool dose) {
   const bool batch = p.number_of_jobs > 1;
-  transport_variant(mesh, batch)<<<grid, kBlockThreads, smem, static_cast<cudaStream_t>(stream)>>>(p);
+  transport_variant(mesh, batch, dose)<<<grid, kBlockThreads, smem, static_cast<cudaStream_t>(stream)>>>(p);
 }
 
 namespace {
@@ -1326,8 +1329,8 @@ void launch_compute_dose(const DoseParams& p, void* stream) {
   compute_dose_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(p);
 }
 
-cudaError_t configure_transport(size_t smem, int* blocks_per_sm, bool mesh, bool batch) {
-  auto kernel = transport_variant(mesh, batch);
+cudaError_t configure_transport(size_t smem, int* blocks_per_sm, bool mesh, bool batch, bool dose) {
+  auto kernel = transport_variant(mesh, batch, dose);
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, kBlockThreads, smem);

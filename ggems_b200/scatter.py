@@ -374,15 +374,49 @@ def make_inputs(geometry, projections):
     return geometry.network_inputs(projections)
 
 
-def judge(predicted, low_count_mc, tolerance=JUDGE_TOLERANCE):
-    """Per projection: the network's output when its integrated scatter is
-    within `tolerance` of the plain-MC estimate's, else the MC estimate."""
-    out, used = [], []
+# Verdicts of the judge, per projection.
+JUDGE_MC, JUDGE_RESCALED, JUDGE_NETWORK = 0, 1, 2
+
+
+def judge(predicted, low_count_mc, tolerance=JUDGE_TOLERANCE, primaries=None, side=None, shape_blocks=4,
+          shape_p=1e-3):
+    """Per projection, against the low-count plain-MC estimate:
+
+    * JUDGE_NETWORK: the network's integrated scatter is within `tolerance` of
+      the MC's, and its output is kept;
+    * otherwise, when `primaries` is given, the network's shape is tested
+      against the MC's on a shape_blocks x shape_blocks grid: a chi-square of
+      the MC's counts per block against the network rescaled to the MC's
+      integral (Poisson variances, shape_blocks^2 - 1 degrees of freedom).
+      JUDGE_RESCALED: the shape passes (p >= shape_p) and the network rescaled
+      to the MC's integral is the output -- the magnitude from the MC (its
+      integral carries ~1/sqrt(counts) noise, about 2 % at 1e6 primaries), the
+      shape from the network;
+    * JUDGE_MC: the MC estimate replaces the network.
+
+    Returns (outputs, verdicts)."""
+    from scipy.stats import chi2
+    out, verdict = [], []
+    limit = chi2.isf(shape_p, shape_blocks * shape_blocks - 1)
     for p, m in zip(predicted, low_count_mc):
-        ok = abs(float(p.sum()) - float(m.sum())) <= tolerance * max(float(m.sum()), 1e-12)
-        out.append(p if ok else m)
-        used.append(bool(ok))
-    return np.stack(out), np.array(used)
+        sp, sm = float(p.sum()), float(m.sum())
+        if abs(sp - sm) <= tolerance * max(sm, 1e-12):
+            out.append(p)
+            verdict.append(JUDGE_NETWORK)
+            continue
+        if primaries is not None and sp > 0.0 and sm > 0.0:
+            n = side if side is not None else p.shape[-1]
+            to_counts = float(primaries) / float(n * n)  # inverse of normalise()
+            counts = block_mean(m, shape_blocks) * (n // shape_blocks) ** 2 * to_counts
+            expected = block_mean(p, shape_blocks) * (n // shape_blocks) ** 2 * to_counts * (sm / sp)
+            stat = float((((counts - expected) ** 2) / np.maximum(expected, 1.0)).sum())
+            if stat <= limit:
+                out.append(p * (sm / sp))
+                verdict.append(JUDGE_RESCALED)
+                continue
+        out.append(m)
+        verdict.append(JUDGE_MC)
+    return np.stack(out), np.array(verdict)
 
 
 def relative_error(a, ref, blocks=16):
@@ -509,7 +543,7 @@ def surrogate_pipeline(geo, net, projections, judge_primaries, seed):
     _, low = geo.finish_simulation(run)
     low = normalise(low, judge_primaries, geo.side)
     t.append(time.perf_counter())
-    final, used = judge(pred, low)
+    final, used = judge(pred, low, primaries=judge_primaries, side=geo.side)
     t.append(time.perf_counter())
     geo.last_breakdown = {"judge_mc_launch": t[1] - t[0], "inputs": t[2] - t[1], "network": t[3] - t[2],
                           "judge_mc_wait": t[4] - t[3], "judge": t[5] - t[4]}
@@ -531,6 +565,7 @@ def main(argv=None):
     ap.add_argument("--chunk", type=int, default=64, help="projections per batched MC launch")
     ap.add_argument("--save", help="write the trained network (.npz)")
     ap.add_argument("--load", help="skip data generation and training: load a trained network (.npz)")
+    ap.add_argument("--seed", type=int, default=11, help="seed of the phantoms, angles and MC streams")
     ap.add_argument("--network-only", action="store_true", help="time the network's forward pass and training step only")
     args = ap.parse_args(argv)
     if args.network_only:
@@ -552,7 +587,7 @@ def main(argv=None):
     import torch  # (CUDA memory for the network's device arrays)
     work = tempfile.mkdtemp(prefix="ggems_scatter_")
     geo = Geometry(args.side, work)
-    rng = np.random.default_rng(11)
+    rng = np.random.default_rng(args.seed)
     side = args.side
 
     def simulate_all(projs, primaries):
@@ -587,7 +622,7 @@ def main(argv=None):
     test_projs = [(float(rng.uniform(0, 360)), random_phantom(rng)) for _ in range(args.test)]
     _, s_ref, _ = simulate_all(test_projs, args.reference_primaries)
     ref = normalise(s_ref, args.reference_primaries, side)
-    final, pred, low, used, _ = surrogate_pipeline(geo, net, test_projs, args.judge_primaries, 1234)
+    final, pred, low, used, _ = surrogate_pipeline(geo, net, test_projs, args.judge_primaries, 1234 + args.seed)
     err_sur = [relative_error(f, r) for f, r in zip(final, ref)]
     err_net = [relative_error(p, r) for p, r in zip(pred, ref)]
     err_low = [relative_error(m, r) for m, r in zip(low, ref)]
@@ -595,7 +630,7 @@ def main(argv=None):
     phantom = random_phantom(rng)
     scan = [(360.0 * k / args.angles, phantom) for k in range(args.angles)]
     surrogate_pipeline(geo, net, scan[:8], args.judge_primaries, 99)  # warm-up
-    s_final, s_pred, s_low, s_used, t_scan = surrogate_pipeline(geo, net, scan, args.judge_primaries, 4321)
+    s_final, s_pred, s_low, s_used, t_scan = surrogate_pipeline(geo, net, scan, args.judge_primaries, 4321 + args.seed)
     breakdown = {k: v / args.angles * 1e3 for k, v in geo.last_breakdown.items()}
     picked = list(range(0, args.angles, args.reference_every))
     _, s_ref_scan, _ = simulate_all([scan[k] for k in picked], args.reference_primaries)
@@ -624,7 +659,8 @@ def main(argv=None):
         "metric": "scatter projections/s (surrogate + 1e6-primary MC judge vs plain MC at <=5% error)",
         "surrogate_projections_per_s": sur_per_s, "plain_mc_projections_per_s": plain_per_s,
         "speedup": sur_per_s / plain_per_s,
-        "scan": {"angles": args.angles, "seconds": t_scan, "judge_kept": float(s_used.mean()),
+        "scan": {"angles": args.angles, "seconds": t_scan, "judge_kept": float((s_used == JUDGE_NETWORK).mean()),
+                 "judge_rescaled": float((s_used == JUDGE_RESCALED).mean()),
                  "error_mean": float(np.mean(scan_err)), "error_max": float(np.max(scan_err)),
                  "low_count_mc_error": e_low, "reference_angles": len(picked),
                  "ms_per_projection": breakdown},
@@ -634,7 +670,8 @@ def main(argv=None):
                                      "projections": len(net_int)},
         "new_phantoms": {"projections": args.test, "network_error": float(np.mean(err_net)),
                          "judged_error": float(np.mean(err_sur)), "judged_error_max": float(np.max(err_sur)),
-                         "low_count_mc_error": float(np.mean(err_low)), "judge_kept": float(used.mean())},
+                         "low_count_mc_error": float(np.mean(err_low)), "judge_kept": float((used == JUDGE_NETWORK).mean()),
+                         "judge_rescaled": float((used == JUDGE_RESCALED).mean())},
         "plain_mc_primaries_for_5pct": n_plain, "plain_mc_error": float(np.mean(plain_err)),
         "mc_primaries_per_s": rate,
         "config": {"side": side, "pairs": args.pairs, "target_primaries": args.primaries, "epochs": args.epochs,

@@ -10,10 +10,23 @@ import scenes
 from ggems_b200 import abi
 
 
+def slots_used(n):
+    """Slots a run of n primaries fills (GGEMSSource::OrganizeParticlesInBatch:
+    ceil(n / 2^20) batches, the first n mod batches of them one particle larger).
+    Slots past these keep whatever an earlier run left there, on the device as in
+    the reference, so only these are compared."""
+    if n <= 0:
+        return 0
+    nb = -(-n // abi.GG_MAXIMUM_PARTICLES)
+    q, r = divmod(n, nb)
+    return q + (1 if r else 0)
+
+
 def run_oracle(sc, src, n, seed=777, states=None, threads=None, fp64=False):
     st = scenes.seed_states(seed) if states is None else states.copy()
     ss = sc.struct()
     P = abi.Particles(min(n, abi.GG_MAXIMUM_PARTICLES))
+    P.used = slots_used(n)
     T = sc.tallies()
     lib = scenes.oracle_fp64() if fp64 else scenes.oracle()
     rc = lib.gg_oracle_run(C.byref(ss), C.byref(src.struct), n, abi.ptr(st, C.c_uint32), C.byref(P.struct),
@@ -29,6 +42,7 @@ def run_gpu(ctx, sc, src, n, seed=777, states=None):
     ctx.set_random_states(st)
     ctx.run(src.struct, n)
     P = abi.Particles(min(n, abi.GG_MAXIMUM_PARTICLES))
+    P.used = slots_used(n)
     ctx.read_particles(P)
     T = sc.tallies()
     ctx.read_tallies(T)
@@ -37,7 +51,10 @@ def run_gpu(ctx, sc, src, n, seed=777, states=None):
 
 
 def history_agreement(Pa, Pb, pos_tol=1e-3, e_rel=1e-5):
-    """Fraction of slots whose final state agrees bit-exactly, and within tolerance."""
+    """Fraction of slots whose final state agrees bit-exactly, and within tolerance
+    (the slots both runs filled)."""
+    k = min(getattr(Pa, "used", Pa.n), getattr(Pb, "used", Pb.n))
+    Pa, Pb = _first(Pa, k), _first(Pb, k)
     ints = (Pa.status == Pb.status) & (Pa.solid_id == Pb.solid_id) & (Pa.scatter == Pb.scatter)
     exact = ints.copy()
     for f in ("E", "px", "py", "pz", "dx", "dy", "dz"):
@@ -47,6 +64,17 @@ def history_agreement(Pa, Pb, pos_tol=1e-3, e_rel=1e-5):
     close = ints & (np.abs(pa - pb).max(1) <= pos_tol) & \
         (np.abs(Pa.E.astype(np.float64) - Pb.E) <= e_rel * np.maximum(np.abs(Pb.E), 1e-6))
     return exact.mean(), close.mean()
+
+
+class _Slice:
+    def __init__(self, P, k):
+        self.n = k
+        for f in abi.Particles.FIELDS + ("status", "scatter", "solid_id"):
+            setattr(self, f, getattr(P, f)[:k])
+
+
+def _first(P, k):
+    return P if P.n == k else _Slice(P, k)
 
 
 def oracle_dose(sc, T, dose_map, solid, scale=1.0, water=False, min_density=0.0):

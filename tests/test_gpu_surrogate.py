@@ -165,12 +165,13 @@ def test_surrogate_beats_low_count_mc(geometry, torch):
     ref = S.normalise(s_ref, 400_000_000, side)
     low = S.normalise(s_low, 1_000_000, side)
     pred = S.predict(net, S.make_inputs(geometry, test))
-    final, used = S.judge(pred, low)
+    final, used = S.judge(pred, low, primaries=1_000_000, side=side)
     e_net = np.mean([S.relative_error(p, r) for p, r in zip(pred, ref)])
     e_low = np.mean([S.relative_error(m, r) for m, r in zip(low, ref)])
     e_fin = np.mean([S.relative_error(f, r) for f, r in zip(final, ref)])
-    print("surrogate: loss %.4f -> %.4f; error vs reference: network %.3f, low-count MC %.3f, judged %.3f (kept %d/8)"
-          % (losses[0], np.mean(losses[-10:]), e_net, e_low, e_fin, used.sum()))
+    print("surrogate: loss %.4f -> %.4f; error vs reference: network %.3f, low-count MC %.3f, judged %.3f "
+          "(kept %d/8, rescaled %d/8)" % (losses[0], np.mean(losses[-10:]), e_net, e_low, e_fin,
+                                          (used == S.JUDGE_NETWORK).sum(), (used == S.JUDGE_RESCALED).sum()))
     assert np.mean(losses[-10:]) < losses[0]
     assert e_net < 0.5 * e_low
     assert e_fin <= e_low + 1e-9
