@@ -1035,7 +1035,10 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
       cached_nav = nav;
     }
 
-    if (phase == kTrackVoxel) {
+    // A step that leaves its solid sets `leave` (1: alive, 2: dead) and breaks
+    // out; the one copy of the exit code below handles every case.
+    int leave = 0;
+    if (phase == kTrackVoxel) do {
       // track_through_ggems_voxelized_solid, TrackThroughGGEMSVoxelizedSolid.cl:133-310
       V3 vs = v3(so.voxel_sizes[0], so.voxel_sizes[1], so.voxel_sizes[2]);
       V3 q = sub(ph.p, bmin);
@@ -1045,8 +1048,8 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
       if (ix >= nx || iy >= ny || iz >= nz || ix < 0 || iy < 0 || iz < 0) {
         ph.psd = kOutOfWorld;
         ph.solid_id = -1;
-        leave_solid(so, false);
-        continue;
+        leave = 1;
+        break;
       }
       int material = __ldg(so.labels + (ix + iy * nx + iz * nx * ny));
       int proc;
@@ -1070,8 +1073,8 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
       if (!in_aabb(ph.p, bmin, bmax)) {
         ph.psd = kOutOfWorld;
         ph.solid_id = -1;
-        leave_solid(so, false);
-        continue;
+        leave = 1;
+        break;
       }
       if (kDose && so.dose_tle) {
         // The step's deposit depends only on the energy before the interaction,
@@ -1093,8 +1096,9 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
         if ((kDose && so.dose_map >= 0)) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
         ph.status = GG_DEAD;
       }
-      if (ph.status == GG_DEAD) leave_solid(so, true);
-    } else if (kFull && phase == kTrackMesh) {
+      if (ph.status == GG_DEAD) leave = 2;
+    } while (0);
+    else if (kFull && phase == kTrackMesh) do {
       // track_through_ggems_meshed_solid, TrackThroughGGEMSMeshSolid.cl:385-518:
       // the parity of the crossing count says whether the photon is inside the
       // mesh; outside, it jumps to the first crossing.  Material 0.
@@ -1103,8 +1107,8 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
       if (x.count == 0) {
         ph.psd = kOutOfWorld;
         ph.solid_id = -1;
-        leave_solid(so, false);
-        continue;
+        leave = 1;
+        break;
       }
       V3 next = x.first;
       if ((x.count & 1) == 0) {
@@ -1142,8 +1146,9 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
         if ((kDose && so.dose_map >= 0)) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
         ph.status = GG_DEAD;
       }
-      if (ph.status == GG_DEAD) leave_solid(so, true);
-    } else {
+      if (ph.status == GG_DEAD) leave = 2;
+    } while (0);
+    else do {
       // track_through_ggems_solid_box, TrackThroughGGEMSSolidBox.cl:122-248
       int proc;
       float nid = next_interaction(rng, nv, sig, energy_id, 0, proc);
@@ -1157,8 +1162,8 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
       if (!in_aabb(ph.p, bmin, bmax)) {
         ph.psd = kOutOfWorld;
         ph.solid_id = -1;
-        leave_solid(so, false);
-        continue;
+        leave = 1;
+        break;
       }
       if (ph.E < so.threshold) ph.status = GG_DEAD;
       trk(GG_TRACK_STEP, ph.solid_id, proc);
@@ -1172,8 +1177,9 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
         ph.E = 0.0f;
         box_histogram(so, ph);
       }
-      if (ph.status == GG_DEAD) leave_solid(so, true);
-    }
+      if (ph.status == GG_DEAD) leave = 2;
+    } while (0);
+    if (leave) leave_solid(so, leave == 2);
   }
 }
 
