@@ -1038,30 +1038,39 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
     // A step that leaves its solid sets `leave` (1: alive, 2: dead) and breaks
     // out; the one copy of the exit code below handles every case.
     int leave = 0;
-    if (phase == kTrackVoxel) do {
-      // track_through_ggems_voxelized_solid, TrackThroughGGEMSVoxelizedSolid.cl:133-310
-      V3 vs = v3(so.voxel_sizes[0], so.voxel_sizes[1], so.voxel_sizes[2]);
-      V3 q = sub(ph.p, bmin);
-      q = so.voxel_pow2 ? mul(q, v3(so.inv_voxel_sizes[0], so.inv_voxel_sizes[1], so.inv_voxel_sizes[2])) : divv(q, vs);
-      int ix = __float2int_rz(q.x), iy = __float2int_rz(q.y), iz = __float2int_rz(q.z);
-      const int nx = so.number_of_voxels[0], ny = so.number_of_voxels[1], nz = so.number_of_voxels[2];
-      if (ix >= nx || iy >= ny || iz >= nz || ix < 0 || iy < 0 || iz < 0) {
-        ph.psd = kOutOfWorld;
-        ph.solid_id = -1;
-        leave = 1;
-        break;
+    if (!kFull || phase != kTrackMesh) do {
+      // One step through a voxelized solid (track_through_ggems_voxelized_solid,
+      // TrackThroughGGEMSVoxelizedSolid.cl:133-310) or a detector box
+      // (track_through_ggems_solid_box, TrackThroughGGEMSSolidBox.cl:122-248):
+      // the same sampling and slab test against the current voxel or the whole
+      // box (material 0), then each solid's own tail.
+      const bool voxel = phase == kTrackVoxel;
+      V3 vmin = bmin, vmax = bmax;
+      int material = 0;
+      if (voxel) {
+        V3 vs = v3(so.voxel_sizes[0], so.voxel_sizes[1], so.voxel_sizes[2]);
+        V3 q = sub(ph.p, bmin);
+        q = so.voxel_pow2 ? mul(q, v3(so.inv_voxel_sizes[0], so.inv_voxel_sizes[1], so.inv_voxel_sizes[2])) : divv(q, vs);
+        int ix = __float2int_rz(q.x), iy = __float2int_rz(q.y), iz = __float2int_rz(q.z);
+        const int nx = so.number_of_voxels[0], ny = so.number_of_voxels[1], nz = so.number_of_voxels[2];
+        if (ix >= nx || iy >= ny || iz >= nz || ix < 0 || iy < 0 || iz < 0) {
+          ph.psd = kOutOfWorld;
+          ph.solid_id = -1;
+          leave = 1;
+          break;
+        }
+        material = __ldg(so.labels + (ix + iy * nx + iz * nx * ny));
+        vmin = add(bmin, mul(v3(static_cast<float>(ix), static_cast<float>(iy), static_cast<float>(iz)), vs));
+        vmax = add(vmin, vs);
       }
-      int material = __ldg(so.labels + (ix + iy * nx + iz * nx * ny));
       int proc;
       float nid = next_interaction(rng, nv, sig, energy_id, material, proc);
-      V3 vmin = add(bmin, mul(v3(static_cast<float>(ix), static_cast<float>(iy), static_cast<float>(iz)), vs));
-      V3 vmax = add(vmin, vs);
       ph.p = safety_inside(ph.p, vmin, vmax);
       float dtb = distance_to_aabb(ph.p, ph.d, inv_d, vmin, vmax);
       if (dtb <= nid) {
         nid = dtb + kTolerance;
         proc = GG_TRANSPORTATION;
-        if ((kDose && so.dose_map >= 0)) {
+        if (kDose && voxel && so.dose_map >= 0) {
           const DevDoseMap& dm = P.dose_maps[so.dose_map];
           if (dm.photon_tracking) {
             int id = dosel(dm, ph.p);
@@ -1076,7 +1085,9 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
         leave = 1;
         break;
       }
-      if (kDose && so.dose_tle) {
+      if (!voxel) {
+        if (ph.E < so.threshold) ph.status = GG_DEAD;
+      } else if (kDose && so.dose_tle) {
         // The step's deposit depends only on the energy before the interaction,
         // so it is recorded here even when the interaction itself is deferred.
         dose_record(P.dose_maps[so.dose_map], tle_edep(tab.attenuation(nav), material, ph.E, nid), ph.p);
@@ -1087,14 +1098,22 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
         phase = kInteract;
         continue;
       }
-      if (proc == GG_PHOTOELECTRIC_EFFECT) {
-        if ((kDose && so.dose_map >= 0) && !so.dose_tle) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
-        ph.status = GG_DEAD;
-        ph.E = 0.0f;
-      }
-      if (ph.E <= tab.photon_cut(nav)[material]) {
-        if ((kDose && so.dose_map >= 0)) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
-        ph.status = GG_DEAD;
+      if (!voxel) {
+        if (proc == GG_PHOTOELECTRIC_EFFECT) {
+          ph.status = GG_DEAD;
+          ph.E = 0.0f;
+          box_histogram(so, ph);
+        }
+      } else {
+        if (proc == GG_PHOTOELECTRIC_EFFECT) {
+          if (kDose && so.dose_map >= 0 && !so.dose_tle) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
+          ph.status = GG_DEAD;
+          ph.E = 0.0f;
+        }
+        if (ph.E <= tab.photon_cut(nav)[material]) {
+          if (kDose && so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
+          ph.status = GG_DEAD;
+        }
       }
       if (ph.status == GG_DEAD) leave = 2;
     } while (0);
@@ -1145,37 +1164,6 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
       if (ph.E <= tab.photon_cut(nav)[0]) {
         if ((kDose && so.dose_map >= 0)) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
         ph.status = GG_DEAD;
-      }
-      if (ph.status == GG_DEAD) leave = 2;
-    } while (0);
-    else do {
-      // track_through_ggems_solid_box, TrackThroughGGEMSSolidBox.cl:122-248
-      int proc;
-      float nid = next_interaction(rng, nv, sig, energy_id, 0, proc);
-      ph.p = safety_inside(ph.p, bmin, bmax);
-      float dtb = distance_to_aabb(ph.p, ph.d, inv_d, bmin, bmax);
-      if (dtb <= nid) {
-        nid = dtb + kTolerance;
-        proc = GG_TRANSPORTATION;
-      }
-      ph.p = safety_outside(add(ph.p, scale(ph.d, nid)), bmin, bmax);
-      if (!in_aabb(ph.p, bmin, bmax)) {
-        ph.psd = kOutOfWorld;
-        ph.solid_id = -1;
-        leave = 1;
-        break;
-      }
-      if (ph.E < so.threshold) ph.status = GG_DEAD;
-      trk(GG_TRACK_STEP, ph.solid_id, proc);
-      if (proc == GG_COMPTON_SCATTERING || proc == GG_RAYLEIGH_SCATTERING) {
-        pending = proc << 8;
-        phase = kInteract;
-        continue;
-      }
-      if (proc == GG_PHOTOELECTRIC_EFFECT) {
-        ph.status = GG_DEAD;
-        ph.E = 0.0f;
-        box_histogram(so, ph);
       }
       if (ph.status == GG_DEAD) leave = 2;
     } while (0);
