@@ -183,8 +183,8 @@ struct DoseParams {
   float* uncertainty;
 };
 
-void launch_transport(const TransportParams& p, int grid, size_t smem, void* stream, bool mesh, bool dose);
-cudaError_t configure_transport(size_t smem, int* blocks_per_sm, bool mesh, bool batch, bool dose);
+void launch_transport(const TransportParams& p, int grid, size_t smem, void* stream, bool mesh, bool dose, bool aux);
+cudaError_t configure_transport(size_t smem, int* blocks_per_sm, bool mesh, bool batch, bool dose, bool aux);
 cudaError_t set_rayleigh_fit(const float* pp);
 void launch_compute_dose(const DoseParams& p, void* stream);
 

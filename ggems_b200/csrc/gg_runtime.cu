@@ -785,6 +785,7 @@ struct JobLaunch {
   size_t smem = 0;
   bool mesh = false;
   bool dose = false;  // some solid tallies into a dose map
+  bool aux = false;   // world grid or particle tracking
   bool empty = true;
 };
 
@@ -829,6 +830,7 @@ int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*
     }
   }
   if (dj.empty()) return GG_OK;
+  bool aux = false;
   bool dose = false;
   for (int s = 0; s < c->number_of_solids; ++s) dose |= c->solid_dev_host[s].dose_map >= 0;
   for (const gg::DevSolid& d : job_solids) dose |= d.dose_map >= 0;
@@ -865,7 +867,7 @@ int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*
     P.tracking_capacity = c->tracking_capacity;
     P.tracking_points = c->tracking_points;
     P.tracking_count = c->tracking_count;
-    mesh = true;  // recorded by the full kernel variant
+    aux = true;  // recorded by the full kernel variant
   }
   if (c->world_cells) {
     std::memcpy(P.world_dimensions, c->world_dimensions, sizeof(P.world_dimensions));
@@ -874,12 +876,12 @@ int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*
     P.world_energy = c->world_energy;
     P.world_energy_squared = c->world_energy_squared;
     P.world_momentum = c->world_momentum;
-    mesh = true;  // the world walk lives in the full kernel variant
+    aux = true;  // the world walk lives in the full kernel variant
   }
   out->smem = (c->tables_in_smem ? c->table_bytes : 0) + sizeof(gg::DevSolid) * c->number_of_solids +
               sizeof(gg::DevNavigator) * c->number_of_navigators + 16;
   int blocks_per_sm = 0;
-  GG_CUDA(gg::configure_transport(out->smem, &blocks_per_sm, mesh, P.number_of_jobs > 1, dose));
+  GG_CUDA(gg::configure_transport(out->smem, &blocks_per_sm, mesh, P.number_of_jobs > 1, dose, aux));
   if (blocks_per_sm < 1) return fail(GG_ERROR_CUDA, "transport kernel does not fit on an SM");
   if (c->blocks_per_sm > 0 && c->blocks_per_sm < blocks_per_sm) blocks_per_sm = c->blocks_per_sm;
   uint64_t grid = static_cast<uint64_t>(blocks_per_sm) * c->sm_count;
@@ -888,6 +890,7 @@ int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*
   out->grid = static_cast<int>(grid);
   out->mesh = mesh;
   out->dose = dose;
+  out->aux = aux;
   out->empty = false;
   return GG_OK;
 }
@@ -897,7 +900,7 @@ int enqueue_jobs(gg_context* c, const JobLaunch& L) {
   GG_CUDA(cudaMemsetAsync(c->slot_counter, 0, sizeof(unsigned int), c->stream));
   if (L.params.tracking_count) GG_CUDA(cudaMemsetAsync(L.params.tracking_count, 0, sizeof(int32_t), c->stream));
   GG_CUDA(cudaMemsetAsync(c->error, 0, sizeof(int), c->stream));
-  gg::launch_transport(L.params, L.grid, L.smem, c->stream, L.mesh, L.dose);
+  gg::launch_transport(L.params, L.grid, L.smem, c->stream, L.mesh, L.dose, L.aux);
   GG_CUDA(cudaGetLastError());
   return GG_OK;
 }

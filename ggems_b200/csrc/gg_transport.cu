@@ -762,12 +762,14 @@ __device__ bool stage_tables(unsigned char* dst, const unsigned char* src, uint3
 
 extern __shared__ __align__(16) unsigned char g_smem[];
 
-// kFull: the scene has a meshed solid or records world tracking.  Scenes
-// with neither run the variant compiled without the mesh phase and the world
-// walk, so their code and registers stay out of the voxel / detector hot loop.
+// kFull: the scene has a meshed solid, a world grid or a tracked particle;
+// kAux: the world walk and particle tracking are compiled in.  Scenes without
+// them run variants compiled without that code, so its instructions and
+// registers stay out of the voxel / detector (or mesh) hot loop.
+// kDose: some solid tallies into a dose map.
 // kBatch: several jobs (source runs) in one launch, each with its own solids.
-template <bool kFull, bool kBatch, bool kDose>
-__global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) transport_kernel(TransportParams P) {
+template <bool kFull, bool kBatch, bool kDose, bool kAux>
+__global__ void __launch_bounds__(kBlockThreads, kAux ? 2 : (kFull ? 3 : (kBatch ? 3 : 4))) transport_kernel(TransportParams P) {
   // shared memory: [tables][solids][navigators][mbarrier]
   unsigned char* tables = g_smem;
   DevSolid* scene_solids = reinterpret_cast<DevSolid*>(g_smem + (P.tables_in_smem ? P.table_bytes : 0));
@@ -806,7 +808,7 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
   // particle tracking (full variant only): a point of this lane's photon when
   // its slot is the tracked one
   auto trk = [&](int kind, int solid, int process) {
-    if (kFull && P.tracking_points && static_cast<int>(slot) == P.tracking_slot)
+    if (kAux && P.tracking_points && static_cast<int>(slot) == P.tracking_slot)
       track_point(P.tracking_points, P.tracking_count, P.tracking_capacity, kind, solid, process, history_number, ph.p,
                   ph.d, ph.E);
   };
@@ -957,7 +959,7 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
         ph.psd = kOutOfWorld;
         rounds = 0;
         phase = kFind;
-        if (kFull) {
+        if (kAux) {
           ++history_number;
           trk(GG_TRACK_PRIMARY, -1, -1);
         }
@@ -986,7 +988,7 @@ __global__ void __launch_bounds__(kBlockThreads, kFull ? 2 : (kBatch ? 3 : 4)) t
             ph.solid_id = s;
           }
         }
-        if (kFull && P.world_dimensions[0] > 0 && ph.status != GG_DEAD) world_track(ph.p, ph.d, ph.E, ph.psd, P);
+        if (kAux && P.world_dimensions[0] > 0 && ph.status != GG_DEAD) world_track(ph.p, ph.d, ph.E, ph.psd, P);
         // project_to_* (ProjectToGGEMS*.cl:44-129)
         if (ph.solid_id == -1) ph.status = GG_DEAD;
         if (ph.psd == kOutOfWorld) {
@@ -1218,18 +1220,20 @@ __global__ void compute_dose_kernel(DoseParams P) {
 
 namespace {
 using TransportKernel = void (*)(TransportParams);
-// kFull: meshes, world grid or particle tracking (dose code always in);
-// otherwise the dose-map code is compiled in only for scenes that tally dose.
-TransportKernel transport_variant(bool mesh, bool batch, bool dose) {
-  if (mesh) return batch ? transport_kernel<true, true, true> : transport_kernel<true, false, true>;
-  if (dose) return batch ? transport_kernel<false, true, true> : transport_kernel<false, false, true>;
-  return batch ? transport_kernel<false, true, false> : transport_kernel<false, false, false>;
+// kFull: meshed solids, world grid or particle tracking (dose code always in),
+// kAux: world grid or particle tracking; otherwise the dose-map code is
+// compiled in only for scenes that tally dose.
+TransportKernel transport_variant(bool mesh, bool batch, bool dose, bool aux) {
+  if (aux) return batch ? transport_kernel<true, true, true, true> : transport_kernel<true, false, true, true>;
+  if (mesh) return batch ? transport_kernel<true, true, true, false> : transport_kernel<true, false, true, false>;
+  if (dose) return batch ? transport_kernel<false, true, true, false> : transport_kernel<false, false, true, false>;
+  return batch ? transport_kernel<false, true, false, false> : transport_kernel<false, false, false, false>;
 }
 }  // namespace
 
-void launch_transport(const TransportParams& p, int grid, size_t smem, void* stream, bool mesh, bool dose) {
+void launch_transport(const TransportParams& p, int grid, size_t smem, void* stream, bool mesh, bool dose, bool aux) {
   const bool batch = p.number_of_jobs > 1;
-  transport_variant(mesh, batch, dose)<<<grid, kBlockThreads, smem, static_cast<cudaStream_t>(stream)>>>(p);
+  transport_variant(mesh, batch, dose, aux)<<<grid, kBlockThreads, smem, static_cast<cudaStream_t>(stream)>>>(p);
 }
 
 namespace {
@@ -1323,8 +1327,8 @@ void launch_compute_dose(const DoseParams& p, void* stream) {
   compute_dose_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(p);
 }
 
-cudaError_t configure_transport(size_t smem, int* blocks_per_sm, bool mesh, bool batch, bool dose) {
-  auto kernel = transport_variant(mesh, batch, dose);
+cudaError_t configure_transport(size_t smem, int* blocks_per_sm, bool mesh, bool batch, bool dose, bool aux) {
+  auto kernel = transport_variant(mesh, batch, dose, aux);
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, kBlockThreads, smem);
