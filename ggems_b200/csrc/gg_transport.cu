@@ -909,6 +909,11 @@ __global__ void __launch_bounds__(kBlockThreads, kAux ? 2 : (kFull ? 3 : (kBatch
     const unsigned tracking =
         __ballot_sync(0xffffffffu, phase == kTrackVoxel || phase == kTrackBox || (kFull && phase == kTrackMesh));
     const int n_other = __popc(active & ~tracking);
+    // A step or an interaction that ends the photon's stay in its solid sets
+    // `leave` (1: alive, 2: dead) and `leaving`, and jumps to the one copy of
+    // the exit code at the end of the loop body.
+    int leave = 0;
+    const DevSolid* leaving = nullptr;
     if (n_other > 0 && (n_other >= regroup || 4 * n_other >= ratio4 * __popc(tracking))) {
       // A round serves one kind of rare work: the interaction samplers, or the
       // new-history / FindSolid chain, whichever more lanes wait for; the
@@ -940,11 +945,12 @@ __global__ void __launch_bounds__(kBlockThreads, kAux ? 2 : (kFull ? 3 : (kBatch
           box_histogram(so, ph);
         }
         if (ph.status == GG_DEAD) {
-          leave_solid(so, true);
-        } else {
-          inv_d = reciprocal(ph.d);
-          phase = track_phase(so.type);
+          leave = 2;
+          leaving = &so;
+          goto exit_solid;
         }
+        inv_d = reciprocal(ph.d);
+        phase = track_phase(so.type);
         continue;
       }
       if (phase == kNewHistory) {
@@ -1023,6 +1029,7 @@ __global__ void __launch_bounds__(kBlockThreads, kAux ? 2 : (kFull ? 3 : (kBatch
       continue;
     }
     if (phase != kTrackVoxel && phase != kTrackBox && !(kFull && phase == kTrackMesh)) continue;
+    {
 
     // ---- one tracking step inside solid ph.solid_id ----
     const DevSolid& so = solids[ph.solid_id];
@@ -1037,9 +1044,7 @@ __global__ void __launch_bounds__(kBlockThreads, kAux ? 2 : (kFull ? 3 : (kBatch
       cached_nav = nav;
     }
 
-    // A step that leaves its solid sets `leave` (1: alive, 2: dead) and breaks
-    // out; the one copy of the exit code below handles every case.
-    int leave = 0;
+    leaving = &so;
     if (!kFull || phase != kTrackMesh) do {
       // One step through a voxelized solid (track_through_ggems_voxelized_solid,
       // TrackThroughGGEMSVoxelizedSolid.cl:133-310) or a detector box
@@ -1169,7 +1174,9 @@ __global__ void __launch_bounds__(kBlockThreads, kAux ? 2 : (kFull ? 3 : (kBatch
       }
       if (ph.status == GG_DEAD) leave = 2;
     } while (0);
-    if (leave) leave_solid(so, leave == 2);
+    }
+  exit_solid:
+    if (leave) leave_solid(*leaving, leave == 2);
   }
 }
 
