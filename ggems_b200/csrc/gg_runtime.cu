@@ -63,6 +63,10 @@ struct gg_context {
   uint32_t* rng = nullptr;
   gg::DevParticles particles{};
   std::vector<void*> scene_allocations;  // freed on re-upload / destroy
+  // Re-uploads reuse the previous scene's buffers of the same sizes (no
+  // cudaFree / cudaMalloc per upload when only the contents change).
+  std::map<void*, size_t> scene_bytes;
+  std::vector<std::pair<void*, size_t>> scene_spares;
   std::vector<void*> run_allocations;    // source arrays of the last run
   gg::DevSolid* solids = nullptr;
   int number_of_solids = 0;
@@ -107,7 +111,18 @@ int dev_copy_to(gg_context* c, std::vector<void*>& owner, const T* host, size_t 
   *out = nullptr;
   if (n == 0) return GG_OK;
   void* p = nullptr;
-  GG_CUDA(cudaMalloc(&p, n * sizeof(T)));
+  const size_t bytes = n * sizeof(T);
+  const bool scene = &owner == &c->scene_allocations;
+  if (scene) {
+    for (size_t i = 0; i < c->scene_spares.size(); ++i)
+      if (c->scene_spares[i].second == bytes) {
+        p = c->scene_spares[i].first;
+        c->scene_spares.erase(c->scene_spares.begin() + static_cast<std::ptrdiff_t>(i));
+        break;
+      }
+  }
+  if (!p) GG_CUDA(cudaMalloc(&p, bytes));
+  if (scene) c->scene_bytes[p] = bytes;
   owner.push_back(p);
   if (host) GG_CUDA(cudaMemcpyAsync(p, host, n * sizeof(T), cudaMemcpyHostToDevice, c->stream));
   else GG_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), c->stream));
@@ -120,8 +135,24 @@ int dev_copy(gg_context* c, const T* host, size_t n, T** out) {
   return dev_copy_to(c, c->scene_allocations, host, n, out);
 }
 
-void free_scene(gg_context* c) {
-  for (void* p : c->scene_allocations) cudaFree(p);
+// keep_buffers: the scene's device buffers become spares for the next upload
+// (release_spares() frees what that upload did not reuse).
+void release_spares(gg_context* c) {
+  for (auto& sp : c->scene_spares) {
+    c->scene_bytes.erase(sp.first);
+    cudaFree(sp.first);
+  }
+  c->scene_spares.clear();
+}
+void free_scene(gg_context* c, bool keep_buffers = false) {
+  for (void* p : c->scene_allocations) {
+    if (keep_buffers) c->scene_spares.emplace_back(p, c->scene_bytes[p]);
+    else {
+      c->scene_bytes.erase(p);
+      cudaFree(p);
+    }
+  }
+  if (!keep_buffers) release_spares(c);
   c->scene_allocations.clear();
   c->solids = nullptr;
   c->navigators = nullptr;
@@ -554,7 +585,7 @@ GG_API int gg_upload_scene(gg_context* c, const gg_scene* sc) {
   if (!sc->rayleigh_fit) return fail(GG_ERROR_INVALID_ARGUMENT, "scene has no Rayleigh fit table");
   GG_CUDA(cudaSetDevice(c->device));
   GG_CUDA(cudaStreamSynchronize(c->stream));
-  free_scene(c);
+  free_scene(c, true);
   GG_CUDA(gg::set_rayleigh_fit(sc->rayleigh_fit));
 
   // Navigators that need the TLE attenuation tables.
@@ -699,6 +730,7 @@ GG_API int gg_upload_scene(gg_context* c, const gg_scene* sc) {
   c->tables_in_smem = c->table_bytes + fixed <= 96 * 1024;
   GG_CUDA(cudaStreamSynchronize(c->stream));
   c->scene_ready = true;
+  release_spares(c);
   return GG_OK;
 }
 
