@@ -769,7 +769,7 @@ extern __shared__ __align__(16) unsigned char g_smem[];
 // kDose: some solid tallies into a dose map.
 // kBatch: several jobs (source runs) in one launch, each with its own solids.
 template <bool kFull, bool kBatch, bool kDose, bool kAux>
-__global__ void __launch_bounds__(kBlockThreads, kAux ? 2 : (kFull ? 3 : (kBatch ? 3 : 4))) transport_kernel(TransportParams P) {
+__global__ void __launch_bounds__(kBlockThreads, kAux ? 2 : (kFull ? 3 : (kBatch && kDose ? 3 : 4))) transport_kernel(TransportParams P) {
   // shared memory: [tables][solids][navigators][mbarrier]
   unsigned char* tables = g_smem;
   DevSolid* scene_solids = reinterpret_cast<DevSolid*>(g_smem + (P.tables_in_smem ? P.table_bytes : 0));

@@ -38,6 +38,7 @@ MATERIALS = os.path.join(ROOT, "ggems_b200", "data", "materials.txt")
 PHANTOM_N, PHANTOM_VOXEL = 64, 2.0
 ENERGY_MEV = 0.060
 JUDGE_TOLERANCE = 0.05
+JUDGE_BLOCKS_PER_SM = 3  # transport CTAs per SM for the judge MC (0: as many as fit)
 
 
 def _lib():
@@ -534,7 +535,17 @@ def surrogate_pipeline(geo, net, projections, judge_primaries, seed):
     t = [time.perf_counter()]
     # the MC estimates run on the transport context's stream while the
     # projector (its own context) and the network (its own stream) work
-    run = geo.start_simulation(projections, int(judge_primaries), seed=seed, totals=False)
+    # The judge MC runs three CTAs per SM instead of the four that fit: the
+    # registers left on every SM let the projector's and the network's kernels
+    # run beside it instead of after it.
+    from ._native import check
+    lanes, ratio4 = C.c_int32(), C.c_int32()
+    check(geo.lib.gg_get_transport_tuning(geo.ctx, None, C.byref(lanes), C.byref(ratio4)), "tuning")
+    check(geo.lib.gg_set_transport_tuning(geo.ctx, JUDGE_BLOCKS_PER_SM, lanes.value, ratio4.value), "tuning")
+    try:
+        run = geo.start_simulation(projections, int(judge_primaries), seed=seed, totals=False)
+    finally:
+        check(geo.lib.gg_set_transport_tuning(geo.ctx, 0, lanes.value, ratio4.value), "tuning")
     t.append(time.perf_counter())
     x = make_inputs(geo, projections)
     t.append(time.perf_counter())
