@@ -140,6 +140,12 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def _smi_device(local=0):
+    """The nvidia-smi id (index or UUID) of this process's CUDA device `local`."""
+    vis = [d.strip() for d in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if d.strip()]
+    return vis[local] if local < len(vis) else str(local)
+
+
 def _profile_value(key):
     """A figure from the committed ncu summary of the transport kernel ("key: value" lines)."""
     path = os.path.join(ROOT, "profiles", "transport_kernel_cbct256.md")
@@ -159,6 +165,24 @@ def _profile_traffic():
     return _profile_value("dram_bytes_per_full_launch")
 
 
+def _issue_roofline(primaries_per_s, clocks):
+    """The transport kernel's real limit: warp instructions issued per second
+    (warp instructions per primary, from the committed ncu summary of this
+    workload, x primaries/s) against the issue ceiling of one warp instruction
+    per scheduler per cycle (SMs x 4 schedulers x median SM clock sampled during
+    the timed region)."""
+    per_primary = _profile_value("warp_instructions_per_primary")
+    if not per_primary or not clocks or not clocks.get("sm_mhz"):
+        return None
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    ceiling = sms * 4 * clocks["sm_mhz"] * 1e6
+    achieved = per_primary * primaries_per_s
+    return {"bound": "issue", "achieved": achieved / 1e12, "peak": ceiling / 1e12, "unit": "T warp-inst/s",
+            "frac": achieved / ceiling, "warp_instructions_per_primary": per_primary, "sms": sms,
+            "sm_mhz": clocks["sm_mhz"]}
+
+
 def _peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -166,10 +190,11 @@ def _peaks():
         return None
 
 
-def cpu_reference_run(scene_ptr, source, n, threads, kind):
+def cpu_reference_run(scene_ptr, source, n, threads, kind, states):
     """Run n primaries of the workload on the host with the reference kernels
     (oracle/_ref, GGEMS's own device code compiled for the host) or the oracle
-    port.  Returns (seconds, counts per primary or None)."""
+    port, from a copy of `states` (5 x 2^20 JKISS words).  Returns (seconds,
+    counts per primary or None)."""
     from ggems_b200 import abi
     import numpy as np
     if kind == "reference":
@@ -182,9 +207,7 @@ def cpu_reference_run(scene_ptr, source, n, threads, kind):
     fn.argtypes = [C.POINTER(abi.gg_scene), C.POINTER(abi.gg_source), C.c_uint64, C.POINTER(C.c_uint32),
                    C.POINTER(abi.gg_particle_buffers), C.POINTER(abi.gg_tally_buffers), C.c_int]
     sc = scene_ptr.contents
-    states = np.zeros(5 * abi.GG_MAXIMUM_PARTICLES, np.uint32)
-    from ggems_b200._native import lib as native
-    native.gg_seed_random_states(abi.ptr(states, C.c_uint32), abi.GG_MAXIMUM_PARTICLES, 777, 0)
+    st = np.array(states, np.uint32, copy=True)
     hs = [int(sc.histogram_sizes[i]) for i in range(sc.number_of_histograms)]
     ds = [int(sc.dose_maps[i].total_number_of_dosels) for i in range(sc.number_of_dose_maps)]
     tallies = abi.Tallies(hs, ds)
@@ -193,7 +216,7 @@ def cpu_reference_run(scene_ptr, source, n, threads, kind):
         lib.gg_oracle_counts.argtypes = [C.POINTER(C.c_uint64), C.c_int]
         lib.gg_oracle_counts(None, 1)
     t0 = time.perf_counter()
-    rc = fn(scene_ptr, C.byref(source), n, abi.ptr(states, C.c_uint32), None, C.byref(tallies.struct), threads)
+    rc = fn(scene_ptr, C.byref(source), n, abi.ptr(st, C.c_uint32), None, C.byref(tallies.struct), threads)
     dt = time.perf_counter() - t0
     if rc != 0:
         raise RuntimeError("CPU run failed: %d" % rc)
@@ -214,17 +237,53 @@ def _ensure_oracle():
         subprocess.check_call([sys.executable, os.path.join(ROOT, "oracle", "build.py")])
 
 
-def _sample_size(scene_ptr, source, threads, kind, budget_s):
+def _seed_states(seed=777):
+    """GGEMS's seeding (std::mt19937(seed), 4 words per slot) from the oracle side."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import scenes
+    return scenes.seed_states(seed)
+
+
+def _sample_size(scene_ptr, source, threads, kind, budget_s, states):
     """Primaries for about budget_s seconds of host work (pilot run first)."""
     pilot = 20000
     while True:
-        dt, _ = cpu_reference_run(scene_ptr, source, pilot, threads, kind)
+        dt, _ = cpu_reference_run(scene_ptr, source, pilot, threads, kind, states)
         # a pilot shorter than a second is dominated by thread start-up: grow it
         if dt >= 1.0 or pilot >= 4 * 1048576:
             break
         pilot = min(pilot * max(2, int(1.0 / max(dt, 1e-3))), 4 * 1048576)
     n = int(pilot * budget_s / max(dt, 1e-3))
     return max(pilot, min(n, 64 * 1048576))
+
+
+def _batch_sizes(primaries):
+    """GGEMSSource::OrganizeParticlesInBatch: ceil(n / 2^20) batches, the first
+    n mod batches of them one primary larger."""
+    nb = -(-primaries // 1048576)
+    q, r = divmod(primaries, nb)
+    return [q + 1 if i < r else q for i in range(nb)]
+
+
+def _cbct_sample(scene_ptr, source, threads, kind, budget_s, states, primaries=PRIMARIES):
+    """A bounded sample of the projection: its first k whole batches (the same
+    slots and random streams as the projection's first k batches), k chosen so
+    that one run takes about budget_s on these threads.  Returns (k, primaries)."""
+    sizes = _batch_sizes(primaries)
+    dt, _ = cpu_reference_run(scene_ptr, source, sizes[0], threads, kind, states)
+    k = max(1, min(len(sizes), int(round(budget_s / max(dt, 1e-3)))))
+    return k, sum(sizes[:k])
+
+
+def _cbct_config(primaries, batches, world):
+    """The workload both arms report (same dict on the product and the reference arm)."""
+    return {"workload": WORKLOAD, "phantom": "256x256x256 uint8, 1 mm, air/water/bone(1.85)",
+            "primaries_per_step": primaries, "batches_per_step": batches,
+            "detector": "flat 512x512 GOS, 0.8 mm, SDD 1500 / SID 1000",
+            "processes": "Compton, photoelectric, Rayleigh",
+            "parallelism": ("%d ranks, independent histories, one tally all-reduce per run" % world) if world > 1
+            else "single GPU",
+            "l2": "256 MB buffer written between timed steps (inputs 17 MB < L2)"}
 
 
 def main():
@@ -247,14 +306,13 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
 
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
     _ensure_built()
     _ensure_oracle()
     tmp = tempfile.mkdtemp(prefix="ggems_bench_")
     from ggems_b200 import workloads
     files = workloads.cbct_files(tmp, 256, 1.0, seed=1)
-
-    if args.impl == "reference":
-        return run_reference_arm(args, files, rank, world)
     if args.workload == "batched":
         return run_batched(args, tmp, rank)
     if args.workload == "mesh":
@@ -272,7 +330,6 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    os.environ.setdefault("CUDA_VISIBLE_DEVICES", os.environ.get("CUDA_VISIBLE_DEVICES", ""))
 
     gg = _configure(files, args.primaries)
     from ggems_b200 import abi, distributed
@@ -280,8 +337,9 @@ def main():
     if world > 1:
         gg.GGEMSOpenCLManager().set_device_index(local)
     ggems = gg.GGEMS()
-    # Rank r takes random streams after those of ranks < r (device order of GGEMSPseudoRandomGenerator).
-    ggems.initialize(777 + 0 * rank)
+    # Every rank seeds 777; rank r then takes the random streams after those of
+    # ranks < r (device order of GGEMSPseudoRandomGenerator), set just below.
+    ggems.initialize(777)
     ctx = lib.ggems_device_context(ggems.obj, 0)
     if rank > 0:
         import numpy as np
@@ -318,7 +376,7 @@ def main():
     # ---- device-timed region (inputs resident in HBM) ----
     times, launches = [], 0
     barrier()
-    with ClockSampler(local if world > 1 else int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)) as clk:
+    with ClockSampler(_smi_device(local)) as clk:
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
@@ -378,16 +436,21 @@ def main():
     batches = int(nb.value)
 
     # ---- CPU baseline and roofline (rank 0, N = 1 only) ----
+    # The same sample the reference arm times: the projection's first whole
+    # batches from GGEMS's seeding of 777, on every host thread.
     cpu_baseline, counts = None, None
     kind = _cpu_kind()
+    ref_states = _seed_states(777)
     if not args.no_cpu_baseline and world == 1:
         threads = os.cpu_count() or 1
-        n = _sample_size(scene_ptr, src, threads, kind, 15.0)
-        dt, _ = cpu_reference_run(scene_ptr, src, n, threads, kind)
+        k, n = _cbct_sample(scene_ptr, src, threads, kind, 4.0, ref_states, args.primaries)
+        dts = [cpu_reference_run(scene_ptr, src, n, threads, kind, ref_states)[0] for _ in range(3)]
+        dt = statistics.median(dts)
         cpu_baseline = {"value": n / dt, "unit": "primaries/s", "cores": threads, "kind": kind,
-                        "sample": "%d primaries of the same projection (1 batch, seed 777) on %d host threads, %.1f s"
-                                  % (n, threads, dt)}
-    _, counts = cpu_reference_run(scene_ptr, src, 20000 if args.no_cpu_baseline else 100000, os.cpu_count() or 1, "port")
+                        "sample": "the projection's first %d of %d batches (%d primaries, seed 777) on %d host "
+                                  "threads, median of 3 runs of %.1f s" % (k, batches, n, threads, dt)}
+    _, counts = cpu_reference_run(scene_ptr, src, 20000 if args.no_cpu_baseline else 100000, os.cpu_count() or 1,
+                                  "port", ref_states)
     S, box, D, H = counts
     # algorithmic bytes per primary: source state 40 B + 1 B label per voxel step + 20 B per dose
     # deposit + 8 B per detector count + 28 B final state
@@ -396,6 +459,7 @@ def main():
     peak = peaks["hbm_gbs"] if peaks else 6650.0
     achieved = value / world * bytes_per_primary / 1e9
     per_launch_traffic = _profile_traffic()
+    clocks = clk.summary()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": per_launch_traffic,
                 "peak_source": "measured" if peaks else "fallback",
@@ -404,20 +468,18 @@ def main():
                 # issue-bound kernel: what the ncu summary says about the issue slots and lanes
                 "l2_hit_rate_pct": _profile_value("l2_hit_rate_pct"),
                 "issue_active_pct": _profile_value("issue_active_pct"),
-                "lanes_active_pct": _profile_value("lanes_active_pct")}
+                "lanes_active_pct": _profile_value("lanes_active_pct"),
+                "issue": _issue_roofline(value / world, clocks)}
     line = {
         "metric": "primaries/s (CBCT 256^3, 120 kVp)", "value": value, "unit": "primaries/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantom generator, synthetic 120 kVp spectrum)",
-        "config": {"workload": WORKLOAD, "phantom": "256x256x256 uint8, 1 mm, air/water/bone(1.85)",
-                   "primaries_per_step": args.primaries, "batches_per_step": batches, "detector": "flat 512x512 GOS, 0.8 mm, SDD 1500 / SID 1000",
-                   "processes": "Compton, photoelectric, Rayleigh", "parallelism": ("%d ranks, independent histories, one tally all-reduce per run" % world) if world > 1 else "single GPU",
-                   "l2": "256 MB buffer written between timed steps (inputs 17 MB < L2)"},
+        "config": _cbct_config(args.primaries, batches, world),
         "e2e": {"value": e2e_value, "unit": "primaries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "roofline": roofline,
         "cpu_baseline": cpu_baseline,
-        "clocks": clk.summary(),
+        "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
     if dist is not None:
@@ -505,7 +567,7 @@ def run_batched(args, tmp, rank):
     for _ in range(args.warmup):
         step()
     times, launches = [], 0
-    with ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)) as clk:
+    with ClockSampler(_smi_device()) as clk:
         for _ in range(args.steps):
             t, n = step()
             times.append(t)
@@ -587,7 +649,7 @@ def run_mesh(args, tmp, rank):
     for _ in range(args.warmup):
         step()
     times, launches = [], 0
-    with ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)) as clk:
+    with ClockSampler(_smi_device()) as clk:
         for _ in range(args.steps):
             t, n = step()
             times.append(t)
@@ -690,7 +752,7 @@ def run_curved(args, tmp, rank):
     for _ in range(args.warmup):
         step()
     times, launches = [], 0
-    with ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)) as clk:
+    with ClockSampler(_smi_device()) as clk:
         for _ in range(args.steps):
             t, n = step()
             times.append(t)
@@ -700,8 +762,9 @@ def run_curved(args, tmp, rank):
     if not args.no_cpu_baseline:
         kind = _cpu_kind()
         threads = os.cpu_count() or 1
-        m = _sample_size(scene_ptr, s, threads, kind, 10.0)
-        dt, _ = cpu_reference_run(scene_ptr, s, m, threads, kind)
+        st = _seed_states(777)
+        m = _sample_size(scene_ptr, s, threads, kind, 10.0, st)
+        dt, _ = cpu_reference_run(scene_ptr, s, m, threads, kind, st)
         cpu = {"value": m / dt, "unit": "primaries/s", "cores": threads, "kind": kind,
                "sample": "%d primaries of the same projection (seed 777) on %d host threads, %.1f s" % (m, threads, dt)}
     if rank == 0:
@@ -757,7 +820,7 @@ def run_water(args, tmp, rank):
     for _ in range(args.warmup):
         step()
     times, launches = [], 0
-    with ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)) as clk:
+    with ClockSampler(_smi_device()) as clk:
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
@@ -784,8 +847,9 @@ def run_water(args, tmp, rank):
     if not args.no_cpu_baseline:
         kind = _cpu_kind()
         threads = os.cpu_count() or 1
-        m = _sample_size(scene_ptr, src, threads, kind, 10.0)
-        dt, _ = cpu_reference_run(scene_ptr, src, m, threads, kind)
+        st = _seed_states(777)
+        m = _sample_size(scene_ptr, src, threads, kind, 10.0, st)
+        dt, _ = cpu_reference_run(scene_ptr, src, m, threads, kind, st)
         cpu = {"value": m / dt, "unit": "primaries/s", "cores": threads, "kind": kind,
                "sample": "%d primaries of the same run (seed 777) on %d host threads, %.1f s" % (m, threads, dt)}
     if rank == 0:
@@ -844,7 +908,7 @@ def run_volume(args, rank):
     for _ in range(args.warmup):
         step()
     times = []
-    with ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)) as clk:
+    with ClockSampler(_smi_device()) as clk:
         for _ in range(args.steps):
             times.append(step())
     total_ms = sum(times)
@@ -900,50 +964,46 @@ def run_volume(args, rank):
     return 0
 
 
-def run_reference_arm(args, files, rank, world):
-    """The reference's CPU implementation of the path (GGEMS's kernels built for
-    the host when available, else the oracle port) on all host threads."""
+def run_reference_arm(args, rank, world):
+    """The reference's CPU implementation of the path on all host threads:
+    GGEMS's own kernels built for the host (oracle/_ref) when available, else
+    the oracle port, replaying GGEMS::RunOnDevice batch by batch.  The scene,
+    tables and random streams come from the oracle side (tests/scenes.py:
+    the oracle's table builder, GGEMS's mt19937 seeding), so nothing of the
+    product library is loaded.  Each step is a bounded sample of the projection
+    (its first whole batches, the same slots and streams as the projection);
+    `config` is the product arm's."""
     if rank != 0:
         return 0
+    _ensure_oracle()
     kind = _cpu_kind()
-    gg = _configure(files, args.primaries)
-    from ggems_b200 import abi
-    from ggems_b200.api import lib
-    # Tables and scene come from the same API; no GPU work is done here.
-    scene_ptr, src = _host_scene(gg, lib)
-    if scene_ptr is None:
-        print(json.dumps({"impl": "reference", "unavailable": "could not build the host scene"}))
-        return 0
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import scenes
+    scene, source = scenes.cbct_api_scene(256, 1.0, seed=1)
+    ss = scene.struct()
+    scene_ptr = C.pointer(ss)
+    src = source.struct
+    states = scenes.seed_states(777)
     threads = os.cpu_count() or 1
-    n = _sample_size(scene_ptr, src, threads, kind, max(5.0, 60.0 / max(args.steps + args.warmup, 1)))
+    budget = min(8.0, max(1.0, 150.0 / max(args.steps + args.warmup, 1)))
+    k, n = _cbct_sample(scene_ptr, src, threads, kind, budget, states, args.primaries)
     for _ in range(args.warmup):
-        cpu_reference_run(scene_ptr, src, n, threads, kind)
-    times = [cpu_reference_run(scene_ptr, src, n, threads, kind)[0] for _ in range(args.steps)]
+        cpu_reference_run(scene_ptr, src, n, threads, kind, states)
+    times = [cpu_reference_run(scene_ptr, src, n, threads, kind, states)[0] for _ in range(args.steps)]
     value = n * args.steps / sum(times)
-    sample = "%d primaries per step of the 1e8-primary projection on %d host threads" % (n, threads)
+    batches = len(_batch_sizes(args.primaries))
+    sample = ("each step: the projection's first %d of %d batches (%d primaries, seed 777) on %d host threads"
+              % (k, batches, n, threads))
     print(json.dumps({
         "impl": "reference", "metric": "primaries/s (CBCT 256^3, 120 kVp)", "value": value, "unit": "primaries/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded phantom generator, synthetic 120 kVp spectrum)",
-        "config": {"workload": WORKLOAD, "primaries_per_step": n},
+        "config": _cbct_config(args.primaries, batches, world),
         "cpu_baseline": {"value": value, "unit": "primaries/s", "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": "primaries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
     return 0
-
-
-def _host_scene(gg, lib):
-    """Scene of the configured simulation without a GPU (host-side initialisation only)."""
-    from ggems_b200 import abi
-    fn = lib.ggems_host_scene
-    fn.restype = C.POINTER(abi.gg_scene)
-    p = fn()
-    if not p:
-        return None, None
-    src = abi.gg_source()
-    assert lib.ggems_source_descriptor(0, C.byref(src), None) == 0
-    return p, src
 
 
 if __name__ == "__main__":

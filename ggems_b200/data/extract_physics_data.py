@@ -86,7 +86,7 @@ def elements(ref):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GGEMS_REFERENCE_DIR", "/root/reference")
     lines = ["#include <cstdio>", "#include <cstring>", "#include <cstdint>",
              "static void put(FILE* f, const char* name, unsigned code, unsigned n, const void* p, unsigned es) {",
              "  char nm[32]; std::memset(nm, 0, 32); std::strncpy(nm, name, 31); std::fwrite(nm, 1, 32, f);",

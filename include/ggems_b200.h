@@ -369,8 +369,11 @@ GG_API int gg_compute_dose(gg_context* context, int32_t dose_map, int32_t solid,
  * floats (16 MiB), held from library load until process exit; larger dose maps
  * are rejected with GG_ERROR_INVALID_ARGUMENT.  The first call on a device looks
  * up that array's address (once per device), so make it before any stream
- * capture.  All calls on one device share the array: calls that overlap (two
- * threads, or two contexts on the same GPU) race and must be serialised by the
+ * capture.  The address is kept for the life of the process: after a
+ * cudaDeviceReset on a device that has already made a call, this entry point
+ * is not supported on that device (the module is reloaded at a new address).
+ * All calls on one device share the array: calls that overlap (two threads,
+ * or two contexts on the same GPU) race and must be serialised by the
  * caller. */
 #define GG_NO_ALLOC_MAX_DOSELS 2097152
 GG_API int gg_compute_dose_no_alloc(gg_context* context, int32_t dose_map, int32_t solid, float scale_factor,

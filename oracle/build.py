@@ -22,7 +22,14 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 BUILD = os.path.join(HERE, "_build")
 REF_OUT = os.path.join(HERE, "_ref")
-DEFAULT_REFERENCE = "/root/reference"
+# The reference checkout: $GGEMS_REFERENCE_DIR, else the path this recipe was
+# written against.  Only this recipe (and the scripts that call it) read it.
+DEFAULT_REFERENCE = os.environ.get("GGEMS_REFERENCE_DIR", "/root/reference")
+
+
+def reference_dir():
+    """The reference checkout, or None when it is not on this machine."""
+    return DEFAULT_REFERENCE if os.path.isdir(os.path.join(DEFAULT_REFERENCE, "src", "kernels")) else None
 
 CXX = ["g++", "-std=c++20", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math"]
 

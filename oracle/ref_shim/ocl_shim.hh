@@ -5,7 +5,7 @@
 // the reference's own kernel code run on the host.
 //
 // Nothing in the product links this file.  It is force-included (g++ -include)
-// before each .cl translation unit by oracle/build_ref.py.
+// before each .cl translation unit by oracle/build.py (build_ref).
 //
 // Semantics chosen where OpenCL leaves them to the runtime (and mirrored
 // exactly by the product kernels and the oracle restatement):

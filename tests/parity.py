@@ -10,6 +10,16 @@ import scenes
 from ggems_b200 import abi
 
 
+def reference_dir():
+    """The GGEMS checkout the oracle pin is built from (oracle/build.py's
+    choice: $GGEMS_REFERENCE_DIR or its default), or None when absent."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("oracle_build", os.path.join(scenes.ROOT, "oracle", "build.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.reference_dir()
+
+
 def slots_used(n):
     """Slots a run of n primaries fills (GGEMSSource::OrganizeParticlesInBatch:
     ceil(n / 2^20) batches, the first n mod batches of them one particle larger).

@@ -469,6 +469,23 @@ def cbct_scene(n=256, voxel=1.0, elements=(512, 512, 1), element_size=(0.8, 0.8,
     return sc
 
 
+def cbct_api_scene(n=256, voxel=1.0, seed=1, aperture_deg=11.0):
+    """The CBCT projection exactly as the GGEMS-API configuration builds it
+    (phantom rotation then position calls, detector rotation call; 120 kVp
+    spectrum through its file format; source at (-1000, 0, 0) mm): (scene,
+    source).  tests/test_host_api.py checks it field by field against the
+    scene the API prepares."""
+    from ggems_b200 import workloads
+    sc = Scene()
+    t = sc.add_tables(Tables(["Air", "Water", "Bone185"]))
+    sc.add_voxelized(workloads.cbct_labels(n, voxel, seed), (voxel, voxel, voxel), t,
+                     ops=[("rotation", (0.0, 0.0, 0.0)), ("translation", (0.0, 0.0, 0.0))])
+    td = sc.add_tables(Tables(["GOS"]))
+    sc.add_flat_detector(td, (512, 512, 1), (0.8, 0.8, 10.0), 1500.0, 1000.0, F(10.0) * KEV,
+                         extra_rotation=(0.0, 0.0, 0.0))
+    return sc, XRaySource(spectrum=synthetic_spectrum(), aperture_deg=aperture_deg)
+
+
 _libm.asinf.restype = C.c_float
 _libm.asinf.argtypes = [C.c_float]
 _libm.sqrtf.restype = C.c_float

@@ -42,13 +42,7 @@ def test_cbct_scene_matches_restatement(tmp_path):
         from ggems_b200.api import lib
         lib.ggems_host_scene.restype = C.POINTER(abi.gg_scene)
         sc = lib.ggems_host_scene().contents
-        ref = scenes.Scene()
-        t = ref.add_tables(scenes.Tables(["Air", "Water", "Bone185"]))
-        ref.add_voxelized(workloads.cbct_labels(64, 4.0, 5), (4.0, 4.0, 4.0), t,
-                          ops=[("rotation", (0.0, 0.0, 0.0)), ("translation", (0.0, 0.0, 0.0))])
-        td = ref.add_tables(scenes.Tables(["GOS"]))
-        ref.add_flat_detector(td, (512, 512, 1), (0.8, 0.8, 10.0), 1500.0, 1000.0, np.float32(10.0) * np.float32(1e-3),
-                              extra_rotation=(0.0, 0.0, 0.0))
+        ref, rsrc = scenes.cbct_api_scene(64, 4.0, 5)
         rs = ref.struct()
         assert sc.number_of_solids == 2 and sc.number_of_tables == 2 and sc.number_of_histograms == 2
         for i in range(2):
@@ -72,7 +66,6 @@ def test_cbct_scene_matches_restatement(tmp_path):
                 assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), (i, f)
         src = abi.gg_source()
         assert lib.ggems_source_descriptor(0, C.byref(src), None) == 0
-        rsrc = scenes.XRaySource(spectrum=scenes.synthetic_spectrum(), aperture_deg=11.0)
         assert np.array_equal(np.array(src.matrix, np.float32), rsrc.matrix.reshape(-1))
         assert np.float32(src.beam_aperture) == np.float32(rsrc.struct.beam_aperture)
         m = src.number_of_energy_bins + 1

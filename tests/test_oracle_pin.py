@@ -23,7 +23,7 @@ REF = os.path.join(scenes.ROOT, "oracle", "_ref", "libgg_ref.so")
 
 def _ref_lib():
     if not os.path.exists(REF):
-        if os.path.isdir("/root/reference/src/kernels"):
+        if parity.reference_dir():
             import subprocess
             import sys
             subprocess.check_call([sys.executable, os.path.join(scenes.ROOT, "oracle", "build.py")])
