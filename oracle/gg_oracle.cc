@@ -13,6 +13,7 @@
 // The restatement is pinned against the reference's own kernels, compiled
 // from the reference checkout through oracle/ref_shim (oracle/_ref), by
 // tests/test_oracle_pin.py.
+#include <algorithm>
 #include <atomic>
 #include <cfloat>
 #include <cmath>
@@ -230,6 +231,34 @@ void atomic_add_double(double* addr, double v) {
   }
 }
 void atomic_add_int(int32_t* addr, int32_t v) { __atomic_fetch_add(addr, v, __ATOMIC_RELAXED); }
+
+// Squared-count tallies of the detector histograms (statistical tests only):
+// when registered, every history's increments are collected per (histogram,
+// bin) and k^2 is added for each bin the history counted k times in, so that
+// sum k^2 - (sum k)^2 / n estimates each bin's variance over n primaries.  A
+// primary can count more than once in one bin (a Compton site then a
+// photoelectric site in the same detector element), so the bins are not
+// Poisson.  Not part of the reference's algorithm; off by default.
+int64_t* const* g_histogram_squares = nullptr;
+thread_local std::vector<std::pair<int, int>> t_history_counts;
+
+void record_histogram(int histogram, int index) {
+  if (g_histogram_squares && g_histogram_squares[histogram]) t_history_counts.emplace_back(histogram, index);
+}
+
+void flush_history_counts() {
+  auto& v = t_history_counts;
+  if (v.empty()) return;
+  std::sort(v.begin(), v.end());
+  for (size_t i = 0; i < v.size();) {
+    size_t j = i;
+    while (j < v.size() && v[j] == v[i]) ++j;
+    const int64_t k = static_cast<int64_t>(j - i);
+    __atomic_fetch_add(&g_histogram_squares[v[i].first][v[i].second], k * k, __ATOMIC_RELAXED);
+    i = j;
+  }
+  v.clear();
+}
 
 // dose_record_standard / dose_photon_tracking (GGEMSDoseRecording.hh:65-118).
 bool dosel_index(const gg_dose_map& dm, V3 p, int* gid) {
@@ -646,9 +675,14 @@ void track_box(Photon& ph, Kiss& rng, const gg_scene& sc, const gg_solid& s, int
         int ix = static_cast<int>(q.x), iy = static_cast<int>(q.y);
         int index = ix + iy * vx;
         ++t_counts[3];
-        if (t.out->histograms && t.out->histograms[s.histogram]) atomic_add_int(&t.out->histograms[s.histogram][index], 1);
-        if (s.scatter_histogram >= 0 && ph.scatter == 1 && t.out->histograms && t.out->histograms[s.scatter_histogram])
+        if (t.out->histograms && t.out->histograms[s.histogram]) {
+          atomic_add_int(&t.out->histograms[s.histogram][index], 1);
+          record_histogram(s.histogram, index);
+        }
+        if (s.scatter_histogram >= 0 && ph.scatter == 1 && t.out->histograms && t.out->histograms[s.scatter_histogram]) {
           atomic_add_int(&t.out->histograms[s.scatter_histogram][index], 1);
+          record_histogram(s.scatter_histogram, index);
+        }
       }
     }
   } while (ph.status == GG_ALIVE);
@@ -881,6 +915,13 @@ __attribute__((visibility("default"))) void gg_oracle_counts(uint64_t* out, int 
   }
 }
 
+// Register (or, with NULL, drop) the squared-count tallies of the detector
+// histograms: one int64 array per histogram of the scene (NULL entries skip a
+// histogram), summed into by every following run.
+__attribute__((visibility("default"))) void gg_oracle_set_histogram_squares(int64_t* const* squares) {
+  g_histogram_squares = squares;
+}
+
 // Register the Rayleigh form-factor fit tables PP0..PP8 (101 floats each).
 __attribute__((visibility("default"))) void gg_oracle_set_rayleigh_fit(const float* const* pp) {
   for (int i = 0; i < 9; ++i) g_rayleigh_fit.pp[i] = pp[i];
@@ -926,6 +967,7 @@ __attribute__((visibility("default"))) int gg_oracle_run(const gg_scene* scene, 
         if (source->type == GG_SOURCE_XRAY) xray_primary(ph, rng, *source);
         else voxelized_primary(ph, rng, *source);
         transport(ph, rng, *scene, t);
+        flush_history_counts();
       }
       random_states[slot] = rng.s1;
       random_states[S + slot] = rng.s2;

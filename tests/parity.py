@@ -134,3 +134,53 @@ def z_scores(a, b, var_a, var_b):
     with np.errstate(divide="ignore", invalid="ignore"):
         z = np.where(v > 0, (a - b) / np.sqrt(v), 0.0)
     return z
+
+
+def mean_z(sum_a, sq_a, n_a, sum_b, sq_b, n_b):
+    """Per-bin z of two independent tallies of a per-primary score, compared as
+    means per primary: sum = sum of the scores in the bin, sq = sum of their
+    squares (the E^2 tally), n = primaries.  Var(sum) is estimated as
+    sq - sum^2 / n (the scores of one bin are taken as one score per primary)."""
+    sum_a, sum_b = np.asarray(sum_a, np.float64), np.asarray(sum_b, np.float64)
+    va = np.maximum(np.asarray(sq_a, np.float64) - sum_a ** 2 / n_a, 0.0) / float(n_a) ** 2
+    vb = np.maximum(np.asarray(sq_b, np.float64) - sum_b ** 2 / n_b, 0.0) / float(n_b) ** 2
+    return z_scores(sum_a / n_a, sum_b / n_b, va, vb)
+
+
+def run_oracle_squares(sc, src, n, seed=777):
+    """run_oracle plus the squared-count tally of every detector histogram:
+    (tallies, [sum over primaries of k^2 per bin, one int64 array per histogram])."""
+    sq = [np.zeros(h, np.int64) for h in sc.histogram_sizes]
+    ptrs = (C.POINTER(C.c_int64) * max(len(sq), 1))(*[abi.ptr(a, C.c_int64) for a in sq])
+    lib = scenes.oracle()
+    lib.gg_oracle_set_histogram_squares.argtypes = [C.c_void_p]
+    lib.gg_oracle_set_histogram_squares(C.cast(ptrs, C.c_void_p))
+    try:
+        _, T, _ = run_oracle(sc, src, n, seed=seed)
+    finally:
+        lib.gg_oracle_set_histogram_squares(None)
+    return T, sq
+
+
+def count_z_var(a, n_a, b, n_b, sq_b):
+    """Per-bin z of two independent count histograms compared per primary, with
+    each bin's variance per primary estimated from the second histogram's
+    squared-count tally (sq_b = sum of k^2 over its primaries):
+    s^2 = sq_b / n_b - (b / n_b)^2, bounded below by the pooled rate (a count
+    made of whole counts per primary has variance >= mean)."""
+    a, b, sq_b = np.asarray(a, np.float64), np.asarray(b, np.float64), np.asarray(sq_b, np.float64)
+    s2 = sq_b / n_b - (b / n_b) ** 2
+    p = (a + b) / (n_a + n_b)
+    v = np.maximum(s2, p) * (1.0 / n_a + 1.0 / n_b)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return np.where(v > 0, (a / n_a - b / n_b) / np.sqrt(v), 0.0)
+
+
+def count_z(a, n_a, b, n_b):
+    """Per-bin z of two independent count histograms (Poisson), compared per
+    primary with the pooled rate: p = (a + b) / (n_a + n_b), Var = p (1/n_a + 1/n_b)."""
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    p = (a + b) / (n_a + n_b)
+    v = p * (1.0 / n_a + 1.0 / n_b)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return np.where(v > 0, (a / n_a - b / n_b) / np.sqrt(v), 0.0)

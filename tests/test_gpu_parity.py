@@ -9,6 +9,10 @@ bits of a direction and can occasionally flip a later comparison.  The bar:
 >= 99.9 % of random streams identical at the end (same number of draws), and
 tallies statistically identical (|z| < 3 in >= 99.7 % of bins, totals within
 0.5 %).  The bit-exact fraction is reported (about 0.9 for the water case).
+Runs that share their random streams agree far more closely than independent
+estimates would, so the tally z-tests here are consistency checks; the
+statistical criterion proper, on independent streams, and the parity checks at
+each configuration's full size are in tests/test_gpu_at_size.py.
 """
 
 import numpy as np
