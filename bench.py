@@ -969,8 +969,9 @@ def run_reference_arm(args, rank, world):
     GGEMS's own kernels built for the host (oracle/_ref) when available, else
     the oracle port, replaying GGEMS::RunOnDevice batch by batch.  The scene,
     tables and random streams come from the oracle side (tests/scenes.py:
-    the oracle's table builder, GGEMS's mt19937 seeding), so nothing of the
-    product library is loaded.  Each step is a bounded sample of the projection
+    GGEMS's own host table builders, oracle/_ref/libgg_ref_tables.so, else the
+    oracle's restatement; GGEMS's mt19937 seeding), so nothing of the product
+    library is loaded.  Each step is a bounded sample of the projection
     (its first whole batches, the same slots and streams as the projection);
     `config` is the product arm's."""
     if rank != 0:
@@ -979,7 +980,9 @@ def run_reference_arm(args, rank, world):
     kind = _cpu_kind()
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import scenes
-    scene, source = scenes.cbct_api_scene(256, 1.0, seed=1)
+    # tables from GGEMS's own host code when it was built here (bit-identical to the oracle's)
+    builder = "reference" if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libgg_ref_tables.so")) else "oracle"
+    scene, source = scenes.cbct_api_scene(256, 1.0, seed=1, builder=builder)
     ss = scene.struct()
     scene_ptr = C.pointer(ss)
     src = source.struct

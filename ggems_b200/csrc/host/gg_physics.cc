@@ -339,6 +339,11 @@ void build_attenuations(NavigatorTables& t, const MaterialsDatabase& db) {
   const PhysicsData& pd = physics_data();
   const int32_t* rows_of = pd.get<int32_t>("mu_nb_energy_bins");
   const int32_t* first_row = pd.get<int32_t>("mu_index_energy");
+  // GGEMSMuDataConstants has rows for Z = 1..92 only (kMuNbElements); GGEMS
+  // reads past the end of its tables for heavier elements (undefined values).
+  // Here such elements add nothing to mu and mu_en, which only the TLE dose
+  // mode reads.
+  const int max_z = static_cast<int>(pd.count("mu_index_energy", 4)) - 1;
   const float* raw = pd.get<float>("mu_data");
   const size_t n_rows = pd.count("mu_data", 4) / 3;
   std::vector<float> e(n_rows), mu(n_rows), mu_en(n_rows);
@@ -365,6 +370,7 @@ void build_attenuations(NavigatorTables& t, const MaterialsDatabase& db) {
       float a = 0.0f, b = 0.0f;
       for (size_t k = 0; k < mat.element_names.size(); ++k) {
         const int Z = db.element(mat.element_names[k]).Z;
+        if (Z > max_z) continue;
         const float w = mat.fractions[k];
         // bisection over rows [0, first_row[Z] + rows_of[Z]) (GGEMSMathAlgorithms.hh BinarySearch)
         int left = 0, right = first_row[Z] + rows_of[Z] - 1, row = -1;
@@ -378,6 +384,13 @@ void build_attenuations(NavigatorTables& t, const MaterialsDatabase& db) {
         if (row == first_row[Z]) {
           a += mu[row];
           b += mu_en[row];
+        } else if (row == 0) {
+          // GGEMS interpolates from the row before the table here (row -1, an
+          // out-of-range read); the energy is at or above row 0's (the bins
+          // start at the table's first energy), where LinearInterpolation
+          // returns row 0's value whatever the row before holds.
+          a += w * mu[0];
+          b += w * mu_en[0];
         } else {
           a += w * lerp_table(e[row - 1], mu[row - 1], e[row], mu[row], energy);
           b += w * lerp_table(e[row - 1], mu_en[row - 1], e[row], mu_en[row], energy);

@@ -100,12 +100,54 @@ def build_ref(reference):
     return out
 
 
+# GGEMS's host sources the table pin compiles (material database, material
+# tables and range cuts, cross sections and the three per-atom formulas,
+# attenuations, and the text reader / printing / exception helpers they call).
+REF_HOST_SOURCES = [
+    "src/materials/GGEMSMaterialsDatabaseManager.cc", "src/materials/GGEMSMaterials.cc",
+    "src/materials/GGEMSIonizationParamsMaterial.cc", "src/physics/GGEMSCrossSections.cc",
+    "src/physics/GGEMSEMProcess.cc", "src/physics/GGEMSComptonScattering.cc",
+    "src/physics/GGEMSPhotoElectricEffect.cc", "src/physics/GGEMSRayleighScattering.cc",
+    "src/physics/GGEMSRangeCuts.cc", "src/physics/GGEMSLogEnergyTable.cc", "src/physics/GGEMSProcessesManager.cc",
+    "src/physics/GGEMSAttenuations.cc", "src/io/GGEMSTextReader.cc", "src/tools/GGEMSPrint.cc",
+    "src/tools/GGEMSTools.cc",
+]
+
+
+def build_ref_tables(reference, extra_flags=(), name="libgg_ref_tables.so"):
+    """GGEMS's host table builders, compiled unmodified from the checkout with
+    oracle/ref_host (a host stand-in for the OpenCL header and the few
+    GGEMSOpenCLManager members they call) into oracle/_ref/<name>."""
+    if not os.path.isdir(os.path.join(reference, "src", "physics")):
+        return None
+    os.makedirs(REF_OUT, exist_ok=True)
+    host = os.path.join(HERE, "ref_host")
+    common = ["g++", "-std=c++17", "-O2", "-fPIC", "-w"] + list(extra_flags) + [
+        "-I" + host, "-I" + os.path.join(HERE, "ref_shim"), "-I" + os.path.join(reference, "include")]
+    if not extra_flags:
+        common += ["-ffp-contract=off", "-fno-fast-math"]
+    tag = os.path.splitext(name)[0]
+    objs = []
+    for src in REF_HOST_SOURCES + [os.path.join(host, "gg_ref_tables.cc")]:
+        path = src if os.path.isabs(src) else os.path.join(reference, src)
+        obj = os.path.join(REF_OUT, "%s_%s.o" % (tag, os.path.splitext(os.path.basename(path))[0]))
+        run(common + ["-c", path, "-o", obj])
+        objs.append(obj)
+    out = os.path.join(REF_OUT, name)
+    run(["g++", "-shared", "-o", out] + objs + ["-lpthread"])
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=DEFAULT_REFERENCE)
     args = ap.parse_args()
     print(build_oracle())
     print(build_ref(args.ref))
+    print(build_ref_tables(args.ref))
+    # the same sources with the reference's own release flags (CMakeLists.txt:163-164):
+    # -O3 -march=native lets g++ contract a*b+c into FMA on hosts that have it
+    print(build_ref_tables(args.ref, ("-O3", "-march=native"), "libgg_ref_tables_native.so"))
 
 
 if __name__ == "__main__":

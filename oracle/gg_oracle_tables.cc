@@ -465,6 +465,7 @@ __attribute__((visibility("default"))) int gg_oracle_build_attenuations(
       float mu_over_rho = 0.0f, mu_en_over_rho = 0.0f;
       for (size_t k = 0; k < mat.elements.size(); ++k) {
         const int Z = z_of.at(mat.elements[k]);
+        if (Z > n_elem_tables) continue;  // no mu data beyond Z = 92 (GGEMS reads past its table)
         const float frac = mat.fractions[k];
         const int first = index_energy[Z];
         int low = 0, high = first + nb_bins[Z] - 1;  // BinarySearch (GGEMSMathAlgorithms.hh:46-63)
@@ -484,6 +485,11 @@ __attribute__((visibility("default"))) int gg_oracle_build_attenuations(
         if (e_index == first) {
           mu_over_rho += mu_t[e_index];
           mu_en_over_rho += mu_en_t[e_index];
+        } else if (e_index == 0) {
+          // the reference reads the row before its table here; LinearInterpolation
+          // then returns row 0's value (x >= its energy)
+          mu_over_rho += frac * mu_t[0];
+          mu_en_over_rho += frac * mu_en_t[0];
         } else {
           mu_over_rho += frac * lerp(energies[e_index - 1], mu_t[e_index - 1], energies[e_index], mu_t[e_index], energy);
           mu_en_over_rho +=

@@ -147,7 +147,10 @@ class Tables:
     """One navigator's physics tables (oracle restatement of the host builders)."""
 
     def __init__(self, materials, number_of_bins=220, min_energy=1.0 * KEV, max_energy=1.0 * MEV,
-                 processes=(0, 1, 2), photon_cut=0.1, materials_file=MATERIALS):
+                 processes=(0, 1, 2), photon_cut=0.1, materials_file=MATERIALS, builder="oracle"):
+        """builder: "oracle" (the restatement) or "reference" (GGEMS's own host
+        code, oracle/_ref/libgg_ref_tables.so; bit-identical, see
+        tests/test_tables.py) for the material and cross-section tables."""
         lib = oracle()
         nm, nb = len(materials), number_of_bins
         self.materials = list(materials)
@@ -163,8 +166,12 @@ class Tables:
         total = C.c_int32(0)
         names = (C.c_char_p * nm)(*[m.encode() for m in materials])
         procs = (C.c_int * 3)(*processes)
-        lib.gg_oracle_build_tables.restype = C.c_int
-        rc = lib.gg_oracle_build_tables(
+        if builder == "reference":
+            ref = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libgg_ref_tables.so"))
+            build = lambda *a: ref.gg_ref_build_tables(a[0], *a[2:])  # noqa: E731  (no physics-data file)
+        else:
+            build = lib.gg_oracle_build_tables
+        rc = build(
             MATERIALS.encode() if materials_file is None else materials_file.encode(), PHYSICS.encode(), names, nm, nb,
             C.c_float(min_energy), C.c_float(max_energy), procs, len(processes), C.c_float(photon_cut),
             abi.ptr(self.energy_bins, C.c_float), abi.ptr(self.cross_sections, C.c_float),
@@ -469,7 +476,7 @@ def cbct_scene(n=256, voxel=1.0, elements=(512, 512, 1), element_size=(0.8, 0.8,
     return sc
 
 
-def cbct_api_scene(n=256, voxel=1.0, seed=1, aperture_deg=11.0):
+def cbct_api_scene(n=256, voxel=1.0, seed=1, aperture_deg=11.0, builder="oracle"):
     """The CBCT projection exactly as the GGEMS-API configuration builds it
     (phantom rotation then position calls, detector rotation call; 120 kVp
     spectrum through its file format; source at (-1000, 0, 0) mm): (scene,
@@ -477,10 +484,10 @@ def cbct_api_scene(n=256, voxel=1.0, seed=1, aperture_deg=11.0):
     scene the API prepares."""
     from ggems_b200 import workloads
     sc = Scene()
-    t = sc.add_tables(Tables(["Air", "Water", "Bone185"]))
+    t = sc.add_tables(Tables(["Air", "Water", "Bone185"], builder=builder))
     sc.add_voxelized(workloads.cbct_labels(n, voxel, seed), (voxel, voxel, voxel), t,
                      ops=[("rotation", (0.0, 0.0, 0.0)), ("translation", (0.0, 0.0, 0.0))])
-    td = sc.add_tables(Tables(["GOS"]))
+    td = sc.add_tables(Tables(["GOS"], builder=builder))
     sc.add_flat_detector(td, (512, 512, 1), (0.8, 0.8, 10.0), 1500.0, 1000.0, F(10.0) * KEV,
                          extra_rotation=(0.0, 0.0, 0.0))
     return sc, XRaySource(spectrum=synthetic_spectrum(), aperture_deg=aperture_deg)

@@ -139,3 +139,185 @@ def test_attenuation_tables_bit_exact(materials, tmp_path):
     ref_mu_en = o.mu_en.reshape(nm, -1)[:, :keep]
     assert np.array_equal(mu.view(np.uint32), ref_mu.view(np.uint32))
     assert np.array_equal(mu_en.view(np.uint32), ref_mu_en.view(np.uint32))
+
+
+# ---- pin against GGEMS's own host code ----
+#
+# oracle/_ref/libgg_ref_tables.so is GGEMS's table-building host code
+# (GGEMSMaterialsDatabaseManager, GGEMSMaterials + GGEMSRangeCuts,
+# GGEMSCrossSections + GGEMSEMProcess and the Compton / photoelectric / Rayleigh
+# per-atom formulas, GGEMSAttenuations) compiled unmodified from the reference
+# checkout by oracle/build.py, with the same floating-point contract as the
+# product's host build (-ffp-contract=off).  Skipped where the checkout is not
+# available.
+
+REF_TABLES = scenes.os.path.join(scenes.ROOT, "oracle", "_ref", "libgg_ref_tables.so")
+REF_TABLES_NATIVE = scenes.os.path.join(scenes.ROOT, "oracle", "_ref", "libgg_ref_tables_native.so")
+TABLE_KEYS = ("energy_bins", "cross_sections", "rayleigh", "density", "photon_cut", "n_elements", "offset", "Z",
+              "atom_density")
+
+
+def _ref_tables_lib(path=REF_TABLES):
+    import parity
+    if not scenes.os.path.exists(path):
+        if parity.reference_dir() is None:
+            pytest.skip("reference checkout not available")
+        import subprocess
+        import sys
+        subprocess.check_call([sys.executable, scenes.os.path.join(scenes.ROOT, "oracle", "build.py")])
+    lib = C.CDLL(path)
+    lib.gg_ref_tables_error.restype = C.c_char_p
+    return lib
+
+
+def _table_arrays(nm, nb):
+    return dict(energy_bins=np.zeros(nb, np.float32), cross_sections=np.zeros(3 * nm * nb, np.float32),
+                rayleigh=np.zeros(101 * nb, np.float32), density=np.zeros(nm, np.float32),
+                photon_cut=np.zeros(nm, np.float32), n_elements=np.zeros(nm, np.int32),
+                offset=np.zeros(nm, np.int32), Z=np.zeros(nm * 32, np.uint8), atom_density=np.zeros(nm * 32, np.float32))
+
+
+def _ctype(a):
+    return {np.float32: C.c_float, np.int32: C.c_int32, np.uint8: C.c_uint8}[a.dtype.type]
+
+
+def _reference_tables(lib, materials_file, materials, nb, emin, emax, procs, cut):
+    nm = len(materials)
+    out = _table_arrays(nm, nb)
+    total = C.c_int32()
+    names = (C.c_char_p * nm)(*[m.encode() for m in materials])
+    p = (C.c_int * 3)(*procs)
+    rc = lib.gg_ref_build_tables(materials_file.encode(), names, nm, nb, C.c_float(emin), C.c_float(emax), p,
+                                 len(procs), C.c_float(cut), *[abi.ptr(out[k], _ctype(out[k])) for k in TABLE_KEYS],
+                                 C.byref(total))
+    assert rc == 0, lib.gg_ref_tables_error()
+    out["total"] = total.value
+    return out
+
+
+def _assert_same_tables(a, b, procs):
+    t = b["total"]
+    assert a["total"] == t
+    for k in ("energy_bins", "cross_sections", "density", "photon_cut"):
+        assert np.array_equal(a[k].view(np.uint32), b[k].view(np.uint32)), k
+    if 2 in procs:
+        assert np.array_equal(a["rayleigh"].view(np.uint32), b["rayleigh"].view(np.uint32))
+    for k in ("n_elements", "offset"):
+        assert np.array_equal(a[k], b[k]), k
+    assert np.array_equal(a["Z"][:t], b["Z"][:t])
+    assert np.array_equal(a["atom_density"][:t].view(np.uint32), b["atom_density"][:t].view(np.uint32))
+
+
+@pytest.mark.parametrize("materials,nb,emin,emax,procs,cut", CASES)
+def test_tables_match_reference_host_code(materials, nb, emin, emax, procs, cut):
+    """Energy bins, per-material and Rayleigh per-atom cross sections, densities,
+    photon energy cuts and element tables: the product's builder and the
+    oracle's restatement against GGEMS's own host code, bit for bit."""
+    ref = _reference_tables(_ref_tables_lib(), scenes.MATERIALS, materials, nb, np.float32(emin), np.float32(emax),
+                            procs, cut)
+    prod = _product_tables(materials, nb, np.float32(emin), np.float32(emax), procs, cut)
+    _assert_same_tables(prod, ref, procs)
+    o = scenes.Tables(materials, number_of_bins=nb, min_energy=emin, max_energy=emax, processes=procs, photon_cut=cut)
+    orc = dict(energy_bins=o.energy_bins, cross_sections=o.cross_sections, rayleigh=o.rayleigh, density=o.density,
+               photon_cut=o.photon_cut, n_elements=o.n_elements, offset=o.offset, Z=o.Z, atom_density=o.atom_density,
+               total=o.total)
+    _assert_same_tables(orc, ref, procs)
+
+
+@pytest.mark.parametrize("materials", [["Water"], ["Air", "Water", "Bone185"], ["GOS", "Aluminium", "RibBone"]])
+def test_attenuation_tables_match_reference_host_code(materials):
+    """mu and mu_en (GGEMSAttenuations::Initialize) of the oracle's restatement,
+    which the product's builder equals (test_attenuation_tables_bit_exact),
+    against GGEMS's own host code, bit for bit."""
+    lib = _ref_tables_lib()
+    nm = len(materials)
+    bins = np.zeros(abi.GG_ATTENUATION_BINS, np.float32)
+    mu = np.zeros(nm * abi.GG_ATTENUATION_BINS, np.float32)
+    mu_en = np.zeros_like(mu)
+    names = (C.c_char_p * nm)(*[m.encode() for m in materials])
+    rc = lib.gg_ref_build_attenuations(scenes.MATERIALS.encode(), names, nm, abi.ptr(bins, C.c_float),
+                                       abi.ptr(mu, C.c_float), abi.ptr(mu_en, C.c_float))
+    assert rc == 0, lib.gg_ref_tables_error()
+    o = scenes.Tables(materials)
+    assert np.array_equal(bins.view(np.uint32), o.attenuation_energy_bins.view(np.uint32))
+    assert np.array_equal(mu.view(np.uint32), o.mu.view(np.uint32))
+    assert np.array_equal(mu_en.view(np.uint32), o.mu_en.view(np.uint32))
+
+
+def test_every_reference_material_matches_reference_host_code(tmp_path):
+    """Every material of the reference's own database (data/materials.txt, 169
+    entries): the product's builder against GGEMS's host code, bit for bit, 220
+    bins from 1 keV to 1 MeV, the three processes, a 0.7 mm photon cut; and the
+    mu / mu_en tables of every material whose elements have mu data (GGEMS's
+    tables stop at Z = 92 and it reads past them for heavier elements).  Run in
+    a fresh process: both material databases are process-wide."""
+    import os
+    import subprocess
+    import sys
+    import textwrap
+    import parity
+    ref = parity.reference_dir()
+    if ref is None:
+        pytest.skip("reference checkout not available")
+    _ref_tables_lib()
+    db = os.path.join(ref, "data", "materials.txt")
+    code = textwrap.dedent(r'''
+        import re, sys
+        import numpy as np
+        import test_tables as T
+        db = sys.argv[1]
+        names = [m.group(1) for m in re.finditer(r"^([A-Za-z0-9_+\-]+):\s*d=", open(db).read(), re.M)]
+        assert len(names) > 100, len(names)
+        lib = T._ref_tables_lib()
+        T.scenes.MATERIALS = db
+        import ctypes as C
+        from ggems_b200 import abi
+        checked_mu = 0
+        for i in range(0, len(names), 64):
+            chunk = names[i:i + 64]
+            args = (chunk, 220, np.float32(1e-3), np.float32(1.0), (0, 1, 2), 0.7)
+            ref = T._reference_tables(lib, db, *args)
+            T._assert_same_tables(T._product_tables(*args), ref, (0, 1, 2))
+            # mu / mu_en: the oracle's restatement (equal to the product's builder) against
+            # GGEMS's, for materials whose elements all have mu data (Z <= 92; GGEMS's
+            # own builder reads past its tables, and can fault, for heavier ones)
+            ok = [m for j, m in enumerate(chunk)
+                  if ref["Z"][ref["offset"][j]:ref["offset"][j] + ref["n_elements"][j]].max() <= 92]
+            nm = len(ok)
+            bins = np.zeros(abi.GG_ATTENUATION_BINS, np.float32)
+            mu = np.zeros(nm * abi.GG_ATTENUATION_BINS, np.float32)
+            mu_en = np.zeros_like(mu)
+            cn = (C.c_char_p * nm)(*[m.encode() for m in ok])
+            assert lib.gg_ref_build_attenuations(db.encode(), cn, nm, abi.ptr(bins, C.c_float), abi.ptr(mu, C.c_float),
+                                                 abi.ptr(mu_en, C.c_float)) == 0
+            o = T.scenes.Tables(ok, photon_cut=0.7, materials_file=db)
+            assert np.array_equal(mu.view(np.uint32), o.mu.view(np.uint32))
+            assert np.array_equal(mu_en.view(np.uint32), o.mu_en.view(np.uint32))
+            checked_mu += nm
+        print("materials", len(names), "with mu / mu_en", checked_mu)
+    ''')
+    (tmp_path / "case.py").write_text(code)
+    env = dict(os.environ, PYTHONPATH=os.pathsep.join([scenes.ROOT, os.path.join(scenes.ROOT, "tests")]))
+    out = subprocess.run([sys.executable, "case.py", db], capture_output=True, text=True, env=env, cwd=str(tmp_path),
+                         timeout=600)
+    assert out.returncode == 0, out.stdout + out.stderr
+    print(out.stdout.strip())
+
+
+def test_reference_release_build_differs_only_by_contraction():
+    """The same reference host code built with the reference's release flags
+    (-O3 -march=native, CMakeLists.txt:163-164): on a host with FMA, g++ then
+    contracts a*b+c in the per-atom fits, so its tables can differ from the
+    as-written arithmetic in the last bits.  Measured: a few hundred cross
+    sections per material set, at most ~4e-6 relative; everything else equal."""
+    lib = _ref_tables_lib(REF_TABLES_NATIVE)
+    worst = 0.0
+    for materials, nb, emin, emax, procs, cut in CASES:
+        a = _reference_tables(lib, scenes.MATERIALS, materials, nb, np.float32(emin), np.float32(emax), procs, cut)
+        b = _product_tables(materials, nb, np.float32(emin), np.float32(emax), procs, cut)
+        for k in ("energy_bins", "density", "photon_cut", "n_elements", "offset", "Z"):
+            assert np.array_equal(a[k], b[k]), k
+        x, y = a["cross_sections"].astype(np.float64), b["cross_sections"].astype(np.float64)
+        worst = max(worst, float((np.abs(x - y) / np.maximum(np.abs(y), 1e-30)).max()))
+    print("release-flag build: largest relative cross-section difference %.1e" % worst)
+    assert worst < 1e-5
