@@ -275,6 +275,43 @@ def _cbct_sample(scene_ptr, source, threads, kind, budget_s, states, primaries=P
     return k, sum(sizes[:k])
 
 
+SURROGATE_NET = os.path.join(ROOT, "ggems_b200", "data", "unet_scatter256.npz")
+
+
+def surrogate_measurement(tmp, angles=360, reference_every=10):
+    """The second metric: scatter projections/s of the learned surrogate (the
+    committed trained network + the 1e6-primary plain-MC judge, as specified)
+    against plain MC at <= 5 % error, on a 360-angle CBCT scan of a new phantom,
+    errors against 1e9-primary references on every `reference_every`-th angle.
+    Run by ggems_b200.scatter in a process of its own (the GGEMS API's managers
+    are process-wide).  Returns the summary dict, or None without the network."""
+    if not os.path.exists(SURROGATE_NET):
+        return None
+    out = os.path.join(tmp, "surrogate.json")
+    cmd = [sys.executable, "-m", "ggems_b200.scatter", "--load", SURROGATE_NET, "--test", "0", "--angles",
+           str(angles), "--reference-every", str(reference_every), "--json-out", out]
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=1200)
+    if r.returncode != 0:
+        return {"error": (r.stdout + r.stderr)[-800:]}
+    d = json.load(open(out))
+    scan, plain = d["scan"], d["plain_mc"]
+    return {"metric": d["metric"], "value": d["value"], "unit": "projections/s",
+            "plain_mc_projections_per_s": {k: plain[k]["projections_per_s"] for k in ("blocks16", "full")},
+            "speedup_vs_plain_mc": {k: plain[k]["speedup"] for k in ("blocks16", "full")},
+            "plain_mc_primaries_for_5pct": {k: plain[k]["primaries_for_5pct"] for k in ("blocks16", "full")},
+            "plain_mc_error_blocks16": plain["blocks16"]["error_mean"],
+            "plain_mc_primaries_per_s": plain["mc_primaries_per_s"],
+            "error": scan["error"], "network_error": scan["network_error"], "judge_mc_error": scan["judge_mc_error"],
+            "network_kept": scan["network_kept"], "replaced_by_mc": scan["replaced_by_mc"],
+            "judge": d["judge"], "with_rescaling": d["with_rescaling"],
+            "integrated_scatter_error": d["integrated_scatter_error"],
+            "scan": {"angles": scan["angles"], "seconds": scan["seconds"], "reference_angles": scan["reference_angles"],
+                     "ms_per_projection": scan["ms_per_projection"]},
+            "errors": d["errors"], "network": os.path.basename(SURROGATE_NET),
+            "config": {"phantom": "64^3 x 2 mm random water/bone/air, 60 keV, 256^2 panel", "judge_primaries": 1e6,
+                       "reference_primaries": 1e9, "training": "2000 MC pairs at 1e8 primaries, 60 epochs"}}
+
+
 def _cbct_config(primaries, batches, world):
     """The workload both arms report (same dict on the product and the reference arm)."""
     return {"workload": WORKLOAD, "phantom": "256x256x256 uint8, 1 mm, air/water/bone(1.85)",
@@ -295,10 +332,13 @@ def main():
     ap.add_argument("--primaries", type=int, default=PRIMARIES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
-    ap.add_argument("--workload", default="cbct", choices=["cbct", "water", "batched", "mesh", "volume", "curved"],
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-surrogate measurement")
+    ap.add_argument("--workload", default="cbct",
+                    choices=["cbct", "water", "batched", "mesh", "volume", "curved", "surrogate"],
                     help="cbct: the CBCT projection (default); water: 64^3 water dosimetry, 1e6 primaries; "
                          "batched: 360 angles + 16 phantoms in one launch; mesh: meshed-phantom dosimetry; "
-                         "volume: CT image -> material labels on the device")
+                         "volume: CT image -> material labels on the device; surrogate: learned scatter "
+                         "projections/s vs plain MC (also part of the cbct line)")
     ap.add_argument("--mesh-subdivisions", type=int, default=6, help="icosphere subdivisions of the mesh body")
     ap.add_argument("--primaries-per-job", type=int, default=10_000_000)
     args = ap.parse_args()
@@ -323,6 +363,10 @@ def main():
         return run_water(args, tmp, rank)
     if args.workload == "curved":
         return run_curved(args, tmp, rank)
+    if args.workload == "surrogate":
+        if rank == 0:
+            print(json.dumps(surrogate_measurement(tmp) or {"unavailable": "no trained network"}), flush=True)
+        return 0
 
     import torch
     dist = None
@@ -412,9 +456,9 @@ def main():
         check(lib.gg_upload_scene(ctx, scene_ptr), "gg_upload_scene")
         check(lib.gg_set_random_states(ctx, abi.ptr(states, C.c_uint32), abi.GG_MAXIMUM_PARTICLES), "random states")
         step()
+        if world > 1:  # the run's one exchange: sum the device tallies over ranks (NCCL, in place, exact)
+            distributed.reduce_device_tallies(ctx)
         check(lib.gg_read_tallies(ctx, C.byref(tallies.struct)), "gg_read_tallies")
-        if world > 1:  # the run's one exchange: sum the detector tallies over ranks
-            distributed.reduce_tallies(tallies)
         t1 = time.perf_counter()
         if k > 0:  # first pass warms the host allocations
             e2e_times.append(t1 - t0)
@@ -481,6 +525,8 @@ def main():
         "cpu_baseline": cpu_baseline,
         "clocks": clocks,
     }
+    if not args.no_surrogate and world == 1:
+        line["surrogate"] = surrogate_measurement(tmp)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -546,10 +592,16 @@ def run_batched(args, tmp, rank):
             raise RuntimeError("%s: %s" % (what, lib.gg_last_error().decode()))
 
     check(lib.gg_upload_scene(ctx, C.byref(w.scene)), "gg_upload_scene")
+    # tune on a sample of the job mix itself: every 12th angle and every 4th
+    # phantom, 2e6 primaries each
+    sample = [(s, min(n, 2_000_000), solids) for s, n, solids in w.jobs[:360:12] + w.jobs[360::4]]
+    sarr, skeep = _native._job_array(sample)
     ms = C.c_float()
-    check(lib.gg_autotune(ctx, C.byref(w.jobs[0][0]), 4 * abi.GG_MAXIMUM_PARTICLES, C.byref(ms)), "gg_autotune")
+    check(lib.gg_autotune_jobs(ctx, sarr, len(skeep), C.byref(ms)), "gg_autotune_jobs")
     bps, lanes, ratio = C.c_int32(), C.c_int32(), C.c_int32()
     lib.gg_get_transport_tuning(ctx, C.byref(bps), C.byref(lanes), C.byref(ratio))
+    threads, grain = C.c_int32(), C.c_int32()
+    lib.gg_get_transport_launch(ctx, C.byref(threads), C.byref(grain))
     arr, keep = _native._job_array(w.jobs)
     graph = C.c_void_p()
     check(lib.gg_capture_jobs(ctx, arr, len(keep), C.byref(graph)), "gg_capture_jobs")
@@ -583,8 +635,10 @@ def run_batched(args, tmp, rank):
             "dtype": "f32", "data": "synthetic (64^3 water phantom; seeded ellipsoid phantoms)",
             "config": {"workload": "batched_360x%d_16phantoms" % args.primaries_per_job,
                        "jobs": len(w.jobs), "primaries_per_step": w.total_primaries,
-                       "phantom_edges": w.phantom_edges, "tuning": {"blocks_per_sm": bps.value,
-                                                                    "regroup_ratio4": ratio.value},
+                       "phantom_edges": w.phantom_edges,
+                       "tuning": {"blocks_per_sm": bps.value, "regroup_ratio4": ratio.value,
+                                  "block_threads": threads.value, "slots_per_claim": grain.value,
+                                  "tuned_on": "%d sampled jobs of the mix, 2e6 primaries each" % len(sample)},
                        "launch": "one persistent kernel per step, replayed CUDA graph",
                        "l2": "256 MB buffer written between timed steps"},
             "gpu_launches": launches, "clocks": clk.summary()}), flush=True)

@@ -46,6 +46,10 @@ def _load():
         "gg_set_transport_tuning": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
         "gg_get_transport_tuning": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32), P(C.c_int32)]),
         "gg_autotune": (C.c_int, [C.c_void_p, P(abi.gg_source), C.c_uint64, P(C.c_float)]),
+        "gg_autotune_jobs": (C.c_int, [C.c_void_p, P(abi.gg_job), C.c_int32, P(C.c_float)]),
+        "gg_set_transport_launch": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+        "gg_get_transport_launch": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32)]),
+        "gg_device_tallies": (C.c_int, [C.c_void_p, P(abi.gg_device_tally), C.c_int32, P(C.c_int32)]),
         "gg_set_tracking": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
         "gg_read_tracking": (C.c_int, [C.c_void_p, P(abi.gg_track_point), C.c_int32, P(C.c_int32)]),
         "gg_volume_create": (C.c_int, [C.c_int32, C.c_int32, P(C.c_int32), P(C.c_float), P(C.c_void_p)]),
@@ -147,9 +151,25 @@ class Context:
         check(lib.gg_get_transport_tuning(self.handle, C.byref(a), C.byref(b), C.byref(c)), "gg_get_transport_tuning")
         return a.value, b.value, c.value
 
+    def set_launch(self, block_threads=256, slots_per_claim=1):
+        check(lib.gg_set_transport_launch(self.handle, block_threads, slots_per_claim), "gg_set_transport_launch")
+
+    def launch(self):
+        """(block threads, slots per claim) of the transport launch."""
+        a, b = C.c_int32(), C.c_int32()
+        check(lib.gg_get_transport_launch(self.handle, C.byref(a), C.byref(b)), "gg_get_transport_launch")
+        return a.value, b.value
+
     def autotune(self, source, number_of_particles):
         ms = C.c_float()
         check(lib.gg_autotune(self.handle, C.byref(source), number_of_particles, C.byref(ms)), "gg_autotune")
+        return ms.value
+
+    def autotune_jobs(self, jobs):
+        """gg_autotune on a batched launch of `jobs` (as run_jobs takes them)."""
+        arr, keep = _job_array(jobs)
+        ms = C.c_float()
+        check(lib.gg_autotune_jobs(self.handle, arr, len(keep), C.byref(ms)), "gg_autotune_jobs")
         return ms.value
 
     def set_tracking(self, slot, capacity=4096):

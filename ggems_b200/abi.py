@@ -103,6 +103,13 @@ class gg_job(C.Structure):
     _fields_ = [("source", gg_source), ("number_of_particles", C.c_uint64), ("solids", C.POINTER(gg_solid))]
 
 
+GG_TALLY_INT32, GG_TALLY_INT64, GG_TALLY_FP64 = 0, 1, 2
+
+
+class gg_device_tally(C.Structure):
+    _fields_ = [("address", C.c_void_p), ("count", C.c_int64), ("type", C.c_int32)]
+
+
 class gg_particle_buffers(C.Structure):
     _fields_ = [("E", FP), ("px", FP), ("py", FP), ("pz", FP), ("dx", FP), ("dy", FP), ("dz", FP),
                 ("status", C.POINTER(C.c_int8)), ("scatter", C.POINTER(C.c_int8)), ("solid_id", IP)]

@@ -25,7 +25,7 @@ namespace gg {
 
 constexpr int kMaxSolids = 64;
 constexpr int kMaxNavigators = 16;
-constexpr int kBlockThreads = 256;
+constexpr int kBlockThreads = 256;  // default transport block size (the autotuner tries 128 and 512 too)
 // Fixed-point scale of the energy tally: edep is accumulated as int64 multiples of 2^-32 MeV.
 constexpr double kEdepScale = 4294967296.0;
 
@@ -167,6 +167,7 @@ struct TransportParams {
   int32_t* tracking_count;
   int32_t regroup_lanes;            // waiting lanes that start a round of the rare phases (1..32)
   int32_t regroup_ratio4;           // ... or 4 x waiting >= regroup_ratio4 x tracking lanes
+  uint32_t slots_per_claim;         // consecutive slots a lane takes from the work queue at a time (power of two)
 };
 
 struct DoseParams {
@@ -183,8 +184,9 @@ struct DoseParams {
   float* uncertainty;
 };
 
-void launch_transport(const TransportParams& p, int grid, size_t smem, void* stream, bool mesh, bool dose, bool aux);
-cudaError_t configure_transport(size_t smem, int* blocks_per_sm, bool mesh, bool batch, bool dose, bool aux);
+void launch_transport(const TransportParams& p, int grid, int threads, size_t smem, void* stream, bool mesh, bool dose,
+                      bool aux);
+cudaError_t configure_transport(size_t smem, int threads, int* blocks_per_sm, bool mesh, bool batch, bool dose, bool aux);
 cudaError_t set_rayleigh_fit(const float* pp);
 void launch_compute_dose(const DoseParams& p, void* stream);
 

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <random>
@@ -59,6 +60,8 @@ struct gg_context {
   int regroup_lanes = 32;
   int regroup_ratio4 = 4;
   int blocks_per_sm = 0;  // 0: as many as fit (the autotuner may lower it)
+  int block_threads = gg::kBlockThreads;  // transport block size: 128, 256 or 512
+  int slots_per_claim = 1;                // photons per thread: slots a lane takes per work-queue grab
   size_t smem_optin = 0;
   uint32_t* rng = nullptr;
   gg::DevParticles particles{};
@@ -754,6 +757,33 @@ GG_API int gg_reset_tallies(gg_context* c) {
   return GG_OK;
 }
 
+GG_API int gg_device_tallies(gg_context* c, gg_device_tally* out, int32_t capacity, int32_t* count) {
+  if (!c || !count) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL context or count");
+  if (!c->scene_ready) return fail(GG_ERROR_STATE, "no scene uploaded");
+  std::vector<gg_device_tally> list;
+  auto add = [&](void* p, size_t n, int type) {
+    if (p && n) list.push_back(gg_device_tally{p, static_cast<int64_t>(n), type});
+  };
+  for (size_t h = 0; h < c->histograms.size(); ++h) add(c->histograms[h], c->histogram_sizes[h], GG_TALLY_INT32);
+  for (auto& m : c->dose_host) {
+    const size_t n = static_cast<size_t>(m.total_number_of_dosels);
+    add(m.edep, n, GG_TALLY_INT64);
+    add(m.edep_squared, n, GG_TALLY_FP64);
+    add(m.hit, n, GG_TALLY_INT32);
+    add(m.photon_tracking, n, GG_TALLY_INT32);
+  }
+  const size_t w = c->world_cells;
+  add(c->world_photon, w, GG_TALLY_INT32);
+  add(c->world_energy, w, GG_TALLY_INT64);
+  add(c->world_energy_squared, w, GG_TALLY_FP64);
+  add(c->world_momentum, 3 * w, GG_TALLY_INT64);
+  *count = static_cast<int32_t>(list.size());
+  if (!out) return GG_OK;
+  if (capacity < *count) return fail(GG_ERROR_INVALID_ARGUMENT, "capacity below the number of tally buffers");
+  std::copy(list.begin(), list.end(), out);
+  return GG_OK;
+}
+
 GG_API int gg_batch_plan(uint64_t number_of_particles, uint64_t* batch_sizes, int64_t max_batches, int64_t* count) {
   if (!count) return fail(GG_ERROR_INVALID_ARGUMENT, "count is NULL");
   // GGEMSSource::OrganizeParticlesInBatch (src/sources/GGEMSSource.cc:403-425): float ceil.
@@ -814,6 +844,7 @@ int make_dev_source(gg_context* c, const gg_source* src, gg::DevSource* out, std
 struct JobLaunch {
   gg::TransportParams params{};
   int grid = 0;
+  int threads = gg::kBlockThreads;
   size_t smem = 0;
   bool mesh = false;
   bool dose = false;  // some solid tallies into a dose map
@@ -893,6 +924,7 @@ int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*
   P.error = c->error;
   P.regroup_lanes = c->regroup_lanes;
   P.regroup_ratio4 = c->regroup_ratio4;
+  P.slots_per_claim = static_cast<uint32_t>(c->slots_per_claim);
   P.tracking_slot = -1;
   if (c->tracking_slot >= 0 && c->tracking_points) {
     P.tracking_slot = c->tracking_slot;
@@ -913,13 +945,15 @@ int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*
   out->smem = (c->tables_in_smem ? c->table_bytes : 0) + sizeof(gg::DevSolid) * c->number_of_solids +
               sizeof(gg::DevNavigator) * c->number_of_navigators + 16;
   int blocks_per_sm = 0;
-  GG_CUDA(gg::configure_transport(out->smem, &blocks_per_sm, mesh, P.number_of_jobs > 1, dose, aux));
+  GG_CUDA(gg::configure_transport(out->smem, c->block_threads, &blocks_per_sm, mesh, P.number_of_jobs > 1, dose, aux));
   if (blocks_per_sm < 1) return fail(GG_ERROR_CUDA, "transport kernel does not fit on an SM");
   if (c->blocks_per_sm > 0 && c->blocks_per_sm < blocks_per_sm) blocks_per_sm = c->blocks_per_sm;
   uint64_t grid = static_cast<uint64_t>(blocks_per_sm) * c->sm_count;
-  const uint64_t needed = (max_slots + gg::kBlockThreads - 1) / gg::kBlockThreads;
+  const uint64_t lanes_needed = (max_slots + c->slots_per_claim - 1) / c->slots_per_claim;
+  const uint64_t needed = (lanes_needed + c->block_threads - 1) / c->block_threads;
   if (grid > needed) grid = needed;
   out->grid = static_cast<int>(grid);
+  out->threads = c->block_threads;
   out->mesh = mesh;
   out->dose = dose;
   out->aux = aux;
@@ -932,7 +966,7 @@ int enqueue_jobs(gg_context* c, const JobLaunch& L) {
   GG_CUDA(cudaMemsetAsync(c->slot_counter, 0, sizeof(unsigned int), c->stream));
   if (L.params.tracking_count) GG_CUDA(cudaMemsetAsync(L.params.tracking_count, 0, sizeof(int32_t), c->stream));
   GG_CUDA(cudaMemsetAsync(c->error, 0, sizeof(int), c->stream));
-  gg::launch_transport(L.params, L.grid, L.smem, c->stream, L.mesh, L.dose, L.aux);
+  gg::launch_transport(L.params, L.grid, L.threads, L.smem, c->stream, L.mesh, L.dose, L.aux);
   GG_CUDA(cudaGetLastError());
   return GG_OK;
 }
@@ -1065,49 +1099,105 @@ GG_API int gg_get_transport_tuning(gg_context* c, int32_t* blocks_per_sm, int32_
   return GG_OK;
 }
 
-// Times `number_of_particles` primaries of `source` for each launch shape in a
-// small grid (resident blocks per SM x rare-phase regroup ratio), restoring the
-// random states before each trial, and keeps the fastest.
-GG_API int gg_autotune(gg_context* c, const gg_source* source, uint64_t number_of_particles, float* best_ms) {
-  if (!c || !source || number_of_particles == 0) return fail(GG_ERROR_INVALID_ARGUMENT, "bad autotune arguments");
-  if (!c->scene_ready) return fail(GG_ERROR_STATE, "no scene uploaded");
+GG_API int gg_set_transport_launch(gg_context* c, int32_t block_threads, int32_t slots_per_claim) {
+  if (!c || (block_threads != 128 && block_threads != 256 && block_threads != 512) || slots_per_claim < 1 ||
+      slots_per_claim > 64 || (slots_per_claim & (slots_per_claim - 1)) != 0)
+    return fail(GG_ERROR_INVALID_ARGUMENT,
+                "bad transport launch (block_threads 128/256/512, slots_per_claim a power of two up to 64)");
+  c->block_threads = block_threads;
+  c->slots_per_claim = slots_per_claim;
+  return GG_OK;
+}
+
+GG_API int gg_get_transport_launch(gg_context* c, int32_t* block_threads, int32_t* slots_per_claim) {
+  if (!c) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL context");
+  if (block_threads) *block_threads = c->block_threads;
+  if (slots_per_claim) *slots_per_claim = c->slots_per_claim;
+  return GG_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// The launch shape the autotuner varies: resident blocks per SM, the
+// rare-phase regroup ratio, the block size and the photons per thread (slots a
+// lane claims per work-queue grab).
+struct LaunchShape {
+  int blocks_per_sm, regroup_ratio4, block_threads, slots_per_claim;
+};
+
+void apply_shape(gg_context* c, const LaunchShape& s) {
+  c->blocks_per_sm = s.blocks_per_sm;
+  c->regroup_lanes = 32;
+  c->regroup_ratio4 = s.regroup_ratio4;
+  c->block_threads = s.block_threads;
+  c->slots_per_claim = s.slots_per_claim;
+}
+
+// Times `trial` (one launch of the workload to tune on) for each launch shape
+// of a coordinate search, restoring the random states before every trial, and
+// keeps the fastest:
+//   1. resident blocks per SM (4..1) x regroup ratio (3/4, 4/4, 6/4) at 256 threads, one slot per claim;
+//   2. block size 128 and 512 at the same resident threads per SM as the best of 1;
+//   3. 2, 4 and 8 slots per claim at the best of 1-2.
+// The tallies are zeroed and the random states restored afterwards.
+int autotune(gg_context* c, const std::function<int()>& trial, float* best_ms) {
   GG_CUDA(cudaSetDevice(c->device));
   const size_t bytes = static_cast<size_t>(5) * GG_MAXIMUM_PARTICLES * sizeof(uint32_t);
   void* saved = nullptr;
   GG_CUDA(cudaMalloc(&saved, bytes));
   auto restore = [&]() { return cudaMemcpyAsync(c->rng, saved, bytes, cudaMemcpyDeviceToDevice, c->stream); };
   cudaError_t e = cudaMemcpyAsync(saved, c->rng, bytes, cudaMemcpyDeviceToDevice, c->stream);
-  int best[3] = {c->blocks_per_sm, c->regroup_lanes, c->regroup_ratio4};
+  const LaunchShape start{c->blocks_per_sm, c->regroup_ratio4, c->block_threads, c->slots_per_claim};
+  LaunchShape best = start;
   float best_time = -1.0f;
   int rc = GG_OK;
-  const int ratios[3] = {3, 4, 6};
-  for (int bps = 4; bps >= 1 && e == cudaSuccess && rc == GG_OK; --bps) {
-    for (int r : ratios) {
-      c->blocks_per_sm = bps;
-      c->regroup_lanes = 32;
-      c->regroup_ratio4 = r;
-      if ((e = restore()) != cudaSuccess) break;
-      if ((rc = gg_run_source(c, source, number_of_particles)) != GG_OK) break;
-      if ((rc = gg_synchronize(c)) != GG_OK) break;
-      if (best_time < 0.0f || c->last_ms < best_time) {
-        best_time = c->last_ms;
-        best[0] = bps;
-        best[1] = 32;
-        best[2] = r;
-      }
+  auto run = [&](const LaunchShape& s) {
+    if (e != cudaSuccess || rc != GG_OK) return;
+    apply_shape(c, s);
+    if ((e = restore()) != cudaSuccess) return;
+    if ((rc = trial()) != GG_OK) return;
+    if ((rc = gg_synchronize(c)) != GG_OK) return;
+    if (best_time < 0.0f || c->last_ms < best_time) {
+      best_time = c->last_ms;
+      best = s;
     }
+  };
+  for (int bps = 4; bps >= 1; --bps)
+    for (int r : {3, 4, 6}) run({bps, r, gg::kBlockThreads, 1});
+  const LaunchShape stage1 = best;
+  for (int threads : {128, 512}) {
+    const int bps = stage1.blocks_per_sm * gg::kBlockThreads / threads;
+    if (bps >= 1) run({bps, stage1.regroup_ratio4, threads, 1});
   }
+  const LaunchShape stage2 = best;
+  for (int k : {2, 4, 8}) run({stage2.blocks_per_sm, stage2.regroup_ratio4, stage2.block_threads, k});
   if (e == cudaSuccess) e = restore();
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   cudaFree(saved);
-  c->blocks_per_sm = best[0];
-  c->regroup_lanes = best[1];
-  c->regroup_ratio4 = best[2];
+  apply_shape(c, best_time < 0.0f ? start : best);
   if (e != cudaSuccess) return fail(GG_ERROR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
   if (rc != GG_OK) return rc;
   if ((rc = gg_reset_tallies(c)) != GG_OK) return rc;
   if (best_ms) *best_ms = best_time;
   return GG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+GG_API int gg_autotune(gg_context* c, const gg_source* source, uint64_t number_of_particles, float* best_ms) {
+  if (!c || !source || number_of_particles == 0) return fail(GG_ERROR_INVALID_ARGUMENT, "bad autotune arguments");
+  if (!c->scene_ready) return fail(GG_ERROR_STATE, "no scene uploaded");
+  return autotune(c, [&]() { return gg_run_source(c, source, number_of_particles); }, best_ms);
+}
+
+GG_API int gg_autotune_jobs(gg_context* c, const gg_job* jobs, int32_t number_of_jobs, float* best_ms) {
+  if (!c || !jobs || number_of_jobs < 1) return fail(GG_ERROR_INVALID_ARGUMENT, "bad autotune arguments");
+  if (!c->scene_ready) return fail(GG_ERROR_STATE, "no scene uploaded");
+  return autotune(c, [&]() { return gg_run_jobs(c, jobs, number_of_jobs); }, best_ms);
 }
 
 GG_API int gg_line_integrals(gg_context* c, const gg_solid* phantom, const gg_solid* detector, const float* source_position,

@@ -728,8 +728,12 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 }
 
 // Copies `bytes` (multiple of 16) from HBM into shared memory with
-// cp.async.bulk and waits on an mbarrier for at most ~`limit` polls.
-// Returns false (and sets *error) when the copy did not complete in time.
+// cp.async.bulk and waits on an mbarrier for at most 2^22 polls (far longer
+// than a 15 KB copy takes).  Returns false (and sets *error) when the copy did
+// not complete in time; the CTA then exits, possibly with the copy still in
+// flight, so the run reports GG_ERROR_TIMEOUT and the context must be
+// recreated (include/ggems_b200.h).  Extra wait code here, even out of line,
+// changes the register allocation of the whole kernel (more spills).
 __device__ bool stage_tables(unsigned char* dst, const unsigned char* src, uint32_t bytes, uint64_t* bar, int* error) {
   constexpr uint32_t kChunk = 16384;
   if (threadIdx.x == 0) {
@@ -762,14 +766,21 @@ __device__ bool stage_tables(unsigned char* dst, const unsigned char* src, uint3
 
 extern __shared__ __align__(16) unsigned char g_smem[];
 
+// Register budget of a variant: what 256-thread blocks need to keep `blocks`
+// of them resident per SM (64, 80 or 128 registers), fixed per kernel so that
+// the block size stays a launch parameter (128, 256 or 512 threads).
+constexpr int transport_registers(int blocks) { return (65536 / (kBlockThreads * blocks)) & ~7; }
+
 // kFull: the scene has a meshed solid, a world grid or a tracked particle;
 // kAux: the world walk and particle tracking are compiled in.  Scenes without
 // them run variants compiled without that code, so its instructions and
 // registers stay out of the voxel / detector (or mesh) hot loop.
 // kDose: some solid tallies into a dose map.
 // kBatch: several jobs (source runs) in one launch, each with its own solids.
+
 template <bool kFull, bool kBatch, bool kDose, bool kAux>
-__global__ void __launch_bounds__(kBlockThreads, kAux ? 2 : (kFull ? 3 : (kBatch && kDose ? 3 : 4))) transport_kernel(TransportParams P) {
+__global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : (kBatch && kDose ? 3 : 4))))
+    transport_kernel(TransportParams P) {
   // shared memory: [tables][solids][navigators][mbarrier]
   unsigned char* tables = g_smem;
   DevSolid* scene_solids = reinterpret_cast<DevSolid*>(g_smem + (P.tables_in_smem ? P.table_bytes : 0));
@@ -795,7 +806,7 @@ __global__ void __launch_bounds__(kBlockThreads, kAux ? 2 : (kFull ? 3 : (kBatch
   Kiss rng{0, 0, 0, 0, 0};
   Photon ph{};
   ph.solid_id = -1;
-  uint32_t slot = 0;
+  uint32_t slot = ~0u;
   uint32_t histories_left = 0;
   int rounds = 0;
   int phase = kDone;
@@ -832,9 +843,13 @@ __global__ void __launch_bounds__(kBlockThreads, kAux ? 2 : (kFull ? 3 : (kBatch
     }
     return false;
   };
-  // Grab the next slot.
+  // Grab the next slot: the lane takes slots_per_claim consecutive slots from
+  // the work queue at a time and runs their photons one after another.  The
+  // queue hands out runs starting at multiples of slots_per_claim (a power of
+  // two), so the run is used up when the next slot is such a multiple (slot
+  // starts at ~0u: the first call claims).
   auto next_slot = [&]() -> bool {
-    slot = atomicAdd(P.slot_counter, 1u);
+    if ((++slot & (P.slots_per_claim - 1)) == 0) slot = atomicAdd(P.slot_counter, P.slots_per_claim);
     if (slot >= P.number_of_slots) return false;
     rng = Kiss{P.rng[slot], P.rng[S + slot], P.rng[2 * S + slot], P.rng[3 * S + slot], P.rng[4 * S + slot]};
     return enter_job(0);
@@ -1238,9 +1253,10 @@ TransportKernel transport_variant(bool mesh, bool batch, bool dose, bool aux) {
 }
 }  // namespace
 
-void launch_transport(const TransportParams& p, int grid, size_t smem, void* stream, bool mesh, bool dose, bool aux) {
+void launch_transport(const TransportParams& p, int grid, int threads, size_t smem, void* stream, bool mesh, bool dose,
+                      bool aux) {
   const bool batch = p.number_of_jobs > 1;
-  transport_variant(mesh, batch, dose, aux)<<<grid, kBlockThreads, smem, static_cast<cudaStream_t>(stream)>>>(p);
+  transport_variant(mesh, batch, dose, aux)<<<grid, threads, smem, static_cast<cudaStream_t>(stream)>>>(p);
 }
 
 namespace {
@@ -1334,11 +1350,12 @@ void launch_compute_dose(const DoseParams& p, void* stream) {
   compute_dose_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(p);
 }
 
-cudaError_t configure_transport(size_t smem, int* blocks_per_sm, bool mesh, bool batch, bool dose, bool aux) {
+cudaError_t configure_transport(size_t smem, int threads, int* blocks_per_sm, bool mesh, bool batch, bool dose,
+                                bool aux) {
   auto kernel = transport_variant(mesh, batch, dose, aux);
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, kBlockThreads, smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, threads, smem);
 }
 
 cudaError_t set_rayleigh_fit(const float* pp /* 9*101 */) {

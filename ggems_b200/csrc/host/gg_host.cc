@@ -5,6 +5,8 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <climits>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <iostream>
@@ -71,7 +73,10 @@ std::string data_directory() {
   if (const char* env = std::getenv("GGEMS_B200_DATA")) return std::string(env) + "/";
   Dl_info info;
   if (dladdr(reinterpret_cast<void*>(&data_directory), &info) && info.dli_fname) {
-    std::string lib(info.dli_fname);
+    // the library's own directory, not that of a link to it (GGEMS's Python
+    // module loads libggems.so from beside the module, often a link)
+    char resolved[PATH_MAX];
+    std::string lib(realpath(info.dli_fname, resolved) ? resolved : info.dli_fname);
     size_t pos = lib.find_last_of('/');
     return (pos == std::string::npos ? std::string("./") : lib.substr(0, pos + 1)) + "data/";
   }

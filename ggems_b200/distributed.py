@@ -16,9 +16,14 @@ play the roles of GGEMS's activated devices:
   (GGEMS overwrites the hit and energy-squared maps per device instead of
   summing them, GGEMSDosimetryCalculator.cc:623,713; that is not reproduced).
 
-Energy deposits are exact multiples of 2^-32 MeV (int64 fixed point on the
-device), so their double sums are exact and the reduced map does not depend
-on the rank order.
+On GPUs the reduction runs on the device tallies themselves
+(reduce_device_tallies): every buffer a context tallies into (gg_device_tallies)
+is all-reduced in place over NCCL, the energy maps as the int64 fixed-point
+integers the kernels add (LSB 2^-32 MeV), so the sums are exact at any size
+and independent of the rank order, and nothing crosses to the host before
+gg_read_tallies.  reduce_tallies does the same on host copies (gloo ranks,
+CPU tests); there the energy arrives as doubles, exact while a dosel holds
+less than 2^21 MeV.
 """
 
 import ctypes as C
@@ -66,6 +71,41 @@ def _all_reduce_sum(array, dist, group):
     if array.dtype.kind in "iu" and (out > np.iinfo(array.dtype).max).any():
         raise OverflowError("tally sum exceeds %s" % array.dtype)
     array[...] = out.astype(array.dtype)
+
+
+class _DeviceArray:
+    """A device buffer seen through __cuda_array_interface__ (zero copy)."""
+
+    TYPESTR = {abi.GG_TALLY_INT32: "<i4", abi.GG_TALLY_INT64: "<i8", abi.GG_TALLY_FP64: "<f8"}
+
+    def __init__(self, tally):
+        self.__cuda_array_interface__ = {"shape": (int(tally.count),), "typestr": self.TYPESTR[tally.type],
+                                         "data": (int(tally.address), False), "version": 3, "strides": None}
+
+
+def device_tallies(context):
+    """The context's device tally buffers (gg_device_tallies) as torch tensors
+    that alias them."""
+    import torch
+    from ._native import lib, check
+    n = C.c_int32()
+    check(lib.gg_device_tallies(context, None, 0, C.byref(n)), "gg_device_tallies")
+    arr = (abi.gg_device_tally * max(n.value, 1))()
+    check(lib.gg_device_tallies(context, arr, n.value, C.byref(n)), "gg_device_tallies")
+    return [torch.as_tensor(_DeviceArray(arr[i]), device="cuda") for i in range(n.value)]
+
+
+def reduce_device_tallies(context, group=None):
+    """Sum the tallies of `context` (a gg_context handle) over all ranks of
+    `group`, in place on every rank's GPU (NCCL): call after the run has
+    finished (gg_synchronize), then read them with gg_read_tallies."""
+    import torch
+    import torch.distributed as dist
+    tensors = device_tallies(context)
+    for t in tensors:
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    torch.cuda.synchronize()
+    return len(tensors)
 
 
 def reduce_tallies(tallies, group=None):

@@ -379,51 +379,85 @@ def make_inputs(geometry, projections):
 JUDGE_MC, JUDGE_RESCALED, JUDGE_NETWORK = 0, 1, 2
 
 
-def judge(predicted, low_count_mc, tolerance=JUDGE_TOLERANCE, primaries=None, side=None, shape_blocks=4,
-          shape_p=1e-3):
-    """Per projection, against the low-count plain-MC estimate:
+def judge(predicted, low_count_mc, tolerance=JUDGE_TOLERANCE):
+    """The judge as specified, per projection against the low-count plain-MC
+    estimate: JUDGE_NETWORK when the network's integrated scatter is within
+    `tolerance` of the MC's (the network's output is kept), else JUDGE_MC (the
+    MC estimate replaces it).  Returns (outputs, verdicts)."""
+    out, verdict = [], []
+    for p, m in zip(predicted, low_count_mc):
+        sp, sm = float(p.sum()), float(m.sum())
+        keep = abs(sp - sm) <= tolerance * max(sm, 1e-12)
+        out.append(p if keep else m)
+        verdict.append(JUDGE_NETWORK if keep else JUDGE_MC)
+    return np.stack(out), np.array(verdict)
 
-    * JUDGE_NETWORK: the network's integrated scatter is within `tolerance` of
-      the MC's, and its output is kept;
-    * otherwise, when `primaries` is given, the network's shape is tested
-      against the MC's on a shape_blocks x shape_blocks grid: a chi-square of
-      the MC's counts per block against the network rescaled to the MC's
-      integral (Poisson variances, shape_blocks^2 - 1 degrees of freedom).
-      JUDGE_RESCALED: the shape passes (p >= shape_p) and the network rescaled
-      to the MC's integral is the output -- the magnitude from the MC (its
-      integral carries ~1/sqrt(counts) noise, about 2 % at 1e6 primaries), the
-      shape from the network;
-    * JUDGE_MC: the MC estimate replaces the network.
 
-    Returns (outputs, verdicts)."""
+def judge_rescaled(predicted, low_count_mc, primaries, side=None, tolerance=JUDGE_TOLERANCE, shape_blocks=4,
+                   shape_p=1e-3):
+    """A variant of the judge with a third verdict (reported beside the judge
+    as specified, not in its place): a projection outside the 5 % band whose
+    network shape agrees with the MC's counts on a shape_blocks x shape_blocks
+    grid (chi-square of the MC's counts per block against the network rescaled
+    to the MC's integral, Poisson variances, shape_blocks^2 - 1 degrees of
+    freedom, p >= shape_p) gets the network rescaled to the MC's integral
+    (JUDGE_RESCALED) instead of the MC estimate; the MC's integral carries
+    ~1/sqrt(counts) noise, about 2 % at 1e6 primaries.  Returns (outputs,
+    verdicts)."""
     from scipy.stats import chi2
     out, verdict = [], []
     limit = chi2.isf(shape_p, shape_blocks * shape_blocks - 1)
-    for p, m in zip(predicted, low_count_mc):
+    final, used = judge(predicted, low_count_mc, tolerance)
+    for p, m, f, v in zip(predicted, low_count_mc, final, used):
         sp, sm = float(p.sum()), float(m.sum())
-        if abs(sp - sm) <= tolerance * max(sm, 1e-12):
-            out.append(p)
-            verdict.append(JUDGE_NETWORK)
+        if v == JUDGE_NETWORK or sp <= 0.0 or sm <= 0.0:
+            out.append(f)
+            verdict.append(v)
             continue
-        if primaries is not None and sp > 0.0 and sm > 0.0:
-            n = side if side is not None else p.shape[-1]
-            to_counts = float(primaries) / float(n * n)  # inverse of normalise()
-            counts = block_mean(m, shape_blocks) * (n // shape_blocks) ** 2 * to_counts
-            expected = block_mean(p, shape_blocks) * (n // shape_blocks) ** 2 * to_counts * (sm / sp)
-            stat = float((((counts - expected) ** 2) / np.maximum(expected, 1.0)).sum())
-            if stat <= limit:
-                out.append(p * (sm / sp))
-                verdict.append(JUDGE_RESCALED)
-                continue
-        out.append(m)
-        verdict.append(JUDGE_MC)
+        n = side if side is not None else p.shape[-1]
+        to_counts = float(primaries) / float(n * n)  # inverse of normalise()
+        counts = block_mean(m, shape_blocks) * (n // shape_blocks) ** 2 * to_counts
+        expected = block_mean(p, shape_blocks) * (n // shape_blocks) ** 2 * to_counts * (sm / sp)
+        stat = float((((counts - expected) ** 2) / np.maximum(expected, 1.0)).sum())
+        if stat <= limit:
+            out.append(p * (sm / sp))
+            verdict.append(JUDGE_RESCALED)
+        else:
+            out.append(m)
+            verdict.append(JUDGE_MC)
     return np.stack(out), np.array(verdict)
 
 
 def relative_error(a, ref, blocks=16):
-    """Relative L2 error of a scatter projection on a blocks x blocks grid."""
-    a, ref = block_mean(a, blocks), block_mean(ref, blocks)
+    """Relative L2 error of a scatter projection, on a blocks x blocks grid of
+    block means (blocks=None: per element, at full resolution)."""
+    if blocks is not None:
+        a, ref = block_mean(a, blocks), block_mean(ref, blocks)
+    a, ref = np.asarray(a, np.float64), np.asarray(ref, np.float64)
     return float(np.linalg.norm(a - ref) / max(np.linalg.norm(ref), 1e-30))
+
+
+def reference_noise(ref, primaries, blocks=16):
+    """Relative L2 norm of a reference's own counting noise, in the units of
+    relative_error: a reference of `primaries` primaries (normalised counts
+    `ref`) has Poisson variance counts x (side^2 / primaries)^2 per element;
+    block means divide it by the block's element count."""
+    ref = np.asarray(ref, np.float64)
+    side = ref.shape[-1]
+    scale = float(side * side) / float(primaries)
+    var = ref * scale  # = counts * scale^2
+    if blocks is not None:
+        b = side // blocks
+        var = block_mean(var, blocks) / (b * b)
+        ref = block_mean(ref, blocks)
+    return float(np.sqrt(var.sum()) / max(np.linalg.norm(ref), 1e-30))
+
+
+def error_vs_truth(err, floor):
+    """An estimate's error against the (unknown) true scatter image, from its
+    error against a reference whose own noise is `floor`: the two errors are
+    independent, so err^2 = true_err^2 + floor^2."""
+    return float(np.sqrt(max(err * err - floor * floor, 0.0)))
 
 
 def learning_rate(step, total, lr, warmup=100, floor=0.01):
@@ -515,13 +549,39 @@ def time_network(side=256, batch=8, repeats=20):
     return ms, forward_flops(side, batch) / (ms * 1e-3) / 1e12, train_ms
 
 
+def _conv_weight_mask(count):
+    """True at the 3x3 convolution weights of the parameter vector (layer by
+    layer: weights [9][C_out][C_in], then biases; then the 1x1 output layer)."""
+    mask = np.zeros(count, bool)
+    off = 0
+    for ci, co, _ in LAYERS:
+        mask[off:off + 9 * ci * co] = True
+        off += 9 * ci * co + co
+    return mask
+
+
 def save_network(net, path):
-    np.savez(path, parameters=net.parameters(), target_scale=np.float64(getattr(net, "target_scale", 1.0)))
+    """The trained network: the convolution weights as BF16 bits (the forward
+    pass rounds the FP32 master weights to BF16 the same way, round to nearest
+    even, so inference is unchanged), biases and the output layer in FP32."""
+    p = net.parameters()
+    mask = _conv_weight_mask(len(p))
+    bits = p[mask].view(np.uint32).astype(np.uint64)
+    bf16 = ((bits + 0x7FFF + ((bits >> 16) & 1)) >> 16).astype(np.uint16)
+    np.savez_compressed(path, conv_weights_bf16=bf16, other_fp32=p[~mask],
+                        target_scale=np.float64(getattr(net, "target_scale", 1.0)))
 
 
 def load_network(net, path):
     z = np.load(path)
-    net.set_parameters(z["parameters"])
+    if "parameters" in z.files:
+        p = z["parameters"]
+    else:
+        p = np.zeros(net.parameter_count(), np.float32)
+        mask = _conv_weight_mask(len(p))
+        p[mask] = (z["conv_weights_bf16"].astype(np.uint32) << 16).view(np.float32)
+        p[~mask] = z["other_fp32"]
+    net.set_parameters(p)
     net.target_scale = float(z["target_scale"])
 
 
@@ -529,7 +589,8 @@ def surrogate_pipeline(geo, net, projections, judge_primaries, seed):
     """The surrogate at inference: per projection the deterministic inputs and
     the network's scatter estimate, the low-count plain-MC estimate of all
     projections (one batched launch per chunk of jobs) and the 5 % judge.
-    Returns (final, prediction, low-count MC, kept flags, seconds)."""
+    Returns (final, prediction, low-count MC, verdicts, seconds); the
+    variant with rescaling (judge_rescaled) is left in geo.last_rescaled."""
     import torch
     torch.cuda.synchronize()
     t = [time.perf_counter()]
@@ -539,13 +600,13 @@ def surrogate_pipeline(geo, net, projections, judge_primaries, seed):
     # registers left on every SM let the projector's and the network's kernels
     # run beside it instead of after it.
     from ._native import check
-    lanes, ratio4 = C.c_int32(), C.c_int32()
-    check(geo.lib.gg_get_transport_tuning(geo.ctx, None, C.byref(lanes), C.byref(ratio4)), "tuning")
+    bps, lanes, ratio4 = C.c_int32(), C.c_int32(), C.c_int32()
+    check(geo.lib.gg_get_transport_tuning(geo.ctx, C.byref(bps), C.byref(lanes), C.byref(ratio4)), "tuning")
     check(geo.lib.gg_set_transport_tuning(geo.ctx, JUDGE_BLOCKS_PER_SM, lanes.value, ratio4.value), "tuning")
     try:
         run = geo.start_simulation(projections, int(judge_primaries), seed=seed, totals=False)
     finally:
-        check(geo.lib.gg_set_transport_tuning(geo.ctx, 0, lanes.value, ratio4.value), "tuning")
+        check(geo.lib.gg_set_transport_tuning(geo.ctx, bps.value, lanes.value, ratio4.value), "tuning")
     t.append(time.perf_counter())
     x = make_inputs(geo, projections)
     t.append(time.perf_counter())
@@ -554,11 +615,123 @@ def surrogate_pipeline(geo, net, projections, judge_primaries, seed):
     _, low = geo.finish_simulation(run)
     low = normalise(low, judge_primaries, geo.side)
     t.append(time.perf_counter())
-    final, used = judge(pred, low, primaries=judge_primaries, side=geo.side)
+    final, used = judge(pred, low)
     t.append(time.perf_counter())
+    geo.last_rescaled = judge_rescaled(pred, low, judge_primaries, geo.side)
     geo.last_breakdown = {"judge_mc_launch": t[1] - t[0], "inputs": t[2] - t[1], "network": t[3] - t[2],
                           "judge_mc_wait": t[4] - t[3], "judge": t[5] - t[4]}
     return final, pred, low, used, t[-1] - t[0]
+
+
+METRIC = "scatter projections/s (surrogate + 1e6-primary MC judge vs plain MC at <=5% error)"
+ERROR_GRIDS = (("blocks16", 16), ("full", None))
+
+
+def _errors(est, refs, ref_primaries):
+    """Per projection: error against the reference and against the truth (the
+    reference's counting noise removed), on the 16x16 block grid and at full
+    resolution."""
+    out = {}
+    for name, blocks in ERROR_GRIDS:
+        raw = [relative_error(e, r, blocks) for e, r in zip(est, refs)]
+        floor = [reference_noise(r, ref_primaries, blocks) for r in refs]
+        out[name] = {"raw": raw, "floor": floor, "truth": [error_vs_truth(a, b) for a, b in zip(raw, floor)]}
+    return out
+
+
+def _summary(err):
+    return {name: {"mean": float(np.mean(e["truth"])), "max": float(np.max(e["truth"])),
+                   "mean_raw": float(np.mean(e["raw"])), "reference_noise": float(np.mean(e["floor"]))}
+            for name, e in err.items()}
+
+
+def evaluate(geo, net, rng, args, simulate_all):
+    """The surrogate's measurement: a CBCT scan of a new phantom at args.angles
+    angles through the whole pipeline (timed), its errors against
+    reference_primaries-primary references on every args.reference_every-th
+    angle, and plain MC timed at the primaries that give 5 % error on the same
+    metric.  Optionally args.test new phantoms at random angles as well."""
+    import torch
+    side = geo.side
+    out = {"metric": METRIC, "unit": "projections/s", "higher_is_better": True}
+    if args.test > 0:
+        test_projs = [(float(rng.uniform(0, 360)), random_phantom(rng)) for _ in range(args.test)]
+        _, s_ref, _ = simulate_all(test_projs, args.reference_primaries)
+        ref = normalise(s_ref, args.reference_primaries, side)
+        final, pred, low, used, _ = surrogate_pipeline(geo, net, test_projs, args.judge_primaries, 1234 + args.seed)
+        resc, _ = geo.last_rescaled
+        out["new_phantoms"] = {
+            "projections": args.test, "network_kept": float((used == JUDGE_NETWORK).mean()),
+            "judged": _summary(_errors(final, ref, args.reference_primaries)),
+            "network": _summary(_errors(pred, ref, args.reference_primaries)),
+            "judge_mc": _summary(_errors(low, ref, args.reference_primaries)),
+            "judged_with_rescaling": _summary(_errors(resc, ref, args.reference_primaries))}
+    phantom = random_phantom(rng)
+    scan = [(360.0 * k / args.angles, phantom) for k in range(args.angles)]
+    # warm-up at the scan's own size: device pools, job tables and pinned buffers
+    # reach their working sizes before the timed scan
+    surrogate_pipeline(geo, net, scan, args.judge_primaries, 99)
+    s_final, s_pred, s_low, s_used, t_scan = surrogate_pipeline(geo, net, scan, args.judge_primaries,
+                                                                4321 + args.seed)
+    s_resc, s_resc_used = geo.last_rescaled
+    breakdown = {k: v / args.angles * 1e3 for k, v in geo.last_breakdown.items()}
+    picked = list(range(0, args.angles, args.reference_every))
+    _, s_ref_scan, _ = simulate_all([scan[k] for k in picked], args.reference_primaries)
+    ref_scan = normalise(s_ref_scan, args.reference_primaries, side)
+    e_final = _errors([s_final[k] for k in picked], ref_scan, args.reference_primaries)
+    e_pred = _errors([s_pred[k] for k in picked], ref_scan, args.reference_primaries)
+    e_low = _errors([s_low[k] for k in picked], ref_scan, args.reference_primaries)
+    e_resc = _errors([s_resc[k] for k in picked], ref_scan, args.reference_primaries)
+    sur_per_s = args.angles / t_scan
+    # Plain MC at 5 %: it is unbiased, so its error against the truth falls as
+    # 1/sqrt(primaries) from the judge MC's (measured on the same angles).  Its
+    # rate is the device time of one batched launch of plain_angles angles at
+    # the block-grid count (no host overhead counted against it); the
+    # full-resolution count is far larger and uses that measured rate.
+    n_plain = {name: float(args.judge_primaries * (float(np.mean(e_low[name]["truth"])) / 0.05) ** 2)
+               for name, _ in ERROR_GRIDS}
+    angles = [scan[k] for k in picked[:args.plain_angles]]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, s_plain, plain_ms = simulate_all(angles, n_plain["blocks16"])
+    t_plain = time.perf_counter() - t0
+    rate = len(angles) * n_plain["blocks16"] / (plain_ms * 1e-3)
+    e_plain = _errors(normalise(s_plain, n_plain["blocks16"], side), ref_scan[:len(angles)],
+                      args.reference_primaries)
+    plain = {"mc_primaries_per_s": rate, "projections_timed": len(angles),
+             "wall_projections_per_s": len(angles) / t_plain}
+    for name, _ in ERROR_GRIDS:
+        per_s = rate / n_plain[name]
+        plain[name] = {"primaries_for_5pct": n_plain[name], "projections_per_s": per_s,
+                       "speedup": sur_per_s / per_s,
+                       "error_mean": float(np.mean(e_plain[name]["truth"])) if name == "blocks16" else None}
+
+    def integral_errors(est, refs):
+        return [abs(float(e.sum()) - float(r.sum())) / float(r.sum()) for e, r in zip(est, refs)]
+    net_int = integral_errors([s_pred[k] for k in picked], ref_scan)
+    low_int = integral_errors([s_low[k] for k in picked], ref_scan)
+    out.update({
+        "value": sur_per_s,
+        "judge": "as specified: network kept within 5 % of the judge MC's integrated scatter, else replaced by it",
+        "scan": {"angles": args.angles, "seconds": t_scan, "network_kept": float((s_used == JUDGE_NETWORK).mean()),
+                 "replaced_by_mc": float((s_used == JUDGE_MC).mean()), "reference_angles": len(picked),
+                 "ms_per_projection": breakdown,
+                 "error": _summary(e_final), "network_error": _summary(e_pred), "judge_mc_error": _summary(e_low)},
+        "plain_mc": plain,
+        "with_rescaling": {"judge": "judge_rescaled: outside the 5 % band, a network of the right shape is rescaled "
+                                    "to the MC's integral instead of replaced",
+                           "network_kept": float((s_resc_used == JUDGE_NETWORK).mean()),
+                           "rescaled": float((s_resc_used == JUDGE_RESCALED).mean()),
+                           "error": _summary(e_resc)},
+        "integrated_scatter_error": {"network_rms": float(np.sqrt(np.mean(np.square(net_int)))),
+                                     "network_max": float(np.max(net_int)),
+                                     "judge_mc_rms": float(np.sqrt(np.mean(np.square(low_int)))),
+                                     "projections": len(net_int)},
+        "errors": "relative L2 against the truth: error against the reference with the reference's own counting "
+                  "noise removed in quadrature (raw errors beside); 'blocks16' on a 16x16 grid of block means, "
+                  "'full' per detector element at full resolution; the network's training targets are 32x32 "
+                  "block means"})
+    return out
 
 
 def main(argv=None):
@@ -578,6 +751,8 @@ def main(argv=None):
     ap.add_argument("--load", help="skip data generation and training: load a trained network (.npz)")
     ap.add_argument("--seed", type=int, default=11, help="seed of the phantoms, angles and MC streams")
     ap.add_argument("--network-only", action="store_true", help="time the network's forward pass and training step only")
+    ap.add_argument("--plain-angles", type=int, default=16, help="scan angles plain MC is timed on")
+    ap.add_argument("--json-out", help="also write the JSON line to this file")
     args = ap.parse_args(argv)
     if args.network_only:
         ms, tflops, train_ms = time_network(args.side, args.batch)
@@ -629,69 +804,17 @@ def main(argv=None):
         del x_train, y_train
         if args.save:
             save_network(net, args.save)
-    # (1) new phantoms at random angles
-    test_projs = [(float(rng.uniform(0, 360)), random_phantom(rng)) for _ in range(args.test)]
-    _, s_ref, _ = simulate_all(test_projs, args.reference_primaries)
-    ref = normalise(s_ref, args.reference_primaries, side)
-    final, pred, low, used, _ = surrogate_pipeline(geo, net, test_projs, args.judge_primaries, 1234 + args.seed)
-    err_sur = [relative_error(f, r) for f, r in zip(final, ref)]
-    err_net = [relative_error(p, r) for p, r in zip(pred, ref)]
-    err_low = [relative_error(m, r) for m, r in zip(low, ref)]
-    # (2) a CBCT scan: one new phantom, `angles` projections through the whole pipeline
-    phantom = random_phantom(rng)
-    scan = [(360.0 * k / args.angles, phantom) for k in range(args.angles)]
-    # warm-up at the scan's own size: device pools, job tables and pinned buffers
-    # reach their working sizes before the timed scan
-    surrogate_pipeline(geo, net, scan, args.judge_primaries, 99)
-    s_final, s_pred, s_low, s_used, t_scan = surrogate_pipeline(geo, net, scan, args.judge_primaries, 4321 + args.seed)
-    breakdown = {k: v / args.angles * 1e3 for k, v in geo.last_breakdown.items()}
-    picked = list(range(0, args.angles, args.reference_every))
-    _, s_ref_scan, _ = simulate_all([scan[k] for k in picked], args.reference_primaries)
-    ref_scan = normalise(s_ref_scan, args.reference_primaries, side)
-    scan_err = [relative_error(s_final[k], r) for k, r in zip(picked, ref_scan)]
-    scan_low = [relative_error(s_low[k], r) for k, r in zip(picked, ref_scan)]
-
-    def integral_errors(est, refs):
-        return [abs(float(e.sum()) - float(r.sum())) / float(r.sum()) for e, r in zip(est, refs)]
-    net_int = integral_errors([s_pred[k] for k in picked], ref_scan) + integral_errors(pred, ref)
-    low_int = integral_errors([s_low[k] for k in picked], ref_scan) + integral_errors(low, ref)
-    # plain MC: primaries for 5 % error by Poisson scaling of the low-count error; its
-    # projections/s timed directly on 16 scan angles at that count (one batched launch)
-    e_low = float(np.mean(scan_low))
-    n_plain = args.judge_primaries * (e_low / 0.05) ** 2
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    _, s_plain, _ = simulate_all(scan[:16], n_plain)
-    t_plain = time.perf_counter() - t0
-    plain_err = [relative_error(normalise(s_plain[k], n_plain, side), ref_scan[k // args.reference_every])
-                 for k in range(0, 16, args.reference_every)]
-    rate = 16 * n_plain / t_plain
-    plain_per_s = 16 / t_plain
-    sur_per_s = args.angles / t_scan
-    print(json.dumps({
-        "metric": "scatter projections/s (surrogate + 1e6-primary MC judge vs plain MC at <=5% error)",
-        "surrogate_projections_per_s": sur_per_s, "plain_mc_projections_per_s": plain_per_s,
-        "speedup": sur_per_s / plain_per_s,
-        "scan": {"angles": args.angles, "seconds": t_scan, "judge_kept": float((s_used == JUDGE_NETWORK).mean()),
-                 "judge_rescaled": float((s_used == JUDGE_RESCALED).mean()),
-                 "error_mean": float(np.mean(scan_err)), "error_max": float(np.max(scan_err)),
-                 "low_count_mc_error": e_low, "reference_angles": len(picked),
-                 "ms_per_projection": breakdown},
-        "integrated_scatter_error": {"network_rms": float(np.sqrt(np.mean(np.square(net_int)))),
-                                     "network_max": float(np.max(net_int)),
-                                     "judge_mc_rms": float(np.sqrt(np.mean(np.square(low_int)))),
-                                     "projections": len(net_int)},
-        "new_phantoms": {"projections": args.test, "network_error": float(np.mean(err_net)),
-                         "judged_error": float(np.mean(err_sur)), "judged_error_max": float(np.max(err_sur)),
-                         "low_count_mc_error": float(np.mean(err_low)), "judge_kept": float((used == JUDGE_NETWORK).mean()),
-                         "judge_rescaled": float((used == JUDGE_RESCALED).mean())},
-        "plain_mc_primaries_for_5pct": n_plain, "plain_mc_error": float(np.mean(plain_err)),
-        "mc_primaries_per_s": rate,
-        "config": {"side": side, "pairs": args.pairs, "target_primaries": args.primaries, "epochs": args.epochs,
-                   "judge_primaries": args.judge_primaries, "reference_primaries": args.reference_primaries,
-                   "loaded": bool(args.load)},
-        "times_s": {"data": t_data, "train": t_train, "train_mc_ms": mc_ms},
-        "final_loss": float(np.mean(losses[-20:])) if losses else None}), flush=True)
+    out = evaluate(geo, net, rng, args, simulate_all)
+    out["config"] = {"side": side, "pairs": args.pairs, "target_primaries": args.primaries, "epochs": args.epochs,
+                     "judge_primaries": args.judge_primaries, "reference_primaries": args.reference_primaries,
+                     "loaded": bool(args.load), "network": os.path.basename(args.load) if args.load else None}
+    out["times_s"] = {"data": t_data, "train": t_train, "train_mc_ms": mc_ms}
+    out["final_loss"] = float(np.mean(losses[-20:])) if losses else None
+    line = json.dumps(out)
+    print(line, flush=True)
+    if args.json_out:
+        with open(args.json_out, "w") as f:
+            f.write(line + "\n")
     net.close()
     return 0
 

@@ -43,6 +43,10 @@ typedef enum gg_status {
   GG_ERROR_NO_DEVICE = 3,
   GG_ERROR_OUT_OF_MEMORY = 4,
   GG_ERROR_STATE = 5,
+  /* A bounded wait inside a kernel gave up (the transport kernel's table
+   * staging, the tensor-core convolution's operand pipeline).  The failing
+   * blocks may have exited with copies into their shared memory still in
+   * flight: destroy and recreate the context before running on. */
   GG_ERROR_TIMEOUT = 6
 } gg_status;
 
@@ -299,18 +303,29 @@ GG_API int gg_capture_jobs(gg_context* context, const gg_job* jobs, int32_t numb
 GG_API int gg_graph_launch(gg_graph* graph);
 GG_API int gg_graph_destroy(gg_graph* graph);
 
-/* Launch shape of the transport kernel (no counterpart in the reference):
- * resident blocks per SM (0: as many as fit) and the warp scheduling of the
- * rare phases (regroup_lanes 1..32, regroup_ratio4 0..128).  gg_autotune
- * times short runs of `source` over a set of shapes, keeps the fastest and
- * reports it; it restores the random states and zeroes the tallies
- * afterwards, so call it before the real run. */
+/* Launch shape of the transport kernel (no counterpart in the reference; its
+ * GGEMSOpenCLManager::GetBestWorkItem / GetWorkGroupSize pick one work item
+ * per photon and a fixed work-group size):
+ * - resident blocks per SM (0: as many as fit) and the warp scheduling of the
+ *   rare phases (regroup_lanes 1..32, regroup_ratio4 0..128):
+ *   gg_set_transport_tuning;
+ * - the block size (128, 256 or 512 threads) and the photons per thread, i.e.
+ *   the consecutive random slots a lane takes from the work queue at a time
+ *   and runs one after another (a power of two, 1..64): gg_set_transport_launch.
+ * gg_autotune times short runs of `source` (gg_autotune_jobs: of a batched
+ * launch of `jobs`, e.g. a sample of the job mix to run) over a coordinate
+ * search of these four knobs, keeps the fastest and reports its time; it
+ * restores the random states and zeroes the tallies afterwards, so call it
+ * before the real run.  The results do not depend on the launch shape. */
 GG_API int gg_set_transport_tuning(gg_context* context, int32_t blocks_per_sm, int32_t regroup_lanes,
                                    int32_t regroup_ratio4);
 GG_API int gg_get_transport_tuning(gg_context* context, int32_t* blocks_per_sm, int32_t* regroup_lanes,
                                    int32_t* regroup_ratio4);
+GG_API int gg_set_transport_launch(gg_context* context, int32_t block_threads, int32_t slots_per_claim);
+GG_API int gg_get_transport_launch(gg_context* context, int32_t* block_threads, int32_t* slots_per_claim);
 GG_API int gg_autotune(gg_context* context, const gg_source* source, uint64_t number_of_particles,
                        float* best_milliseconds);
+GG_API int gg_autotune_jobs(gg_context* context, const gg_job* jobs, int32_t number_of_jobs, float* best_milliseconds);
 
 /* ---- scatter surrogate (no counterpart in the reference) ----
  * A 4-level BF16 U-Net (base 32 channels, FP32 accumulation) mapping a CBCT
@@ -352,6 +367,27 @@ GG_API const char* gg_unet_last_error(void);
 /* Batch plan of GGEMSSource::OrganizeParticlesInBatch for one device.
  * Writes at most max_batches sizes; returns the number of batches in *count. */
 GG_API int gg_batch_plan(uint64_t number_of_particles, uint64_t* batch_sizes, int64_t max_batches, int64_t* count);
+
+/* ---- device tallies for collectives (no counterpart in the reference:
+ * GGEMSSystem::SaveResults and GGEMSDosimetryCalculator read every device's
+ * buffers back and sum them on the host) ----
+ * The device buffers that hold a context's tallies, in a fixed order
+ * (histograms; per dose map edep, edep^2, hit, photon tracking where
+ * recorded; world photon count, energy, energy^2, momentum where recorded),
+ * so that a multi-GPU run sums them across GPUs in place (one all-reduce per
+ * buffer, e.g. NCCL over NVLink) before gg_read_tallies.  Addresses stay
+ * valid until the next gg_upload_scene.  edep, world energy and momentum are
+ * int64 fixed point (LSB 2^-32 MeV): their sums are exact and do not depend
+ * on the order.  With tallies == NULL only *count is set. */
+#define GG_TALLY_INT32 0
+#define GG_TALLY_INT64 1
+#define GG_TALLY_FP64 2
+typedef struct gg_device_tally {
+  void* address;  /* device address */
+  int64_t count;  /* elements */
+  int32_t type;   /* GG_TALLY_* */
+} gg_device_tally;
+GG_API int gg_device_tallies(gg_context* context, gg_device_tally* tallies, int32_t capacity, int32_t* count);
 
 /* ---- dose finalisation (ComputeDoseGGEMSVoxelizedSolid.cl) ----
  * Converts the edep tally of dose_map (recorded inside solid) into Gy and the
