@@ -18,19 +18,6 @@ LIB = os.path.join(HERE, "libggems.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
-def _cute_include():
-    """CuTe / CUTLASS header tree (its sm100 UMMA descriptor definitions are
-    used by the tensor-core convolution); the copy that ships with flashinfer."""
-    import importlib.util
-    for pkg, sub in (("flashinfer", ("data", "cutlass", "include")), ("tilelang", ("3rdparty", "cutlass", "include"))):
-        spec = importlib.util.find_spec(pkg)
-        if spec and spec.submodule_search_locations:
-            path = os.path.join(spec.submodule_search_locations[0], *sub)
-            if os.path.exists(os.path.join(path, "cute", "arch", "mma_sm100_desc.hpp")):
-                return path
-    raise RuntimeError("CuTe headers (cute/arch/mma_sm100_desc.hpp) not found")
-
-
 NVCC = ["nvcc", "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include"),
         "-I" + CSRC] + ARCH
 # Host code: no fused multiply-add so host-side table building rounds like the reference's host build.
@@ -56,8 +43,7 @@ def build(verbose=False):
     for src in sorted(glob.glob(os.path.join(CSRC, "*.cu"))):
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
         if _newer(src, obj, headers):
-            cmd = NVCC + FMAD.get(os.path.basename(src), []) + ["-I" + _cute_include(), "-Xptxas", "-v", "-c", src,
-                                                                "-o", obj]
+            cmd = NVCC + FMAD.get(os.path.basename(src), []) + ["-Xptxas", "-v", "-c", src, "-o", obj]
             out = subprocess.run(cmd, capture_output=True, text=True)
             if out.returncode != 0:
                 raise RuntimeError("nvcc failed for %s:\n%s" % (src, out.stderr))

@@ -20,8 +20,8 @@
 //
 // Every mbarrier wait is bounded; a wait that gives up sets *error, the CTA
 // stops issuing work, waits (bounded) for the copies it started, frees its
-// TMEM and returns.  The shared-memory descriptors and the instruction
-// descriptor use CuTe's bitfield definitions (cute/arch/mma_sm100_desc.hpp).
+// TMEM and returns.  The shared-memory and instruction descriptors are
+// encoded by gg_umma_desc.cuh (the PTX ISA's bit layout).
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
@@ -31,7 +31,7 @@
 #include <cstdlib>
 #include <cstring>
 
-#include <cute/arch/mma_sm100_desc.hpp>
+#include "gg_umma_desc.cuh"
 
 #include "gg_unet_umma.cuh"
 
@@ -114,18 +114,8 @@ __device__ __forceinline__ void tmem_load_32(uint32_t taddr, float (&v)[32]) {
 // K-major operand tile of `rows` rows of `row_bytes` (32, 64 or 128) bytes,
 // swizzled over the row length, 8-row groups `8 * row_bytes` apart.
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, int row_bytes) {
-  cute::UMMA::SmemDescriptor d;
-  d.desc_ = 0;
-  d.start_address_ = static_cast<uint16_t>(addr >> 4);
-  d.leading_byte_offset_ = 1;
-  d.stride_byte_offset_ = static_cast<uint16_t>((8 * row_bytes) >> 4);
-  d.version_ = 1;
-  d.base_offset_ = 0;
-  d.lbo_mode_ = 0;
-  d.layout_type_ = static_cast<uint8_t>(row_bytes == 128 ? cute::UMMA::LayoutType::SWIZZLE_128B
-                                        : row_bytes == 64 ? cute::UMMA::LayoutType::SWIZZLE_64B
-                                                          : cute::UMMA::LayoutType::SWIZZLE_32B);
-  return d.desc_;
+  // leading byte offset unused by swizzled K-major tiles (encoded as 1 unit)
+  return gg::umma_smem_desc(addr, 16, 8 * row_bytes, gg::umma_row_swizzle(row_bytes));
 }
 
 template <int kMode>
@@ -268,18 +258,7 @@ __device__ __forceinline__ void tmem_load_16(uint32_t taddr, float (&v)[16]) {
 // (32/64/128-byte rows, swizzled over that length), 8-row groups 16 * atom
 // bytes apart, successive channel atoms `lbo` bytes apart.
 __device__ __forceinline__ uint64_t smem_desc_mn(uint32_t addr, int atom, uint32_t lbo) {
-  cute::UMMA::SmemDescriptor d;
-  d.desc_ = 0;
-  d.start_address_ = static_cast<uint16_t>(addr >> 4);
-  d.leading_byte_offset_ = static_cast<uint16_t>(lbo >> 4);
-  d.stride_byte_offset_ = static_cast<uint16_t>((8 * atom * 2) >> 4);
-  d.version_ = 1;
-  d.base_offset_ = 0;
-  d.lbo_mode_ = 0;
-  d.layout_type_ = static_cast<uint8_t>(atom == 64 ? cute::UMMA::LayoutType::SWIZZLE_128B
-                                        : atom == 32 ? cute::UMMA::LayoutType::SWIZZLE_64B
-                                                     : cute::UMMA::LayoutType::SWIZZLE_32B);
-  return d.desc_;
+  return gg::umma_smem_desc(addr, lbo, 8 * atom * 2, gg::umma_row_swizzle(2 * atom));
 }
 
 constexpr int kChunk = 64;               // pixels per reduction chunk
@@ -485,16 +464,7 @@ const char* make_plan(ConvPlan* p, const void* x, const void* w, int batch, int 
   const size_t tmem_cap_smem = 228 * 1024 / (512 / a.tmem_cols + 1) + 1;
   if (p->smem < tmem_cap_smem) p->smem = tmem_cap_smem;
   // instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128, N = n_tile
-  cute::UMMA::InstrDescriptor id;
-  id.desc_ = 0;
-  id.c_format_ = 1;  // F32
-  id.a_format_ = 1;  // BF16
-  id.b_format_ = 1;  // BF16
-  id.a_major_ = 0;
-  id.b_major_ = 0;
-  id.n_dim_ = static_cast<uint16_t>(a.n_tile >> 3);
-  id.m_dim_ = static_cast<uint16_t>(128 >> 4);
-  a.idesc = id.desc_;
+  a.idesc = gg::umma_idesc_bf16_f32(128, a.n_tile, false, false);
   // activation boxes: 128 pixels as whole rows, or whole images
   const int bw = width < 128 ? width : 128;
   const int bh = (128 / bw) < height ? 128 / bw : height;
@@ -570,16 +540,8 @@ const char* make_wgrad_plan(WgradPlan* p, const void* x, const void* dy, int bat
   const size_t tmem_cap_smem = 228 * 1024 / (512 / a.tmem_cols + 1) + 1;
   if (p->smem < tmem_cap_smem) p->smem = tmem_cap_smem;
   if (p->smem > 227 * 1024) return "operand tiles do not fit in shared memory";
-  cute::UMMA::InstrDescriptor id;
-  id.desc_ = 0;
-  id.c_format_ = 1;  // F32
-  id.a_format_ = 1;  // BF16
-  id.b_format_ = 1;  // BF16
-  id.a_major_ = 1;   // MN-major: channels contiguous, pixels (the reduction) strided
-  id.b_major_ = 1;
-  id.n_dim_ = static_cast<uint16_t>(a.n_tile >> 3);
-  id.m_dim_ = static_cast<uint16_t>(128 >> 4);
-  a.idesc = id.desc_;
+  // MN-major: channels contiguous, pixels (the reduction) strided
+  a.idesc = gg::umma_idesc_bf16_f32(128, a.n_tile, true, true);
   // 64-pixel boxes: a run of one row, or whole rows
   const int bw = width < kChunk ? width : kChunk;
   const int bh = (kChunk / bw) < height ? kChunk / bw : height;

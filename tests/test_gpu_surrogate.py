@@ -177,27 +177,40 @@ def test_surrogate_beats_low_count_mc(geometry, torch):
     net.close()
 
 
-def test_committed_network_predicts_new_phantoms(geometry, torch):
+def test_committed_network_predicts_new_phantoms(tmp_path):
     """The trained network shipped with the package (ggems_b200/data/
     unet_scatter256.npz, loaded by bench.py's surrogate measurement) at its own
     size: on new phantoms at random angles its scatter projection is within 3 %
     of the truth on the 16x16 block grid and within 6 % per element at full
     resolution (errors against 2e8-primary MC references with the references'
-    own counting noise removed)."""
-    import tempfile
-    from ggems_b200 import scatter as S
-    geo = S.Geometry(256, tempfile.mkdtemp())
-    net = S.UNet(4, 256, seed=1)
-    S.load_network(net, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "ggems_b200",
-                                     "data", "unet_scatter256.npz"))
-    rng = np.random.default_rng(31)
-    projs = [(float(rng.uniform(0, 360)), S.random_phantom(rng)) for _ in range(4)]
-    n_ref = 200_000_000
-    _, s_ref = geo.simulate(projs, n_ref, seed=77)
-    ref = S.normalise(s_ref, n_ref, 256)
-    pred = S.predict(net, S.make_inputs(geo, projs))
-    err = S._summary(S._errors(pred, ref, n_ref))
+    own counting noise removed).  In a process of its own: the GGEMS API's
+    managers are process-wide and this module's fixture holds a 64^2 geometry."""
+    import subprocess
+    import textwrap
+    code = textwrap.dedent(r'''
+        import json, os, sys, tempfile
+        import numpy as np
+        import torch
+        from ggems_b200 import scatter as S
+        geo = S.Geometry(256, tempfile.mkdtemp())
+        net = S.UNet(4, 256, seed=1)
+        S.load_network(net, os.path.join(sys.argv[1], "ggems_b200", "data", "unet_scatter256.npz"))
+        rng = np.random.default_rng(31)
+        projs = [(float(rng.uniform(0, 360)), S.random_phantom(rng)) for _ in range(4)]
+        n_ref = 200_000_000
+        _, s_ref = geo.simulate(projs, n_ref, seed=77)
+        ref = S.normalise(s_ref, n_ref, 256)
+        pred = S.predict(net, S.make_inputs(geo, projs))
+        print(json.dumps(S._summary(S._errors(pred, ref, n_ref))))
+        net.close()
+    ''')
+    (tmp_path / "case.py").write_text(code)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, str(tmp_path / "case.py"), root], capture_output=True, text=True,
+                         timeout=600, env=dict(os.environ, PYTHONPATH=root))
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-3000:]
+    import json
+    err = json.loads(out.stdout.strip().splitlines()[-1])
     print("committed network on 4 new phantoms:", err)
     assert err["blocks16"]["mean"] < 0.03
     assert err["full"]["mean"] < 0.06
-    net.close()
