@@ -385,11 +385,13 @@ def main():
     # ranks < r (device order of GGEMSPseudoRandomGenerator), set just below.
     ggems.initialize(777)
     ctx = lib.ggems_device_context(ggems.obj, 0)
+    import numpy as np
+    rank_states = None  # this rank's initial streams (rank 0: GGEMS's own seeding above)
     if rank > 0:
-        import numpy as np
-        st = np.zeros(5 * abi.GG_MAXIMUM_PARTICLES, np.uint32)
-        lib.gg_seed_random_states(abi.ptr(st, C.c_uint32), abi.GG_MAXIMUM_PARTICLES, 777, rank * abi.GG_MAXIMUM_PARTICLES)
-        lib.gg_set_random_states(ctx, abi.ptr(st, C.c_uint32), abi.GG_MAXIMUM_PARTICLES)
+        rank_states = np.zeros(5 * abi.GG_MAXIMUM_PARTICLES, np.uint32)
+        lib.gg_seed_random_states(abi.ptr(rank_states, C.c_uint32), abi.GG_MAXIMUM_PARTICLES, 777,
+                                  rank * abi.GG_MAXIMUM_PARTICLES)
+        lib.gg_set_random_states(ctx, abi.ptr(rank_states, C.c_uint32), abi.GG_MAXIMUM_PARTICLES)
     src = abi.gg_source()
     n_src = C.c_uint64()
     assert lib.ggems_source_descriptor(0, C.byref(src), C.byref(n_src)) == 0
@@ -436,12 +438,11 @@ def main():
     value = world * args.primaries * args.steps / (total_ms * 1e-3)
 
     # ---- end to end through the C ABI: host scene -> device, run, tallies -> host ----
-    import numpy as np
     sc = scene_ptr.contents
     hs = [int(sc.histogram_sizes[i]) for i in range(sc.number_of_histograms)]
     tallies = abi.Tallies(hs, [])
-    states = np.frombuffer(C.string_at(lib.ggems_initial_random_states(ggems.obj, 0),
-                                       5 * abi.GG_MAXIMUM_PARTICLES * 4), np.uint32).copy()
+    states = rank_states if rank_states is not None else np.frombuffer(
+        C.string_at(lib.ggems_initial_random_states(ggems.obj, 0), 5 * abi.GG_MAXIMUM_PARTICLES * 4), np.uint32).copy()
     h2d = sum(int(sc.solids[i].number_of_voxels[0]) * sc.solids[i].number_of_voxels[1] * sc.solids[i].number_of_voxels[2]
               for i in range(sc.number_of_solids) if sc.solids[i].type == abi.GG_SOLID_VOXELIZED)
     for i in range(sc.number_of_tables):

@@ -71,6 +71,10 @@ struct gg_context {
   std::map<void*, size_t> scene_bytes;
   std::vector<std::pair<void*, size_t>> scene_spares;
   std::vector<void*> run_allocations;    // source arrays of the last run
+  // gg_compute_dose's device outputs, grown on demand and kept: a cudaFree per
+  // call would synchronise the whole device
+  float* dose_out = nullptr;
+  size_t dose_out_floats = 0;
   gg::DevSolid* solids = nullptr;
   int number_of_solids = 0;
   gg::DevNavigator* navigators = nullptr;
@@ -532,6 +536,7 @@ GG_API int gg_context_destroy(gg_context* c) {
   cudaFree(c->particles.solid_id);
   cudaFree(c->slot_counter);
   cudaFree(c->error);
+  if (c->dose_out) cudaFree(c->dose_out);
   if (c->start) cudaEventDestroy(c->start);
   if (c->stop) cudaEventDestroy(c->stop);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -1432,22 +1437,22 @@ GG_API int gg_compute_dose(gg_context* c, int32_t dose_map, int32_t solid, float
   P.is_water_reference = is_water_reference;
   P.minimum_density = minimum_density;
   const size_t n = static_cast<size_t>(P.map.total_number_of_dosels);
-  float* d_dose = nullptr;
-  float* d_unc = nullptr;
-  GG_CUDA(cudaMalloc(&d_dose, n * 4));
-  if (uncertainty && cudaMalloc(&d_unc, n * 4) != cudaSuccess) {
-    cudaFree(d_dose);
-    return fail(GG_ERROR_OUT_OF_MEMORY, "uncertainty buffer");
+  if (c->dose_out_floats < 2 * n) {  // grow once; later calls reuse the buffer
+    GG_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->dose_out) cudaFree(c->dose_out);
+    c->dose_out = nullptr;
+    c->dose_out_floats = 0;
+    if (cudaMalloc(&c->dose_out, 2 * n * sizeof(float)) != cudaSuccess)
+      return fail(GG_ERROR_OUT_OF_MEMORY, "dose output buffer");
+    c->dose_out_floats = 2 * n;
   }
-  P.dose = d_dose;
-  P.uncertainty = d_unc;
+  P.dose = c->dose_out;
+  P.uncertainty = uncertainty ? c->dose_out + n : nullptr;
   gg::launch_compute_dose(P, c->stream);
   cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaMemcpyAsync(dose, d_dose, n * 4, cudaMemcpyDeviceToHost, c->stream);
-  if (e == cudaSuccess && uncertainty) e = cudaMemcpyAsync(uncertainty, d_unc, n * 4, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dose, P.dose, n * 4, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && uncertainty) e = cudaMemcpyAsync(uncertainty, P.uncertainty, n * 4, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  cudaFree(d_dose);
-  if (d_unc) cudaFree(d_unc);
   if (e != cudaSuccess) return fail(GG_ERROR_CUDA, std::string("compute dose: ") + cudaGetErrorString(e));
   return GG_OK;
 }

@@ -91,25 +91,33 @@ __global__ void sat_rows_kernel(const float* __restrict__ in, double* __restrict
   }
 }
 
-// Pass 2: one thread per column (coalesced across threads), prefix sums down the
-// column, the next rows' loads issued ahead of the dependent additions.
+// Pass 2: prefix sums down the columns.  A block takes 32 adjacent columns
+// (coalesced) and splits each into kSatSegments segments of S / kSatSegments
+// rows, one thread per segment: each thread sums its segment, the block adds
+// the sums of the segments above it, and each thread writes its segment's
+// running sums.  (One thread per column left most SMs idle: 4096 threads.)
+constexpr int kSatSegments = 8;
 __global__ void sat_cols_kernel(double* __restrict__ sat, int batch, int S) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // (b, m, x)
-  if (t >= batch * 2 * S) return;
+  __shared__ double seg_sum[kSatSegments][32];
+  const int cx = threadIdx.x & 31, seg = threadIdx.x >> 5;  // blockDim = 32 * kSatSegments
+  const int t = blockIdx.x * 32 + cx;                         // (b, m, x) column
+  const bool valid = t < batch * 2 * S;
   const int x = t % S, bm = t / S;
-  double* col = sat + static_cast<size_t>(bm) * (S + 1) * (S + 1) + x + 1;
   const size_t W = S + 1;
+  const int rows = S / kSatSegments;
+  double* col = sat + static_cast<size_t>(bm) * W * W + x + 1 + static_cast<size_t>(1 + seg * rows) * W;
+  double local = 0.0;
+  if (valid)
+    for (int y = 0; y < rows; ++y) local += col[static_cast<size_t>(y) * W];
+  seg_sum[seg][cx] = local;
+  __syncthreads();
   double acc = 0.0;
-  for (int y = 1; y <= S; y += 8) {
-    double v[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = col[static_cast<size_t>(y + k) * W];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      acc += v[k];
-      col[static_cast<size_t>(y + k) * W] = acc;
+  for (int k = 0; k < seg; ++k) acc += seg_sum[k][cx];
+  if (valid)
+    for (int y = 0; y < rows; ++y) {
+      acc += col[static_cast<size_t>(y) * W];
+      col[static_cast<size_t>(y) * W] = acc;
     }
-  }
 }
 
 __device__ __forceinline__ double box_sum(const double* I, int S, int x, int y, int r) {
@@ -143,77 +151,116 @@ __global__ void pack_input_kernel(const float* __restrict__ in, const double* __
   dst[1] = *reinterpret_cast<uint4*>(v + 8);
 }
 
-// 2x2 average pool, NHWC
+// 8 BF16 channels moved as one 16-byte vector
+struct alignas(16) Bf16x8 {
+  bf16 v[8];
+};
+
+// 2x2 average pool, NHWC; each thread 8 channels (c is a multiple of 8)
 __global__ void pool_kernel(const bf16* __restrict__ x, bf16* __restrict__ y, int batch, int h, int w, int c) {
-  const size_t n = static_cast<size_t>(batch) * (h / 2) * (w / 2) * c;
+  const int c8 = c / 8;
+  const size_t n = static_cast<size_t>(batch) * (h / 2) * (w / 2) * c8;
+  const Bf16x8* X = reinterpret_cast<const Bf16x8*>(x);
+  Bf16x8* Y = reinterpret_cast<Bf16x8*>(y);
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    const int ch = i % c;
-    size_t r = i / c;
+    const int ch8 = i % c8;
+    size_t r = i / c8;
     const int ox = r % (w / 2);
     r /= (w / 2);
     const int oy = r % (h / 2);
     const int b = static_cast<int>(r / (h / 2));
-    const size_t base = ((static_cast<size_t>(b) * h + 2 * oy) * w + 2 * ox) * c + ch;
-    const float s = __bfloat162float(x[base]) + __bfloat162float(x[base + c]) + __bfloat162float(x[base + static_cast<size_t>(w) * c]) +
-                    __bfloat162float(x[base + static_cast<size_t>(w) * c + c]);
-    y[i] = __float2bfloat16(0.25f * s);
+    const size_t base = ((static_cast<size_t>(b) * h + 2 * oy) * w + 2 * ox) * c8 + ch8;
+    const Bf16x8 a = X[base], bb = X[base + c8], cc = X[base + static_cast<size_t>(w) * c8],
+                 d = X[base + static_cast<size_t>(w) * c8 + c8];
+    Bf16x8 o;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const float s = __bfloat162float(a.v[k]) + __bfloat162float(bb.v[k]) + __bfloat162float(cc.v[k]) +
+                      __bfloat162float(d.v[k]);
+      o.v[k] = __float2bfloat16(0.25f * s);
+    }
+    Y[i] = o;
   }
 }
 
-// gradient of the pool: dx (FP32, h x w) += dy / 4 (dy at h/2 x w/2)
+// gradient of the pool: dx (FP32, h x w) += dy / 4 (dy at h/2 x w/2); 4 channels per thread
 __global__ void pool_backward_kernel(const float* __restrict__ dy, float* __restrict__ dx, int batch, int h, int w, int c) {
-  const size_t n = static_cast<size_t>(batch) * h * w * c;
+  const int c4 = c / 4;
+  const size_t n = static_cast<size_t>(batch) * h * w * c4;
+  const float4* DY = reinterpret_cast<const float4*>(dy);
+  float4* DX = reinterpret_cast<float4*>(dx);
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    const int ch = i % c;
-    size_t r = i / c;
+    const int ch4 = i % c4;
+    size_t r = i / c4;
     const int x = r % w;
     r /= w;
     const int y = r % h;
     const int b = static_cast<int>(r / h);
-    dx[i] += 0.25f * dy[((static_cast<size_t>(b) * (h / 2) + y / 2) * (w / 2) + x / 2) * c + ch];
+    const float4 g = DY[((static_cast<size_t>(b) * (h / 2) + y / 2) * (w / 2) + x / 2) * c4 + ch4];
+    float4 d = DX[i];
+    d.x += 0.25f * g.x;
+    d.y += 0.25f * g.y;
+    d.z += 0.25f * g.z;
+    d.w += 0.25f * g.w;
+    DX[i] = d;
   }
 }
 
-// concat(up2(a) [c1 channels, h/2 x w/2], skip [c2 channels, h x w]) -> y [c1 + c2, h x w]
+// concat(up2(a) [c1 channels, h/2 x w/2], skip [c2 channels, h x w]) -> y [c1 + c2, h x w];
+// each thread copies 8 channels (c1 and c2 are multiples of 8)
 __global__ void up_concat_kernel(const bf16* __restrict__ a, const bf16* __restrict__ skip, bf16* __restrict__ y, int batch,
                                  int h, int w, int c1, int c2) {
-  const int c = c1 + c2;
-  const size_t n = static_cast<size_t>(batch) * h * w * c;
+  const int a8 = c1 / 8, s8 = c2 / 8, c8 = a8 + s8;
+  const size_t n = static_cast<size_t>(batch) * h * w * c8;
+  const Bf16x8* A = reinterpret_cast<const Bf16x8*>(a);
+  const Bf16x8* K = reinterpret_cast<const Bf16x8*>(skip);
+  Bf16x8* Y = reinterpret_cast<Bf16x8*>(y);
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    const int ch = i % c;
-    const size_t p = i / c;
+    const int ch8 = i % c8;
+    const size_t p = i / c8;
     const int x = p % w;
     const size_t r = p / w;
     const int yy = r % h;
     const int b = static_cast<int>(r / h);
-    y[i] = ch < c1 ? a[((static_cast<size_t>(b) * (h / 2) + yy / 2) * (w / 2) + x / 2) * c1 + ch]
-                   : skip[p * c2 + (ch - c1)];
+    Y[i] = ch8 < a8 ? A[((static_cast<size_t>(b) * (h / 2) + yy / 2) * (w / 2) + x / 2) * a8 + ch8]
+                    : K[p * s8 + (ch8 - a8)];
   }
 }
 
-// gradient of up_concat: da (h/2 x w/2, FP32) = sum of the 2x2 block; dskip = (zero ? set : add)
+// gradient of up_concat: da (h/2 x w/2, FP32) = sum of the 2x2 block; dskip = (zero ? set : add);
+// 4 channels per thread (c1 and c2 are multiples of 4)
 __global__ void up_concat_backward_kernel(const float* __restrict__ dy, float* __restrict__ da, float* __restrict__ dskip,
                                           int batch, int h, int w, int c1, int c2, int skip_set) {
-  const int c = c1 + c2;
-  const size_t na = static_cast<size_t>(batch) * (h / 2) * (w / 2) * c1;
-  const size_t ns = static_cast<size_t>(batch) * h * w * c2;
+  const int a4 = c1 / 4, s4 = c2 / 4, c4 = a4 + s4;
+  const size_t na = static_cast<size_t>(batch) * (h / 2) * (w / 2) * a4;
+  const size_t ns = static_cast<size_t>(batch) * h * w * s4;
   const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+  const float4* DY = reinterpret_cast<const float4*>(dy);
+  float4* DA = reinterpret_cast<float4*>(da);
+  float4* DS = reinterpret_cast<float4*>(dskip);
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < na + ns; i += stride) {
     if (i < na) {
-      const int ch = i % c1;
-      size_t r = i / c1;
+      const int ch4 = i % a4;
+      size_t r = i / a4;
       const int ox = r % (w / 2);
       r /= (w / 2);
       const int oy = r % (h / 2);
       const int b = static_cast<int>(r / (h / 2));
-      const size_t base = ((static_cast<size_t>(b) * h + 2 * oy) * w + 2 * ox) * c + ch;
-      da[i] = dy[base] + dy[base + c] + dy[base + static_cast<size_t>(w) * c] + dy[base + static_cast<size_t>(w) * c + c];
+      const size_t base = ((static_cast<size_t>(b) * h + 2 * oy) * w + 2 * ox) * c4 + ch4;
+      const float4 p = DY[base], q = DY[base + c4], u = DY[base + static_cast<size_t>(w) * c4],
+                   v = DY[base + static_cast<size_t>(w) * c4 + c4];
+      DA[i] = make_float4(p.x + q.x + u.x + v.x, p.y + q.y + u.y + v.y, p.z + q.z + u.z + v.z, p.w + q.w + u.w + v.w);
     } else {
       const size_t j = i - na;
-      const int ch = j % c2;
-      const size_t p = j / c2;
-      const float v = dy[p * c + c1 + ch];
-      dskip[j] = skip_set ? v : dskip[j] + v;
+      const int ch4 = j % s4;
+      const size_t px = j / s4;
+      const float4 g = DY[px * c4 + a4 + ch4];
+      if (skip_set) {
+        DS[j] = g;
+      } else {
+        float4 d = DS[j];
+        DS[j] = make_float4(d.x + g.x, d.y + g.y, d.z + g.z, d.w + g.w);
+      }
     }
   }
 }
@@ -221,8 +268,20 @@ __global__ void up_concat_backward_kernel(const float* __restrict__ dy, float* _
 // relu gradient: dpre (BF16) = dact * (act > 0)
 __global__ void relu_backward_kernel(const float* __restrict__ dact, const bf16* __restrict__ act, bf16* __restrict__ dpre,
                                      size_t n) {
-  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x)
-    dpre[i] = __float2bfloat16(__bfloat162float(act[i]) > 0.0f ? dact[i] : 0.0f);
+  // 8 elements per thread (n is a multiple of 8: whole pixels of >= 32 channels)
+  const Bf16x8* A = reinterpret_cast<const Bf16x8*>(act);
+  const float4* D = reinterpret_cast<const float4*>(dact);
+  Bf16x8* O = reinterpret_cast<Bf16x8*>(dpre);
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n / 8;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const Bf16x8 a = A[i];
+    const float4 d0 = D[2 * i], d1 = D[2 * i + 1];
+    const float d[8] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
+    Bf16x8 o;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) o.v[k] = __float2bfloat16(__bfloat162float(a.v[k]) > 0.0f ? d[k] : 0.0f);
+    O[i] = o;
+  }
 }
 
 // bias gradient: db[c] += sum_p dpre[p][c]
@@ -240,8 +299,13 @@ __global__ void out_forward_kernel(const bf16* __restrict__ a, const float* __re
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= pixels) return;
   float s = b[0];
+  const Bf16x8* row = reinterpret_cast<const Bf16x8*>(a + static_cast<size_t>(p) * 32);
 #pragma unroll
-  for (int c = 0; c < 32; ++c) s += __bfloat162float(a[static_cast<size_t>(p) * 32 + c]) * w[c];
+  for (int q = 0; q < 4; ++q) {
+    const Bf16x8 v = row[q];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += __bfloat162float(v.v[k]) * w[8 * q + k];
+  }
   y[p] = s;
 }
 
@@ -304,14 +368,29 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, 
 
 // BF16 copies of a 3x3 layer's weights: w [tap][co][ci] and the flipped /
 // transposed wt [tap][ci][co] = w[8 - tap][co][ci]
-__global__ void cast_weights_kernel(const float* __restrict__ w32, bf16* __restrict__ w, bf16* __restrict__ wt, int cout,
-                                    int cin) {
-  const int n = 9 * cout * cin;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+// The BF16 copies of every layer's 3x3 weights ([9][cout][cin], and the
+// transposed, tap-flipped [9][cin][cout] the data gradient uses), all layers in
+// one launch: `start` is the running weight count, layer by layer.
+constexpr int kCastLayers = 14;
+struct CastTable {
+  const float* w32[kCastLayers];
+  bf16* w[kCastLayers];
+  bf16* wt[kCastLayers];
+  int cout[kCastLayers];
+  int cin[kCastLayers];
+  int start[kCastLayers + 1];
+};
+
+__global__ void cast_weights_kernel(const __grid_constant__ CastTable T) {
+  const int total = T.start[kCastLayers];
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    int l = 0;
+    while (g >= T.start[l + 1]) ++l;
+    const int i = g - T.start[l], cin = T.cin[l], cout = T.cout[l];
     const int ci = i % cin, r = i / cin, co = r % cout, tap = r / cout;
-    const bf16 v = __float2bfloat16(w32[i]);
-    w[i] = v;
-    wt[(static_cast<size_t>(8 - tap) * cin + ci) * cout + co] = v;
+    const bf16 v = __float2bfloat16(T.w32[l][i]);
+    T.w[l][i] = v;
+    T.wt[l][(static_cast<size_t>(8 - tap) * cin + ci) * cout + co] = v;
   }
 }
 
@@ -405,17 +484,17 @@ int forward(gg_unet* n, const float* input) {
   const int B = n->batch, S = n->size;
   const int pixels = B * S * S;
   sat_rows_kernel<<<(B * 2 * S * 32 + 255) / 256, 256, 0, n->stream>>>(input, n->sat, B, S);
-  sat_cols_kernel<<<(B * 2 * S + 127) / 128, 128, 0, n->stream>>>(n->sat, B, S);
+  sat_cols_kernel<<<(B * 2 * S + 31) / 32, 32 * kSatSegments, 0, n->stream>>>(n->sat, B, S);
   pack_input_kernel<<<(pixels + 255) / 256, 256, 0, n->stream>>>(input, n->sat, n->x0, B, S);
   auto& L = n->layers;
   int rc;
   for (int i = 0; i < 14; ++i) {
-    if (i == 2) pool_kernel<<<grid_for(static_cast<size_t>(B) * S * S / 4 * 32), 256, 0, n->stream>>>(L[1].act, n->pool1, B, S, S, 32);
-    if (i == 4) pool_kernel<<<grid_for(static_cast<size_t>(B) * S * S / 16 * 64), 256, 0, n->stream>>>(L[3].act, n->pool2, B, S / 2, S / 2, 64);
-    if (i == 6) pool_kernel<<<grid_for(static_cast<size_t>(B) * S * S / 64 * 128), 256, 0, n->stream>>>(L[5].act, n->pool3, B, S / 4, S / 4, 128);
-    if (i == 8) up_concat_kernel<<<grid_for(static_cast<size_t>(B) * (S / 4) * (S / 4) * 384), 256, 0, n->stream>>>(L[7].act, L[5].act, n->cat8, B, S / 4, S / 4, 256, 128);
-    if (i == 10) up_concat_kernel<<<grid_for(static_cast<size_t>(B) * (S / 2) * (S / 2) * 192), 256, 0, n->stream>>>(L[9].act, L[3].act, n->cat10, B, S / 2, S / 2, 128, 64);
-    if (i == 12) up_concat_kernel<<<grid_for(static_cast<size_t>(B) * S * S * 96), 256, 0, n->stream>>>(L[11].act, L[1].act, n->cat12, B, S, S, 64, 32);
+    if (i == 2) pool_kernel<<<grid_for(static_cast<size_t>(B) * S * S / 4 * 32 / 8), 256, 0, n->stream>>>(L[1].act, n->pool1, B, S, S, 32);
+    if (i == 4) pool_kernel<<<grid_for(static_cast<size_t>(B) * S * S / 16 * 64 / 8), 256, 0, n->stream>>>(L[3].act, n->pool2, B, S / 2, S / 2, 64);
+    if (i == 6) pool_kernel<<<grid_for(static_cast<size_t>(B) * S * S / 64 * 128 / 8), 256, 0, n->stream>>>(L[5].act, n->pool3, B, S / 4, S / 4, 128);
+    if (i == 8) up_concat_kernel<<<grid_for(static_cast<size_t>(B) * (S / 4) * (S / 4) * 384 / 8), 256, 0, n->stream>>>(L[7].act, L[5].act, n->cat8, B, S / 4, S / 4, 256, 128);
+    if (i == 10) up_concat_kernel<<<grid_for(static_cast<size_t>(B) * (S / 2) * (S / 2) * 192 / 8), 256, 0, n->stream>>>(L[9].act, L[3].act, n->cat10, B, S / 2, S / 2, 128, 64);
+    if (i == 12) up_concat_kernel<<<grid_for(static_cast<size_t>(B) * S * S * 96 / 8), 256, 0, n->stream>>>(L[11].act, L[1].act, n->cat12, B, S, S, 64, 32);
     if ((rc = run_conv(n, L[i], 0, L[i].act))) return rc;
   }
   out_forward_kernel<<<(pixels + 255) / 256, 256, 0, n->stream>>>(L[13].act, n->params + n->out_w_off,
@@ -438,7 +517,7 @@ int backward(gg_unet* n, const float* target) {
     const auto& l = L[i];
     const int px = B * l.side * l.side;
     const size_t na = static_cast<size_t>(px) * l.cout;
-    relu_backward_kernel<<<grid_for(na), 256, 0, n->stream>>>(l.dact, l.act, l.dpre, na);
+    relu_backward_kernel<<<grid_for(na / 8), 256, 0, n->stream>>>(l.dact, l.act, l.dpre, na);
     bias_grad_kernel<<<dim3(std::min(px, 1024), (l.cout + 127) / 128), 128, 0, n->stream>>>(l.dpre, n->grads + l.b_off, px, l.cout);
     UNET_CUDA(gg_umma::launch_wgrad(l.wgrad, n->grads + l.w_off, n->conv_error, n->stream));
     if (i == 0) break;
@@ -447,21 +526,30 @@ int backward(gg_unet* n, const float* target) {
               : (i == 2) ? n->dpool1 : (i == 4) ? n->dpool2 : (i == 6) ? n->dpool3 : L[i - 1].dact;
     int rc;
     if ((rc = run_conv(n, l, 1, dx))) return rc;
-    if (i == 12) up_concat_backward_kernel<<<grid_for(static_cast<size_t>(px) * 96), 256, 0, n->stream>>>(n->dcat12, L[11].dact, L[1].dact, B, S, S, 64, 32, 1);
-    if (i == 10) up_concat_backward_kernel<<<grid_for(static_cast<size_t>(px) * 192), 256, 0, n->stream>>>(n->dcat10, L[9].dact, L[3].dact, B, S / 2, S / 2, 128, 64, 1);
-    if (i == 8) up_concat_backward_kernel<<<grid_for(static_cast<size_t>(px) * 384), 256, 0, n->stream>>>(n->dcat8, L[7].dact, L[5].dact, B, S / 4, S / 4, 256, 128, 1);
-    if (i == 6) pool_backward_kernel<<<grid_for(static_cast<size_t>(B) * (S / 4) * (S / 4) * 128), 256, 0, n->stream>>>(n->dpool3, L[5].dact, B, S / 4, S / 4, 128);
-    if (i == 4) pool_backward_kernel<<<grid_for(static_cast<size_t>(B) * (S / 2) * (S / 2) * 64), 256, 0, n->stream>>>(n->dpool2, L[3].dact, B, S / 2, S / 2, 64);
-    if (i == 2) pool_backward_kernel<<<grid_for(static_cast<size_t>(B) * S * S * 32), 256, 0, n->stream>>>(n->dpool1, L[1].dact, B, S, S, 32);
+    if (i == 12) up_concat_backward_kernel<<<grid_for(static_cast<size_t>(px) * 96 / 4), 256, 0, n->stream>>>(n->dcat12, L[11].dact, L[1].dact, B, S, S, 64, 32, 1);
+    if (i == 10) up_concat_backward_kernel<<<grid_for(static_cast<size_t>(px) * 192 / 4), 256, 0, n->stream>>>(n->dcat10, L[9].dact, L[3].dact, B, S / 2, S / 2, 128, 64, 1);
+    if (i == 8) up_concat_backward_kernel<<<grid_for(static_cast<size_t>(px) * 384 / 4), 256, 0, n->stream>>>(n->dcat8, L[7].dact, L[5].dact, B, S / 4, S / 4, 256, 128, 1);
+    if (i == 6) pool_backward_kernel<<<grid_for(static_cast<size_t>(B) * (S / 4) * (S / 4) * 128 / 4), 256, 0, n->stream>>>(n->dpool3, L[5].dact, B, S / 4, S / 4, 128);
+    if (i == 4) pool_backward_kernel<<<grid_for(static_cast<size_t>(B) * (S / 2) * (S / 2) * 64 / 4), 256, 0, n->stream>>>(n->dpool2, L[3].dact, B, S / 2, S / 2, 64);
+    if (i == 2) pool_backward_kernel<<<grid_for(static_cast<size_t>(B) * S * S * 32 / 4), 256, 0, n->stream>>>(n->dpool1, L[1].dact, B, S, S, 32);
     UNET_CUDA(cudaGetLastError());
   }
   return GG_OK;
 }
 
 int refresh_weights(gg_unet* n) {
-  for (auto& l : n->layers)
-    cast_weights_kernel<<<grid_for(9 * static_cast<size_t>(l.cout) * l.cin), 256, 0, n->stream>>>(n->params + l.w_off, l.w, l.wt,
-                                                                                                  l.cout, l.cin);
+  CastTable T{};
+  T.start[0] = 0;
+  for (int i = 0; i < kCastLayers; ++i) {
+    const auto& l = n->layers[i];
+    T.w32[i] = n->params + l.w_off;
+    T.w[i] = l.w;
+    T.wt[i] = l.wt;
+    T.cout[i] = l.cout;
+    T.cin[i] = l.cin;
+    T.start[i + 1] = T.start[i] + 9 * l.cout * l.cin;
+  }
+  cast_weights_kernel<<<grid_for(static_cast<size_t>(T.start[kCastLayers])), 256, 0, n->stream>>>(T);
   UNET_CUDA(cudaGetLastError());
   return GG_OK;
 }
