@@ -284,13 +284,32 @@ __global__ void relu_backward_kernel(const float* __restrict__ dact, const bf16*
   }
 }
 
-// bias gradient: db[c] += sum_p dpre[p][c]
+// bias gradient: db[c] += sum_p dpre[p][c].  A block takes every
+// gridDim.x-th group of pixels: its threads read 8 channels each (16-byte
+// loads, c / 8 threads per pixel, 256 / (c / 8) pixels at a time), sum over
+// their pixels in registers, then the block adds its pixel groups in shared
+// memory and issues one atomic per channel.
+constexpr int kBiasThreads = 256;
 __global__ void bias_grad_kernel(const bf16* __restrict__ dpre, float* __restrict__ db, int pixels, int c) {
-  const int ch = blockIdx.y * blockDim.x + threadIdx.x;
-  if (ch >= c) return;
-  float s = 0.0f;
-  for (int p = blockIdx.x; p < pixels; p += gridDim.x) s += __bfloat162float(dpre[static_cast<size_t>(p) * c + ch]);
-  atomicAdd(db + ch, s);
+  __shared__ float part[kBiasThreads * 8];  // [groups][c], groups * c = 8 * kBiasThreads
+  const int c8 = c / 8;                      // divides kBiasThreads (c = 32 ... 256)
+  const int groups = kBiasThreads / c8;
+  const int g = threadIdx.x / c8, v = threadIdx.x % c8;
+  float acc[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+  const Bf16x8* X = reinterpret_cast<const Bf16x8*>(dpre);
+  for (int p = blockIdx.x * groups + g; p < pixels; p += gridDim.x * groups) {
+    const Bf16x8 x = X[static_cast<size_t>(p) * c8 + v];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc[k] += __bfloat162float(x.v[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) part[g * c + 8 * v + k] = acc[k];
+  __syncthreads();
+  for (int ch = threadIdx.x; ch < c; ch += kBiasThreads) {
+    float sum = 0.0f;
+    for (int q = 0; q < groups; ++q) sum += part[q * c + ch];
+    atomicAdd(db + ch, sum);
+  }
 }
 
 // 1x1 output layer (32 -> 1, linear) and its gradients
@@ -309,29 +328,42 @@ __global__ void out_forward_kernel(const bf16* __restrict__ a, const float* __re
   y[p] = s;
 }
 
-// loss = mean (y - target)^2; dy = 2 (y - target) / n; da = dy w; dw, db accumulated
+// loss = mean (y - target)^2; dy = 2 (y - target) / n; da = dy w; dw, db accumulated.
+// Each thread takes several pixels (grid-stride), reads its 32 activations as
+// four 16-byte vectors and writes da as eight float4, and reduces dw / db /
+// loss once at the end (warp shuffles, then one shared-memory and one global
+// atomic per value per block).
 __global__ void out_backward_kernel(const bf16* __restrict__ a, const float* __restrict__ w, const float* __restrict__ y,
                                     const float* __restrict__ target, float* __restrict__ da, float* __restrict__ dw,
                                     float* __restrict__ db, float* __restrict__ loss, int pixels) {
   __shared__ float red[34];
   if (threadIdx.x < 34) red[threadIdx.x] = 0.0f;
   __syncthreads();
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
   float gw[32];
+  float wl[32];
 #pragma unroll
-  for (int c = 0; c < 32; ++c) gw[c] = 0.0f;
+  for (int c = 0; c < 32; ++c) {
+    gw[c] = 0.0f;
+    wl[c] = w[c];
+  }
   float gb = 0.0f, l = 0.0f;
-  if (p < pixels) {
+  const float inv_n = 1.0f / static_cast<float>(pixels);
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < pixels; p += gridDim.x * blockDim.x) {
     const float diff = y[p] - target[p];
     const float dy = 2.0f * diff / static_cast<float>(pixels);
-    l = diff * diff / static_cast<float>(pixels);
-    gb = dy;
+    l += diff * diff * inv_n;
+    gb += dy;
+    const Bf16x8* row = reinterpret_cast<const Bf16x8*>(a + static_cast<size_t>(p) * 32);
+    float4* drow = reinterpret_cast<float4*>(da + static_cast<size_t>(p) * 32);
 #pragma unroll
-    for (int c = 0; c < 32; ++c) {
-      const float av = __bfloat162float(a[static_cast<size_t>(p) * 32 + c]);
-      gw[c] = dy * av;
-      da[static_cast<size_t>(p) * 32 + c] = dy * w[c];
+    for (int q = 0; q < 4; ++q) {
+      const Bf16x8 v = row[q];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) gw[8 * q + k] += dy * __bfloat162float(v.v[k]);
     }
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      drow[q] = make_float4(dy * wl[4 * q], dy * wl[4 * q + 1], dy * wl[4 * q + 2], dy * wl[4 * q + 3]);
   }
 #pragma unroll
   for (int c = 0; c < 32; ++c) {
@@ -510,7 +542,7 @@ int backward(gg_unet* n, const float* target) {
   auto& L = n->layers;
   UNET_CUDA(cudaMemsetAsync(n->grads, 0, n->n_params * sizeof(float), n->stream));
   UNET_CUDA(cudaMemsetAsync(n->loss, 0, sizeof(float), n->stream));
-  out_backward_kernel<<<(pixels + 255) / 256, 256, 0, n->stream>>>(L[13].act, n->params + n->out_w_off, n->y, target,
+  out_backward_kernel<<<std::min((pixels + 255) / 256, 148 * 4), 256, 0, n->stream>>>(L[13].act, n->params + n->out_w_off, n->y, target,
                                                                      L[13].dact, n->grads + n->out_w_off,
                                                                      n->grads + n->out_b_off, n->loss, pixels);
   for (int i = 13; i >= 0; --i) {
@@ -518,7 +550,8 @@ int backward(gg_unet* n, const float* target) {
     const int px = B * l.side * l.side;
     const size_t na = static_cast<size_t>(px) * l.cout;
     relu_backward_kernel<<<grid_for(na / 8), 256, 0, n->stream>>>(l.dact, l.act, l.dpre, na);
-    bias_grad_kernel<<<dim3(std::min(px, 1024), (l.cout + 127) / 128), 128, 0, n->stream>>>(l.dpre, n->grads + l.b_off, px, l.cout);
+    bias_grad_kernel<<<std::min((px + kBiasThreads / (l.cout / 8) - 1) / (kBiasThreads / (l.cout / 8)), 148 * 4),
+                       kBiasThreads, 0, n->stream>>>(l.dpre, n->grads + l.b_off, px, l.cout);
     UNET_CUDA(gg_umma::launch_wgrad(l.wgrad, n->grads + l.w_off, n->conv_error, n->stream));
     if (i == 0) break;
     // data gradient of the layer input (FP32)
