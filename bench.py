@@ -312,6 +312,16 @@ def surrogate_measurement(tmp, angles=360, reference_every=10):
                        "reference_primaries": 1e9, "training": "2000 MC pairs at 1e8 primaries, 60 epochs"}}
 
 
+def _transport_launch(lib, ctx):
+    """The transport kernel's launch knobs on this context."""
+    v = [C.c_int32() for _ in range(7)]
+    lib.gg_get_transport_tuning(ctx, C.byref(v[0]), C.byref(v[1]), C.byref(v[2]))
+    lib.gg_get_transport_launch(ctx, C.byref(v[3]), C.byref(v[4]))
+    lib.gg_get_transport_stash(ctx, C.byref(v[5]), C.byref(v[6]))
+    return {"blocks_per_sm": v[0].value or "as many as fit", "regroup_ratio4": v[2].value, "block_threads": v[3].value,
+            "slots_per_claim": v[4].value, "stash_registers": v[5].value, "stash_swap_lanes": v[6].value}
+
+
 def _cbct_config(primaries, batches, world):
     """The workload both arms report (same dict on the product and the reference arm)."""
     return {"workload": WORKLOAD, "phantom": "256x256x256 uint8, 1 mm, air/water/bone(1.85)",
@@ -525,6 +535,7 @@ def main():
         "roofline": roofline,
         "cpu_baseline": cpu_baseline,
         "clocks": clocks,
+        "transport": _transport_launch(lib, ctx),
     }
     if not args.no_surrogate and world == 1:
         line["surrogate"] = surrogate_measurement(tmp)
@@ -603,6 +614,8 @@ def run_batched(args, tmp, rank):
     lib.gg_get_transport_tuning(ctx, C.byref(bps), C.byref(lanes), C.byref(ratio))
     threads, grain = C.c_int32(), C.c_int32()
     lib.gg_get_transport_launch(ctx, C.byref(threads), C.byref(grain))
+    stash, swap = C.c_int32(), C.c_int32()
+    lib.gg_get_transport_stash(ctx, C.byref(stash), C.byref(swap))
     arr, keep = _native._job_array(w.jobs)
     graph = C.c_void_p()
     check(lib.gg_capture_jobs(ctx, arr, len(keep), C.byref(graph)), "gg_capture_jobs")
@@ -639,7 +652,7 @@ def run_batched(args, tmp, rank):
                        "phantom_edges": w.phantom_edges,
                        "tuning": {"blocks_per_sm": bps.value, "regroup_ratio4": ratio.value,
                                   "block_threads": threads.value, "slots_per_claim": grain.value,
-                                  "tuned_on": "%d sampled jobs of the mix, 2e6 primaries each" % len(sample)},
+                                  "stash_registers": stash.value, "tuned_on": "%d sampled jobs of the mix, 2e6 primaries each" % len(sample)},
                        "launch": "one persistent kernel per step, replayed CUDA graph",
                        "l2": "256 MB buffer written between timed steps"},
             "gpu_launches": launches, "clocks": clk.summary()}), flush=True)

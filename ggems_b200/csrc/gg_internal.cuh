@@ -168,7 +168,17 @@ struct TransportParams {
   int32_t regroup_lanes;            // waiting lanes that start a round of the rare phases (1..32)
   int32_t regroup_ratio4;           // ... or 4 x waiting >= regroup_ratio4 x tracking lanes
   uint32_t slots_per_claim;         // consecutive slots a lane takes from the work queue at a time (power of two)
+  int32_t stash_swap_lanes;         // stash variant: waiting lanes that start an exchange with ready photons (1..32)
 };
+
+// Photon stash of the stash variant: per warp, kStashRecords photon records in
+// shared memory, one 32-bit word per field and record (field-major), and a
+// 32-entry index table.
+constexpr int kStashRecords = 32;
+__host__ __device__ constexpr int stash_words(bool batch, bool aux) { return 25 + (batch ? 1 : 0) + (aux ? 1 : 0); }
+constexpr size_t stash_bytes_per_warp(bool batch, bool aux) {
+  return sizeof(uint32_t) * (static_cast<size_t>(stash_words(batch, aux)) * kStashRecords + kStashRecords);
+}
 
 struct DoseParams {
   DevDoseMap map;
@@ -185,8 +195,9 @@ struct DoseParams {
 };
 
 void launch_transport(const TransportParams& p, int grid, int threads, size_t smem, void* stream, bool mesh, bool dose,
-                      bool aux);
-cudaError_t configure_transport(size_t smem, int threads, int* blocks_per_sm, bool mesh, bool batch, bool dose, bool aux);
+                      bool aux, int stash);
+cudaError_t configure_transport(size_t smem, int threads, int* blocks_per_sm, bool mesh, bool batch, bool dose, bool aux,
+                                int stash);
 cudaError_t set_rayleigh_fit(const float* pp);
 void launch_compute_dose(const DoseParams& p, void* stream);
 

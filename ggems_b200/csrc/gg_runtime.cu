@@ -62,6 +62,8 @@ struct gg_context {
   int blocks_per_sm = 0;  // 0: as many as fit (the autotuner may lower it)
   int block_threads = gg::kBlockThreads;  // transport block size: 128, 256 or 512
   int slots_per_claim = 1;                // photons per thread: slots a lane takes per work-queue grab
+  int stash_registers = 80;               // photon stash variant (voxel / detector scenes): 0 off, 64 or 80 registers
+  int stash_swap_lanes = 4;               // waiting lanes that start an exchange with the stash
   size_t smem_optin = 0;
   uint32_t* rng = nullptr;
   gg::DevParticles particles{};
@@ -490,6 +492,14 @@ GG_API int gg_context_create(int32_t device_index, gg_context** context) {
     int r = std::atoi(v);
     if (r >= 0 && r <= 128) c->regroup_ratio4 = r;
   }
+  if (const char* v = std::getenv("GGEMS_B200_STASH_REGISTERS")) {
+    int r = std::atoi(v);
+    if (r == 0 || r == 64 || r == 80) c->stash_registers = r;
+  }
+  if (const char* v = std::getenv("GGEMS_B200_STASH_SWAP")) {
+    int r = std::atoi(v);
+    if (r >= 1 && r <= 32) c->stash_swap_lanes = r;
+  }
   const size_t S = GG_MAXIMUM_PARTICLES;
   auto cleanup = [&](int code) {
     gg_context_destroy(c);
@@ -854,6 +864,7 @@ struct JobLaunch {
   bool mesh = false;
   bool dose = false;  // some solid tallies into a dose map
   bool aux = false;   // world grid or particle tracking
+  int stash = 0;       // photon stash variant (1: 64 registers, 2: 80)
   bool empty = true;
 };
 
@@ -930,6 +941,7 @@ int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*
   P.regroup_lanes = c->regroup_lanes;
   P.regroup_ratio4 = c->regroup_ratio4;
   P.slots_per_claim = static_cast<uint32_t>(c->slots_per_claim);
+  P.stash_swap_lanes = c->stash_swap_lanes;
   P.tracking_slot = -1;
   if (c->tracking_slot >= 0 && c->tracking_points) {
     P.tracking_slot = c->tracking_slot;
@@ -947,10 +959,13 @@ int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*
     P.world_momentum = c->world_momentum;
     aux = true;  // the world walk lives in the full kernel variant
   }
+  const bool batch = P.number_of_jobs > 1;
+  const int stash = (mesh || aux) ? 0 : (c->stash_registers == 64 ? 1 : (c->stash_registers == 80 ? 2 : 0));
   out->smem = (c->tables_in_smem ? c->table_bytes : 0) + sizeof(gg::DevSolid) * c->number_of_solids +
               sizeof(gg::DevNavigator) * c->number_of_navigators + 16;
+  if (stash) out->smem += (c->block_threads / 32) * gg::stash_bytes_per_warp(batch, false);
   int blocks_per_sm = 0;
-  GG_CUDA(gg::configure_transport(out->smem, c->block_threads, &blocks_per_sm, mesh, P.number_of_jobs > 1, dose, aux));
+  GG_CUDA(gg::configure_transport(out->smem, c->block_threads, &blocks_per_sm, mesh, batch, dose, aux, stash));
   if (blocks_per_sm < 1) return fail(GG_ERROR_CUDA, "transport kernel does not fit on an SM");
   if (c->blocks_per_sm > 0 && c->blocks_per_sm < blocks_per_sm) blocks_per_sm = c->blocks_per_sm;
   uint64_t grid = static_cast<uint64_t>(blocks_per_sm) * c->sm_count;
@@ -962,6 +977,7 @@ int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*
   out->mesh = mesh;
   out->dose = dose;
   out->aux = aux;
+  out->stash = stash;
   out->empty = false;
   return GG_OK;
 }
@@ -971,7 +987,7 @@ int enqueue_jobs(gg_context* c, const JobLaunch& L) {
   GG_CUDA(cudaMemsetAsync(c->slot_counter, 0, sizeof(unsigned int), c->stream));
   if (L.params.tracking_count) GG_CUDA(cudaMemsetAsync(L.params.tracking_count, 0, sizeof(int32_t), c->stream));
   GG_CUDA(cudaMemsetAsync(c->error, 0, sizeof(int), c->stream));
-  gg::launch_transport(L.params, L.grid, L.threads, L.smem, c->stream, L.mesh, L.dose, L.aux);
+  gg::launch_transport(L.params, L.grid, L.threads, L.smem, c->stream, L.mesh, L.dose, L.aux, L.stash);
   GG_CUDA(cudaGetLastError());
   return GG_OK;
 }
@@ -1121,18 +1137,34 @@ GG_API int gg_get_transport_launch(gg_context* c, int32_t* block_threads, int32_
   return GG_OK;
 }
 
+GG_API int gg_set_transport_stash(gg_context* c, int32_t registers, int32_t swap_lanes) {
+  if (!c || (registers != 0 && registers != 64 && registers != 80) || swap_lanes < 1 || swap_lanes > 32)
+    return fail(GG_ERROR_INVALID_ARGUMENT, "bad photon stash (registers 0, 64 or 80; swap_lanes 1..32)");
+  c->stash_registers = registers;
+  c->stash_swap_lanes = swap_lanes;
+  return GG_OK;
+}
+
+GG_API int gg_get_transport_stash(gg_context* c, int32_t* registers, int32_t* swap_lanes) {
+  if (!c) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL context");
+  if (registers) *registers = c->stash_registers;
+  if (swap_lanes) *swap_lanes = c->stash_swap_lanes;
+  return GG_OK;
+}
+
 }  // extern "C"
 
 namespace {
 
-// The launch shape the autotuner varies: resident blocks per SM, the
-// rare-phase regroup ratio, the block size and the photons per thread (slots a
-// lane claims per work-queue grab).
+// The launch shape the autotuner varies: the photon stash (off, 64 or 80
+// registers), resident blocks per SM, the rare-phase regroup ratio, the block
+// size and the photons per thread (slots a lane claims per work-queue grab).
 struct LaunchShape {
-  int blocks_per_sm, regroup_ratio4, block_threads, slots_per_claim;
+  int stash_registers, blocks_per_sm, regroup_ratio4, block_threads, slots_per_claim;
 };
 
 void apply_shape(gg_context* c, const LaunchShape& s) {
+  c->stash_registers = s.stash_registers;
   c->blocks_per_sm = s.blocks_per_sm;
   c->regroup_lanes = 32;
   c->regroup_ratio4 = s.regroup_ratio4;
@@ -1143,7 +1175,9 @@ void apply_shape(gg_context* c, const LaunchShape& s) {
 // Times `trial` (one launch of the workload to tune on) for each launch shape
 // of a coordinate search, restoring the random states before every trial, and
 // keeps the fastest:
-//   1. resident blocks per SM (4..1) x regroup ratio (3/4, 4/4, 6/4) at 256 threads, one slot per claim;
+//   1. photon stash (off, 64, 80 registers) x resident blocks per SM (4..1, as
+//      many as the registers allow) x regroup ratio (3/4, 4/4, 6/4) at 256
+//      threads, one slot per claim;
 //   2. block size 128 and 512 at the same resident threads per SM as the best of 1;
 //   3. 2, 4 and 8 slots per claim at the best of 1-2.
 // The tallies are zeroed and the random states restored afterwards.
@@ -1154,7 +1188,8 @@ int autotune(gg_context* c, const std::function<int()>& trial, float* best_ms) {
   GG_CUDA(cudaMalloc(&saved, bytes));
   auto restore = [&]() { return cudaMemcpyAsync(c->rng, saved, bytes, cudaMemcpyDeviceToDevice, c->stream); };
   cudaError_t e = cudaMemcpyAsync(saved, c->rng, bytes, cudaMemcpyDeviceToDevice, c->stream);
-  const LaunchShape start{c->blocks_per_sm, c->regroup_ratio4, c->block_threads, c->slots_per_claim};
+  const LaunchShape start{c->stash_registers, c->blocks_per_sm, c->regroup_ratio4, c->block_threads,
+                          c->slots_per_claim};
   LaunchShape best = start;
   float best_time = -1.0f;
   int rc = GG_OK;
@@ -1169,15 +1204,17 @@ int autotune(gg_context* c, const std::function<int()>& trial, float* best_ms) {
       best = s;
     }
   };
-  for (int bps = 4; bps >= 1; --bps)
-    for (int r : {3, 4, 6}) run({bps, r, gg::kBlockThreads, 1});
+  for (int stash : {0, 64, 80})
+    for (int bps = stash == 80 ? 3 : 4; bps >= 1; --bps)
+      for (int r : {3, 4, 6}) run({stash, bps, r, gg::kBlockThreads, 1});
   const LaunchShape stage1 = best;
   for (int threads : {128, 512}) {
     const int bps = stage1.blocks_per_sm * gg::kBlockThreads / threads;
-    if (bps >= 1) run({bps, stage1.regroup_ratio4, threads, 1});
+    if (bps >= 1) run({stage1.stash_registers, bps, stage1.regroup_ratio4, threads, 1});
   }
   const LaunchShape stage2 = best;
-  for (int k : {2, 4, 8}) run({stage2.blocks_per_sm, stage2.regroup_ratio4, stage2.block_threads, k});
+  for (int k : {2, 4, 8})
+    run({stage2.stash_registers, stage2.blocks_per_sm, stage2.regroup_ratio4, stage2.block_threads, k});
   if (e == cudaSuccess) e = restore();
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   cudaFree(saved);

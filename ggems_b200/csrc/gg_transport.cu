@@ -777,11 +777,14 @@ constexpr int transport_registers(int blocks) { return (65536 / (kBlockThreads *
 // registers stay out of the voxel / detector (or mesh) hot loop.
 // kDose: some solid tallies into a dose map.
 // kBatch: several jobs (source runs) in one launch, each with its own solids.
+// kStash: each warp keeps a second set of photons in shared memory and
+// exchanges them with its lanes, so that lanes waiting for a rare phase track
+// a parked photon meanwhile and rare rounds run on full warps.
 
-template <bool kFull, bool kBatch, bool kDose, bool kAux>
-__global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : (kBatch && kDose ? 3 : 4))))
+template <bool kFull, bool kBatch, bool kDose, bool kAux, int kStash>
+__global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : ((kBatch && kDose) || kStash == 2 ? 3 : 4))))
     transport_kernel(TransportParams P) {
-  // shared memory: [tables][solids][navigators][mbarrier]
+  // shared memory: [tables][solids][navigators][mbarrier][stash]
   unsigned char* tables = g_smem;
   DevSolid* scene_solids = reinterpret_cast<DevSolid*>(g_smem + (P.tables_in_smem ? P.table_bytes : 0));
   DevNavigator* navs = reinterpret_cast<DevNavigator*>(scene_solids + P.number_of_solids);
@@ -905,6 +908,133 @@ __global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : (kBatch 
     return type == GG_SOLID_VOXELIZED ? kTrackVoxel : (kFull && type == GG_SOLID_MESHED) ? kTrackMesh : kTrackBox;
   };
 
+  // ---- photon stash (kStash) ----
+  // Per warp, kStashRecords photon records in shared memory (field f of record
+  // r at w_stash[f * 32 + r]: a lane's accesses hit 32 different banks) and
+  // three warp-uniform masks saying which records hold a photon ready to track
+  // (st_ready), waiting for an interaction (st_int) or for a new history /
+  // FindSolid round (st_find); a record in none of them is empty.  A photon
+  // carries its whole state, slot and random stream included, so moving it
+  // between a lane and a record never changes what its slot computes.
+  constexpr int kWords = stash_words(kBatch, kAux);
+  const int lane = threadIdx.x & 31;
+  const unsigned lanes_below = (1u << lane) - 1u;
+  uint32_t* w_stash = nullptr;
+  int* w_index = nullptr;
+  unsigned st_ready = 0, st_int = 0, st_find = 0;
+  if (kStash) {
+    uint32_t* base = reinterpret_cast<uint32_t*>(bar + 2);
+    w_stash = base + (threadIdx.x >> 5) * (kWords * kStashRecords + kStashRecords);
+    w_index = reinterpret_cast<int*>(w_stash + kWords * kStashRecords);
+  }
+  // Exchanges this lane's photon with record r.
+  auto swap_record = [&](int r) {
+    uint32_t* q = w_stash + r;
+    auto xu = [&](int f, uint32_t& v) {
+      const uint32_t t = q[f * kStashRecords];
+      q[f * kStashRecords] = v;
+      v = t;
+    };
+    auto xf = [&](int f, float& v) {
+      const uint32_t t = q[f * kStashRecords];
+      q[f * kStashRecords] = __float_as_uint(v);
+      v = __uint_as_float(t);
+    };
+    auto xi = [&](int f, int& v) {
+      const uint32_t t = q[f * kStashRecords];
+      q[f * kStashRecords] = static_cast<uint32_t>(v);
+      v = static_cast<int>(t);
+    };
+    xu(0, rng.s1);
+    xu(1, rng.s2);
+    xu(2, rng.s3);
+    xu(3, rng.s4);
+    xu(4, rng.s5);
+    xf(5, ph.p.x);
+    xf(6, ph.p.y);
+    xf(7, ph.p.z);
+    xf(8, ph.d.x);
+    xf(9, ph.d.y);
+    xf(10, ph.d.z);
+    xf(11, ph.E);
+    xf(12, ph.psd);
+    xi(13, ph.solid_id);
+    uint32_t packed = static_cast<uint32_t>(static_cast<uint8_t>(ph.status)) |
+                      (static_cast<uint32_t>(static_cast<uint8_t>(ph.scatter)) << 8) |
+                      (static_cast<uint32_t>(phase) << 16);
+    xu(14, packed);
+    ph.status = static_cast<int8_t>(packed & 0xffu);
+    ph.scatter = static_cast<int8_t>((packed >> 8) & 0xffu);
+    phase = static_cast<int>(packed >> 16);
+    xu(15, slot);
+    xu(16, histories_left);
+    xi(17, rounds);
+    xi(18, pending);
+    xf(19, inv_d.x);
+    xf(20, inv_d.y);
+    xf(21, inv_d.z);
+    xi(22, energy_id);
+    xf(23, cached_E);
+    xi(24, cached_nav);
+    if (kBatch) {
+      xi(25, job);
+      solids = P.job_solids + static_cast<size_t>(job) * P.number_of_solids;
+    }
+    if (kAux) xi(kWords - 1, history_number);
+  };
+  // The k-th lane of `lanes` (in lane order) gets the k-th record of
+  // `records`; -1 for the other lanes.  Called by the whole warp.
+  auto match = [&](unsigned lanes, unsigned records) -> int {
+    if ((records >> lane) & 1u) w_index[__popc(records & lanes_below)] = lane;
+    __syncwarp();
+    int r = -1;
+    if ((lanes >> lane) & 1u) {
+      const int k = __popc(lanes & lanes_below);
+      if (k < __popc(records)) r = w_index[k];
+    }
+    __syncwarp();
+    return r;
+  };
+  auto is_rare = [](int ph_phase) { return ph_phase == kNewHistory || ph_phase == kFind || ph_phase == kInteract; };
+  // Lanes of `lanes` exchange their photons with records of `records`; the
+  // masks then say what each touched record holds.  Called by the whole warp.
+  auto exchange = [&](unsigned lanes, unsigned records) {
+    const int r = match(lanes, records);
+    const int old = phase;
+    if (r >= 0) swap_record(r);
+    const unsigned bit = r >= 0 ? (1u << r) : 0u;
+    const unsigned moved = __reduce_or_sync(0xffffffffu, bit);
+    const unsigned to_int = __reduce_or_sync(0xffffffffu, old == kInteract ? bit : 0u);
+    const unsigned to_find = __reduce_or_sync(0xffffffffu, (old == kNewHistory || old == kFind) ? bit : 0u);
+    const unsigned to_empty = __reduce_or_sync(0xffffffffu, old == kDone ? bit : 0u);
+    st_int = (st_int & ~moved) | to_int;
+    st_find = (st_find & ~moved) | to_find;
+    st_ready = (st_ready & ~moved) | (moved & ~(to_int | to_find | to_empty));
+  };
+
+  if (kStash) {
+    // Fill the records first: each lane claims a slot (a run of its own) for
+    // record `lane`, then one for itself.
+    phase = next_slot() ? kNewHistory : kDone;
+    st_find = __ballot_sync(0xffffffffu, phase == kNewHistory);
+    swap_record(lane);  // the lane receives whatever the record held before: reset below
+    slot = ~0u;
+    histories_left = 0;
+    rounds = 0;
+    pending = 0;
+    energy_id = 0;
+    cached_E = -1.0f;
+    cached_nav = -1;
+    history_number = -1;
+    ph = Photon{};
+    ph.solid_id = -1;
+    inv_d = v3(0.0f, 0.0f, 0.0f);
+    if (kBatch) {
+      job = 0;
+      solids = scene_solids;
+    }
+    phase = kDone;
+  }
   if (next_slot()) phase = kNewHistory;
 
   // Warp-level phase scheduling.  Tracking steps (voxel or detector box) are
@@ -918,24 +1048,58 @@ __global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : (kBatch 
   // what.
   const int regroup = P.regroup_lanes;
   const int ratio4 = P.regroup_ratio4;
+  const int swap_lanes = P.stash_swap_lanes;
   for (;;) {
-    const unsigned active = __ballot_sync(0xffffffffu, phase != kDone);
-    if (active == 0) break;
-    const unsigned tracking =
-        __ballot_sync(0xffffffffu, phase == kTrackVoxel || phase == kTrackBox || (kFull && phase == kTrackMesh));
-    const int n_other = __popc(active & ~tracking);
+    bool round = false, serve_interact = false;
+    if (kStash) {
+      unsigned active = __ballot_sync(0xffffffffu, phase != kDone);
+      if (active == 0 && (st_ready | st_int | st_find) == 0) break;
+      unsigned waiting = __ballot_sync(0xffffffffu, is_rare(phase));
+      // Lanes waiting for a rare phase, and lanes without a photon, take
+      // ready photons from the stash (once enough of them wait: an exchange
+      // costs the warp two shared-memory accesses per word).
+      const unsigned want = waiting | ~active;
+      if (st_ready != 0 && __popc(want) >= min(swap_lanes, __popc(st_ready))) {
+        exchange(want, st_ready);
+        active = __ballot_sync(0xffffffffu, phase != kDone);
+        waiting = __ballot_sync(0xffffffffu, is_rare(phase));
+      }
+      // A round of one kind of rare work when a full warp of it is waiting
+      // (lanes and records), or when the waiting lanes are many against the
+      // tracking ones and no ready photon is left to replace them.
+      const unsigned w_int = __ballot_sync(0xffffffffu, phase == kInteract);
+      const int n_int = __popc(w_int) + __popc(st_int);
+      const int n_find = __popc(waiting & ~w_int) + __popc(st_find);
+      const int n_wait = __popc(waiting), n_track = __popc(active & ~waiting);
+      round = n_int + n_find > 0 &&
+              (n_int >= 32 || n_find >= 32 || n_track == 0 ||
+               (n_wait > 0 && (n_wait >= regroup || 4 * n_wait >= ratio4 * n_track)));
+      if (round) {
+        serve_interact = n_int >= 32 ? (n_find < 32 || n_int >= n_find) : (n_find < 32 && n_int >= n_find);
+        // gather: lanes without a photon of the served kind take one from the stash
+        const unsigned kind_lanes = serve_interact ? w_int : (waiting & ~w_int);
+        const unsigned kind_records = serve_interact ? st_int : st_find;
+        if (kind_records != 0 && kind_lanes != 0xffffffffu) exchange(~kind_lanes, kind_records);
+      }
+    } else {
+      const unsigned active = __ballot_sync(0xffffffffu, phase != kDone);
+      if (active == 0) break;
+      const unsigned tracking =
+          __ballot_sync(0xffffffffu, phase == kTrackVoxel || phase == kTrackBox || (kFull && phase == kTrackMesh));
+      const int n_other = __popc(active & ~tracking);
+      round = n_other > 0 && (n_other >= regroup || 4 * n_other >= ratio4 * __popc(tracking));
+      // A round serves one kind of rare work: the interaction samplers, or the
+      // new-history / FindSolid chain, whichever more lanes wait for; the
+      // others wait for the next round (their code paths stay out of this
+      // one).  Measured +1.4 % on the CBCT projection.
+      if (round) serve_interact = 2 * __popc(__ballot_sync(0xffffffffu, phase == kInteract)) >= n_other;
+    }
     // A step or an interaction that ends the photon's stay in its solid sets
     // `leave` (1: alive, 2: dead) and `leaving`, and jumps to the one copy of
     // the exit code at the end of the loop body.
     int leave = 0;
     const DevSolid* leaving = nullptr;
-    if (n_other > 0 && (n_other >= regroup || 4 * n_other >= ratio4 * __popc(tracking))) {
-      // A round serves one kind of rare work: the interaction samplers, or the
-      // new-history / FindSolid chain, whichever more lanes wait for; the
-      // others wait for the next round (their code paths stay out of this
-      // one).  Measured +1.4 % on the CBCT projection.
-      const int n_interact = __popc(__ballot_sync(0xffffffffu, phase == kInteract));
-      const bool serve_interact = 2 * n_interact >= n_other;
+    if (round) {
       if ((phase == kInteract) != serve_interact) continue;
       if (phase == kInteract) {
         // The Compton / Rayleigh part of a tracking step (the tail of
@@ -1245,18 +1409,28 @@ using TransportKernel = void (*)(TransportParams);
 // kFull: meshed solids, world grid or particle tracking (dose code always in),
 // kAux: world grid or particle tracking; otherwise the dose-map code is
 // compiled in only for scenes that tally dose.
-TransportKernel transport_variant(bool mesh, bool batch, bool dose, bool aux) {
-  if (aux) return batch ? transport_kernel<true, true, true, true> : transport_kernel<true, false, true, true>;
-  if (mesh) return batch ? transport_kernel<true, true, true, false> : transport_kernel<true, false, true, false>;
-  if (dose) return batch ? transport_kernel<false, true, true, false> : transport_kernel<false, false, true, false>;
-  return batch ? transport_kernel<false, true, false, false> : transport_kernel<false, false, false, false>;
+// kStash: the photon stash (voxel / detector scenes without world grid or
+// particle tracking).
+TransportKernel transport_variant(bool mesh, bool batch, bool dose, bool aux, int stash) {
+  if (aux) return batch ? transport_kernel<true, true, true, true, 0> : transport_kernel<true, false, true, true, 0>;
+  if (mesh) return batch ? transport_kernel<true, true, true, false, 0> : transport_kernel<true, false, true, false, 0>;
+  if (stash == 1) {
+    if (dose) return batch ? transport_kernel<false, true, true, false, 1> : transport_kernel<false, false, true, false, 1>;
+    return batch ? transport_kernel<false, true, false, false, 1> : transport_kernel<false, false, false, false, 1>;
+  }
+  if (stash == 2) {
+    if (dose) return batch ? transport_kernel<false, true, true, false, 2> : transport_kernel<false, false, true, false, 2>;
+    return batch ? transport_kernel<false, true, false, false, 2> : transport_kernel<false, false, false, false, 2>;
+  }
+  if (dose) return batch ? transport_kernel<false, true, true, false, 0> : transport_kernel<false, false, true, false, 0>;
+  return batch ? transport_kernel<false, true, false, false, 0> : transport_kernel<false, false, false, false, 0>;
 }
 }  // namespace
 
 void launch_transport(const TransportParams& p, int grid, int threads, size_t smem, void* stream, bool mesh, bool dose,
-                      bool aux) {
+                      bool aux, int stash) {
   const bool batch = p.number_of_jobs > 1;
-  transport_variant(mesh, batch, dose, aux)<<<grid, threads, smem, static_cast<cudaStream_t>(stream)>>>(p);
+  transport_variant(mesh, batch, dose, aux, stash)<<<grid, threads, smem, static_cast<cudaStream_t>(stream)>>>(p);
 }
 
 namespace {
@@ -1351,8 +1525,8 @@ void launch_compute_dose(const DoseParams& p, void* stream) {
 }
 
 cudaError_t configure_transport(size_t smem, int threads, int* blocks_per_sm, bool mesh, bool batch, bool dose,
-                                bool aux) {
-  auto kernel = transport_variant(mesh, batch, dose, aux);
+                                bool aux, int stash) {
+  auto kernel = transport_variant(mesh, batch, dose, aux, stash);
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kernel, threads, smem);

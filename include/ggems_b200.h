@@ -314,7 +314,7 @@ GG_API int gg_graph_destroy(gg_graph* graph);
  *   and runs one after another (a power of two, 1..64): gg_set_transport_launch.
  * gg_autotune times short runs of `source` (gg_autotune_jobs: of a batched
  * launch of `jobs`, e.g. a sample of the job mix to run) over a coordinate
- * search of these four knobs, keeps the fastest and reports its time; it
+ * search of these knobs and the photon stash (gg_set_transport_stash), keeps the fastest and reports its time; it
  * restores the random states and zeroes the tallies afterwards, so call it
  * before the real run.  The results do not depend on the launch shape. */
 GG_API int gg_set_transport_tuning(gg_context* context, int32_t blocks_per_sm, int32_t regroup_lanes,
@@ -323,6 +323,18 @@ GG_API int gg_get_transport_tuning(gg_context* context, int32_t* blocks_per_sm, 
                                    int32_t* regroup_ratio4);
 GG_API int gg_set_transport_launch(gg_context* context, int32_t block_threads, int32_t slots_per_claim);
 GG_API int gg_get_transport_launch(gg_context* context, int32_t* block_threads, int32_t* slots_per_claim);
+/* Photon stash (voxelized and box solids without a world grid or particle
+ * tracking; meshed scenes ignore it): each warp parks a second set of photons
+ * in shared memory and exchanges them with its lanes, so that a lane whose
+ * photon waits for a rare phase (new history, FindSolid, Compton / Rayleigh
+ * sampling) tracks a parked photon meanwhile, and the rare phases run on full
+ * warps.  registers: 0 (off), 64 or 80 per thread (the kernel variant's
+ * budget: 4 or 3 resident 256-thread blocks per SM); swap_lanes (1..32): the
+ * waiting lanes that start an exchange.  Default 80 and 4 (environment
+ * override at context creation: GGEMS_B200_STASH_REGISTERS).  The results do
+ * not depend on it. */
+GG_API int gg_set_transport_stash(gg_context* context, int32_t registers, int32_t swap_lanes);
+GG_API int gg_get_transport_stash(gg_context* context, int32_t* registers, int32_t* swap_lanes);
 GG_API int gg_autotune(gg_context* context, const gg_source* source, uint64_t number_of_particles,
                        float* best_milliseconds);
 GG_API int gg_autotune_jobs(gg_context* context, const gg_job* jobs, int32_t number_of_jobs, float* best_milliseconds);

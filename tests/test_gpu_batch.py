@@ -149,9 +149,9 @@ def test_graph_replay_equals_repeated_runs(ctx):
 
 
 def test_autotune_restores_state(ctx):
-    """gg_autotune searches resident blocks per SM, regroup ratio, block size
-    and photons per thread (slots per work-queue claim), keeps the fastest,
-    and leaves the random states and tallies as they were."""
+    """gg_autotune searches the photon stash, resident blocks per SM, regroup
+    ratio, block size and photons per thread (slots per work-queue claim),
+    keeps the fastest, and leaves the random states and tallies as they were."""
     sc = scenes.cbct_scene(n=32, voxel=8.0, elements=(64, 64, 1), element_size=(6.4, 6.4, 10.0))
     src = scenes.XRaySource(spectrum=scenes.synthetic_spectrum(), aperture_deg=11.0)
     ctx.upload_scene(sc.struct())
@@ -160,10 +160,11 @@ def test_autotune_restores_state(ctx):
     ms = ctx.autotune(src.struct, 2 * abi.GG_MAXIMUM_PARTICLES)
     bps, lanes, ratio = ctx.tuning()
     threads, grain = ctx.launch()
+    stash, swap = ctx.stash()
     print("autotune: %.2f ms for 2^21 primaries with %d blocks/SM of %d threads, regroup ratio %d/4, "
-          "%d slot(s) per claim" % (ms, bps, threads, ratio, grain))
+          "%d slot(s) per claim, stash %d registers" % (ms, bps, threads, ratio, grain, stash))
     assert ms > 0 and 1 <= bps <= 8 and 1 <= lanes <= 32
-    assert threads in (128, 256, 512) and grain in (1, 2, 4, 8)
+    assert threads in (128, 256, 512) and grain in (1, 2, 4, 8) and stash in (0, 64, 80)
     assert bps * threads <= 1024
     st = np.zeros_like(st0)
     ctx.get_random_states(st)
@@ -176,27 +177,32 @@ def test_autotune_restores_state(ctx):
     assert parity.history_agreement(Pg, Po)[1] > 0.995
     ctx.set_tuning()
     ctx.set_launch()
+    ctx.set_stash()
 
 
 def test_launch_shape_does_not_change_results(ctx):
     """Every slot's histories are the same whatever the launch shape: block
-    size, blocks per SM and photons per thread change which lane runs a slot,
-    not what the slot computes (final states, streams and integer tallies
-    identical)."""
+    size, blocks per SM, photons per thread and the photon stash (on, with
+    either register budget, or off) change which lane runs a slot, not what
+    the slot computes (final states, streams and integer tallies identical)."""
     sc = scenes.cbct_scene(n=32, voxel=8.0, elements=(64, 64, 1), element_size=(6.4, 6.4, 10.0))
     src = scenes.XRaySource(spectrum=scenes.synthetic_spectrum(), aperture_deg=11.0)
     n = 2_500_000
     try:
         ref = parity.run_gpu(ctx, sc, src, n)
-        for threads, bps, grain in ((128, 6, 1), (512, 1, 4), (256, 3, 8)):
+        for threads, bps, grain, stash in ((128, 6, 1, 80), (512, 1, 4, 80), (256, 3, 8, 64), (256, 0, 1, 0),
+                                           (128, 0, 2, 0), (256, 0, 1, 64)):
             ctx.set_launch(threads, grain)
             ctx.set_tuning(bps)
+            ctx.set_stash(stash, 1 if stash == 64 else 4)
+            shape = (threads, bps, grain, stash)
             P, T, st = parity.run_gpu(ctx, sc, src, n)
-            assert np.array_equal(st, ref[2]), (threads, bps, grain)
+            assert np.array_equal(st, ref[2]), shape
             for f in ("E", "px", "py", "pz", "dx", "dy", "dz", "status", "scatter", "solid_id"):
-                assert np.array_equal(getattr(P, f), getattr(ref[0], f)), (threads, bps, grain, f)
+                assert np.array_equal(getattr(P, f), getattr(ref[0], f)), shape + (f,)
             for a, b in zip(T.histograms, ref[1].histograms):
-                assert np.array_equal(a, b), (threads, bps, grain)
+                assert np.array_equal(a, b), shape
     finally:
         ctx.set_tuning()
         ctx.set_launch()
+        ctx.set_stash()
