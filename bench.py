@@ -314,12 +314,13 @@ def surrogate_measurement(tmp, angles=360, reference_every=10):
 
 def _transport_launch(lib, ctx):
     """The transport kernel's launch knobs on this context."""
-    v = [C.c_int32() for _ in range(7)]
+    v = [C.c_int32() for _ in range(8)]
     lib.gg_get_transport_tuning(ctx, C.byref(v[0]), C.byref(v[1]), C.byref(v[2]))
     lib.gg_get_transport_launch(ctx, C.byref(v[3]), C.byref(v[4]))
-    lib.gg_get_transport_stash(ctx, C.byref(v[5]), C.byref(v[6]))
+    lib.gg_get_transport_stash(ctx, C.byref(v[5]), C.byref(v[6]), C.byref(v[7]))
     return {"blocks_per_sm": v[0].value or "as many as fit", "regroup_ratio4": v[2].value, "block_threads": v[3].value,
-            "slots_per_claim": v[4].value, "stash_registers": v[5].value, "stash_swap_lanes": v[6].value}
+            "slots_per_claim": v[4].value, "stash_registers": v[5].value, "stash_swap_lanes": v[6].value,
+            "stash_round_photons": v[7].value}
 
 
 def _cbct_config(primaries, batches, world):
@@ -614,8 +615,8 @@ def run_batched(args, tmp, rank):
     lib.gg_get_transport_tuning(ctx, C.byref(bps), C.byref(lanes), C.byref(ratio))
     threads, grain = C.c_int32(), C.c_int32()
     lib.gg_get_transport_launch(ctx, C.byref(threads), C.byref(grain))
-    stash, swap = C.c_int32(), C.c_int32()
-    lib.gg_get_transport_stash(ctx, C.byref(stash), C.byref(swap))
+    stash, swap, round_photons = C.c_int32(), C.c_int32(), C.c_int32()
+    lib.gg_get_transport_stash(ctx, C.byref(stash), C.byref(swap), C.byref(round_photons))
     arr, keep = _native._job_array(w.jobs)
     graph = C.c_void_p()
     check(lib.gg_capture_jobs(ctx, arr, len(keep), C.byref(graph)), "gg_capture_jobs")
@@ -652,7 +653,8 @@ def run_batched(args, tmp, rank):
                        "phantom_edges": w.phantom_edges,
                        "tuning": {"blocks_per_sm": bps.value, "regroup_ratio4": ratio.value,
                                   "block_threads": threads.value, "slots_per_claim": grain.value,
-                                  "stash_registers": stash.value, "tuned_on": "%d sampled jobs of the mix, 2e6 primaries each" % len(sample)},
+                                  "stash_registers": stash.value, "stash_round_photons": round_photons.value,
+                                  "tuned_on": "%d sampled jobs of the mix, 2e6 primaries each" % len(sample)},
                        "launch": "one persistent kernel per step, replayed CUDA graph",
                        "l2": "256 MB buffer written between timed steps"},
             "gpu_launches": launches, "clocks": clk.summary()}), flush=True)

@@ -49,8 +49,8 @@ def _load():
         "gg_autotune_jobs": (C.c_int, [C.c_void_p, P(abi.gg_job), C.c_int32, P(C.c_float)]),
         "gg_set_transport_launch": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
         "gg_get_transport_launch": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32)]),
-        "gg_set_transport_stash": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
-        "gg_get_transport_stash": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32)]),
+        "gg_set_transport_stash": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
+        "gg_get_transport_stash": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32), P(C.c_int32)]),
         "gg_device_tallies": (C.c_int, [C.c_void_p, P(abi.gg_device_tally), C.c_int32, P(C.c_int32)]),
         "gg_set_tracking": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
         "gg_read_tracking": (C.c_int, [C.c_void_p, P(abi.gg_track_point), C.c_int32, P(C.c_int32)]),
@@ -162,15 +162,15 @@ class Context:
         check(lib.gg_get_transport_launch(self.handle, C.byref(a), C.byref(b)), "gg_get_transport_launch")
         return a.value, b.value
 
-    def set_stash(self, registers=80, swap_lanes=4):
+    def set_stash(self, registers=80, swap_lanes=4, round_photons=40):
         """Photon stash of the transport kernel: 0 (off), 64 or 80 registers."""
-        check(lib.gg_set_transport_stash(self.handle, registers, swap_lanes), "gg_set_transport_stash")
+        check(lib.gg_set_transport_stash(self.handle, registers, swap_lanes, round_photons), "gg_set_transport_stash")
 
     def stash(self):
-        """(registers, swap lanes) of the photon stash; 0 registers = off."""
-        a, b = C.c_int32(), C.c_int32()
-        check(lib.gg_get_transport_stash(self.handle, C.byref(a), C.byref(b)), "gg_get_transport_stash")
-        return a.value, b.value
+        """(registers, swap lanes, round photons) of the photon stash; 0 registers = off."""
+        a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib.gg_get_transport_stash(self.handle, C.byref(a), C.byref(b), C.byref(c)), "gg_get_transport_stash")
+        return a.value, b.value, c.value
 
     def autotune(self, source, number_of_particles):
         ms = C.c_float()

@@ -169,6 +169,7 @@ struct TransportParams {
   int32_t regroup_ratio4;           // ... or 4 x waiting >= regroup_ratio4 x tracking lanes
   uint32_t slots_per_claim;         // consecutive slots a lane takes from the work queue at a time (power of two)
   int32_t stash_swap_lanes;         // stash variant: waiting lanes that start an exchange with ready photons (1..32)
+  int32_t stash_round_photons;      // stash variant: waiting photons (lanes + records) that start a rare round
 };
 
 // Photon stash of the stash variant: per warp, kStashRecords photon records in

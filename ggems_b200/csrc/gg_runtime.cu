@@ -64,6 +64,7 @@ struct gg_context {
   int slots_per_claim = 1;                // photons per thread: slots a lane takes per work-queue grab
   int stash_registers = 80;               // photon stash variant (voxel / detector scenes): 0 off, 64 or 80 registers
   int stash_swap_lanes = 4;               // waiting lanes that start an exchange with the stash
+  int stash_round_photons = 40;           // waiting photons of a warp (lanes + records) that start a rare round
   size_t smem_optin = 0;
   uint32_t* rng = nullptr;
   gg::DevParticles particles{};
@@ -491,6 +492,10 @@ GG_API int gg_context_create(int32_t device_index, gg_context** context) {
   if (const char* v = std::getenv("GGEMS_B200_REGROUP_RATIO4")) {
     int r = std::atoi(v);
     if (r >= 0 && r <= 128) c->regroup_ratio4 = r;
+  }
+  if (const char* v = std::getenv("GGEMS_B200_STASH_ROUND")) {
+    int r = std::atoi(v);
+    if (r >= 1 && r <= 64) c->stash_round_photons = r;
   }
   if (const char* v = std::getenv("GGEMS_B200_STASH_REGISTERS")) {
     int r = std::atoi(v);
@@ -942,6 +947,7 @@ int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*
   P.regroup_ratio4 = c->regroup_ratio4;
   P.slots_per_claim = static_cast<uint32_t>(c->slots_per_claim);
   P.stash_swap_lanes = c->stash_swap_lanes;
+  P.stash_round_photons = c->stash_round_photons;
   P.tracking_slot = -1;
   if (c->tracking_slot >= 0 && c->tracking_points) {
     P.tracking_slot = c->tracking_slot;
@@ -1137,18 +1143,22 @@ GG_API int gg_get_transport_launch(gg_context* c, int32_t* block_threads, int32_
   return GG_OK;
 }
 
-GG_API int gg_set_transport_stash(gg_context* c, int32_t registers, int32_t swap_lanes) {
-  if (!c || (registers != 0 && registers != 64 && registers != 80) || swap_lanes < 1 || swap_lanes > 32)
-    return fail(GG_ERROR_INVALID_ARGUMENT, "bad photon stash (registers 0, 64 or 80; swap_lanes 1..32)");
+GG_API int gg_set_transport_stash(gg_context* c, int32_t registers, int32_t swap_lanes, int32_t round_photons) {
+  if (!c || (registers != 0 && registers != 64 && registers != 80) || swap_lanes < 1 || swap_lanes > 32 ||
+      round_photons < 1 || round_photons > 2 * gg::kStashRecords)
+    return fail(GG_ERROR_INVALID_ARGUMENT,
+                "bad photon stash (registers 0, 64 or 80; swap_lanes 1..32; round_photons 1..64)");
   c->stash_registers = registers;
   c->stash_swap_lanes = swap_lanes;
+  c->stash_round_photons = round_photons;
   return GG_OK;
 }
 
-GG_API int gg_get_transport_stash(gg_context* c, int32_t* registers, int32_t* swap_lanes) {
+GG_API int gg_get_transport_stash(gg_context* c, int32_t* registers, int32_t* swap_lanes, int32_t* round_photons) {
   if (!c) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL context");
   if (registers) *registers = c->stash_registers;
   if (swap_lanes) *swap_lanes = c->stash_swap_lanes;
+  if (round_photons) *round_photons = c->stash_round_photons;
   return GG_OK;
 }
 
@@ -1160,11 +1170,12 @@ namespace {
 // registers), resident blocks per SM, the rare-phase regroup ratio, the block
 // size and the photons per thread (slots a lane claims per work-queue grab).
 struct LaunchShape {
-  int stash_registers, blocks_per_sm, regroup_ratio4, block_threads, slots_per_claim;
+  int stash_registers, blocks_per_sm, regroup_ratio4, block_threads, slots_per_claim, stash_round_photons;
 };
 
 void apply_shape(gg_context* c, const LaunchShape& s) {
   c->stash_registers = s.stash_registers;
+  c->stash_round_photons = s.stash_round_photons;
   c->blocks_per_sm = s.blocks_per_sm;
   c->regroup_lanes = 32;
   c->regroup_ratio4 = s.regroup_ratio4;
@@ -1179,7 +1190,8 @@ void apply_shape(gg_context* c, const LaunchShape& s) {
 //      many as the registers allow) x regroup ratio (3/4, 4/4, 6/4) at 256
 //      threads, one slot per claim;
 //   2. block size 128 and 512 at the same resident threads per SM as the best of 1;
-//   3. 2, 4 and 8 slots per claim at the best of 1-2.
+//   3. 2, 4 and 8 slots per claim at the best of 1-2;
+//   4. with the stash, 32 and 48 waiting photons per rare round (default 40).
 // The tallies are zeroed and the random states restored afterwards.
 int autotune(gg_context* c, const std::function<int()>& trial, float* best_ms) {
   GG_CUDA(cudaSetDevice(c->device));
@@ -1189,7 +1201,8 @@ int autotune(gg_context* c, const std::function<int()>& trial, float* best_ms) {
   auto restore = [&]() { return cudaMemcpyAsync(c->rng, saved, bytes, cudaMemcpyDeviceToDevice, c->stream); };
   cudaError_t e = cudaMemcpyAsync(saved, c->rng, bytes, cudaMemcpyDeviceToDevice, c->stream);
   const LaunchShape start{c->stash_registers, c->blocks_per_sm, c->regroup_ratio4, c->block_threads,
-                          c->slots_per_claim};
+                          c->slots_per_claim, c->stash_round_photons};
+  const int round0 = c->stash_round_photons;
   LaunchShape best = start;
   float best_time = -1.0f;
   int rc = GG_OK;
@@ -1206,15 +1219,20 @@ int autotune(gg_context* c, const std::function<int()>& trial, float* best_ms) {
   };
   for (int stash : {0, 64, 80})
     for (int bps = stash == 80 ? 3 : 4; bps >= 1; --bps)
-      for (int r : {3, 4, 6}) run({stash, bps, r, gg::kBlockThreads, 1});
+      for (int r : {3, 4, 6}) run({stash, bps, r, gg::kBlockThreads, 1, round0});
   const LaunchShape stage1 = best;
   for (int threads : {128, 512}) {
     const int bps = stage1.blocks_per_sm * gg::kBlockThreads / threads;
-    if (bps >= 1) run({stage1.stash_registers, bps, stage1.regroup_ratio4, threads, 1});
+    if (bps >= 1) run({stage1.stash_registers, bps, stage1.regroup_ratio4, threads, 1, round0});
   }
   const LaunchShape stage2 = best;
   for (int k : {2, 4, 8})
-    run({stage2.stash_registers, stage2.blocks_per_sm, stage2.regroup_ratio4, stage2.block_threads, k});
+    run({stage2.stash_registers, stage2.blocks_per_sm, stage2.regroup_ratio4, stage2.block_threads, k, round0});
+  const LaunchShape stage3 = best;
+  if (stage3.stash_registers != 0)
+    for (int t : {32, 48})
+      run({stage3.stash_registers, stage3.blocks_per_sm, stage3.regroup_ratio4, stage3.block_threads,
+           stage3.slots_per_claim, t});
   if (e == cudaSuccess) e = restore();
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   cudaFree(saved);

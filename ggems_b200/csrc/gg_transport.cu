@@ -1049,6 +1049,7 @@ __global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : ((kBatch
   const int regroup = P.regroup_lanes;
   const int ratio4 = P.regroup_ratio4;
   const int swap_lanes = P.stash_swap_lanes;
+  const int round_photons = P.stash_round_photons;
   for (;;) {
     bool round = false, serve_interact = false;
     if (kStash) {
@@ -1072,7 +1073,7 @@ __global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : ((kBatch
       const int n_find = __popc(waiting & ~w_int) + __popc(st_find);
       const int n_wait = __popc(waiting), n_track = __popc(active & ~waiting);
       round = n_int + n_find > 0 &&
-              (n_int >= 32 || n_find >= 32 || n_track == 0 ||
+              (n_int >= 32 || n_find >= 32 || n_int + n_find >= round_photons || n_track == 0 ||
                (n_wait > 0 && (n_wait >= regroup || 4 * n_wait >= ratio4 * n_track)));
       if (round) {
         serve_interact = n_int >= 32 ? (n_find < 32 || n_int >= n_find) : (n_find < 32 && n_int >= n_find);

@@ -330,11 +330,14 @@ GG_API int gg_get_transport_launch(gg_context* context, int32_t* block_threads, 
  * sampling) tracks a parked photon meanwhile, and the rare phases run on full
  * warps.  registers: 0 (off), 64 or 80 per thread (the kernel variant's
  * budget: 4 or 3 resident 256-thread blocks per SM); swap_lanes (1..32): the
- * waiting lanes that start an exchange.  Default 80 and 4 (environment
- * override at context creation: GGEMS_B200_STASH_REGISTERS).  The results do
- * not depend on it. */
-GG_API int gg_set_transport_stash(gg_context* context, int32_t registers, int32_t swap_lanes);
-GG_API int gg_get_transport_stash(gg_context* context, int32_t* registers, int32_t* swap_lanes);
+ * waiting lanes that start an exchange; round_photons (1..64): the photons of
+ * a warp (lanes and records) waiting for a rare phase that start a rare round.
+ * Default 80, 4 and 40 (environment overrides at context creation:
+ * GGEMS_B200_STASH_REGISTERS, GGEMS_B200_STASH_SWAP, GGEMS_B200_STASH_ROUND).
+ * The results do not depend on them. */
+GG_API int gg_set_transport_stash(gg_context* context, int32_t registers, int32_t swap_lanes, int32_t round_photons);
+GG_API int gg_get_transport_stash(gg_context* context, int32_t* registers, int32_t* swap_lanes,
+                                  int32_t* round_photons);
 GG_API int gg_autotune(gg_context* context, const gg_source* source, uint64_t number_of_particles,
                        float* best_milliseconds);
 GG_API int gg_autotune_jobs(gg_context* context, const gg_job* jobs, int32_t number_of_jobs, float* best_milliseconds);

@@ -160,7 +160,7 @@ def test_autotune_restores_state(ctx):
     ms = ctx.autotune(src.struct, 2 * abi.GG_MAXIMUM_PARTICLES)
     bps, lanes, ratio = ctx.tuning()
     threads, grain = ctx.launch()
-    stash, swap = ctx.stash()
+    stash, swap, rnd = ctx.stash()
     print("autotune: %.2f ms for 2^21 primaries with %d blocks/SM of %d threads, regroup ratio %d/4, "
           "%d slot(s) per claim, stash %d registers" % (ms, bps, threads, ratio, grain, stash))
     assert ms > 0 and 1 <= bps <= 8 and 1 <= lanes <= 32
@@ -190,12 +190,12 @@ def test_launch_shape_does_not_change_results(ctx):
     n = 2_500_000
     try:
         ref = parity.run_gpu(ctx, sc, src, n)
-        for threads, bps, grain, stash in ((128, 6, 1, 80), (512, 1, 4, 80), (256, 3, 8, 64), (256, 0, 1, 0),
-                                           (128, 0, 2, 0), (256, 0, 1, 64)):
+        for threads, bps, grain, stash, rnd in ((128, 6, 1, 80, 40), (512, 1, 4, 80, 64), (256, 3, 8, 64, 24),
+                                                (256, 0, 1, 0, 40), (128, 0, 2, 0, 40), (256, 0, 1, 64, 32)):
             ctx.set_launch(threads, grain)
             ctx.set_tuning(bps)
-            ctx.set_stash(stash, 1 if stash == 64 else 4)
-            shape = (threads, bps, grain, stash)
+            ctx.set_stash(stash, 1 if stash == 64 else 4, rnd)
+            shape = (threads, bps, grain, stash, rnd)
             P, T, st = parity.run_gpu(ctx, sc, src, n)
             assert np.array_equal(st, ref[2]), shape
             for f in ("E", "px", "py", "pz", "dx", "dy", "dz", "status", "scatter", "solid_id"):
