@@ -227,6 +227,34 @@ def cpu_reference_run(scene_ptr, source, n, threads, kind, states):
     return dt, counts
 
 
+def _cpu_sample(scene_ptr, source, what):
+    """About 10 s of the reference kernels on every host thread for `scene`."""
+    kind = _cpu_kind()
+    threads = os.cpu_count() or 1
+    st = _seed_states(777)
+    m = _sample_size(scene_ptr, source, threads, kind, 10.0, st)
+    dt, _ = cpu_reference_run(scene_ptr, source, m, threads, kind, st)
+    return {"value": m / dt, "unit": "primaries/s", "cores": threads, "kind": kind,
+            "sample": "%d primaries of %s (seed 777) on %d host threads, %.1f s, in a process that has not imported "
+                      "torch" % (m, what, threads, dt)}
+
+
+def _cpu_leg_process(args):
+    """_cpu_sample of this workload's scene in a process of its own that builds
+    the scene through the GGEMS API and imports no torch (it does hold a CUDA
+    context: the volume creator and GGEMS::Initialize need one)."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--workload", args.workload, "--cpu-leg", "--primaries",
+           str(args.primaries)]
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "LOCAL_RANK", "WORLD_SIZE")}
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=900, env=env)
+    for line in r.stdout.splitlines():
+        if line.startswith("{"):
+            d = json.loads(line).get("cpu_baseline")
+            if d:
+                return d
+    return {"unavailable": "CPU baseline process failed: " + (r.stderr.strip().splitlines() or ["?"])[-1]}
+
+
 def _cpu_kind():
     ref = os.path.join(ROOT, "oracle", "_ref", "libgg_ref.so")
     return "reference" if os.path.exists(ref) else "port"
@@ -344,6 +372,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned-surrogate measurement")
+    ap.add_argument("--cpu-leg", action="store_true",
+                    help="water / curved: print only the CPU baseline of the workload's scene (run by the bench "
+                         "itself in a process that imports no torch)")
     ap.add_argument("--workload", default="cbct",
                     choices=["cbct", "water", "batched", "mesh", "volume", "curved", "surrogate"],
                     help="cbct: the CBCT projection (default); water: 64^3 water dosimetry, 1e6 primaries; "
@@ -374,6 +405,16 @@ def main():
         return run_water(args, tmp, rank)
     if args.workload == "curved":
         return run_curved(args, tmp, rank)
+    # The CBCT line's CPU baseline is taken first, the way the reference arm
+    # takes it: on the B200 hosts it was measured on, the same host code ran
+    # ~1.6x slower (1.6x the user CPU time) once any process on the host had
+    # imported torch, even an idle one, and the timed GPU steps below need torch.
+    args.cpu_baseline_early = None
+    if args.workload == "cbct" and not args.no_cpu_baseline and rank == 0 and world == 1:
+        m = _reference_measurement(args.primaries, 2, 1)
+        m["cpu_baseline"]["sample"] += (", 1 warm-up and 2 timed runs before this process imports torch (the "
+                                        "reference arm's measurement)")
+        args.cpu_baseline_early = m["cpu_baseline"]
     if args.workload == "surrogate":
         if rank == 0:
             print(json.dumps(surrogate_measurement(tmp) or {"unavailable": "no trained network"}), flush=True)
@@ -498,13 +539,7 @@ def main():
     kind = _cpu_kind()
     ref_states = _seed_states(777)
     if not args.no_cpu_baseline and world == 1:
-        threads = os.cpu_count() or 1
-        k, n = _cbct_sample(scene_ptr, src, threads, kind, 4.0, ref_states, args.primaries)
-        dts = [cpu_reference_run(scene_ptr, src, n, threads, kind, ref_states)[0] for _ in range(3)]
-        dt = statistics.median(dts)
-        cpu_baseline = {"value": n / dt, "unit": "primaries/s", "cores": threads, "kind": kind,
-                        "sample": "the projection's first %d of %d batches (%d primaries, seed 777) on %d host "
-                                  "threads, median of 3 runs of %.1f s" % (k, batches, n, threads, dt)}
+        cpu_baseline = args.cpu_baseline_early
     _, counts = cpu_reference_run(scene_ptr, src, 20000 if args.no_cpu_baseline else 100000, os.cpu_count() or 1,
                                   "port", ref_states)
     S, box, D, H = counts
@@ -749,7 +784,6 @@ def run_curved(args, tmp, rank):
     API.  One step = one projection of --primaries; `cpu_baseline` = the same scene
     on the host cores."""
     import numpy as np
-    import torch
     import ggems_b200 as gg
     from ggems_b200 import abi, workloads
     from ggems_b200.api import lib
@@ -808,6 +842,10 @@ def run_curved(args, tmp, rank):
     assert lib.ggems_source_descriptor(0, C.byref(s), None) == 0
     scene_ptr = lib.ggems_scene(ggems.obj)
     sc = scene_ptr.contents
+    if args.cpu_leg:
+        print(json.dumps({"cpu_baseline": _cpu_sample(scene_ptr, s, "the same projection")}), flush=True)
+        return 0
+    import torch
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
     def step():
@@ -828,15 +866,7 @@ def run_curved(args, tmp, rank):
             times.append(t)
             launches += n
     total_ms = sum(times)
-    cpu = None
-    if not args.no_cpu_baseline:
-        kind = _cpu_kind()
-        threads = os.cpu_count() or 1
-        st = _seed_states(777)
-        m = _sample_size(scene_ptr, s, threads, kind, 10.0, st)
-        dt, _ = cpu_reference_run(scene_ptr, s, m, threads, kind, st)
-        cpu = {"value": m / dt, "unit": "primaries/s", "cores": threads, "kind": kind,
-               "sample": "%d primaries of the same projection (seed 777) on %d host threads, %.1f s" % (m, threads, dt)}
+    cpu = None if args.no_cpu_baseline else _cpu_leg_process(args)
     if rank == 0:
         print(json.dumps({
             "metric": "primaries/s (curved 46-module CT)", "value": args.primaries * args.steps / (total_ms * 1e-3),
@@ -858,7 +888,6 @@ def run_water(args, tmp, rank):
     launch; `e2e` = scene and random states uploaded, run, dose finalised and
     tallies read back to host memory, wall-clocked."""
     import numpy as np
-    import torch
     from ggems_b200 import abi, workloads
     from ggems_b200.api import lib
     n = 1_000_000 if args.primaries == PRIMARIES else args.primaries
@@ -871,6 +900,10 @@ def run_water(args, tmp, rank):
     assert lib.ggems_source_descriptor(0, C.byref(src), None) == 0
     scene_ptr = lib.ggems_scene(ggems.obj)
     sc = scene_ptr.contents
+    if args.cpu_leg:
+        print(json.dumps({"cpu_baseline": _cpu_sample(scene_ptr, src, "the same run")}), flush=True)
+        return 0
+    import torch
     dm = sc.dose_maps[0]
     nd = int(dm.total_number_of_dosels)
     dose, unc = np.empty(nd, np.float32), np.empty(nd, np.float32)
@@ -913,15 +946,7 @@ def run_water(args, tmp, rank):
         check(lib.gg_read_tallies(ctx, C.byref(tallies.struct)), "gg_read_tallies")
         if k:
             e2e.append(time.perf_counter() - t0)
-    cpu = None
-    if not args.no_cpu_baseline:
-        kind = _cpu_kind()
-        threads = os.cpu_count() or 1
-        st = _seed_states(777)
-        m = _sample_size(scene_ptr, src, threads, kind, 10.0, st)
-        dt, _ = cpu_reference_run(scene_ptr, src, m, threads, kind, st)
-        cpu = {"value": m / dt, "unit": "primaries/s", "cores": threads, "kind": kind,
-               "sample": "%d primaries of the same run (seed 777) on %d host threads, %.1f s" % (m, threads, dt)}
+    cpu = None if args.no_cpu_baseline else _cpu_leg_process(args)
     if rank == 0:
         print(json.dumps({
             "metric": "primaries/s (64^3 water dosimetry, 60 keV)", "value": value, "unit": "primaries/s",
@@ -1034,18 +1059,11 @@ def run_volume(args, rank):
     return 0
 
 
-def run_reference_arm(args, rank, world):
-    """The reference's CPU implementation of the path on all host threads:
-    GGEMS's own kernels built for the host (oracle/_ref) when available, else
-    the oracle port, replaying GGEMS::RunOnDevice batch by batch.  The scene,
-    tables and random streams come from the oracle side (tests/scenes.py:
-    GGEMS's own host table builders, oracle/_ref/libgg_ref_tables.so, else the
-    oracle's restatement; GGEMS's mt19937 seeding), so nothing of the product
-    library is loaded.  Each step is a bounded sample of the projection
-    (its first whole batches, the same slots and streams as the projection);
-    `config` is the product arm's."""
-    if rank != 0:
-        return 0
+def _reference_measurement(primaries, steps, warmup):
+    """GGEMS's kernels built for the host (oracle/_ref; else the oracle port)
+    on all host threads, replaying GGEMS::RunOnDevice batch by batch on the
+    CBCT scene built from the oracle side, `warmup` untimed and `steps` timed
+    runs, each of the projection's first whole batches."""
     _ensure_oracle()
     kind = _cpu_kind()
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -1058,22 +1076,40 @@ def run_reference_arm(args, rank, world):
     src = source.struct
     states = scenes.seed_states(777)
     threads = os.cpu_count() or 1
-    budget = min(8.0, max(1.0, 150.0 / max(args.steps + args.warmup, 1)))
-    k, n = _cbct_sample(scene_ptr, src, threads, kind, budget, states, args.primaries)
-    for _ in range(args.warmup):
+    budget = min(8.0, max(1.0, 150.0 / max(steps + warmup, 1)))
+    k, n = _cbct_sample(scene_ptr, src, threads, kind, budget, states, primaries)
+    for _ in range(warmup):
         cpu_reference_run(scene_ptr, src, n, threads, kind, states)
-    times = [cpu_reference_run(scene_ptr, src, n, threads, kind, states)[0] for _ in range(args.steps)]
-    value = n * args.steps / sum(times)
-    batches = len(_batch_sizes(args.primaries))
+    times = [cpu_reference_run(scene_ptr, src, n, threads, kind, states)[0] for _ in range(steps)]
+    value = n * steps / sum(times)
+    batches = len(_batch_sizes(primaries))
     sample = ("each step: the projection's first %d of %d batches (%d primaries, seed 777) on %d host threads"
               % (k, batches, n, threads))
+    return {"value": value, "times": times, "batches": batches,
+            "cpu_baseline": {"value": value, "unit": "primaries/s", "cores": threads, "kind": kind, "sample": sample}}
+
+
+def run_reference_arm(args, rank, world):
+    """The reference's CPU implementation of the path on all host threads:
+    GGEMS's own kernels built for the host (oracle/_ref) when available, else
+    the oracle port, replaying GGEMS::RunOnDevice batch by batch.  The scene,
+    tables and random streams come from the oracle side (tests/scenes.py:
+    GGEMS's own host table builders, oracle/_ref/libgg_ref_tables.so, else the
+    oracle's restatement; GGEMS's mt19937 seeding), so nothing of the product
+    library is loaded.  Each step is a bounded sample of the projection
+    (its first whole batches, the same slots and streams as the projection);
+    `config` is the product arm's."""
+    if rank != 0:
+        return 0
+    m = _reference_measurement(args.primaries, args.steps, args.warmup)
+    value, times, batches = m["value"], m["times"], m["batches"]
     print(json.dumps({
         "impl": "reference", "metric": "primaries/s (CBCT 256^3, 120 kVp)", "value": value, "unit": "primaries/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded phantom generator, synthetic 120 kVp spectrum)",
         "config": _cbct_config(args.primaries, batches, world),
-        "cpu_baseline": {"value": value, "unit": "primaries/s", "cores": threads, "kind": kind, "sample": sample},
+        "cpu_baseline": m["cpu_baseline"],
         "e2e": {"value": value, "unit": "primaries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
     return 0

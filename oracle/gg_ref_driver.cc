@@ -9,11 +9,15 @@
 //
 // Exposes gg_ref_run() with the signature of gg_oracle_run(), so tests can
 // pin the oracle restatement against the reference's own kernel code.  Built
-// by oracle/build_ref.py into oracle/_ref/ (never committed, never shipped).
+// by oracle/build.py into oracle/_ref/ (never committed, never shipped).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <functional>
 #include <memory>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -78,6 +82,78 @@ void draw_ggems_sphere_float(ulong, float3, int3, float3, float, float, float*);
 
 namespace {
 
+// One kernel launch of n work items on `threads` host threads, the way an
+// OpenCL CPU runtime runs an NDRange: a pool of worker threads created once per
+// process (not per launch) takes the items in chunks from a shared counter, so
+// a core that is busy with something else delays only the chunks it holds.
+class Pool {
+ public:
+  ~Pool() {
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      stop_ = true;
+    }
+    wake_.notify_all();
+    for (auto& t : workers_) t.join();
+  }
+  void run(size_t n, int threads, const std::function<void(size_t, size_t)>& body) {
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      while (static_cast<int>(workers_.size()) < threads - 1) {
+        const int index = static_cast<int>(workers_.size());
+        workers_.emplace_back([this, index, seen = generation_]() { loop(index, seen); });
+      }
+      body_ = &body;
+      n_ = n;
+      chunk_ = std::max<size_t>(64, n / (static_cast<size_t>(threads) * 64));
+      next_.store(0);
+      helpers_ = threads - 1;
+      running_ = static_cast<int>(workers_.size());
+      ++generation_;
+    }
+    wake_.notify_all();
+    work();
+    std::unique_lock<std::mutex> lk(m_);
+    done_.wait(lk, [this]() { return running_ == 0; });
+  }
+
+ private:
+  void work() {
+    for (;;) {
+      const size_t b = next_.fetch_add(chunk_);
+      if (b >= n_) return;
+      (*body_)(b, std::min(n_, b + chunk_));
+    }
+  }
+  void loop(int index, uint64_t seen) {
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(m_);
+        wake_.wait(lk, [&]() { return stop_ || generation_ != seen; });
+        if (stop_) return;
+        seen = generation_;
+      }
+      if (index < helpers_) work();
+      std::lock_guard<std::mutex> lk(m_);
+      if (--running_ == 0) done_.notify_one();
+    }
+  }
+  std::mutex m_;
+  std::condition_variable wake_, done_;
+  std::vector<std::thread> workers_;
+  const std::function<void(size_t, size_t)>* body_ = nullptr;
+  size_t n_ = 0, chunk_ = 1;
+  std::atomic<size_t> next_{0};
+  uint64_t generation_ = 0;
+  int helpers_ = 0, running_ = 0;
+  bool stop_ = false;
+};
+
+Pool& pool() {
+  static Pool p;
+  return p;
+}
+
 template <class F>
 void parallel_for(size_t n, int threads, F f) {
   if (threads <= 1 || n < 4096) {
@@ -87,17 +163,13 @@ void parallel_for(size_t n, int threads, F f) {
     }
     return;
   }
-  std::vector<std::thread> pool;
-  for (int t = 0; t < threads; ++t) {
-    size_t b = n * t / threads, e = n * (t + 1) / threads;
-    pool.emplace_back([b, e, &f]() {
-      for (size_t i = b; i < e; ++i) {
-        gg_shim_global_id = i;
-        f();
-      }
-    });
-  }
-  for (auto& th : pool) th.join();
+  const std::function<void(size_t, size_t)> body = [&f](size_t b, size_t e) {
+    for (size_t i = b; i < e; ++i) {
+      gg_shim_global_id = i;
+      f();
+    }
+  };
+  pool().run(n, threads, body);
 }
 
 void set_obb(GGEMSOBB& o, const gg_obb& g) {
