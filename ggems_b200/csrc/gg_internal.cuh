@@ -29,15 +29,17 @@ constexpr int kBlockThreads = 256;  // default transport block size (the autotun
 // Fixed-point scale of the energy tally: edep is accumulated as int64 multiples of 2^-32 MeV.
 constexpr double kEdepScale = 4294967296.0;
 
-struct DevNavigator {
+struct alignas(16) DevNavigator {
+  // read by every tracking step: the first 16 bytes, one vector load
   int32_t number_of_bins;
+  uint32_t process_pack;         // number_of_processes | process_id[0] << 8 | process_id[1] << 16 | process_id[2] << 24
+  // byte offsets into the table blob (shared memory copy when it fits)
+  uint32_t sigma_offset;         // float4[number_of_materials * number_of_bins]
+  uint32_t photon_cut_offset;    // float[number_of_materials]
   int32_t number_of_materials;
   int32_t number_of_processes;
   int32_t process_id[3];
-  // byte offsets into the table blob (shared memory copy when it fits)
   uint32_t energy_bins_offset;   // float[number_of_bins]
-  uint32_t sigma_offset;         // float4[number_of_materials * number_of_bins]
-  uint32_t photon_cut_offset;    // float[number_of_materials]
   uint32_t attenuation_offset;   // float[GG_ATTENUATION_BINS] energies, then mu_en (TLE navigators only)
   // HBM arrays read on Rayleigh interactions
   const int32_t* number_of_elements;
@@ -61,18 +63,19 @@ struct DevDoseMap {
   int32_t* photon_tracking;      // nullptr when not recorded
 };
 
-struct DevSolid {
-  int32_t type;
-  int32_t navigator;
-  float matrix[16];
+struct alignas(16) DevSolid {
+  // read by every tracking step: the first 80 bytes, five vector loads
   float border_min[3];
   float border_max[3];
-  float threshold;
-  int32_t number_of_voxels[3];
   float voxel_sizes[3];
   float inv_voxel_sizes[3];      // exact 2^-k when voxel_pow2
-  int32_t voxel_pow2;            // every voxel size is a power of two
+  int32_t number_of_voxels[3];
+  int32_t navigator;
   const uint8_t* labels;
+  int32_t type;
+  int32_t voxel_pow2;            // every voxel size is a power of two
+  float matrix[16];
+  float threshold;
   int32_t virtual_element_number[3];
   float box_size[3];
   int32_t* histogram;            // nullptr when none

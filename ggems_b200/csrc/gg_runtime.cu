@@ -636,6 +636,8 @@ GG_API int gg_upload_scene(gg_context* c, const gg_scene* sc) {
     d.number_of_materials = t.number_of_materials;
     d.number_of_processes = t.number_of_processes;
     for (int p = 0; p < 3; ++p) d.process_id[p] = t.process_id[p];
+    d.process_pack = static_cast<uint32_t>(t.number_of_processes);
+    for (int p = 0; p < t.number_of_processes; ++p) d.process_pack |= static_cast<uint32_t>(t.process_id[p]) << (8 * (p + 1));
     const uint32_t nb = t.number_of_bins, nm = t.number_of_materials;
     d.energy_bins_offset = static_cast<uint32_t>(blob.size());
     blob.resize(align16(d.energy_bins_offset + nb * 4), 0);
@@ -966,7 +968,8 @@ int prepare_jobs(gg_context* c, const gg_job* jobs, int32_t n, std::vector<void*
     aux = true;  // the world walk lives in the full kernel variant
   }
   const bool batch = P.number_of_jobs > 1;
-  const int stash = (mesh || aux) ? 0 : (c->stash_registers == 64 ? 1 : (c->stash_registers == 80 ? 2 : 0));
+  // meshed scenes: the 80-register stash variant only (the mesh variant has 80 registers already)
+  const int stash = aux ? 0 : (c->stash_registers == 64 ? (mesh ? 2 : 1) : (c->stash_registers == 80 ? 2 : 0));
   out->smem = (c->tables_in_smem ? c->table_bytes : 0) + sizeof(gg::DevSolid) * c->number_of_solids +
               sizeof(gg::DevNavigator) * c->number_of_navigators + 16;
   if (stash) out->smem += (c->block_threads / 32) * gg::stash_bytes_per_warp(batch, false);

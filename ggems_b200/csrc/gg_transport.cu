@@ -237,14 +237,18 @@ struct Tab {
 __device__ __forceinline__ float pick(float4 s, int pid) { return pid == 0 ? s.x : (pid == 1 ? s.y : s.z); }
 
 // GetPhotonNextInteraction, GGEMSPhotonNavigator.hh:57-93.  Returns the
-// distance, writes the process; energy_id is the cached BinarySearch result.
-__device__ __forceinline__ float next_interaction(Kiss& rng, const DevNavigator& nv, const float4* sig, int energy_id,
-                                                  int material, int& proc) {
-  float4 s = sig[material * nv.number_of_bins + energy_id];
+// distance, writes the process; energy_id is the cached BinarySearch result,
+// process_pack the navigator's process count and ids (DevNavigator).
+__device__ __forceinline__ float next_interaction(Kiss& rng, int number_of_bins, uint32_t process_pack,
+                                                  const float4* sig, int energy_id, int material, int& proc) {
+  float4 s = sig[material * number_of_bins + energy_id];
   float nid = kOutOfWorld;
   proc = kNoProcess;
-  for (int i = 0; i < nv.number_of_processes; ++i) {
-    int pid = nv.process_id[i];
+  const int n = static_cast<int>(process_pack & 0xffu);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    if (i >= n) break;
+    const int pid = static_cast<int>((process_pack >> (8 * (i + 1))) & 0xffu);
     float dist = -logf(rng.uniform()) / pick(s, pid);
     if (dist < nid) {
       nid = dist;
@@ -253,6 +257,10 @@ __device__ __forceinline__ float next_interaction(Kiss& rng, const DevNavigator&
   }
   return nid;
 }
+
+// 16-byte shared-memory (or global) loads of a struct's leading fields.
+__device__ __forceinline__ float4 load4f(const void* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ int4 load4i(const void* p) { return *reinterpret_cast<const int4*>(p); }
 
 // State handed to and returned by the (out-of-line) interaction samplers.
 // Passed by value so that the photon and its random state stay in registers
@@ -1212,14 +1220,21 @@ __global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : ((kBatch
     {
 
     // ---- one tracking step inside solid ph.solid_id ----
+    // the solid's and navigator's per-step fields in six 16-byte loads
+    // (DevSolid / DevNavigator lead with them)
     const DevSolid& so = solids[ph.solid_id];
-    const int nav = so.navigator;
-    const DevNavigator& nv = navs[nav];
-    const float4* sig = tab.sigma(nav);
-    V3 bmin = v3(so.border_min[0], so.border_min[1], so.border_min[2]);
-    V3 bmax = v3(so.border_max[0], so.border_max[1], so.border_max[2]);
+    const float4 s0 = load4f(&so.border_min[0]);     // border_min xyz, border_max x
+    const float4 s1 = load4f(&so.border_max[1]);     // border_max yz, voxel_sizes xy
+    const float4 s2 = load4f(&so.voxel_sizes[2]);    // voxel_sizes z, inv_voxel_sizes xyz
+    const int4 s3 = load4i(&so.number_of_voxels[0]);  // number_of_voxels xyz, navigator
+    const int4 s4 = load4i(&so.labels);               // labels (2 words), type, voxel_pow2
+    const int nav = s3.w;
+    const int4 n0 = load4i(&navs[nav]);               // number_of_bins, process_pack, sigma / cut offsets
+    const float4* sig = reinterpret_cast<const float4*>(tab.base + static_cast<uint32_t>(n0.z));
+    V3 bmin = v3(s0.x, s0.y, s0.z);
+    V3 bmax = v3(s0.w, s1.x, s1.y);
     if (ph.E != cached_E || nav != cached_nav) {
-      energy_id = binary_search(ph.E, tab.energy_bins(nav), nv.number_of_bins);
+      energy_id = binary_search(ph.E, tab.energy_bins(nav), n0.x);
       cached_E = ph.E;
       cached_nav = nav;
     }
@@ -1235,23 +1250,25 @@ __global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : ((kBatch
       V3 vmin = bmin, vmax = bmax;
       int material = 0;
       if (voxel) {
-        V3 vs = v3(so.voxel_sizes[0], so.voxel_sizes[1], so.voxel_sizes[2]);
+        V3 vs = v3(s1.z, s1.w, s2.x);
         V3 q = sub(ph.p, bmin);
-        q = so.voxel_pow2 ? mul(q, v3(so.inv_voxel_sizes[0], so.inv_voxel_sizes[1], so.inv_voxel_sizes[2])) : divv(q, vs);
+        q = s4.w ? mul(q, v3(s2.y, s2.z, s2.w)) : divv(q, vs);
         int ix = __float2int_rz(q.x), iy = __float2int_rz(q.y), iz = __float2int_rz(q.z);
-        const int nx = so.number_of_voxels[0], ny = so.number_of_voxels[1], nz = so.number_of_voxels[2];
+        const int nx = s3.x, ny = s3.y, nz = s3.z;
         if (ix >= nx || iy >= ny || iz >= nz || ix < 0 || iy < 0 || iz < 0) {
           ph.psd = kOutOfWorld;
           ph.solid_id = -1;
           leave = 1;
           break;
         }
-        material = __ldg(so.labels + (ix + iy * nx + iz * nx * ny));
+        const uint8_t* labels = reinterpret_cast<const uint8_t*>(
+            (static_cast<unsigned long long>(static_cast<uint32_t>(s4.y)) << 32) | static_cast<uint32_t>(s4.x));
+        material = __ldg(labels + (ix + iy * nx + iz * nx * ny));
         vmin = add(bmin, mul(v3(static_cast<float>(ix), static_cast<float>(iy), static_cast<float>(iz)), vs));
         vmax = add(vmin, vs);
       }
       int proc;
-      float nid = next_interaction(rng, nv, sig, energy_id, material, proc);
+      float nid = next_interaction(rng, n0.x, static_cast<uint32_t>(n0.y), sig, energy_id, material, proc);
       ph.p = safety_inside(ph.p, vmin, vmax);
       float dtb = distance_to_aabb(ph.p, ph.d, inv_d, vmin, vmax);
       if (dtb <= nid) {
@@ -1297,7 +1314,7 @@ __global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : ((kBatch
           ph.status = GG_DEAD;
           ph.E = 0.0f;
         }
-        if (ph.E <= tab.photon_cut(nav)[material]) {
+        if (ph.E <= reinterpret_cast<const float*>(tab.base + static_cast<uint32_t>(n0.w))[material]) {
           if (kDose && so.dose_map >= 0) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
           ph.status = GG_DEAD;
         }
@@ -1322,7 +1339,7 @@ __global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : ((kBatch
         next = x.second;
       }
       int proc;
-      float nid = next_interaction(rng, nv, sig, energy_id, 0, proc);
+      float nid = next_interaction(rng, n0.x, static_cast<uint32_t>(n0.y), sig, energy_id, 0, proc);
       const float dx = next.x - ph.p.x, dy = next.y - ph.p.y, dz = next.z - ph.p.z;
       const float to_next = sqrtf(dx * dx + dy * dy + dz * dz);
       if (to_next <= nid) {
@@ -1348,7 +1365,7 @@ __global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : ((kBatch
         ph.status = GG_DEAD;
         ph.E = 0.0f;
       }
-      if (ph.E <= tab.photon_cut(nav)[0]) {
+      if (ph.E <= reinterpret_cast<const float*>(tab.base + static_cast<uint32_t>(n0.w))[0]) {
         if ((kDose && so.dose_map >= 0)) dose_record(P.dose_maps[so.dose_map], ph.E, ph.p);
         ph.status = GG_DEAD;
       }
@@ -1414,7 +1431,10 @@ using TransportKernel = void (*)(TransportParams);
 // particle tracking).
 TransportKernel transport_variant(bool mesh, bool batch, bool dose, bool aux, int stash) {
   if (aux) return batch ? transport_kernel<true, true, true, true, 0> : transport_kernel<true, false, true, true, 0>;
-  if (mesh) return batch ? transport_kernel<true, true, true, false, 0> : transport_kernel<true, false, true, false, 0>;
+  if (mesh) {
+    if (stash) return batch ? transport_kernel<true, true, true, false, 2> : transport_kernel<true, false, true, false, 2>;
+    return batch ? transport_kernel<true, true, true, false, 0> : transport_kernel<true, false, true, false, 0>;
+  }
   if (stash == 1) {
     if (dose) return batch ? transport_kernel<false, true, true, false, 1> : transport_kernel<false, false, true, false, 1>;
     return batch ? transport_kernel<false, true, false, false, 1> : transport_kernel<false, false, false, false, 1>;

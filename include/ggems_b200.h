@@ -323,8 +323,8 @@ GG_API int gg_get_transport_tuning(gg_context* context, int32_t* blocks_per_sm, 
                                    int32_t* regroup_ratio4);
 GG_API int gg_set_transport_launch(gg_context* context, int32_t block_threads, int32_t slots_per_claim);
 GG_API int gg_get_transport_launch(gg_context* context, int32_t* block_threads, int32_t* slots_per_claim);
-/* Photon stash (voxelized and box solids without a world grid or particle
- * tracking; meshed scenes ignore it): each warp parks a second set of photons
+/* Photon stash (scenes without a world grid or particle tracking; meshed
+ * scenes use it at 80 registers whenever it is on): each warp parks a second set of photons
  * in shared memory and exchanges them with its lanes, so that a lane whose
  * photon waits for a rare phase (new history, FindSolid, Compton / Rayleigh
  * sampling) tracks a parked photon meanwhile, and the rare phases run on full
