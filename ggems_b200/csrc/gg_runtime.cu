@@ -495,7 +495,7 @@ GG_API int gg_context_create(int32_t device_index, gg_context** context) {
   }
   if (const char* v = std::getenv("GGEMS_B200_STASH_ROUND")) {
     int r = std::atoi(v);
-    if (r >= 1 && r <= 64) c->stash_round_photons = r;
+    if (r >= 1 && r <= 2 * gg::kStashRecords) c->stash_round_photons = r;
   }
   if (const char* v = std::getenv("GGEMS_B200_STASH_REGISTERS")) {
     int r = std::atoi(v);

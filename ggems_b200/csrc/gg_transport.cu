@@ -28,6 +28,7 @@
 // multiply-add is contracted; the CPU oracle does the same.
 #include <cfloat>
 #include <cstdint>
+#include <type_traits>
 
 #include "gg_internal.cuh"
 
@@ -774,6 +775,20 @@ __device__ bool stage_tables(unsigned char* dst, const unsigned char* src, uint3
 
 extern __shared__ __align__(16) unsigned char g_smem[];
 
+// Masks over a warp's stash records (one bit per record).
+using StashMask = std::conditional_t<(kStashRecords > 32), unsigned long long, unsigned>;
+__device__ __forceinline__ int stash_popc(unsigned m) { return __popc(m); }
+__device__ __forceinline__ int stash_popc(unsigned long long m) { return __popcll(m); }
+// 32-bit part h of a mask, and a 32-bit part placed at h
+__device__ __forceinline__ unsigned stash_part(StashMask m, int h) {
+  if constexpr (kStashRecords > 32) return static_cast<unsigned>(m >> (32 * h));
+  else return m;
+}
+__device__ __forceinline__ StashMask stash_mask(unsigned part, int h) {
+  if constexpr (kStashRecords > 32) return static_cast<StashMask>(part) << (32 * h);
+  else return part;
+}
+
 // Register budget of a variant: what 256-thread blocks need to keep `blocks`
 // of them resident per SM (64, 80 or 128 registers), fixed per kernel so that
 // the block size stays a launch parameter (128, 256 or 512 threads).
@@ -929,7 +944,7 @@ __global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : ((kBatch
   const unsigned lanes_below = (1u << lane) - 1u;
   uint32_t* w_stash = nullptr;
   int* w_index = nullptr;
-  unsigned st_ready = 0, st_int = 0, st_find = 0;
+  StashMask st_ready = 0, st_int = 0, st_find = 0;
   if (kStash) {
     uint32_t* base = reinterpret_cast<uint32_t*>(bar + 2);
     w_stash = base + (threadIdx.x >> 5) * (kWords * kStashRecords + kStashRecords);
@@ -992,13 +1007,19 @@ __global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : ((kBatch
   };
   // The k-th lane of `lanes` (in lane order) gets the k-th record of
   // `records`; -1 for the other lanes.  Called by the whole warp.
-  auto match = [&](unsigned lanes, unsigned records) -> int {
-    if ((records >> lane) & 1u) w_index[__popc(records & lanes_below)] = lane;
+  auto match = [&](unsigned lanes, StashMask records) -> int {
+    int ranked = 0;
+#pragma unroll
+    for (int h = 0; h < kStashRecords / 32; ++h) {
+      const unsigned part = stash_part(records, h);
+      if ((part >> lane) & 1u) w_index[ranked + __popc(part & lanes_below)] = lane + 32 * h;
+      ranked += __popc(part);
+    }
     __syncwarp();
     int r = -1;
     if ((lanes >> lane) & 1u) {
       const int k = __popc(lanes & lanes_below);
-      if (k < __popc(records)) r = w_index[k];
+      if (k < ranked) r = w_index[k];
     }
     __syncwarp();
     return r;
@@ -1006,15 +1027,19 @@ __global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : ((kBatch
   auto is_rare = [](int ph_phase) { return ph_phase == kNewHistory || ph_phase == kFind || ph_phase == kInteract; };
   // Lanes of `lanes` exchange their photons with records of `records`; the
   // masks then say what each touched record holds.  Called by the whole warp.
-  auto exchange = [&](unsigned lanes, unsigned records) {
+  auto exchange = [&](unsigned lanes, StashMask records) {
     const int r = match(lanes, records);
     const int old = phase;
     if (r >= 0) swap_record(r);
-    const unsigned bit = r >= 0 ? (1u << r) : 0u;
-    const unsigned moved = __reduce_or_sync(0xffffffffu, bit);
-    const unsigned to_int = __reduce_or_sync(0xffffffffu, old == kInteract ? bit : 0u);
-    const unsigned to_find = __reduce_or_sync(0xffffffffu, (old == kNewHistory || old == kFind) ? bit : 0u);
-    const unsigned to_empty = __reduce_or_sync(0xffffffffu, old == kDone ? bit : 0u);
+    StashMask moved = 0, to_int = 0, to_find = 0, to_empty = 0;
+#pragma unroll
+    for (int h = 0; h < kStashRecords / 32; ++h) {
+      const unsigned bit = (r >= 32 * h && r < 32 * h + 32) ? (1u << (r - 32 * h)) : 0u;
+      moved |= stash_mask(__reduce_or_sync(0xffffffffu, bit), h);
+      to_int |= stash_mask(__reduce_or_sync(0xffffffffu, old == kInteract ? bit : 0u), h);
+      to_find |= stash_mask(__reduce_or_sync(0xffffffffu, (old == kNewHistory || old == kFind) ? bit : 0u), h);
+      to_empty |= stash_mask(__reduce_or_sync(0xffffffffu, old == kDone ? bit : 0u), h);
+    }
     st_int = (st_int & ~moved) | to_int;
     st_find = (st_find & ~moved) | to_find;
     st_ready = (st_ready & ~moved) | (moved & ~(to_int | to_find | to_empty));
@@ -1022,10 +1047,12 @@ __global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : ((kBatch
 
   if (kStash) {
     // Fill the records first: each lane claims a slot (a run of its own) for
-    // record `lane`, then one for itself.
+    // records lane, lane + 32, ..., then one for itself.
+#pragma unroll 1
+    for (int h = 0; h < kStashRecords / 32; ++h) {
     phase = next_slot() ? kNewHistory : kDone;
-    st_find = __ballot_sync(0xffffffffu, phase == kNewHistory);
-    swap_record(lane);  // the lane receives whatever the record held before: reset below
+    st_find |= stash_mask(__ballot_sync(0xffffffffu, phase == kNewHistory), h);
+    swap_record(lane + 32 * h);  // the lane receives whatever the record held before: reset below
     slot = ~0u;
     histories_left = 0;
     rounds = 0;
@@ -1042,6 +1069,7 @@ __global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : ((kBatch
       solids = scene_solids;
     }
     phase = kDone;
+    }
   }
   if (next_slot()) phase = kNewHistory;
 
@@ -1068,7 +1096,7 @@ __global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : ((kBatch
       // ready photons from the stash (once enough of them wait: an exchange
       // costs the warp two shared-memory accesses per word).
       const unsigned want = waiting | ~active;
-      if (st_ready != 0 && __popc(want) >= min(swap_lanes, __popc(st_ready))) {
+      if (st_ready != 0 && __popc(want) >= min(swap_lanes, stash_popc(st_ready))) {
         exchange(want, st_ready);
         active = __ballot_sync(0xffffffffu, phase != kDone);
         waiting = __ballot_sync(0xffffffffu, is_rare(phase));
@@ -1077,8 +1105,8 @@ __global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : ((kBatch
       // (lanes and records), or when the waiting lanes are many against the
       // tracking ones and no ready photon is left to replace them.
       const unsigned w_int = __ballot_sync(0xffffffffu, phase == kInteract);
-      const int n_int = __popc(w_int) + __popc(st_int);
-      const int n_find = __popc(waiting & ~w_int) + __popc(st_find);
+      const int n_int = __popc(w_int) + stash_popc(st_int);
+      const int n_find = __popc(waiting & ~w_int) + stash_popc(st_find);
       const int n_wait = __popc(waiting), n_track = __popc(active & ~waiting);
       round = n_int + n_find > 0 &&
               (n_int >= 32 || n_find >= 32 || n_int + n_find >= round_photons || n_track == 0 ||
@@ -1087,7 +1115,7 @@ __global__ void __maxnreg__(transport_registers(kAux ? 2 : (kFull ? 3 : ((kBatch
         serve_interact = n_int >= 32 ? (n_find < 32 || n_int >= n_find) : (n_find < 32 && n_int >= n_find);
         // gather: lanes without a photon of the served kind take one from the stash
         const unsigned kind_lanes = serve_interact ? w_int : (waiting & ~w_int);
-        const unsigned kind_records = serve_interact ? st_int : st_find;
+        const StashMask kind_records = serve_interact ? st_int : st_find;
         if (kind_records != 0 && kind_lanes != 0xffffffffu) exchange(~kind_lanes, kind_records);
       }
     } else {
