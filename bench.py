@@ -317,7 +317,7 @@ def surrogate_measurement(tmp, angles=360, reference_every=10):
         return None
     out = os.path.join(tmp, "surrogate.json")
     cmd = [sys.executable, "-m", "ggems_b200.scatter", "--load", SURROGATE_NET, "--test", "0", "--angles",
-           str(angles), "--reference-every", str(reference_every), "--json-out", out]
+           str(angles), "--reference-every", str(reference_every), "--batch", "40", "--json-out", out]
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=1200)
     if r.returncode != 0:
         return {"error": (r.stdout + r.stderr)[-800:]}

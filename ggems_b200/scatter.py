@@ -38,7 +38,15 @@ MATERIALS = os.path.join(ROOT, "ggems_b200", "data", "materials.txt")
 PHANTOM_N, PHANTOM_VOXEL = 64, 2.0
 ENERGY_MEV = 0.060
 JUDGE_TOLERANCE = 0.05
-JUDGE_BLOCKS_PER_SM = 3  # transport CTAs per SM for the judge MC (0: as many as fit)
+# Launch shape of the judge MC, a persistent kernel that holds its SMs for the
+# whole scan: transport CTAs per SM and the photon stash's register budget (0:
+# off); GGEMS_B200_JUDGE="blocks,registers" overrides both.  Measured on the
+# 360-angle scan (projections/s): 3 CTAs with the 80-register stash 657, with
+# the 64-register one 589, without the stash 577; 2 CTAs (more room for the
+# network's kernels beside it) 534 / 521 / 345: a slower MC costs more than
+# the overlap gains.
+JUDGE_BLOCKS_PER_SM, JUDGE_STASH_REGISTERS = (
+    tuple(int(v) for v in os.environ["GGEMS_B200_JUDGE"].split(",")) if "GGEMS_B200_JUDGE" in os.environ else (3, 80))
 
 
 def _lib():
@@ -345,6 +353,23 @@ class Geometry:
         h = hist.reshape(n, 2, side, side)
         return h[:, 0].astype(np.float32), h[:, 1].astype(np.float32)
 
+    def finish_simulation_device(self, run):
+        """finish_simulation without the copy to the host: CUDA float32 tensors
+        [n, side, side] built from the context's histogram buffers."""
+        import torch
+        from ._native import check
+        from .distributed import device_tallies
+        lib, n, side = self.lib, run["n"], self.side
+        check(lib.gg_synchronize(self.ctx), "gg_synchronize")
+        ms, la = C.c_float(), C.c_int64()
+        lib.gg_last_run_stats(self.ctx, C.byref(ms), C.byref(la))
+        self.last_ms = ms.value
+        hist = device_tallies(self.ctx)[:run["nh"]]
+        if not run["totals"]:
+            return None, torch.stack(hist[1:]).to(torch.float32).view(n, side, side)
+        h = torch.stack(hist).to(torch.float32).view(n, 2, side, side)
+        return h[:, 0], h[:, 1]
+
     def simulate(self, projections, primaries, seed=777, totals=True):
         """start_simulation + finish_simulation."""
         return self.finish_simulation(self.start_simulation(projections, primaries, seed, totals))
@@ -391,6 +416,17 @@ def judge(predicted, low_count_mc, tolerance=JUDGE_TOLERANCE):
         out.append(p if keep else m)
         verdict.append(JUDGE_NETWORK if keep else JUDGE_MC)
     return np.stack(out), np.array(verdict)
+
+
+def judge_device(predicted, low_count_mc, tolerance=JUDGE_TOLERANCE):
+    """judge() on CUDA tensors [n, side, side] (integrated scatter summed in
+    FP64): (outputs as a CUDA tensor, verdicts as a host array)."""
+    import torch
+    sp = predicted.to(torch.float64).sum(dim=(1, 2))
+    sm = low_count_mc.to(torch.float64).sum(dim=(1, 2))
+    keep = (sp - sm).abs() <= tolerance * sm.clamp(min=1e-12)
+    out = torch.where(keep[:, None, None], predicted, low_count_mc)
+    return out, np.where(keep.cpu().numpy(), JUDGE_NETWORK, JUDGE_MC)
 
 
 def judge_rescaled(predicted, low_count_mc, primaries, side=None, tolerance=JUDGE_TOLERANCE, shape_blocks=4,
@@ -493,17 +529,24 @@ def train(net, inputs, targets, epochs, lr=1e-3, seed=0):
     return losses
 
 
-def predict(net, inputs):
+def predict_device(net, inputs):
+    """The network's scatter estimates of host `inputs` [n, side, side, 2] as a
+    CUDA tensor: one copy to the device, the forward passes back to back over
+    batches of net.batch."""
     import torch
-    out = []
-    B = net.batch
-    for s in range(0, len(inputs), B):
-        xb = np.zeros((B,) + inputs.shape[1:], np.float32)
-        m = min(B, len(inputs) - s)
-        xb[:m] = inputs[s:s + m]
-        y = net.forward(torch.from_numpy(xb).cuda()).cpu().numpy()
-        out.append(y[:m] * getattr(net, "target_scale", 1.0))
-    return np.concatenate(out)
+    B, n = net.batch, len(inputs)
+    X = torch.from_numpy(np.ascontiguousarray(inputs, np.float32)).cuda()
+    out = torch.empty((n, net.side, net.side), dtype=torch.float32, device=X.device)
+    for s in range(0, n, B):
+        m = min(B, n - s)
+        xb = X[s:s + B] if m == B else torch.cat([X[s:], X.new_zeros((B - m,) + tuple(X.shape[1:]))])
+        out[s:s + m] = net.forward(xb)[:m]
+    return out * getattr(net, "target_scale", 1.0)
+
+
+def predict(net, inputs):
+    """predict_device, copied to the host."""
+    return predict_device(net, inputs).cpu().numpy()
 
 
 # (C_in, C_out, down-sampling factor) of the 14 3x3 convolutions (csrc/gg_unet.cu)
@@ -596,27 +639,32 @@ def surrogate_pipeline(geo, net, projections, judge_primaries, seed):
     t = [time.perf_counter()]
     # the MC estimates run on the transport context's stream while the
     # projector (its own context) and the network (its own stream) work
-    # The judge MC runs three CTAs per SM instead of the four that fit: the
-    # registers left on every SM let the projector's and the network's kernels
-    # run beside it instead of after it.
+    # beside them, in the registers the judge's launch shape leaves free on
+    # every SM (JUDGE_BLOCKS_PER_SM, JUDGE_STASH_REGISTERS).
     from ._native import check
     bps, lanes, ratio4 = C.c_int32(), C.c_int32(), C.c_int32()
+    stash, swap, rnd = C.c_int32(), C.c_int32(), C.c_int32()
     check(geo.lib.gg_get_transport_tuning(geo.ctx, C.byref(bps), C.byref(lanes), C.byref(ratio4)), "tuning")
+    check(geo.lib.gg_get_transport_stash(geo.ctx, C.byref(stash), C.byref(swap), C.byref(rnd)), "stash")
     check(geo.lib.gg_set_transport_tuning(geo.ctx, JUDGE_BLOCKS_PER_SM, lanes.value, ratio4.value), "tuning")
+    check(geo.lib.gg_set_transport_stash(geo.ctx, JUDGE_STASH_REGISTERS, swap.value, rnd.value), "stash")
     try:
         run = geo.start_simulation(projections, int(judge_primaries), seed=seed, totals=False)
     finally:
         check(geo.lib.gg_set_transport_tuning(geo.ctx, bps.value, lanes.value, ratio4.value), "tuning")
+        check(geo.lib.gg_set_transport_stash(geo.ctx, stash.value, swap.value, rnd.value), "stash")
     t.append(time.perf_counter())
     x = make_inputs(geo, projections)
     t.append(time.perf_counter())
-    pred = predict(net, x)  # host arrays: the network's own stream is synchronised
+    pred_d = predict_device(net, x)
     t.append(time.perf_counter())
-    _, low = geo.finish_simulation(run)
-    low = normalise(low, judge_primaries, geo.side)
+    _, low_d = geo.finish_simulation_device(run)
+    low_d = normalise(low_d, judge_primaries, geo.side)
     t.append(time.perf_counter())
-    final, used = judge(pred, low)
+    final_d, used = judge_device(pred_d, low_d)
+    final = final_d.cpu().numpy()  # the scan's output, on the host
     t.append(time.perf_counter())
+    pred, low = pred_d.cpu().numpy(), low_d.cpu().numpy()
     geo.last_rescaled = judge_rescaled(pred, low, judge_primaries, geo.side)
     geo.last_breakdown = {"judge_mc_launch": t[1] - t[0], "inputs": t[2] - t[1], "network": t[3] - t[2],
                           "judge_mc_wait": t[4] - t[3], "judge": t[5] - t[4]}

@@ -177,6 +177,28 @@ def test_surrogate_beats_low_count_mc(geometry, torch):
     net.close()
 
 
+def test_device_judge_matches_host_judge(geometry, torch):
+    """The scan's device path (histograms read on the GPU, normalised, judged
+    there) gives the host path's counts, estimates and verdicts."""
+    from ggems_b200 import scatter as S
+    rng = np.random.default_rng(9)
+    side = 64
+    projs = [(float(rng.uniform(0, 360)), S.random_phantom(rng)) for _ in range(6)]
+    run = geometry.start_simulation(projs, 200_000, seed=31, totals=False)
+    _, low_d = geometry.finish_simulation_device(run)
+    _, low_h = geometry.simulate(projs, 200_000, seed=31, totals=False)
+    assert np.array_equal(low_d.cpu().numpy(), low_h)
+    low_h = S.normalise(low_h, 200_000, side)
+    low_d = S.normalise(low_d, 200_000, side)
+    # estimates 2 % off the MC (kept) and 10 % off (replaced), clear of the 5 % band
+    pred = np.stack([low_h[k] * (1.02 if k % 2 == 0 else 1.10) for k in range(len(projs))]).astype(np.float32)
+    out_h, used_h = S.judge(pred, low_h)
+    out_d, used_d = S.judge_device(torch.from_numpy(pred).cuda(), low_d)
+    assert np.array_equal(used_h, used_d)
+    assert list(used_h) == [S.JUDGE_NETWORK, S.JUDGE_MC] * 3
+    assert np.array_equal(out_d.cpu().numpy(), out_h)
+
+
 def test_committed_network_predicts_new_phantoms(tmp_path):
     """The trained network shipped with the package (ggems_b200/data/
     unet_scatter256.npz, loaded by bench.py's surrogate measurement) at its own
