@@ -1331,13 +1331,20 @@ GG_API int gg_line_integrals_batch(gg_context* c, const gg_solid* phantom, const
   GG_CUDA(cudaSetDevice(c->device));
   const size_t n = static_cast<size_t>(ex) * ey;
   const size_t nv = static_cast<size_t>(phantom->number_of_voxels[0]) * phantom->number_of_voxels[1] * phantom->number_of_voxels[2];
+  // `inputs` in this device's memory: the kernels write it directly
+  cudaPointerAttributes pa{};
+  const bool on_device = cudaPointerGetAttributes(&pa, inputs) == cudaSuccess &&
+                         (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged) && pa.device == c->device;
+  cudaGetLastError();  // a host pointer unknown to CUDA is not an error here
   // stream-ordered buffers: no device-wide synchronisation (cudaFree would wait
   // for transport running on other streams)
   float *dmu = nullptr, *dout = nullptr;
   uint8_t* dlab = nullptr;
   cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&dmu), number_of_materials * sizeof(float), c->stream);
   if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void**>(&dlab), nv, c->stream);
-  if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void**>(&dout), 2 * n * count * sizeof(float), c->stream);
+  if (e == cudaSuccess && !on_device)
+    e = cudaMallocAsync(reinterpret_cast<void**>(&dout), 2 * n * count * sizeof(float), c->stream);
+  float* const target = on_device ? inputs : dout;
   auto cleanup = [&]() {
     if (dmu) cudaFreeAsync(dmu, c->stream);
     if (dlab) cudaFreeAsync(dlab, c->stream);
@@ -1363,12 +1370,13 @@ GG_API int gg_line_integrals_batch(gg_context* c, const gg_solid* phantom, const
     std::memcpy(P.source, source_positions + 3 * k, sizeof(P.source));
     P.mu = dmu;
     P.labels = dlab;
-    P.out = dout + 2 * n * k;
+    P.out = target + 2 * n * k;
     P.network_input = 1;
     gg::launch_line_integrals(P, c->stream);
     e = cudaGetLastError();
   }
-  if (e == cudaSuccess) e = cudaMemcpyAsync(inputs, dout, 2 * n * count * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && !on_device)
+    e = cudaMemcpyAsync(inputs, dout, 2 * n * count * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
   cleanup();
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return fail(GG_ERROR_CUDA, std::string("line integrals: ") + cudaGetErrorString(e));

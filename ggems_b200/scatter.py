@@ -269,10 +269,15 @@ class Geometry:
             raise RuntimeError(lib.gg_last_error().decode())
         return out.reshape(self.side, self.side)
 
-    def network_inputs(self, projections):
+    def network_inputs(self, projections, device=False):
         """[n, side, side, 2] FP32 network inputs (exp(-L), L): one batched
-        projector call per run of projections that share a phantom."""
-        out = np.empty((len(projections), self.side, self.side, 2), np.float32)
+        projector call per run of projections that share a phantom; a CUDA
+        tensor written in place with device=True, else a host array."""
+        if device:
+            import torch
+            out = torch.empty((len(projections), self.side, self.side, 2), dtype=torch.float32, device="cuda")
+        else:
+            out = np.empty((len(projections), self.side, self.side, 2), np.float32)
         lib = _lib()
         k = 0
         while k < len(projections):
@@ -287,9 +292,10 @@ class Geometry:
                 src, ph, det = self.projection(projections[j][0], labels, 0)
                 dets[j - k] = det
                 pos[j - k] = (src.matrix[3], src.matrix[7], src.matrix[11])
+            target = C.cast(C.c_void_p(out[k:e].data_ptr()), C.POINTER(C.c_float)) if device \
+                else abi.ptr(out[k:e], C.c_float)
             rc = lib.gg_line_integrals_batch(self.projector_ctx, C.byref(ph), dets, abi.ptr(pos, C.c_float), e - k,
-                                             abi.ptr(self.mu, C.c_float), len(self.mu),
-                                             abi.ptr(out[k:e], C.c_float))
+                                             abi.ptr(self.mu, C.c_float), len(self.mu), target)
             if rc != 0:
                 raise RuntimeError(lib.gg_last_error().decode())
             k = e
@@ -395,9 +401,10 @@ def smooth(img, blocks=32):
     return np.repeat(np.repeat(block_mean(img, blocks), b, axis=-2), b, axis=-1).astype(np.float32)
 
 
-def make_inputs(geometry, projections):
-    """[n, side, side, 2]: primary transmission exp(-L) and line integral L."""
-    return geometry.network_inputs(projections)
+def make_inputs(geometry, projections, device=False):
+    """[n, side, side, 2]: primary transmission exp(-L) and line integral L
+    (a CUDA tensor with device=True, else a host array)."""
+    return geometry.network_inputs(projections, device)
 
 
 # Verdicts of the judge, per projection.
@@ -530,12 +537,12 @@ def train(net, inputs, targets, epochs, lr=1e-3, seed=0):
 
 
 def predict_device(net, inputs):
-    """The network's scatter estimates of host `inputs` [n, side, side, 2] as a
-    CUDA tensor: one copy to the device, the forward passes back to back over
-    batches of net.batch."""
+    """The network's scatter estimates of `inputs` [n, side, side, 2] (a host
+    array, copied up once, or a CUDA tensor) as a CUDA tensor: the forward
+    passes back to back over batches of net.batch."""
     import torch
     B, n = net.batch, len(inputs)
-    X = torch.from_numpy(np.ascontiguousarray(inputs, np.float32)).cuda()
+    X = inputs if torch.is_tensor(inputs) else torch.from_numpy(np.ascontiguousarray(inputs, np.float32)).cuda()
     out = torch.empty((n, net.side, net.side), dtype=torch.float32, device=X.device)
     for s in range(0, n, B):
         m = min(B, n - s)
@@ -654,7 +661,7 @@ def surrogate_pipeline(geo, net, projections, judge_primaries, seed):
         check(geo.lib.gg_set_transport_tuning(geo.ctx, bps.value, lanes.value, ratio4.value), "tuning")
         check(geo.lib.gg_set_transport_stash(geo.ctx, stash.value, swap.value, rnd.value), "stash")
     t.append(time.perf_counter())
-    x = make_inputs(geo, projections)
+    x = make_inputs(geo, projections, device=True)
     t.append(time.perf_counter())
     pred_d = predict_device(net, x)
     t.append(time.perf_counter())

@@ -362,7 +362,9 @@ GG_API int gg_line_integrals(gg_context* context, const gg_solid* phantom, const
                              float* line_integrals);
 /* The same for `count` projections of one phantom (a scan): detectors[count]
  * and source_positions[count][3], written as the surrogate network's input,
- * inputs[count][ey][ex][2] = (exp(-L), L) (host array, FP32). */
+ * inputs[count][ey][ex][2] = (exp(-L), L) (FP32; a host array, or an array in
+ * the context's device memory, which the kernels then write directly).  Returns
+ * once the inputs are written. */
 GG_API int gg_line_integrals_batch(gg_context* context, const gg_solid* phantom, const gg_solid* detectors,
                                    const float* source_positions, int32_t count, const float* mu,
                                    int32_t number_of_materials, float* inputs);

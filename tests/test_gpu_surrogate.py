@@ -177,6 +177,19 @@ def test_surrogate_beats_low_count_mc(geometry, torch):
     net.close()
 
 
+def test_device_inputs_match_host_inputs(geometry, torch):
+    """The projector writes the same network inputs into device memory as into
+    a host array."""
+    from ggems_b200 import scatter as S
+    rng = np.random.default_rng(10)
+    projs = [(float(rng.uniform(0, 360)), S.random_phantom(rng)) for _ in range(3)]
+    projs += [(float(rng.uniform(0, 360)), projs[0][1]) for _ in range(2)]
+    host = S.make_inputs(geometry, projs)
+    dev = S.make_inputs(geometry, projs, device=True)
+    assert torch.is_tensor(dev) and dev.is_cuda
+    assert np.array_equal(dev.cpu().numpy(), host)
+
+
 def test_device_judge_matches_host_judge(geometry, torch):
     """The scan's device path (histograms read on the GPU, normalised, judged
     there) gives the host path's counts, estimates and verdicts."""
