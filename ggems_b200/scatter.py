@@ -669,7 +669,11 @@ def surrogate_pipeline(geo, net, projections, judge_primaries, seed):
     low_d = normalise(low_d, judge_primaries, geo.side)
     t.append(time.perf_counter())
     final_d, used = judge_device(pred_d, low_d)
-    final = final_d.cpu().numpy()  # the scan's output, on the host
+    # the scan's output, on the host (page-locked: torch's host allocator keeps
+    # the block for the next scan once this one is released)
+    final = torch.empty(final_d.shape, dtype=final_d.dtype, pin_memory=True)
+    final.copy_(final_d)
+    final = final.numpy()
     t.append(time.perf_counter())
     pred, low = pred_d.cpu().numpy(), low_d.cpu().numpy()
     geo.last_rescaled = judge_rescaled(pred, low, judge_primaries, geo.side)
