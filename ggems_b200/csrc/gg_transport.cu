@@ -42,10 +42,15 @@ constexpr float kEps6 = 1.0e-06f;                         // GGEMSGeometryConsta
 constexpr float kOutOfWorld = FLT_MAX;                    // GGEMSParticleConstants.hh:44
 constexpr int kNoProcess = 99;
 constexpr float kRayleighFactor = 32526509815670243328.0f;  // GGEMSRayleighScatteringModels.hh:36
-// KissUniform's (float)((double)x / 4294967295.0 * (1 - 2^-23)) equals
-// (float)((double)x * kKissScale) for every float x = (float)(uint32): checked
-// exhaustively over all 83,886,080 such values (tests/test_rng.py).
-constexpr double kKissScale = (1.0 / 4294967295.0) * 0.99999988079071044921875;
+// KissUniform's (float)((double)x / 4294967295.0 * (1 - 2^-23)) equals, for
+// every float x = (float)(uint32), the single-precision fused multiply-add
+// fma(x, kKissCorrection, x * 2^-32): x * 2^-32 is exact and
+// x * kKissCorrection + x * 2^-32 = x * 2^-32 * (1 - 2^-23 + 2^-32) is rounded
+// once, which lands on the same float as the reference's double arithmetic for
+// all 83,886,080 such x (checked exhaustively in tests/test_rng.py, against
+// the division and against the double product).
+constexpr float kKissTwoToMinus32 = 0x1p-32f;
+constexpr float kKissCorrection = -0x1.ffp-56f;  // -(2^-23 - 2^-32) * 2^-32, exact in float
 
 enum Phase : int { kNewHistory = 0, kFind = 1, kTrackVoxel = 2, kTrackBox = 3, kTrackMesh = 4, kInteract = 5, kDone = 6 };
 
@@ -203,7 +208,8 @@ struct Kiss {
     s5 = t < 0;
     s4 = static_cast<uint32_t>(t) & 2147483647u;
     s1 += 1411392427u;
-    return __double2float_rn(static_cast<double>(__uint2float_rn(s1 + s2 + s4)) * kKissScale);
+    const float x = __uint2float_rn(s1 + s2 + s4);
+    return __fmaf_rn(x, kKissCorrection, x * kKissTwoToMinus32);
   }
 };
 

@@ -4,8 +4,9 @@
   the C++ standard's 10000th-output check, the product's seeding against
   numpy's MT19937, and the per-device skip.
 * KissUniform's double division (GGEMSKissEngine.hh:72-74) replaced by one
-  double multiply on the GPU: checked over every float value a uint32 sum
-  can round to (83,886,080 values).
+  double multiply, and that by one single-precision fused multiply-add (the
+  GPU's form): both checked over every float value a uint32 sum can round to
+  (83,886,080 values).
 * JKISS sequence: the oracle's and the product's state after N draws.
 """
 
@@ -64,6 +65,26 @@ def test_kiss_scale_is_exact():
         assert np.array_equal(ref, fast)
         n += x.size
     assert n == 83886081  # includes 2^32 (the rounding of 0xffffffff)
+
+
+def test_kiss_scale_single_precision_fma_is_exact():
+    """The transport kernel's form: fma(x, c, x * 2^-32) in float32 with
+    c = -(2^-23 - 2^-32) * 2^-32.  x * c + x * 2^-32 = (2^32 - 511) m 2^(k-64)
+    for x = m 2^k (m < 2^24) needs at most 56 bits, so it is exact in x87
+    extended precision (64 bits) and one cast to float32 is the fused
+    multiply-add's single rounding."""
+    c = float.fromhex("-0x1.ffp-56")
+    assert c == -(2.0 ** -23 - 2.0 ** -32) * 2.0 ** -32 and float(np.float32(c)) == c
+    assert np.finfo(np.longdouble).nmant >= 63
+    k = 1.0 - 2.0 ** -23
+    n = 0
+    for x in _float_values_of_uint32():
+        ref = ((x / 4294967295.0) * k).astype(np.float32)
+        y = (x.astype(np.float32) * np.float32(2.0 ** -32)).astype(np.longdouble)
+        fma = (x.astype(np.longdouble) * np.longdouble(c) + y).astype(np.float32)
+        assert np.array_equal(ref, fma)
+        n += x.size
+    assert n == 83886081
 
 
 def _kiss_numpy(state, draws):
