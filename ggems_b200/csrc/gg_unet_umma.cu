@@ -240,6 +240,187 @@ __global__ void __launch_bounds__(kThreads, 1) conv_umma_kernel(const __grid_con
   if (threadIdx.x == 0 && cta_error) atomicExch(a.error, 1);
 }
 
+// Row-streaming 3x3 convolution for images whose width is a multiple of 128.
+// A CTA owns `rows` (R) consecutive output rows of one 128-pixel row segment
+// and keeps one TMEM accumulator (128 lanes x N columns) per output row.  Per
+// input-channel chunk it loads the chunk's weights of all 9 taps once (one
+// 3-D TMA box, double-buffered across chunks), then streams the input rows
+// y0-1 .. y0+R, each as ONE 130-pixel tile (pixels x0-1 .. x0+128; TMA's zero
+// fill supplies the padding outside the image).  The three x-taps of a row
+// are the same tile addressed 0, 1 and 2 pixel rows in: the shared-memory
+// swizzle is a function of the absolute address, so a K-major descriptor may
+// start at any 128/64/32-byte row of a tile written by TMA (matrix base offset
+// 0); the tile is padded to 136 rows so that every read stays inside it.
+// Each input row feeds the up-to-three output rows it touches (y-taps), so an
+// activation tile is written (R+2)/R times per output row instead of 9 times.
+// An MMA costs max(N/2, operand bytes / 128) cycles here, so the single
+// issuing thread keeps per-MMA work to a few adds on precomputed descriptors.
+template <int kMode, int KC>
+__global__ void __launch_bounds__(kThreads, 1) conv_rows_kernel(const __grid_constant__ CUtensorMap tmx,
+                                                             const __grid_constant__ CUtensorMap tmw, ConvArgs a) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem = smem_raw + ((1024 - (smem_addr(smem_raw) & 1023)) & 1023);
+  const int S = a.stages, R = a.rows, N = a.n_tile;
+  unsigned char* wbuf = smem;                                        // 2 x w_bytes
+  unsigned char* ring = smem + 2 * static_cast<size_t>(a.w_bytes);  // S x a_tile_bytes
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ring + static_cast<size_t>(S) * a.a_tile_bytes);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + S;
+  uint64_t* wfull = bars + 2 * S;
+  uint64_t* wempty = bars + 2 * S + 2;
+  uint64_t* acc = bars + 2 * S + 4;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc + 1);
+  __shared__ int cta_error;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int segs = a.width / 128, groups = a.height / R;
+  const int seg = blockIdx.x % segs, t = blockIdx.x / segs;
+  const int grp = t % groups, b0 = t / groups;
+  const int x0 = seg * 128, y0 = grp * R;
+  const int n0 = blockIdx.y * N;
+
+  if (threadIdx.x == 0) {
+    cta_error = 0;
+    for (int i = 0; i < 2 * S + 5; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bars + i)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                 "r"(a.tmem_cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  const int per_chunk = R + 2;  // input rows per chunk
+  const uint32_t a_tx = static_cast<uint32_t>(a.a_bytes);
+  const uint32_t w_tx = static_cast<uint32_t>(9 * N * KC * 2);
+  if (warp == 0 && lane == 0) {
+    // ---- producer: per chunk the 9-tap weight box, then the input rows ----
+    int issued = 0, w_issued = 0;
+    bool ok = true;
+    for (int c = 0; c < a.chunks && ok; ++c) {
+      const int wb = c & 1;
+      if (c >= 2 && !wait_parity(smem_addr(wempty + wb), ((c >> 1) + 1) & 1, a.error)) {
+        ok = false;
+        break;
+      }
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(wfull + wb)), "r"(w_tx)
+                   : "memory");
+      tma_load_3d(smem_addr(wbuf + wb * static_cast<size_t>(a.w_bytes)), &tmw, c * KC, n0, 0, smem_addr(wfull + wb));
+      ++w_issued;
+      for (int j = 0; j < per_chunk; ++j) {
+        const int it = c * per_chunk + j;
+        const int s = it % S;
+        if (it >= S && !wait_parity(smem_addr(empty + s), ((it / S) + 1) & 1, a.error)) {
+          ok = false;
+          break;
+        }
+        const uint32_t bar = smem_addr(full + s);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(a_tx) : "memory");
+        tma_load_4d(smem_addr(ring + static_cast<size_t>(s) * a.a_tile_bytes), &tmx, c * KC, x0 - 1, y0 - 1 + j, b0,
+                    bar);
+        ++issued;
+      }
+    }
+    if (!ok) atomicExch(&cta_error, 1);
+    // copies still in flight land before the CTA can end
+    for (int it = issued > S ? issued - S : 0; it < issued; ++it)
+      if (!wait_parity(smem_addr(full + it % S), (it / S) & 1, a.error)) atomicExch(&cta_error, 1);
+    for (int c = w_issued > 2 ? w_issued - 2 : 0; c < w_issued; ++c)
+      if (!wait_parity(smem_addr(wfull + (c & 1)), (c >> 1) & 1, a.error)) atomicExch(&cta_error, 1);
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer ----
+    // descriptors advance by constant steps (start address field = address / 16)
+    const uint64_t ring_desc = smem_desc(smem_addr(ring), KC * 2);
+    const uint64_t w_desc[2] = {smem_desc(smem_addr(wbuf), KC * 2),
+                                smem_desc(smem_addr(wbuf + a.w_bytes), KC * 2)};
+    const uint64_t stage_step = static_cast<uint64_t>(a.a_tile_bytes >> 4);
+    const uint64_t tap_step = static_cast<uint64_t>((N * KC * 2) >> 4);
+    constexpr uint64_t kRowStep = (KC * 2) >> 4;  // one pixel row of the tile
+    bool ok = true;
+    for (int c = 0; c < a.chunks && ok; ++c) {
+      const int wb = c & 1;
+      if (!wait_parity(smem_addr(wfull + wb), (c >> 1) & 1, a.error)) {
+        ok = false;
+        break;
+      }
+      const uint64_t wd = w_desc[wb];
+      for (int j = 0; j < per_chunk; ++j) {
+        const int it = c * per_chunk + j;
+        const int s = it % S;
+        if (!wait_parity(smem_addr(full + s), (it / S) & 1, a.error)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint64_t ad = ring_desc + static_cast<uint64_t>(s) * stage_step;
+#pragma unroll
+        for (int ky = 0; ky < 3; ++ky) {
+          const int r = j - ky;  // output row y0 + r takes input row y0 - 1 + j through y-tap ky
+          if (r < 0 || r >= R) continue;
+          const uint32_t d = tmem + static_cast<uint32_t>(r * N);
+          const uint32_t fresh = (c == 0 && ky == 0) ? 1u : 0u;  // this row's first MMA starts its accumulator
+#pragma unroll
+          for (int kx = 0; kx < 3; ++kx) {
+            const uint64_t bd = wd + static_cast<uint64_t>(3 * ky + kx) * tap_step;
+            const uint64_t axd = ad + static_cast<uint64_t>(kx) * kRowStep;
+#pragma unroll
+            for (int k = 0; k < KC / 16; ++k)
+              umma_f16(d, axd + 2 * k, bd + 2 * k, a.idesc, (fresh && kx == 0 && k == 0) ? 0u : 1u);
+          }
+        }
+        umma_commit(smem_addr(empty + s));
+      }
+      umma_commit(smem_addr(wempty + wb));
+    }
+    if (ok) umma_commit(smem_addr(acc));
+    else atomicExch(&cta_error, 1);
+  }
+  __syncwarp();
+
+  // ---- epilogue: TMEM lanes 32*warp .. +31 = pixels x0 + 32*warp + lane; columns r*N .. = row y0 + r ----
+  const bool ready = wait_parity(smem_addr(acc), 0, a.error);
+  if (!ready) atomicExch(&cta_error, 1);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (!cta_error) {
+    const int x = x0 + warp * 32 + lane;
+    for (int r = 0; r < R; ++r) {
+      const long long pixel = (static_cast<long long>(b0) * a.height + (y0 + r)) * a.width + x;
+      for (int cb = 0; cb < N / 32; ++cb) {
+        float v[32];
+        tmem_load_32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(r * N + cb * 32), v);
+        const int co = n0 + cb * 32;
+        if (kMode == 0) {
+          __align__(16) __nv_bfloat162 h[16];
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const float lo = fmaxf(v[2 * q] + a.bias[co + 2 * q], 0.0f);
+            const float hi = fmaxf(v[2 * q + 1] + a.bias[co + 2 * q + 1], 0.0f);
+            h[q] = __floats2bfloat162_rn(lo, hi);
+          }
+          uint4* dst = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(a.y) + pixel * a.cout + co);
+          const uint4* src = reinterpret_cast<const uint4*>(h);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) dst[q] = src[q];
+        } else {
+          float4* dst = reinterpret_cast<float4*>(static_cast<float*>(a.y) + pixel * a.cout + co);
+#pragma unroll
+          for (int q = 0; q < 8; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.tmem_cols));
+  if (threadIdx.x == 0 && cta_error) atomicExch(a.error, 1);
+}
+
 // 32 lanes x 16 columns of FP32 from TMEM into 16 registers per thread.
 __device__ __forceinline__ void tmem_load_16(uint32_t taddr, float (&v)[16]) {
   uint32_t r[16];
@@ -413,6 +594,77 @@ int pow2_at_least(int v, int lo) {
 
 bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
 
+// Plan of the row-streaming kernel (width a multiple of 128).  Rows per CTA:
+// R x N TMEM columns <= 256 so that two CTAs fit an SM (knob
+// GGEMS_B200_CONV_ROWS: rows per CTA, a power of two; 0 selects the tile
+// kernel); chunks of 64 / 32 / 16 channels, the widest whose two weight buffers
+// and a ring of at least 3 row tiles fit two CTAs per SM (one if none does).
+const char* make_rows_plan(ConvPlan* p, const void* x, const void* w, int batch, int height, int width, int cin,
+                           int cout, int rows_knob, PFN_cuTensorMapEncodeTiled_v12000 fn) {
+  ConvArgs& a = p->args;
+  a.n_tile = cout <= 256 ? cout : (cout % 128 == 0 ? 128 : 64);
+  if (cout % a.n_tile != 0 || a.n_tile % 32 != 0) return "unsupported output channel count";
+  const int N = a.n_tile;
+  int R = rows_knob > 0 ? rows_knob : 256 / N;
+  while (R > 1 && R * N > 512) R >>= 1;
+  if (R < 1) R = 1;
+  if (R > height) R = height;
+  if ((R & (R - 1)) != 0 || R * N > 512) return "rows per CTA must be a power of two with rows x channels <= 512";
+  a.rows = R;
+  a.tmem_cols = pow2_at_least(R * N, 32);
+  auto w_bytes = [&](int kc) { return ((9 * N * kc * 2 + 1023) / 1024) * 1024; };
+  auto tile_bytes = [&](int kc) { return ((136 * kc * 2 + 1023) / 1024) * 1024; };
+  const int budgets[2] = {110 * 1024, 200 * 1024};  // two CTAs per SM, else one
+  a.kc = 0;
+  for (int budget : budgets) {
+    for (int kc : {64, 32, 16}) {
+      if (cin % kc != 0) continue;
+      if (2 * w_bytes(kc) + 3 * tile_bytes(kc) <= budget) {
+        a.kc = kc;
+        break;
+      }
+    }
+    if (a.kc) {
+      a.stages = (budget - 2 * w_bytes(a.kc)) / tile_bytes(a.kc);
+      break;
+    }
+  }
+  if (a.kc == 0) return "weights of a chunk do not fit in shared memory";
+  if (a.stages > 8) a.stages = 8;
+  a.chunks = cin / a.kc;
+  a.w_bytes = w_bytes(a.kc);
+  a.a_tile_bytes = tile_bytes(a.kc);
+  a.a_bytes = 130 * a.kc * 2;  // the 130 pixels TMA writes
+  a.b_bytes = 9 * N * a.kc * 2;
+  a.stage_bytes = a.a_tile_bytes;
+  p->smem = 2 * static_cast<size_t>(a.w_bytes) + static_cast<size_t>(a.stages) * a.a_tile_bytes +
+            (2 * a.stages + 5) * 8 + 16 + 1024;
+  const size_t tmem_cap_smem = 228 * 1024 / (512 / a.tmem_cols + 1) + 1;
+  if (p->smem < tmem_cap_smem) p->smem = tmem_cap_smem;
+  if (p->smem > 227 * 1024) return "row kernel does not fit in shared memory";
+  a.idesc = gg::umma_idesc_bf16_f32(128, N, false, false);
+  cuuint32_t ones[4] = {1, 1, 1, 1};
+  cuuint64_t xd[4] = {static_cast<cuuint64_t>(cin), static_cast<cuuint64_t>(width), static_cast<cuuint64_t>(height),
+                      static_cast<cuuint64_t>(batch)};
+  cuuint64_t xs[3] = {static_cast<cuuint64_t>(cin) * 2, static_cast<cuuint64_t>(width) * cin * 2,
+                      static_cast<cuuint64_t>(height) * width * cin * 2};
+  cuuint32_t xbox[4] = {static_cast<cuuint32_t>(a.kc), 130, 1, 1};
+  if (fn(&p->tmap_x, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(x), xd, xs, xbox, ones,
+         CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_for(a.kc * 2), CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return "activation tensor map rejected";
+  cuuint64_t wd[3] = {static_cast<cuuint64_t>(cin), static_cast<cuuint64_t>(cout), 9};
+  cuuint64_t ws[2] = {static_cast<cuuint64_t>(cin) * 2, static_cast<cuuint64_t>(cout) * cin * 2};
+  cuuint32_t wbox[3] = {static_cast<cuuint32_t>(a.kc), static_cast<cuuint32_t>(N), 9};
+  if (fn(&p->tmap_w, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(w), wd, ws, wbox, ones,
+         CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_for(a.kc * 2), CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return "weight tensor map rejected";
+  p->grid_m = batch * (height / R) * (width / 128);
+  p->grid_n = cout / N;
+  return nullptr;
+}
+
 }  // namespace
 
 const char* make_plan(ConvPlan* p, const void* x, const void* w, int batch, int height, int width, int cin, int cout) {
@@ -427,6 +679,11 @@ const char* make_plan(ConvPlan* p, const void* x, const void* w, int batch, int 
   a.cin = cin;
   a.cout = cout;
   a.pixels = static_cast<long long>(batch) * height * width;
+  static const int rows_knob = [] {
+    const char* e = std::getenv("GGEMS_B200_CONV_ROWS");
+    return e ? std::atoi(e) : -1;
+  }();
+  if (width % 128 == 0 && rows_knob != 0) return make_rows_plan(p, x, w, batch, height, width, cin, cout, rows_knob, fn);
   a.kc = cin % 64 == 0 ? 64 : (cin % 32 == 0 ? 32 : 16);
   a.n_tile = cout <= 256 ? cout : (cout % 128 == 0 ? 128 : 64);
   if (cout > 256 && cout % a.n_tile != 0) return "unsupported output channel count";
@@ -498,7 +755,15 @@ cudaError_t launch(const ConvPlan& p, int mode, const float* bias, void* y, int*
   a.y = y;
   a.error = error;
   dim3 grid(p.grid_m, p.grid_n);
-  if (mode == 0) {
+  if (a.rows > 0) {
+    using K = void (*)(const CUtensorMap, const CUtensorMap, ConvArgs);
+    K k = nullptr;
+    if (a.kc == 64) k = mode == 0 ? conv_rows_kernel<0, 64> : conv_rows_kernel<1, 64>;
+    else if (a.kc == 32) k = mode == 0 ? conv_rows_kernel<0, 32> : conv_rows_kernel<1, 32>;
+    else k = mode == 0 ? conv_rows_kernel<0, 16> : conv_rows_kernel<1, 16>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(p.smem));
+    k<<<grid, kThreads, p.smem, stream>>>(p.tmap_x, p.tmap_w, a);
+  } else if (mode == 0) {
     cudaFuncSetAttribute(conv_umma_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(p.smem));
     conv_umma_kernel<0><<<grid, kThreads, p.smem, stream>>>(p.tmap_x, p.tmap_w, a);
   } else {

@@ -23,6 +23,11 @@ struct ConvArgs {
   int stages;         // shared-memory ring depth
   int a_tile_bytes, a_bytes, b_bytes, stage_bytes;
   uint32_t idesc;     // tcgen05.mma instruction descriptor
+  // row-streaming kernel (rows > 0, images at least 128 pixels wide): a CTA
+  // computes `rows` output rows of one 128-pixel row segment
+  int rows;           // output rows per CTA (0: the tile kernel)
+  int chunks;         // cin / kc
+  int w_bytes;        // one weight buffer: 9 taps x n_tile x kc BF16 (1024-aligned)
   const float* bias;  // mode 0 only
   void* y;            // mode 0: BF16 [pixels][cout]; mode 1: FP32 [pixels][cout]
   int* error;         // set to 1 when a wait gave up
@@ -37,7 +42,8 @@ struct ConvPlan {
 };
 
 // x: [batch][height][width][cin] BF16, w: [9][cout][cin] BF16 (device).
-// Returns NULL, or why the shape is not supported.
+// Images whose width is a multiple of 128 use the row-streaming kernel, the
+// others the tile kernel.  Returns NULL, or why the shape is not supported.
 const char* make_plan(ConvPlan* plan, const void* x, const void* w, int batch, int height, int width, int cin, int cout);
 
 // mode 0: y = relu(conv + bias) as BF16; mode 1: y = conv as FP32.
