@@ -340,6 +340,17 @@ def surrogate_measurement(tmp, angles=360, reference_every=10):
                        "reference_primaries": 1e9, "training": "2000 MC pairs at 1e8 primaries, 60 epochs"}}
 
 
+def _pinned(n, dtype):
+    """A zeroed page-locked host array (torch's host allocator), so that the
+    end-to-end copies run at DMA speed as a caller with pinned buffers gets."""
+    import numpy as np
+    import torch
+    dtype = np.dtype(dtype)
+    tdt = {np.dtype(np.int32): torch.int32, np.dtype(np.uint32): torch.int32, np.dtype(np.float64): torch.float64,
+           np.dtype(np.float32): torch.float32, np.dtype(np.int16): torch.int16}[dtype]
+    return torch.zeros(int(n), dtype=tdt, pin_memory=True).numpy().view(dtype)
+
+
 def _transport_launch(lib, ctx):
     """The transport kernel's launch knobs on this context."""
     v = [C.c_int32() for _ in range(8)]
@@ -492,9 +503,11 @@ def main():
     # ---- end to end through the C ABI: host scene -> device, run, tallies -> host ----
     sc = scene_ptr.contents
     hs = [int(sc.histogram_sizes[i]) for i in range(sc.number_of_histograms)]
-    tallies = abi.Tallies(hs, [])
-    states = rank_states if rank_states is not None else np.frombuffer(
-        C.string_at(lib.ggems_initial_random_states(ggems.obj, 0), 5 * abi.GG_MAXIMUM_PARTICLES * 4), np.uint32).copy()
+    # inputs and results in page-locked host memory
+    tallies = abi.Tallies(hs, [], alloc=_pinned)
+    states = _pinned(5 * abi.GG_MAXIMUM_PARTICLES, np.uint32)
+    states[:] = rank_states if rank_states is not None else np.frombuffer(
+        C.string_at(lib.ggems_initial_random_states(ggems.obj, 0), 5 * abi.GG_MAXIMUM_PARTICLES * 4), np.uint32)
     h2d = sum(int(sc.solids[i].number_of_voxels[0]) * sc.solids[i].number_of_voxels[1] * sc.solids[i].number_of_voxels[2]
               for i in range(sc.number_of_solids) if sc.solids[i].type == abi.GG_SOLID_VOXELIZED)
     for i in range(sc.number_of_tables):
@@ -906,7 +919,7 @@ def run_water(args, tmp, rank):
     import torch
     dm = sc.dose_maps[0]
     nd = int(dm.total_number_of_dosels)
-    dose, unc = np.empty(nd, np.float32), np.empty(nd, np.float32)
+    dose, unc = _pinned(nd, np.float32), _pinned(nd, np.float32)  # page-locked results
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
     def check(rc, what):
@@ -932,9 +945,10 @@ def run_water(args, tmp, rank):
             launches += k
     total_ms = sum(times)
     value = n * args.steps / (total_ms * 1e-3)
-    states = np.frombuffer(C.string_at(lib.ggems_initial_random_states(ggems.obj, 0), 5 * abi.GG_MAXIMUM_PARTICLES * 4),
-                           np.uint32).copy()
-    tallies = abi.Tallies([], [nd])
+    states = _pinned(5 * abi.GG_MAXIMUM_PARTICLES, np.uint32)
+    states[:] = np.frombuffer(C.string_at(lib.ggems_initial_random_states(ggems.obj, 0),
+                                          5 * abi.GG_MAXIMUM_PARTICLES * 4), np.uint32)
+    tallies = abi.Tallies([], [nd], alloc=_pinned)
     e2e = []
     for k in range(args.steps + 1):
         t0 = time.perf_counter()

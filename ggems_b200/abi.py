@@ -152,12 +152,13 @@ class Particles:
 class Tallies:
     """Host tally buffers matching a scene's histograms and dose maps."""
 
-    def __init__(self, histogram_sizes, dose_sizes, world_size=0):
-        self.histograms = [np.zeros(n, np.int32) for n in histogram_sizes]
-        self.edep = [np.zeros(n, np.float64) for n in dose_sizes]
-        self.edep_squared = [np.zeros(n, np.float64) for n in dose_sizes]
-        self.hit = [np.zeros(n, np.int32) for n in dose_sizes]
-        self.photon_tracking = [np.zeros(n, np.int32) for n in dose_sizes]
+    def __init__(self, histogram_sizes, dose_sizes, world_size=0, alloc=np.zeros):
+        """alloc(n, dtype) makes each zeroed host array (e.g. page-locked memory)."""
+        self.histograms = [alloc(n, np.int32) for n in histogram_sizes]
+        self.edep = [alloc(n, np.float64) for n in dose_sizes]
+        self.edep_squared = [alloc(n, np.float64) for n in dose_sizes]
+        self.hit = [alloc(n, np.int32) for n in dose_sizes]
+        self.photon_tracking = [alloc(n, np.int32) for n in dose_sizes]
 
         def arr(lst, ctype):
             a = (C.POINTER(ctype) * max(len(lst), 1))(*[ptr(x, ctype) for x in lst])

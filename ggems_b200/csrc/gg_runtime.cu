@@ -1426,6 +1426,27 @@ GG_API int gg_last_run_stats(gg_context* c, float* milliseconds, int64_t* kernel
   return GG_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// n int64 fixed-point tallies (LSB 2^-32 MeV) into the caller's doubles: the
+// integers land in the caller's array itself (same size), whose page-locked
+// memory the copy then uses if it is, and are converted in place.
+cudaError_t read_fixed_point(double* dst, const unsigned long long* src, size_t n) {
+  cudaError_t e = cudaMemcpy(dst, src, n * 8, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return e;
+  long long* q = reinterpret_cast<long long*>(dst);
+  for (size_t i = 0; i < n; ++i) {
+    long long v;
+    std::memcpy(&v, q + i, sizeof(v));
+    dst[i] = static_cast<double>(v) / gg::kEdepScale;
+  }
+  return cudaSuccess;
+}
+}  // namespace
+
+extern "C" {
+
 GG_API int gg_read_tallies(gg_context* c, gg_tally_buffers* t) {
   if (!c || !t) return fail(GG_ERROR_INVALID_ARGUMENT, "NULL argument");
   if (!c->scene_ready) return fail(GG_ERROR_STATE, "no scene uploaded");
@@ -1437,11 +1458,7 @@ GG_API int gg_read_tallies(gg_context* c, gg_tally_buffers* t) {
   for (size_t d = 0; d < c->dose_host.size(); ++d) {
     const gg::DevDoseMap& m = c->dose_host[d];
     const size_t n = static_cast<size_t>(m.total_number_of_dosels);
-    if (t->edep && t->edep[d]) {
-      std::vector<long long> q(n);
-      GG_CUDA(cudaMemcpy(q.data(), m.edep, n * 8, cudaMemcpyDeviceToHost));
-      for (size_t i = 0; i < n; ++i) t->edep[d][i] = static_cast<double>(q[i]) / gg::kEdepScale;
-    }
+    if (t->edep && t->edep[d]) GG_CUDA(read_fixed_point(t->edep[d], m.edep, n));
     if (t->edep_squared && t->edep_squared[d] && m.edep_squared)
       GG_CUDA(cudaMemcpy(t->edep_squared[d], m.edep_squared, n * 8, cudaMemcpyDeviceToHost));
     if (t->hit && t->hit[d] && m.hit) GG_CUDA(cudaMemcpy(t->hit[d], m.hit, n * 4, cudaMemcpyDeviceToHost));
@@ -1449,12 +1466,7 @@ GG_API int gg_read_tallies(gg_context* c, gg_tally_buffers* t) {
       GG_CUDA(cudaMemcpy(t->photon_tracking[d], m.photon_tracking, n * 4, cudaMemcpyDeviceToHost));
   }
   const size_t w = c->world_cells;
-  auto read_fixed = [&](double* dst, const unsigned long long* src) -> cudaError_t {
-    std::vector<long long> q(w);
-    cudaError_t e = cudaMemcpy(q.data(), src, w * 8, cudaMemcpyDeviceToHost);
-    for (size_t i = 0; e == cudaSuccess && i < w; ++i) dst[i] = static_cast<double>(q[i]) / gg::kEdepScale;
-    return e;
-  };
+  auto read_fixed = [&](double* dst, const unsigned long long* src) { return read_fixed_point(dst, src, w); };
   if (t->world_photon_tracking && c->world_photon)
     GG_CUDA(cudaMemcpy(t->world_photon_tracking, c->world_photon, w * 4, cudaMemcpyDeviceToHost));
   if (t->world_energy && c->world_energy) GG_CUDA(read_fixed(t->world_energy, c->world_energy));
