@@ -41,10 +41,10 @@ JUDGE_TOLERANCE = 0.05
 # Launch shape of the judge MC, a persistent kernel that holds its SMs for the
 # whole scan: transport CTAs per SM and the photon stash's register budget (0:
 # off); GGEMS_B200_JUDGE="blocks,registers" overrides both.  Measured on the
-# 360-angle scan (projections/s): 3 CTAs with the 80-register stash 657, with
-# the 64-register one 589, without the stash 577; 2 CTAs (more room for the
-# network's kernels beside it) 534 / 521 / 345: a slower MC costs more than
-# the overlap gains.
+# 360-angle scan (projections/s): 3 CTAs with the 80-register stash 1,030, with
+# the 64-register one 906, 4 CTAs with the 64-register stash 893-982, without
+# the stash 925; 2 CTAs (more room for the network's kernels beside it) were
+# slower still: the network mostly runs after the MC.
 JUDGE_BLOCKS_PER_SM, JUDGE_STASH_REGISTERS = (
     tuple(int(v) for v in os.environ["GGEMS_B200_JUDGE"].split(",")) if "GGEMS_B200_JUDGE" in os.environ else (3, 80))
 
