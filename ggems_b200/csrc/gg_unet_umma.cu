@@ -268,8 +268,8 @@ __global__ void __launch_bounds__(kThreads, 1) conv_rows_kernel(const __grid_con
   uint64_t* empty = bars + S;
   uint64_t* wfull = bars + 2 * S;
   uint64_t* wempty = bars + 2 * S + 2;
-  uint64_t* acc = bars + 2 * S + 4;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc + 1);
+  uint64_t* acc = bars + 2 * S + 4;  // one per output row: its accumulator is complete
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc + R);
   __shared__ int cta_error;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -281,7 +281,8 @@ __global__ void __launch_bounds__(kThreads, 1) conv_rows_kernel(const __grid_con
 
   if (threadIdx.x == 0) {
     cta_error = 0;
-    for (int i = 0; i < 2 * S + 5; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bars + i)));
+    for (int i = 0; i < 2 * S + 4 + R; ++i)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bars + i)));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncwarp();
@@ -374,22 +375,28 @@ __global__ void __launch_bounds__(kThreads, 1) conv_rows_kernel(const __grid_con
           }
         }
         umma_commit(smem_addr(empty + s));
+        // In the last chunk, input row j brings output row j - 2 its last tap:
+        // that row's accumulator is complete once these MMAs are, and its
+        // epilogue can run while the later rows still load and multiply.
+        if (c == a.chunks - 1 && j >= 2) umma_commit(smem_addr(acc + (j - 2)));
       }
       umma_commit(smem_addr(wempty + wb));
     }
-    if (ok) umma_commit(smem_addr(acc));
-    else atomicExch(&cta_error, 1);
+    if (!ok) atomicExch(&cta_error, 1);
   }
   __syncwarp();
 
-  // ---- epilogue: TMEM lanes 32*warp .. +31 = pixels x0 + 32*warp + lane; columns r*N .. = row y0 + r ----
-  const bool ready = wait_parity(smem_addr(acc), 0, a.error);
-  if (!ready) atomicExch(&cta_error, 1);
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  __syncthreads();
-  if (!cta_error) {
+  // ---- epilogue, row by row as the rows complete: TMEM lanes 32*warp .. +31 =
+  // pixels x0 + 32*warp + lane; columns r*N .. = row y0 + r ----
+  {
     const int x = x0 + warp * 32 + lane;
     for (int r = 0; r < R; ++r) {
+      // warp-uniform, so that the warp's tcgen05.ld below stays converged
+      if (!__all_sync(0xffffffffu, wait_parity(smem_addr(acc + r), 0, a.error))) {
+        atomicExch(&cta_error, 1);
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const long long pixel = (static_cast<long long>(b0) * a.height + (y0 + r)) * a.width + x;
       for (int cb = 0; cb < N / 32; ++cb) {
         float v[32];
@@ -638,7 +645,7 @@ const char* make_rows_plan(ConvPlan* p, const void* x, const void* w, int batch,
   a.b_bytes = 9 * N * a.kc * 2;
   a.stage_bytes = a.a_tile_bytes;
   p->smem = 2 * static_cast<size_t>(a.w_bytes) + static_cast<size_t>(a.stages) * a.a_tile_bytes +
-            (2 * a.stages + 5) * 8 + 16 + 1024;
+            (2 * a.stages + 4 + R) * 8 + 16 + 1024;
   const size_t tmem_cap_smem = 228 * 1024 / (512 / a.tmem_cols + 1) + 1;
   if (p->smem < tmem_cap_smem) p->smem = tmem_cap_smem;
   if (p->smem > 227 * 1024) return "row kernel does not fit in shared memory";
